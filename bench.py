@@ -1,0 +1,389 @@
+"""Benchmark of the KinectFusion per-frame path (one step = one depth frame).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config c2]
+
+Workload (default): 640x480 uint16 depth, 512^3 int16+uint16 TSDF over a 3 m
+cube, 3-level ICP (10/5/4), bilateral filter sigma_s 4.5 px / sigma_r 30 mm,
+seeded synthetic room of 20 boxes and spheres with axial noise and 2 %
+dropout. Every frame is tracked against the model of the previous one, fused
+and raycast. `value` is frames/s with the depth frames resident in HBM; `e2e`
+is the same loop through the C-ABI with pinned host depth copied in and the
+pose copied out every frame. The volume (512 MiB) is larger than L2.
+
+Multi-GPU: the path does not shard a single sequence; N GPUs run N independent
+sequences (different seeds), one process per GPU, no collective on the frame
+path (weak scaling); timing is the max over ranks.
+
+`--impl reference` runs the CPU implementation of the same equations (the
+FP32 OpenMP build of the oracle restatement) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "frames/s 640x480 @512³ vol, plain vs learned-warm-start ICP at equal pose error"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index),
+                                      f"--query-gpu={self.Q}", "--format=csv,noheader,nounits"],
+                                     capture_output=True, text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def pose_errors(hist, gt):
+    rots, trans = [], []
+    for P, G in zip(hist, gt):
+        R = P[:3, :3].T @ G[:3, :3]
+        rots.append(float(np.arccos(np.clip((np.trace(R) - 1) / 2, -1, 1))))
+        trans.append(float(np.linalg.norm(P[:3, 3] - G[:3, 3])))
+    return rots, trans
+
+
+# ------------------------------------------------------------- CPU baseline
+
+def cpu_frames_per_s(cfg, seq, seconds: float, max_frames: int):
+    """FP32 OpenMP build of the oracle restatement on the host cores."""
+    from oracle import CpuTracker, Oracle
+    o = Oracle("f32")
+    tr = CpuTracker(o, cfg, seq.poses[0])
+    tr.process(seq.depth[0])      # frame 0 (fuse only) is not timed
+    n, t0 = 0, time.perf_counter()
+    while n < max_frames and (n < 3 or time.perf_counter() - t0 < seconds):
+        tr.process(seq.depth[1 + n])
+        n += 1
+    dt = time.perf_counter() - t0
+    tr.close()
+    return n / dt, n, dt, o.threads()
+
+
+# ------------------------------------------------------------------- arms
+
+def run_reference(args, cfg, world, rank):
+    if rank != 0:
+        return
+    import openfusion_b200 as of
+    frames = 1 + args.warmup + args.steps
+    seq = of.make_sequence(cfg, frames=min(frames, 1 + args.warmup + args.steps))
+    from oracle import CpuTracker, Oracle
+    o = Oracle("f32")
+    tr = CpuTracker(o, cfg, seq.poses[0])
+    tr.process(seq.depth[0])
+    t_w = time.perf_counter()
+    for k in range(args.warmup):
+        tr.process(seq.depth[1 + k])
+    per = (time.perf_counter() - t_w) / max(1, args.warmup)
+    # keep the whole run within a few minutes: time at most ~150 s of frames
+    steps = args.steps
+    if per > 0 and steps * per > 150.0:
+        steps = max(3, int(150.0 / per))
+    t0 = time.perf_counter()
+    for k in range(steps):
+        tr.process(seq.depth[1 + args.warmup + k])
+    dt = time.perf_counter() - t0
+    tr.close()
+    fps = steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": fps, "unit": "frames/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * dt / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded analytic room scene)",
+        "config": {"workload": cfg.name, "width": cfg.width, "height": cfg.height,
+                   "volume": f"{cfg.resolution}^3 over {cfg.size_mm / 1000:g} m",
+                   "icp_iters": list(cfg.iters), "frames_requested": args.steps},
+        "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": o.threads(), "kind": "port",
+                         "sample": f"{steps} consecutive frames of the same sequence after "
+                                   f"{args.warmup} warm-up frames (FP32 OpenMP restatement)"},
+        "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, cfg, world, rank, local):
+    import torch
+    import openfusion_b200 as of
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if rank:
+        import dataclasses
+        cfg = dataclasses.replace(cfg, seed=cfg.seed + 7919 * rank)
+    frames = 1 + args.warmup + args.steps
+    seq = of.make_sequence(cfg, frames=frames)
+    depth_dev = torch.from_numpy(seq.depth.astype(np.int16)).to(dev)
+    depth_host = torch.from_numpy(seq.depth.astype(np.int16)).pin_memory()
+    stream = torch.cuda.current_stream(dev)
+
+    # ---- device-resident loop: value
+    tr = of.Tracker(cfg, seq.poses[0], use_graph=True, pose_history=frames)
+    tr.process(depth_dev[0])
+    for k in range(args.warmup):
+        tr.process(depth_dev[1 + k])
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    with sampler:
+        ev0.record(stream)
+        for k in range(args.steps):
+            tr.process(depth_dev[1 + args.warmup + k])
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms, world)
+    bufs = tr.buffers()
+    kernels = bufs.kernels_track * args.steps
+    hist = tr.pose_history(frames)
+    _, st = tr.pose()
+    tr.close()
+    rots, trans = pose_errors(hist, seq.poses)
+
+    # ---- end to end through the C-ABI: pinned host depth in, pose out
+    tr = of.Tracker(cfg, seq.poses[0], use_graph=True, pose_history=frames)
+    pose_out = torch.zeros((frames, 16), dtype=torch.float64).pin_memory()
+    tr.process(depth_host[0])
+    for k in range(args.warmup):
+        tr.process(depth_host[1 + k])
+        tr.pose(out=pose_out[1 + k])
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
+    for k in range(args.steps):
+        i = 1 + args.warmup + k
+        tr.process(depth_host[i])
+        tr.pose(out=pose_out[i])
+    ev3.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = max_over_ranks(ev2.elapsed_time(ev3), world)
+    e2e_hist = pose_out.numpy().reshape(frames, 4, 4)
+    assert np.allclose(e2e_hist[1 + args.warmup:], hist[1 + args.warmup:], atol=1e-6), \
+        "end-to-end poses differ from the device-resident run"
+    tr.close()
+
+    # ---- per-stage kernel times (stage-wise launches with CUDA events)
+    stages = stage_times(of, cfg, seq, depth_dev, args, dev)
+
+    fps = world * args.steps / (ms_max / 1e3)
+    e2e_fps = world * args.steps / (e2e_ms / 1e3)
+    if rank != 0:
+        return
+    peak, peak_kind = peaks()
+    integ_bytes = stages["integrate_alg_bytes"]
+    achieved = integ_bytes / (stages["integrate_ms"] / 1e3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "integrate_traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    line = {
+        "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded analytic room scene, axial noise + 2% dropout)",
+        "config": {"workload": cfg.name, "width": cfg.width, "height": cfg.height,
+                   "volume": f"{cfg.resolution}^3 int16+uint16 over {cfg.size_mm / 1000:g} m",
+                   "icp": "3 levels, 10/5/4 iterations, plain (no warm start)",
+                   "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (512 MiB volume)"},
+        "stages_ms": {k: v for k, v in stages.items() if k.endswith("_ms")},
+        "pose_error": {"max_rot_deg": float(np.degrees(max(rots))),
+                       "max_trans_mm": float(max(trans)),
+                       "mean_trans_mm": float(np.mean(trans)),
+                       "last_icp_status": int(st.status), "last_inliers": int(st.inliers)},
+        "roofline": {"kernel": "k_integrate", "bound": "hbm", "achieved": achieved,
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "alg_bytes_per_launch": integ_bytes},
+        "e2e": {"value": e2e_fps, "unit": "frames/s",
+                "h2d_bytes_per_step": cfg.width * cfg.height * 2, "d2h_bytes_per_step": 128},
+        "gpu_launches": kernels,
+        "clocks": sampler.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        cps, n, dt, cores = cpu_frames_per_s(cfg, seq, args.cpu_seconds, frames - 1)
+        line["cpu_baseline"] = {"value": cps, "unit": "frames/s", "cores": cores, "kind": "port",
+                                "sample": f"{n} consecutive frames ({dt:.1f} s) of the same "
+                                          "sequence, FP32 OpenMP restatement"}
+    print(json.dumps(line), flush=True)
+
+
+def stage_times(of, cfg, seq, depth_dev, args, dev):
+    """Average device time of each stage, launched stage by stage on the
+    current stream and bracketed by CUDA events, over the same frames."""
+    import torch
+    vol = of.new_volume(cfg, dev)
+    lam = of.lambda_table(cfg, dev)
+    frame = of.new_pyramid(cfg, dev)
+    model = of.new_pyramid(cfg, dev)
+    ws = of.icp_workspace(cfg, dev)
+    pose = torch.tensor(seq.poses[0].reshape(16), dtype=torch.float64, device=dev)
+    of.integrate(cfg, vol, depth_dev[0], pose, lam)
+    of.raycast(cfg, vol, pose, model)
+    acc = {"preprocess": 0.0, "icp": 0.0, "integrate": 0.0, "raycast": 0.0}
+    s = torch.cuda.current_stream(dev)
+    poses = [pose.clone()]
+    n = 0
+    for k in range(1, 1 + args.warmup + args.steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+        ev[0].record(s)
+        of.preprocess(cfg, depth_dev[k], frame)
+        ev[1].record(s)
+        of.icp_track(cfg, frame, model, pose, ws)
+        ev[2].record(s)
+        of.integrate(cfg, vol, depth_dev[k], pose, lam)
+        ev[3].record(s)
+        of.raycast(cfg, vol, pose, model)
+        ev[4].record(s)
+        poses.append(pose.clone())
+        torch.cuda.synchronize()
+        if k > args.warmup:
+            for i, name in enumerate(acc):
+                acc[name] += ev[i].elapsed_time(ev[i + 1])
+            n += 1
+    # Algorithmic bytes of one integration launch: 4 B read + 4 B write per
+    # updated voxel plus 2 B per depth pixel. The census launch counts the
+    # updated voxels with the same decisions and no writes; it replays the
+    # same frames at the same poses on a second volume, outside any timing.
+    vol2 = of.new_volume(cfg, dev)
+    upd = []
+    for k in range(0, 1 + args.warmup + args.steps):
+        if k > args.warmup:
+            upd.append(of.integrate_census(cfg, vol2, depth_dev[k], poses[k], lam))
+        of.integrate(cfg, vol2, depth_dev[k], poses[k], lam)
+    out = {f"{k}_ms": v / max(n, 1) for k, v in acc.items()}
+    out["integrate_alg_bytes"] = 8.0 * float(np.mean(upd)) + 2.0 * cfg.width * cfg.height
+    out["integrate_updated_voxels"] = float(np.mean(upd))
+    del vol, vol2
+    torch.cuda.empty_cache()
+    return out
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup()
+    import openfusion_b200 as of
+    cfg = of.CONFIGS[args.config]
+    try:
+        if args.impl == "reference":
+            run_reference(args, cfg, world, rank)
+        else:
+            run_ours(args, cfg, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,282 @@
+/*
+ * openfusion_b200.h -- C-ABI of the B200 (sm_100a) KinectFusion per-frame path.
+ *
+ * Plain C: no CUDA or torch types. Every device pointer is a plain pointer
+ * into CUDA device memory of the current device; every stream argument is a
+ * cudaStream_t passed as `of_stream_t` (NULL = legacy default stream). Every
+ * entry point returns an `of_status_t`; none of them exits the process.
+ *
+ * Conventions (kept from the reference so that its callers see the same
+ * numbers):
+ *   - units are millimetres;
+ *   - camera space is the reference's: a pixel (u, v) with depth D > 0 (mm)
+ *     back-projects to X = -D (u - cx) / fx, Y = -D (v - cy) / fy, Z = -D
+ *     (Source/include/CudaUtilities.cuh:24-33, CameraHandler.cu:87), and
+ *     projects as u = fx X / Z + cx (CudaUtilities.cuh:9-21);
+ *   - a pose is a row-major 4x4 camera-to-world matrix, kept in FP64 on the
+ *     device (the reference keeps it as float[16], Source/src/MainApp.cpp:613);
+ *   - the TSDF cube of edge `size_mm` is centred at the world origin and voxel
+ *     (i, j, k) has its centre at -size/2 + (i + 0.5) size/N
+ *     (Source/src/VolumeIntegrator.cu:40-48).
+ *
+ * Memory is owned by the caller, as in the reference, where RunApp allocates
+ * every shared buffer (Source/src/MainApp.cpp:591-647): `*_bytes` queries give
+ * the sizes. The tracker object (of_tracker_*) is the exception: it owns the
+ * whole per-frame state, like RunApp, and replays the frame as a CUDA graph.
+ */
+#ifndef OPENFUSION_B200_H_
+#define OPENFUSION_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OF_ABI_VERSION 1
+
+typedef int32_t of_status_t;
+#define OF_OK 0
+#define OF_ERR_INVALID_ARGUMENT 1 /* a size, pointer or parameter is out of range */
+#define OF_ERR_CUDA 2             /* a CUDA runtime call failed */
+#define OF_ERR_OUT_OF_MEMORY 3    /* the tracker could not allocate device memory */
+#define OF_ERR_NOT_READY 4        /* called in the wrong order (e.g. track before the first frame) */
+#define OF_ERR_TOO_LARGE 5        /* a size beyond a fixed maximum of the entry point */
+
+typedef void *of_stream_t; /* cudaStream_t */
+
+/* TSDF storage of one voxel: one 32-bit word, low half tsdf, high half weight. */
+#define OF_TSDF_I16 0 /* int16 tsdf/trunc * 32767 + uint16 weight */
+#define OF_TSDF_F16 1 /* IEEE half tsdf/trunc + uint16 weight */
+
+/* Replaces CameraParams (Source/include/BasicTypes.h:88-103); only the fields
+ * the fusion path reads (CameraHandler.cu:80-87, VolumeIntegrator.cu:131). */
+typedef struct of_camera {
+  int32_t width;
+  int32_t height;
+  float fx, fy, cx, cy;  /* m_intrinsic, pixels */
+  float min_depth_mm;    /* m_min_depth */
+  float max_depth_mm;    /* m_max_depth */
+} of_camera_t;
+
+/* Replaces the compile-time worldVolume / VOLUME_SIZE / TRUNCATION /
+ * MAX_WEIGHT constants (Source/include/Constants.h:23-55). */
+typedef struct of_volume_desc {
+  int32_t resolution; /* N voxels per edge; multiple of 8, 8..2048 */
+  int32_t storage;    /* OF_TSDF_I16 or OF_TSDF_F16 */
+  float size_mm;      /* cube edge */
+  float trunc_mm;     /* truncation distance */
+  int32_t max_weight; /* running-average weight cap, 1..65535 */
+  int32_t reserved;
+} of_volume_desc_t;
+
+/* Depth pre-processing (no reference counterpart: bilateral filter of
+ * Tomasi & Manduchi 1998 and the KinectFusion depth pyramid). */
+typedef struct of_filter_params {
+  float sigma_space_px; /* 4.5 */
+  float sigma_range_mm; /* 30 */
+  int32_t radius_px;    /* window half-width; 0 = ceil(2 sigma_space) */
+  int32_t levels;       /* pyramid levels, 1..4 */
+} of_filter_params_t;
+
+/* Ray marching (replaces the fixed constants of Source/src/Raycaster.cu:109-112). */
+typedef struct of_raycast_params {
+  float min_step_vox;    /* smallest march step, voxels (0.75) */
+  float far_step_frac;   /* step as a fraction of tsdf*trunc when far from the surface (0.8) */
+  int32_t refine_iters;  /* regula-falsi refinements of the zero crossing (3) */
+  int32_t reserved;
+} of_raycast_params_t;
+
+/* ICP (replaces ICP_ITERATIONS, DISTANCE_THRESHOLD, NORMAL_THRESHOLD,
+ * Source/include/Constants.h:48-50). */
+typedef struct of_icp_params {
+  int32_t levels;          /* 1..4 */
+  int32_t iters[4];        /* iterations per level, finest level first: {10, 5, 4} */
+  float dist_thresh_mm;    /* 25 */
+  float normal_thresh;     /* cosine, 0.65 */
+} of_icp_params_t;
+
+/* Per-frame ICP result, written by the device. */
+typedef struct of_icp_stats {
+  int32_t status;        /* 0 = tracked; 1 = singular system, pose restored (ICP.cpp:152-158) */
+  int32_t inliers;       /* correspondences of the last iteration run */
+  int32_t iterations;    /* iterations run */
+  int32_t reserved;
+  double residual_sq;    /* sum of squared point-to-plane residuals, mm^2, last iteration */
+  double min_pivot;      /* smallest Cholesky pivot / largest diagonal, last iteration */
+} of_icp_stats_t;
+
+/* Device layout of a pre-processed frame and of a raycast model: per pyramid
+ * level l (0 = finest, W_l = ceil(W / 2^l)), a 256-byte aligned block. */
+typedef struct of_pyramid_layout {
+  int32_t levels;
+  int32_t width[4];
+  int32_t height[4];
+  size_t depth_offset[4];  /* float depth, mm (frame only; 0 = invalid) */
+  size_t points_offset[4]; /* float4 [2 * W_l * H_l]: vertex (x, y, z, valid), normal (x, y, z, valid) */
+  size_t total_bytes;
+} of_pyramid_layout_t;
+
+/* ---- library --------------------------------------------------------- */
+
+int32_t of_abi_version(void);
+const char *of_status_string(of_status_t status);
+/* Fills defaults for every parameter block (the values of the full-size
+ * 640x480 / 512^3 configuration). Any pointer may be NULL. */
+void of_default_params(of_filter_params_t *filter, of_raycast_params_t *raycast,
+                       of_icp_params_t *icp);
+/* Intrinsics of pyramid level `level` (fx/2^l, cx_{l+1} = (cx_l - 0.5) / 2). */
+of_status_t of_camera_level(const of_camera_t *cam, int32_t level, of_camera_t *out);
+
+/* ---- volume (replaces General::InitVoxelArray, General.cpp:42-49) ----- */
+
+/* Bytes of a volume: N^3 x 4 (8^3-voxel bricks, brick-major). */
+of_status_t of_volume_bytes(const of_volume_desc_t *desc, size_t *bytes);
+/* Resets every voxel to weight 0 (tsdf reads as +trunc), replacing
+ * d_initVoxelArray (Source/src/General.cu:27-50). */
+of_status_t of_volume_reset(const of_volume_desc_t *desc, void *d_volume, of_stream_t stream);
+/* Writes the volume in the reference's layout: float tsdf in mm and the
+ * weight, index x*N*N + y*N + z (Source/src/MainApp.cpp:181-276 dumps the
+ * same float array). Either output may be NULL. */
+of_status_t of_volume_export(const of_volume_desc_t *desc, const void *d_volume,
+                             float *d_tsdf_mm, uint16_t *d_weight, of_stream_t stream);
+/* Overwrites the volume from the reference layout (for resume / import). */
+of_status_t of_volume_import(const of_volume_desc_t *desc, void *d_volume,
+                             const float *d_tsdf_mm, const uint16_t *d_weight,
+                             of_stream_t stream);
+
+/* ---- pre-processing (replaces CameraHandler::updateCameraData,
+ *      Source/src/CameraSupport/CameraHandler.cu:134-143) ----------------- */
+
+of_status_t of_pyramid_layout(const of_camera_t *cam, int32_t levels, of_pyramid_layout_t *out);
+/* uint16 depth (mm, row pitch `pitch_px` pixels) -> bilateral-filtered depth
+ * pyramid + camera-space vertex and normal maps at every level, into
+ * `d_frame` (of_pyramid_layout). Invalid depth (outside [min, max]) is 0. */
+of_status_t of_preprocess(const of_camera_t *cam, const of_filter_params_t *filter,
+                          const uint16_t *d_depth, int32_t pitch_px, void *d_frame,
+                          of_stream_t stream);
+
+/* ---- integration (replaces VolumeIntegrator::Integrate,
+ *      Source/src/VolumeIntegrator.cu:86-201) ---------------------------- */
+
+/* Fuses the raw depth frame into the volume at pose `d_pose` (device,
+ * FP64 4x4 camera-to-world). `d_lambda` is the per-pixel ray-length table
+ * of of_lambda_table (device, float2 [W * H]). */
+of_status_t of_integrate(const of_volume_desc_t *desc, void *d_volume, const of_camera_t *cam,
+                         const uint16_t *d_depth, int32_t pitch_px, const double *d_pose,
+                         const float *d_lambda, of_stream_t stream);
+/* Bytes of the ray-length table (W * H * 8). */
+of_status_t of_lambda_bytes(const of_camera_t *cam, size_t *bytes);
+/* Fills the table: for every pixel, sqrt(1 + ((u-cx)/fx)^2 + ((v-cy)/fy)^2)
+ * as an unevaluated float pair (hi, lo), computed in FP64. */
+of_status_t of_lambda_table(const of_camera_t *cam, float *d_lambda, of_stream_t stream);
+/* Counts the voxels one of_integrate call would update (same decisions, no
+ * volume write). `d_count` is one device uint64. */
+of_status_t of_integrate_census(const of_volume_desc_t *desc, const void *d_volume,
+                                const of_camera_t *cam, const uint16_t *d_depth,
+                                int32_t pitch_px, const double *d_pose, const float *d_lambda,
+                                unsigned long long *d_count, of_stream_t stream);
+
+/* ---- raycast (replaces Raycaster::Raycast, Source/src/Raycaster.cu:97-242) */
+
+/* Casts one ray per pixel of level 0 from pose `d_pose` and writes world-space
+ * vertex/normal maps into `d_model` (of_pyramid_layout; only points_offset
+ * is used), then fills levels 1.. by guarded 2x2 averaging. `d_rgba` (may be
+ * NULL) receives the reference's shaded image (Raycaster.cu:214-228). */
+of_status_t of_raycast(const of_volume_desc_t *desc, const void *d_volume, const of_camera_t *cam,
+                       const of_raycast_params_t *params, int32_t levels, const double *d_pose,
+                       void *d_model, uint32_t *d_rgba, of_stream_t stream);
+
+/* ---- ICP (replaces ICP::Iterate_ICP, Source/src/ICP.cpp:84-182, with the
+ *      correspondence kernel of Source/src/ICP.cu:116-251) --------------- */
+
+of_status_t of_icp_workspace_bytes(const of_camera_t *cam, size_t *bytes);
+/* Refines `d_pose` (device FP64 4x4, in/out) of the frame in `d_frame`
+ * against the model `d_model`, coarse to fine, all on the device: fused
+ * association + point-to-plane rows + compensated 27-value reduction, then
+ * an FP64 6x6 Cholesky solve and SE(3) composition by the last block of
+ * every iteration. `d_stats` (device, may be NULL) gets of_icp_stats_t. */
+of_status_t of_icp_track(const of_camera_t *cam, const of_icp_params_t *params,
+                         const void *d_frame, const void *d_model, double *d_pose,
+                         void *d_workspace, of_icp_stats_t *d_stats, of_stream_t stream);
+/* One FindCorresponding pass (ICP.cu:116-262) at `level`: the 21 upper
+ * J^T J entries (row-major i<=j), 6 J^T r entries, sum r^2 and the inlier
+ * count as 29 floats into `d_system`, for the pose `d_pose`. */
+of_status_t of_icp_system(const of_camera_t *cam, const of_icp_params_t *params, int32_t level,
+                          const void *d_frame, const void *d_model, const double *d_pose,
+                          void *d_workspace, float *d_system, of_stream_t stream);
+
+/* ---- tracker: the whole frame (RunApp::display, MainApp.cpp:786-964) ---- */
+
+typedef struct of_tracker *of_tracker_t;
+
+typedef struct of_tracker_desc {
+  of_camera_t camera;
+  of_volume_desc_t volume;
+  of_filter_params_t filter;
+  of_raycast_params_t raycast;
+  of_icp_params_t icp;
+  double initial_pose[16]; /* camera-to-world of frame 0 */
+  int32_t use_graph;       /* 1 = replay each frame as a captured CUDA graph */
+  int32_t pose_history;    /* frames of pose history kept on the device (0 = 1024) */
+} of_tracker_desc_t;
+
+of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_tracker_t *out);
+of_status_t of_tracker_destroy(of_tracker_t tracker);
+/* Processes one depth frame: frame 0 is fused at the initial pose; every
+ * later frame is tracked against the model of the previous one, then fused
+ * and raycast. `depth_is_host` != 0: `depth` is host memory (pinned for an
+ * asynchronous copy) and is copied on `stream`. */
+of_status_t of_tracker_process(of_tracker_t tracker, const uint16_t *depth, int32_t depth_is_host,
+                               of_stream_t stream);
+/* Sets the starting pose of the next frame's ICP to `pose_delta` x previous
+ * pose (host FP64 4x4, world frame); used for a warm start. NULL clears it. */
+of_status_t of_tracker_set_prior(of_tracker_t tracker, const double *pose_delta);
+/* Copies the current pose (FP64 4x4) to `pose` (host; asynchronous on
+ * `stream` when the buffer is pinned) and, if `stats` != NULL, the last
+ * frame's ICP statistics. */
+of_status_t of_tracker_pose(of_tracker_t tracker, double *pose, of_icp_stats_t *stats,
+                            of_stream_t stream);
+/* Copies the poses of the last `count` frames (oldest first) to host memory. */
+of_status_t of_tracker_pose_history(of_tracker_t tracker, double *poses, int32_t count,
+                                    of_stream_t stream);
+/* Raw device pointers of the tracker's state, for inspection and for the
+ * reference-shaped C++ wrappers. */
+typedef struct of_tracker_buffers {
+  void *volume;
+  void *frame;
+  void *model;
+  double *pose;
+  uint16_t *depth;
+  float *lambda;
+  of_icp_stats_t *stats;
+  int64_t frames;
+  int32_t kernels_first;  /* kernel launches of frame 0's graph */
+  int32_t kernels_track;  /* kernel launches of every later frame's graph */
+} of_tracker_buffers_t;
+of_status_t of_tracker_buffers(of_tracker_t tracker, of_tracker_buffers_t *out);
+
+/* ---- reference-layout adapters (for the reference's PointInfo /
+ *      CameraData: AoS float3, BAD_VERTEX = FLT_MAX, BasicTypes.h:40-49) --- */
+
+/* Level 0 of a model/frame -> AoS float3 maps; invalid vertex = FLT_MAX,
+ * invalid normal = 0. If `d_pose` is not NULL the points are camera-space
+ * and are transformed to world space first (frame maps). */
+of_status_t of_points_to_reference(const of_camera_t *cam, const void *d_pyramid,
+                                   const double *d_pose, float *d_vertex3, float *d_normal3,
+                                   of_stream_t stream);
+/* AoS float3 world maps (reference PointInfo) -> level 0.. of a model. */
+of_status_t of_points_from_reference(const of_camera_t *cam, int32_t levels,
+                                     const float *d_vertex3, const float *d_normal3,
+                                     void *d_model, of_stream_t stream);
+/* float[16] pose <-> FP64 device pose. */
+of_status_t of_pose_from_float(const float *d_pose_f32, double *d_pose, of_stream_t stream);
+of_status_t of_pose_to_float(const double *d_pose, float *d_pose_f32, float *d_inv_pose_f32,
+                             float *d_camera_position3, of_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OPENFUSION_B200_H_ */

@@ -1,0 +1,21 @@
+"""openfusion_b200 -- a from-scratch sm_100a KinectFusion per-frame path.
+
+Pre-processing (bilateral filter, depth pyramid, vertex/normal maps), TSDF
+integration, raycasting and multi-level point-to-plane ICP run as hand-written
+CUDA kernels behind the C-ABI of include/openfusion_b200.h; this package is the
+Python mirror of the reference's per-frame interfaces over that ABI.
+"""
+from . import _native
+from .api import (CONFIGS, Config, Sequence, Tracker, icp_system, icp_track, icp_workspace,
+                  integrate, integrate_census, lambda_table, level_camera, linear_to_volume,
+                  make_scene, make_sequence, make_trajectory, new_pyramid, new_volume,
+                  preprocess, pyramid_layout, raycast, render, unpack_depth, unpack_points,
+                  volume_bytes, volume_to_linear)
+
+__all__ = [
+    "CONFIGS", "Config", "Sequence", "Tracker", "icp_system", "icp_track", "icp_workspace",
+    "integrate", "integrate_census", "lambda_table", "level_camera", "linear_to_volume",
+    "make_scene", "make_sequence", "make_trajectory", "new_pyramid", "new_volume", "preprocess",
+    "pyramid_layout", "raycast", "render", "unpack_depth", "unpack_points", "volume_bytes",
+    "volume_to_linear",
+]

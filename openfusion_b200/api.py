@@ -1,0 +1,358 @@
+"""Python mirror of the reference's per-frame interfaces over the C-ABI.
+
+The reference exposes VolumeIntegrator::Integrate, Raycaster::Raycast,
+ICP::Iterate_ICP and CameraHandler::updateCameraData over raw device
+pointers (Source/include/VolumeIntegrator.h:9-17, Raycaster.h:6-13,
+ICP.h:50-70, CameraHandler.h:24). Here the same stages take torch CUDA
+tensors (device memory and streams only) and call the CUDA library; the
+`Tracker` is the whole frame loop of RunApp::display (MainApp.cpp:786-964).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+
+STORAGE = {"i16": 0, "f16": 1}
+
+
+@dataclass
+class Config:
+    """One workload: camera, volume and algorithm parameters."""
+    name: str
+    width: int
+    height: int
+    fx: float
+    fy: float
+    cx: float
+    cy: float
+    resolution: int
+    size_mm: float
+    trunc_mm: float
+    max_weight: int = 128
+    storage: str = "i16"
+    min_depth_mm: float = 300.0
+    max_depth_mm: float = 5000.0
+    sigma_space_px: float = 4.5
+    sigma_range_mm: float = 30.0
+    radius_px: int = 0
+    levels: int = 3
+    iters: tuple = (10, 5, 4)
+    dist_thresh_mm: float = 25.0
+    normal_thresh: float = 0.65
+    min_step_vox: float = 0.75
+    far_step_frac: float = 0.8
+    refine_iters: int = 3
+    scene_kind: int = 1
+    motion: int = 0
+    noise: float = 1.0
+    dropout: float = 0.0
+    frames: int = 300
+    seed: int = 2000
+
+    def camera(self) -> N.Camera:
+        return N.Camera(self.width, self.height, self.fx, self.fy, self.cx, self.cy,
+                        self.min_depth_mm, self.max_depth_mm)
+
+    def volume(self) -> N.VolumeDesc:
+        return N.VolumeDesc(self.resolution, STORAGE[self.storage], self.size_mm, self.trunc_mm,
+                            self.max_weight, 0)
+
+    def filter(self) -> N.FilterParams:
+        return N.FilterParams(self.sigma_space_px, self.sigma_range_mm, self.radius_px,
+                              self.levels)
+
+    def raycast(self) -> N.RaycastParams:
+        return N.RaycastParams(self.min_step_vox, self.far_step_frac, self.refine_iters, 0)
+
+    def icp(self) -> N.IcpParams:
+        it = (C.c_int32 * 4)(*(list(self.iters) + [0] * (4 - len(self.iters))))
+        return N.IcpParams(self.levels, it, self.dist_thresh_mm, self.normal_thresh)
+
+    def radius(self) -> int:
+        return self.radius_px if self.radius_px > 0 else int(np.ceil(2.0 * self.sigma_space_px))
+
+
+# The workloads of the benchmark configurations: C1 small plain method,
+# C2 full-size plain method, C3 precision study (1024^3 fp16), C5 large motion.
+CONFIGS = {
+    "c1": Config("c1_320x240_128^3", 320, 240, 262.5, 262.5, 160.0, 120.0, 128, 2000.0, 60.0,
+                 max_weight=128, scene_kind=0, frames=30, seed=1000, dropout=0.0),
+    "c2": Config("c2_640x480_512^3", 640, 480, 525.0, 525.0, 319.5, 239.5, 512, 3000.0, 30.0,
+                 max_weight=128, scene_kind=1, frames=300, seed=2000, dropout=0.02),
+    "c3": Config("c3_640x480_1024^3_f16", 640, 480, 525.0, 525.0, 319.5, 239.5, 1024, 4000.0,
+                 30.0, max_weight=128, storage="f16", scene_kind=1, frames=300, seed=2000,
+                 dropout=0.02),
+    "c5": Config("c5_640x480_512^3_large_motion", 640, 480, 525.0, 525.0, 319.5, 239.5, 512,
+                 3000.0, 30.0, max_weight=128, scene_kind=1, motion=1, frames=300, seed=5000,
+                 dropout=0.02),
+}
+
+
+def _stream(stream=None) -> int:
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def _ptr(t) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def pyramid_layout(cfg: Config, levels: int | None = None) -> N.PyramidLayout:
+    lay = N.PyramidLayout()
+    N.check("of_pyramid_layout",
+            N.lib().of_pyramid_layout(C.byref(cfg.camera()), levels or cfg.levels, C.byref(lay)))
+    return lay
+
+
+def level_camera(cfg: Config, level: int) -> N.Camera:
+    out = N.Camera()
+    N.check("of_camera_level", N.lib().of_camera_level(C.byref(cfg.camera()), level, C.byref(out)))
+    return out
+
+
+def volume_bytes(cfg: Config) -> int:
+    n = C.c_size_t()
+    N.check("of_volume_bytes", N.lib().of_volume_bytes(C.byref(cfg.volume()), C.byref(n)))
+    return n.value
+
+
+# ------------------------------------------------------------------ stages --
+
+def new_volume(cfg: Config, device="cuda"):
+    import torch
+    vol = torch.empty(volume_bytes(cfg) // 4, dtype=torch.int32, device=device)
+    N.check("of_volume_reset", N.lib().of_volume_reset(C.byref(cfg.volume()), _ptr(vol), _stream()))
+    return vol
+
+
+def new_pyramid(cfg: Config, device="cuda"):
+    import torch
+    return torch.zeros(pyramid_layout(cfg).total_bytes, dtype=torch.uint8, device=device)
+
+
+def lambda_table(cfg: Config, device="cuda"):
+    import torch
+    lam = torch.empty(cfg.width * cfg.height * 2, dtype=torch.float32, device=device)
+    N.check("of_lambda_table", N.lib().of_lambda_table(C.byref(cfg.camera()), _ptr(lam), _stream()))
+    return lam
+
+
+def preprocess(cfg: Config, depth, frame=None):
+    """CameraHandler::updateCameraData: uint16 depth -> filtered pyramid + maps."""
+    frame = new_pyramid(cfg, depth.device) if frame is None else frame
+    N.check("of_preprocess", N.lib().of_preprocess(C.byref(cfg.camera()), C.byref(cfg.filter()),
+                                                   _ptr(depth), cfg.width, _ptr(frame), _stream()))
+    return frame
+
+
+def integrate(cfg: Config, vol, depth, pose, lam):
+    """VolumeIntegrator::Integrate: fuse `depth` at FP64 device pose `pose`."""
+    N.check("of_integrate", N.lib().of_integrate(C.byref(cfg.volume()), _ptr(vol),
+                                                 C.byref(cfg.camera()), _ptr(depth), cfg.width,
+                                                 _ptr(pose), _ptr(lam), _stream()))
+
+
+def integrate_census(cfg: Config, vol, depth, pose, lam) -> int:
+    import torch
+    cnt = torch.zeros(1, dtype=torch.int64, device=vol.device)
+    N.check("of_integrate_census",
+            N.lib().of_integrate_census(C.byref(cfg.volume()), _ptr(vol), C.byref(cfg.camera()),
+                                        _ptr(depth), cfg.width, _ptr(pose), _ptr(lam), _ptr(cnt),
+                                        _stream()))
+    return int(cnt.item())
+
+
+def raycast(cfg: Config, vol, pose, model=None, rgba=None):
+    """Raycaster::Raycast: world vertex/normal pyramid of the volume at `pose`."""
+    model = new_pyramid(cfg, vol.device) if model is None else model
+    N.check("of_raycast", N.lib().of_raycast(C.byref(cfg.volume()), _ptr(vol),
+                                             C.byref(cfg.camera()), C.byref(cfg.raycast()),
+                                             cfg.levels, _ptr(pose), _ptr(model), _ptr(rgba),
+                                             _stream()))
+    return model
+
+
+def icp_workspace(cfg: Config, device="cuda"):
+    import torch
+    n = C.c_size_t()
+    N.check("of_icp_workspace_bytes",
+            N.lib().of_icp_workspace_bytes(C.byref(cfg.camera()), C.byref(n)))
+    return torch.zeros(n.value, dtype=torch.uint8, device=device)
+
+
+def icp_track(cfg: Config, frame, model, pose, ws, stats=None):
+    """ICP::Iterate_ICP: refine the FP64 device pose in place."""
+    N.check("of_icp_track", N.lib().of_icp_track(C.byref(cfg.camera()), C.byref(cfg.icp()),
+                                                 _ptr(frame), _ptr(model), _ptr(pose), _ptr(ws),
+                                                 _ptr(stats), _stream()))
+
+
+def icp_system(cfg: Config, level: int, frame, model, pose, ws):
+    """One correspondence + reduction pass (ICP::FindCorresponding): 29 floats."""
+    import torch
+    out = torch.zeros(29, dtype=torch.float32, device=frame.device)
+    N.check("of_icp_system", N.lib().of_icp_system(C.byref(cfg.camera()), C.byref(cfg.icp()),
+                                                   level, _ptr(frame), _ptr(model), _ptr(pose),
+                                                   _ptr(ws), _ptr(out), _stream()))
+    return out
+
+
+def unpack_points(cfg: Config, pyr, level: int = 0):
+    """(vertex[H,W,4], normal[H,W,4]) views of one level of a pyramid buffer."""
+    import torch
+    lay = pyramid_layout(cfg)
+    w, h = lay.width[level], lay.height[level]
+    off = lay.points_offset[level]
+    pts = pyr[off: off + w * h * 32].view(torch.float32).view(h, w, 2, 4)
+    return pts[:, :, 0, :], pts[:, :, 1, :]
+
+
+def unpack_depth(cfg: Config, pyr, level: int = 0):
+    import torch
+    lay = pyramid_layout(cfg)
+    w, h = lay.width[level], lay.height[level]
+    off = lay.depth_offset[level]
+    return pyr[off: off + w * h * 4].view(torch.float32).view(h, w)
+
+
+def volume_to_linear(cfg: Config, vol_words: np.ndarray):
+    """Brick-major voxel words -> (tsdf_q int16 or f16 bits, weight) in x,y,z order."""
+    n = cfg.resolution
+    nb = n // 8
+    w = np.asarray(vol_words).view(np.uint32).reshape(nb, nb, nb, 8, 8, 8)
+    w = w.transpose(0, 3, 1, 4, 2, 5).reshape(n, n, n)
+    return (w & 0xFFFF).astype(np.uint16), (w >> 16).astype(np.uint16)
+
+
+def linear_to_volume(cfg: Config, q: np.ndarray, weight: np.ndarray) -> np.ndarray:
+    n = cfg.resolution
+    nb = n // 8
+    words = (q.astype(np.uint32) & 0xFFFF) | (weight.astype(np.uint32) << 16)
+    words = words.reshape(nb, 8, nb, 8, nb, 8).transpose(0, 2, 4, 1, 3, 5).reshape(-1)
+    return words.view(np.int32)
+
+
+# ----------------------------------------------------------------- tracker --
+
+class Tracker:
+    """Owns the per-frame state of RunApp (MainApp.cpp:591-647) and runs the
+    frame loop (MainApp.cpp:786-964) as one CUDA graph per frame."""
+
+    def __init__(self, cfg: Config, initial_pose: np.ndarray, use_graph: bool = True,
+                 pose_history: int = 1024):
+        self.cfg = cfg
+        d = N.TrackerDesc()
+        d.camera = cfg.camera()
+        d.volume = cfg.volume()
+        d.filter = cfg.filter()
+        d.raycast = cfg.raycast()
+        d.icp = cfg.icp()
+        d.initial_pose = (C.c_double * 16)(*np.asarray(initial_pose, np.float64).reshape(16))
+        d.use_graph = 1 if use_graph else 0
+        d.pose_history = pose_history
+        h = C.c_void_p()
+        N.check("of_tracker_create", N.lib().of_tracker_create(C.byref(d), C.byref(h)))
+        self._h = h
+        self.frames = 0
+
+    def close(self):
+        if self._h:
+            N.lib().of_tracker_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def process(self, depth, stream=None):
+        """`depth`: CUDA uint16 tensor, or a (pinned) CPU tensor copied on `stream`."""
+        on_host = 0 if depth.is_cuda else 1
+        N.check("of_tracker_process",
+                N.lib().of_tracker_process(self._h, depth.data_ptr(), on_host, _stream(stream)))
+        self.frames += 1
+
+    def set_prior(self, delta: np.ndarray | None):
+        arr = None if delta is None else (C.c_double * 16)(*np.asarray(delta, np.float64).reshape(16))
+        N.check("of_tracker_set_prior", N.lib().of_tracker_set_prior(self._h, arr))
+
+    def pose(self, out=None, stats_out=None, stream=None):
+        """Copies the current pose into `out` (pinned float64 tensor [16]) asynchronously,
+        or returns a numpy array after a synchronous copy."""
+        import torch
+        if out is None:
+            buf = (C.c_double * 16)()
+            st = N.IcpStats()
+            N.check("of_tracker_pose", N.lib().of_tracker_pose(self._h, buf, C.byref(st),
+                                                               _stream(stream)))
+            torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
+            return np.array(buf[:]).reshape(4, 4), st
+        N.check("of_tracker_pose", N.lib().of_tracker_pose(self._h, out.data_ptr(),
+                                                           _ptr(stats_out), _stream(stream)))
+        return out
+
+    def pose_history(self, count: int) -> np.ndarray:
+        buf = np.zeros((count, 16), np.float64)
+        N.check("of_tracker_pose_history",
+                N.lib().of_tracker_pose_history(self._h, buf.ctypes.data, count, _stream()))
+        return buf.reshape(count, 4, 4)
+
+    def buffers(self) -> N.TrackerBuffers:
+        b = N.TrackerBuffers()
+        N.check("of_tracker_buffers", N.lib().of_tracker_buffers(self._h, C.byref(b)))
+        return b
+
+
+# --------------------------------------------------------------- synthetic --
+
+@dataclass
+class Sequence:
+    cfg: Config
+    scene: N.SynthScene
+    poses: np.ndarray            # [F, 4, 4] ground-truth camera-to-world
+    depth: np.ndarray = field(default=None)   # [F, H, W] uint16
+
+
+def make_scene(kind: int, seed: int, cube_mm: float) -> N.SynthScene:
+    sc = N.SynthScene()
+    if N.synth().of_synth_scene(kind, seed, cube_mm, C.byref(sc)) != 0:
+        raise ValueError("of_synth_scene: bad arguments")
+    return sc
+
+
+def make_trajectory(motion: int, seed: int, cube_mm: float, frames: int) -> np.ndarray:
+    out = np.zeros((frames, 16), np.float64)
+    if N.synth().of_synth_trajectory(motion, seed, cube_mm, frames, out.ctypes.data) != 0:
+        raise ValueError("of_synth_trajectory: bad arguments")
+    return out.reshape(frames, 4, 4)
+
+
+def render(cfg: Config, scene: N.SynthScene, pose: np.ndarray, frame: int,
+           noise: float | None = None, dropout: float | None = None, exact: bool = False):
+    depth = np.zeros((cfg.height, cfg.width), np.uint16)
+    ex = np.zeros((cfg.height, cfg.width), np.float32) if exact else None
+    P = np.ascontiguousarray(pose, np.float64)
+    r = N.synth().of_synth_render(C.byref(scene), cfg.width, cfg.height, cfg.fx, cfg.fy, cfg.cx,
+                                  cfg.cy, P.ctypes.data, cfg.seed + 2, frame,
+                                  cfg.noise if noise is None else noise,
+                                  cfg.dropout if dropout is None else dropout, depth.ctypes.data,
+                                  None if ex is None else ex.ctypes.data)
+    if r != 0:
+        raise ValueError("of_synth_render: bad arguments")
+    return (depth, ex) if exact else depth
+
+
+def make_sequence(cfg: Config, frames: int | None = None, render_depth: bool = True) -> Sequence:
+    f = cfg.frames if frames is None else frames
+    scene = make_scene(cfg.scene_kind, cfg.seed, cfg.size_mm)
+    poses = make_trajectory(cfg.motion, cfg.seed + 1, cfg.size_mm, f)
+    seq = Sequence(cfg, scene, poses)
+    if render_depth:
+        seq.depth = np.stack([render(cfg, scene, poses[k], k) for k in range(f)])
+    return seq

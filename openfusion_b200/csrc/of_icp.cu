@@ -1,0 +1,369 @@
+// of_icp.cu -- multi-level point-to-plane ICP, entirely on the device.
+//
+// One launch per iteration. Each launch fuses what the reference spreads over
+// d_find_corresponding (Source/src/ICP.cu:116-251) and the host loop of
+// ICP::Iterate_ICP (Source/src/ICP.cpp:84-182):
+//   for every model pixel with a valid world vertex s and normal n_s:
+//     s_c = T^-1 s; pixel = roundFloat(project(s_c)), rejected when outside
+//     the image or s_c.z >= -eps (ICP.cu:90-95, :152-167);
+//     d = T v(pixel), n_d = R n(pixel) from the frame's camera-space maps
+//     (the reference re-converts the frame to world space at every
+//     iteration instead, ICP.cpp:174);
+//     inlier if |d - s| < dist and thresh < n_d . n_s < 1 + eps (ICP.cu:179-181);
+//     row A = [n_s x d, n_s], b = n_s . (s - d) (ICP.cu:186-201);
+//   sum the 21 upper A^T A entries, 6 A^T b entries, b^2 and the inlier count
+//   in FP32 (Kahan per thread, shuffle trees per warp and block);
+//   the last block to finish combines the per-block partials (Kahan + tree),
+//   solves A^T A x = A^T b by FP64 Cholesky, negates the rotation part
+//   (ICP.cpp:162-168), builds dT = [Rz(g) Ry(b) Rx(a) | t] and composes
+//   T <- dT T in FP64 (ICP.cu:266-305). A singular system restores the frame's
+//   starting pose and stops the remaining iterations (ICP.cpp:152-158).
+#include "of_common.cuh"
+
+using namespace of;
+
+bool of_camera_valid(const of_camera_t *c);
+
+namespace {
+
+constexpr int kIcpThreads = 256;
+constexpr int kIcpMaxBlocks = 2 * kSmCount;
+constexpr int kVals = 29;  // 21 + 6 + residual^2 + inliers
+constexpr float kEps = 1e-6f;  // _EPSILON_ (Constants.h:14)
+
+struct IcpWorkspace {
+  unsigned int ticket;
+  int stop;
+  int iterations;
+  int pad;
+  double pose_init[16];
+  double prior[16];
+  int has_prior;
+  int pad2[3];
+  float partials[kIcpMaxBlocks][32];
+};
+
+enum IcpMode { kModeUpdate = 0, kModeSystem = 1 };
+
+__device__ __forceinline__ void kahan_add(float &sum, float &comp, float x) {
+  float y = x - comp;
+  float t = sum + y;
+  comp = (t - sum) - y;
+  sum = t;
+}
+
+// FP64 6x6 Cholesky solve of H x = g (H given by its 21 upper entries).
+// Returns false when a pivot is not larger than 1e-12 x the largest diagonal
+// entry or is not finite; *minpiv gets the smallest pivot / largest diagonal.
+__device__ bool chol_solve6(const double *up, const double *g, double *x, double *minpiv) {
+  double H[6][6];
+  int q = 0;
+  for (int i = 0; i < 6; ++i)
+    for (int j = i; j < 6; ++j) {
+      H[i][j] = up[q];
+      H[j][i] = up[q];
+      ++q;
+    }
+  double dmax = 0.0;
+  for (int i = 0; i < 6; ++i) dmax = fmax(dmax, H[i][i]);
+  double L[6][6] = {};
+  double mp = 1e300;
+  bool ok = dmax > 0.0 && isfinite(dmax);
+  for (int j = 0; j < 6 && ok; ++j) {
+    double s = H[j][j];
+    for (int k = 0; k < j; ++k) s -= L[j][k] * L[j][k];
+    mp = fmin(mp, s / dmax);
+    if (!(s > 1e-12 * dmax) || !isfinite(s)) { ok = false; break; }
+    double ljj = sqrt(s);
+    L[j][j] = ljj;
+    for (int i = j + 1; i < 6; ++i) {
+      double t = H[i][j];
+      for (int k = 0; k < j; ++k) t -= L[i][k] * L[j][k];
+      L[i][j] = t / ljj;
+    }
+  }
+  *minpiv = ok ? mp : fmin(mp, 0.0);
+  if (!ok) return false;
+  double y[6];
+  for (int i = 0; i < 6; ++i) {
+    double t = g[i];
+    for (int k = 0; k < i; ++k) t -= L[i][k] * y[k];
+    y[i] = t / L[i][i];
+  }
+  for (int i = 5; i >= 0; --i) {
+    double t = y[i];
+    for (int k = i + 1; k < 6; ++k) t -= L[k][i] * x[k];
+    x[i] = t / L[i][i];
+  }
+  return true;
+}
+
+// dT of Cpu_buildNewTransformMatrix (ICP.cu:266-290) in FP64, then P <- dT P.
+__device__ void compose_increment(const double *xo, double *P) {
+  double al = xo[0], be = xo[1], ga = xo[2];
+  double ca = cos(al), sa = sin(al), cb = cos(be), sb = sin(be), cg = cos(ga), sg = sin(ga);
+  double D[16] = {cg * cb, -sg * ca + cg * sb * sa, sg * sa + cg * sb * ca, xo[3],
+                  sg * cb, cg * ca + sg * sb * sa,  -cg * sa + sg * sb * ca, xo[4],
+                  -sb,     cb * sa,                 cb * ca,                 xo[5],
+                  0.0,     0.0,                     0.0,                     1.0};
+  double O[16];
+  for (int i = 0; i < 16; ++i) O[i] = P[i];
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) {
+      double a = 0.0;
+      for (int k = 0; k < 4; ++k) a += D[4 * i + k] * O[4 * k + j];
+      P[4 * i + j] = a;
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kIcpThreads)
+    k_icp_iter(const float4 *__restrict__ model, int mw, int mh, const float4 *__restrict__ frame,
+               Cam cam, float dist_thresh, float normal_thresh, double *pose, IcpWorkspace *ws,
+               of_icp_stats_t *stats, float *system_out) {
+  __shared__ Rigid s_c2w, s_w2c;
+  __shared__ int s_stop;
+  __shared__ float s_red[kIcpThreads / 32][32];
+  __shared__ bool s_last;
+  if (threadIdx.x == 0) {
+    s_stop = (MODE == kModeUpdate) ? ws->stop : 0;
+    if (!s_stop) pose_to_rigid(pose, &s_c2w, &s_w2c);
+  }
+  __syncthreads();
+  if (s_stop) return;
+
+  float acc[kVals], cmp[kVals];
+#pragma unroll
+  for (int v = 0; v < kVals; ++v) { acc[v] = 0.f; cmp[v] = 0.f; }
+
+  const int npx = mw * mh;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npx; p += gridDim.x * blockDim.x) {
+    float4 s = model[2 * p];
+    float4 ns = model[2 * p + 1];
+    if (s.w == 0.f || ns.w == 0.f) continue;
+    float3 sc = apply(s_w2c, make_float3(s.x, s.y, s.z));
+    if (sc.z >= -kEps) continue;
+    float rz = __frcp_rn(sc.z);
+    int pu = round_ref(fmaf(cam.fx * sc.x, rz, cam.cx));
+    int pv = round_ref(fmaf(cam.fy * sc.y, rz, cam.cy));
+    if (pu < 0 || pu >= cam.w || pv < 0 || pv >= cam.h) continue;
+    size_t q = (size_t)pv * cam.w + pu;
+    float4 dc = __ldg(frame + 2 * q);
+    float4 nc = __ldg(frame + 2 * q + 1);
+    if (dc.w == 0.f || nc.w == 0.f) continue;
+    float3 d = apply(s_c2w, make_float3(dc.x, dc.y, dc.z));
+    float3 nd = rotate(s_c2w, make_float3(nc.x, nc.y, nc.z));
+    float ex = d.x - s.x, ey = d.y - s.y, ez = d.z - s.z;
+    if (!(sqrtf(ex * ex + ey * ey + ez * ez) < dist_thresh)) continue;
+    float dn = nd.x * ns.x + nd.y * ns.y + nd.z * ns.z;
+    if (!(dn > normal_thresh && dn < 1.f + kEps)) continue;
+    float a[6];
+    a[0] = ns.y * d.z - ns.z * d.y;
+    a[1] = ns.z * d.x - ns.x * d.z;
+    a[2] = ns.x * d.y - ns.y * d.x;
+    a[3] = ns.x; a[4] = ns.y; a[5] = ns.z;
+    float b = -(ns.x * ex + ns.y * ey + ns.z * ez);
+    int k = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int j = i; j < 6; ++j) { kahan_add(acc[k], cmp[k], a[i] * a[j]); ++k; }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) kahan_add(acc[21 + i], cmp[21 + i], a[i] * b);
+    kahan_add(acc[27], cmp[27], b * b);
+    acc[28] += 1.f;
+  }
+  // warp tree, then block tree over the 8 warps
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int v = 0; v < kVals; ++v) {
+    float x = acc[v] - cmp[v];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) s_red[warp][v] = x;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    float x = 0.f;
+    if (lane < kVals) {
+      float y[kIcpThreads / 32];
+#pragma unroll
+      for (int w = 0; w < kIcpThreads / 32; ++w) y[w] = s_red[w][lane];
+#pragma unroll
+      for (int span = 1; span < kIcpThreads / 32; span *= 2)
+#pragma unroll
+        for (int w = 0; w + span < kIcpThreads / 32; w += 2 * span) y[w] += y[w + span];
+      x = y[0];
+    }
+    ws->partials[blockIdx.x][lane] = x;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(&ws->ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+
+  // ---- last block: combine the per-block partials (Kahan per group, tree)
+  {
+    const int v = threadIdx.x & 31, grp = threadIdx.x >> 5;
+    float sum = 0.f, c = 0.f;
+    if (v < kVals)
+      for (int r = grp; r < (int)gridDim.x; r += kIcpThreads / 32)
+        kahan_add(sum, c, __ldcg(&ws->partials[r][v]));
+    s_red[grp][v] = sum - c;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  float tot[kVals];
+  for (int v = 0; v < kVals; ++v) {
+    float y[kIcpThreads / 32];
+    for (int w = 0; w < kIcpThreads / 32; ++w) y[w] = s_red[w][v];
+    for (int span = 1; span < kIcpThreads / 32; span *= 2)
+      for (int w = 0; w + span < kIcpThreads / 32; w += 2 * span) y[w] += y[w + span];
+    tot[v] = y[0];
+  }
+  ws->ticket = 0;
+  if (MODE == kModeSystem) {
+    for (int v = 0; v < kVals; ++v) system_out[v] = tot[v];
+    return;
+  }
+  double up[21], g[6], xs[6], minpiv = 0.0;
+  for (int v = 0; v < 21; ++v) up[v] = (double)tot[v];
+  for (int v = 0; v < 6; ++v) g[v] = (double)tot[21 + v];
+  int inliers = (int)tot[28];
+  bool ok = inliers >= 6 && chol_solve6(up, g, xs, &minpiv);
+  ws->iterations += 1;
+  if (ok) {
+    double xo[6] = {-xs[0], -xs[1], -xs[2], xs[3], xs[4], xs[5]};
+    compose_increment(xo, pose);
+  } else {
+    for (int i = 0; i < 16; ++i) pose[i] = ws->pose_init[i];
+    ws->stop = 1;
+  }
+  if (stats) {
+    stats->status = ok ? 0 : 1;
+    stats->inliers = inliers;
+    stats->iterations = ws->iterations;
+    stats->residual_sq = (double)tot[27];
+    stats->min_pivot = minpiv;
+  }
+}
+
+// Start of a frame's tracking: remember the starting pose, apply the
+// optional warm-start increment, clear the flags.
+__global__ void k_icp_begin(double *pose, IcpWorkspace *ws, of_icp_stats_t *stats) {
+  if (threadIdx.x != 0) return;
+  if (ws->has_prior) {
+    double O[16];
+    for (int i = 0; i < 16; ++i) O[i] = pose[i];
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) {
+        double a = 0.0;
+        for (int k = 0; k < 4; ++k) a += ws->prior[4 * i + k] * O[4 * k + j];
+        pose[4 * i + j] = a;
+      }
+    ws->has_prior = 0;  // a prior applies to one frame
+  }
+  for (int i = 0; i < 16; ++i) ws->pose_init[i] = pose[i];
+  ws->ticket = 0;
+  ws->stop = 0;
+  ws->iterations = 0;
+  if (stats) {
+    stats->status = 0;
+    stats->inliers = 0;
+    stats->iterations = 0;
+    stats->residual_sq = 0.0;
+    stats->min_pivot = 0.0;
+  }
+}
+
+int icp_blocks(int npx) {
+  int g = (npx + kIcpThreads - 1) / kIcpThreads;
+  return g < 1 ? 1 : (g > kIcpMaxBlocks ? kIcpMaxBlocks : g);
+}
+
+}  // namespace
+
+size_t of_icp_workspace_size() { return sizeof(IcpWorkspace); }
+
+of_status_t of_icp_set_prior(void *d_workspace, const double *prior_host, cudaStream_t s) {
+  IcpWorkspace *ws = (IcpWorkspace *)d_workspace;
+  static const int zero = 0, one = 1;
+  if (prior_host) {
+    OF_CUDA_TRY(cudaMemcpyAsync(ws->prior, prior_host, 16 * sizeof(double),
+                                cudaMemcpyHostToDevice, s));
+    OF_CUDA_TRY(cudaMemcpyAsync(&ws->has_prior, &one, sizeof(int), cudaMemcpyHostToDevice, s));
+  } else {
+    OF_CUDA_TRY(cudaMemcpyAsync(&ws->has_prior, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
+  }
+  return OF_OK;
+}
+
+extern "C" of_status_t of_icp_workspace_bytes(const of_camera_t *cam, size_t *bytes) {
+  if (!of_camera_valid(cam) || !bytes) return OF_ERR_INVALID_ARGUMENT;
+  *bytes = sizeof(IcpWorkspace);
+  return OF_OK;
+}
+
+static bool icp_params_ok(const of_icp_params_t *p) {
+  if (!p || p->levels < 1 || p->levels > kMaxLevels) return false;
+  for (int l = 0; l < p->levels; ++l)
+    if (p->iters[l] < 0 || p->iters[l] > 1000) return false;
+  return p->dist_thresh_mm > 0.f;
+}
+
+// Launches the iterations of every level, coarse to fine.
+of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, const void *d_frame,
+                          const void *d_model, double *pose, void *d_ws, of_icp_stats_t *stats,
+                          cudaStream_t s) {
+  of_pyramid_layout_t lay;
+  of_status_t st = of_pyramid_layout(cam, ip->levels, &lay);
+  if (st != OF_OK) return st;
+  IcpWorkspace *ws = (IcpWorkspace *)d_ws;
+  k_icp_begin<<<1, 32, 0, s>>>(pose, ws, stats);
+  for (int l = ip->levels - 1; l >= 0; --l) {
+    of_camera_t cl = camera_level(*cam, l);
+    Cam c = make_cam(cl);
+    const float4 *fr = (const float4 *)((const char *)d_frame + lay.points_offset[l]);
+    const float4 *md = (const float4 *)((const char *)d_model + lay.points_offset[l]);
+    int g = icp_blocks(cl.width * cl.height);
+    for (int it = 0; it < ip->iters[l]; ++it)
+      k_icp_iter<kModeUpdate><<<g, kIcpThreads, 0, s>>>(md, cl.width, cl.height, fr, c,
+                                                        ip->dist_thresh_mm, ip->normal_thresh,
+                                                        pose, ws, stats, nullptr);
+  }
+  return of_launch_status();
+}
+
+extern "C" of_status_t of_icp_track(const of_camera_t *cam, const of_icp_params_t *ip,
+                                    const void *d_frame, const void *d_model, double *pose,
+                                    void *d_ws, of_icp_stats_t *stats, of_stream_t s) {
+  if (!of_camera_valid(cam) || !icp_params_ok(ip) || !d_frame || !d_model || !pose || !d_ws)
+    return OF_ERR_INVALID_ARGUMENT;
+  return of_icp_launch(cam, ip, d_frame, d_model, pose, d_ws, stats, (cudaStream_t)s);
+}
+
+extern "C" of_status_t of_icp_system(const of_camera_t *cam, const of_icp_params_t *ip,
+                                     int32_t level, const void *d_frame, const void *d_model,
+                                     const double *pose, void *d_ws, float *d_system,
+                                     of_stream_t stream) {
+  if (!of_camera_valid(cam) || !icp_params_ok(ip) || !d_frame || !d_model || !pose || !d_ws ||
+      !d_system || level < 0 || level >= ip->levels)
+    return OF_ERR_INVALID_ARGUMENT;
+  of_pyramid_layout_t lay;
+  of_status_t st = of_pyramid_layout(cam, ip->levels, &lay);
+  if (st != OF_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  IcpWorkspace *ws = (IcpWorkspace *)d_ws;
+  OF_CUDA_TRY(cudaMemsetAsync(&ws->ticket, 0, sizeof(unsigned int), s));
+  of_camera_t cl = camera_level(*cam, level);
+  Cam c = make_cam(cl);
+  const float4 *fr = (const float4 *)((const char *)d_frame + lay.points_offset[level]);
+  const float4 *md = (const float4 *)((const char *)d_model + lay.points_offset[level]);
+  int g = icp_blocks(cl.width * cl.height);
+  k_icp_iter<kModeSystem><<<g, kIcpThreads, 0, s>>>(md, cl.width, cl.height, fr, c,
+                                                    ip->dist_thresh_mm, ip->normal_thresh,
+                                                    (double *)pose, ws, nullptr, d_system);
+  return of_launch_status();
+}

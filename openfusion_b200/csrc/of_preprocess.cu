@@ -1,0 +1,185 @@
+// of_preprocess.cu -- depth pre-processing: bilateral filter (Tomasi &
+// Manduchi 1998, as used by KinectFusion, Newcombe et al. ISMAR 2011 s3.2),
+// guarded 2x2 depth pyramid and per-level camera-space vertex/normal maps.
+//
+// The vertex map follows d_convertDepthToWorldVertices
+// (Source/src/CameraSupport/CameraHandler.cu:65-89) in camera space, and the
+// normal map follows d_convertDepthToWorldNormals (CameraHandler.cu:91-132):
+// n = normalize((v(x+1,y) - v) x (v(x,y+1) - v)), invalid on the last
+// row/column, where a neighbour is invalid, or where the cross product is zero.
+// The world transform the reference applies at every ICP iteration
+// (ICP.cpp:174) is applied on the fly inside the ICP kernel instead.
+#include "of_common.cuh"
+
+using namespace of;
+
+bool of_camera_valid(const of_camera_t *c);
+
+namespace {
+
+constexpr int kTileX = 32;
+constexpr int kTileY = 8;
+constexpr int kMaxRadius = 16;
+
+__device__ __forceinline__ bool depth_valid(float d, float dmin, float dmax) {
+  return d > 0.f && d >= dmin && d <= dmax;
+}
+
+// Bilateral filter of the raw uint16 depth. Invalid centre -> 0; invalid
+// neighbours get weight 0. Weight = 2^-(r^2 ks + delta^2 kr) with
+// ks = log2(e)/(2 sigma_s^2), kr = log2(e)/(2 sigma_r^2).
+__global__ void __launch_bounds__(256) k_bilateral(const uint16_t *__restrict__ depth, int pitch,
+                                                   int w, int h, float dmin, float dmax, int R,
+                                                   float ks, float kr, float *__restrict__ out) {
+  extern __shared__ float tile[];
+  const int tw = kTileX + 2 * R;
+  const int th = kTileY + 2 * R;
+  const int x0 = blockIdx.x * kTileX - R;
+  const int y0 = blockIdx.y * kTileY - R;
+  for (int i = threadIdx.x; i < tw * th; i += blockDim.x) {
+    int tx = i % tw, ty = i / tw;
+    int gx = x0 + tx, gy = y0 + ty;
+    float d = 0.f;
+    if (gx >= 0 && gx < w && gy >= 0 && gy < h) {
+      d = (float)__ldg(depth + (size_t)gy * pitch + gx);
+      if (!depth_valid(d, dmin, dmax)) d = 0.f;
+    }
+    tile[i] = d;
+  }
+  __syncthreads();
+  const int lx = threadIdx.x % kTileX, ly = threadIdx.x / kTileX;
+  const int x = blockIdx.x * kTileX + lx, y = blockIdx.y * kTileY + ly;
+  if (x >= w || y >= h) return;
+  const float c = tile[(ly + R) * tw + lx + R];
+  float result = 0.f;
+  if (c > 0.f) {
+    float sw = 0.f, sd = 0.f;
+    for (int dy = -R; dy <= R; ++dy) {
+      const float *row = tile + (ly + R + dy) * tw + lx + R;
+      const float ry = (float)(dy * dy) * ks;
+      for (int dx = -R; dx <= R; ++dx) {
+        float q = row[dx];
+        float del = q - c;
+        float e = fmaf(del * del, kr, fmaf((float)(dx * dx), ks, ry));
+        float wt = q > 0.f ? exp2f(-e) : 0.f;
+        sw += wt;
+        sd = fmaf(wt, q, sd);
+      }
+    }
+    result = sd / sw;
+  }
+  out[(size_t)y * w + x] = result;
+}
+
+// Level l -> l+1: pixel (x, y) averages the valid pixels of the 2x2 block
+// {2x, 2x+1} x {2y, 2y+1} that lie within 3 sigma_r of the block's first
+// valid pixel (row-major order); 0 if the block has none.
+__global__ void k_pyr_down(const float *__restrict__ src, int sw, int sh, float *__restrict__ dst,
+                           int dw, int dh, float guard) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= dw || y >= dh) return;
+  float ref = 0.f, sum = 0.f;
+  int cnt = 0;
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      int sx = 2 * x + i, sy = 2 * y + j;
+      if (sx < sw && sy < sh) {
+        float d = src[(size_t)sy * sw + sx];
+        if (d > 0.f) {
+          if (cnt == 0) ref = d;
+          if (fabsf(d - ref) <= guard) {
+            sum += d;
+            ++cnt;
+          }
+        }
+      }
+    }
+  dst[(size_t)y * dw + x] = cnt ? sum / (float)cnt : 0.f;
+}
+
+// Camera-space vertex and normal of every pixel of one level. Differences
+// of neighbouring vertices are formed from depth differences (no
+// cancellation between large coordinates).
+__global__ void k_vertex_normal(const float *__restrict__ depth, int w, int h, float cx, float cy,
+                                float ifx, float ify, float4 *__restrict__ pts) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= w || y >= h) return;
+  size_t p = (size_t)y * w + x;
+  float d = depth[p];
+  float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 n = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (d > 0.f) {
+    float ax = (float)x - cx, ay = (float)y - cy;
+    v = make_float4(-d * ax * ifx, -d * ay * ify, -d, 1.f);
+    if (x + 1 < w && y + 1 < h) {
+      float d10 = depth[p + 1];
+      float d01 = depth[p + w];
+      if (d10 > 0.f && d01 > 0.f) {
+        float e10 = d10 - d, e01 = d01 - d;
+        float3 a = make_float3(-ifx * fmaf(e10, ax, d10), -ify * ay * e10, -e10);
+        float3 b = make_float3(-ifx * ax * e01, -ify * fmaf(e01, ay, d01), -e01);
+        float3 c = make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+        float l2 = c.x * c.x + c.y * c.y + c.z * c.z;
+        if (l2 > 0.f) {
+          float il = rsqrtf(l2);
+          il = il * (1.5f - 0.5f * l2 * il * il);  // one Newton step on rsqrt
+          n = make_float4(c.x * il, c.y * il, c.z * il, 1.f);
+        }
+      }
+    }
+  }
+  pts[2 * p] = v;
+  pts[2 * p + 1] = n;
+}
+
+}  // namespace
+
+extern "C" of_status_t of_preprocess(const of_camera_t *cam, const of_filter_params_t *fp,
+                                     const uint16_t *d_depth, int32_t pitch, void *d_frame,
+                                     of_stream_t stream) {
+  if (!of_camera_valid(cam) || !fp || !d_depth || !d_frame || pitch < cam->width)
+    return OF_ERR_INVALID_ARGUMENT;
+  if (fp->levels < 1 || fp->levels > kMaxLevels || fp->sigma_space_px <= 0.f ||
+      fp->sigma_range_mm <= 0.f)
+    return OF_ERR_INVALID_ARGUMENT;
+  int R = fp->radius_px > 0 ? fp->radius_px : (int)ceilf(2.0f * fp->sigma_space_px);
+  if (R > kMaxRadius) return OF_ERR_INVALID_ARGUMENT;
+  of_pyramid_layout_t lay;
+  of_status_t st = of_pyramid_layout(cam, fp->levels, &lay);
+  if (st != OF_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  char *base = (char *)d_frame;
+  const double log2e = 1.4426950408889634;
+  float ks = (float)(log2e / (2.0 * (double)fp->sigma_space_px * fp->sigma_space_px));
+  float kr = (float)(log2e / (2.0 * (double)fp->sigma_range_mm * fp->sigma_range_mm));
+  {
+    dim3 grid((cam->width + kTileX - 1) / kTileX, (cam->height + kTileY - 1) / kTileY);
+    size_t smem = (size_t)(kTileX + 2 * R) * (kTileY + 2 * R) * sizeof(float);
+    k_bilateral<<<grid, kTileX * kTileY, smem, s>>>(
+        d_depth, pitch, cam->width, cam->height, cam->min_depth_mm, cam->max_depth_mm, R, ks, kr,
+        (float *)(base + lay.depth_offset[0]));
+  }
+  float guard = 3.0f * fp->sigma_range_mm;
+  for (int l = 1; l < fp->levels; ++l) {
+    dim3 blk(32, 8);
+    dim3 grid((lay.width[l] + 31) / 32, (lay.height[l] + 7) / 8);
+    k_pyr_down<<<grid, blk, 0, s>>>((const float *)(base + lay.depth_offset[l - 1]),
+                                    lay.width[l - 1], lay.height[l - 1],
+                                    (float *)(base + lay.depth_offset[l]), lay.width[l],
+                                    lay.height[l], guard);
+  }
+  for (int l = 0; l < fp->levels; ++l) {
+    of_camera_t c = camera_level(*cam, l);
+    dim3 blk(32, 8);
+    dim3 grid((c.width + 31) / 32, (c.height + 7) / 8);
+    k_vertex_normal<<<grid, blk, 0, s>>>((const float *)(base + lay.depth_offset[l]), c.width,
+                                         c.height, c.cx, c.cy, (float)(1.0 / (double)c.fx),
+                                         (float)(1.0 / (double)c.fy),
+                                         (float4 *)(base + lay.points_offset[l]));
+  }
+  return of_launch_status();
+}

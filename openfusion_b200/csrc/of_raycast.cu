@@ -1,0 +1,230 @@
+// of_raycast.cu -- surface prediction by ray marching the TSDF.
+//
+// Follows d_raycast (Source/src/Raycaster.cu:97-230): one ray per pixel from
+// the camera position through the pixel's point at z = -1 in camera space
+// (:117-125), clipped to the cube with a slab test (:35-55, here the box of
+// voxel centres), marched until the first surface, writing the world-space
+// vertex and normal maps (:202-212) and optionally the shaded RGBA of
+// :214-228. Where the reference samples the nearest voxel at fixed 1.5 mm
+// steps and stops at the first tsdf <= 0 (:152-188), this kernel follows the
+// KinectFusion method the reference left commented out (:246-351): trilinear
+// samples, steps of max(min_step, far_frac * tsdf * trunc), a + to - zero
+// crossing refined by regula falsi on the trilinear field, and the normal as
+// the central-difference gradient of trilinear samples one voxel apart. The
+// march runs between the min and max depth along the ray.
+#include "of_common.cuh"
+
+using namespace of;
+
+bool of_camera_valid(const of_camera_t *c);
+bool of_volume_valid(const of_volume_desc_t *d);
+
+namespace {
+
+struct RaySetup {
+  Rigid c2w;
+  float cpos[3];
+  float lo, hi;   // box of voxel centres, mm (same for every axis)
+  float inv_vs;
+};
+
+template <int STORAGE>
+__device__ __forceinline__ float trilinear(const uint32_t *__restrict__ vol, int n, int nb,
+                                           float org, float inv_vs, float px, float py, float pz) {
+  float gx = (px - org) * inv_vs - 0.5f;
+  float gy = (py - org) * inv_vs - 0.5f;
+  float gz = (pz - org) * inv_vs - 0.5f;
+  int ix = min(max((int)floorf(gx), 0), n - 2);
+  int iy = min(max((int)floorf(gy), 0), n - 2);
+  int iz = min(max((int)floorf(gz), 0), n - 2);
+  float fx = gx - (float)ix, fy = gy - (float)iy, fz = gz - (float)iz;
+  float c[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    int a = (q >> 2) & 1, b = (q >> 1) & 1, d = q & 1;
+    c[q] = vox_value<STORAGE>(__ldg(vol + vox_index(nb, ix + a, iy + b, iz + d)));
+  }
+  float c00 = fmaf(fz, c[1] - c[0], c[0]);
+  float c01 = fmaf(fz, c[3] - c[2], c[2]);
+  float c10 = fmaf(fz, c[5] - c[4], c[4]);
+  float c11 = fmaf(fz, c[7] - c[6], c[6]);
+  float c0 = fmaf(fy, c01 - c00, c00);
+  float c1 = fmaf(fy, c11 - c10, c10);
+  return fmaf(fx, c1 - c0, c0);
+}
+
+__device__ __forceinline__ uint32_t rgba_pack(float x, float y, float z, float w) {
+  // rgbaFloatToInt (Raycaster.cu:26-33)
+  x = __saturatef(x); y = __saturatef(y); z = __saturatef(z); w = __saturatef(w);
+  return ((uint32_t)(w * 255.f) << 24) | ((uint32_t)(z * 255.f) << 16) |
+         ((uint32_t)(y * 255.f) << 8) | (uint32_t)(x * 255.f);
+}
+
+template <int STORAGE>
+__global__ void __launch_bounds__(256) k_raycast(const uint32_t *__restrict__ vol,
+                                                 of_volume_desc_t desc, Cam cam,
+                                                 of_raycast_params_t rp,
+                                                 const double *__restrict__ pose,
+                                                 float4 *__restrict__ pts, uint32_t *rgba) {
+  __shared__ RaySetup S;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    pose_to_rigid(pose, &S.c2w, nullptr);
+    S.cpos[0] = S.c2w.t[0]; S.cpos[1] = S.c2w.t[1]; S.cpos[2] = S.c2w.t[2];
+    double vs = (double)desc.size_mm / desc.resolution;
+    S.lo = (float)(-0.5 * desc.size_mm + 0.5 * vs + 1e-3);
+    S.hi = (float)(0.5 * desc.size_mm - 0.5 * vs - 1e-3);
+    S.inv_vs = (float)(1.0 / vs);
+  }
+  __syncthreads();
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= cam.w || y >= cam.h) return;
+  const int n = desc.resolution, nb = n >> 3;
+  const float vs = desc.size_mm / (float)n;
+  const float org = -0.5f * desc.size_mm;
+  const float T = desc.trunc_mm;
+  // ray direction: pixel at z = -1 (Raycaster.cu:117-125)
+  float3 dc = make_float3(-((float)x - cam.cx) * cam.ifx, -((float)y - cam.cy) * cam.ify, -1.f);
+  float lam = sqrtf(dc.x * dc.x + dc.y * dc.y + 1.f);
+  float3 dw = rotate(S.c2w, dc);
+  float il = 1.f / lam;
+  float3 dir = make_float3(dw.x * il, dw.y * il, dw.z * il);
+  const float ox = S.cpos[0], oy = S.cpos[1], oz = S.cpos[2];
+  // slab test (Raycaster.cu:35-55) against the box of voxel centres
+  float tnear = -1e30f, tfar = 1e30f;
+  {
+    const float o3[3] = {ox, oy, oz};
+    const float d3[3] = {dir.x, dir.y, dir.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (fabsf(d3[a]) < 1e-12f) {
+        if (o3[a] < S.lo || o3[a] > S.hi) { tnear = 1e30f; tfar = -1e30f; }
+      } else {
+        float inv = 1.f / d3[a];
+        float t0 = (S.lo - o3[a]) * inv, t1 = (S.hi - o3[a]) * inv;
+        tnear = fmaxf(tnear, fminf(t0, t1));
+        tfar = fminf(tfar, fmaxf(t0, t1));
+      }
+    }
+  }
+  float t0 = fmaxf(tnear, cam.dmin * lam);
+  float t1 = fminf(tfar, cam.dmax * lam);
+  bool hit = false;
+  float ts = 0.f;
+  if (t0 < t1) {
+    const float min_step = rp.min_step_vox * vs;
+    const float far_k = rp.far_step_frac * T;
+    float t = t0;
+    float fp = trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, fmaf(t, dir.x, ox), fmaf(t, dir.y, oy),
+                                  fmaf(t, dir.z, oz));
+    for (int it = 0; it < (1 << 16); ++it) {
+      float step = fp > 0.f ? fmaxf(min_step, far_k * fp) : min_step;
+      float tn = t + step;
+      if (tn > t1) break;
+      float fn = trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, fmaf(tn, dir.x, ox),
+                                    fmaf(tn, dir.y, oy), fmaf(tn, dir.z, oz));
+      if (fp > 0.f && fn <= 0.f) {
+        float ta = t, fa = fp, tb = tn, fb = fn;
+        for (int r = 0; r < rp.refine_iters; ++r) {
+          float tm = fmaf(tb - ta, fa / (fa - fb), ta);
+          float fm = trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, fmaf(tm, dir.x, ox),
+                                        fmaf(tm, dir.y, oy), fmaf(tm, dir.z, oz));
+          if (fm > 0.f) { ta = tm; fa = fm; } else { tb = tm; fb = fm; }
+        }
+        ts = fmaf(tb - ta, fa / (fa - fb), ta);
+        hit = true;
+        break;
+      }
+      if (fp < 0.f && fn > 0.f) break;  // back face
+      t = tn;
+      fp = fn;
+    }
+  }
+  const size_t p = (size_t)y * cam.w + x;
+  float4 vtx = make_float4(0.f, 0.f, 0.f, 0.f), nrm = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (hit) {
+    float px = fmaf(ts, dir.x, ox), py = fmaf(ts, dir.y, oy), pz = fmaf(ts, dir.z, oz);
+    vtx = make_float4(px, py, pz, 1.f);
+    float lo = S.lo, hi = S.hi;
+    if (px - vs >= lo && px + vs <= hi && py - vs >= lo && py + vs <= hi && pz - vs >= lo &&
+        pz + vs <= hi) {
+      float gx = trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, px + vs, py, pz) -
+                 trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, px - vs, py, pz);
+      float gy = trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, px, py + vs, pz) -
+                 trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, px, py - vs, pz);
+      float gz = trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, px, py, pz + vs) -
+                 trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, px, py, pz - vs);
+      float l2 = gx * gx + gy * gy + gz * gz;
+      if (l2 > 0.f) {
+        float inv = rsqrtf(l2);
+        inv = inv * (1.5f - 0.5f * l2 * inv * inv);
+        nrm = make_float4(gx * inv, gy * inv, gz * inv, 1.f);
+      }
+    }
+  }
+  pts[2 * p] = vtx;
+  pts[2 * p + 1] = nrm;
+  if (rgba) {
+    // shaded output of Raycaster.cu:221-227 (showNormal == false)
+    float dd = -(dir.x * nrm.x + dir.y * nrm.y + dir.z * nrm.z);
+    float g = fabsf(dd) < 1e-6f ? 0.f : 0.6f * dd + 0.2f;
+    rgba[p] = fabsf(dd) < 1e-6f ? rgba_pack(0.f, 0.f, 0.f, 0.f) : rgba_pack(g, g, g, 0.f);
+  }
+}
+
+// Model level l -> l+1 by subsampling pixel (2x, 2y): model points are used
+// by ICP only through their world positions, so the subset fixes nothing
+// about the model pixels' intrinsics.
+__global__ void k_model_down(const float4 *__restrict__ src, int sw, float4 *__restrict__ dst,
+                             int dw, int dh) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= dw || y >= dh) return;
+  size_t sp = (size_t)(2 * y) * sw + 2 * x;
+  size_t dp = (size_t)y * dw + x;
+  dst[2 * dp] = src[2 * sp];
+  dst[2 * dp + 1] = src[2 * sp + 1];
+}
+
+}  // namespace
+
+of_status_t of_model_pyramid(const of_camera_t *cam, int levels, void *d_model, cudaStream_t s) {
+  of_pyramid_layout_t lay;
+  of_status_t st = of_pyramid_layout(cam, levels, &lay);
+  if (st != OF_OK) return st;
+  char *base = (char *)d_model;
+  for (int l = 1; l < levels; ++l) {
+    dim3 blk(32, 8);
+    dim3 grid((lay.width[l] + 31) / 32, (lay.height[l] + 7) / 8);
+    k_model_down<<<grid, blk, 0, s>>>((const float4 *)(base + lay.points_offset[l - 1]),
+                                      lay.width[l - 1], (float4 *)(base + lay.points_offset[l]),
+                                      lay.width[l], lay.height[l]);
+  }
+  return of_launch_status();
+}
+
+extern "C" of_status_t of_raycast(const of_volume_desc_t *d, const void *vol,
+                                  const of_camera_t *cam, const of_raycast_params_t *rp,
+                                  int32_t levels, const double *pose, void *d_model,
+                                  uint32_t *rgba, of_stream_t stream) {
+  if (!of_volume_valid(d) || !of_camera_valid(cam) || !rp || !vol || !pose || !d_model)
+    return OF_ERR_INVALID_ARGUMENT;
+  if (levels < 1 || levels > kMaxLevels || rp->min_step_vox <= 0.f || rp->far_step_frac < 0.f ||
+      rp->refine_iters < 0 || rp->refine_iters > 16)
+    return OF_ERR_INVALID_ARGUMENT;
+  of_pyramid_layout_t lay;
+  of_status_t st = of_pyramid_layout(cam, levels, &lay);
+  if (st != OF_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  dim3 blk(16, 16);
+  dim3 grid((cam->width + 15) / 16, (cam->height + 15) / 16);
+  Cam c = make_cam(*cam);
+  float4 *pts = (float4 *)((char *)d_model + lay.points_offset[0]);
+  if (d->storage == OF_TSDF_I16)
+    k_raycast<OF_TSDF_I16><<<grid, blk, 0, s>>>((const uint32_t *)vol, *d, c, *rp, pose, pts, rgba);
+  else
+    k_raycast<OF_TSDF_F16><<<grid, blk, 0, s>>>((const uint32_t *)vol, *d, c, *rp, pose, pts, rgba);
+  st = of_launch_status();
+  if (st != OF_OK) return st;
+  return of_model_pyramid(cam, levels, d_model, s);
+}

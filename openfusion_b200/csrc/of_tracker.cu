@@ -1,0 +1,256 @@
+// of_tracker.cu -- the whole per-frame pipeline, owned state and CUDA graphs.
+//
+// Replaces RunApp::display (Source/src/MainApp.cpp:786-964) without its host
+// round trips: frame k is pre-processed, tracked against the model raycast
+// after frame k-1, fused at the tracked pose and raycast at that pose for
+// frame k+1. The reference's order (integrate(k-1) -> raycast(k-1) ->
+// convert(k) -> ICP(k) -> UpdateTransforms) is the same sequence rotated by
+// one stage. The state the reference allocates in RunApp::initCudaPointers
+// (MainApp.cpp:591-647) lives here; the per-frame launch sequence is captured
+// once as a CUDA graph and replayed.
+#include "of_common.cuh"
+
+#include <new>
+#include <string.h>
+
+using namespace of;
+
+bool of_camera_valid(const of_camera_t *c);
+bool of_volume_valid(const of_volume_desc_t *d);
+size_t of_icp_workspace_size();
+of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, const void *d_frame,
+                          const void *d_model, double *pose, void *d_ws, of_icp_stats_t *stats,
+                          cudaStream_t s);
+of_status_t of_icp_set_prior(void *d_workspace, const double *prior_host, cudaStream_t s);
+
+struct of_tracker {
+  of_tracker_desc_t desc;
+  of_pyramid_layout_t lay;
+  cudaStream_t cap;
+  void *volume = nullptr;
+  void *frame = nullptr;
+  void *model = nullptr;
+  void *icp_ws = nullptr;
+  double *pose = nullptr;
+  double *hist = nullptr;
+  unsigned long long *hist_count = nullptr;
+  uint16_t *depth = nullptr;
+  float *lambda = nullptr;
+  of_icp_stats_t *stats = nullptr;
+  int hist_cap = 1024;
+  int64_t frames = 0;
+  int kernels_first = 0;
+  int kernels_track = 0;
+  cudaGraphExec_t g_first = nullptr;
+  cudaGraphExec_t g_track = nullptr;
+};
+
+namespace {
+
+__global__ void k_record_pose(const double *pose, double *hist, unsigned long long *count,
+                              int cap) {
+  if (threadIdx.x != 0) return;
+  unsigned long long c = *count;
+  double *dst = hist + (size_t)(c % (unsigned long long)cap) * 16;
+  for (int i = 0; i < 16; ++i) dst[i] = pose[i];
+  *count = c + 1;
+}
+
+of_status_t enqueue_frame(of_tracker *t, bool track, cudaStream_t s) {
+  const of_tracker_desc_t &d = t->desc;
+  of_status_t st;
+  if (track) {
+    st = of_preprocess(&d.camera, &d.filter, t->depth, d.camera.width, t->frame, s);
+    if (st != OF_OK) return st;
+    st = of_icp_launch(&d.camera, &d.icp, t->frame, t->model, t->pose, t->icp_ws, t->stats, s);
+    if (st != OF_OK) return st;
+  }
+  st = of_integrate(&d.volume, t->volume, &d.camera, t->depth, d.camera.width, t->pose, t->lambda,
+                    s);
+  if (st != OF_OK) return st;
+  st = of_raycast(&d.volume, t->volume, &d.camera, &d.raycast, d.icp.levels, t->pose, t->model,
+                  nullptr, s);
+  if (st != OF_OK) return st;
+  k_record_pose<<<1, 32, 0, s>>>(t->pose, t->hist, t->hist_count, t->hist_cap);
+  return of_launch_status();
+}
+
+int count_kernel_nodes(cudaGraph_t g) {
+  size_t n = 0;
+  if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return 0;
+  cudaGraphNode_t *nodes = new cudaGraphNode_t[n];
+  int k = 0;
+  if (cudaGraphGetNodes(g, nodes, &n) == cudaSuccess)
+    for (size_t i = 0; i < n; ++i) {
+      cudaGraphNodeType ty;
+      if (cudaGraphNodeGetType(nodes[i], &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) ++k;
+    }
+  delete[] nodes;
+  return k;
+}
+
+of_status_t capture(of_tracker *t, bool track, cudaGraphExec_t *out) {
+  cudaGraph_t g = nullptr;
+  OF_CUDA_TRY(cudaStreamBeginCapture(t->cap, cudaStreamCaptureModeThreadLocal));
+  of_status_t st = enqueue_frame(t, track, t->cap);
+  cudaError_t e = cudaStreamEndCapture(t->cap, &g);
+  if (st != OF_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  if (e != cudaSuccess) return of_set_cuda_error(e);
+  (track ? t->kernels_track : t->kernels_first) = count_kernel_nodes(g);
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return of_set_cuda_error(e);
+  return OF_OK;
+}
+
+void release(of_tracker *t) {
+  if (t->g_first) cudaGraphExecDestroy(t->g_first);
+  if (t->g_track) cudaGraphExecDestroy(t->g_track);
+  void *bufs[] = {t->volume, t->frame, t->model, t->icp_ws, t->pose, t->hist, t->hist_count,
+                  t->depth, t->lambda, t->stats};
+  for (void *b : bufs)
+    if (b) cudaFree(b);
+  if (t->cap) cudaStreamDestroy(t->cap);
+  delete t;
+}
+
+}  // namespace
+
+extern "C" of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_tracker_t *out) {
+  if (!desc || !out || !of_camera_valid(&desc->camera) || !of_volume_valid(&desc->volume))
+    return OF_ERR_INVALID_ARGUMENT;
+  if (desc->filter.levels != desc->icp.levels || desc->icp.levels < 1 ||
+      desc->icp.levels > kMaxLevels || desc->pose_history < 0)
+    return OF_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  of_tracker *t = new (std::nothrow) of_tracker();
+  if (!t) return OF_ERR_OUT_OF_MEMORY;
+  t->desc = *desc;
+  t->hist_cap = desc->pose_history > 0 ? desc->pose_history : 1024;
+  of_status_t st = of_pyramid_layout(&desc->camera, desc->icp.levels, &t->lay);
+  if (st != OF_OK) { release(t); return st; }
+  cudaError_t e = cudaStreamCreateWithFlags(&t->cap, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { release(t); return of_set_cuda_error(e); }
+  size_t vol_bytes = 0, lam_bytes = 0;
+  of_volume_bytes(&desc->volume, &vol_bytes);
+  of_lambda_bytes(&desc->camera, &lam_bytes);
+  size_t px = (size_t)desc->camera.width * desc->camera.height;
+  struct { void **p; size_t n; } allocs[] = {
+      {&t->volume, vol_bytes},
+      {&t->frame, t->lay.total_bytes},
+      {&t->model, t->lay.total_bytes},
+      {&t->icp_ws, of_icp_workspace_size()},
+      {(void **)&t->pose, 16 * sizeof(double)},
+      {(void **)&t->hist, (size_t)t->hist_cap * 16 * sizeof(double)},
+      {(void **)&t->hist_count, sizeof(unsigned long long)},
+      {(void **)&t->depth, px * sizeof(uint16_t)},
+      {(void **)&t->lambda, lam_bytes},
+      {(void **)&t->stats, sizeof(of_icp_stats_t)},
+  };
+  for (auto &a : allocs) {
+    e = cudaMalloc(a.p, a.n);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      release(t);
+      return e == cudaErrorMemoryAllocation ? OF_ERR_OUT_OF_MEMORY : of_set_cuda_error(e);
+    }
+  }
+  cudaStream_t s = t->cap;
+  bool ok = cudaMemsetAsync(t->icp_ws, 0, of_icp_workspace_size(), s) == cudaSuccess &&
+            cudaMemsetAsync(t->hist_count, 0, sizeof(unsigned long long), s) == cudaSuccess &&
+            cudaMemsetAsync(t->stats, 0, sizeof(of_icp_stats_t), s) == cudaSuccess &&
+            cudaMemsetAsync(t->model, 0, t->lay.total_bytes, s) == cudaSuccess &&
+            cudaMemsetAsync(t->frame, 0, t->lay.total_bytes, s) == cudaSuccess &&
+            cudaMemcpyAsync(t->pose, desc->initial_pose, 16 * sizeof(double),
+                            cudaMemcpyHostToDevice, s) == cudaSuccess;
+  if (!ok) { release(t); return of_set_cuda_error(cudaGetLastError()); }
+  st = of_volume_reset(&desc->volume, t->volume, s);
+  if (st == OF_OK) st = of_lambda_table(&desc->camera, t->lambda, s);
+  if (st == OF_OK && cudaStreamSynchronize(s) != cudaSuccess) st = of_set_cuda_error(cudaGetLastError());
+  if (st == OF_OK && desc->use_graph) {
+    st = capture(t, false, &t->g_first);
+    if (st == OF_OK) st = capture(t, true, &t->g_track);
+  }
+  if (st != OF_OK) { release(t); return st; }
+  *out = t;
+  return OF_OK;
+}
+
+extern "C" of_status_t of_tracker_destroy(of_tracker_t t) {
+  if (!t) return OF_ERR_INVALID_ARGUMENT;
+  cudaDeviceSynchronize();
+  release(t);
+  return OF_OK;
+}
+
+extern "C" of_status_t of_tracker_process(of_tracker_t t, const uint16_t *depth, int32_t on_host,
+                                          of_stream_t stream) {
+  if (!t || !depth) return OF_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = (cudaStream_t)stream;
+  size_t bytes = (size_t)t->desc.camera.width * t->desc.camera.height * sizeof(uint16_t);
+  if (on_host) {
+    OF_CUDA_TRY(cudaMemcpyAsync(t->depth, depth, bytes, cudaMemcpyHostToDevice, s));
+  } else if (depth != t->depth) {
+    OF_CUDA_TRY(cudaMemcpyAsync(t->depth, depth, bytes, cudaMemcpyDeviceToDevice, s));
+  }
+  bool track = t->frames > 0;
+  if (t->desc.use_graph) {
+    OF_CUDA_TRY(cudaGraphLaunch(track ? t->g_track : t->g_first, s));
+  } else {
+    of_status_t st = enqueue_frame(t, track, s);
+    if (st != OF_OK) return st;
+  }
+  t->frames += 1;
+  return OF_OK;
+}
+
+extern "C" of_status_t of_tracker_set_prior(of_tracker_t t, const double *delta) {
+  if (!t) return OF_ERR_INVALID_ARGUMENT;
+  of_status_t st = of_icp_set_prior(t->icp_ws, delta, t->cap);
+  if (st != OF_OK) return st;
+  OF_CUDA_TRY(cudaStreamSynchronize(t->cap));
+  return OF_OK;
+}
+
+extern "C" of_status_t of_tracker_pose(of_tracker_t t, double *pose, of_icp_stats_t *stats,
+                                       of_stream_t stream) {
+  if (!t || !pose) return OF_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = (cudaStream_t)stream;
+  OF_CUDA_TRY(cudaMemcpyAsync(pose, t->pose, 16 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (stats)
+    OF_CUDA_TRY(cudaMemcpyAsync(stats, t->stats, sizeof(of_icp_stats_t), cudaMemcpyDeviceToHost, s));
+  return OF_OK;
+}
+
+extern "C" of_status_t of_tracker_pose_history(of_tracker_t t, double *poses, int32_t count,
+                                               of_stream_t stream) {
+  if (!t || !poses || count < 0 || count > t->hist_cap || count > t->frames)
+    return OF_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = (cudaStream_t)stream;
+  OF_CUDA_TRY(cudaStreamSynchronize(s));
+  int64_t first = t->frames - count;
+  for (int32_t i = 0; i < count; ++i) {
+    int64_t slot = (first + i) % t->hist_cap;
+    OF_CUDA_TRY(cudaMemcpy(poses + 16 * (size_t)i, t->hist + 16 * (size_t)slot,
+                           16 * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  return OF_OK;
+}
+
+extern "C" of_status_t of_tracker_buffers(of_tracker_t t, of_tracker_buffers_t *out) {
+  if (!t || !out) return OF_ERR_INVALID_ARGUMENT;
+  out->volume = t->volume;
+  out->frame = t->frame;
+  out->model = t->model;
+  out->pose = t->pose;
+  out->depth = t->depth;
+  out->lambda = t->lambda;
+  out->stats = t->stats;
+  out->frames = t->frames;
+  out->kernels_first = t->kernels_first;
+  out->kernels_track = t->kernels_track;
+  return OF_OK;
+}

@@ -1,0 +1,237 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+`Oracle("f64")` loads the FP64 checker, `Oracle("f32")` the FP32 OpenMP CPU
+baseline; both are the same restatement (of_oracle.c). Only tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline leg use this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+BUILD = HERE / "_build"
+LIBS = {"f64": "liboracle_f64.so", "f32": "libcpu_f32_omp.so"}
+
+
+class Cam(C.Structure):
+    _fields_ = [("w", C.c_int32), ("h", C.c_int32), ("fx", C.c_double), ("fy", C.c_double),
+                ("cx", C.c_double), ("cy", C.c_double), ("dmin", C.c_double),
+                ("dmax", C.c_double)]
+
+
+class Vol(C.Structure):
+    _fields_ = [("n", C.c_int32), ("storage", C.c_int32), ("size", C.c_double),
+                ("trunc", C.c_double), ("max_w", C.c_int32), ("pad", C.c_int32)]
+
+
+class Params(C.Structure):
+    _fields_ = [("sigma_s", C.c_double), ("sigma_r", C.c_double), ("radius", C.c_int32),
+                ("levels", C.c_int32), ("iters", C.c_int32 * 4), ("dist_thresh", C.c_double),
+                ("normal_thresh", C.c_double), ("min_step_vox", C.c_double),
+                ("far_step_frac", C.c_double), ("refine_iters", C.c_int32), ("pad", C.c_int32)]
+
+
+def build() -> None:
+    """Compiles the oracle libraries (gcc; see oracle/Makefile)."""
+    res = subprocess.run(["make", "-s", "-C", str(HERE)], capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + res.stdout + res.stderr)
+
+
+P = C.c_void_p
+
+
+class Oracle:
+    def __init__(self, kind: str = "f64"):
+        path = BUILD / LIBS[kind]
+        if not path.exists():
+            build()
+        self.lib = C.CDLL(str(path))
+        L = self.lib
+        L.ora_real_bytes.restype = C.c_int32
+        L.ora_threads.restype = C.c_int32
+        self.real = np.float64 if L.ora_real_bytes() == 8 else np.float32
+        L.ora_cam_level.argtypes = [C.POINTER(Cam), C.c_int32, C.POINTER(Cam)]
+        L.ora_bilateral.argtypes = [C.POINTER(Cam), P, C.c_double, C.c_double, C.c_int32, P]
+        L.ora_pyr_down.argtypes = [P, C.c_int32, C.c_int32, P, C.c_int32, C.c_int32, C.c_double]
+        L.ora_vertex_normal.argtypes = [C.POINTER(Cam), P, P]
+        L.ora_preprocess.argtypes = [C.POINTER(Cam), C.POINTER(Params), P, P]
+        L.ora_pyramid_elems.argtypes = [C.POINTER(Cam), C.c_int32]
+        L.ora_pyramid_elems.restype = C.c_int64
+        L.ora_integrate.argtypes = [C.POINTER(Vol), P, C.POINTER(Cam), P, P, P]
+        L.ora_integrate.restype = C.c_int64
+        L.ora_raycast.argtypes = [C.POINTER(Vol), P, C.POINTER(Cam), C.POINTER(Params), P, P, P]
+        L.ora_model_down.argtypes = [P, C.c_int32, P, C.c_int32, C.c_int32]
+        L.ora_icp_system.argtypes = [C.POINTER(Cam), P, C.c_int32, C.c_int32, P, P, C.c_double,
+                                     C.c_double, P, P]
+        L.ora_icp_step.argtypes = [P, P, P]
+        L.ora_icp_step.restype = C.c_int32
+        L.ora_icp_track.argtypes = [C.POINTER(Cam), C.POINTER(Params), P, P, P, P]
+        L.ora_icp_track.restype = C.c_int32
+        L.ora_tracker_create.argtypes = [C.POINTER(Cam), C.POINTER(Vol), C.POINTER(Params), P]
+        L.ora_tracker_create.restype = C.c_void_p
+        L.ora_tracker_destroy.argtypes = [P]
+        L.ora_tracker_process.argtypes = [P, P]
+        L.ora_tracker_process.restype = C.c_int32
+        L.ora_tracker_pose.argtypes = [P, P]
+        L.ora_tracker_volume.argtypes = [P]
+        L.ora_tracker_volume.restype = C.c_void_p
+
+    # ----------------------------------------------------------- parameters
+    @staticmethod
+    def cam(cfg, level: int = 0) -> Cam:
+        c = Cam(cfg.width, cfg.height, cfg.fx, cfg.fy, cfg.cx, cfg.cy, cfg.min_depth_mm,
+                cfg.max_depth_mm)
+        if level:
+            out = Cam()
+            Oracle._any().lib.ora_cam_level(C.byref(c), level, C.byref(out))
+            return out
+        return c
+
+    _inst = None
+
+    @staticmethod
+    def _any() -> "Oracle":
+        if Oracle._inst is None:
+            Oracle._inst = Oracle("f64")
+        return Oracle._inst
+
+    @staticmethod
+    def vol(cfg) -> Vol:
+        return Vol(cfg.resolution, 0 if cfg.storage == "i16" else 1, cfg.size_mm, cfg.trunc_mm,
+                   cfg.max_weight, 0)
+
+    @staticmethod
+    def params(cfg) -> Params:
+        it = (C.c_int32 * 4)(*(list(cfg.iters) + [0] * (4 - len(cfg.iters))))
+        return Params(cfg.sigma_space_px, cfg.sigma_range_mm, cfg.radius_px, cfg.levels, it,
+                      cfg.dist_thresh_mm, cfg.normal_thresh, cfg.min_step_vox, cfg.far_step_frac,
+                      cfg.refine_iters, 0)
+
+    # --------------------------------------------------------------- stages
+    def level_dims(self, cfg):
+        out = []
+        for l in range(cfg.levels):
+            c = self.cam(cfg, l)
+            out.append((c.w, c.h))
+        return out
+
+    def preprocess(self, cfg, depth: np.ndarray):
+        """-> list per level of (depth[h,w], pts[h,w,8])"""
+        d = np.ascontiguousarray(depth, np.uint16)
+        n = self.lib.ora_pyramid_elems(C.byref(self.cam(cfg)), cfg.levels)
+        buf = np.zeros(n, self.real)
+        self.lib.ora_preprocess(C.byref(self.cam(cfg)), C.byref(self.params(cfg)), d.ctypes.data,
+                                buf.ctypes.data)
+        return self.split_pyramid(cfg, buf), buf
+
+    def split_pyramid(self, cfg, buf):
+        out, off = [], 0
+        for (w, h) in self.level_dims(cfg):
+            dep = buf[off: off + w * h].reshape(h, w)
+            off += w * h
+            pts = buf[off: off + w * h * 8].reshape(h, w, 8)
+            off += w * h * 8
+            out.append((dep, pts))
+        return out
+
+    def pack_pyramid(self, cfg, levels_pts, levels_depth=None) -> np.ndarray:
+        parts = []
+        for l, (w, h) in enumerate(self.level_dims(cfg)):
+            dep = np.zeros(w * h, self.real) if levels_depth is None else \
+                np.asarray(levels_depth[l], self.real).reshape(-1)
+            parts += [dep, np.asarray(levels_pts[l], self.real).reshape(-1)]
+        return np.ascontiguousarray(np.concatenate(parts))
+
+    def integrate(self, cfg, words: np.ndarray, depth: np.ndarray, pose: np.ndarray,
+                  ambig: bool = False):
+        """In-place update of linear-layout uint32 `words`; returns (updated, ambig mask)."""
+        assert words.dtype == np.uint32 and words.flags.c_contiguous
+        d = np.ascontiguousarray(depth, np.uint16)
+        P_ = np.ascontiguousarray(pose, np.float64)
+        am = np.zeros(words.shape, np.uint8) if ambig else None
+        n = self.lib.ora_integrate(C.byref(self.vol(cfg)), words.ctypes.data,
+                                   C.byref(self.cam(cfg)), d.ctypes.data, P_.ctypes.data,
+                                   None if am is None else am.ctypes.data)
+        return n, am
+
+    def raycast(self, cfg, words: np.ndarray, pose: np.ndarray, ambig: bool = False):
+        P_ = np.ascontiguousarray(pose, np.float64)
+        pts = np.zeros((cfg.height, cfg.width, 8), self.real)
+        am = np.zeros((cfg.height, cfg.width), np.uint8) if ambig else None
+        self.lib.ora_raycast(C.byref(self.vol(cfg)), words.ctypes.data, C.byref(self.cam(cfg)),
+                             C.byref(self.params(cfg)), P_.ctypes.data, pts.ctypes.data,
+                             None if am is None else am.ctypes.data)
+        return pts, am
+
+    def model_pyramid(self, cfg, pts0: np.ndarray):
+        lv = [np.ascontiguousarray(pts0, self.real)]
+        for (w, h) in self.level_dims(cfg)[1:]:
+            src = lv[-1]
+            dst = np.zeros((h, w, 8), self.real)
+            self.lib.ora_model_down(src.ctypes.data, src.shape[1], dst.ctypes.data, w, h)
+            lv.append(dst)
+        return lv
+
+    def icp_system(self, cfg, level: int, frame_pts, model_pts, pose):
+        f = np.ascontiguousarray(frame_pts, self.real)
+        m = np.ascontiguousarray(model_pts, self.real)
+        P_ = np.ascontiguousarray(pose, np.float64)
+        out = np.zeros(29)
+        amb = np.zeros(29)
+        self.lib.ora_icp_system(C.byref(self.cam(cfg, level)), f.ctypes.data, m.shape[1],
+                                m.shape[0], m.ctypes.data, P_.ctypes.data, cfg.dist_thresh_mm,
+                                cfg.normal_thresh, out.ctypes.data, amb.ctypes.data)
+        return out, amb
+
+    def icp_step(self, sys: np.ndarray, pose: np.ndarray):
+        s = np.ascontiguousarray(sys, np.float64)
+        P_ = np.array(pose, np.float64, copy=True)
+        mp = C.c_double()
+        st = self.lib.ora_icp_step(s.ctypes.data, P_.ctypes.data, C.byref(mp))
+        return st, P_, mp.value
+
+    def icp_track(self, cfg, frame_buf: np.ndarray, model_buf: np.ndarray, pose: np.ndarray):
+        P_ = np.array(pose, np.float64, copy=True)
+        its = C.c_int32()
+        st = self.lib.ora_icp_track(C.byref(self.cam(cfg)), C.byref(self.params(cfg)),
+                                    frame_buf.ctypes.data, model_buf.ctypes.data, P_.ctypes.data,
+                                    C.byref(its))
+        return st, P_, its.value
+
+    def threads(self) -> int:
+        return self.lib.ora_threads()
+
+
+class CpuTracker:
+    """The whole frame loop on the CPU (FP64 oracle or FP32 OpenMP baseline)."""
+
+    def __init__(self, oracle: Oracle, cfg, pose0):
+        self.o = oracle
+        self.cfg = cfg
+        P_ = np.ascontiguousarray(pose0, np.float64)
+        self.h = oracle.lib.ora_tracker_create(C.byref(Oracle.cam(cfg)), C.byref(Oracle.vol(cfg)),
+                                               C.byref(Oracle.params(cfg)), P_.ctypes.data)
+        if not self.h:
+            raise MemoryError("ora_tracker_create failed")
+
+    def process(self, depth: np.ndarray) -> int:
+        d = np.ascontiguousarray(depth, np.uint16)
+        return self.o.lib.ora_tracker_process(self.h, d.ctypes.data)
+
+    def pose(self) -> np.ndarray:
+        P_ = np.zeros(16)
+        self.o.lib.ora_tracker_pose(self.h, P_.ctypes.data)
+        return P_.reshape(4, 4)
+
+    def close(self):
+        if self.h:
+            self.o.lib.ora_tracker_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

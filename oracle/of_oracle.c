@@ -1,0 +1,697 @@
+/* of_oracle.c -- CPU restatement of the KinectFusion per-frame path.
+ *
+ * TEST INFRASTRUCTURE ONLY (see of_oracle.h): the checker of the CUDA path,
+ * and, compiled with OF_REAL=float and OpenMP, the CPU baseline.
+ * Reference citations are paths inside gilbs10/OpenFusion.
+ */
+#include "of_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef ora_real R;
+
+#define EPS_REF 1e-6 /* _EPSILON_, Source/include/Constants.h:14 */
+
+int32_t ora_real_bytes(void) { return (int32_t)sizeof(R); }
+
+int32_t ora_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+void ora_cam_level(const ora_cam *c, int32_t level, ora_cam *o) {
+  *o = *c;
+  for (int l = 0; l < level; ++l) {
+    o->w = (o->w + 1) / 2;
+    o->h = (o->h + 1) / 2;
+    o->fx *= 0.5;
+    o->fy *= 0.5;
+    o->cx = (o->cx - 0.5) * 0.5;
+    o->cy = (o->cy - 0.5) * 0.5;
+  }
+}
+
+/* roundFloat: frac < 0.5 ? floor : ceil (Source/include/CudaUtilities.cuh:62-64) */
+static inline int round_ref(R a) {
+  R f = (R)floor(a);
+  return (a - f) < (R)0.5 ? (int)f : (int)ceil(a);
+}
+
+static inline int near_half(double a, double margin) {
+  double f = a - floor(a);
+  return fabs(f - 0.5) < margin;
+}
+
+/* ------------------------------------------------------------------------
+ * Bilateral filter: Tomasi & Manduchi (ICCV 1998) on the raw depth, square
+ * window of half-width `radius`, Gaussian spatial (sigma_s px) and range
+ * (sigma_r mm) weights; invalid depths (outside [dmin, dmax] or 0) take no
+ * part and an invalid centre stays 0 -- the pre-filter of KinectFusion
+ * (Newcombe et al., ISMAR 2011, s3.2). No reference counterpart.
+ * ---------------------------------------------------------------------- */
+static inline int depth_ok(double d, const ora_cam *c) {
+  return d > 0.0 && d >= c->dmin && d <= c->dmax;
+}
+
+void ora_bilateral(const ora_cam *c, const uint16_t *depth, double ss, double sr, int32_t rad,
+                   R *out) {
+  const int w = c->w, h = c->h;
+  const double ks = 1.0 / (2.0 * ss * ss), kr = 1.0 / (2.0 * sr * sr);
+#pragma omp parallel for schedule(static)
+  for (int y = 0; y < h; ++y) {
+    for (int x = 0; x < w; ++x) {
+      double cd = depth[(size_t)y * w + x];
+      R res = 0;
+      if (depth_ok(cd, c)) {
+        R sw = 0, sd = 0;
+        for (int dy = -rad; dy <= rad; ++dy) {
+          int yy = y + dy;
+          if (yy < 0 || yy >= h) continue;
+          for (int dx = -rad; dx <= rad; ++dx) {
+            int xx = x + dx;
+            if (xx < 0 || xx >= w) continue;
+            double q = depth[(size_t)yy * w + xx];
+            if (!depth_ok(q, c)) continue;
+            double del = q - cd;
+            R wt = (R)exp(-((double)(dx * dx + dy * dy) * ks + del * del * kr));
+            sw += wt;
+            sd += wt * (R)q;
+          }
+        }
+        res = sd / sw;
+      }
+      out[(size_t)y * w + x] = res;
+    }
+  }
+}
+
+/* Depth pyramid: block averaging of KinectFusion s3.2 with its 3 sigma_r
+ * guard; a 2x2 block is averaged over its valid depths within `guard` of the
+ * block's first valid depth (row-major). No reference counterpart. */
+void ora_pyr_down(const R *src, int32_t sw, int32_t sh, R *dst, int32_t dw, int32_t dh,
+                  double guard) {
+#pragma omp parallel for schedule(static)
+  for (int y = 0; y < dh; ++y)
+    for (int x = 0; x < dw; ++x) {
+      R ref = 0, sum = 0;
+      int cnt = 0;
+      for (int j = 0; j < 2; ++j)
+        for (int i = 0; i < 2; ++i) {
+          int sx = 2 * x + i, sy = 2 * y + j;
+          if (sx >= sw || sy >= sh) continue;
+          R d = src[(size_t)sy * sw + sx];
+          if (d > 0) {
+            if (cnt == 0) ref = d;
+            if (fabs((double)(d - ref)) <= guard) {
+              sum += d;
+              ++cnt;
+            }
+          }
+        }
+      dst[(size_t)y * dw + x] = cnt ? sum / (R)cnt : (R)0;
+    }
+}
+
+/* Vertex map: d_convertDepthToWorldVertices (CameraHandler.cu:65-89) in
+ * camera space: v = (-d (u-cx)/fx, -d (v-cy)/fy, -d) (CudaUtilities.cuh:24-33
+ * with depth -d). Normal map: d_convertDepthToWorldNormals
+ * (CameraHandler.cu:91-132): normalize((v(x+1,y)-v) x (v(x,y+1)-v)), invalid
+ * on the last row/column or next to an invalid vertex; a zero cross product
+ * stays invalid (cutil_math.h:1131-1137 returns the zero vector). */
+void ora_vertex_normal(const ora_cam *c, const R *depth, R *pts) {
+  const int w = c->w, h = c->h;
+#pragma omp parallel for schedule(static)
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      size_t p = (size_t)y * w + x;
+      R *o = pts + 8 * p;
+      for (int i = 0; i < 8; ++i) o[i] = 0;
+      R d = depth[p];
+      if (!(d > 0)) continue;
+      R ax = (R)((double)x - c->cx), ay = (R)((double)y - c->cy);
+      R vx = -d * ax / (R)c->fx, vy = -d * ay / (R)c->fy, vz = -d;
+      o[0] = vx; o[1] = vy; o[2] = vz; o[3] = 1;
+      if (x + 1 >= w || y + 1 >= h) continue;
+      R d10 = depth[p + 1], d01 = depth[p + w];
+      if (!(d10 > 0 && d01 > 0)) continue;
+      R a0 = -d10 * (ax + 1) / (R)c->fx - vx, a1 = -d10 * ay / (R)c->fy - vy, a2 = -d10 - vz;
+      R b0 = -d01 * ax / (R)c->fx - vx, b1 = -d01 * (ay + 1) / (R)c->fy - vy, b2 = -d01 - vz;
+      R n0 = a1 * b2 - a2 * b1, n1 = a2 * b0 - a0 * b2, n2 = a0 * b1 - a1 * b0;
+      R l2 = n0 * n0 + n1 * n1 + n2 * n2;
+      if (!(l2 > 0)) continue;
+      R il = (R)(1.0 / sqrt((double)l2));
+      o[4] = n0 * il; o[5] = n1 * il; o[6] = n2 * il; o[7] = 1;
+    }
+}
+
+int64_t ora_pyramid_elems(const ora_cam *c, int32_t levels) {
+  int64_t n = 0;
+  for (int l = 0; l < levels; ++l) {
+    ora_cam lc;
+    ora_cam_level(c, l, &lc);
+    n += (int64_t)lc.w * lc.h * 9;
+  }
+  return n;
+}
+
+void ora_preprocess(const ora_cam *c, const ora_params *p, const uint16_t *depth, R *out) {
+  int rad = p->radius > 0 ? p->radius : (int)ceil(2.0 * p->sigma_s);
+  R *lvl_depth[4];
+  R *lvl_pts[4];
+  ora_cam lc[4];
+  R *q = out;
+  for (int l = 0; l < p->levels; ++l) {
+    ora_cam_level(c, l, &lc[l]);
+    lvl_depth[l] = q;
+    q += (size_t)lc[l].w * lc[l].h;
+    lvl_pts[l] = q;
+    q += (size_t)lc[l].w * lc[l].h * 8;
+  }
+  ora_bilateral(c, depth, p->sigma_s, p->sigma_r, rad, lvl_depth[0]);
+  for (int l = 1; l < p->levels; ++l)
+    ora_pyr_down(lvl_depth[l - 1], lc[l - 1].w, lc[l - 1].h, lvl_depth[l], lc[l].w, lc[l].h,
+                 3.0 * p->sigma_r);
+  for (int l = 0; l < p->levels; ++l) ora_vertex_normal(&lc[l], lvl_depth[l], lvl_pts[l]);
+}
+
+/* ------------------------------------------------------------------ voxels */
+
+static inline float half_to_float(uint16_t h) {
+  _Float16 v;
+  memcpy(&v, &h, 2);
+  return (float)v;
+}
+static inline uint16_t float_to_half(double x) {
+  _Float16 v = (_Float16)(float)x;
+  uint16_t h;
+  memcpy(&h, &v, 2);
+  return h;
+}
+
+/* normalised tsdf; weight 0 reads +1 (d_initVoxelArray sets +TRUNCATION,
+ * Source/src/General.cu:27-50) */
+static inline R vox_value(uint32_t w, int storage) {
+  if ((w >> 16) == 0) return 1;
+  uint16_t lo = (uint16_t)(w & 0xffffu);
+  if (storage == 0) return (R)(int16_t)lo / (R)32767.0;
+  return (R)half_to_float(lo);
+}
+
+static inline uint32_t vox_pack(R t, uint32_t weight, int storage) {
+  if (storage == 0) {
+    double q = nearbyint((double)t * 32767.0);
+    if (q > 32767.0) q = 32767.0;
+    if (q < -32767.0) q = -32767.0;
+    return (uint32_t)(uint16_t)(int16_t)q | (weight << 16);
+  }
+  double tc = t > 1 ? 1.0 : (t < -1 ? -1.0 : (double)t);
+  return (uint32_t)float_to_half(tc) | (weight << 16);
+}
+
+/* Integration: d_integrateVolume (Source/src/VolumeIntegrator.cu:86-187) with
+ * voxel x stored in slab x (the reference increments `offset` before its
+ * first use, :115-123, so its voxel x lands in slab x+1):
+ *   centre p_w = -size/2 + (i + 0.5) size/n (convertVoxelsToWorld, :40-48)
+ *   p_c = T^-1 p_w (:126); skip unless -z in [dmin, dmax] and z < 0 (:12-16;
+ *   the z < 0 test keeps voxels behind the camera out, which the reference's
+ *   fabs(z) test lets through); pixel = roundFloat(project) (:127-129); skip
+ *   inside the 2-pixel border (:14-15) or on invalid depth (:136-140);
+ *   SDF = |v_depth - c| - |p_w - c| (:146) with |v_depth - c| = lambda D;
+ *   skip SDF < -trunc, tsdf' = min(SDF, trunc) (:148-160);
+ *   tsdf = (tsdf w + tsdf') / (w + 1), w = min(max_w, w + 1) (:165-166). */
+int64_t ora_integrate(const ora_vol *v, uint32_t *words, const ora_cam *c, const uint16_t *depth,
+                      const double *P, uint8_t *ambig) {
+  const int n = v->n;
+  const double vs = v->size / n, org = -0.5 * v->size, T = v->trunc;
+  const double cpos[3] = {P[3], P[7], P[11]};
+  int64_t updated = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : updated)
+  for (int i = 0; i < n; ++i) {
+    for (int j = 0; j < n; ++j) {
+      for (int k = 0; k < n; ++k) {
+        size_t idx = ((size_t)i * n + j) * n + k;
+        int amb = 0;
+        R pw[3] = {(R)(org + vs * (i + 0.5)), (R)(org + vs * (j + 0.5)), (R)(org + vs * (k + 0.5))};
+        R dlt[3] = {pw[0] - (R)cpos[0], pw[1] - (R)cpos[1], pw[2] - (R)cpos[2]};
+        R X = (R)P[0] * dlt[0] + (R)P[4] * dlt[1] + (R)P[8] * dlt[2];
+        R Y = (R)P[1] * dlt[0] + (R)P[5] * dlt[1] + (R)P[9] * dlt[2];
+        R Z = (R)P[2] * dlt[0] + (R)P[6] * dlt[1] + (R)P[10] * dlt[2];
+        if (ambig) {
+          if (fabs(-(double)Z - c->dmin) < 1e-2 || fabs(-(double)Z - c->dmax) < 1e-2) amb = 1;
+        }
+        int upd = 0;
+        R sn = 0;
+        if (Z < 0 && -Z >= (R)c->dmin && -Z <= (R)c->dmax) {
+          R uf = (R)c->fx * X / Z + (R)c->cx;
+          R vf = (R)c->fy * Y / Z + (R)c->cy;
+          if (ambig && (near_half(uf, 2e-3) || near_half(vf, 2e-3))) amb = 1;
+          int pu = round_ref(uf), pv = round_ref(vf);
+          if (!(pu < 2 || pu >= c->w - 2 || pv < 2 || pv >= c->h - 2)) {
+            double D = depth[(size_t)pv * c->w + pu];
+            if (depth_ok(D, c)) {
+              R a = (R)(((double)pu - c->cx) / c->fx), b = (R)(((double)pv - c->cy) / c->fy);
+              R lam = (R)sqrt((double)(1 + a * a + b * b));
+              R rr = (R)sqrt((double)(dlt[0] * dlt[0] + dlt[1] * dlt[1] + dlt[2] * dlt[2]));
+              R sdf = lam * (R)D - rr;
+              if (ambig && fabs((double)sdf + T) < 1e-3) amb = 1;
+              if (sdf >= -(R)T) {
+                upd = 1;
+                sn = (sdf < (R)T ? sdf : (R)T) / (R)T;
+              }
+            }
+          }
+        }
+        if (ambig) ambig[idx] = (uint8_t)amb;
+        if (!upd) continue;
+        ++updated;
+        uint32_t word = words[idx];
+        uint32_t wt = word >> 16;
+        R told = wt ? vox_value(word, v->storage) : 0;
+        R tn = (told * (R)wt + sn) / (R)(wt + 1);
+        uint32_t wn = wt + 1 < (uint32_t)v->max_w ? wt + 1 : (uint32_t)v->max_w;
+        words[idx] = vox_pack(tn, wn, v->storage);
+      }
+    }
+  }
+  return updated;
+}
+
+/* ---------------------------------------------------------------- raycast */
+
+typedef struct {
+  const uint32_t *w;
+  int n, storage;
+  double org, inv_vs;
+} vol_view;
+
+static R trilinear(const vol_view *V, R px, R py, R pz) {
+  R g[3] = {(R)(((double)px - V->org) * V->inv_vs - 0.5), (R)(((double)py - V->org) * V->inv_vs - 0.5),
+            (R)(((double)pz - V->org) * V->inv_vs - 0.5)};
+  int i0[3];
+  R f[3];
+  for (int a = 0; a < 3; ++a) {
+    int q = (int)floor(g[a]);
+    if (q < 0) q = 0;
+    if (q > V->n - 2) q = V->n - 2;
+    i0[a] = q;
+    f[a] = g[a] - (R)q;
+  }
+  R cval[8];
+  for (int q = 0; q < 8; ++q) {
+    int a = (q >> 2) & 1, b = (q >> 1) & 1, d = q & 1;
+    size_t idx = ((size_t)(i0[0] + a) * V->n + (i0[1] + b)) * V->n + (i0[2] + d);
+    cval[q] = vox_value(V->w[idx], V->storage);
+  }
+  R c00 = cval[0] + f[2] * (cval[1] - cval[0]);
+  R c01 = cval[2] + f[2] * (cval[3] - cval[2]);
+  R c10 = cval[4] + f[2] * (cval[5] - cval[4]);
+  R c11 = cval[6] + f[2] * (cval[7] - cval[6]);
+  R c0 = c00 + f[1] * (c01 - c00);
+  R c1 = c10 + f[1] * (c11 - c10);
+  return c0 + f[0] * (c1 - c0);
+}
+
+/* Raycast: d_raycast (Source/src/Raycaster.cu:97-230) -- ray from the camera
+ * position through the pixel's point at z = -1 (:117-125), slab clip
+ * (:35-55) to the box of voxel centres, march to the first surface. The
+ * sampling follows KinectFusion s3.4 (the trilinear zero-crossing the
+ * reference left disabled, :170-187, :246-351): trilinear tsdf samples, step
+ * max(min_step, far_frac * f * trunc) for f > 0 else min_step, surface at a
+ * + -> - crossing refined by `refine_iters` regula-falsi steps, - -> + ends
+ * the ray; normal = normalised central differences of trilinear samples one
+ * voxel apart; the march is limited to [dmin, dmax] depth. */
+void ora_raycast(const ora_vol *v, const uint32_t *words, const ora_cam *c, const ora_params *p,
+                 const double *P, R *pts, uint8_t *ambig) {
+  const int n = v->n;
+  const double vs = v->size / n;
+  vol_view V = {words, n, v->storage, -0.5 * v->size, 1.0 / vs};
+  const R lo = (R)(-0.5 * v->size + 0.5 * vs + 1e-3), hi = (R)(0.5 * v->size - 0.5 * vs - 1e-3);
+  const R min_step = (R)(p->min_step_vox * vs), far_k = (R)(p->far_step_frac * v->trunc);
+  const R o[3] = {(R)P[3], (R)P[7], (R)P[11]};
+  const R rvs = (R)vs;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int y = 0; y < c->h; ++y) {
+    for (int x = 0; x < c->w; ++x) {
+      size_t pix = (size_t)y * c->w + x;
+      int amb = 0;
+      R dc[3] = {(R)(-((double)x - c->cx) / c->fx), (R)(-((double)y - c->cy) / c->fy), -1};
+      R lam = (R)sqrt((double)(dc[0] * dc[0] + dc[1] * dc[1] + 1));
+      R dir[3];
+      for (int a = 0; a < 3; ++a)
+        dir[a] = ((R)P[4 * a] * dc[0] + (R)P[4 * a + 1] * dc[1] + (R)P[4 * a + 2] * dc[2]) / lam;
+      R tnear = (R)-1e30, tfar = (R)1e30;
+      for (int a = 0; a < 3; ++a) {
+        if (fabs((double)dir[a]) < 1e-12) {
+          if (o[a] < lo || o[a] > hi) { tnear = (R)1e30; tfar = (R)-1e30; }
+        } else {
+          R t0 = (lo - o[a]) / dir[a], t1 = (hi - o[a]) / dir[a];
+          R mn = t0 < t1 ? t0 : t1, mx = t0 < t1 ? t1 : t0;
+          if (mn > tnear) tnear = mn;
+          if (mx < tfar) tfar = mx;
+        }
+      }
+      R t0 = tnear > (R)c->dmin * lam ? tnear : (R)c->dmin * lam;
+      R t1 = tfar < (R)c->dmax * lam ? tfar : (R)c->dmax * lam;
+      int hit = 0;
+      R ts = 0;
+      if (t0 < t1) {
+        R t = t0;
+        R fp = trilinear(&V, o[0] + t * dir[0], o[1] + t * dir[1], o[2] + t * dir[2]);
+        for (int it = 0; it < (1 << 16); ++it) {
+          R step = fp > 0 ? (far_k * fp > min_step ? far_k * fp : min_step) : min_step;
+          R tn = t + step;
+          if (ambig && fabs((double)(tn - t1)) < 0.05) amb = 1;
+          if (tn > t1) break;
+          R fn = trilinear(&V, o[0] + tn * dir[0], o[1] + tn * dir[1], o[2] + tn * dir[2]);
+          if (ambig && fabs((double)fn) < 2e-4) amb = 1;
+          if (fp > 0 && fn <= 0) {
+            R ta = t, fa = fp, tb = tn, fb = fn;
+            for (int r = 0; r < p->refine_iters; ++r) {
+              R tm = ta + (tb - ta) * (fa / (fa - fb));
+              R fm = trilinear(&V, o[0] + tm * dir[0], o[1] + tm * dir[1], o[2] + tm * dir[2]);
+              if (fm > 0) { ta = tm; fa = fm; } else { tb = tm; fb = fm; }
+            }
+            ts = ta + (tb - ta) * (fa / (fa - fb));
+            hit = 1;
+            break;
+          }
+          if (fp < 0 && fn > 0) break;
+          t = tn;
+          fp = fn;
+        }
+      }
+      R *out = pts + 8 * pix;
+      for (int i = 0; i < 8; ++i) out[i] = 0;
+      if (hit) {
+        R px = o[0] + ts * dir[0], py = o[1] + ts * dir[1], pz = o[2] + ts * dir[2];
+        out[0] = px; out[1] = py; out[2] = pz; out[3] = 1;
+        if (px - rvs >= lo && px + rvs <= hi && py - rvs >= lo && py + rvs <= hi &&
+            pz - rvs >= lo && pz + rvs <= hi) {
+          R gx = trilinear(&V, px + rvs, py, pz) - trilinear(&V, px - rvs, py, pz);
+          R gy = trilinear(&V, px, py + rvs, pz) - trilinear(&V, px, py - rvs, pz);
+          R gz = trilinear(&V, px, py, pz + rvs) - trilinear(&V, px, py, pz - rvs);
+          R l2 = gx * gx + gy * gy + gz * gz;
+          if (l2 > 0) {
+            R il = (R)(1.0 / sqrt((double)l2));
+            out[4] = gx * il; out[5] = gy * il; out[6] = gz * il; out[7] = 1;
+          }
+          if (ambig && (fabs((double)px - rvs - lo) < 0.05 || fabs((double)hi - px - rvs) < 0.05 ||
+                        fabs((double)py - rvs - lo) < 0.05 || fabs((double)hi - py - rvs) < 0.05 ||
+                        fabs((double)pz - rvs - lo) < 0.05 || fabs((double)hi - pz - rvs) < 0.05))
+            amb = 1;
+        }
+      }
+      if (ambig) ambig[pix] = (uint8_t)amb;
+    }
+  }
+}
+
+void ora_model_down(const R *src, int32_t sw, R *dst, int32_t dw, int32_t dh) {
+  for (int y = 0; y < dh; ++y)
+    for (int x = 0; x < dw; ++x)
+      memcpy(dst + 8 * ((size_t)y * dw + x), src + 8 * ((size_t)(2 * y) * sw + 2 * x),
+             8 * sizeof(R));
+}
+
+/* -------------------------------------------------------------------- ICP */
+
+/* Correspondence + point-to-plane row of one model pixel:
+ * d_find_corresponding (Source/src/ICP.cu:116-251). Returns 1 and fills
+ * a[6], b when the pixel is an inlier. With `alt` != 0 the other rounding of
+ * the projected coordinate is used on the axes whose bit is set. */
+static int icp_row(const ora_cam *lc, const R *frame, const R *s, const R *ns, const double *P,
+                   const double *W, double dist, double nthr, int alt, R *a, R *b, int *gate_amb,
+                   int *round_amb) {
+  R sc[3];
+  for (int r = 0; r < 3; ++r)
+    sc[r] = (R)W[4 * r] * s[0] + (R)W[4 * r + 1] * s[1] + (R)W[4 * r + 2] * s[2] + (R)W[4 * r + 3];
+  if (sc[2] >= (R)-EPS_REF) return 0;
+  R uf = (R)lc->fx * sc[0] / sc[2] + (R)lc->cx;
+  R vf = (R)lc->fy * sc[1] / sc[2] + (R)lc->cy;
+  if (round_amb) *round_amb = (near_half(uf, 1e-3) ? 1 : 0) | (near_half(vf, 1e-3) ? 2 : 0);
+  int pu = round_ref(uf), pv = round_ref(vf);
+  if (alt & 1) pu = (uf - floor(uf) < 0.5) ? pu + 1 : pu - 1;
+  if (alt & 2) pv = (vf - floor(vf) < 0.5) ? pv + 1 : pv - 1;
+  if (pu < 0 || pu >= lc->w || pv < 0 || pv >= lc->h) return 0;
+  const R *f = frame + 8 * ((size_t)pv * lc->w + pu);
+  if (f[3] == 0 || f[7] == 0) return 0;
+  R d[3], nd[3];
+  for (int r = 0; r < 3; ++r) {
+    d[r] = (R)P[4 * r] * f[0] + (R)P[4 * r + 1] * f[1] + (R)P[4 * r + 2] * f[2] + (R)P[4 * r + 3];
+    nd[r] = (R)P[4 * r] * f[4] + (R)P[4 * r + 1] * f[5] + (R)P[4 * r + 2] * f[6];
+  }
+  R e[3] = {d[0] - s[0], d[1] - s[1], d[2] - s[2]};
+  R len = (R)sqrt((double)(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]));
+  R dn = nd[0] * ns[0] + nd[1] * ns[1] + nd[2] * ns[2];
+  if (gate_amb)
+    *gate_amb = fabs((double)len - dist) < 1e-3 || fabs((double)dn - nthr) < 1e-5 ||
+                fabs((double)dn - (1.0 + EPS_REF)) < 1e-6;
+  a[0] = ns[1] * d[2] - ns[2] * d[1];
+  a[1] = ns[2] * d[0] - ns[0] * d[2];
+  a[2] = ns[0] * d[1] - ns[1] * d[0];
+  a[3] = ns[0]; a[4] = ns[1]; a[5] = ns[2];
+  *b = -(ns[0] * e[0] + ns[1] * e[1] + ns[2] * e[2]);
+  if (!(len < (R)dist)) return gate_amb && *gate_amb ? 2 : 0;
+  if (!(dn > (R)nthr && dn < (R)(1.0 + EPS_REF))) return gate_amb && *gate_amb ? 2 : 0;
+  return 1;
+}
+
+static void row_products(const R *a, R b, double *v) {
+  int k = 0;
+  for (int i = 0; i < 6; ++i)
+    for (int j = i; j < 6; ++j) v[k++] = (double)a[i] * (double)a[j];
+  for (int i = 0; i < 6; ++i) v[21 + i] = (double)a[i] * (double)b;
+  v[27] = (double)b * (double)b;
+  v[28] = 1.0;
+}
+
+static void rigid_inverse(const double *P, double *W) {
+  for (int i = 0; i < 3; ++i) {
+    double acc = 0.0;
+    for (int j = 0; j < 3; ++j) {
+      W[4 * i + j] = P[4 * j + i];
+      acc -= P[4 * j + i] * P[4 * j + 3];
+    }
+    W[4 * i + 3] = acc;
+  }
+  W[12] = W[13] = W[14] = 0.0;
+  W[15] = 1.0;
+}
+
+void ora_icp_system(const ora_cam *lc, const R *frame, int32_t mw, int32_t mh, const R *model,
+                    const double *P, double dist, double nthr, double *out, double *amb) {
+  double W[16];
+  rigid_inverse(P, W);
+  const int npx = mw * mh;
+  double acc[29] = {0}, am[29] = {0};
+  /* rows accumulate per image row, rows combine in order: deterministic */
+  double *rows = (double *)calloc((size_t)mh * 58, sizeof(double));
+#pragma omp parallel for schedule(static)
+  for (int y = 0; y < mh; ++y) {
+    double *ra = rows + (size_t)y * 58, *rm = ra + 29;
+    for (int x = 0; x < mw; ++x) {
+      size_t p = (size_t)y * mw + x;
+      const R *s = model + 8 * p;
+      if (s[3] == 0 || s[7] == 0) continue;
+      R a[6], b;
+      int gamb = 0, ramb = 0;
+      double v[29];
+      int ok = icp_row(lc, frame, s, s + 4, P, W, dist, nthr, 0, a, &b, &gamb, &ramb);
+      if (ok) row_products(a, b, v);
+      if (ok == 1)
+        for (int q = 0; q < 29; ++q) ra[q] += v[q];
+      if (amb && (gamb || ramb)) {
+        if (ok)
+          for (int q = 0; q < 29; ++q) rm[q] += fabs(v[q]);
+        for (int alt = 1; alt < 4; ++alt) {
+          if ((alt & ramb) != alt) continue;
+          R a2[6], b2;
+          if (icp_row(lc, frame, s, s + 4, P, W, dist, nthr, alt, a2, &b2, NULL, NULL) == 1) {
+            row_products(a2, b2, v);
+            for (int q = 0; q < 29; ++q) rm[q] += fabs(v[q]);
+          }
+        }
+      }
+    }
+  }
+  (void)npx;
+  for (int y = 0; y < mh; ++y)
+    for (int q = 0; q < 29; ++q) {
+      acc[q] += rows[(size_t)y * 58 + q];
+      am[q] += rows[(size_t)y * 58 + 29 + q];
+    }
+  free(rows);
+  for (int q = 0; q < 29; ++q) out[q] = acc[q];
+  if (amb)
+    for (int q = 0; q < 29; ++q) amb[q] = am[q];
+}
+
+/* FP64 Cholesky solve of the 6x6 normal equations and the SE(3) update:
+ * ICP::Iterate_ICP (Source/src/ICP.cpp:142-168: symmetrise, singularity test,
+ * llt().solve, rotation part negated) and Cpu_buildNewTransformMatrix
+ * (Source/src/ICP.cu:266-305: dT = [Rz(g) Ry(b) Rx(a) | t], T <- dT T). The
+ * singularity test is a pivot below 1e-12 x the largest diagonal entry or
+ * fewer than 6 inliers, in place of |det| < 1e-6 in FP32. */
+int32_t ora_icp_step(const double *sys, double *P, double *minpiv) {
+  double H[6][6], L[6][6] = {{0}}, g[6], y[6], x[6];
+  int q = 0;
+  for (int i = 0; i < 6; ++i)
+    for (int j = i; j < 6; ++j) { H[i][j] = H[j][i] = sys[q++]; }
+  for (int i = 0; i < 6; ++i) g[i] = sys[21 + i];
+  double dmax = 0.0;
+  for (int i = 0; i < 6; ++i) dmax = fmax(dmax, H[i][i]);
+  double mp = 1e300;
+  int ok = sys[28] >= 6.0 && dmax > 0.0 && isfinite(dmax);
+  for (int j = 0; j < 6 && ok; ++j) {
+    double s = H[j][j];
+    for (int k = 0; k < j; ++k) s -= L[j][k] * L[j][k];
+    mp = fmin(mp, s / dmax);
+    if (!(s > 1e-12 * dmax) || !isfinite(s)) { ok = 0; break; }
+    L[j][j] = sqrt(s);
+    for (int i = j + 1; i < 6; ++i) {
+      double t = H[i][j];
+      for (int k = 0; k < j; ++k) t -= L[i][k] * L[j][k];
+      L[i][j] = t / L[j][j];
+    }
+  }
+  if (minpiv) *minpiv = ok ? mp : fmin(mp, 0.0);
+  if (!ok) return 1;
+  for (int i = 0; i < 6; ++i) {
+    double t = g[i];
+    for (int k = 0; k < i; ++k) t -= L[i][k] * y[k];
+    y[i] = t / L[i][i];
+  }
+  for (int i = 5; i >= 0; --i) {
+    double t = y[i];
+    for (int k = i + 1; k < 6; ++k) t -= L[k][i] * x[k];
+    x[i] = t / L[i][i];
+  }
+  double al = -x[0], be = -x[1], ga = -x[2];
+  double ca = cos(al), sa = sin(al), cb = cos(be), sb = sin(be), cg = cos(ga), sg = sin(ga);
+  double D[16] = {cg * cb, -sg * ca + cg * sb * sa, sg * sa + cg * sb * ca, x[3],
+                  sg * cb, cg * ca + sg * sb * sa,  -cg * sa + sg * sb * ca, x[4],
+                  -sb,     cb * sa,                 cb * ca,                 x[5],
+                  0.0,     0.0,                     0.0,                     1.0};
+  double O[16];
+  memcpy(O, P, sizeof(O));
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) {
+      double a = 0.0;
+      for (int k = 0; k < 4; ++k) a += D[4 * i + k] * O[4 * k + j];
+      P[4 * i + j] = a;
+    }
+  return 0;
+}
+
+static void pyramid_levels(const ora_cam *c, int levels, const R *base, const R **dep,
+                           const R **pts, ora_cam *lc) {
+  const R *q = base;
+  for (int l = 0; l < levels; ++l) {
+    ora_cam_level(c, l, &lc[l]);
+    dep[l] = q;
+    q += (size_t)lc[l].w * lc[l].h;
+    pts[l] = q;
+    q += (size_t)lc[l].w * lc[l].h * 8;
+  }
+}
+
+/* Multi-level ICP, coarse to fine, fixed iteration counts (the reference runs
+ * ICP_ITERATIONS = 15 at one level, Source/include/Constants.h:50). A
+ * singular system restores the starting pose and stops (ICP.cpp:152-158). */
+int32_t ora_icp_track(const ora_cam *c, const ora_params *p, const R *frame, const R *model,
+                      double *P, int32_t *iterations) {
+  const R *fd[4], *fp[4], *md[4], *mp[4];
+  ora_cam lc[4];
+  pyramid_levels(c, p->levels, frame, fd, fp, lc);
+  pyramid_levels(c, p->levels, model, md, mp, lc);
+  double P0[16];
+  memcpy(P0, P, sizeof(P0));
+  int its = 0;
+  for (int l = p->levels - 1; l >= 0; --l) {
+    for (int it = 0; it < p->iters[l]; ++it) {
+      double sys[29];
+      ora_icp_system(&lc[l], fp[l], lc[l].w, lc[l].h, mp[l], P, p->dist_thresh, p->normal_thresh,
+                     sys, NULL);
+      ++its;
+      if (ora_icp_step(sys, P, NULL) != 0) {
+        memcpy(P, P0, sizeof(P0));
+        if (iterations) *iterations = its;
+        return 1;
+      }
+    }
+  }
+  if (iterations) *iterations = its;
+  return 0;
+}
+
+/* ------------------------------------------------------------ CPU tracker */
+
+struct ora_tracker {
+  ora_cam cam;
+  ora_vol vol;
+  ora_params par;
+  double pose[16];
+  uint32_t *words;
+  R *frame, *model;
+  int64_t frames;
+};
+
+ora_tracker *ora_tracker_create(const ora_cam *c, const ora_vol *v, const ora_params *p,
+                                const double *pose0) {
+  ora_tracker *t = (ora_tracker *)calloc(1, sizeof(ora_tracker));
+  if (!t) return NULL;
+  t->cam = *c;
+  t->vol = *v;
+  t->par = *p;
+  memcpy(t->pose, pose0, sizeof(t->pose));
+  size_t nv = (size_t)v->n * v->n * v->n;
+  int64_t pe = ora_pyramid_elems(c, p->levels);
+  t->words = (uint32_t *)calloc(nv, sizeof(uint32_t));
+  t->frame = (R *)calloc((size_t)pe, sizeof(R));
+  t->model = (R *)calloc((size_t)pe, sizeof(R));
+  if (!t->words || !t->frame || !t->model) {
+    ora_tracker_destroy(t);
+    return NULL;
+  }
+  return t;
+}
+
+void ora_tracker_destroy(ora_tracker *t) {
+  if (!t) return;
+  free(t->words);
+  free(t->frame);
+  free(t->model);
+  free(t);
+}
+
+/* RunApp::display (Source/src/MainApp.cpp:786-964) in the order
+ * pre-process -> ICP -> integrate -> raycast. */
+int32_t ora_tracker_process(ora_tracker *t, const uint16_t *depth) {
+  int32_t status = 0;
+  if (t->frames > 0) {
+    ora_preprocess(&t->cam, &t->par, depth, t->frame);
+    status = ora_icp_track(&t->cam, &t->par, t->frame, t->model, t->pose, NULL);
+  }
+  ora_integrate(&t->vol, t->words, &t->cam, depth, t->pose, NULL);
+  const R *md[4], *mp[4];
+  ora_cam lc[4];
+  pyramid_levels(&t->cam, t->par.levels, t->model, md, mp, lc);
+  ora_raycast(&t->vol, t->words, &t->cam, &t->par, t->pose, (R *)mp[0], NULL);
+  for (int l = 1; l < t->par.levels; ++l)
+    ora_model_down(mp[l - 1], lc[l - 1].w, (R *)mp[l], lc[l].w, lc[l].h);
+  t->frames += 1;
+  return status;
+}
+
+void ora_tracker_pose(const ora_tracker *t, double *pose) { memcpy(pose, t->pose, sizeof(t->pose)); }
+
+uint32_t *ora_tracker_volume(ora_tracker *t) { return t->words; }

@@ -1,0 +1,113 @@
+/* of_oracle.h -- CPU restatement of the KinectFusion per-frame path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This is the checker the CUDA path is compared
+ * against; it is never linked into, called by or shipped with the product
+ * (openfusion_b200/). Only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline leg load it.
+ *
+ * The same source builds twice:
+ *   liboracle_f64.so   -- OF_REAL = double: the FP64 oracle (parity checker)
+ *   libcpu_f32_omp.so  -- OF_REAL = float:  a straightforward FP32 OpenMP CPU
+ *                         implementation of the same equations (CPU baseline)
+ *
+ * Pinning: the reference (gilbs10/OpenFusion) ships no tests, golden vectors or
+ * recordings. The stages with a reference counterpart are pinned against the
+ * reference's own kernel sources compiled for the host and run here
+ * (oracle/ref_harness, fixtures in tests/golden/). The stages the reference
+ * does not have (bilateral filter, pyramid, trilinear raycast, FP64 Cholesky)
+ * restate the published methods cited at each function.
+ */
+#ifndef OF_ORACLE_H_
+#define OF_ORACLE_H_
+
+#include <stdint.h>
+
+#ifndef OF_REAL
+#define OF_REAL double
+#endif
+typedef OF_REAL ora_real;
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ora_cam {
+  int32_t w, h;
+  double fx, fy, cx, cy;
+  double dmin, dmax;
+} ora_cam;
+
+typedef struct ora_vol {
+  int32_t n;        /* voxels per edge */
+  int32_t storage;  /* 0 = int16, 1 = fp16 */
+  double size;      /* mm */
+  double trunc;     /* mm */
+  int32_t max_w;
+  int32_t pad;
+} ora_vol;
+
+typedef struct ora_params {
+  double sigma_s, sigma_r;
+  int32_t radius, levels;
+  int32_t iters[4];
+  double dist_thresh, normal_thresh;
+  double min_step_vox, far_step_frac;
+  int32_t refine_iters;
+  int32_t pad;
+} ora_params;
+
+int32_t ora_real_bytes(void);
+void ora_cam_level(const ora_cam *c, int32_t level, ora_cam *out);
+
+/* pre-processing; pts is [h*w][8]: vertex xyz valid, normal xyz valid */
+void ora_bilateral(const ora_cam *c, const uint16_t *depth, double sigma_s, double sigma_r,
+                   int32_t radius, ora_real *out);
+void ora_pyr_down(const ora_real *src, int32_t sw, int32_t sh, ora_real *dst, int32_t dw,
+                  int32_t dh, double guard);
+void ora_vertex_normal(const ora_cam *c, const ora_real *depth, ora_real *pts);
+/* whole pyramid: for level l, depth_l and pts_l are laid out one after the
+ * other: [depth_0 | pts_0 | depth_1 | pts_1 ...] (sizes w_l*h_l and 8*w_l*h_l) */
+void ora_preprocess(const ora_cam *c, const ora_params *p, const uint16_t *depth, ora_real *out);
+int64_t ora_pyramid_elems(const ora_cam *c, int32_t levels);
+
+/* integration into linear-layout voxel words (index (i*n + j)*n + k); returns
+ * the number of voxels updated. ambig (may be NULL, n^3 bytes) flags voxels
+ * whose decisions lie within FP32 rounding of a boundary. */
+int64_t ora_integrate(const ora_vol *v, uint32_t *words, const ora_cam *c, const uint16_t *depth,
+                      const double *pose, uint8_t *ambig);
+
+/* raycast; pts is [h*w][8] world vertex/normal; ambig (may be NULL) flags
+ * pixels whose sign or range decisions are within rounding of a boundary. */
+void ora_raycast(const ora_vol *v, const uint32_t *words, const ora_cam *c, const ora_params *p,
+                 const double *pose, ora_real *pts, uint8_t *ambig);
+/* model level l+1 from level l by subsampling (2x, 2y) */
+void ora_model_down(const ora_real *src, int32_t sw, ora_real *dst, int32_t dw, int32_t dh);
+
+/* one correspondence pass at one level: out[29] = 21 upper A^T A, 6 A^T b,
+ * sum b^2, inliers; amb[29] (may be NULL) = sum of |contribution| of pixels
+ * whose association or gates lie within rounding of a boundary. */
+void ora_icp_system(const ora_cam *lc, const ora_real *frame_pts, int32_t mw, int32_t mh,
+                    const ora_real *model_pts, const double *pose, double dist_thresh,
+                    double normal_thresh, double *out, double *amb);
+/* solve + compose; returns 0 ok, 1 singular (pose untouched) */
+int32_t ora_icp_step(const double *sys, double *pose, double *min_pivot);
+/* multi-level ICP from pyramids laid out as ora_preprocess writes them (the
+ * model uses the same layout; its depth planes are ignored). Returns status. */
+int32_t ora_icp_track(const ora_cam *c, const ora_params *p, const ora_real *frame,
+                      const ora_real *model, double *pose, int32_t *iterations);
+
+/* CPU tracker: the whole frame loop (used as the CPU baseline) */
+typedef struct ora_tracker ora_tracker;
+ora_tracker *ora_tracker_create(const ora_cam *c, const ora_vol *v, const ora_params *p,
+                                const double *pose0);
+void ora_tracker_destroy(ora_tracker *t);
+int32_t ora_tracker_process(ora_tracker *t, const uint16_t *depth);
+void ora_tracker_pose(const ora_tracker *t, double *pose);
+uint32_t *ora_tracker_volume(ora_tracker *t);
+int32_t ora_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,256 @@
+"""Parity of the CUDA path against the FP64 oracle on the same seeded inputs.
+
+Every comparison is stepwise: the oracle consumes the GPU's own input state
+(volume, frame and model maps, pose) for the stage under test, so only that
+stage's arithmetic is compared. Decisions that sit within FP32 rounding of a
+boundary (pixel rounding at .5, a depth at the range limit, an SDF at -trunc,
+a tsdf sample at 0) are flagged by the oracle and excluded; their number is
+bounded. Tolerances (from the path's precision targets):
+  TSDF      within 1 int16 quantisation step (trunc / 32767)
+  vertices  within 1e-4 m = 0.1 mm
+  pose      within 1e-5 rad and 1e-5 m = 0.01 mm
+"""
+import numpy as np
+import pytest
+
+from conftest import pose_error
+
+pytestmark = pytest.mark.gpu
+
+
+def small(of, name="c1", **kw):
+    import dataclasses
+    return dataclasses.replace(of.CONFIGS[name], **kw)
+
+
+def dev_pose(P, device):
+    import torch
+    return torch.tensor(np.asarray(P, np.float64).reshape(16), dtype=torch.float64, device=device)
+
+
+def build_state(of, cfg, frames, device):
+    """Volume after fusing `frames` frames at ground-truth poses."""
+    import torch
+    seq = of.make_sequence(cfg, frames=frames + 1)
+    vol = of.new_volume(cfg, device)
+    lam = of.lambda_table(cfg, device)
+    for k in range(frames):
+        d = torch.from_numpy(seq.depth[k].astype(np.int16)).to(device)
+        of.integrate(cfg, vol, d, dev_pose(seq.poses[k], device), lam)
+    torch.cuda.synchronize()
+    return seq, vol, lam
+
+
+def gpu_pyramid_to_oracle(of, ora, cfg, pyr, with_depth=True):
+    pts, deps = [], []
+    for l in range(cfg.levels):
+        v, n = of.unpack_points(cfg, pyr, l)
+        pts.append(np.concatenate([v.cpu().numpy(), n.cpu().numpy()], axis=-1))
+        deps.append(of.unpack_depth(cfg, pyr, l).cpu().numpy() if with_depth else None)
+    return ora.pack_pyramid(cfg, pts, deps if with_depth else None), pts
+
+
+# ---------------------------------------------------------------- preprocess
+
+@pytest.mark.parametrize("name,size", [("c1", None), ("c2", None), ("c1", (161, 121))])
+def test_preprocess_matches_oracle(of, ora, cuda, name, size):
+    import torch
+    cfg = small(of, name) if size is None else small(
+        of, name, width=size[0], height=size[1], cx=(size[0] - 1) / 2, cy=(size[1] - 1) / 2)
+    seq = of.make_sequence(cfg, frames=1)
+    d = torch.from_numpy(seq.depth[0].astype(np.int16)).to(cuda)
+    pyr = of.preprocess(cfg, d)
+    torch.cuda.synchronize()
+    levels, _ = ora.preprocess(cfg, seq.depth[0])
+    for l, (odep, opts) in enumerate(levels):
+        gdep = of.unpack_depth(cfg, pyr, l).cpu().numpy().astype(np.float64)
+        gv, gn = (t.cpu().numpy().astype(np.float64) for t in of.unpack_points(cfg, pyr, l))
+        valid_o = odep > 0
+        valid_g = gdep > 0
+        # validity decided by integer depths (level 0) and 3 sigma_r guards
+        assert (valid_o != valid_g).mean() < 1e-4, f"level {l} validity mismatch"
+        both = valid_o & valid_g
+        rel = np.abs(gdep[both] - odep[both]) / odep[both]
+        assert rel.max() < 5e-6, f"level {l} filtered depth rel err {rel.max()}"
+        vboth = (gv[..., 3] > 0) & (opts[..., 3] > 0)
+        verr = np.linalg.norm(gv[..., :3][vboth] - opts[..., :3][vboth], axis=-1)
+        assert verr.max() < 0.1, f"level {l} vertex err {verr.max()} mm"
+        nboth = (gn[..., 3] > 0) & (opts[..., 7] > 0)
+        assert ((gn[..., 3] > 0) != (opts[..., 7] > 0)).mean() < 1e-3
+        nerr = np.linalg.norm(gn[..., :3][nboth] - opts[..., 4:7][nboth], axis=-1)
+        assert np.median(nerr) < 1e-4 and nerr.max() < 2e-2, f"level {l} normal err {nerr.max()}"
+
+
+# ---------------------------------------------------------------- integrate
+
+@pytest.mark.parametrize("name,res,storage", [("c1", 128, "i16"), ("c2", 256, "i16"),
+                                              ("c2", 512, "i16"), ("c1", 128, "f16")])
+def test_integrate_matches_oracle(of, ora, cuda, name, res, storage):
+    import torch
+    cfg = small(of, name, resolution=res, storage=storage)
+    seq, vol, lam = build_state(of, cfg, 3, cuda)
+    k = 3
+    q0, w0 = of.volume_to_linear(cfg, vol.cpu().numpy())
+    words = ((q0.astype(np.uint32)) | (w0.astype(np.uint32) << 16)).reshape(-1).copy()
+    d = seq.depth[k]
+    pose = seq.poses[k]
+    n_ora, amb = ora.integrate(cfg, words, d, pose, ambig=True)
+    dt = torch.from_numpy(d.astype(np.int16)).to(cuda)
+    pt = dev_pose(pose, cuda)
+    n_gpu = of.integrate_census(cfg, vol, dt, pt, lam)
+    of.integrate(cfg, vol, dt, pt, lam)
+    torch.cuda.synchronize()
+    q1, w1 = of.volume_to_linear(cfg, vol.cpu().numpy())
+    qo = (words & 0xFFFF).astype(np.uint16).reshape(q1.shape)
+    wo = (words >> 16).astype(np.uint16).reshape(q1.shape)
+    ok = amb.reshape(q1.shape) == 0
+    n_amb = int((~ok).sum())
+    assert abs(n_gpu - n_ora) <= n_amb, (n_gpu, n_ora, n_amb)
+    assert n_amb < 1e-3 * ok.size
+    assert np.array_equal(w1[ok], wo[ok]), "weights differ"
+    if storage == "i16":
+        dq = np.abs(q1[ok].view(np.int16).astype(np.int32) - qo[ok].view(np.int16).astype(np.int32))
+        assert dq.max() <= 1, f"tsdf differs by {dq.max()} int16 steps"
+    else:
+        g = q1[ok].view(np.float16).astype(np.float64)
+        o = qo[ok].view(np.float16).astype(np.float64)
+        # fp16 of a value in [-1, 1]: one ulp is at most 2^-11
+        assert np.abs(g - o).max() <= 2.0 ** -11 * 1.001
+
+
+# ---------------------------------------------------------------- raycast
+
+@pytest.mark.parametrize("name,res", [("c1", 128), ("c2", 512)])
+def test_raycast_matches_oracle(of, ora, cuda, name, res):
+    import torch
+    cfg = small(of, name, resolution=res)
+    seq, vol, lam = build_state(of, cfg, 4, cuda)
+    pose = seq.poses[3]
+    model = of.raycast(cfg, vol, dev_pose(pose, cuda))
+    torch.cuda.synchronize()
+    q, w = of.volume_to_linear(cfg, vol.cpu().numpy())
+    words = (q.astype(np.uint32) | (w.astype(np.uint32) << 16)).reshape(-1).copy()
+    opts, amb = ora.raycast(cfg, words, pose, ambig=True)
+    gv, gn = (t.cpu().numpy().astype(np.float64) for t in of.unpack_points(cfg, model, 0))
+    ok = amb == 0
+    hit_g, hit_o = gv[..., 3] > 0, opts[..., 3] > 0
+    assert hit_o.mean() > 0.5, "scene should be mostly visible"
+    assert (hit_g != hit_o)[ok].mean() < 1e-3
+    both = hit_g & hit_o & ok
+    verr = np.linalg.norm(gv[..., :3][both] - opts[..., :3][both], axis=-1)
+    assert np.quantile(verr, 0.999) < 0.1, f"vertex err q99.9 {np.quantile(verr, 0.999)} mm"
+    assert np.median(verr) < 0.01
+    nb = both & (gn[..., 3] > 0) & (opts[..., 7] > 0)
+    nerr = np.linalg.norm(gn[..., :3][nb] - opts[..., 4:7][nb], axis=-1)
+    assert np.median(nerr) < 1e-3
+
+
+# ---------------------------------------------------------------- ICP
+
+def icp_inputs(of, ora, cfg, cuda):
+    import torch
+    seq, vol, lam = build_state(of, cfg, 4, cuda)
+    model = of.raycast(cfg, vol, dev_pose(seq.poses[3], cuda))
+    d = torch.from_numpy(seq.depth[4].astype(np.int16)).to(cuda)
+    frame = of.preprocess(cfg, d)
+    torch.cuda.synchronize()
+    return seq, vol, lam, model, frame
+
+
+@pytest.mark.parametrize("name", ["c1", "c2"])
+def test_icp_system_matches_oracle(of, ora, cuda, name):
+    cfg = small(of, name)
+    seq, vol, lam, model, frame = icp_inputs(of, ora, cfg, cuda)
+    fbuf, fpts = gpu_pyramid_to_oracle(of, ora, cfg, frame)
+    mbuf, mpts = gpu_pyramid_to_oracle(of, ora, cfg, model, with_depth=False)
+    ws = of.icp_workspace(cfg, cuda)
+    pose = seq.poses[3]  # previous pose: the usual ICP starting point
+    for level in range(cfg.levels):
+        g = of.icp_system(cfg, level, frame, model, dev_pose(pose, cuda), ws).cpu().numpy()
+        o, amb = ora.icp_system(cfg, level, fpts[level], mpts[level], pose)
+        assert o[28] > 100, "too few correspondences"
+        # Cauchy-Schwarz scale of every sum: sqrt(H_ii H_jj), sqrt(H_ii sum b^2)
+        diag = np.array([o[k] for k in (0, 6, 11, 15, 18, 20)])
+        scale = np.zeros(29)
+        k = 0
+        for i in range(6):
+            for j in range(i, 6):
+                scale[k] = np.sqrt(diag[i] * diag[j]); k += 1
+        scale[21:27] = np.sqrt(diag * o[27])
+        scale[27] = o[27]
+        # FP32 rows and compensated FP32 sums vs FP64 sums of the same rows,
+        # plus the whole contribution of pixels at a rounding boundary
+        bound = 2e-5 * scale + amb
+        err = np.abs(g - o)
+        assert np.all(err <= bound + 1e-6), f"level {level}: {err / (scale + 1e-30)}"
+
+
+@pytest.mark.parametrize("name", ["c1", "c2"])
+def test_icp_track_matches_oracle(of, ora, cuda, name):
+    import torch
+    cfg = small(of, name)
+    seq, vol, lam, model, frame = icp_inputs(of, ora, cfg, cuda)
+    fbuf, _ = gpu_pyramid_to_oracle(of, ora, cfg, frame)
+    mbuf, _ = gpu_pyramid_to_oracle(of, ora, cfg, model, with_depth=False)
+    ws = of.icp_workspace(cfg, cuda)
+    pose0 = seq.poses[3]
+    pt = dev_pose(pose0, cuda)
+    stats = torch.zeros(32, dtype=torch.uint8, device=cuda)
+    of.icp_track(cfg, frame, model, pt, ws, stats)
+    gpose = pt.cpu().numpy().reshape(4, 4)
+    st, opose, its = ora.icp_track(cfg, fbuf, mbuf, pose0)
+    assert st == 0
+    status = int(stats[:4].view(torch.int32).item())
+    assert status == 0
+    rot, trans = pose_error(gpose, opose)
+    assert rot < 1e-5 and trans < 1e-2, (rot, trans)
+    # and the tracked pose is close to the ground truth of the frame
+    rot_gt, trans_gt = pose_error(gpose, seq.poses[4])
+    assert rot_gt < np.radians(0.5) and trans_gt < 10.0
+
+
+def test_icp_singular_restores_pose(of, cuda):
+    import torch
+    cfg = small(of, "c1")
+    seq, vol, lam = build_state(of, cfg, 2, cuda)
+    model = of.raycast(cfg, vol, dev_pose(seq.poses[1], cuda))
+    empty = torch.zeros((cfg.height, cfg.width), dtype=torch.int16, device=cuda)
+    frame = of.preprocess(cfg, empty)
+    ws = of.icp_workspace(cfg, cuda)
+    pt = dev_pose(seq.poses[1], cuda)
+    stats = torch.zeros(32, dtype=torch.uint8, device=cuda)
+    of.icp_track(cfg, frame, model, pt, ws, stats)
+    torch.cuda.synchronize()
+    assert int(stats[:4].view(torch.int32).item()) == 1
+    assert np.array_equal(pt.cpu().numpy().reshape(4, 4), seq.poses[1])
+
+
+# ---------------------------------------------------------------- tracker
+
+def test_tracker_graph_equals_eager(of, cuda):
+    import torch
+    cfg = small(of, "c1")
+    seq = of.make_sequence(cfg, frames=6)
+    poses = []
+    for graph in (True, False):
+        tr = of.Tracker(cfg, seq.poses[0], use_graph=graph)
+        for k in range(6):
+            tr.process(torch.from_numpy(seq.depth[k].astype(np.int16)).to(cuda))
+        poses.append(tr.pose_history(6))
+        tr.close()
+    assert np.array_equal(poses[0], poses[1])
+
+
+def test_tracker_follows_ground_truth(of, cuda):
+    import torch
+    cfg = small(of, "c1")
+    seq = of.make_sequence(cfg, frames=30)
+    tr = of.Tracker(cfg, seq.poses[0])
+    pinned = torch.from_numpy(seq.depth.astype(np.int16)).pin_memory()
+    for k in range(30):
+        tr.process(pinned[k])
+    hist = tr.pose_history(30)
+    tr.close()
+    errs = [pose_error(hist[k], seq.poses[k]) for k in range(30)]
+    assert max(e[1] for e in errs) < 5.0, errs
+    assert max(e[0] for e in errs) < np.radians(0.5)
