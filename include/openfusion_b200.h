@@ -63,7 +63,7 @@ typedef struct of_camera {
 /* Replaces the compile-time worldVolume / VOLUME_SIZE / TRUNCATION /
  * MAX_WEIGHT constants (Source/include/Constants.h:23-55). */
 typedef struct of_volume_desc {
-  int32_t resolution; /* N voxels per edge; multiple of 8, 8..2048 */
+  int32_t resolution; /* N voxels per edge; multiple of 8, 8..1024 */
   int32_t storage;    /* OF_TSDF_I16 or OF_TSDF_F16 */
   float size_mm;      /* cube edge */
   float trunc_mm;     /* truncation distance */
@@ -99,7 +99,8 @@ typedef struct of_icp_params {
 
 /* Per-frame ICP result, written by the device. */
 typedef struct of_icp_stats {
-  int32_t status;        /* 0 = tracked; 1 = singular system, pose restored (ICP.cpp:152-158) */
+  int32_t status;        /* 0 = tracked; 1 = singular system, pose restored (ICP.cpp:152-158);
+                            2 = a device-side wait gave up, pose restored */
   int32_t inliers;       /* correspondences of the last iteration run */
   int32_t iterations;    /* iterations run */
   int32_t reserved;

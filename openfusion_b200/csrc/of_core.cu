@@ -65,7 +65,7 @@ static bool camera_ok(const of_camera_t *c) {
 bool of_camera_valid(const of_camera_t *c) { return camera_ok(c); }
 
 bool of_volume_valid(const of_volume_desc_t *d) {
-  return d && d->resolution >= 8 && d->resolution <= 2048 && (d->resolution % 8) == 0 &&
+  return d && d->resolution >= 8 && d->resolution <= 1024 && (d->resolution % 8) == 0 &&
          (d->storage == OF_TSDF_I16 || d->storage == OF_TSDF_F16) && d->size_mm > 0.f &&
          d->trunc_mm > 0.f && d->max_weight >= 1 && d->max_weight <= 65535;
 }

@@ -20,6 +20,8 @@
 //   starting pose and stops the remaining iterations (ICP.cpp:152-158).
 #include "of_common.cuh"
 
+#include <string.h>
+
 using namespace of;
 
 bool of_camera_valid(const of_camera_t *c);
@@ -31,16 +33,26 @@ constexpr int kIcpMaxBlocks = 2 * kSmCount;
 constexpr int kVals = 29;  // 21 + 6 + residual^2 + inliers
 constexpr float kEps = 1e-6f;  // _EPSILON_ (Constants.h:14)
 
+constexpr int kFusedThreads = 512;
+constexpr int kFusedMaxBlocks = 4 * kSmCount;
+// A grid barrier gives up after about 0.25 s (this many 64 ns sleeps) and
+// reports status 2 instead of waiting forever.
+constexpr unsigned kSpinLimit = 1u << 22;
+
 struct IcpWorkspace {
   unsigned int ticket;
   int stop;
   int iterations;
-  int pad;
+  int error;
+  unsigned int bar_count;
+  unsigned int bar_gen;
+  int pad0[2];
   double pose_init[16];
   double prior[16];
   int has_prior;
   int pad2[3];
   float partials[kIcpMaxBlocks][32];
+  float fused_partials[2][kFusedMaxBlocks][32];
 };
 
 enum IcpMode { kModeUpdate = 0, kModeSystem = 1 };
@@ -250,6 +262,201 @@ __global__ void __launch_bounds__(kIcpThreads)
   }
 }
 
+struct IcpLevel {
+  const float4 *model;
+  const float4 *frame;
+  Cam cam;      // level intrinsics (of the frame's image)
+  int mw, mh;   // model map size at this level
+  int iters;
+};
+
+struct IcpPlan {
+  IcpLevel lv[kMaxLevels];
+  int levels;
+  float dist_thresh, normal_thresh;
+};
+
+// Grid-wide barrier for a co-resident grid: arrival counter + generation.
+// The wait is bounded; on timeout the workspace error flag is set.
+__device__ __forceinline__ void grid_barrier(IcpWorkspace *ws, unsigned nblocks) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned *gen = &ws->bar_gen;
+    unsigned g = *gen;
+    __threadfence();
+    if (atomicAdd(&ws->bar_count, 1u) == nblocks - 1) {
+      ws->bar_count = 0;
+      __threadfence();
+      atomicAdd(&ws->bar_gen, 1u);
+    } else {
+      unsigned spins = 0;
+      while (*gen == g) {
+        if (++spins > kSpinLimit) {
+          atomicExch(&ws->error, 1);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// The whole multi-level ICP of one frame in one cooperative launch. Per
+// iteration: every block accumulates its pixels' rows (tree sums), writes 29
+// partials, meets the others at one grid barrier, then reduces all blocks'
+// partials in the same fixed order and solves the 6x6 system itself, so every
+// block holds the same new pose without a second barrier. Partials alternate
+// between two buffers: a block can only overwrite buffer i%2 after the
+// barrier of iteration i+1, which every block reaches only after reading it.
+__global__ void __launch_bounds__(kFusedThreads, 1)
+    k_icp_fused(IcpPlan plan, double *pose, IcpWorkspace *ws, of_icp_stats_t *stats) {
+  __shared__ double s_pose[16];
+  __shared__ Rigid s_c2w, s_w2c;
+  __shared__ float s_red[kFusedThreads / 32][32];
+  __shared__ float s_tot[32];
+  __shared__ int s_stop, s_inl, s_its;
+  __shared__ double s_res, s_piv;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kWarps = kFusedThreads / 32;
+  if (threadIdx.x < 16) s_pose[threadIdx.x] = pose[threadIdx.x];
+  if (threadIdx.x == 0) { s_stop = 0; s_its = 0; s_inl = 0; s_res = 0.0; s_piv = 0.0; }
+  __syncthreads();
+  int iter_global = 0;
+  for (int l = plan.levels - 1; l >= 0 && !s_stop; --l) {
+    const IcpLevel L = plan.lv[l];
+    for (int it = 0; it < L.iters; ++it) {
+      if (threadIdx.x == 0) pose_to_rigid(s_pose, &s_c2w, &s_w2c);
+      __syncthreads();
+      float acc[kVals];
+#pragma unroll
+      for (int v = 0; v < kVals; ++v) acc[v] = 0.f;
+      const int npx = L.mw * L.mh;
+      for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npx; p += gridDim.x * blockDim.x) {
+        float4 s = __ldg(L.model + 2 * p);
+        float4 ns = __ldg(L.model + 2 * p + 1);
+        if (s.w == 0.f || ns.w == 0.f) continue;
+        float3 sc = apply(s_w2c, make_float3(s.x, s.y, s.z));
+        if (sc.z >= -kEps) continue;
+        float rz = __frcp_rn(sc.z);
+        int pu = __float2int_rd(fmaf(L.cam.fx * sc.x, rz, L.cam.cx) + 0.5f);
+        int pv = __float2int_rd(fmaf(L.cam.fy * sc.y, rz, L.cam.cy) + 0.5f);
+        if ((unsigned)pu >= (unsigned)L.cam.w || (unsigned)pv >= (unsigned)L.cam.h) continue;
+        int q = pv * L.cam.w + pu;
+        float4 dc = __ldg(L.frame + 2 * q);
+        float4 nc = __ldg(L.frame + 2 * q + 1);
+        if (dc.w == 0.f || nc.w == 0.f) continue;
+        float3 d = apply(s_c2w, make_float3(dc.x, dc.y, dc.z));
+        float3 nd = rotate(s_c2w, make_float3(nc.x, nc.y, nc.z));
+        float ex = d.x - s.x, ey = d.y - s.y, ez = d.z - s.z;
+        if (!(fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < plan.dist_thresh * plan.dist_thresh)) continue;
+        float dn = nd.x * ns.x + nd.y * ns.y + nd.z * ns.z;
+        if (!(dn > plan.normal_thresh && dn < 1.f + kEps)) continue;
+        float a[6];
+        a[0] = ns.y * d.z - ns.z * d.y;
+        a[1] = ns.z * d.x - ns.x * d.z;
+        a[2] = ns.x * d.y - ns.y * d.x;
+        a[3] = ns.x; a[4] = ns.y; a[5] = ns.z;
+        float b = -(ns.x * ex + ns.y * ey + ns.z * ez);
+        int k = 0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+#pragma unroll
+          for (int j = i; j < 6; ++j) { acc[k] = fmaf(a[i], a[j], acc[k]); ++k; }
+#pragma unroll
+        for (int i = 0; i < 6; ++i) acc[21 + i] = fmaf(a[i], b, acc[21 + i]);
+        acc[27] = fmaf(b, b, acc[27]);
+        acc[28] += 1.f;
+      }
+      // pairwise: warp shuffle tree, then a tree over the block's warps
+#pragma unroll
+      for (int v = 0; v < kVals; ++v) {
+        float x = acc[v];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) s_red[warp][v] = x;
+      }
+      __syncthreads();
+      const int buf = iter_global & 1;
+      if (warp == 0) {
+        float x = 0.f;
+        if (lane < kVals) {
+          float y[kWarps];
+#pragma unroll
+          for (int w = 0; w < kWarps; ++w) y[w] = s_red[w][lane];
+#pragma unroll
+          for (int span = 1; span < kWarps; span *= 2)
+#pragma unroll
+            for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
+          x = y[0];
+        }
+        ws->fused_partials[buf][blockIdx.x][lane] = x;
+      }
+      grid_barrier(ws, gridDim.x);
+      // every block: Kahan over its strided share of the blocks' partials,
+      // then a tree over the groups, in a fixed order
+      {
+        const int v = lane, grp = warp;
+        float sum = 0.f, c = 0.f;
+        if (v < kVals)
+          for (int r = grp; r < (int)gridDim.x; r += kWarps) {
+            float y = __ldcg(&ws->fused_partials[buf][r][v]) - c;
+            float t = sum + y;
+            c = (t - sum) - y;
+            sum = t;
+          }
+        s_red[grp][v] = sum - c;
+      }
+      __syncthreads();
+      if (threadIdx.x < 32) {
+        float y[kWarps];
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) y[w] = s_red[w][threadIdx.x];
+#pragma unroll
+        for (int span = 1; span < kWarps; span *= 2)
+#pragma unroll
+          for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
+        s_tot[threadIdx.x] = y[0];
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double up[21], g[6], xs[6], minpiv = 0.0;
+        for (int v = 0; v < 21; ++v) up[v] = (double)s_tot[v];
+        for (int v = 0; v < 6; ++v) g[v] = (double)s_tot[21 + v];
+        int inliers = (int)s_tot[28];
+        bool ok = inliers >= 6 && chol_solve6(up, g, xs, &minpiv);
+        s_its += 1;
+        s_inl = inliers;
+        s_res = (double)s_tot[27];
+        s_piv = minpiv;
+        if (ok) {
+          double xo[6] = {-xs[0], -xs[1], -xs[2], xs[3], xs[4], xs[5]};
+          compose_increment(xo, s_pose);
+        } else {
+          for (int i = 0; i < 16; ++i) s_pose[i] = ws->pose_init[i];
+          s_stop = 1;
+        }
+      }
+      __syncthreads();
+      ++iter_global;
+      if (s_stop) break;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    int err = *((volatile int *)&ws->error);
+    for (int i = 0; i < 16; ++i) pose[i] = err ? ws->pose_init[i] : s_pose[i];
+    ws->iterations = s_its;
+    if (stats) {
+      stats->status = err ? 2 : (s_stop ? 1 : 0);
+      stats->inliers = s_inl;
+      stats->iterations = s_its;
+      stats->residual_sq = s_res;
+      stats->min_pivot = s_piv;
+    }
+  }
+}
+
 // Start of a frame's tracking: remember the starting pose, apply the
 // optional warm-start increment, clear the flags.
 __global__ void k_icp_begin(double *pose, IcpWorkspace *ws, of_icp_stats_t *stats) {
@@ -269,6 +476,8 @@ __global__ void k_icp_begin(double *pose, IcpWorkspace *ws, of_icp_stats_t *stat
   ws->ticket = 0;
   ws->stop = 0;
   ws->iterations = 0;
+  ws->error = 0;
+  ws->bar_count = 0;
   if (stats) {
     stats->status = 0;
     stats->inliers = 0;
@@ -313,7 +522,22 @@ static bool icp_params_ok(const of_icp_params_t *p) {
   return p->dist_thresh_mm > 0.f;
 }
 
-// Launches the iterations of every level, coarse to fine.
+// Grid of the fused kernel: every block co-resident (cooperative launch).
+static int fused_grid() {
+  static int grid = 0;
+  if (grid == 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_icp_fused, kFusedThreads, 0);
+    int g = sms * (per_sm < 1 ? 1 : per_sm);
+    grid = g > kFusedMaxBlocks ? kFusedMaxBlocks : g;
+  }
+  return grid;
+}
+
+// Launches the whole coarse-to-fine ICP of one frame: a begin kernel and one
+// cooperative launch of the fused kernel.
 of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, const void *d_frame,
                           const void *d_model, double *pose, void *d_ws, of_icp_stats_t *stats,
                           cudaStream_t s) {
@@ -321,19 +545,27 @@ of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, con
   of_status_t st = of_pyramid_layout(cam, ip->levels, &lay);
   if (st != OF_OK) return st;
   IcpWorkspace *ws = (IcpWorkspace *)d_ws;
-  k_icp_begin<<<1, 32, 0, s>>>(pose, ws, stats);
-  for (int l = ip->levels - 1; l >= 0; --l) {
+  IcpPlan plan;
+  memset(&plan, 0, sizeof(plan));
+  plan.levels = ip->levels;
+  plan.dist_thresh = ip->dist_thresh_mm;
+  plan.normal_thresh = ip->normal_thresh;
+  for (int l = 0; l < ip->levels; ++l) {
     of_camera_t cl = camera_level(*cam, l);
-    Cam c = make_cam(cl);
-    const float4 *fr = (const float4 *)((const char *)d_frame + lay.points_offset[l]);
-    const float4 *md = (const float4 *)((const char *)d_model + lay.points_offset[l]);
-    int g = icp_blocks(cl.width * cl.height);
-    for (int it = 0; it < ip->iters[l]; ++it)
-      k_icp_iter<kModeUpdate><<<g, kIcpThreads, 0, s>>>(md, cl.width, cl.height, fr, c,
-                                                        ip->dist_thresh_mm, ip->normal_thresh,
-                                                        pose, ws, stats, nullptr);
+    plan.lv[l].cam = make_cam(cl);
+    plan.lv[l].frame = (const float4 *)((const char *)d_frame + lay.points_offset[l]);
+    plan.lv[l].model = (const float4 *)((const char *)d_model + lay.points_offset[l]);
+    plan.lv[l].mw = cl.width;
+    plan.lv[l].mh = cl.height;
+    plan.lv[l].iters = ip->iters[l];
   }
-  return of_launch_status();
+  k_icp_begin<<<1, 32, 0, s>>>(pose, ws, stats);
+  st = of_launch_status();
+  if (st != OF_OK) return st;
+  void *args[] = {&plan, &pose, &ws, &stats};
+  OF_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)k_icp_fused, dim3(fused_grid()),
+                                          dim3(kFusedThreads), args, 0, s));
+  return OF_OK;
 }
 
 extern "C" of_status_t of_icp_track(const of_camera_t *cam, const of_icp_params_t *ip,

@@ -32,6 +32,8 @@ struct IntegrateSetup {
   float o[3];      // camera-space centre of voxel (0,0,0)
   float vs_hi, vs_lo;
   float oc_hi[3], oc_lo[3];  // (origin + vs/2 - c) per axis, float pair
+  double mb[9];    // world-to-camera rotation scaled by 8 voxels (one brick), FP64
+  double ob[3];    // camera-space centre of voxel (0,0,0), FP64
 };
 
 __device__ void make_setup(const double *P, const of_volume_desc_t &d, IntegrateSetup &S) {
@@ -43,9 +45,11 @@ __device__ void make_setup(const double *P, const of_volume_desc_t &d, Integrate
     for (int b = 0; b < 3; ++b) {
       double rba = P[4 * b + a];  // (R^T)[a][b]
       S.m[3 * a + b] = (float)(rba * vs);
+      S.mb[3 * a + b] = rba * vs * 8.0;
       acc += rba * (org - c[b]);
     }
     S.o[a] = (float)acc;
+    S.ob[a] = acc;
     double oc = org - c[a];
     S.oc_hi[a] = (float)oc;
     S.oc_lo[a] = (float)(oc - (double)S.oc_hi[a]);
@@ -100,25 +104,40 @@ __global__ void __launch_bounds__(256) k_integrate(uint32_t *__restrict__ vol, o
   }
   __syncthreads();
   const int nb = desc.resolution >> 3;
-  const size_t nbricks = (size_t)nb * nb * nb;
+  const int nbricks = nb * nb * nb;
   const int half = threadIdx.x >> 7;
   const int t = threadIdx.x & 127;
   const int lane = threadIdx.x & 31;
-  const size_t b = (size_t)blockIdx.x * 2 + half;
+  const int lx = t >> 4, ly = (t >> 1) & 7, lz0 = (t & 1) * 4;
+  const float T = desc.trunc_mm, inv_T = 1.0f / desc.trunc_mm;
+  const float dspan = cam.dmax - cam.dmin;
+  const unsigned uspan = (unsigned)(cam.w - 4), vspan = (unsigned)(cam.h - 4);
+  // brick b = 2 * pair + half walks the grid with a fixed stride; its (x, y, z)
+  // brick coordinates advance by the stride's digits with carries.
+  int b = 2 * blockIdx.x + half;
+  const int stride = 2 * gridDim.x;
+  const int sz = stride % nb, sy = (stride / nb) % nb, sx = stride / (nb * nb);
+  int bz = b % nb, by = (b / nb) % nb, bx = b / (nb * nb);
   unsigned int my_count = 0;
-  if (b < nbricks) {
-    const int bz = (int)(b % nb);
-    const int by = (int)((b / nb) % nb);
-    const int bx = (int)(b / ((size_t)nb * nb));
+  for (; b < nbricks; b += stride) {
+    // camera-space centre of the brick's voxel (0,0,0), FP64 then rounded:
+    // per-voxel offsets from it stay below 8 voxels, so the FP32 position
+    // error is about one rounding of the brick base.
+    const double fbx = (double)bx, fby = (double)by, fbz = (double)bz;
+    const float BX = (float)fma(S.mb[0], fbx, fma(S.mb[1], fby, fma(S.mb[2], fbz, S.ob[0])));
+    const float BY = (float)fma(S.mb[3], fbx, fma(S.mb[4], fby, fma(S.mb[5], fbz, S.ob[1])));
+    const float BZ = (float)fma(S.mb[6], fbx, fma(S.mb[7], fby, fma(S.mb[8], fbz, S.ob[2])));
+    const int cbx = bx, cby = by, cbz = bz;
+    bz += sz; if (bz >= nb) { bz -= nb; ++by; }
+    by += sy; if (by >= nb) { by -= nb; ++bx; }
+    bx += sx;
     // ---- brick cull: lanes 0..7 take one corner voxel centre each
     bool culled = false;
     {
-      int ci = bx * 8 + ((lane & 4) ? 7 : 0);
-      int cj = by * 8 + ((lane & 2) ? 7 : 0);
-      int ck = bz * 8 + ((lane & 1) ? 7 : 0);
-      float X = fmaf(S.m[0], (float)ci, fmaf(S.m[1], (float)cj, fmaf(S.m[2], (float)ck, S.o[0])));
-      float Y = fmaf(S.m[3], (float)ci, fmaf(S.m[4], (float)cj, fmaf(S.m[5], (float)ck, S.o[1])));
-      float Z = fmaf(S.m[6], (float)ci, fmaf(S.m[7], (float)cj, fmaf(S.m[8], (float)ck, S.o[2])));
+      float ci = (lane & 4) ? 7.f : 0.f, cj = (lane & 2) ? 7.f : 0.f, ck = (lane & 1) ? 7.f : 0.f;
+      float X = fmaf(S.m[0], ci, fmaf(S.m[1], cj, fmaf(S.m[2], ck, BX)));
+      float Y = fmaf(S.m[3], ci, fmaf(S.m[4], cj, fmaf(S.m[5], ck, BY)));
+      float Z = fmaf(S.m[6], ci, fmaf(S.m[7], cj, fmaf(S.m[8], ck, BZ)));
 #pragma unroll
       for (int p = 0; p < 6; ++p) {
         float e = planes[p].a * X + planes[p].b * Y + planes[p].c * Z + planes[p].d;
@@ -126,69 +145,70 @@ __global__ void __launch_bounds__(256) k_integrate(uint32_t *__restrict__ vol, o
         culled |= (out == 0xffu);
       }
     }
-    if (!culled) {
-      const int lx = t >> 4, ly = (t >> 1) & 7, lz0 = (t & 1) * 4;
-      const int i = bx * 8 + lx, j = by * 8 + ly;
-      float X0 = fmaf(S.m[0], (float)i, fmaf(S.m[1], (float)j, S.o[0]));
-      float Y0 = fmaf(S.m[3], (float)i, fmaf(S.m[4], (float)j, S.o[1]));
-      float Z0 = fmaf(S.m[6], (float)i, fmaf(S.m[7], (float)j, S.o[2]));
-      float tnew[4];
-      bool upd[4];
-      bool any = false;
+    if (culled) continue;
+    const int i = cbx * 8 + lx, j = cby * 8 + ly;
+    float X0 = fmaf(S.m[0], (float)lx, fmaf(S.m[1], (float)ly, BX));
+    float Y0 = fmaf(S.m[3], (float)lx, fmaf(S.m[4], (float)ly, BY));
+    float Z0 = fmaf(S.m[6], (float)lx, fmaf(S.m[7], (float)ly, BZ));
+    float tnew[4];
+    unsigned upd = 0;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      const float lz = (float)(lz0 + m);
+      tnew[m] = 0.f;
+      float X = fmaf(S.m[2], lz, X0);
+      float Y = fmaf(S.m[5], lz, Y0);
+      float Z = fmaf(S.m[8], lz, Z0);
+      // -Z in [dmin, dmax] (and Z < 0): one unsigned-style range test
+      if (!(-Z - cam.dmin <= dspan && -Z >= cam.dmin)) continue;
+      float rz = __frcp_rn(Z);
+      // roundFloat as floor(x + 0.5): identical except within one FP32 ulp of
+      // a half-integer
+      int pu = __float2int_rd(fmaf(cam.fx * X, rz, cam.cx) + 0.5f);
+      int pv = __float2int_rd(fmaf(cam.fy * Y, rz, cam.cy) + 0.5f);
+      if ((unsigned)(pu - 2) >= uspan || (unsigned)(pv - 2) >= vspan) continue;
+      float D = (float)__ldg(depth + pv * pitch + pu);
+      if (!(D - cam.dmin <= dspan && D >= cam.dmin && D > 0.f)) continue;
+      float2 lm = __ldg(lam + pv * cam.w + pu);
+      // SDF = L - r with L = lambda D, r = |p_c|; decide on squares first
+      float r2 = fmaf(X, X, fmaf(Y, Y, Z * Z));
+      float L = lm.x * D;
+      const float slack = 0.05f + 1e-5f * L;
+      float far = L + T + slack;            // SDF < -T - slack  <=>  r > far
+      if (r2 > far * far) continue;
+      float nearl = L - T - slack;          // SDF >  T + slack  <=>  r < nearl
+      float sn;
+      if (nearl > 0.f && r2 < nearl * nearl) {
+        sn = 1.0f;
+      } else {
+        float2 rr = voxel_range(S, i, j, cbz * 8 + lz0 + m);
+        float2 Lp = two_prod(lm.x, D);
+        Lp.y = __fmaf_rn(lm.y, D, Lp.y);
+        float sdf2 = __fadd_rn(__fsub_rn(Lp.x, rr.x), __fsub_rn(Lp.y, rr.y));
+        if (sdf2 < -T) continue;
+        sn = fminf(sdf2, T) * inv_T;
+      }
+      upd |= 1u << m;
+      tnew[m] = sn;
+    }
+    if (CENSUS) {
+      my_count += __popc(upd);
+    } else if (upd) {
+      uint4 *p4 = reinterpret_cast<uint4 *>(vol + ((size_t)b << 9)) + t;
+      uint4 wv = *p4;
+      uint32_t w4[4] = {wv.x, wv.y, wv.z, wv.w};
 #pragma unroll
       for (int m = 0; m < 4; ++m) {
-        const int k = bz * 8 + lz0 + m;
-        upd[m] = false;
-        tnew[m] = 0.f;
-        float X = fmaf(S.m[2], (float)k, X0);
-        float Y = fmaf(S.m[5], (float)k, Y0);
-        float Z = fmaf(S.m[8], (float)k, Z0);
-        if (!(Z < 0.f) || -Z < cam.dmin || -Z > cam.dmax) continue;
-        float rz = __frcp_rn(Z);
-        float uf = fmaf(cam.fx * X, rz, cam.cx);
-        float vf = fmaf(cam.fy * Y, rz, cam.cy);
-        int pu = round_ref(uf), pv = round_ref(vf);
-        if (pu < 2 || pu >= cam.w - 2 || pv < 2 || pv >= cam.h - 2) continue;
-        float D = (float)__ldg(depth + (size_t)pv * pitch + pu);
-        if (!(D > 0.f && D >= cam.dmin && D <= cam.dmax)) continue;
-        float2 lm = __ldg(lam + (size_t)pv * cam.w + pu);
-        float r = sqrtf(fmaf(X, X, fmaf(Y, Y, Z * Z)));
-        float sdf = fmaf(lm.x, D, -r);
-        const float slack = 0.05f + 1e-5f * r;
-        if (sdf < -desc.trunc_mm - slack) continue;
-        float sn;
-        if (sdf > desc.trunc_mm + slack) {
-          sn = 1.0f;
-        } else {
-          float2 rr = voxel_range(S, i, j, k);
-          float2 L = two_prod(lm.x, D);
-          L.y = __fmaf_rn(lm.y, D, L.y);
-          float sdf2 = __fadd_rn(__fsub_rn(L.x, rr.x), __fsub_rn(L.y, rr.y));
-          if (sdf2 < -desc.trunc_mm) continue;
-          sn = __fdiv_rn(fminf(sdf2, desc.trunc_mm), desc.trunc_mm);
-        }
-        upd[m] = true;
-        tnew[m] = sn;
-        any = true;
+        if (!(upd & (1u << m))) continue;
+        uint32_t word = w4[m];
+        uint32_t wt = word >> 16;
+        float told = wt ? VoxelCodec<STORAGE>::tsdf(word) : 0.f;
+        // (told w + tsdf') / (w + 1), within a few ulp of the rounded quotient
+        float tn = __fdividef(__fmaf_rn(told, (float)wt, tnew[m]), (float)(wt + 1u));
+        uint32_t wn = min(wt + 1u, (uint32_t)desc.max_weight);
+        w4[m] = VoxelCodec<STORAGE>::pack(tn, wn);
       }
-      if (CENSUS) {
-        my_count = (unsigned)upd[0] + (unsigned)upd[1] + (unsigned)upd[2] + (unsigned)upd[3];
-      } else if (any) {
-        uint4 *p4 = reinterpret_cast<uint4 *>(vol + (b << 9)) + t;
-        uint4 wv = *p4;
-        uint32_t w4[4] = {wv.x, wv.y, wv.z, wv.w};
-#pragma unroll
-        for (int m = 0; m < 4; ++m) {
-          if (!upd[m]) continue;
-          uint32_t word = w4[m];
-          uint32_t wt = word >> 16;
-          float told = wt ? VoxelCodec<STORAGE>::tsdf(word) : 0.f;
-          float tn = __fdiv_rn(__fmaf_rn(told, (float)wt, tnew[m]), (float)(wt + 1u));
-          uint32_t wn = min(wt + 1u, (uint32_t)desc.max_weight);
-          w4[m] = VoxelCodec<STORAGE>::pack(tn, wn);
-        }
-        *p4 = make_uint4(w4[0], w4[1], w4[2], w4[3]);
-      }
+      *p4 = make_uint4(w4[0], w4[1], w4[2], w4[3]);
     }
   }
   if (CENSUS) {
@@ -204,8 +224,9 @@ of_status_t launch_integrate(const of_volume_desc_t *d, void *vol, const of_came
                              const uint16_t *depth, int pitch, const double *pose,
                              const float *lam, unsigned long long *count, cudaStream_t s) {
   size_t nb = (size_t)(d->resolution / 8);
-  size_t nbricks = nb * nb * nb;
-  unsigned blocks = (unsigned)((nbricks + 1) / 2);
+  size_t pairs = (nb * nb * nb + 1) / 2;
+  // persistent grid: 8 resident CTAs of 256 threads per SM
+  unsigned blocks = (unsigned)(pairs < (size_t)kSmCount * 8 ? pairs : (size_t)kSmCount * 8);
   Cam c = make_cam(*cam);
   if (d->storage == OF_TSDF_I16)
     k_integrate<OF_TSDF_I16, CENSUS><<<blocks, 256, 0, s>>>(

@@ -71,6 +71,63 @@ __global__ void __launch_bounds__(256) k_bilateral(const uint16_t *__restrict__ 
   out[(size_t)y * w + x] = result;
 }
 
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Same filter with the radius fixed at compile time (taps fully unrolled).
+// Invalid depths are stored as -1e30 in the tile: their squared range
+// difference overflows to +inf and their weight 2^-inf is exactly 0, so no
+// per-tap select is needed. One ex2 per tap.
+template <int R>
+__global__ void __launch_bounds__(256) k_bilateral_r(const uint16_t *__restrict__ depth, int pitch,
+                                                     int w, int h, float dmin, float dmax,
+                                                     float ks, float kr, float *__restrict__ out) {
+  constexpr int TW = kTileX + 2 * R;
+  constexpr int TH = kTileY + 2 * R;
+  __shared__ float tile[TH * TW];
+  const int x0 = blockIdx.x * kTileX - R;
+  const int y0 = blockIdx.y * kTileY - R;
+  for (int i = threadIdx.x; i < TW * TH; i += blockDim.x) {
+    int tx = i % TW, ty = i / TW;
+    int gx = x0 + tx, gy = y0 + ty;
+    float d = -1e30f;
+    if (gx >= 0 && gx < w && gy >= 0 && gy < h) {
+      float v = (float)__ldg(depth + (size_t)gy * pitch + gx);
+      if (depth_valid(v, dmin, dmax)) d = v;
+    }
+    tile[i] = d;
+  }
+  __syncthreads();
+  const int lx = threadIdx.x % kTileX, ly = threadIdx.x / kTileX;
+  const int x = blockIdx.x * kTileX + lx, y = blockIdx.y * kTileY + ly;
+  if (x >= w || y >= h) return;
+  const float *ctr = tile + (ly + R) * TW + lx + R;
+  const float c = *ctr;
+  float result = 0.f;
+  if (c > 0.f) {
+    const float nkr = -kr;
+    float sw = 0.f, sd = 0.f;
+#pragma unroll
+    for (int dy = -R; dy <= R; ++dy) {
+      const float ry = -(float)(dy * dy) * ks;
+#pragma unroll
+      for (int dx = -R; dx <= R; ++dx) {
+        float q = ctr[dy * TW + dx];
+        float del = q - c;
+        float e = fmaf(del * nkr, del, fmaf(-(float)(dx * dx), ks, ry));
+        float wt = ex2_approx(e);
+        sw += wt;
+        sd = fmaf(wt, q, sd);
+      }
+    }
+    result = sd / sw;
+  }
+  out[(size_t)y * w + x] = result;
+}
+
 // Level l -> l+1: pixel (x, y) averages the valid pixels of the 2x2 block
 // {2x, 2x+1} x {2y, 2y+1} that lie within 3 sigma_r of the block's first
 // valid pixel (row-major order); 0 if the block has none.
@@ -159,9 +216,29 @@ extern "C" of_status_t of_preprocess(const of_camera_t *cam, const of_filter_par
   {
     dim3 grid((cam->width + kTileX - 1) / kTileX, (cam->height + kTileY - 1) / kTileY);
     size_t smem = (size_t)(kTileX + 2 * R) * (kTileY + 2 * R) * sizeof(float);
-    k_bilateral<<<grid, kTileX * kTileY, smem, s>>>(
-        d_depth, pitch, cam->width, cam->height, cam->min_depth_mm, cam->max_depth_mm, R, ks, kr,
-        (float *)(base + lay.depth_offset[0]));
+    float *o = (float *)(base + lay.depth_offset[0]);
+    const int W = cam->width, H = cam->height;
+    const float dmn = cam->min_depth_mm, dmx = cam->max_depth_mm;
+#define OF_BILATERAL_CASE(RR)                                                              \
+  case RR:                                                                                 \
+    k_bilateral_r<RR><<<grid, kTileX * kTileY, 0, s>>>(d_depth, pitch, W, H, dmn, dmx, ks, \
+                                                        kr, o);                           \
+    break;
+    switch (R) {
+      OF_BILATERAL_CASE(3)
+      OF_BILATERAL_CASE(4)
+      OF_BILATERAL_CASE(5)
+      OF_BILATERAL_CASE(6)
+      OF_BILATERAL_CASE(7)
+      OF_BILATERAL_CASE(8)
+      OF_BILATERAL_CASE(9)
+      OF_BILATERAL_CASE(10)
+      OF_BILATERAL_CASE(12)
+      default:
+        k_bilateral<<<grid, kTileX * kTileY, smem, s>>>(d_depth, pitch, W, H, dmn, dmx, R, ks, kr,
+                                                        o);
+    }
+#undef OF_BILATERAL_CASE
   }
   float guard = 3.0f * fp->sigma_range_mm;
   for (int l = 1; l < fp->levels; ++l) {

@@ -28,26 +28,51 @@ struct RaySetup {
   float inv_vs;
 };
 
+// Normalised tsdf of a voxel word for the raycast (weight 0 reads +1). The
+// int16 path converts without I2F: 2^23 + 2^22 + q is exact in FP32.
+template <int STORAGE>
+__device__ __forceinline__ float ray_value(uint32_t w) {
+  if (STORAGE == OF_TSDF_I16) {
+    int q = ((int)(w << 16)) >> 16;
+    float v = (__int_as_float(0x4B400000 + q) - 12582912.0f) * (1.0f / kQ);
+    return w < 65536u ? 1.0f : v;
+  } else {
+    return w < 65536u ? 1.0f : __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
+  }
+}
+
+// Trilinear tsdf at a world position. Corner (i0, j0, k0) is clamped to
+// [0, n-2]; the seven other corners are the base address plus an axis step
+// that crosses into the next brick when the local coordinate is 7. Volume
+// indices fit in 32 bits (n <= 1024).
 template <int STORAGE>
 __device__ __forceinline__ float trilinear(const uint32_t *__restrict__ vol, int n, int nb,
                                            float org, float inv_vs, float px, float py, float pz) {
-  float gx = (px - org) * inv_vs - 0.5f;
-  float gy = (py - org) * inv_vs - 0.5f;
-  float gz = (pz - org) * inv_vs - 0.5f;
-  int ix = min(max((int)floorf(gx), 0), n - 2);
-  int iy = min(max((int)floorf(gy), 0), n - 2);
-  int iz = min(max((int)floorf(gz), 0), n - 2);
+  float gx = fmaf(px - org, inv_vs, -0.5f);
+  float gy = fmaf(py - org, inv_vs, -0.5f);
+  float gz = fmaf(pz - org, inv_vs, -0.5f);
+  int ix = min(max(__float2int_rd(gx), 0), n - 2);
+  int iy = min(max(__float2int_rd(gy), 0), n - 2);
+  int iz = min(max(__float2int_rd(gz), 0), n - 2);
   float fx = gx - (float)ix, fy = gy - (float)iy, fz = gz - (float)iz;
-  float c[8];
-#pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    int a = (q >> 2) & 1, b = (q >> 1) & 1, d = q & 1;
-    c[q] = vox_value<STORAGE>(__ldg(vol + vox_index(nb, ix + a, iy + b, iz + d)));
-  }
-  float c00 = fmaf(fz, c[1] - c[0], c[0]);
-  float c01 = fmaf(fz, c[3] - c[2], c[2]);
-  float c10 = fmaf(fz, c[5] - c[4], c[4]);
-  float c11 = fmaf(fz, c[7] - c[6], c[6]);
+  unsigned base = ((((unsigned)(ix >> 3) * nb + (unsigned)(iy >> 3)) * nb + (unsigned)(iz >> 3)) << 9) |
+                  (unsigned)(((ix & 7) << 6) | ((iy & 7) << 3) | (iz & 7));
+  unsigned dx = (ix & 7) == 7 ? (unsigned)nb * nb * 512u - 448u : 64u;
+  unsigned dy = (iy & 7) == 7 ? (unsigned)nb * 512u - 56u : 8u;
+  unsigned dz = (iz & 7) == 7 ? 505u : 1u;
+  const uint32_t *p0 = vol + base;
+  float c000 = ray_value<STORAGE>(__ldg(p0));
+  float c001 = ray_value<STORAGE>(__ldg(p0 + dz));
+  float c010 = ray_value<STORAGE>(__ldg(p0 + dy));
+  float c011 = ray_value<STORAGE>(__ldg(p0 + dy + dz));
+  float c100 = ray_value<STORAGE>(__ldg(p0 + dx));
+  float c101 = ray_value<STORAGE>(__ldg(p0 + dx + dz));
+  float c110 = ray_value<STORAGE>(__ldg(p0 + dx + dy));
+  float c111 = ray_value<STORAGE>(__ldg(p0 + dx + dy + dz));
+  float c00 = fmaf(fz, c001 - c000, c000);
+  float c01 = fmaf(fz, c011 - c010, c010);
+  float c10 = fmaf(fz, c101 - c100, c100);
+  float c11 = fmaf(fz, c111 - c110, c110);
   float c0 = fmaf(fy, c01 - c00, c00);
   float c1 = fmaf(fy, c11 - c10, c10);
   return fmaf(fx, c1 - c0, c0);

@@ -147,6 +147,20 @@ class Oracle:
             parts += [dep, np.asarray(levels_pts[l], self.real).reshape(-1)]
         return np.ascontiguousarray(np.concatenate(parts))
 
+    def vertex_normal(self, cfg, level: int, depth: np.ndarray) -> np.ndarray:
+        d = np.ascontiguousarray(depth, self.real)
+        pts = np.zeros(d.shape + (8,), self.real)
+        self.lib.ora_vertex_normal(C.byref(self.cam(cfg, level)), d.ctypes.data, pts.ctypes.data)
+        return pts
+
+    def pyr_down(self, cfg, src: np.ndarray) -> np.ndarray:
+        s_ = np.ascontiguousarray(src, self.real)
+        h, w = (s_.shape[0] + 1) // 2, (s_.shape[1] + 1) // 2
+        dst = np.zeros((h, w), self.real)
+        self.lib.ora_pyr_down(s_.ctypes.data, s_.shape[1], s_.shape[0], dst.ctypes.data, w, h,
+                              3.0 * cfg.sigma_range_mm)
+        return dst
+
     def integrate(self, cfg, words: np.ndarray, depth: np.ndarray, pose: np.ndarray,
                   ambig: bool = False):
         """In-place update of linear-layout uint32 `words`; returns (updated, ambig mask)."""

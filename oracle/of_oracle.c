@@ -246,14 +246,14 @@ int64_t ora_integrate(const ora_vol *v, uint32_t *words, const ora_cam *c, const
         R Y = (R)P[1] * dlt[0] + (R)P[5] * dlt[1] + (R)P[9] * dlt[2];
         R Z = (R)P[2] * dlt[0] + (R)P[6] * dlt[1] + (R)P[10] * dlt[2];
         if (ambig) {
-          if (fabs(-(double)Z - c->dmin) < 1e-2 || fabs(-(double)Z - c->dmax) < 1e-2) amb = 1;
+          if (fabs(-(double)Z - c->dmin) < 2e-3 || fabs(-(double)Z - c->dmax) < 2e-3) amb = 1;
         }
         int upd = 0;
         R sn = 0;
         if (Z < 0 && -Z >= (R)c->dmin && -Z <= (R)c->dmax) {
           R uf = (R)c->fx * X / Z + (R)c->cx;
           R vf = (R)c->fy * Y / Z + (R)c->cy;
-          if (ambig && (near_half(uf, 2e-3) || near_half(vf, 2e-3))) amb = 1;
+          if (ambig && (near_half(uf, 1e-3) || near_half(vf, 1e-3))) amb = 1;
           int pu = round_ref(uf), pv = round_ref(vf);
           if (!(pu < 2 || pu >= c->w - 2 || pv < 2 || pv >= c->h - 2)) {
             double D = depth[(size_t)pv * c->w + pu];
