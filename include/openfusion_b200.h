@@ -132,7 +132,8 @@ of_status_t of_camera_level(const of_camera_t *cam, int32_t level, of_camera_t *
 
 /* ---- volume (replaces General::InitVoxelArray, General.cpp:42-49) ----- */
 
-/* Bytes of a volume: N^3 x 4 (8^3-voxel bricks, brick-major). */
+/* Bytes of a volume: N^3 x 4 (8^3-voxel bricks, brick-major) followed by one
+ * flag byte per brick (brick or a neighbour near a surface), padded to 256. */
 of_status_t of_volume_bytes(const of_volume_desc_t *desc, size_t *bytes);
 /* Resets every voxel to weight 0 (tsdf reads as +trunc), replacing
  * d_initVoxelArray (Source/src/General.cu:27-50). */

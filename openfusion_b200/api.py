@@ -221,20 +221,24 @@ def unpack_depth(cfg: Config, pyr, level: int = 0):
 
 
 def volume_to_linear(cfg: Config, vol_words: np.ndarray):
-    """Brick-major voxel words -> (tsdf_q int16 or f16 bits, weight) in x,y,z order."""
+    """Brick-major voxel words -> (tsdf_q int16 or f16 bits, weight) in x,y,z order.
+    `vol_words` is a whole volume buffer (its trailing brick flags are ignored)."""
     n = cfg.resolution
     nb = n // 8
-    w = np.asarray(vol_words).view(np.uint32).reshape(nb, nb, nb, 8, 8, 8)
+    w = np.asarray(vol_words).view(np.uint32)[: n ** 3].reshape(nb, nb, nb, 8, 8, 8)
     w = w.transpose(0, 3, 1, 4, 2, 5).reshape(n, n, n)
     return (w & 0xFFFF).astype(np.uint16), (w >> 16).astype(np.uint16)
 
 
 def linear_to_volume(cfg: Config, q: np.ndarray, weight: np.ndarray) -> np.ndarray:
+    """(q, weight) in x,y,z order -> a whole volume buffer (int32 words) with
+    every brick flagged as near a surface."""
     n = cfg.resolution
     nb = n // 8
     words = (q.astype(np.uint32) & 0xFFFF) | (weight.astype(np.uint32) << 16)
     words = words.reshape(nb, 8, nb, 8, nb, 8).transpose(0, 2, 4, 1, 3, 5).reshape(-1)
-    return words.view(np.int32)
+    flags = np.ones(volume_bytes(cfg) - 4 * n ** 3, np.uint8)
+    return np.concatenate([words.view(np.uint8), flags]).view(np.int32)
 
 
 # ----------------------------------------------------------------- tracker --

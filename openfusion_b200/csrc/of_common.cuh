@@ -173,24 +173,37 @@ __host__ __device__ __forceinline__ size_t vox_index(int nb, int i, int j, int k
   return (b << 9) | (size_t)(((i & 7) << 6) | ((j & 7) << 3) | (k & 7));
 }
 
+// Brick flags follow the voxels: one byte per brick, set (sticky) on a brick
+// and its 26 neighbours when a voxel of the brick is written with |tsdf| < 1.
+// An unflagged brick and all its neighbours hold only saturated (+1) or
+// unobserved voxels.
+__host__ __device__ __forceinline__ uint8_t *brick_flags(void *vol, int n) {
+  return (uint8_t *)vol + (size_t)n * n * n * sizeof(uint32_t);
+}
+
 template <int STORAGE>
 struct VoxelCodec;
 
 template <>
 struct VoxelCodec<OF_TSDF_I16> {
-  // normalised tsdf in [-1, 1]
+  static constexpr uint32_t kOneBits = 32767u;  // stored bits of tsdf = +1
+  // normalised tsdf in [-1, 1]; int16 <-> float without I2F/F2I: for |q| <
+  // 2^22, 1.5 * 2^23 + q is exact in FP32 and adding 1.5 * 2^23 rounds to the
+  // nearest integer, ties to even (the FP32 default rounding).
   __device__ __forceinline__ static float tsdf(uint32_t w) {
-    return (float)(int16_t)(w & 0xffffu) * (1.0f / kQ);
+    int q = ((int)(w << 16)) >> 16;
+    return (__int_as_float(0x4B400000 + q) - 12582912.0f) * (1.0f / kQ);
   }
   __device__ __forceinline__ static uint32_t pack(float tsdf_norm, uint32_t weight) {
-    int q = __float2int_rn(tsdf_norm * kQ);
-    q = max(-32767, min(32767, q));
-    return ((uint32_t)(uint16_t)(int16_t)q) | (weight << 16);
+    float x = fminf(fmaxf(tsdf_norm * kQ, -kQ), kQ);
+    int q = __float_as_int(x + 12582912.0f) - 0x4B400000;
+    return ((uint32_t)q & 0xffffu) | (weight << 16);
   }
 };
 
 template <>
 struct VoxelCodec<OF_TSDF_F16> {
+  static constexpr uint32_t kOneBits = 0x3C00u;  // IEEE half 1.0
   __device__ __forceinline__ static float tsdf(uint32_t w) {
     return __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
   }

@@ -101,14 +101,16 @@ extern "C" of_status_t of_pyramid_layout(const of_camera_t *cam, int32_t levels,
 extern "C" of_status_t of_volume_bytes(const of_volume_desc_t *d, size_t *bytes) {
   if (!of_volume_valid(d) || !bytes) return OF_ERR_INVALID_ARGUMENT;
   size_t n = (size_t)d->resolution;
-  *bytes = n * n * n * sizeof(uint32_t);
+  size_t nb = n / kBrick;
+  *bytes = n * n * n * sizeof(uint32_t) + align256(nb * nb * nb);
   return OF_OK;
 }
 
 extern "C" of_status_t of_volume_reset(const of_volume_desc_t *d, void *vol, of_stream_t s) {
   size_t bytes;
   if (of_volume_bytes(d, &bytes) != OF_OK || !vol) return OF_ERR_INVALID_ARGUMENT;
-  // weight 0 everywhere: every voxel reads as +trunc (General.cu:27-50).
+  // weight 0 everywhere: every voxel reads as +trunc (General.cu:27-50);
+  // every brick flag cleared.
   OF_CUDA_TRY(cudaMemsetAsync(vol, 0, bytes, (cudaStream_t)s));
   return OF_OK;
 }
@@ -170,7 +172,13 @@ extern "C" of_status_t of_volume_import(const of_volume_desc_t *d, void *vol, co
   else
     k_volume_import<OF_TSDF_F16><<<blocks, 256, 0, (cudaStream_t)s>>>((uint32_t *)vol, g, tsdf,
                                                                      weight);
-  return of_launch_status();
+  of_status_t st = of_launch_status();
+  if (st != OF_OK) return st;
+  // imported content is unknown: mark every brick as near a surface
+  size_t n = (size_t)d->resolution, nb = n / kBrick;
+  OF_CUDA_TRY(cudaMemsetAsync((char *)vol + n * n * n * sizeof(uint32_t), 1, nb * nb * nb,
+                              (cudaStream_t)s));
+  return OF_OK;
 }
 
 // ------------------------------------------------------- ray-length table --

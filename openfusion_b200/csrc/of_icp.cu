@@ -33,9 +33,9 @@ constexpr int kIcpMaxBlocks = 2 * kSmCount;
 constexpr int kVals = 29;  // 21 + 6 + residual^2 + inliers
 constexpr float kEps = 1e-6f;  // _EPSILON_ (Constants.h:14)
 
-constexpr int kFusedThreads = 512;
-constexpr int kFusedMaxBlocks = 4 * kSmCount;
-// A grid barrier gives up after about 0.25 s (this many 64 ns sleeps) and
+constexpr int kFusedThreads = 1024;
+constexpr int kFusedMaxBlocks = 2 * kSmCount;
+// A grid barrier gives up after about 0.15 s (this many 32 ns sleeps) and
 // reports status 2 instead of waiting forever.
 constexpr unsigned kSpinLimit = 1u << 22;
 
@@ -67,7 +67,8 @@ __device__ __forceinline__ void kahan_add(float &sum, float &comp, float x) {
 // FP64 6x6 Cholesky solve of H x = g (H given by its 21 upper entries).
 // Returns false when a pivot is not larger than 1e-12 x the largest diagonal
 // entry or is not finite; *minpiv gets the smallest pivot / largest diagonal.
-__device__ bool chol_solve6(const double *up, const double *g, double *x, double *minpiv) {
+__device__ __noinline__ bool chol_solve6(const double *up, const double *g, double *x,
+                                        double *minpiv) {
   double H[6][6];
   int q = 0;
   for (int i = 0; i < 6; ++i)
@@ -81,17 +82,20 @@ __device__ bool chol_solve6(const double *up, const double *g, double *x, double
   double L[6][6] = {};
   double mp = 1e300;
   bool ok = dmax > 0.0 && isfinite(dmax);
+  double inv[6];
+  const double inv_dmax = 1.0 / dmax;
   for (int j = 0; j < 6 && ok; ++j) {
     double s = H[j][j];
     for (int k = 0; k < j; ++k) s -= L[j][k] * L[j][k];
-    mp = fmin(mp, s / dmax);
+    mp = fmin(mp, s * inv_dmax);
     if (!(s > 1e-12 * dmax) || !isfinite(s)) { ok = false; break; }
     double ljj = sqrt(s);
+    inv[j] = 1.0 / ljj;
     L[j][j] = ljj;
     for (int i = j + 1; i < 6; ++i) {
       double t = H[i][j];
       for (int k = 0; k < j; ++k) t -= L[i][k] * L[j][k];
-      L[i][j] = t / ljj;
+      L[i][j] = t * inv[j];
     }
   }
   *minpiv = ok ? mp : fmin(mp, 0.0);
@@ -100,20 +104,23 @@ __device__ bool chol_solve6(const double *up, const double *g, double *x, double
   for (int i = 0; i < 6; ++i) {
     double t = g[i];
     for (int k = 0; k < i; ++k) t -= L[i][k] * y[k];
-    y[i] = t / L[i][i];
+    y[i] = t * inv[i];
   }
   for (int i = 5; i >= 0; --i) {
     double t = y[i];
     for (int k = i + 1; k < 6; ++k) t -= L[k][i] * x[k];
-    x[i] = t / L[i][i];
+    x[i] = t * inv[i];
   }
   return true;
 }
 
 // dT of Cpu_buildNewTransformMatrix (ICP.cu:266-290) in FP64, then P <- dT P.
-__device__ void compose_increment(const double *xo, double *P) {
+__device__ __noinline__ void compose_increment(const double *xo, double *P) {
   double al = xo[0], be = xo[1], ga = xo[2];
-  double ca = cos(al), sa = sin(al), cb = cos(be), sb = sin(be), cg = cos(ga), sg = sin(ga);
+  double ca, sa, cb, sb, cg, sg;
+  sincos(al, &sa, &ca);
+  sincos(be, &sb, &cb);
+  sincos(ga, &sg, &cg);
   double D[16] = {cg * cb, -sg * ca + cg * sb * sa, sg * sa + cg * sb * ca, xo[3],
                   sg * cb, cg * ca + sg * sb * sa,  -cg * sa + sg * sb * ca, xo[4],
                   -sb,     cb * sa,                 cb * ca,                 xo[5],
@@ -295,7 +302,7 @@ __device__ __forceinline__ void grid_barrier(IcpWorkspace *ws, unsigned nblocks)
           atomicExch(&ws->error, 1);
           break;
         }
-        __nanosleep(64);
+        __nanosleep(32);
       }
     }
     __threadfence();
@@ -397,15 +404,23 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       // every block: Kahan over its strided share of the blocks' partials,
       // then a tree over the groups, in a fixed order
       {
+        // all of this lane's loads are issued before the Kahan chain uses them
+        constexpr int kPer = (kFusedMaxBlocks + kWarps - 1) / kWarps;
         const int v = lane, grp = warp;
+        float vals[kPer];
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+          int r = grp + q * kWarps;
+          vals[q] = (v < kVals && r < (int)gridDim.x) ? __ldcg(&ws->fused_partials[buf][r][v]) : 0.f;
+        }
         float sum = 0.f, c = 0.f;
-        if (v < kVals)
-          for (int r = grp; r < (int)gridDim.x; r += kWarps) {
-            float y = __ldcg(&ws->fused_partials[buf][r][v]) - c;
-            float t = sum + y;
-            c = (t - sum) - y;
-            sum = t;
-          }
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+          float y = vals[q] - c;
+          float t = sum + y;
+          c = (t - sum) - y;
+          sum = t;
+        }
         s_red[grp][v] = sum - c;
       }
       __syncthreads();

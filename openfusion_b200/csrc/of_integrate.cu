@@ -75,9 +75,35 @@ __device__ __forceinline__ float2 voxel_range(const IntegrateSetup &S, int i, in
   return df_sqrt(acc);
 }
 
+// Frustum plane in world space: inside <=> n . p + d <= 0.
 struct Plane {
-  float a, b, c, d;  // inside <=> a X + b Y + c Z + d <= 0
+  float nx, ny, nz, d;
 };
+
+// The six frustum planes (pixel border, min/max depth) in world space, with
+// half a pixel / 1 mm of slack: the brick test only has to be conservative,
+// the per-voxel test is exact.
+__device__ void make_planes(const double *P, const Cam &cam, Plane *pl) {
+  double umin = 1.0, umax = (double)cam.w - 2.0;
+  double vmin = 1.0, vmax = (double)cam.h - 2.0;
+  // camera-space planes (a, b, c, d): inside <=> a X + b Y + c Z + d <= 0
+  double cp[6][4] = {{cam.fx, 0.0, cam.cx - umin, 0.0},
+                     {-cam.fx, 0.0, umax - cam.cx, 0.0},
+                     {0.0, cam.fy, cam.cy - vmin, 0.0},
+                     {0.0, -cam.fy, vmax - cam.cy, 0.0},
+                     {0.0, 0.0, 1.0, cam.dmin - 1.0},
+                     {0.0, 0.0, -1.0, -cam.dmax - 1.0}};
+  // X_cam = R^T (p - c): n_w = R n_c, d_w = d - n_w . c
+  for (int q = 0; q < 6; ++q) {
+    double nw[3];
+    for (int i = 0; i < 3; ++i)
+      nw[i] = P[4 * i] * cp[q][0] + P[4 * i + 1] * cp[q][1] + P[4 * i + 2] * cp[q][2];
+    double dw = cp[q][3] - (nw[0] * P[3] + nw[1] * P[7] + nw[2] * P[11]);
+    pl[q] = {(float)nw[0], (float)nw[1], (float)nw[2], (float)dw};
+  }
+}
+
+constexpr int kChunk = 32;  // bricks tested by one warp ballot
 
 template <int STORAGE, bool CENSUS>
 __global__ void __launch_bounds__(256) k_integrate(uint32_t *__restrict__ vol, of_volume_desc_t desc,
@@ -87,24 +113,17 @@ __global__ void __launch_bounds__(256) k_integrate(uint32_t *__restrict__ vol, o
                                                    unsigned long long *count) {
   __shared__ IntegrateSetup S;
   __shared__ Plane planes[6];
+  __shared__ unsigned int s_mask;
   __shared__ unsigned int s_count;
   if (threadIdx.x == 0) {
     make_setup(pose, desc, S);
-    // frustum planes in camera space with half a pixel / 1 mm of slack; the
-    // per-voxel test below is exact, this one only has to be conservative.
-    float umin = 1.5f - 0.5f, umax = (float)cam.w - 2.5f + 0.5f;
-    float vmin = 1.5f - 0.5f, vmax = (float)cam.h - 2.5f + 0.5f;
-    planes[0] = {cam.fx, 0.f, cam.cx - umin, 0.f};
-    planes[1] = {-cam.fx, 0.f, umax - cam.cx, 0.f};
-    planes[2] = {0.f, cam.fy, cam.cy - vmin, 0.f};
-    planes[3] = {0.f, -cam.fy, vmax - cam.cy, 0.f};
-    planes[4] = {0.f, 0.f, 1.f, cam.dmin - 1.f};
-    planes[5] = {0.f, 0.f, -1.f, -cam.dmax - 1.f};
+    make_planes(pose, cam, planes);
     s_count = 0;
   }
   __syncthreads();
   const int nb = desc.resolution >> 3;
   const int nbricks = nb * nb * nb;
+  const int nchunks = (nbricks + kChunk - 1) / kChunk;
   const int half = threadIdx.x >> 7;
   const int t = threadIdx.x & 127;
   const int lane = threadIdx.x & 31;
@@ -112,103 +131,137 @@ __global__ void __launch_bounds__(256) k_integrate(uint32_t *__restrict__ vol, o
   const float T = desc.trunc_mm, inv_T = 1.0f / desc.trunc_mm;
   const float dspan = cam.dmax - cam.dmin;
   const unsigned uspan = (unsigned)(cam.w - 4), vspan = (unsigned)(cam.h - 4);
-  // brick b = 2 * pair + half walks the grid with a fixed stride; its (x, y, z)
-  // brick coordinates advance by the stride's digits with carries.
-  int b = 2 * blockIdx.x + half;
-  const int stride = 2 * gridDim.x;
-  const int sz = stride % nb, sy = (stride / nb) % nb, sx = stride / (nb * nb);
-  int bz = b % nb, by = (b / nb) % nb, bx = b / (nb * nb);
+  const float vs = S.vs_hi;
+  const float org = -0.5f * desc.size_mm;
+  const float hext = 3.5f * vs + 1e-3f;  // half extent of a brick's voxel centres
   unsigned int my_count = 0;
-  for (; b < nbricks; b += stride) {
-    // camera-space centre of the brick's voxel (0,0,0), FP64 then rounded:
-    // per-voxel offsets from it stay below 8 voxels, so the FP32 position
-    // error is about one rounding of the brick base.
-    const double fbx = (double)bx, fby = (double)by, fbz = (double)bz;
-    const float BX = (float)fma(S.mb[0], fbx, fma(S.mb[1], fby, fma(S.mb[2], fbz, S.ob[0])));
-    const float BY = (float)fma(S.mb[3], fbx, fma(S.mb[4], fby, fma(S.mb[5], fbz, S.ob[1])));
-    const float BZ = (float)fma(S.mb[6], fbx, fma(S.mb[7], fby, fma(S.mb[8], fbz, S.ob[2])));
-    const int cbx = bx, cby = by, cbz = bz;
-    bz += sz; if (bz >= nb) { bz -= nb; ++by; }
-    by += sy; if (by >= nb) { by -= nb; ++bx; }
-    bx += sx;
-    // ---- brick cull: lanes 0..7 take one corner voxel centre each
-    bool culled = false;
-    {
-      float ci = (lane & 4) ? 7.f : 0.f, cj = (lane & 2) ? 7.f : 0.f, ck = (lane & 1) ? 7.f : 0.f;
-      float X = fmaf(S.m[0], ci, fmaf(S.m[1], cj, fmaf(S.m[2], ck, BX)));
-      float Y = fmaf(S.m[3], ci, fmaf(S.m[4], cj, fmaf(S.m[5], ck, BY)));
-      float Z = fmaf(S.m[6], ci, fmaf(S.m[7], cj, fmaf(S.m[8], ck, BZ)));
+  const float cxh = cam.cx + 0.5f, cyh = cam.cy + 0.5f;
+  const float dlo = fmaxf(cam.dmin, 0.5f), dhi = cam.dmax;
+  const int nb2 = nb * nb;
+  uint8_t *flags = brick_flags(vol, desc.resolution);
+  for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+    const int b0 = chunk * kChunk;
+    // brick coordinates of the chunk's first brick (one division per chunk)
+    const int bz0 = b0 % nb, by0 = (b0 / nb) % nb, bx0 = b0 / nb2;
+    // ---- visibility of 32 bricks: one lane per brick, world-space box vs planes
+    if (threadIdx.x < 32) {
+      int b = b0 + lane;
+      bool vis = false;
+      if (b < nbricks) {
+        int bz = b % nb, by = (b / nb) % nb, bx = b / nb2;
+        float cx = fmaf(vs, (float)(8 * bx) + 4.0f, org);
+        float cy = fmaf(vs, (float)(8 * by) + 4.0f, org);
+        float cz = fmaf(vs, (float)(8 * bz) + 4.0f, org);
+        vis = true;
 #pragma unroll
-      for (int p = 0; p < 6; ++p) {
-        float e = planes[p].a * X + planes[p].b * Y + planes[p].c * Z + planes[p].d;
-        unsigned out = __ballot_sync(0xffffffffu, e > 0.f) & 0xffu;
-        culled |= (out == 0xffu);
+        for (int q = 0; q < 6; ++q) {
+          const Plane pl = planes[q];
+          float e = fmaf(pl.nx, cx, fmaf(pl.ny, cy, fmaf(pl.nz, cz, pl.d)));
+          float r = hext * (fabsf(pl.nx) + fabsf(pl.ny) + fabsf(pl.nz));
+          vis &= (e - r) <= 0.f;
+        }
       }
+      unsigned m = __ballot_sync(0xffffffffu, vis);
+      if (lane == 0) s_mask = m;
     }
-    if (culled) continue;
-    const int i = cbx * 8 + lx, j = cby * 8 + ly;
-    float X0 = fmaf(S.m[0], (float)lx, fmaf(S.m[1], (float)ly, BX));
-    float Y0 = fmaf(S.m[3], (float)lx, fmaf(S.m[4], (float)ly, BY));
-    float Z0 = fmaf(S.m[6], (float)lx, fmaf(S.m[7], (float)ly, BZ));
-    float tnew[4];
-    unsigned upd = 0;
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-      const float lz = (float)(lz0 + m);
-      tnew[m] = 0.f;
-      float X = fmaf(S.m[2], lz, X0);
-      float Y = fmaf(S.m[5], lz, Y0);
-      float Z = fmaf(S.m[8], lz, Z0);
-      // -Z in [dmin, dmax] (and Z < 0): one unsigned-style range test
-      if (!(-Z - cam.dmin <= dspan && -Z >= cam.dmin)) continue;
-      float rz = __frcp_rn(Z);
-      // roundFloat as floor(x + 0.5): identical except within one FP32 ulp of
-      // a half-integer
-      int pu = __float2int_rd(fmaf(cam.fx * X, rz, cam.cx) + 0.5f);
-      int pv = __float2int_rd(fmaf(cam.fy * Y, rz, cam.cy) + 0.5f);
-      if ((unsigned)(pu - 2) >= uspan || (unsigned)(pv - 2) >= vspan) continue;
-      float D = (float)__ldg(depth + pv * pitch + pu);
-      if (!(D - cam.dmin <= dspan && D >= cam.dmin && D > 0.f)) continue;
-      float2 lm = __ldg(lam + pv * cam.w + pu);
-      // SDF = L - r with L = lambda D, r = |p_c|; decide on squares first
-      float r2 = fmaf(X, X, fmaf(Y, Y, Z * Z));
-      float L = lm.x * D;
-      const float slack = 0.05f + 1e-5f * L;
-      float far = L + T + slack;            // SDF < -T - slack  <=>  r > far
-      if (r2 > far * far) continue;
-      float nearl = L - T - slack;          // SDF >  T + slack  <=>  r < nearl
-      float sn;
-      if (nearl > 0.f && r2 < nearl * nearl) {
-        sn = 1.0f;
-      } else {
-        float2 rr = voxel_range(S, i, j, cbz * 8 + lz0 + m);
-        float2 Lp = two_prod(lm.x, D);
-        Lp.y = __fmaf_rn(lm.y, D, Lp.y);
-        float sdf2 = __fadd_rn(__fsub_rn(Lp.x, rr.x), __fsub_rn(Lp.y, rr.y));
-        if (sdf2 < -T) continue;
-        sn = fminf(sdf2, T) * inv_T;
+    __syncthreads();
+    unsigned mask = s_mask;
+    __syncthreads();
+    // ---- visible bricks, two at a time (one per 128-thread half)
+    int k = 0;
+    while (mask) {
+      int bit = __ffs(mask) - 1;
+      mask &= mask - 1;
+      if ((k++ & 1) != half) continue;
+      const int b = b0 + bit;
+      int bz = bz0 + bit, by = by0, bx = bx0;
+      while (bz >= nb) {
+        bz -= nb;
+        if (++by == nb) { by = 0; ++bx; }
       }
-      upd |= 1u << m;
-      tnew[m] = sn;
-    }
-    if (CENSUS) {
-      my_count += __popc(upd);
-    } else if (upd) {
-      uint4 *p4 = reinterpret_cast<uint4 *>(vol + ((size_t)b << 9)) + t;
-      uint4 wv = *p4;
-      uint32_t w4[4] = {wv.x, wv.y, wv.z, wv.w};
+      // camera-space centre of the brick's voxel (0,0,0), FP64 then rounded:
+      // per-voxel offsets from it stay below 8 voxels, so the FP32 position
+      // error is about one rounding of the brick base.
+      const double fbx = (double)bx, fby = (double)by, fbz = (double)bz;
+      const float BX = (float)fma(S.mb[0], fbx, fma(S.mb[1], fby, fma(S.mb[2], fbz, S.ob[0])));
+      const float BY = (float)fma(S.mb[3], fbx, fma(S.mb[4], fby, fma(S.mb[5], fbz, S.ob[1])));
+      const float BZ = (float)fma(S.mb[6], fbx, fma(S.mb[7], fby, fma(S.mb[8], fbz, S.ob[2])));
+      float X0 = fmaf(S.m[0], (float)lx, fmaf(S.m[1], (float)ly, BX));
+      float Y0 = fmaf(S.m[3], (float)lx, fmaf(S.m[4], (float)ly, BY));
+      float Z0 = fmaf(S.m[6], (float)lx, fmaf(S.m[7], (float)ly, BZ));
+      float tnew[4];
+      unsigned upd = 0;
+      bool near = false;
 #pragma unroll
       for (int m = 0; m < 4; ++m) {
-        if (!(upd & (1u << m))) continue;
-        uint32_t word = w4[m];
-        uint32_t wt = word >> 16;
-        float told = wt ? VoxelCodec<STORAGE>::tsdf(word) : 0.f;
-        // (told w + tsdf') / (w + 1), within a few ulp of the rounded quotient
-        float tn = __fdividef(__fmaf_rn(told, (float)wt, tnew[m]), (float)(wt + 1u));
-        uint32_t wn = min(wt + 1u, (uint32_t)desc.max_weight);
-        w4[m] = VoxelCodec<STORAGE>::pack(tn, wn);
+        const float lz = (float)(lz0 + m);
+        tnew[m] = 0.f;
+        float X = fmaf(S.m[2], lz, X0);
+        float Y = fmaf(S.m[5], lz, Y0);
+        float Z = fmaf(S.m[8], lz, Z0);
+        // -Z in [dmin, dmax] (and Z < 0)
+        if (!(-Z - cam.dmin <= dspan && -Z >= cam.dmin)) continue;
+        float rz = __fdividef(1.0f, Z);
+        // roundFloat as floor(x + 0.5): identical except within FP32
+        // rounding of a half-integer
+        int pu = __float2int_rd(fmaf(cam.fx * X, rz, cxh));
+        int pv = __float2int_rd(fmaf(cam.fy * Y, rz, cyh));
+        if ((unsigned)(pu - 2) >= uspan || (unsigned)(pv - 2) >= vspan) continue;
+        const int pix = pv * cam.w + pu;
+        // uint16 -> float without I2F: 2^23 + d is exact
+        float D = __int_as_float(0x4B000000 | (int)__ldg(depth + pv * pitch + pu)) - 8388608.0f;
+        if (!(D >= dlo && D <= dhi)) continue;
+        float lhi = __ldg(reinterpret_cast<const float *>(lam) + 2 * pix);
+        // SDF = L - r with L = lambda D, r = |p_c|; decide on squares first
+        float r2 = fmaf(X, X, fmaf(Y, Y, Z * Z));
+        float L = lhi * D;
+        const float slack = fmaf(1e-5f, L, 0.05f);
+        float far = L + T + slack;            // SDF < -T - slack  <=>  r > far
+        if (r2 > far * far) continue;
+        float nearl = L - T - slack;          // SDF >  T + slack  <=>  r < nearl
+        float sn = 1.0f;
+        if (!(nearl > 0.f && r2 < nearl * nearl)) {
+          float2 rr = voxel_range(S, bx * 8 + lx, by * 8 + ly, bz * 8 + lz0 + m);
+          float llo = __ldg(reinterpret_cast<const float *>(lam) + 2 * pix + 1);
+          float2 Lp = two_prod(lhi, D);
+          Lp.y = __fmaf_rn(llo, D, Lp.y);
+          float sdf2 = __fadd_rn(__fsub_rn(Lp.x, rr.x), __fsub_rn(Lp.y, rr.y));
+          if (sdf2 < -T) continue;
+          sn = fminf(sdf2, T) * inv_T;
+        }
+        upd |= 1u << m;
+        tnew[m] = sn;
       }
-      *p4 = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+      if (CENSUS) {
+        my_count += __popc(upd);
+      } else if (upd) {
+        uint4 *p4 = reinterpret_cast<uint4 *>(vol + ((size_t)b << 9)) + t;
+        uint4 wv = *p4;
+        uint32_t w4[4] = {wv.x, wv.y, wv.z, wv.w};
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          if (!(upd & (1u << m))) continue;
+          uint32_t word = w4[m];
+          uint32_t wt = word >> 16;
+          // weight as float without I2F (2^23 + w is exact)
+          float wf = __int_as_float(0x4B000000 | (int)wt) - 8388608.0f;
+          float told = wt ? VoxelCodec<STORAGE>::tsdf(word) : 0.f;
+          // (told w + tsdf') / (w + 1), within a few ulp of the rounded quotient
+          float tn = __fdividef(__fmaf_rn(told, wf, tnew[m]), wf + 1.0f);
+          uint32_t wn = min(wt + 1u, (uint32_t)desc.max_weight);
+          w4[m] = VoxelCodec<STORAGE>::pack(tn, wn);
+          near |= (w4[m] & 0xffffu) != VoxelCodec<STORAGE>::kOneBits;
+        }
+        *p4 = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+      }
+      // a warp that wrote a non-saturated voxel flags the brick and its 26
+      // neighbours (idempotent byte stores, lanes 0..26)
+      if (!CENSUS && __any_sync(0xffffffffu, near) && lane < 27) {
+        int ox = lane / 9 - 1, oy = (lane / 3) % 3 - 1, oz = lane % 3 - 1;
+        int qx = bx + ox, qy = by + oy, qz = bz + oz;
+        if ((unsigned)qx < (unsigned)nb && (unsigned)qy < (unsigned)nb && (unsigned)qz < (unsigned)nb)
+          flags[(qx * nb + qy) * nb + qz] = 1;
+      }
     }
   }
   if (CENSUS) {
@@ -224,9 +277,9 @@ of_status_t launch_integrate(const of_volume_desc_t *d, void *vol, const of_came
                              const uint16_t *depth, int pitch, const double *pose,
                              const float *lam, unsigned long long *count, cudaStream_t s) {
   size_t nb = (size_t)(d->resolution / 8);
-  size_t pairs = (nb * nb * nb + 1) / 2;
+  size_t chunks = (nb * nb * nb + kChunk - 1) / kChunk;
   // persistent grid: 8 resident CTAs of 256 threads per SM
-  unsigned blocks = (unsigned)(pairs < (size_t)kSmCount * 8 ? pairs : (size_t)kSmCount * 8);
+  unsigned blocks = (unsigned)(chunks < (size_t)kSmCount * 8 ? chunks : (size_t)kSmCount * 8);
   Cam c = make_cam(*cam);
   if (d->storage == OF_TSDF_I16)
     k_integrate<OF_TSDF_I16, CENSUS><<<blocks, 256, 0, s>>>(

@@ -139,20 +139,51 @@ __global__ void __launch_bounds__(256) k_raycast(const uint32_t *__restrict__ vo
   if (t0 < t1) {
     const float min_step = rp.min_step_vox * vs;
     const float far_k = rp.far_step_frac * T;
+    const uint8_t *__restrict__ flags = brick_flags((void *)vol, n);
+    const float inv_vs = S.inv_vs;
+    // brick-region bounds: the cell base floor(g) of a position lies in brick
+    // b along an axis for g in [8b, 8b + 8), i.e. p in
+    // [org + vs (8b + 0.5), org + vs (8b + 8.5)).
+    const float bvs = 8.0f * vs;
+    const float eps = 0.01f * vs;
     float t = t0;
-    float fp = trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, fmaf(t, dir.x, ox), fmaf(t, dir.y, oy),
-                                  fmaf(t, dir.z, oz));
+    float fp = 1.0f;
+    bool sampled = false;
     for (int it = 0; it < (1 << 16); ++it) {
+      const float px = fmaf(t, dir.x, ox), py = fmaf(t, dir.y, oy), pz = fmaf(t, dir.z, oz);
+      int bi = min(max(__float2int_rd(fmaf(px - org, inv_vs, -0.5f)), 0), n - 2) >> 3;
+      int bj = min(max(__float2int_rd(fmaf(py - org, inv_vs, -0.5f)), 0), n - 2) >> 3;
+      int bk = min(max(__float2int_rd(fmaf(pz - org, inv_vs, -0.5f)), 0), n - 2) >> 3;
+      if (!__ldg(flags + (bi * nb + bj) * nb + bk)) {
+        // every sample with its cell base in this brick reads exactly +1:
+        // jump just past the brick region; the landing cell is +1 as well
+        float ex = (dir.x > 0.f ? fmaf(bvs, (float)(bi + 1), org + 0.5f * vs) : fmaf(bvs, (float)bi, org + 0.5f * vs)) - ox;
+        float ey = (dir.y > 0.f ? fmaf(bvs, (float)(bj + 1), org + 0.5f * vs) : fmaf(bvs, (float)bj, org + 0.5f * vs)) - oy;
+        float ez = (dir.z > 0.f ? fmaf(bvs, (float)(bk + 1), org + 0.5f * vs) : fmaf(bvs, (float)bk, org + 0.5f * vs)) - oz;
+        float te = 1e30f;
+        if (fabsf(dir.x) > 1e-12f) te = fminf(te, ex / dir.x);
+        if (fabsf(dir.y) > 1e-12f) te = fminf(te, ey / dir.y);
+        if (fabsf(dir.z) > 1e-12f) te = fminf(te, ez / dir.z);
+        t = fmaxf(te, t) + eps;
+        fp = 1.0f;
+        sampled = true;
+        if (t > t1) break;
+        continue;
+      }
+      if (!sampled) {
+        fp = trilinear<STORAGE>(vol, n, nb, org, inv_vs, px, py, pz);
+        sampled = true;
+      }
       float step = fp > 0.f ? fmaxf(min_step, far_k * fp) : min_step;
       float tn = t + step;
       if (tn > t1) break;
-      float fn = trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, fmaf(tn, dir.x, ox),
+      float fn = trilinear<STORAGE>(vol, n, nb, org, inv_vs, fmaf(tn, dir.x, ox),
                                     fmaf(tn, dir.y, oy), fmaf(tn, dir.z, oz));
       if (fp > 0.f && fn <= 0.f) {
         float ta = t, fa = fp, tb = tn, fb = fn;
         for (int r = 0; r < rp.refine_iters; ++r) {
           float tm = fmaf(tb - ta, fa / (fa - fb), ta);
-          float fm = trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, fmaf(tm, dir.x, ox),
+          float fm = trilinear<STORAGE>(vol, n, nb, org, inv_vs, fmaf(tm, dir.x, ox),
                                         fmaf(tm, dir.y, oy), fmaf(tm, dir.z, oz));
           if (fm > 0.f) { ta = tm; fa = fm; } else { tb = tm; fb = fm; }
         }
