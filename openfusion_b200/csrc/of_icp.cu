@@ -310,6 +310,104 @@ __device__ __forceinline__ void grid_barrier(IcpWorkspace *ws, unsigned nblocks)
   __syncthreads();
 }
 
+__device__ __forceinline__ double shfl_d(double v, int src) {
+  return __shfl_sync(0xffffffffu, v, src);
+}
+
+// Warp-parallel FP64 solve of the 6x6 normal equations (21 upper entries and
+// 6 right-hand sides in tot[0..26], inliers in tot[28]) and the SE(3) update
+// of P (row-major 4x4, shared memory). All 32 lanes of one warp call it; lane
+// i < 6 owns row i. LDL^T factorisation (one reciprocal per column, no square
+// roots; the pivots d_j equal the squared Cholesky pivots), forward and back
+// substitution by shuffles, the three sincos in three lanes, and the 4x4
+// product with one entry per lane. Returns the warp-uniform success flag;
+// *minpiv gets min d_j / max H_ii. Same singularity rule as chol_solve6.
+__device__ bool warp_solve_update(const float *tot, double *P, double *minpiv) {
+  const int lane = threadIdx.x & 31;
+  const int row = lane < 6 ? lane : 5;
+  double h[6];
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    int a = row < j ? row : j, b = row < j ? j : row;
+    h[j] = (double)tot[a * 6 - a * (a - 1) / 2 + (b - a)];
+  }
+  double dmax = 0.0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) dmax = fmax(dmax, (double)tot[i * 6 - i * (i - 1) / 2]);
+  bool ok = tot[28] >= 6.f && dmax > 0.0 && isfinite(dmax);
+  double L[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // row `row` of unit-lower L
+  double d[6], dinv[6];
+  double mp = 1e300;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    // pivot d_j = H_jj - sum_k L_jk^2 d_k (lane j), broadcast
+    double s = h[j];
+#pragma unroll
+    for (int k = 0; k < j; ++k) s -= L[k] * L[k] * d[k];
+    double dj = shfl_d(s, j);
+    mp = fmin(mp, dj / dmax);
+    ok = ok && (dj > 1e-12 * dmax) && isfinite(dj);
+    d[j] = dj;
+    dinv[j] = 1.0 / dj;
+    // L_ij = (H_ij - sum_k L_ik L_jk d_k) / d_j for rows i > j
+    double Lj[6];
+#pragma unroll
+    for (int k = 0; k < j; ++k) Lj[k] = shfl_d(L[k], j);
+    double t = h[j];
+#pragma unroll
+    for (int k = 0; k < j; ++k) t -= L[k] * Lj[k] * d[k];
+    if (row > j) L[j] = t * dinv[j];
+    if (row == j) L[j] = 1.0;
+  }
+  *minpiv = ok ? mp : fmin(mp, 0.0);
+  if (!ok) return false;
+  // forward: L z = g (unit diagonal), then y = z / d
+  double z[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    double t = (double)tot[21 + i];
+#pragma unroll
+    for (int k = 0; k < i; ++k) t -= L[k] * z[k];
+    z[i] = shfl_d(t, i);
+  }
+  // back: L^T x = z / d; the sum over rows k > i gathers L_ki from lane k
+  double x[6];
+#pragma unroll
+  for (int i = 5; i >= 0; --i) {
+    double c = 0.0;
+    if (lane > i && lane < 6) {
+#pragma unroll
+      for (int k = i + 1; k < 6; ++k)
+        if (lane == k) c = L[i] * x[k];
+    }
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    c = shfl_d(c, 0) ;
+    x[i] = z[i] * dinv[i] - c;
+  }
+  // rotation part negated (ICP.cpp:162-168): alpha, beta, gamma = -x[0..2]
+  double sv = 0.0, cv = 1.0;
+  if (lane < 3) sincos(-x[lane], &sv, &cv);
+  const double sa = shfl_d(sv, 0), ca = shfl_d(cv, 0);
+  const double sb = shfl_d(sv, 1), cb = shfl_d(cv, 1);
+  const double sg = shfl_d(sv, 2), cg = shfl_d(cv, 2);
+  // dT = [Rz(g) Ry(b) Rx(a) | t] (ICP.cu:274-290); lane l < 16 forms entry
+  // (l/4, l%4) of dT P
+  const int r = (lane >> 2) & 3, c = lane & 3;
+  double D[4];
+  if (r == 0) { D[0] = cg * cb; D[1] = -sg * ca + cg * sb * sa; D[2] = sg * sa + cg * sb * ca; D[3] = x[3]; }
+  else if (r == 1) { D[0] = sg * cb; D[1] = cg * ca + sg * sb * sa; D[2] = -cg * sa + sg * sb * ca; D[3] = x[4]; }
+  else if (r == 2) { D[0] = -sb; D[1] = cb * sa; D[2] = cb * ca; D[3] = x[5]; }
+  else { D[0] = 0.0; D[1] = 0.0; D[2] = 0.0; D[3] = 1.0; }
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) acc += D[k] * P[4 * k + c];
+  __syncwarp();
+  if (lane < 16) P[lane] = acc;
+  __syncwarp();
+  return true;
+}
+
 // The whole multi-level ICP of one frame in one cooperative launch. Per
 // iteration: every block accumulates its pixels' rows (tree sums), writes 29
 // partials, meets the others at one grid barrier, then reduces all blocks'
@@ -435,22 +533,18 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         s_tot[threadIdx.x] = y[0];
       }
       __syncthreads();
-      if (threadIdx.x == 0) {
-        double up[21], g[6], xs[6], minpiv = 0.0;
-        for (int v = 0; v < 21; ++v) up[v] = (double)s_tot[v];
-        for (int v = 0; v < 6; ++v) g[v] = (double)s_tot[21 + v];
-        int inliers = (int)s_tot[28];
-        bool ok = inliers >= 6 && chol_solve6(up, g, xs, &minpiv);
-        s_its += 1;
-        s_inl = inliers;
-        s_res = (double)s_tot[27];
-        s_piv = minpiv;
-        if (ok) {
-          double xo[6] = {-xs[0], -xs[1], -xs[2], xs[3], xs[4], xs[5]};
-          compose_increment(xo, s_pose);
-        } else {
-          for (int i = 0; i < 16; ++i) s_pose[i] = ws->pose_init[i];
-          s_stop = 1;
+      if (warp == 0) {
+        double minpiv = 0.0;
+        bool ok = warp_solve_update(s_tot, s_pose, &minpiv);
+        if (lane == 0) {
+          s_its += 1;
+          s_inl = (int)s_tot[28];
+          s_res = (double)s_tot[27];
+          s_piv = minpiv;
+          if (!ok) {
+            for (int i = 0; i < 16; ++i) s_pose[i] = ws->pose_init[i];
+            s_stop = 1;
+          }
         }
       }
       __syncthreads();

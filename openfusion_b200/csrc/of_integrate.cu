@@ -58,21 +58,15 @@ __device__ void make_setup(const double *P, const of_volume_desc_t &d, Integrate
   S.vs_lo = (float)(vs - (double)S.vs_hi);
 }
 
-// |p_w - c| for voxel index (i, j, k) as a float pair.
-__device__ __forceinline__ float2 voxel_range(const IntegrateSetup &S, int i, int j, int k) {
-  float2 acc = make_float2(0.f, 0.f);
-  const int idx[3] = {i, j, k};
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    float fi = (float)idx[a];
-    float2 p = two_prod(fi, S.vs_hi);
-    p.y = __fmaf_rn(fi, S.vs_lo, p.y);
-    float2 q = two_sum(p.x, S.oc_hi[a]);
-    float lo = __fadd_rn(__fadd_rn(p.y, q.y), S.oc_lo[a]);
-    float2 dd = two_sum(q.x, lo);
-    acc = df_add(acc, df_sq(dd.x, dd.y));
-  }
-  return df_sqrt(acc);
+// (p_w - c)^2 along axis a for voxel index i, as a float pair.
+__device__ __forceinline__ float2 axis_sq(const IntegrateSetup &S, int a, int i) {
+  float fi = (float)i;
+  float2 p = two_prod(fi, S.vs_hi);
+  p.y = __fmaf_rn(fi, S.vs_lo, p.y);
+  float2 q = two_sum(p.x, S.oc_hi[a]);
+  float lo = __fadd_rn(__fadd_rn(p.y, q.y), S.oc_lo[a]);
+  float2 dd = two_sum(q.x, lo);
+  return df_sq(dd.x, dd.y);
 }
 
 // Frustum plane in world space: inside <=> n . p + d <= 0.
@@ -192,46 +186,75 @@ __global__ void __launch_bounds__(256) k_integrate(uint32_t *__restrict__ vol, o
       float tnew[4];
       unsigned upd = 0;
       bool near = false;
+      // phase 1: project the four voxels; phase 2: issue every gather before
+      // any result is used; phase 3: decide
+      float Xv[4], Yv[4], Zv[4];
+      int pix[4], dix[4];
+      unsigned inb = 0;
 #pragma unroll
       for (int m = 0; m < 4; ++m) {
         const float lz = (float)(lz0 + m);
-        tnew[m] = 0.f;
         float X = fmaf(S.m[2], lz, X0);
         float Y = fmaf(S.m[5], lz, Y0);
         float Z = fmaf(S.m[8], lz, Z0);
-        // -Z in [dmin, dmax] (and Z < 0)
-        if (!(-Z - cam.dmin <= dspan && -Z >= cam.dmin)) continue;
+        Xv[m] = X; Yv[m] = Y; Zv[m] = Z;
         float rz = __fdividef(1.0f, Z);
         // roundFloat as floor(x + 0.5): identical except within FP32
         // rounding of a half-integer
         int pu = __float2int_rd(fmaf(cam.fx * X, rz, cxh));
         int pv = __float2int_rd(fmaf(cam.fy * Y, rz, cyh));
-        if ((unsigned)(pu - 2) >= uspan || (unsigned)(pv - 2) >= vspan) continue;
-        const int pix = pv * cam.w + pu;
-        // uint16 -> float without I2F: 2^23 + d is exact
-        float D = __int_as_float(0x4B000000 | (int)__ldg(depth + pv * pitch + pu)) - 8388608.0f;
-        if (!(D >= dlo && D <= dhi)) continue;
-        float lhi = __ldg(reinterpret_cast<const float *>(lam) + 2 * pix);
-        // SDF = L - r with L = lambda D, r = |p_c|; decide on squares first
-        float r2 = fmaf(X, X, fmaf(Y, Y, Z * Z));
-        float L = lhi * D;
-        const float slack = fmaf(1e-5f, L, 0.05f);
-        float far = L + T + slack;            // SDF < -T - slack  <=>  r > far
-        if (r2 > far * far) continue;
-        float nearl = L - T - slack;          // SDF >  T + slack  <=>  r < nearl
-        float sn = 1.0f;
-        if (!(nearl > 0.f && r2 < nearl * nearl)) {
-          float2 rr = voxel_range(S, bx * 8 + lx, by * 8 + ly, bz * 8 + lz0 + m);
-          float llo = __ldg(reinterpret_cast<const float *>(lam) + 2 * pix + 1);
-          float2 Lp = two_prod(lhi, D);
-          Lp.y = __fmaf_rn(llo, D, Lp.y);
-          float sdf2 = __fadd_rn(__fsub_rn(Lp.x, rr.x), __fsub_rn(Lp.y, rr.y));
-          if (sdf2 < -T) continue;
-          sn = fminf(sdf2, T) * inv_T;
-        }
-        upd |= 1u << m;
-        tnew[m] = sn;
+        // -Z in [dmin, dmax] (and Z < 0), pixel outside the 2-pixel border
+        bool ok = (-Z - cam.dmin <= dspan) && (-Z >= cam.dmin) &&
+                  (unsigned)(pu - 2) < uspan && (unsigned)(pv - 2) < vspan;
+        inb |= ok ? (1u << m) : 0u;
+        pix[m] = ok ? pv * cam.w + pu : 0;
+        dix[m] = ok ? pv * pitch + pu : 0;
       }
+      if (!inb) goto brick_done;
+      {
+        float Dv[4], Lh[4];
+        bool have_xy = false;
+        float2 sxy = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          // uint16 -> float without I2F: 2^23 + d is exact
+          Dv[m] = __int_as_float(0x4B000000 | (int)__ldg(depth + dix[m])) - 8388608.0f;
+          Lh[m] = __ldg(reinterpret_cast<const float *>(lam) + 2 * pix[m]);
+        }
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          tnew[m] = 0.f;
+          const float D = Dv[m];
+          if (!((inb >> m) & 1u) || !(D >= dlo && D <= dhi)) continue;
+          const float X = Xv[m], Y = Yv[m], Z = Zv[m];
+          // SDF = L - r with L = lambda D, r = |p_c|; decide on squares first
+          float r2 = fmaf(X, X, fmaf(Y, Y, Z * Z));
+          float L = Lh[m] * D;
+          const float slack = fmaf(1e-5f, L, 0.05f);
+          float far = L + T + slack;            // SDF < -T - slack  <=>  r > far
+          if (r2 > far * far) continue;
+          float nearl = L - T - slack;          // SDF >  T + slack  <=>  r < nearl
+          float sn = 1.0f;
+          if (!(nearl > 0.f && r2 < nearl * nearl)) {
+            // |p_w - c| as a float pair: the x and y terms are the thread's
+            // constants within the brick, computed on first use
+            if (!have_xy) {
+              sxy = df_add(axis_sq(S, 0, bx * 8 + lx), axis_sq(S, 1, by * 8 + ly));
+              have_xy = true;
+            }
+            float2 rr = df_sqrt(df_add(sxy, axis_sq(S, 2, bz * 8 + lz0 + m)));
+            float llo = __ldg(reinterpret_cast<const float *>(lam) + 2 * pix[m] + 1);
+            float2 Lp = two_prod(Lh[m], D);
+            Lp.y = __fmaf_rn(llo, D, Lp.y);
+            float sdf2 = __fadd_rn(__fsub_rn(Lp.x, rr.x), __fsub_rn(Lp.y, rr.y));
+            if (sdf2 < -T) continue;
+            sn = fminf(sdf2, T) * inv_T;
+          }
+          upd |= 1u << m;
+          tnew[m] = sn;
+        }
+      }
+    brick_done:
       if (CENSUS) {
         my_count += __popc(upd);
       } else if (upd) {

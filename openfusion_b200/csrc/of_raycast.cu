@@ -9,7 +9,8 @@
 // steps and stops at the first tsdf <= 0 (:152-188), this kernel follows the
 // KinectFusion method the reference left commented out (:246-351): trilinear
 // samples, steps of max(min_step, far_frac * tsdf * trunc), a + to - zero
-// crossing refined by regula falsi on the trilinear field, and the normal as
+// crossing whose bracket is first narrowed to one minimum step and then refined
+// by Illinois regula falsi on the trilinear field, and the normal as
 // the central-difference gradient of trilinear samples one voxel apart. The
 // march runs between the min and max depth along the ray.
 #include "of_common.cuh"
@@ -181,11 +182,29 @@ __global__ void __launch_bounds__(256) k_raycast(const uint32_t *__restrict__ vo
                                     fmaf(tn, dir.y, oy), fmaf(tn, dir.z, oz));
       if (fp > 0.f && fn <= 0.f) {
         float ta = t, fa = fp, tb = tn, fb = fn;
+        // shrink a long bracket with minimum steps from its positive end, so
+        // the refined root does not depend on where the march samples fell
+        while (tb - ta > min_step * 1.0001f) {
+          float tm = ta + min_step;
+          float fm = trilinear<STORAGE>(vol, n, nb, org, inv_vs, fmaf(tm, dir.x, ox),
+                                        fmaf(tm, dir.y, oy), fmaf(tm, dir.z, oz));
+          if (fm > 0.f) { ta = tm; fa = fm; } else { tb = tm; fb = fm; break; }
+        }
+        // Illinois regula falsi on the trilinear field
+        int side = 0;
         for (int r = 0; r < rp.refine_iters; ++r) {
           float tm = fmaf(tb - ta, fa / (fa - fb), ta);
           float fm = trilinear<STORAGE>(vol, n, nb, org, inv_vs, fmaf(tm, dir.x, ox),
                                         fmaf(tm, dir.y, oy), fmaf(tm, dir.z, oz));
-          if (fm > 0.f) { ta = tm; fa = fm; } else { tb = tm; fb = fm; }
+          if (fm > 0.f) {
+            ta = tm; fa = fm;
+            if (side == 1) fb *= 0.5f;
+            side = 1;
+          } else {
+            tb = tm; fb = fm;
+            if (side == -1) fa *= 0.5f;
+            side = -1;
+          }
         }
         ts = fmaf(tb - ta, fa / (fa - fb), ta);
         hit = true;

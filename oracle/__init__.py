@@ -64,7 +64,7 @@ class Oracle:
         L.ora_pyramid_elems.restype = C.c_int64
         L.ora_integrate.argtypes = [C.POINTER(Vol), P, C.POINTER(Cam), P, P, P]
         L.ora_integrate.restype = C.c_int64
-        L.ora_raycast.argtypes = [C.POINTER(Vol), P, C.POINTER(Cam), C.POINTER(Params), P, P, P]
+        L.ora_raycast.argtypes = [C.POINTER(Vol), P, P, C.POINTER(Cam), C.POINTER(Params), P, P, P]
         L.ora_model_down.argtypes = [P, C.c_int32, P, C.c_int32, C.c_int32]
         L.ora_icp_system.argtypes = [C.POINTER(Cam), P, C.c_int32, C.c_int32, P, P, C.c_double,
                                      C.c_double, P, P]
@@ -173,11 +173,14 @@ class Oracle:
                                    None if am is None else am.ctypes.data)
         return n, am
 
-    def raycast(self, cfg, words: np.ndarray, pose: np.ndarray, ambig: bool = False):
+    def raycast(self, cfg, words: np.ndarray, pose: np.ndarray, ambig: bool = False,
+                flags: np.ndarray | None = None):
         P_ = np.ascontiguousarray(pose, np.float64)
         pts = np.zeros((cfg.height, cfg.width, 8), self.real)
         am = np.zeros((cfg.height, cfg.width), np.uint8) if ambig else None
-        self.lib.ora_raycast(C.byref(self.vol(cfg)), words.ctypes.data, C.byref(self.cam(cfg)),
+        fl = None if flags is None else np.ascontiguousarray(flags, np.uint8)
+        self.lib.ora_raycast(C.byref(self.vol(cfg)), words.ctypes.data,
+                             None if fl is None else fl.ctypes.data, C.byref(self.cam(cfg)),
                              C.byref(self.params(cfg)), P_.ctypes.data, pts.ctypes.data,
                              None if am is None else am.ctypes.data)
         return pts, am

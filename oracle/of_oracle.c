@@ -326,11 +326,17 @@ static R trilinear(const vol_view *V, R px, R py, R pz) {
  * sampling follows KinectFusion s3.4 (the trilinear zero-crossing the
  * reference left disabled, :170-187, :246-351): trilinear tsdf samples, step
  * max(min_step, far_frac * f * trunc) for f > 0 else min_step, surface at a
- * + -> - crossing refined by `refine_iters` regula-falsi steps, - -> + ends
+ * + -> - crossing whose bracket is narrowed to one min_step by stepping from
+ * its positive end, then refined by `refine_iters` Illinois regula-falsi
+ * steps, - -> + ends
  * the ray; normal = normalised central differences of trilinear samples one
- * voxel apart; the march is limited to [dmin, dmax] depth. */
-void ora_raycast(const ora_vol *v, const uint32_t *words, const ora_cam *c, const ora_params *p,
-                 const double *P, R *pts, uint8_t *ambig) {
+ * voxel apart; the march is limited to [dmin, dmax] depth. With `flags` (one
+ * byte per 8^3 brick, clear = the brick and its 26 neighbours hold only +1
+ * voxels) the march jumps over clear bricks: empty-space skipping, as the
+ * CUDA kernel does; it cannot change which crossing is found, only where the
+ * samples before it fall. */
+void ora_raycast(const ora_vol *v, const uint32_t *words, const uint8_t *flags, const ora_cam *c,
+                 const ora_params *p, const double *P, R *pts, uint8_t *ambig) {
   const int n = v->n;
   const double vs = v->size / n;
   vol_view V = {words, n, v->storage, -0.5 * v->size, 1.0 / vs};
@@ -365,8 +371,44 @@ void ora_raycast(const ora_vol *v, const uint32_t *words, const ora_cam *c, cons
       R ts = 0;
       if (t0 < t1) {
         R t = t0;
-        R fp = trilinear(&V, o[0] + t * dir[0], o[1] + t * dir[1], o[2] + t * dir[2]);
+        R fp = 1;
+        int sampled = 0;
         for (int it = 0; it < (1 << 16); ++it) {
+          R px = o[0] + t * dir[0], py = o[1] + t * dir[1], pz = o[2] + t * dir[2];
+          if (flags) {
+            /* empty-space skip: a brick whose flag is clear holds, with its
+             * 26 neighbours, only +1 voxels; every sample whose cell base is
+             * in it reads +1, so the march jumps past its region */
+            int bi[3];
+            R pp[3] = {px, py, pz};
+            for (int a = 0; a < 3; ++a) {
+              int q = (int)floor(((double)pp[a] - V.org) * V.inv_vs - 0.5);
+              if (q < 0) q = 0;
+              if (q > n - 2) q = n - 2;
+              bi[a] = q >> 3;
+            }
+            int nbk = n / 8;
+            if (!flags[((size_t)bi[0] * nbk + bi[1]) * nbk + bi[2]]) {
+              R te = (R)1e30;
+              for (int a = 0; a < 3; ++a) {
+                if (fabs((double)dir[a]) <= 1e-12) continue;
+                double edge = dir[a] > 0 ? V.org + vs * (8.0 * (bi[a] + 1) + 0.5)
+                                         : V.org + vs * (8.0 * bi[a] + 0.5);
+                R ta = (R)((edge - (double)o[a]) / (double)dir[a]);
+                if (ta < te) te = ta;
+              }
+              t = (te > t ? te : t) + (R)(0.01 * vs);
+              fp = 1;
+              sampled = 1;
+              if (ambig && fabs((double)(t - t1)) < 0.05) amb = 1;
+              if (t > t1) break;
+              continue;
+            }
+          }
+          if (!sampled) {
+            fp = trilinear(&V, px, py, pz);
+            sampled = 1;
+          }
           R step = fp > 0 ? (far_k * fp > min_step ? far_k * fp : min_step) : min_step;
           R tn = t + step;
           if (ambig && fabs((double)(tn - t1)) < 0.05) amb = 1;
@@ -375,10 +417,26 @@ void ora_raycast(const ora_vol *v, const uint32_t *words, const ora_cam *c, cons
           if (ambig && fabs((double)fn) < 2e-4) amb = 1;
           if (fp > 0 && fn <= 0) {
             R ta = t, fa = fp, tb = tn, fb = fn;
+            /* narrow a long bracket with minimum steps from its positive end */
+            while (tb - ta > min_step * (R)1.0001) {
+              R tm = ta + min_step;
+              R fm = trilinear(&V, o[0] + tm * dir[0], o[1] + tm * dir[1], o[2] + tm * dir[2]);
+              if (fm > 0) { ta = tm; fa = fm; } else { tb = tm; fb = fm; break; }
+            }
+            /* Illinois regula falsi (Dowell & Jarratt 1971) */
+            int side = 0;
             for (int r = 0; r < p->refine_iters; ++r) {
               R tm = ta + (tb - ta) * (fa / (fa - fb));
               R fm = trilinear(&V, o[0] + tm * dir[0], o[1] + tm * dir[1], o[2] + tm * dir[2]);
-              if (fm > 0) { ta = tm; fa = fm; } else { tb = tm; fb = fm; }
+              if (fm > 0) {
+                ta = tm; fa = fm;
+                if (side == 1) fb *= (R)0.5;
+                side = 1;
+              } else {
+                tb = tm; fb = fm;
+                if (side == -1) fa *= (R)0.5;
+                side = -1;
+              }
             }
             ts = ta + (tb - ta) * (fa / (fa - fb));
             hit = 1;
@@ -685,7 +743,7 @@ int32_t ora_tracker_process(ora_tracker *t, const uint16_t *depth) {
   const R *md[4], *mp[4];
   ora_cam lc[4];
   pyramid_levels(&t->cam, t->par.levels, t->model, md, mp, lc);
-  ora_raycast(&t->vol, t->words, &t->cam, &t->par, t->pose, (R *)mp[0], NULL);
+  ora_raycast(&t->vol, t->words, NULL, &t->cam, &t->par, t->pose, (R *)mp[0], NULL);
   for (int l = 1; l < t->par.levels; ++l)
     ora_model_down(mp[l - 1], lc[l - 1].w, (R *)mp[l], lc[l].w, lc[l].h);
   t->frames += 1;

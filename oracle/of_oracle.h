@@ -76,10 +76,11 @@ int64_t ora_pyramid_elems(const ora_cam *c, int32_t levels);
 int64_t ora_integrate(const ora_vol *v, uint32_t *words, const ora_cam *c, const uint16_t *depth,
                       const double *pose, uint8_t *ambig);
 
-/* raycast; pts is [h*w][8] world vertex/normal; ambig (may be NULL) flags
- * pixels whose sign or range decisions are within rounding of a boundary. */
-void ora_raycast(const ora_vol *v, const uint32_t *words, const ora_cam *c, const ora_params *p,
-                 const double *pose, ora_real *pts, uint8_t *ambig);
+/* raycast; pts is [h*w][8] world vertex/normal; flags (may be NULL): one
+ * byte per brick for empty-space skipping; ambig (may be NULL) flags pixels
+ * whose sign or range decisions are within rounding of a boundary. */
+void ora_raycast(const ora_vol *v, const uint32_t *words, const uint8_t *flags, const ora_cam *c,
+                 const ora_params *p, const double *pose, ora_real *pts, uint8_t *ambig);
 /* model level l+1 from level l by subsampling (2x, 2y) */
 void ora_model_down(const ora_real *src, int32_t sw, ora_real *dst, int32_t dw, int32_t dh);
 

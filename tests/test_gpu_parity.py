@@ -140,9 +140,18 @@ def test_raycast_matches_oracle(of, ora, cuda, name, res):
     pose = seq.poses[3]
     model = of.raycast(cfg, vol, dev_pose(pose, cuda))
     torch.cuda.synchronize()
-    q, w = of.volume_to_linear(cfg, vol.cpu().numpy())
+    host = vol.cpu().numpy()
+    q, w = of.volume_to_linear(cfg, host)
     words = (q.astype(np.uint32) | (w.astype(np.uint32) << 16)).reshape(-1).copy()
-    opts, amb = ora.raycast(cfg, words, pose, ambig=True)
+    nb = cfg.resolution // 8
+    flags = host.view(np.uint8)[4 * cfg.resolution ** 3:][: nb ** 3].copy()
+    opts, amb = ora.raycast(cfg, words, pose, ambig=True, flags=flags)
+    # the skip is exact: the oracle without it finds the same surface
+    plain, _ = ora.raycast(cfg, words, pose)
+    hp = (plain[..., 3] > 0) & (opts[..., 3] > 0)
+    assert ((plain[..., 3] > 0) != (opts[..., 3] > 0)).mean() < 5e-3
+    dp = np.linalg.norm(plain[..., :3][hp] - opts[..., :3][hp], axis=-1)
+    assert np.quantile(dp, 0.99) < 0.1
     gv, gn = (t.cpu().numpy().astype(np.float64) for t in of.unpack_points(cfg, model, 0))
     ok = amb == 0
     hit_g, hit_o = gv[..., 3] > 0, opts[..., 3] > 0
