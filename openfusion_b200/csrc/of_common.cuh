@@ -12,7 +12,7 @@
 #include <stdint.h>
 #include <math.h>
 
-#include "../../include/openfusion_b200.h"
+#include "openfusion_b200.h"
 
 #define OF_CUDA_TRY(expr)                                   \
   do {                                                      \

@@ -474,29 +474,37 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         acc[27] = fmaf(b, b, acc[27]);
         acc[28] += 1.f;
       }
-      // pairwise: warp shuffle tree, then a tree over the block's warps
+      // pairwise sums: a recursive-halving exchange across the warp (lanes
+      // trade half of their remaining values each step, 31 shuffles for 32
+      // values) leaves lane v with the warp's sum of value v; then a tree
+      // over the block's warps.
+      {
+        float r[32];
 #pragma unroll
-      for (int v = 0; v < kVals; ++v) {
-        float x = acc[v];
+        for (int v = 0; v < 32; ++v) r[v] = v < kVals ? acc[v] : 0.f;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        if (lane == 0) s_red[warp][v] = x;
+        for (int sft = 16; sft >= 1; sft >>= 1) {
+          const bool upper = (lane & sft) != 0;
+#pragma unroll
+          for (int i = 0; i < sft; ++i) {
+            float send = upper ? r[i] : r[i + sft];
+            float keep = upper ? r[i + sft] : r[i];
+            r[i] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
+          }
+        }
+        s_red[warp][lane] = r[0];
       }
       __syncthreads();
       const int buf = iter_global & 1;
       if (warp == 0) {
-        float x = 0.f;
-        if (lane < kVals) {
-          float y[kWarps];
+        float y[kWarps];
 #pragma unroll
-          for (int w = 0; w < kWarps; ++w) y[w] = s_red[w][lane];
+        for (int w = 0; w < kWarps; ++w) y[w] = s_red[w][lane];
 #pragma unroll
-          for (int span = 1; span < kWarps; span *= 2)
+        for (int span = 1; span < kWarps; span *= 2)
 #pragma unroll
-            for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
-          x = y[0];
-        }
-        ws->fused_partials[buf][blockIdx.x][lane] = x;
+          for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
+        ws->fused_partials[buf][blockIdx.x][lane] = lane < kVals ? y[0] : 0.f;
       }
       grid_barrier(ws, gridDim.x);
       // every block: Kahan over its strided share of the blocks' partials,

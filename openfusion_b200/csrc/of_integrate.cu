@@ -97,17 +97,18 @@ __device__ void make_planes(const double *P, const Cam &cam, Plane *pl) {
   }
 }
 
-constexpr int kChunk = 32;  // bricks tested by one warp ballot
+constexpr int kChunk = 32;  // bricks tested per batch (one warp ballot)
 
 template <int STORAGE, bool CENSUS>
-__global__ void __launch_bounds__(256) k_integrate(uint32_t *__restrict__ vol, of_volume_desc_t desc,
+__global__ void __launch_bounds__(256, 4) k_integrate(uint32_t *__restrict__ vol, of_volume_desc_t desc,
                                                    Cam cam, const uint16_t *__restrict__ depth,
                                                    int pitch, const double *__restrict__ pose,
                                                    const float2 *__restrict__ lam,
                                                    unsigned long long *count) {
   __shared__ IntegrateSetup S;
   __shared__ Plane planes[6];
-  __shared__ unsigned int s_mask;
+  __shared__ int s_list[kChunk][4];  // visible bricks of a batch: b, bx, by, bz
+  __shared__ int s_nvis;
   __shared__ unsigned int s_count;
   if (threadIdx.x == 0) {
     make_setup(pose, desc, S);
@@ -117,7 +118,6 @@ __global__ void __launch_bounds__(256) k_integrate(uint32_t *__restrict__ vol, o
   __syncthreads();
   const int nb = desc.resolution >> 3;
   const int nbricks = nb * nb * nb;
-  const int nchunks = (nbricks + kChunk - 1) / kChunk;
   const int half = threadIdx.x >> 7;
   const int t = threadIdx.x & 127;
   const int lane = threadIdx.x & 31;
@@ -133,16 +133,19 @@ __global__ void __launch_bounds__(256) k_integrate(uint32_t *__restrict__ vol, o
   const float dlo = fmaxf(cam.dmin, 0.5f), dhi = cam.dmax;
   const int nb2 = nb * nb;
   uint8_t *flags = brick_flags(vol, desc.resolution);
-  for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
-    const int b0 = chunk * kChunk;
-    // brick coordinates of the chunk's first brick (one division per chunk)
-    const int bz0 = b0 % nb, by0 = (b0 / nb) % nb, bx0 = b0 / nb2;
-    // ---- visibility of 32 bricks: one lane per brick, world-space box vs planes
+  // Bricks are dealt round-robin (brick b goes to CTA b mod grid), so every
+  // CTA gets a spatially spread, statistically equal share of the frustum.
+  // Per batch, warp 0 tests 32 of the CTA's bricks (one lane each) and
+  // compacts the visible ones into a shared list; the two 128-thread halves
+  // then take list entries alternately.
+  const int G = gridDim.x;
+  for (int q0 = 0; blockIdx.x + q0 * G < nbricks; q0 += kChunk) {
     if (threadIdx.x < 32) {
-      int b = b0 + lane;
+      int b = blockIdx.x + (q0 + lane) * G;
       bool vis = false;
+      int bx = 0, by = 0, bz = 0;
       if (b < nbricks) {
-        int bz = b % nb, by = (b / nb) % nb, bx = b / nb2;
+        bz = b % nb; by = (b / nb) % nb; bx = b / nb2;
         float cx = fmaf(vs, (float)(8 * bx) + 4.0f, org);
         float cy = fmaf(vs, (float)(8 * by) + 4.0f, org);
         float cz = fmaf(vs, (float)(8 * bz) + 4.0f, org);
@@ -156,23 +159,16 @@ __global__ void __launch_bounds__(256) k_integrate(uint32_t *__restrict__ vol, o
         }
       }
       unsigned m = __ballot_sync(0xffffffffu, vis);
-      if (lane == 0) s_mask = m;
+      if (vis) {
+        int slot = __popc(m & ((1u << lane) - 1u));
+        s_list[slot][0] = b; s_list[slot][1] = bx; s_list[slot][2] = by; s_list[slot][3] = bz;
+      }
+      if (lane == 0) s_nvis = __popc(m);
     }
     __syncthreads();
-    unsigned mask = s_mask;
-    __syncthreads();
-    // ---- visible bricks, two at a time (one per 128-thread half)
-    int k = 0;
-    while (mask) {
-      int bit = __ffs(mask) - 1;
-      mask &= mask - 1;
-      if ((k++ & 1) != half) continue;
-      const int b = b0 + bit;
-      int bz = bz0 + bit, by = by0, bx = bx0;
-      while (bz >= nb) {
-        bz -= nb;
-        if (++by == nb) { by = 0; ++bx; }
-      }
+    const int nvis = s_nvis;
+    for (int e = half; e < nvis; e += 2) {
+      const int b = s_list[e][0], bx = s_list[e][1], by = s_list[e][2], bz = s_list[e][3];
       // camera-space centre of the brick's voxel (0,0,0), FP64 then rounded:
       // per-voxel offsets from it stay below 8 voxels, so the FP32 position
       // error is about one rounding of the brick base.
@@ -286,6 +282,7 @@ __global__ void __launch_bounds__(256) k_integrate(uint32_t *__restrict__ vol, o
           flags[(qx * nb + qy) * nb + qz] = 1;
       }
     }
+    __syncthreads();
   }
   if (CENSUS) {
     for (int o = 16; o > 0; o >>= 1) my_count += __shfl_xor_sync(0xffffffffu, my_count, o);
@@ -300,9 +297,9 @@ of_status_t launch_integrate(const of_volume_desc_t *d, void *vol, const of_came
                              const uint16_t *depth, int pitch, const double *pose,
                              const float *lam, unsigned long long *count, cudaStream_t s) {
   size_t nb = (size_t)(d->resolution / 8);
-  size_t chunks = (nb * nb * nb + kChunk - 1) / kChunk;
-  // persistent grid: 8 resident CTAs of 256 threads per SM
-  unsigned blocks = (unsigned)(chunks < (size_t)kSmCount * 8 ? chunks : (size_t)kSmCount * 8);
+  size_t nbr = nb * nb * nb;
+  // persistent grid: 4 resident CTAs of 256 threads per SM
+  unsigned blocks = (unsigned)(nbr < (size_t)kSmCount * 4 ? nbr : (size_t)kSmCount * 4);
   Cam c = make_cam(*cam);
   if (d->storage == OF_TSDF_I16)
     k_integrate<OF_TSDF_I16, CENSUS><<<blocks, 256, 0, s>>>(
