@@ -76,7 +76,8 @@ typedef struct of_volume_desc {
 typedef struct of_filter_params {
   float sigma_space_px; /* 4.5 */
   float sigma_range_mm; /* 30 */
-  int32_t radius_px;    /* window half-width; 0 = ceil(2 sigma_space) */
+  int32_t radius_px;    /* window half-width; 0 = ceil(2 sigma_space); -1 = no filter
+                           (raw depth, as CameraHandler.cu:65-89 converts it) */
   int32_t levels;       /* pyramid levels, 1..4 */
 } of_filter_params_t;
 
@@ -202,6 +203,12 @@ of_status_t of_icp_workspace_bytes(const of_camera_t *cam, size_t *bytes);
 of_status_t of_icp_track(const of_camera_t *cam, const of_icp_params_t *params,
                          const void *d_frame, const void *d_model, double *d_pose,
                          void *d_workspace, of_icp_stats_t *d_stats, of_stream_t stream);
+/* Fault injection for failure-detection tests (no reference counterpart):
+ * every grid barrier of later of_icp_track calls on this workspace waits for
+ * `extra` block arrivals that never come. Each such wait gives up after about
+ * 0.15 s; the call then stops, restores the starting pose and reports status 2
+ * in of_icp_stats_t. `extra` = 0 restores normal operation. */
+of_status_t of_icp_workspace_hold_barrier(void *d_workspace, int32_t extra, of_stream_t stream);
 /* One FindCorresponding pass (ICP.cu:116-262) at `level`: the 21 upper
  * J^T J entries (row-major i<=j), 6 J^T r entries, sum r^2 and the inlier
  * count as 29 floats into `d_system`, for the pose `d_pose`. */
@@ -272,8 +279,11 @@ of_status_t of_points_to_reference(const of_camera_t *cam, const void *d_pyramid
 of_status_t of_points_from_reference(const of_camera_t *cam, int32_t levels,
                                      const float *d_vertex3, const float *d_normal3,
                                      void *d_model, of_stream_t stream);
-/* float[16] pose <-> FP64 device pose. */
-of_status_t of_pose_from_float(const float *d_pose_f32, double *d_pose, of_stream_t stream);
+/* float[16] pose <-> FP64 device pose. With `invert` != 0 the input is a
+ * world-to-camera matrix (the reference's d_invCurrentTransform) and the
+ * camera-to-world pose is its rigid inverse, formed in FP64. */
+of_status_t of_pose_from_float(const float *d_pose_f32, double *d_pose, int32_t invert,
+                               of_stream_t stream);
 of_status_t of_pose_to_float(const double *d_pose, float *d_pose_f32, float *d_inv_pose_f32,
                              float *d_camera_position3, of_stream_t stream);
 

@@ -98,6 +98,7 @@ _SIGS = {
     "of_icp_workspace_bytes": (c_status, [C.POINTER(Camera), C.POINTER(C.c_size_t)]),
     "of_icp_track": (c_status, [C.POINTER(Camera), C.POINTER(IcpParams), P, P, P, P, P,
                                 c_stream]),
+    "of_icp_workspace_hold_barrier": (c_status, [P, C.c_int32, c_stream]),
     "of_icp_system": (c_status, [C.POINTER(Camera), C.POINTER(IcpParams), C.c_int32, P, P, P, P,
                                  P, c_stream]),
     "of_tracker_create": (c_status, [C.POINTER(TrackerDesc), C.POINTER(C.c_void_p)]),
@@ -109,7 +110,7 @@ _SIGS = {
     "of_tracker_buffers": (c_status, [P, C.POINTER(TrackerBuffers)]),
     "of_points_to_reference": (c_status, [C.POINTER(Camera), P, P, P, P, c_stream]),
     "of_points_from_reference": (c_status, [C.POINTER(Camera), C.c_int32, P, P, P, c_stream]),
-    "of_pose_from_float": (c_status, [P, P, c_stream]),
+    "of_pose_from_float": (c_status, [P, P, C.c_int32, c_stream]),
     "of_pose_to_float": (c_status, [P, P, P, P, c_stream]),
 }
 

@@ -209,9 +209,24 @@ extern "C" of_status_t of_lambda_table(const of_camera_t *cam, float *d_lambda, 
 
 // ------------------------------------------------------------ pose adapters --
 
-__global__ void k_pose_from_float(const float *pf, double *pd) {
-  int i = threadIdx.x;
-  if (i < 16) pd[i] = (double)pf[i];
+__global__ void k_pose_from_float(const float *pf, double *pd, int invert) {
+  if (threadIdx.x != 0) return;
+  double m[16];
+  for (int i = 0; i < 16; ++i) m[i] = (double)pf[i];
+  if (!invert) {
+    for (int i = 0; i < 16; ++i) pd[i] = m[i];
+    return;
+  }
+  for (int i = 0; i < 3; ++i) {
+    double acc = 0.0;
+    for (int j = 0; j < 3; ++j) {
+      pd[4 * i + j] = m[4 * j + i];
+      acc -= m[4 * j + i] * m[4 * j + 3];
+    }
+    pd[4 * i + 3] = acc;
+  }
+  pd[12] = pd[13] = pd[14] = 0.0;
+  pd[15] = 1.0;
 }
 
 __global__ void k_pose_to_float(const double *pd, float *pf, float *inv, float *campos) {
@@ -239,9 +254,10 @@ __global__ void k_pose_to_float(const double *pd, float *pf, float *inv, float *
   }
 }
 
-extern "C" of_status_t of_pose_from_float(const float *pf, double *pd, of_stream_t s) {
+extern "C" of_status_t of_pose_from_float(const float *pf, double *pd, int32_t invert,
+                                          of_stream_t s) {
   if (!pf || !pd) return OF_ERR_INVALID_ARGUMENT;
-  k_pose_from_float<<<1, 32, 0, (cudaStream_t)s>>>(pf, pd);
+  k_pose_from_float<<<1, 32, 0, (cudaStream_t)s>>>(pf, pd, invert);
   return of_launch_status();
 }
 

@@ -50,7 +50,8 @@ struct IcpWorkspace {
   double pose_init[16];
   double prior[16];
   int has_prior;
-  int pad2[3];
+  int hold_barrier;  // fault injection: arrivals a grid barrier waits for that never come
+  int pad2[2];
   float partials[kIcpMaxBlocks][32];
   float fused_partials[2][kFusedMaxBlocks][32];
 };
@@ -285,13 +286,13 @@ struct IcpPlan {
 
 // Grid-wide barrier for a co-resident grid: arrival counter + generation.
 // The wait is bounded; on timeout the workspace error flag is set.
-__device__ __forceinline__ void grid_barrier(IcpWorkspace *ws, unsigned nblocks) {
+__device__ __forceinline__ void grid_barrier(IcpWorkspace *ws, unsigned nexpect) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned *gen = &ws->bar_gen;
     unsigned g = *gen;
     __threadfence();
-    if (atomicAdd(&ws->bar_count, 1u) == nblocks - 1) {
+    if (atomicAdd(&ws->bar_count, 1u) == nexpect - 1) {
       ws->bar_count = 0;
       __threadfence();
       atomicAdd(&ws->bar_gen, 1u);
@@ -421,15 +422,18 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   __shared__ Rigid s_c2w, s_w2c;
   __shared__ float s_red[kFusedThreads / 32][32];
   __shared__ float s_tot[32];
-  __shared__ int s_stop, s_inl, s_its;
+  __shared__ int s_stop, s_inl, s_its, s_err;
   __shared__ double s_res, s_piv;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int kWarps = kFusedThreads / 32;
   if (threadIdx.x < 16) s_pose[threadIdx.x] = pose[threadIdx.x];
-  if (threadIdx.x == 0) { s_stop = 0; s_its = 0; s_inl = 0; s_res = 0.0; s_piv = 0.0; }
+  if (threadIdx.x == 0) { s_stop = 0; s_err = 0; s_its = 0; s_inl = 0; s_res = 0.0; s_piv = 0.0; }
   __syncthreads();
+  // blocks a barrier waits for: the grid, plus any arrivals held back by the
+  // fault-injection hook (which then never come)
+  const unsigned nexpect = gridDim.x + (unsigned)max(0, ws->hold_barrier);
   int iter_global = 0;
-  for (int l = plan.levels - 1; l >= 0 && !s_stop; --l) {
+  for (int l = plan.levels - 1; l >= 0 && !s_stop && !s_err; --l) {
     const IcpLevel L = plan.lv[l];
     for (int it = 0; it < L.iters; ++it) {
       if (threadIdx.x == 0) pose_to_rigid(s_pose, &s_c2w, &s_w2c);
@@ -506,7 +510,11 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
           for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
         ws->fused_partials[buf][blockIdx.x][lane] = lane < kVals ? y[0] : 0.f;
       }
-      grid_barrier(ws, gridDim.x);
+      grid_barrier(ws, nexpect);
+      // a barrier that gave up ends this frame's tracking in every block
+      if (threadIdx.x == 0) s_err = *((volatile int *)&ws->error);
+      __syncthreads();
+      if (s_err) break;
       // every block: Kahan over its strided share of the blocks' partials,
       // then a tree over the groups, in a fixed order
       {
@@ -612,6 +620,18 @@ int icp_blocks(int npx) {
 }  // namespace
 
 size_t of_icp_workspace_size() { return sizeof(IcpWorkspace); }
+
+extern "C" of_status_t of_icp_workspace_hold_barrier(void *d_workspace, int32_t extra,
+                                                     of_stream_t stream) {
+  if (!d_workspace || extra < 0 || extra > 1024) return OF_ERR_INVALID_ARGUMENT;
+  IcpWorkspace *ws = (IcpWorkspace *)d_workspace;
+  static int values[1025];
+  values[extra] = extra;
+  OF_CUDA_TRY(cudaMemcpyAsync(&ws->hold_barrier, &values[extra], sizeof(int),
+                              cudaMemcpyHostToDevice, (cudaStream_t)stream));
+  OF_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  return OF_OK;
+}
 
 of_status_t of_icp_set_prior(void *d_workspace, const double *prior_host, cudaStream_t s) {
   IcpWorkspace *ws = (IcpWorkspace *)d_workspace;

@@ -128,6 +128,17 @@ __global__ void __launch_bounds__(256) k_bilateral_r(const uint16_t *__restrict_
   out[(size_t)y * w + x] = result;
 }
 
+// No filter: the raw depth as float, invalid -> 0 (the reference converts the
+// raw depth, CameraHandler.cu:65-89).
+__global__ void k_depth_raw(const uint16_t *__restrict__ depth, int pitch, int w, int h,
+                            float dmin, float dmax, float *__restrict__ out) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= w || y >= h) return;
+  float d = (float)depth[(size_t)y * pitch + x];
+  out[(size_t)y * w + x] = depth_valid(d, dmin, dmax) ? d : 0.f;
+}
+
 // Level l -> l+1: pixel (x, y) averages the valid pixels of the 2x2 block
 // {2x, 2x+1} x {2y, 2y+1} that lie within 3 sigma_r of the block's first
 // valid pixel (row-major order); 0 if the block has none.
@@ -204,7 +215,7 @@ extern "C" of_status_t of_preprocess(const of_camera_t *cam, const of_filter_par
       fp->sigma_range_mm <= 0.f)
     return OF_ERR_INVALID_ARGUMENT;
   int R = fp->radius_px > 0 ? fp->radius_px : (int)ceilf(2.0f * fp->sigma_space_px);
-  if (R > kMaxRadius) return OF_ERR_INVALID_ARGUMENT;
+  if (R > kMaxRadius || fp->radius_px < -1) return OF_ERR_INVALID_ARGUMENT;
   of_pyramid_layout_t lay;
   of_status_t st = of_pyramid_layout(cam, fp->levels, &lay);
   if (st != OF_OK) return st;
@@ -213,7 +224,12 @@ extern "C" of_status_t of_preprocess(const of_camera_t *cam, const of_filter_par
   const double log2e = 1.4426950408889634;
   float ks = (float)(log2e / (2.0 * (double)fp->sigma_space_px * fp->sigma_space_px));
   float kr = (float)(log2e / (2.0 * (double)fp->sigma_range_mm * fp->sigma_range_mm));
-  {
+  if (fp->radius_px == -1) {
+    dim3 blk(32, 8);
+    dim3 grid((cam->width + 31) / 32, (cam->height + 7) / 8);
+    k_depth_raw<<<grid, blk, 0, s>>>(d_depth, pitch, cam->width, cam->height, cam->min_depth_mm,
+                                     cam->max_depth_mm, (float *)(base + lay.depth_offset[0]));
+  } else {
     dim3 grid((cam->width + kTileX - 1) / kTileX, (cam->height + kTileY - 1) / kTileY);
     size_t smem = (size_t)(kTileX + 2 * R) * (kTileY + 2 * R) * sizeof(float);
     float *o = (float *)(base + lay.depth_offset[0]);

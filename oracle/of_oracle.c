@@ -176,7 +176,13 @@ void ora_preprocess(const ora_cam *c, const ora_params *p, const uint16_t *depth
     lvl_pts[l] = q;
     q += (size_t)lc[l].w * lc[l].h * 8;
   }
-  ora_bilateral(c, depth, p->sigma_s, p->sigma_r, rad, lvl_depth[0]);
+  if (p->radius == -1) {
+    /* no filter: the raw depth (CameraHandler.cu:65-89 converts it unfiltered) */
+    for (size_t i = 0; i < (size_t)c->w * c->h; ++i)
+      lvl_depth[0][i] = depth_ok(depth[i], c) ? (R)depth[i] : (R)0;
+  } else {
+    ora_bilateral(c, depth, p->sigma_s, p->sigma_r, rad, lvl_depth[0]);
+  }
   for (int l = 1; l < p->levels; ++l)
     ora_pyr_down(lvl_depth[l - 1], lc[l - 1].w, lc[l - 1].h, lvl_depth[l], lc[l].w, lc[l].h,
                  3.0 * p->sigma_r);

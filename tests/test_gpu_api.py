@@ -1,0 +1,148 @@
+"""GPU tests of the boundary itself: the reference-shaped C++ classes, the
+adapters to the reference's data layouts, volume export/import, the raw-depth
+mode, and failure detection of the ICP grid barrier (a wait that nothing
+completes must end with a status, not a hang)."""
+import ctypes as C
+import json
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import pose_error
+
+pytestmark = pytest.mark.gpu
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def dev_pose(P, device):
+    import torch
+    return torch.tensor(np.asarray(P, np.float64).reshape(16), dtype=torch.float64, device=device)
+
+
+def c1(of, **kw):
+    import dataclasses
+    return dataclasses.replace(of.CONFIGS["c1"], **kw)
+
+
+def test_cpp_reference_shaped_classes_track(of, cuda):
+    sys.path.insert(0, str(ROOT / "tests" / "cpp"))
+    import build_shim
+    exe = build_shim.build()
+    out = subprocess.run([str(exe), "20"], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    res = json.loads(out.stdout.strip().splitlines()[-1])
+    assert res["cuda"] == "no error"
+    assert res["bad_status"] == 0
+    assert res["max_trans_mm"] < 5.0 and res["max_rot_rad"] < np.radians(0.5), res
+
+
+def test_icp_barrier_timeout_reports_status(of, cuda):
+    import torch
+    cfg = c1(of)
+    seq = of.make_sequence(cfg, frames=3)
+    vol, lam = of.new_volume(cfg, cuda), of.lambda_table(cfg, cuda)
+    for k in range(2):
+        of.integrate(cfg, vol, torch.from_numpy(seq.depth[k].astype(np.int16)).to(cuda),
+                     dev_pose(seq.poses[k], cuda), lam)
+    model = of.raycast(cfg, vol, dev_pose(seq.poses[1], cuda))
+    frame = of.preprocess(cfg, torch.from_numpy(seq.depth[2].astype(np.int16)).to(cuda))
+    ws = of.icp_workspace(cfg, cuda)
+    lib = of._native.lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    # hold every grid barrier for one arrival that never comes
+    assert lib.of_icp_workspace_hold_barrier(ws.data_ptr(), 1, stream) == 0
+    pose = dev_pose(seq.poses[1], cuda)
+    stats = torch.zeros(32, dtype=torch.uint8, device=cuda)
+    t0 = time.perf_counter()
+    of.icp_track(cfg, frame, model, pose, ws, stats)
+    torch.cuda.synchronize()
+    elapsed = time.perf_counter() - t0
+    assert int(stats[:4].view(torch.int32).item()) == 2
+    assert np.array_equal(pose.cpu().numpy().reshape(4, 4), seq.poses[1])
+    assert elapsed < 5.0
+    # the context is still usable and the workspace recovers
+    assert lib.of_icp_workspace_hold_barrier(ws.data_ptr(), 0, stream) == 0
+    of.icp_track(cfg, frame, model, pose, ws, stats)
+    ws2 = of.icp_workspace(cfg, cuda)
+    pose2 = dev_pose(seq.poses[1], cuda)
+    of.icp_track(cfg, frame, model, pose2, ws2)
+    torch.cuda.synchronize()
+    assert int(stats[:4].view(torch.int32).item()) == 0
+    assert np.array_equal(pose.cpu().numpy(), pose2.cpu().numpy())
+
+
+def test_volume_export_import_roundtrip(of, cuda):
+    import torch
+    cfg = c1(of, resolution=64)
+    seq = of.make_sequence(cfg, frames=2)
+    vol, lam = of.new_volume(cfg, cuda), of.lambda_table(cfg, cuda)
+    for k in range(2):
+        of.integrate(cfg, vol, torch.from_numpy(seq.depth[k].astype(np.int16)).to(cuda),
+                     dev_pose(seq.poses[k], cuda), lam)
+    n = cfg.resolution
+    tsdf = torch.empty(n ** 3, dtype=torch.float32, device=cuda)
+    wgt = torch.empty(n ** 3, dtype=torch.int16, device=cuda)
+    lib = of._native.lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    assert lib.of_volume_export(C.byref(cfg.volume()), vol.data_ptr(), tsdf.data_ptr(),
+                                wgt.data_ptr(), stream) == 0
+    q, w = of.volume_to_linear(cfg, vol.cpu().numpy())
+    t = tsdf.cpu().numpy().reshape(n, n, n)
+    expect = np.where(w > 0, q.view(np.int16) / 32767.0 * cfg.trunc_mm, cfg.trunc_mm)
+    assert np.allclose(t, expect, atol=1e-6 * cfg.trunc_mm)
+    assert np.array_equal(wgt.cpu().numpy().view(np.uint16).reshape(n, n, n), w)
+    vol2 = of.new_volume(cfg, cuda)
+    assert lib.of_volume_import(C.byref(cfg.volume()), vol2.data_ptr(), tsdf.data_ptr(),
+                                wgt.data_ptr(), stream) == 0
+    q2, w2 = of.volume_to_linear(cfg, vol2.cpu().numpy())
+    assert np.array_equal(w2, w) and np.array_equal(q2[w > 0], q[w > 0])
+    # imported bricks are all flagged, so the raycast cannot skip observed voxels
+    flags = vol2.cpu().numpy().view(np.uint8)[4 * n ** 3:][: (n // 8) ** 3]
+    assert flags.min() == 1
+
+
+def test_reference_point_layout_roundtrip(of, cuda):
+    import torch
+    cfg = c1(of)
+    seq = of.make_sequence(cfg, frames=2)
+    vol, lam = of.new_volume(cfg, cuda), of.lambda_table(cfg, cuda)
+    of.integrate(cfg, vol, torch.from_numpy(seq.depth[0].astype(np.int16)).to(cuda),
+                 dev_pose(seq.poses[0], cuda), lam)
+    model = of.raycast(cfg, vol, dev_pose(seq.poses[0], cuda))
+    npx = cfg.width * cfg.height
+    v3 = torch.empty(npx * 3, dtype=torch.float32, device=cuda)
+    n3 = torch.empty(npx * 3, dtype=torch.float32, device=cuda)
+    lib = of._native.lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    assert lib.of_points_to_reference(C.byref(cfg.camera()), model.data_ptr(), None,
+                                      v3.data_ptr(), n3.data_ptr(), stream) == 0
+    vv = v3.cpu().numpy().reshape(cfg.height, cfg.width, 3)
+    gv, gn = (t.cpu().numpy() for t in of.unpack_points(cfg, model, 0))
+    bad = gv[..., 3] == 0
+    assert np.all(vv[bad] == np.finfo(np.float32).max)       # BAD_VERTEX = FLT_MAX
+    assert np.array_equal(vv[~bad], gv[..., :3][~bad])
+    model2 = of.new_pyramid(cfg, cuda)
+    assert lib.of_points_from_reference(C.byref(cfg.camera()), cfg.levels, v3.data_ptr(),
+                                        n3.data_ptr(), model2.data_ptr(), stream) == 0
+    for l in range(cfg.levels):
+        a = [t.cpu().numpy() for t in of.unpack_points(cfg, model, l)]
+        b = [t.cpu().numpy() for t in of.unpack_points(cfg, model2, l)]
+        valid = (a[0][..., 3] > 0) & (a[1][..., 3] > 0)
+        assert np.array_equal(a[0][valid], b[0][valid]) and np.array_equal(a[1][valid], b[1][valid])
+
+
+def test_raw_depth_mode_matches_reference_conversion(of, ora, cuda):
+    import torch
+    cfg = c1(of, radius_px=-1)
+    seq = of.make_sequence(cfg, frames=1)
+    frame = of.preprocess(cfg, torch.from_numpy(seq.depth[0].astype(np.int16)).to(cuda))
+    d0 = of.unpack_depth(cfg, frame, 0).cpu().numpy()
+    raw = seq.depth[0].astype(np.float32)
+    valid = (raw >= cfg.min_depth_mm) & (raw <= cfg.max_depth_mm)
+    assert np.array_equal(d0, np.where(valid, raw, 0.0).astype(np.float32))
+    levels, _ = ora.preprocess(cfg, seq.depth[0])
+    assert np.array_equal(levels[0][0], np.where(valid, raw, 0.0))
