@@ -203,6 +203,22 @@ of_status_t of_icp_workspace_bytes(const of_camera_t *cam, size_t *bytes);
 of_status_t of_icp_track(const of_camera_t *cam, const of_icp_params_t *params,
                          const void *d_frame, const void *d_model, double *d_pose,
                          void *d_workspace, of_icp_stats_t *d_stats, of_stream_t stream);
+/* of_icp_track without a workspace argument (no counterpart in the
+ * reference): for callers that cannot allocate device memory once they run --
+ * hosts that own every device allocation up front, such as plugin hosts with
+ * a fixed memory budget, or real-time loops where cudaMalloc's implicit
+ * synchronisation and a possible failure mid-session are not acceptable. It
+ * allocates nothing: its scratch is one file-scope device array of about
+ * 115 KB (per-block partial sums for at most 296 cooperating blocks) that every
+ * GPU loading the library holds until the process exits; a device that would
+ * need more blocks gets OF_ERR_TOO_LARGE. The first call on a device looks up
+ * and zeroes that array (with the device current) and should come before any
+ * stream capture. All calls share the one array and each starts by clearing
+ * the state it needs cleared; calls whose executions overlap on the GPU race
+ * with each other -- order them on one stream. Results equal of_icp_track's. */
+of_status_t of_icp_track_static(const of_camera_t *cam, const of_icp_params_t *params,
+                                const void *d_frame, const void *d_model, double *d_pose,
+                                of_icp_stats_t *d_stats, of_stream_t stream);
 /* Fault injection for failure-detection tests (no reference counterpart):
  * every grid barrier of later of_icp_track calls on this workspace waits for
  * `extra` block arrivals that never come. Each such wait gives up after about

@@ -99,6 +99,8 @@ _SIGS = {
     "of_icp_track": (c_status, [C.POINTER(Camera), C.POINTER(IcpParams), P, P, P, P, P,
                                 c_stream]),
     "of_icp_workspace_hold_barrier": (c_status, [P, C.c_int32, c_stream]),
+    "of_icp_track_static": (c_status, [C.POINTER(Camera), C.POINTER(IcpParams), P, P, P, P,
+                                       c_stream]),
     "of_icp_system": (c_status, [C.POINTER(Camera), C.POINTER(IcpParams), C.c_int32, P, P, P, P,
                                  P, c_stream]),
     "of_tracker_create": (c_status, [C.POINTER(TrackerDesc), C.POINTER(C.c_void_p)]),

@@ -20,6 +20,7 @@
 //   starting pose and stops the remaining iterations (ICP.cpp:152-158).
 #include "of_common.cuh"
 
+#include <mutex>
 #include <string.h>
 
 using namespace of;
@@ -735,4 +736,65 @@ extern "C" of_status_t of_icp_system(const of_camera_t *cam, const of_icp_params
                                                     ip->dist_thresh_mm, ip->normal_thresh,
                                                     (double *)pose, ws, nullptr, d_system);
   return of_launch_status();
+}
+
+// ---------------------------------------------------------------------------
+// Tracking without a caller-provided workspace.
+//
+// For callers that cannot allocate device memory while they run (hosts that own
+// every device allocation up front, such as plugin hosts with a fixed memory
+// budget or real-time loops where cudaMalloc's implicit synchronisation and a
+// possible failure mid-session are not acceptable), of_icp_track_static uses a
+// workspace that lives in this file-scope array instead. Every GPU that loads
+// the library holds it (sizeof(IcpWorkspace), about 115 KB) until the process
+// exits. It holds the per-block partial sums of at most kFusedMaxBlocks
+// cooperating blocks.
+static __device__ __align__(256) unsigned char g_static_icp_ws[sizeof(IcpWorkspace)];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_static_ws_mutex;
+void *g_static_ws_ptr[kMaxDevices] = {};
+}  // namespace
+
+// Device address of the array on the current device. In host code the array's
+// name is only a host-side stand-in, so the address is queried once per device
+// (with that device current) and cached; the first query also zeroes the
+// workspace.
+static of_status_t static_icp_workspace(void **out) {
+  int dev = 0;
+  OF_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return OF_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(g_static_ws_mutex);
+  if (!g_static_ws_ptr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_icp_ws);
+    if (e != cudaSuccess || !p) return of_set_cuda_error(e != cudaSuccess ? e : cudaErrorUnknown);
+    e = cudaMemset(p, 0, sizeof(IcpWorkspace));
+    if (e != cudaSuccess) return of_set_cuda_error(e);
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return of_set_cuda_error(e);
+    g_static_ws_ptr[dev] = p;
+  }
+  *out = g_static_ws_ptr[dev];
+  return OF_OK;
+}
+
+extern "C" of_status_t of_icp_track_static(const of_camera_t *cam, const of_icp_params_t *ip,
+                                           const void *d_frame, const void *d_model,
+                                           double *pose, of_icp_stats_t *stats,
+                                           of_stream_t stream) {
+  if (!of_camera_valid(cam) || !icp_params_ok(ip) || !d_frame || !d_model || !pose)
+    return OF_ERR_INVALID_ARGUMENT;
+  // the array holds partials for kFusedMaxBlocks blocks: a device whose
+  // co-resident grid would need more is refused
+  int dev = 0, sms = 0, per_sm = 0;
+  OF_CUDA_TRY(cudaGetDevice(&dev));
+  OF_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  OF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_icp_fused, kFusedThreads, 0));
+  if ((long)sms * (per_sm < 1 ? 1 : per_sm) > kFusedMaxBlocks) return OF_ERR_TOO_LARGE;
+  void *ws = nullptr;
+  of_status_t st = static_icp_workspace(&ws);
+  if (st != OF_OK) return st;
+  return of_icp_launch(cam, ip, d_frame, d_model, pose, ws, stats, (cudaStream_t)stream);
 }
