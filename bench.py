@@ -40,8 +40,9 @@ METRIC = "frames/s 640x480 @512³ vol, plain vs learned-warm-start ICP at equal 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--frames", type=int, default=300, help="rendered frames (ping-pong)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -60,7 +61,8 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms during the
+    timed region (one background nvidia-smi process)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -69,41 +71,55 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.rows = []
-        self._stop = threading.Event()
-        self._t = None
-
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index),
-                                      f"--query-gpu={self.Q}", "--format=csv,noheader,nounits"],
-                                     capture_output=True, text=True, timeout=5).stdout.strip()
-                if out:
-                    self.rows.append([x.strip() for x in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        self._p = None
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+        try:
+            self._p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                        "--format=csv,noheader,nounits", "-lms", "100"],
+                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            time.sleep(0.3)  # first sample before the timed work starts
+        except Exception:
+            self._p = None
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        if self._p is None:
+            return
+        time.sleep(0.15)
+        self._p.terminate()
+        try:
+            out, _ = self._p.communicate(timeout=10)
+        except Exception:
+            self._p.kill()
+            out = ""
+        self.rows = [[x.strip() for x in line.split(",")] for line in out.splitlines() if line.strip()]
 
     def summary(self):
-        if not self.rows:
+        rows = [r for r in self.rows if len(r) >= 9]
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [v for v in (num(r[1]) for r in rows) if v is not None]
+        mx = [v for v in (num(r[2]) for r in rows) if v is not None]
+        pw = [v for v in (num(r[3]) for r in rows) if v is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4)
-                          if len(r) > 5 + i and r[5 + i].lower() == "active"})
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.rows)}
+                "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(pw) if pw else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def frame_index(i: int, n: int) -> int:
+    """Ping-pong through n rendered frames: consecutive steps stay adjacent poses."""
+    period = 2 * (n - 1)
+    j = i % period
+    return j if j < n else period - j
 
 
 def dist_setup():
@@ -146,15 +162,16 @@ def pose_errors(hist, gt):
 
 # ------------------------------------------------------------- CPU baseline
 
-def cpu_frames_per_s(cfg, seq, seconds: float, max_frames: int):
+def cpu_frames_per_s(cfg, seq, seconds: float):
     """FP32 OpenMP build of the oracle restatement on the host cores."""
     from oracle import CpuTracker, Oracle
     o = Oracle("f32")
+    n_seq = len(seq.depth)
     tr = CpuTracker(o, cfg, seq.poses[0])
     tr.process(seq.depth[0])      # frame 0 (fuse only) is not timed
     n, t0 = 0, time.perf_counter()
-    while n < max_frames and (n < 3 or time.perf_counter() - t0 < seconds):
-        tr.process(seq.depth[1 + n])
+    while n < 3 or time.perf_counter() - t0 < seconds:
+        tr.process(seq.depth[frame_index(1 + n, n_seq)])
         n += 1
     dt = time.perf_counter() - t0
     tr.close()
@@ -167,23 +184,23 @@ def run_reference(args, cfg, world, rank):
     if rank != 0:
         return
     import openfusion_b200 as of
-    frames = 1 + args.warmup + args.steps
-    seq = of.make_sequence(cfg, frames=min(frames, 1 + args.warmup + args.steps))
+    seq = of.make_sequence(cfg, frames=args.frames)
+    n_seq = len(seq.depth)
     from oracle import CpuTracker, Oracle
     o = Oracle("f32")
     tr = CpuTracker(o, cfg, seq.poses[0])
     tr.process(seq.depth[0])
     t_w = time.perf_counter()
     for k in range(args.warmup):
-        tr.process(seq.depth[1 + k])
+        tr.process(seq.depth[frame_index(1 + k, n_seq)])
     per = (time.perf_counter() - t_w) / max(1, args.warmup)
-    # keep the whole run within a few minutes: time at most ~150 s of frames
+    # keep the whole run within a few minutes: time at most ~120 s of frames
     steps = args.steps
-    if per > 0 and steps * per > 150.0:
-        steps = max(3, int(150.0 / per))
+    if per > 0 and steps * per > 120.0:
+        steps = max(3, int(120.0 / per))
     t0 = time.perf_counter()
     for k in range(steps):
-        tr.process(seq.depth[1 + args.warmup + k])
+        tr.process(seq.depth[frame_index(1 + args.warmup + k, n_seq)])
     dt = time.perf_counter() - t0
     tr.close()
     fps = steps / dt
@@ -196,8 +213,8 @@ def run_reference(args, cfg, world, rank):
                    "volume": f"{cfg.resolution}^3 over {cfg.size_mm / 1000:g} m",
                    "icp_iters": list(cfg.iters), "frames_requested": args.steps},
         "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": o.threads(), "kind": "port",
-                         "sample": f"{steps} consecutive frames of the same sequence after "
-                                   f"{args.warmup} warm-up frames (FP32 OpenMP restatement)"},
+                         "sample": f"{steps} consecutive frames after {args.warmup} warm-up "
+                                   "frames (FP32 OpenMP restatement of the same equations)"},
         "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -212,17 +229,19 @@ def run_ours(args, cfg, world, rank, local):
     if rank:
         import dataclasses
         cfg = dataclasses.replace(cfg, seed=cfg.seed + 7919 * rank)
-    frames = 1 + args.warmup + args.steps
-    seq = of.make_sequence(cfg, frames=frames)
+    seq = of.make_sequence(cfg, frames=args.frames)
+    n_seq = len(seq.depth)
+    total = 1 + args.warmup + args.steps
+    order = [frame_index(i, n_seq) for i in range(total)]
     depth_dev = torch.from_numpy(seq.depth.astype(np.int16)).to(dev)
     depth_host = torch.from_numpy(seq.depth.astype(np.int16)).pin_memory()
     stream = torch.cuda.current_stream(dev)
 
     # ---- device-resident loop: value
-    tr = of.Tracker(cfg, seq.poses[0], use_graph=True, pose_history=frames)
-    tr.process(depth_dev[0])
-    for k in range(args.warmup):
-        tr.process(depth_dev[1 + k])
+    tr = of.Tracker(cfg, seq.poses[0], use_graph=True, pose_history=total)
+    tr.process(depth_dev[order[0]])
+    for i in range(1, 1 + args.warmup):
+        tr.process(depth_dev[order[i]])
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     sampler = ClockSampler(local)
@@ -230,8 +249,8 @@ def run_ours(args, cfg, world, rank, local):
     torch.cuda.synchronize()
     with sampler:
         ev0.record(stream)
-        for k in range(args.steps):
-            tr.process(depth_dev[1 + args.warmup + k])
+        for i in range(1 + args.warmup, total):
+            tr.process(depth_dev[order[i]])
         ev1.record(stream)
         torch.cuda.synchronize()
     barrier(world)
@@ -239,38 +258,37 @@ def run_ours(args, cfg, world, rank, local):
     ms_max = max_over_ranks(ms, world)
     bufs = tr.buffers()
     kernels = bufs.kernels_track * args.steps
-    hist = tr.pose_history(frames)
+    hist = tr.pose_history(total)
     _, st = tr.pose()
     tr.close()
-    rots, trans = pose_errors(hist, seq.poses)
+    rots, trans = pose_errors(hist, [seq.poses[j] for j in order])
 
     # ---- end to end through the C-ABI: pinned host depth in, pose out
-    tr = of.Tracker(cfg, seq.poses[0], use_graph=True, pose_history=frames)
-    pose_out = torch.zeros((frames, 16), dtype=torch.float64).pin_memory()
-    tr.process(depth_host[0])
-    for k in range(args.warmup):
-        tr.process(depth_host[1 + k])
-        tr.pose(out=pose_out[1 + k])
+    tr = of.Tracker(cfg, seq.poses[0], use_graph=True, pose_history=total)
+    pose_out = torch.zeros((total, 16), dtype=torch.float64).pin_memory()
+    tr.process(depth_host[order[0]])
+    for i in range(1, 1 + args.warmup):
+        tr.process(depth_host[order[i]])
+        tr.pose(out=pose_out[i])
     torch.cuda.synchronize()
     barrier(world)
     torch.cuda.synchronize()
     ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev2.record(stream)
-    for k in range(args.steps):
-        i = 1 + args.warmup + k
-        tr.process(depth_host[i])
+    for i in range(1 + args.warmup, total):
+        tr.process(depth_host[order[i]])
         tr.pose(out=pose_out[i])
     ev3.record(stream)
     torch.cuda.synchronize()
     barrier(world)
     e2e_ms = max_over_ranks(ev2.elapsed_time(ev3), world)
-    e2e_hist = pose_out.numpy().reshape(frames, 4, 4)
+    e2e_hist = pose_out.numpy().reshape(total, 4, 4)
     assert np.allclose(e2e_hist[1 + args.warmup:], hist[1 + args.warmup:], atol=1e-6), \
         "end-to-end poses differ from the device-resident run"
     tr.close()
 
     # ---- per-stage kernel times (stage-wise launches with CUDA events)
-    stages = stage_times(of, cfg, seq, depth_dev, args, dev)
+    stages = stage_times(of, cfg, seq, depth_dev, order, args, dev)
 
     fps = world * args.steps / (ms_max / 1e3)
     e2e_fps = world * args.steps / (e2e_ms / 1e3)
@@ -294,6 +312,7 @@ def run_ours(args, cfg, world, rank, local):
         "config": {"workload": cfg.name, "width": cfg.width, "height": cfg.height,
                    "volume": f"{cfg.resolution}^3 int16+uint16 over {cfg.size_mm / 1000:g} m",
                    "icp": "3 levels, 10/5/4 iterations, plain (no warm start)",
+                   "frames": f"{n_seq} rendered frames, traversed forward and back",
                    "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (512 MiB volume)"},
         "stages_ms": {k: v for k, v in stages.items() if k.endswith("_ms")},
@@ -304,21 +323,22 @@ def run_ours(args, cfg, world, rank, local):
         "roofline": {"kernel": "k_integrate", "bound": "hbm", "achieved": achieved,
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "alg_bytes_per_launch": integ_bytes},
+                     "alg_bytes_per_launch": integ_bytes,
+                     "updated_voxels_per_launch": stages["integrate_updated_voxels"]},
         "e2e": {"value": e2e_fps, "unit": "frames/s",
                 "h2d_bytes_per_step": cfg.width * cfg.height * 2, "d2h_bytes_per_step": 128},
         "gpu_launches": kernels,
         "clocks": sampler.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
-        cps, n, dt, cores = cpu_frames_per_s(cfg, seq, args.cpu_seconds, frames - 1)
+        cps, n, dt, cores = cpu_frames_per_s(cfg, seq, args.cpu_seconds)
         line["cpu_baseline"] = {"value": cps, "unit": "frames/s", "cores": cores, "kind": "port",
                                 "sample": f"{n} consecutive frames ({dt:.1f} s) of the same "
                                           "sequence, FP32 OpenMP restatement"}
     print(json.dumps(line), flush=True)
 
 
-def stage_times(of, cfg, seq, depth_dev, args, dev):
+def stage_times(of, cfg, seq, depth_dev, order, args, dev):
     """Average device time of each stage, launched stage by stage on the
     current stream and bracketed by CUDA events, over the same frames."""
     import torch
@@ -328,28 +348,32 @@ def stage_times(of, cfg, seq, depth_dev, args, dev):
     model = of.new_pyramid(cfg, dev)
     ws = of.icp_workspace(cfg, dev)
     pose = torch.tensor(seq.poses[0].reshape(16), dtype=torch.float64, device=dev)
-    of.integrate(cfg, vol, depth_dev[0], pose, lam)
+    of.integrate(cfg, vol, depth_dev[order[0]], pose, lam)
     of.raycast(cfg, vol, pose, model)
     acc = {"preprocess": 0.0, "icp": 0.0, "integrate": 0.0, "raycast": 0.0}
     s = torch.cuda.current_stream(dev)
     poses = [pose.clone()]
     n = 0
-    for k in range(1, 1 + args.warmup + args.steps):
+    total = len(order)
+    for i in range(1, total):
+        d = depth_dev[order[i]]
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
         ev[0].record(s)
-        of.preprocess(cfg, depth_dev[k], frame)
+        of.preprocess(cfg, d, frame)
         ev[1].record(s)
         of.icp_track(cfg, frame, model, pose, ws)
         ev[2].record(s)
-        of.integrate(cfg, vol, depth_dev[k], pose, lam)
+        of.integrate(cfg, vol, d, pose, lam)
         ev[3].record(s)
         of.raycast(cfg, vol, pose, model)
         ev[4].record(s)
         poses.append(pose.clone())
-        torch.cuda.synchronize()
-        if k > args.warmup:
-            for i, name in enumerate(acc):
-                acc[name] += ev[i].elapsed_time(ev[i + 1])
+        if i % 50 == 0 or i == total - 1:
+            torch.cuda.synchronize()
+        if i > args.warmup:
+            s.synchronize()
+            for j, name in enumerate(acc):
+                acc[name] += ev[j].elapsed_time(ev[j + 1])
             n += 1
     # Algorithmic bytes of one integration launch: 4 B read + 4 B write per
     # updated voxel plus 2 B per depth pixel. The census launch counts the
@@ -357,10 +381,11 @@ def stage_times(of, cfg, seq, depth_dev, args, dev):
     # same frames at the same poses on a second volume, outside any timing.
     vol2 = of.new_volume(cfg, dev)
     upd = []
-    for k in range(0, 1 + args.warmup + args.steps):
-        if k > args.warmup:
-            upd.append(of.integrate_census(cfg, vol2, depth_dev[k], poses[k], lam))
-        of.integrate(cfg, vol2, depth_dev[k], poses[k], lam)
+    for i in range(total):
+        d = depth_dev[order[i]]
+        if i > args.warmup and (i - args.warmup) % 10 == 0:
+            upd.append(of.integrate_census(cfg, vol2, d, poses[i], lam))
+        of.integrate(cfg, vol2, d, poses[i], lam)
     out = {f"{k}_ms": v / max(n, 1) for k, v in acc.items()}
     out["integrate_alg_bytes"] = 8.0 * float(np.mean(upd)) + 2.0 * cfg.width * cfg.height
     out["integrate_updated_voxels"] = float(np.mean(upd))
