@@ -81,8 +81,29 @@ def render(sc, T, frame):
     return d
 
 
-def main(out: Path):
+def load():
     lib = C.CDLL(str(ROOT / "oracle" / "_ref" / "libref_kernels.so"))
+    P = C.c_void_p
+    sigs = {
+        "ref_volume_size": (C.c_int, []), "ref_max_weight": (C.c_int, []),
+        "ref_world_volume": (C.c_float, []), "ref_truncation": (C.c_float, []),
+        "ref_volume_init": (C.c_int, []), "ref_volume_free": (C.c_int, []),
+        "ref_convert": (C.c_int, [P, P, P, P, P]),
+        "ref_integrate": (C.c_int, [P, P, P, P]),
+        "ref_volume_read": (C.c_int, [P, C.c_int64, P, P]),
+        "ref_raycast": (C.c_int, [P, P, P, P, P, P]),
+        "ref_find_corresponding": (C.c_int, [P, P, P, P, P, P, P, P, P, P]),
+        "ref_build_transform": (None, [P, P, P]),
+    }
+    for name, (res, args) in sigs.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+def main(out: Path):
+    lib = load()
     cam = ref_cam()
     n = lib.ref_volume_size()
     sc = scene()
@@ -161,8 +182,8 @@ def main(out: Path):
                         vertex0=v0, normal0=n0, model_vertex=mv, model_normal=mn, rgba=rgba,
                         new_vertex=v1c, new_normal=n1c, AtA=AtA, Atb=Atb, blocks=nblk.value,
                         vertex1=v1, normal1=n1, xopt=xs, built=np.stack(built),
-                        volume=np.array([n, lib.ref_world_volume.__call__() if False else 1024.0,
-                                         10.0, 120.0]))
+                        volume=np.array([n, lib.ref_world_volume(), lib.ref_truncation(),
+                                         lib.ref_max_weight()], np.float64))
     np.savez_compressed(out / "ref_volume.npz", idx=idx.astype(np.int16), tsdf1=t1, w1=w1,
                         tsdf2=t2, w2=w2)
     print("updated voxels in the sample after frame 0:", int((w1 > 0).sum()), "of", len(w1))
