@@ -28,6 +28,17 @@ class Vol(C.Structure):
                 ("trunc", C.c_double), ("max_w", C.c_int32), ("pad", C.c_int32)]
 
 
+class RefCam(C.Structure):
+    _fields_ = [("w", C.c_int32), ("h", C.c_int32), ("fx", C.c_double), ("fy", C.c_double),
+                ("cx", C.c_double), ("cy", C.c_double), ("ifx", C.c_double), ("ify", C.c_double),
+                ("icx", C.c_double), ("icy", C.c_double), ("dmin", C.c_double), ("dmax", C.c_double)]
+
+
+class RefVol(C.Structure):
+    _fields_ = [("n", C.c_int32), ("b1", C.c_int32), ("world", C.c_double), ("trunc", C.c_double),
+                ("max_w", C.c_int32), ("pad", C.c_int32)]
+
+
 class Params(C.Structure):
     _fields_ = [("sigma_s", C.c_double), ("sigma_r", C.c_double), ("radius", C.c_int32),
                 ("levels", C.c_int32), ("iters", C.c_int32 * 4), ("dist_thresh", C.c_double),
@@ -72,6 +83,13 @@ class Oracle:
         L.ora_icp_step.restype = C.c_int32
         L.ora_icp_track.argtypes = [C.POINTER(Cam), C.POINTER(Params), P, P, P, P]
         L.ora_icp_track.restype = C.c_int32
+        L.ora_ref_convert.argtypes = [C.POINTER(RefCam), P, P, P, P]
+        L.ora_ref_integrate_voxels.argtypes = [C.POINTER(RefVol), C.POINTER(RefCam), P, P, P, P,
+                                               C.c_int64, P, P, P, P, P]
+        L.ora_ref_integrate_full.argtypes = [C.POINTER(RefVol), C.POINTER(RefCam), P, P, P, P, P]
+        L.ora_ref_raycast.argtypes = [C.POINTER(RefVol), P, C.POINTER(RefCam), P, P, P, P, P]
+        L.ora_ref_icp_system.argtypes = [C.POINTER(RefCam), P, P, P, P, P, P, P, P, P, P]
+        L.ora_ref_compose.argtypes = [P, P, P]
         L.ora_tracker_create.argtypes = [C.POINTER(Cam), C.POINTER(Vol), C.POINTER(Params), P]
         L.ora_tracker_create.restype = C.c_void_p
         L.ora_tracker_destroy.argtypes = [P]
@@ -222,6 +240,83 @@ class Oracle:
 
     def threads(self) -> int:
         return self.lib.ora_threads()
+
+
+class RefSemantics:
+    """The reference-semantics functions of the oracle (FP64), for comparison
+    with outputs of the reference's own kernels."""
+
+    def __init__(self, oracle: "Oracle"):
+        self.L = oracle.lib
+
+    @staticmethod
+    def cam(w, h, fx, fy, cx, cy, ifx, ify, icx, icy, dmin, dmax) -> RefCam:
+        return RefCam(w, h, fx, fy, cx, cy, ifx, ify, icx, icy, dmin, dmax)
+
+    @staticmethod
+    def vol(n, world, trunc, max_w, b1=1) -> RefVol:
+        return RefVol(n, b1, world, trunc, max_w, 0)
+
+    def convert(self, cam, depth, T):
+        d = np.ascontiguousarray(depth, np.uint16)
+        T_ = np.ascontiguousarray(T, np.float64)
+        v = np.zeros((cam.h, cam.w, 3))
+        n = np.zeros((cam.h, cam.w, 3))
+        self.L.ora_ref_convert(C.byref(cam), d.ctypes.data, T_.ctypes.data, v.ctypes.data,
+                               n.ctypes.data)
+        return v, n
+
+    def integrate_voxels(self, vol, cam, vertex, invT, cpos, storage, prev_t, prev_w):
+        vx = np.ascontiguousarray(vertex, np.float64)
+        iT = np.ascontiguousarray(invT, np.float64)
+        cp = np.ascontiguousarray(cpos, np.float64)
+        st = np.ascontiguousarray(storage, np.int64)
+        pt = np.ascontiguousarray(prev_t, np.float64)
+        pw = np.ascontiguousarray(prev_w, np.int32)
+        ot = np.zeros(len(st))
+        ow = np.zeros(len(st), np.int32)
+        am = np.zeros(len(st), np.uint8)
+        self.L.ora_ref_integrate_voxels(C.byref(vol), C.byref(cam), vx.ctypes.data, iT.ctypes.data,
+                                        cp.ctypes.data, st.ctypes.data, len(st), pt.ctypes.data,
+                                        pw.ctypes.data, ot.ctypes.data, ow.ctypes.data,
+                                        am.ctypes.data)
+        return ot, ow, am
+
+    def integrate_full(self, vol, cam, vertex, invT, cpos, trunc):
+        n = vol.n
+        t = np.full((n + 1) * n * n, trunc, np.float32)
+        w = np.zeros((n + 1) * n * n, np.uint8)
+        vx = np.ascontiguousarray(vertex, np.float64)
+        iT = np.ascontiguousarray(invT, np.float64)
+        cp = np.ascontiguousarray(cpos, np.float64)
+        self.L.ora_ref_integrate_full(C.byref(vol), C.byref(cam), vx.ctypes.data, iT.ctypes.data,
+                                      cp.ctypes.data, t.ctypes.data, w.ctypes.data)
+        return t, w
+
+    def raycast(self, vol, tsdf, cam, T, cpos):
+        T_ = np.ascontiguousarray(T, np.float64)
+        cp = np.ascontiguousarray(cpos, np.float64)
+        v = np.zeros((cam.h, cam.w, 3))
+        nn = np.zeros((cam.h, cam.w, 3))
+        am = np.zeros((cam.h, cam.w), np.uint8)
+        self.L.ora_ref_raycast(C.byref(vol), tsdf.ctypes.data, C.byref(cam), T_.ctypes.data,
+                               cp.ctypes.data, v.ctypes.data, nn.ctypes.data, am.ctypes.data)
+        return v, nn, am
+
+    def icp_system(self, cam, depth, new_v, new_n, model_v, model_n, invT):
+        args = [np.ascontiguousarray(a, np.float64) for a in (new_v, new_n, model_v, model_n, invT)]
+        d = np.ascontiguousarray(depth, np.uint16)
+        o36, o6, a36, a6 = np.zeros(36), np.zeros(6), np.zeros(36), np.zeros(6)
+        self.L.ora_ref_icp_system(C.byref(cam), d.ctypes.data, *[a.ctypes.data for a in args],
+                                  o36.ctypes.data, o6.ctypes.data, a36.ctypes.data, a6.ctypes.data)
+        return o36, o6, a36, a6
+
+    def compose(self, xopt, T, full):
+        x = np.ascontiguousarray(xopt, np.float64)
+        T_ = np.array(T, np.float64, copy=True).reshape(16)
+        F = np.array(full, np.float64, copy=True).reshape(16)
+        self.L.ora_ref_compose(x.ctypes.data, T_.ctypes.data, F.ctypes.data)
+        return T_.reshape(4, 4), F.reshape(4, 4)
 
 
 class CpuTracker:

@@ -51,6 +51,82 @@ static inline int near_half(double a, double margin) {
   return fabs(f - 0.5) < margin;
 }
 
+
+/* ---------------------------------------------------------------------------
+ * Helpers shared by the main oracle and the reference-semantics functions
+ * below (which are pinned against the reference's own kernels), so that the
+ * pinning covers the arithmetic both use.
+ * ------------------------------------------------------------------------ */
+
+/* convertVoxelsToWorld (Source/src/VolumeIntegrator.cu:40-48): centre of
+ * voxel i of n over a cube of edge `size` centred at 0. */
+static inline double voxel_centre(double size, int n, int i) {
+  double ratio = size / n;
+  return i * ratio - 0.5 * size + 0.5 * ratio;
+}
+
+/* CameraToImage (Source/include/CudaUtilities.cuh:9-21): u = (fx X + cx Z) / Z. */
+static inline void cam_project(double fx, double fy, double cx, double cy, double X, double Y,
+                               double Z, double *u, double *v) {
+  *u = (fx * X + cx * Z) / Z;
+  *v = (fy * Y + cy * Z) / Z;
+}
+
+/* Truncation of VolumeIntegrator.cu:148-160: returns 0 when the voxel is not
+ * updated (SDF < -trunc), else 1 with the truncated value in *t. */
+static inline int tsdf_truncate(double sdf, double trunc, double *t) {
+  if (sdf > 0.0) {
+    *t = sdf < trunc ? sdf : trunc;
+    return 1;
+  }
+  if (sdf >= -trunc) {
+    *t = sdf;
+    return 1;
+  }
+  return 0;
+}
+
+/* Running average with weight 1 (VolumeIntegrator.cu:165-166). */
+static inline void tsdf_average(double prev, unsigned w, double t, unsigned max_w, double *out,
+                                unsigned *w_out) {
+  *out = (prev * (double)w + t) / (double)(w + 1);
+  *w_out = w + 1 < max_w ? w + 1 : max_w;
+}
+
+/* Point-to-plane row of d_find_corresponding (Source/src/ICP.cu:186-201):
+ * A = [n_s x d, n_s], b = n_s . (s - d). */
+static inline void icp_row_terms(const double *ns, const double *d, const double *s, double *a,
+                                 double *b) {
+  a[0] = ns[1] * d[2] - ns[2] * d[1];
+  a[1] = ns[2] * d[0] - ns[0] * d[2];
+  a[2] = ns[0] * d[1] - ns[1] * d[0];
+  a[3] = ns[0]; a[4] = ns[1]; a[5] = ns[2];
+  *b = ns[0] * (s[0] - d[0]) + ns[1] * (s[1] - d[1]) + ns[2] * (s[2] - d[2]);
+}
+
+/* Incremental transform of Cpu_buildNewTransformMatrix (Source/src/ICP.cu:266-290):
+ * R = Rz(g) Ry(b) Rx(a), t = (tx, ty, tz), from xo = (a, b, g, tx, ty, tz). */
+static void euler_increment(const double *xo, double *D) {
+  double al = xo[0], be = xo[1], ga = xo[2];
+  double ca = cos(al), sa = sin(al), cb = cos(be), sb = sin(be), cg = cos(ga), sg = sin(ga);
+  double M[16] = {cg * cb, -sg * ca + cg * sb * sa, sg * sa + cg * sb * ca, xo[3],
+                  sg * cb, cg * ca + sg * sb * sa,  -cg * sa + sg * sb * ca, xo[4],
+                  -sb,     cb * sa,                 cb * ca,                 xo[5],
+                  0.0,     0.0,                     0.0,                     1.0};
+  memcpy(D, M, sizeof(M));
+}
+
+static void matmul4(const double *A, const double *B, double *C) {
+  double T[16];
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) {
+      double a = 0.0;
+      for (int k = 0; k < 4; ++k) a += A[4 * i + k] * B[4 * k + j];
+      T[4 * i + j] = a;
+    }
+  memcpy(C, T, sizeof(T));
+}
+
 /* ------------------------------------------------------------------------
  * Bilateral filter: Tomasi & Manduchi (ICCV 1998) on the raw depth, square
  * window of half-width `radius`, Gaussian spatial (sigma_s px) and range
@@ -237,7 +313,7 @@ static inline uint32_t vox_pack(R t, uint32_t weight, int storage) {
 int64_t ora_integrate(const ora_vol *v, uint32_t *words, const ora_cam *c, const uint16_t *depth,
                       const double *P, uint8_t *ambig) {
   const int n = v->n;
-  const double vs = v->size / n, org = -0.5 * v->size, T = v->trunc;
+  const double T = v->trunc;
   const double cpos[3] = {P[3], P[7], P[11]};
   int64_t updated = 0;
 #pragma omp parallel for schedule(dynamic, 1) reduction(+ : updated)
@@ -246,7 +322,8 @@ int64_t ora_integrate(const ora_vol *v, uint32_t *words, const ora_cam *c, const
       for (int k = 0; k < n; ++k) {
         size_t idx = ((size_t)i * n + j) * n + k;
         int amb = 0;
-        R pw[3] = {(R)(org + vs * (i + 0.5)), (R)(org + vs * (j + 0.5)), (R)(org + vs * (k + 0.5))};
+        R pw[3] = {(R)voxel_centre(v->size, n, i), (R)voxel_centre(v->size, n, j),
+                   (R)voxel_centre(v->size, n, k)};
         R dlt[3] = {pw[0] - (R)cpos[0], pw[1] - (R)cpos[1], pw[2] - (R)cpos[2]};
         R X = (R)P[0] * dlt[0] + (R)P[4] * dlt[1] + (R)P[8] * dlt[2];
         R Y = (R)P[1] * dlt[0] + (R)P[5] * dlt[1] + (R)P[9] * dlt[2];
@@ -257,8 +334,9 @@ int64_t ora_integrate(const ora_vol *v, uint32_t *words, const ora_cam *c, const
         int upd = 0;
         R sn = 0;
         if (Z < 0 && -Z >= (R)c->dmin && -Z <= (R)c->dmax) {
-          R uf = (R)c->fx * X / Z + (R)c->cx;
-          R vf = (R)c->fy * Y / Z + (R)c->cy;
+          double ud, vd;
+          cam_project(c->fx, c->fy, c->cx, c->cy, X, Y, Z, &ud, &vd);
+          R uf = (R)ud, vf = (R)vd;
           if (ambig && (near_half(uf, 1e-3) || near_half(vf, 1e-3))) amb = 1;
           int pu = round_ref(uf), pv = round_ref(vf);
           if (!(pu < 2 || pu >= c->w - 2 || pv < 2 || pv >= c->h - 2)) {
@@ -269,9 +347,10 @@ int64_t ora_integrate(const ora_vol *v, uint32_t *words, const ora_cam *c, const
               R rr = (R)sqrt((double)(dlt[0] * dlt[0] + dlt[1] * dlt[1] + dlt[2] * dlt[2]));
               R sdf = lam * (R)D - rr;
               if (ambig && fabs((double)sdf + T) < 1e-3) amb = 1;
-              if (sdf >= -(R)T) {
+              double tt;
+              if (tsdf_truncate((double)sdf, T, &tt)) {
                 upd = 1;
-                sn = (sdf < (R)T ? sdf : (R)T) / (R)T;
+                sn = (R)(tt / T);
               }
             }
           }
@@ -282,8 +361,10 @@ int64_t ora_integrate(const ora_vol *v, uint32_t *words, const ora_cam *c, const
         uint32_t word = words[idx];
         uint32_t wt = word >> 16;
         R told = wt ? vox_value(word, v->storage) : 0;
-        R tn = (told * (R)wt + sn) / (R)(wt + 1);
-        uint32_t wn = wt + 1 < (uint32_t)v->max_w ? wt + 1 : (uint32_t)v->max_w;
+        double tnd;
+        unsigned wn;
+        tsdf_average((double)told, wt, (double)sn, (unsigned)v->max_w, &tnd, &wn);
+        R tn = (R)tnd;
         words[idx] = vox_pack(tn, wn, v->storage);
       }
     }
@@ -519,11 +600,13 @@ static int icp_row(const ora_cam *lc, const R *frame, const R *s, const R *ns, c
   if (gate_amb)
     *gate_amb = fabs((double)len - dist) < 1e-3 || fabs((double)dn - nthr) < 1e-5 ||
                 fabs((double)dn - (1.0 + EPS_REF)) < 1e-6;
-  a[0] = ns[1] * d[2] - ns[2] * d[1];
-  a[1] = ns[2] * d[0] - ns[0] * d[2];
-  a[2] = ns[0] * d[1] - ns[1] * d[0];
-  a[3] = ns[0]; a[4] = ns[1]; a[5] = ns[2];
-  *b = -(ns[0] * e[0] + ns[1] * e[1] + ns[2] * e[2]);
+  {
+    double nsd[3] = {ns[0], ns[1], ns[2]}, dd[3] = {d[0], d[1], d[2]}, sd[3] = {s[0], s[1], s[2]};
+    double ad[6], bd;
+    icp_row_terms(nsd, dd, sd, ad, &bd);
+    for (int q = 0; q < 6; ++q) a[q] = (R)ad[q];
+    *b = (R)bd;
+  }
   if (!(len < (R)dist)) return gate_amb && *gate_amb ? 2 : 0;
   if (!(dn > (R)nthr && dn < (R)(1.0 + EPS_REF))) return gate_amb && *gate_amb ? 2 : 0;
   return 1;
@@ -639,20 +722,10 @@ int32_t ora_icp_step(const double *sys, double *P, double *minpiv) {
     for (int k = i + 1; k < 6; ++k) t -= L[k][i] * x[k];
     x[i] = t / L[i][i];
   }
-  double al = -x[0], be = -x[1], ga = -x[2];
-  double ca = cos(al), sa = sin(al), cb = cos(be), sb = sin(be), cg = cos(ga), sg = sin(ga);
-  double D[16] = {cg * cb, -sg * ca + cg * sb * sa, sg * sa + cg * sb * ca, x[3],
-                  sg * cb, cg * ca + sg * sb * sa,  -cg * sa + sg * sb * ca, x[4],
-                  -sb,     cb * sa,                 cb * ca,                 x[5],
-                  0.0,     0.0,                     0.0,                     1.0};
-  double O[16];
-  memcpy(O, P, sizeof(O));
-  for (int i = 0; i < 4; ++i)
-    for (int j = 0; j < 4; ++j) {
-      double a = 0.0;
-      for (int k = 0; k < 4; ++k) a += D[4 * i + k] * O[4 * k + j];
-      P[4 * i + j] = a;
-    }
+  double xo[6] = {-x[0], -x[1], -x[2], x[3], x[4], x[5]};
+  double D[16];
+  euler_increment(xo, D);
+  matmul4(D, P, P);
   return 0;
 }
 
@@ -759,3 +832,304 @@ int32_t ora_tracker_process(ora_tracker *t, const uint16_t *depth) {
 void ora_tracker_pose(const ora_tracker *t, double *pose) { memcpy(pose, t->pose, sizeof(t->pose)); }
 
 uint32_t *ora_tracker_volume(ora_tracker *t) { return t->words; }
+
+/* ===========================================================================
+ * Reference semantics. These restate the reference's kernels as they are
+ * (float storage, uint8 weights, nearest-voxel raycast, single-pass
+ * correspondences), in FP64, for comparison with the reference's own kernels
+ * run on the same inputs (tests/golden/ref_*.npz). They share the helpers
+ * above with the main oracle.
+ * ======================================================================== */
+
+#define REF_BAD 3.4028234663852886e38 /* BAD_VERTEX = FLT_MAX (Constants.h:36) */
+
+static inline int ref_bad(const double *v) {
+  return v[0] == REF_BAD || v[1] == REF_BAD || v[2] == REF_BAD;
+}
+
+/* d_convertDepthToWorldVertices + d_convertDepthToWorldNormals
+ * (Source/src/CameraSupport/CameraHandler.cu:65-132) with the inverse
+ * intrinsics the caller passes (m_invIntrinsic). */
+void ora_ref_convert(const ora_refcam *c, const uint16_t *depth, const double *T, double *vertex,
+                     double *normal) {
+  const int w = c->w, h = c->h;
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      size_t p = (size_t)y * w + x;
+      double D = depth[p];
+      double *v = vertex + 3 * p;
+      if (fabs(D) < c->dmin || fabs(D) > c->dmax) {
+        v[0] = v[1] = v[2] = REF_BAD;
+        continue;
+      }
+      double d = -D;  /* ImageToCamera with depth -newDepth (CameraHandler.cu:87) */
+      double cam[3] = {d * (c->ifx * x + c->icx), d * (c->ify * y + c->icy), d};
+      for (int r = 0; r < 3; ++r)
+        v[r] = T[4 * r] * cam[0] + T[4 * r + 1] * cam[1] + T[4 * r + 2] * cam[2] + T[4 * r + 3];
+    }
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      size_t p = (size_t)y * w + x;
+      double *n = normal + 3 * p;
+      n[0] = n[1] = n[2] = 0.0;
+      const double *v = vertex + 3 * p;
+      if (ref_bad(v) || x + 1 >= w || y + 1 >= h) continue;
+      const double *a = vertex + 3 * (p + 1), *b = vertex + 3 * (p + w);
+      if (ref_bad(a) || ref_bad(b)) continue;
+      double e1[3] = {a[0] - v[0], a[1] - v[1], a[2] - v[2]};
+      double e2[3] = {b[0] - v[0], b[1] - v[1], b[2] - v[2]};
+      double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                      e1[0] * e2[1] - e1[1] * e2[0]};
+      double l2 = cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2];
+      if (l2 == 0.0) continue;  /* normalize keeps the zero vector (cutil_math.h:1131-1137) */
+      double il = 1.0 / sqrt(l2);
+      n[0] = cr[0] * il; n[1] = cr[1] * il; n[2] = cr[2] * il;
+    }
+}
+
+/* One voxel of d_integrateVolume (VolumeIntegrator.cu:119-166) against a world
+ * vertex map: returns 1 and the truncated SDF when the voxel is updated. */
+static int ref_voxel_sdf(const ora_refvol *v, const ora_refcam *c, const double *vertex,
+                         const double *invT, const double *cpos, int x, int y, int z, double *t,
+                         int *amb) {
+  double p[3] = {voxel_centre(v->world, v->n, x), voxel_centre(v->world, v->n, y),
+                 voxel_centre(v->world, v->n, z)};
+  double cam[3];
+  for (int r = 0; r < 3; ++r)
+    cam[r] = invT[4 * r] * p[0] + invT[4 * r + 1] * p[1] + invT[4 * r + 2] * p[2] + invT[4 * r + 3];
+  if (fabs(cam[2]) < 1e-6) return 0; /* CameraToImage returns BAD_VERTEX; the frustum test rejects it */
+  double u, w_;
+  cam_project(c->fx, c->fy, c->cx, c->cy, cam[0], cam[1], cam[2], &u, &w_);
+  if (amb && (near_half(u, 1e-3) || near_half(w_, 1e-3) || fabs(fabs(cam[2]) - c->dmin) < 1e-2 ||
+              fabs(fabs(cam[2]) - c->dmax) < 1e-2))
+    *amb = 1;
+  int pu = round_ref((R)u), pv = round_ref((R)w_);
+  /* notInFrustum (VolumeIntegrator.cu:12-16) */
+  if (pu < 2 || pu >= c->w - 2 || pv < 2 || pv >= c->h - 2 || fabs(cam[2]) > c->dmax ||
+      fabs(cam[2]) < c->dmin)
+    return 0;
+  const double *dv = vertex + 3 * ((size_t)pv * c->w + pu);
+  if (ref_bad(dv)) return 0;
+  double a2 = 0.0, b2 = 0.0;
+  for (int r = 0; r < 3; ++r) {
+    a2 += (dv[r] - cpos[r]) * (dv[r] - cpos[r]);
+    b2 += (p[r] - cpos[r]) * (p[r] - cpos[r]);
+  }
+  double sdf = sqrt(a2) - sqrt(b2); /* VolumeIntegrator.cu:146 */
+  if (amb && fabs(sdf + v->trunc) < 1e-3) *amb = 1;
+  return tsdf_truncate(sdf, v->trunc, t);
+}
+
+/* d_integrateVolume at the given storage indices (x*n*n + y*n + z, x up to
+ * n): with v->b1 the kernel's storage shift applies (voxel x lives in slab
+ * x + 1, VolumeIntegrator.cu:115-123). prev_* are the stored values before the
+ * call; out_* after. */
+void ora_ref_integrate_voxels(const ora_refvol *v, const ora_refcam *c, const double *vertex,
+                              const double *invT, const double *cpos, const int64_t *storage,
+                              int64_t count, const double *prev_tsdf, const int32_t *prev_w,
+                              double *out_tsdf, int32_t *out_w, uint8_t *ambig) {
+  const int64_t n = v->n;
+#pragma omp parallel for schedule(static)
+  for (int64_t q = 0; q < count; ++q) {
+    int64_t s = storage[q];
+    int sx = (int)(s / (n * n)), sy = (int)((s / n) % n), sz = (int)(s % n);
+    int x = v->b1 ? sx - 1 : sx;
+    out_tsdf[q] = prev_tsdf[q];
+    out_w[q] = prev_w[q];
+    int amb = 0;
+    double t;
+    if (x >= 0 && x < n && ref_voxel_sdf(v, c, vertex, invT, cpos, x, sy, sz, &t, &amb)) {
+      double o;
+      unsigned wo;
+      tsdf_average(prev_tsdf[q], (unsigned)prev_w[q], t, (unsigned)v->max_w, &o, &wo);
+      out_tsdf[q] = (double)(float)o; /* the reference stores float */
+      out_w[q] = (int32_t)wo;
+    }
+    if (ambig) ambig[q] = (uint8_t)amb;
+  }
+}
+
+/* The whole float volume (storage of (n + 1) n^2 elements), for the raycast. */
+void ora_ref_integrate_full(const ora_refvol *v, const ora_refcam *c, const double *vertex,
+                            const double *invT, const double *cpos, float *tsdf, uint8_t *w) {
+  const int n = v->n;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int x = 0; x < n; ++x)
+    for (int y = 0; y < n; ++y)
+      for (int z = 0; z < n; ++z) {
+        double t;
+        if (!ref_voxel_sdf(v, c, vertex, invT, cpos, x, y, z, &t, NULL)) continue;
+        size_t s = ((size_t)(v->b1 ? x + 1 : x) * n + y) * n + z;
+        double o;
+        unsigned wo;
+        tsdf_average(tsdf[s], w[s], t, (unsigned)v->max_w, &o, &wo);
+        tsdf[s] = (float)o;
+        w[s] = (uint8_t)wo;
+      }
+}
+
+/* d_raycast (Source/src/Raycaster.cu:97-230) with its fixed constants
+ * (maxSteps 850, tstep 1.5 mm, zPlane -1, stop at tfar - 2): nearest-voxel
+ * samples, the first tsdf <= 0 is the surface, central-difference normal at
+ * that voxel (zero on the volume faces). `tsdf` is the storage array read by
+ * slab floor(position). */
+void ora_ref_raycast(const ora_refvol *v, const float *tsdf, const ora_refcam *c, const double *T,
+                     const double *cpos, double *vertex, double *normal, uint8_t *ambig) {
+  const int n = v->n;
+  const double half = 0.5 * v->world;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int y = 0; y < c->h; ++y)
+    for (int x = 0; x < c->w; ++x) {
+      size_t p = (size_t)y * c->w + x;
+      double *vo = vertex + 3 * p, *no = normal + 3 * p;
+      int amb = 0;
+      /* ray: pixel at z = -1 in camera space, to world, minus the origin (:117-125) */
+      double cc[3] = {-(c->ifx * x + c->icx), -(c->ify * y + c->icy), -1.0};
+      double d[3];
+      for (int r = 0; r < 3; ++r)
+        d[r] = T[4 * r] * cc[0] + T[4 * r + 1] * cc[1] + T[4 * r + 2] * cc[2] + T[4 * r + 3] - cpos[r];
+      double dl = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      for (int r = 0; r < 3; ++r) d[r] /= dl;
+      /* intersectBox (:35-55) */
+      double tmin[3], tmax[3];
+      for (int r = 0; r < 3; ++r) {
+        double inv = 1.0 / d[r];
+        double tb = inv * (-half - cpos[r]), tt = inv * (half - cpos[r]);
+        tmin[r] = tt < tb ? tt : tb;
+        tmax[r] = tt < tb ? tb : tt;
+      }
+      double tnear = fmax(fmax(tmin[0], tmin[1]), fmax(tmin[0], tmin[2]));
+      double tfar = fmin(fmin(tmax[0], tmax[1]), fmin(tmax[0], tmax[2]));
+      no[0] = no[1] = no[2] = 0.0;
+      if (!(tfar > tnear)) {
+        vo[0] = vo[1] = vo[2] = REF_BAD;
+        if (ambig) ambig[p] = (uint8_t)(fabs(tfar - tnear) < 1e-3);
+        continue;
+      }
+      if (tnear < 0.0) tnear = 0.0;
+      double t = tnear;
+      double start[3] = {cpos[0] + d[0] * tnear, cpos[1] + d[1] * tnear, cpos[2] + d[2] * tnear};
+      double surf[3] = {REF_BAD, REF_BAD, REF_BAD};
+      int flag = 0, cur[3] = {-1, -1, -1};
+      for (int s = 1; s < 850; ++s) {
+        double pos[3];
+        for (int r = 0; r < 3; ++r) pos[r] = start[r] + s * (d[r] * 1.5);
+        double gg[3];
+        for (int r = 0; r < 3; ++r) {
+          gg[r] = (pos[r] / v->world + 0.5) * n;
+          cur[r] = (int)floor(gg[r]);
+        }
+        if (cur[0] < 0 || cur[0] >= n || cur[1] < 0 || cur[1] >= n || cur[2] < 0 || cur[2] >= n)
+          break;
+        float val = tsdf[((size_t)cur[0] * n + cur[1]) * n + cur[2]];
+        if (ambig) {
+          if (fabs(val) < 1e-4) amb = 1;
+          /* a sample within FP32 rounding of a voxel face matters only when
+           * the voxel across the face would flip the surface decision */
+          for (int r = 0; r < 3; ++r) {
+            double fr = gg[r] - floor(gg[r]);
+            int alt = fr < 1e-4 ? -1 : (fr > 1.0 - 1e-4 ? 1 : 0);
+            if (!alt) continue;
+            int q[3] = {cur[0], cur[1], cur[2]};
+            q[r] += alt;
+            if (q[r] < 0 || q[r] >= n) { amb = 1; continue; }
+            float va = tsdf[((size_t)q[0] * n + q[1]) * n + q[2]];
+            if ((va <= 0.f) != (val <= 0.f)) amb = 1;
+          }
+        }
+        if (val <= 0.f) {
+          for (int r = 0; r < 3; ++r) surf[r] = pos[r];
+          flag = 1;
+          break;
+        }
+        t += 1.5;
+        if (ambig && fabs(t - (tfar - 2.0)) < 1e-3) amb = 1;
+        if (t > tfar - 2.0) break;
+      }
+      for (int r = 0; r < 3; ++r) vo[r] = surf[r];
+      if (flag) {
+        int X = cur[0], Y = cur[1], Z = cur[2];
+        if (!(X <= 0 || X + 1 >= n || Y <= 0 || Y + 1 >= n || Z <= 0 || Z + 1 >= n)) {
+#define RV(a, b, e) ((double)tsdf[((size_t)(a) * n + (b)) * n + (e)])
+          double g[3] = {RV(X + 1, Y, Z) - RV(X - 1, Y, Z), RV(X, Y + 1, Z) - RV(X, Y - 1, Z),
+                         RV(X, Y, Z + 1) - RV(X, Y, Z - 1)};
+#undef RV
+          double l2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+          if (l2 > 0.0) {
+            double il = 1.0 / sqrt(l2);
+            no[0] = g[0] * il; no[1] = g[1] * il; no[2] = g[2] * il;
+          }
+        }
+      }
+      if (ambig) ambig[p] = (uint8_t)amb;
+    }
+}
+
+/* d_find_corresponding (Source/src/ICP.cu:116-251) over the whole image:
+ * new depth tested at the model pixel's own offset (:139-149), projection of
+ * the model point with the current world-to-camera transform, rejection
+ * outside the image or at z >= -eps (:90-95), distance and normal gates
+ * (:179-181), row terms (:186-201). out36: AtA as the reference stores it
+ * (upper entries i <= j at [6 i + j]); out6: Atb; amb36/amb6 (may be NULL):
+ * sums of |terms| of pixels within rounding of a decision. */
+void ora_ref_icp_system(const ora_refcam *c, const uint16_t *new_depth, const double *new_vertex,
+                        const double *new_normal, const double *model_vertex,
+                        const double *model_normal, const double *invT, double *out36,
+                        double *out6, double *amb36, double *amb6) {
+  for (int q = 0; q < 36; ++q) { out36[q] = 0.0; if (amb36) amb36[q] = 0.0; }
+  for (int q = 0; q < 6; ++q) { out6[q] = 0.0; if (amb6) amb6[q] = 0.0; }
+  for (int y = 0; y < c->h; ++y)
+    for (int x = 0; x < c->w; ++x) {
+      size_t p = (size_t)y * c->w + x;
+      double nd0 = new_depth[p];
+      const double *s = model_vertex + 3 * p, *ns = model_normal + 3 * p;
+      if (fabs(nd0) < c->dmin || fabs(nd0) > c->dmax || ref_bad(s)) continue;
+      double sc[3];
+      for (int r = 0; r < 3; ++r)
+        sc[r] = invT[4 * r] * s[0] + invT[4 * r + 1] * s[1] + invT[4 * r + 2] * s[2] + invT[4 * r + 3];
+      if (fabs(sc[2]) < 1e-6) continue;
+      double u, w_;
+      cam_project(c->fx, c->fy, c->cx, c->cy, sc[0], sc[1], sc[2], &u, &w_);
+      int amb = near_half(u, 1e-3) || near_half(w_, 1e-3);
+      int col = round_ref((R)u), row = round_ref((R)w_);
+      if (col < 0 || col >= c->w || row < 0 || row >= c->h || sc[2] >= -1e-6) continue;
+      size_t o = (size_t)row * c->w + col;
+      const double *dv = new_vertex + 3 * o, *dn = new_normal + 3 * o;
+      double e[3] = {dv[0] - s[0], dv[1] - s[1], dv[2] - s[2]};
+      double len = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+      double dot = dn[0] * ns[0] + dn[1] * ns[1] + dn[2] * ns[2];
+      amb |= fabs(len - 25.0) < 1e-3 || fabs(dot - 0.65) < 1e-5;
+      if (!(len < 25.0 && dot > 0.65 && dot < 1.0 + 1e-6)) {
+        if (amb && amb36 && len < 1e30) {
+          double a[6], b;
+          icp_row_terms(ns, dv, s, a, &b);
+          for (int i = 0; i < 6; ++i) {
+            for (int j = i; j < 6; ++j) amb36[6 * i + j] += fabs(a[i] * a[j]);
+            amb6[i] += fabs(a[i] * b);
+          }
+        }
+        continue;
+      }
+      double a[6], b;
+      icp_row_terms(ns, dv, s, a, &b);
+      for (int i = 0; i < 6; ++i) {
+        for (int j = i; j < 6; ++j) out36[6 * i + j] += a[i] * a[j];
+        out6[i] += a[i] * b;
+      }
+      if (amb && amb36) {
+        for (int i = 0; i < 6; ++i) {
+          for (int j = i; j < 6; ++j) amb36[6 * i + j] += fabs(a[i] * a[j]);
+          amb6[i] += fabs(a[i] * b);
+        }
+      }
+    }
+}
+
+/* Cpu_buildNewTransformMatrix (Source/src/ICP.cu:266-321) in FP64:
+ * T <- dT T, full <- full dT. */
+void ora_ref_compose(const double *xopt, double *T, double *full) {
+  double D[16];
+  euler_increment(xopt, D);
+  matmul4(D, T, T);
+  matmul4(full, D, full);
+}

@@ -97,6 +97,39 @@ int32_t ora_icp_step(const double *sys, double *pose, double *min_pivot);
 int32_t ora_icp_track(const ora_cam *c, const ora_params *p, const ora_real *frame,
                       const ora_real *model, double *pose, int32_t *iterations);
 
+/* ---- reference semantics (pinned against the reference's own kernels) ---- */
+typedef struct ora_refcam {
+  int32_t w, h;
+  double fx, fy, cx, cy;      /* m_intrinsic */
+  double ifx, ify, icx, icy;  /* m_invIntrinsic */
+  double dmin, dmax;
+} ora_refcam;
+
+typedef struct ora_refvol {
+  int32_t n;       /* VOLUME_SIZE */
+  int32_t b1;      /* 1: the kernel's storage shift (voxel x in slab x + 1) */
+  double world;    /* worldVolume, mm */
+  double trunc;    /* TRUNCATION, mm */
+  int32_t max_w;   /* MAX_WEIGHT */
+  int32_t pad;
+} ora_refvol;
+
+void ora_ref_convert(const ora_refcam *c, const uint16_t *depth, const double *T, double *vertex,
+                     double *normal);
+void ora_ref_integrate_voxels(const ora_refvol *v, const ora_refcam *c, const double *vertex,
+                              const double *invT, const double *cpos, const int64_t *storage,
+                              int64_t count, const double *prev_tsdf, const int32_t *prev_w,
+                              double *out_tsdf, int32_t *out_w, uint8_t *ambig);
+void ora_ref_integrate_full(const ora_refvol *v, const ora_refcam *c, const double *vertex,
+                            const double *invT, const double *cpos, float *tsdf, uint8_t *w);
+void ora_ref_raycast(const ora_refvol *v, const float *tsdf, const ora_refcam *c, const double *T,
+                     const double *cpos, double *vertex, double *normal, uint8_t *ambig);
+void ora_ref_icp_system(const ora_refcam *c, const uint16_t *new_depth, const double *new_vertex,
+                        const double *new_normal, const double *model_vertex,
+                        const double *model_normal, const double *invT, double *out36,
+                        double *out6, double *amb36, double *amb6);
+void ora_ref_compose(const double *xopt, double *T, double *full);
+
 /* CPU tracker: the whole frame loop (used as the CPU baseline) */
 typedef struct ora_tracker ora_tracker;
 ora_tracker *ora_tracker_create(const ora_cam *c, const ora_vol *v, const ora_params *p,
