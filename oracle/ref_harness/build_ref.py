@@ -14,7 +14,8 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 OUT = HERE.parent / "_ref"
 REF = Path("/root/reference/Source")
-TUS = ["ref_camera.cu", "ref_volume.cu", "ref_general.cu", "ref_raycast.cu", "ref_icp.cu"]
+TUS = ["ref_camera.cu", "ref_volume.cu", "ref_general.cu", "ref_raycast.cu", "ref_icp.cu",
+       "ref_pipeline.cu"]
 
 
 def build() -> Path | None:
@@ -28,7 +29,7 @@ def build() -> Path | None:
     nvcc = "/usr/local/cuda/bin/nvcc"
     inc = ["-I", str(HERE / "stubs"), "-I", str(HERE), "-I", str(REF / "include"),
            "-I", str(REF / "include" / "Utils"), "-I", str(REF / "src"),
-           "-I", str(REF / "src" / "CameraSupport")]
+           "-I", str(REF / "src" / "CameraSupport"), "-I", str(REF / "include" / "Eigen" / "..")]
     objs = []
     procs = []
     for s in srcs:

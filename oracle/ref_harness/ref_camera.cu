@@ -41,3 +41,19 @@ extern "C" int ref_convert(const ref_cam *c, const uint16_t *h_depth, const floa
   cudaFree(dd); cudaFree(d.vertex); cudaFree(d.normal); cudaFree(dT);
   return 0;
 }
+
+// CameraHandler::m_params is a private static set by the CameraHandler
+// constructor (CameraHandler.cpp:121), which probes camera hardware; the
+// harness sets it directly. An explicit template instantiation may name a
+// private member, which yields its address here.
+template <typename Tag, typename Tag::type M>
+struct ref_member_address {
+  friend typename Tag::type ref_get(Tag) { return M; }
+};
+struct ref_params_tag {
+  typedef CameraParams *type;
+  friend type ref_get(ref_params_tag);
+};
+template struct ref_member_address<ref_params_tag, &CameraHandler::m_params>;
+
+extern "C" void ref_set_camera_params(const ref_cam *c) { *ref_get(ref_params_tag()) = to_params(c); }

@@ -93,5 +93,6 @@ extern "C" int ref_volume_read(const int64_t *idx, int64_t count, float *tsdf, u
   return 0;
 }
 
-// Whole arrays (N^3 + N^2 elements each) for the raycast harness.
+// Whole arrays (N^3 + N^2 elements each) for the raycast and pipeline harness.
 extern "C" void *ref_volume_device_tsdf(void) { return g_vol.tsdf; }
+void *ref_volume_device_weight(void) { return g_vol.w; }
