@@ -344,11 +344,12 @@ def stage_times(of, cfg, seq, depth_dev, order, args, dev):
     import torch
     vol = of.new_volume(cfg, dev)
     lam = of.lambda_table(cfg, dev)
+    scratch = of.integrate_scratch(cfg, dev)
     frame = of.new_pyramid(cfg, dev)
     model = of.new_pyramid(cfg, dev)
     ws = of.icp_workspace(cfg, dev)
     pose = torch.tensor(seq.poses[0].reshape(16), dtype=torch.float64, device=dev)
-    of.integrate(cfg, vol, depth_dev[order[0]], pose, lam)
+    of.integrate(cfg, vol, depth_dev[order[0]], pose, lam, scratch)
     of.raycast(cfg, vol, pose, model)
     acc = {"preprocess": 0.0, "icp": 0.0, "integrate": 0.0, "raycast": 0.0}
     s = torch.cuda.current_stream(dev)
@@ -363,7 +364,7 @@ def stage_times(of, cfg, seq, depth_dev, order, args, dev):
         ev[1].record(s)
         of.icp_track(cfg, frame, model, pose, ws)
         ev[2].record(s)
-        of.integrate(cfg, vol, d, pose, lam)
+        of.integrate(cfg, vol, d, pose, lam, scratch)
         ev[3].record(s)
         of.raycast(cfg, vol, pose, model)
         ev[4].record(s)
@@ -385,7 +386,7 @@ def stage_times(of, cfg, seq, depth_dev, order, args, dev):
         d = depth_dev[order[i]]
         if i > args.warmup and (i - args.warmup) % 10 == 0:
             upd.append(of.integrate_census(cfg, vol2, d, poses[i], lam))
-        of.integrate(cfg, vol2, d, poses[i], lam)
+        of.integrate(cfg, vol2, d, poses[i], lam, scratch)
     out = {f"{k}_ms": v / max(n, 1) for k, v in acc.items()}
     out["integrate_alg_bytes"] = 8.0 * float(np.mean(upd)) + 2.0 * cfg.width * cfg.height
     out["integrate_updated_voxels"] = float(np.mean(upd))

@@ -174,6 +174,22 @@ of_status_t of_lambda_bytes(const of_camera_t *cam, size_t *bytes);
 /* Fills the table: for every pixel, sqrt(1 + ((u-cx)/fx)^2 + ((v-cy)/fy)^2)
  * as an unevaluated float pair (hi, lo), computed in FP64. */
 of_status_t of_lambda_table(const of_camera_t *cam, float *d_lambda, of_stream_t stream);
+/* The same integration with whole-brick decisions: the call first bounds
+ * lambda * D over every 8x8 pixel tile of the frame, then lists the bricks
+ * in the frustum, skipping those entirely behind the surface beyond the
+ * truncation band and marking those entirely in free space (updated without
+ * per-voxel projection), then integrates the listed bricks. `d_scratch` is
+ * device scratch of of_integrate_scratch_bytes, 256-byte aligned; two calls
+ * in flight must not share it. The volume written is bit-identical to
+ * of_integrate's. Also replaces VolumeIntegrator::Integrate. */
+of_status_t of_integrate_tiled(const of_volume_desc_t *desc, void *d_volume,
+                               const of_camera_t *cam, const uint16_t *d_depth, int32_t pitch_px,
+                               const double *d_pose, const float *d_lambda, void *d_scratch,
+                               of_stream_t stream);
+/* Bytes of of_integrate_tiled's scratch: 768 + 8 B per 8x8 pixel tile
+ * (rounded up to 256) + 16 B per 8^3 brick. */
+of_status_t of_integrate_scratch_bytes(const of_volume_desc_t *desc, const of_camera_t *cam,
+                                       size_t *bytes);
 /* Counts the voxels one of_integrate call would update (same decisions, no
  * volume write). `d_count` is one device uint64. */
 of_status_t of_integrate_census(const of_volume_desc_t *desc, const void *d_volume,

@@ -149,7 +149,8 @@ class VolumeIntegrator {
  public:
   VolumeIntegrator(CameraParams *cameraParams, const Settings &s = Settings())
       : m_cam(to_camera(*cameraParams)), m_s(s),
-        m_lambda((size_t)m_cam.width * m_cam.height * 8), m_pose(16 * sizeof(double)) {
+        m_lambda(bytes_of(of_lambda_bytes, m_cam)), m_scratch(scratch_bytes(m_s, m_cam)),
+        m_pose(16 * sizeof(double)) {
     check(of_lambda_table(&m_cam, m_lambda.ptr, 0), "of_lambda_table");
   }
   // invTransform: world-to-camera float[16] on the device (the reference's
@@ -158,15 +159,26 @@ class VolumeIntegrator {
                  const CameraData &depthMap, const float3 * /*d_cameraPosition*/,
                  cudaStream_t stream = 0) {
     check(of_pose_from_float(invTransform, m_pose.ptr, 1, stream), "of_pose_from_float");
-    check(of_integrate(&m_s.volume, d_voxel_array, &m_cam, depthMap.depth, m_cam.width, m_pose.ptr,
-                       m_lambda.ptr, stream),
-          "of_integrate");
+    check(of_integrate_tiled(&m_s.volume, d_voxel_array, &m_cam, depthMap.depth, m_cam.width,
+                             m_pose.ptr, m_lambda.ptr, m_scratch.ptr, stream),
+          "of_integrate_tiled");
   }
 
  private:
+  static size_t bytes_of(of_status_t (*f)(const of_camera_t *, size_t *), const of_camera_t &c) {
+    size_t n = 0;
+    check(f(&c, &n), "size query");
+    return n;
+  }
+  static size_t scratch_bytes(const Settings &s, const of_camera_t &c) {
+    size_t n = 0;
+    check(of_integrate_scratch_bytes(&s.volume, &c, &n), "of_integrate_scratch_bytes");
+    return n;
+  }
   of_camera_t m_cam;
   Settings m_s;
   DeviceBuffer<float> m_lambda;
+  DeviceBuffer<unsigned char> m_scratch;
   DeviceBuffer<double> m_pose;
 };
 

@@ -89,6 +89,10 @@ _SIGS = {
                                  c_stream]),
     "of_integrate": (c_status, [C.POINTER(VolumeDesc), P, C.POINTER(Camera), P, C.c_int32, P, P,
                                 c_stream]),
+    "of_integrate_tiled": (c_status, [C.POINTER(VolumeDesc), P, C.POINTER(Camera), P, C.c_int32,
+                                      P, P, P, c_stream]),
+    "of_integrate_scratch_bytes": (c_status, [C.POINTER(VolumeDesc), C.POINTER(Camera),
+                                              C.POINTER(C.c_size_t)]),
     "of_lambda_bytes": (c_status, [C.POINTER(Camera), C.POINTER(C.c_size_t)]),
     "of_lambda_table": (c_status, [C.POINTER(Camera), P, c_stream]),
     "of_integrate_census": (c_status, [C.POINTER(VolumeDesc), P, C.POINTER(Camera), P, C.c_int32,

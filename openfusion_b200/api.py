@@ -150,11 +150,29 @@ def preprocess(cfg: Config, depth, frame=None):
     return frame
 
 
-def integrate(cfg: Config, vol, depth, pose, lam):
-    """VolumeIntegrator::Integrate: fuse `depth` at FP64 device pose `pose`."""
-    N.check("of_integrate", N.lib().of_integrate(C.byref(cfg.volume()), _ptr(vol),
-                                                 C.byref(cfg.camera()), _ptr(depth), cfg.width,
-                                                 _ptr(pose), _ptr(lam), _stream()))
+def integrate_scratch(cfg: Config, device="cuda"):
+    """Scratch of of_integrate_tiled (tile depth bounds and brick work list)."""
+    import torch
+    n = C.c_size_t()
+    N.check("of_integrate_scratch_bytes",
+            N.lib().of_integrate_scratch_bytes(C.byref(cfg.volume()), C.byref(cfg.camera()),
+                                               C.byref(n)))
+    return torch.empty(n.value, dtype=torch.uint8, device=device)
+
+
+def integrate(cfg: Config, vol, depth, pose, lam, scratch=None):
+    """VolumeIntegrator::Integrate: fuse `depth` at FP64 device pose `pose`.
+    With `scratch` (integrate_scratch) whole bricks are decided from per-tile
+    depth bounds (of_integrate_tiled); the volume written is the same."""
+    if scratch is None:
+        N.check("of_integrate", N.lib().of_integrate(C.byref(cfg.volume()), _ptr(vol),
+                                                     C.byref(cfg.camera()), _ptr(depth), cfg.width,
+                                                     _ptr(pose), _ptr(lam), _stream()))
+    else:
+        N.check("of_integrate_tiled",
+                N.lib().of_integrate_tiled(C.byref(cfg.volume()), _ptr(vol), C.byref(cfg.camera()),
+                                           _ptr(depth), cfg.width, _ptr(pose), _ptr(lam),
+                                           _ptr(scratch), _stream()))
 
 
 def integrate_census(cfg: Config, vol, depth, pose, lam) -> int:

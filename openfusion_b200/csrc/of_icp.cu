@@ -283,201 +283,295 @@ struct IcpPlan {
   IcpLevel lv[kMaxLevels];
   int levels;
   float dist_thresh, normal_thresh;
+  int cache_pts;  // model points a block keeps in shared memory per level
 };
 
-// Grid-wide barrier for a co-resident grid: arrival counter + generation.
-// The wait is bounded; on timeout the workspace error flag is set.
-__device__ __forceinline__ void grid_barrier(IcpWorkspace *ws, unsigned nexpect) {
+// Grid-wide barrier for a co-resident grid. The arrival counter only grows
+// within a frame (the begin kernel zeroes it): barrier k of the frame is
+// passed once it reaches k * nexpect, so a barrier costs one atomic per block
+// plus the polling. The wait is bounded; on timeout the workspace error flag
+// is set.
+__device__ __forceinline__ void grid_barrier(IcpWorkspace *ws, unsigned target) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned *gen = &ws->bar_gen;
-    unsigned g = *gen;
     __threadfence();
-    if (atomicAdd(&ws->bar_count, 1u) == nexpect - 1) {
-      ws->bar_count = 0;
-      __threadfence();
-      atomicAdd(&ws->bar_gen, 1u);
-    } else {
-      unsigned spins = 0;
-      while (*gen == g) {
-        if (++spins > kSpinLimit) {
-          atomicExch(&ws->error, 1);
-          break;
-        }
-        __nanosleep(32);
+    atomicAdd(&ws->bar_count, 1u);
+    volatile unsigned *cnt = &ws->bar_count;
+    unsigned spins = 0;
+    while ((int)(*cnt - target) < 0) {
+      if (++spins > kSpinLimit) {
+        atomicExch(&ws->error, 1);
+        break;
       }
+      __nanosleep(32);
     }
     __threadfence();
   }
   __syncthreads();
 }
 
-__device__ __forceinline__ double shfl_d(double v, int src) {
-  return __shfl_sync(0xffffffffu, v, src);
+// 1 / d for a positive FP64 d by Newton's iteration r <- r + r (1 - d r)
+// from the FP32 reciprocal: each step squares the relative error
+// (2^-23 -> 2^-46 -> below FP64 rounding).
+__device__ __forceinline__ double recip_pos(double d) {
+  const float df = (float)d;
+  if (!(df > 1e-30f && df < 1e30f)) return 1.0 / d;
+  double r = (double)__frcp_rn(df);
+  double e = fma(-d, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-d, r, 1.0);
+  return fma(r, e, r);
 }
 
-// Warp-parallel FP64 solve of the 6x6 normal equations (21 upper entries and
-// 6 right-hand sides in tot[0..26], inliers in tot[28]) and the SE(3) update
-// of P (row-major 4x4, shared memory). All 32 lanes of one warp call it; lane
-// i < 6 owns row i. LDL^T factorisation (one reciprocal per column, no square
-// roots; the pivots d_j equal the squared Cholesky pivots), forward and back
-// substitution by shuffles, the three sincos in three lanes, and the 4x4
-// product with one entry per lane. Returns the warp-uniform success flag;
-// *minpiv gets min d_j / max H_ii. Same singularity rule as chol_solve6.
-__device__ bool warp_solve_update(const float *tot, double *P, double *minpiv) {
-  const int lane = threadIdx.x & 31;
-  const int row = lane < 6 ? lane : 5;
-  double h[6];
-#pragma unroll
-  for (int j = 0; j < 6; ++j) {
-    int a = row < j ? row : j, b = row < j ? j : row;
-    h[j] = (double)tot[a * 6 - a * (a - 1) / 2 + (b - a)];
+// sin and cos from their Maclaurin series (Horner in x^2): through x^13 and
+// x^14 the truncation error for |x| <= 1/4 is below 1e-20, far under FP64
+// rounding. Larger angles use the library.
+__device__ __forceinline__ void sincos_small(double x, double *s, double *c) {
+  if (!(fabs(x) <= 0.25)) {
+    sincos(x, s, c);
+    return;
   }
+  const double x2 = x * x;
+  double ps = -1.0 / 6227020800.0;            // -1/13!
+  ps = fma(ps, x2, 1.0 / 39916800.0);         // 1/11!
+  ps = fma(ps, x2, -1.0 / 362880.0);          // -1/9!
+  ps = fma(ps, x2, 1.0 / 5040.0);             // 1/7!
+  ps = fma(ps, x2, -1.0 / 120.0);             // -1/5!
+  ps = fma(ps, x2, 1.0 / 6.0);                // 1/3!
+  // sin x = x - x^3 q(x^2) with q = 1/3! - x^2/5! + x^4/7! - ... + x^10/13!
+  *s = fma(-x * x2, ps, x);
+  double pc = 1.0 / 87178291200.0;            // 1/14!
+  pc = fma(pc, x2, -1.0 / 479001600.0);       // -1/12!
+  pc = fma(pc, x2, 1.0 / 3628800.0);          // 1/10!
+  pc = fma(pc, x2, -1.0 / 40320.0);           // -1/8!
+  pc = fma(pc, x2, 1.0 / 720.0);              // 1/6!
+  pc = fma(pc, x2, -1.0 / 24.0);              // -1/4!
+  pc = fma(pc, x2, 0.5);                      // 1/2!
+  // cos x = 1 - x2/2! + x2^2/4! - ... = 1 - x2 (1/2! - x2/4! + ...)
+  *c = fma(-x2, pc, 1.0);
+}
+
+// One-thread FP64 solve of the 6x6 normal equations (21 upper entries and 6
+// right-hand sides in tot[0..26], inliers in tot[28]) and the SE(3) update of
+// P (row-major 4x4). LDL^T factorisation (its pivots d_j equal the squared
+// Cholesky pivots, so the singularity rule is the Cholesky solve's: a pivot
+// not above 1e-12 x the largest diagonal entry, a non-finite pivot, or fewer
+// than 6 inliers), forward and back substitution, rotation part negated
+// (ICP.cpp:162-168), dT = [Rz(g) Ry(b) Rx(a) | t] (ICP.cu:274-290), P <- dT P.
+// The unit-lower factor lives in `Ls` (36 doubles of shared memory) so that
+// the solve does not compete for the kernel's registers. Returns the success
+// flag; *minpiv gets min d_j / max H_ii.
+__device__ __forceinline__ int upper_index(int i, int j) {  // i <= j
+  return i * 6 - i * (i - 1) / 2 + (j - i);
+}
+__device__ __noinline__ bool lane_solve_update(const float *tot, double *P, double *Ls,
+                                               double *minpiv) {
   double dmax = 0.0;
 #pragma unroll
-  for (int i = 0; i < 6; ++i) dmax = fmax(dmax, (double)tot[i * 6 - i * (i - 1) / 2]);
+  for (int i = 0; i < 6; ++i) dmax = fmax(dmax, (double)tot[upper_index(i, i)]);
   bool ok = tot[28] >= 6.f && dmax > 0.0 && isfinite(dmax);
-  double L[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // row `row` of unit-lower L
-  double d[6], dinv[6];
+  const double inv_dmax = 1.0 / dmax;
+  double d[6], r[6];
   double mp = 1e300;
 #pragma unroll
   for (int j = 0; j < 6; ++j) {
-    // pivot d_j = H_jj - sum_k L_jk^2 d_k (lane j), broadcast
-    double s = h[j];
+    // L_ij d_j = H_ij - sum_k L_ik L_jk d_k for i >= j (i = j gives d_j)
 #pragma unroll
-    for (int k = 0; k < j; ++k) s -= L[k] * L[k] * d[k];
-    double dj = shfl_d(s, j);
-    mp = fmin(mp, dj / dmax);
-    ok = ok && (dj > 1e-12 * dmax) && isfinite(dj);
-    d[j] = dj;
-    dinv[j] = 1.0 / dj;
-    // L_ij = (H_ij - sum_k L_ik L_jk d_k) / d_j for rows i > j
-    double Lj[6];
+    for (int i = j; i < 6; ++i) {
+      double t = (double)tot[upper_index(j, i)];
 #pragma unroll
-    for (int k = 0; k < j; ++k) Lj[k] = shfl_d(L[k], j);
-    double t = h[j];
-#pragma unroll
-    for (int k = 0; k < j; ++k) t -= L[k] * Lj[k] * d[k];
-    if (row > j) L[j] = t * dinv[j];
-    if (row == j) L[j] = 1.0;
+      for (int k = 0; k < j; ++k) t = fma(-Ls[6 * i + k] * d[k], Ls[6 * j + k], t);
+      if (i == j) {
+        d[j] = t;
+        mp = fmin(mp, t * inv_dmax);
+        ok = ok && (t > 1e-12 * dmax) && isfinite(t);
+        r[j] = recip_pos(fmax(t, 1e-300));
+      } else {
+        Ls[6 * i + j] = t * r[j];
+      }
+    }
   }
   *minpiv = ok ? mp : fmin(mp, 0.0);
   if (!ok) return false;
-  // forward: L z = g (unit diagonal), then y = z / d
-  double z[6];
+  double z[6], x[6];
 #pragma unroll
   for (int i = 0; i < 6; ++i) {
     double t = (double)tot[21 + i];
 #pragma unroll
-    for (int k = 0; k < i; ++k) t -= L[k] * z[k];
-    z[i] = shfl_d(t, i);
+    for (int k = 0; k < i; ++k) t = fma(-Ls[6 * i + k], z[k], t);
+    z[i] = t;
   }
-  // back: L^T x = z / d; the sum over rows k > i gathers L_ki from lane k
-  double x[6];
 #pragma unroll
   for (int i = 5; i >= 0; --i) {
-    double c = 0.0;
-    if (lane > i && lane < 6) {
+    double t = z[i] * r[i];
 #pragma unroll
-      for (int k = i + 1; k < 6; ++k)
-        if (lane == k) c = L[i] * x[k];
-    }
-#pragma unroll
-    for (int o = 4; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    c = shfl_d(c, 0) ;
-    x[i] = z[i] * dinv[i] - c;
+    for (int k = i + 1; k < 6; ++k) t = fma(-Ls[6 * k + i], x[k], t);
+    x[i] = t;
   }
-  // rotation part negated (ICP.cpp:162-168): alpha, beta, gamma = -x[0..2]
-  double sv = 0.0, cv = 1.0;
-  if (lane < 3) sincos(-x[lane], &sv, &cv);
-  const double sa = shfl_d(sv, 0), ca = shfl_d(cv, 0);
-  const double sb = shfl_d(sv, 1), cb = shfl_d(cv, 1);
-  const double sg = shfl_d(sv, 2), cg = shfl_d(cv, 2);
-  // dT = [Rz(g) Ry(b) Rx(a) | t] (ICP.cu:274-290); lane l < 16 forms entry
-  // (l/4, l%4) of dT P
-  const int r = (lane >> 2) & 3, c = lane & 3;
-  double D[4];
-  if (r == 0) { D[0] = cg * cb; D[1] = -sg * ca + cg * sb * sa; D[2] = sg * sa + cg * sb * ca; D[3] = x[3]; }
-  else if (r == 1) { D[0] = sg * cb; D[1] = cg * ca + sg * sb * sa; D[2] = -cg * sa + sg * sb * ca; D[3] = x[4]; }
-  else if (r == 2) { D[0] = -sb; D[1] = cb * sa; D[2] = cb * ca; D[3] = x[5]; }
-  else { D[0] = 0.0; D[1] = 0.0; D[2] = 0.0; D[3] = 1.0; }
-  double acc = 0.0;
+  double sa, ca, sb, cb, sg, cg;
+  sincos_small(-x[0], &sa, &ca);
+  sincos_small(-x[1], &sb, &cb);
+  sincos_small(-x[2], &sg, &cg);
+  const double D[12] = {cg * cb, -sg * ca + cg * sb * sa, sg * sa + cg * sb * ca, x[3],
+                        sg * cb, cg * ca + sg * sb * sa,  -cg * sa + sg * sb * ca, x[4],
+                        -sb,     cb * sa,                 cb * ca,                 x[5]};
+  // column j of dT P depends only on column j of P: update in place, rows
+  // 0..2 (row 3 of both is 0 0 0 1)
 #pragma unroll
-  for (int k = 0; k < 4; ++k) acc += D[k] * P[4 * k + c];
-  __syncwarp();
-  if (lane < 16) P[lane] = acc;
-  __syncwarp();
+  for (int j = 0; j < 4; ++j) {
+    const double p0 = P[j], p1 = P[4 + j], p2 = P[8 + j], p3 = P[12 + j];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      P[4 * i + j] = fma(D[4 * i], p0, fma(D[4 * i + 1], p1, fma(D[4 * i + 2], p2, D[4 * i + 3] * p3)));
+  }
   return true;
 }
 
-// The whole multi-level ICP of one frame in one cooperative launch. Per
-// iteration: every block accumulates its pixels' rows (tree sums), writes 29
+// Point-to-plane row of one correspondence (ICP.cu:186-201) added to acc.
+__device__ __forceinline__ void add_row(float *acc, float4 s, float4 ns, float3 d) {
+  const float ex = d.x - s.x, ey = d.y - s.y, ez = d.z - s.z;
+  float a[6];
+  a[0] = ns.y * d.z - ns.z * d.y;
+  a[1] = ns.z * d.x - ns.x * d.z;
+  a[2] = ns.x * d.y - ns.y * d.x;
+  a[3] = ns.x; a[4] = ns.y; a[5] = ns.z;
+  const float b = -(ns.x * ex + ns.y * ey + ns.z * ez);
+  int k = 0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+#pragma unroll
+    for (int j = i; j < 6; ++j) { acc[k] = fmaf(a[i], a[j], acc[k]); ++k; }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) acc[21 + i] = fmaf(a[i], b, acc[21 + i]);
+  acc[27] = fmaf(b, b, acc[27]);
+  acc[28] += 1.f;
+}
+
+// Data association of one model point (ICP.cu:90-95, :152-181): the frame
+// pixel it projects to, or -1.
+__device__ __forceinline__ int associate(const Rigid &w2c, const Cam &cam, float4 s) {
+  const float3 sc = apply(w2c, make_float3(s.x, s.y, s.z));
+  if (sc.z >= -kEps) return -1;
+  const float rz = __frcp_rn(sc.z);
+  const int pu = __float2int_rd(fmaf(cam.fx * sc.x, rz, cam.cx) + 0.5f);
+  const int pv = __float2int_rd(fmaf(cam.fy * sc.y, rz, cam.cy) + 0.5f);
+  if ((unsigned)pu >= (unsigned)cam.w || (unsigned)pv >= (unsigned)cam.h) return -1;
+  return pv * cam.w + pu;
+}
+
+// Inlier test and row of a model point s, n_s and the frame point at its pixel.
+__device__ __forceinline__ void try_row(float *acc, const Rigid &c2w, float4 s, float4 ns,
+                                        float4 dc, float4 nc, float dist2, float nthr) {
+  if (dc.w == 0.f || nc.w == 0.f) return;
+  const float3 d = apply(c2w, make_float3(dc.x, dc.y, dc.z));
+  const float3 nd = rotate(c2w, make_float3(nc.x, nc.y, nc.z));
+  const float ex = d.x - s.x, ey = d.y - s.y, ez = d.z - s.z;
+  if (!(fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < dist2)) return;
+  const float dn = nd.x * ns.x + nd.y * ns.y + nd.z * ns.z;
+  if (!(dn > nthr && dn < 1.f + kEps)) return;
+  add_row(acc, s, ns, d);
+}
+
+// The whole multi-level ICP of one frame in one cooperative launch. Each
+// block owns a contiguous slice of every level's model pixels; at the start
+// of a level it copies the slice's valid model points (vertex, normal) into
+// shared memory in pixel order, up to the dynamic shared-memory capacity (the
+// rest of the slice is read from global memory at every iteration). Per
+// iteration: every block associates its points two at a time (both frame
+// gathers in flight together), accumulates the rows (tree sums), writes 29
 // partials, meets the others at one grid barrier, then reduces all blocks'
-// partials in the same fixed order and solves the 6x6 system itself, so every
-// block holds the same new pose without a second barrier. Partials alternate
-// between two buffers: a block can only overwrite buffer i%2 after the
-// barrier of iteration i+1, which every block reaches only after reading it.
+// partials in the same fixed order and one thread solves the 6x6 system, so
+// every block holds the same new pose without a second barrier. Partials
+// alternate between two buffers: a block can only overwrite buffer i%2 after
+// the barrier of iteration i+1, which every block reaches only after reading it.
 __global__ void __launch_bounds__(kFusedThreads, 1)
     k_icp_fused(IcpPlan plan, double *pose, IcpWorkspace *ws, of_icp_stats_t *stats) {
+  extern __shared__ float4 s_pts[];  // 2 per cached model point
   __shared__ double s_pose[16];
+  __shared__ double s_L[36];
   __shared__ Rigid s_c2w, s_w2c;
   __shared__ float s_red[kFusedThreads / 32][32];
   __shared__ float s_tot[32];
-  __shared__ int s_stop, s_inl, s_its, s_err;
+  __shared__ int s_warp_n[kFusedThreads / 32];
+  __shared__ int s_stop, s_inl, s_its, s_err, s_npts;
   __shared__ double s_res, s_piv;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int kWarps = kFusedThreads / 32;
   if (threadIdx.x < 16) s_pose[threadIdx.x] = pose[threadIdx.x];
-  if (threadIdx.x == 0) { s_stop = 0; s_err = 0; s_its = 0; s_inl = 0; s_res = 0.0; s_piv = 0.0; }
-  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_stop = 0; s_err = 0; s_its = 0; s_inl = 0; s_res = 0.0; s_piv = 0.0;
+    pose_to_rigid(pose, &s_c2w, &s_w2c);
+  }
+  __syncthreads();  // every thread reads s_stop / s_err / the pose below
   // blocks a barrier waits for: the grid, plus any arrivals held back by the
   // fault-injection hook (which then never come)
   const unsigned nexpect = gridDim.x + (unsigned)max(0, ws->hold_barrier);
+  const float dist2 = plan.dist_thresh * plan.dist_thresh, nthr = plan.normal_thresh;
   int iter_global = 0;
   for (int l = plan.levels - 1; l >= 0 && !s_stop && !s_err; --l) {
     const IcpLevel L = plan.lv[l];
-    for (int it = 0; it < L.iters; ++it) {
-      if (threadIdx.x == 0) pose_to_rigid(s_pose, &s_c2w, &s_w2c);
+    const int npx = L.mw * L.mh;
+    const int chunk = (npx + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int p0 = min((int)blockIdx.x * chunk, npx), p1 = min(p0 + chunk, npx);
+    const int pc = min(p1, p0 + plan.cache_pts);  // [p0, pc) cached, [pc, p1) not
+    // ---- cache this block's valid model points of the level, in pixel order
+    if (threadIdx.x == 0) s_npts = 0;
+    __syncthreads();
+    for (int base = p0; base < pc; base += kFusedThreads) {
+      const int p = base + threadIdx.x;
+      float4 s = make_float4(0.f, 0.f, 0.f, 0.f), ns = s;
+      bool valid = false;
+      if (p < pc) {
+        s = __ldg(L.model + 2 * p);
+        ns = __ldg(L.model + 2 * p + 1);
+        valid = s.w != 0.f && ns.w != 0.f;
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, valid);
+      if (lane == 0) s_warp_n[warp] = __popc(m);
       __syncthreads();
+      int off = s_npts;
+      for (int w = 0; w < warp; ++w) off += s_warp_n[w];
+      if (valid) {
+        const int slot = off + __popc(m & ((1u << lane) - 1u));
+        s_pts[2 * slot] = s;
+        s_pts[2 * slot + 1] = ns;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int w = 0; w < kWarps; ++w) tot += s_warp_n[w];
+        s_npts += tot;
+      }
+      __syncthreads();
+    }
+    const int n = s_npts;
+    for (int it = 0; it < L.iters; ++it) {
       float acc[kVals];
 #pragma unroll
       for (int v = 0; v < kVals; ++v) acc[v] = 0.f;
-      const int npx = L.mw * L.mh;
-      for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npx; p += gridDim.x * blockDim.x) {
-        float4 s = __ldg(L.model + 2 * p);
-        float4 ns = __ldg(L.model + 2 * p + 1);
+      // cached points, two per step
+      for (int i = threadIdx.x; i < n; i += 2 * kFusedThreads) {
+        const int j = i + kFusedThreads;
+        const int qA = associate(s_w2c, L.cam, s_pts[2 * i]);
+        const int qB = j < n ? associate(s_w2c, L.cam, s_pts[2 * j]) : -1;
+        float4 dA = make_float4(0.f, 0.f, 0.f, 0.f), cA = dA, dB = dA, cB = dA;
+        if (qA >= 0) { dA = __ldg(L.frame + 2 * qA); cA = __ldg(L.frame + 2 * qA + 1); }
+        if (qB >= 0) { dB = __ldg(L.frame + 2 * qB); cB = __ldg(L.frame + 2 * qB + 1); }
+        // the model points are read again from shared memory rather than
+        // held in registers across the gathers
+        asm volatile("" ::: "memory");
+        if (qA >= 0) try_row(acc, s_c2w, s_pts[2 * i], s_pts[2 * i + 1], dA, cA, dist2, nthr);
+        if (qB >= 0) try_row(acc, s_c2w, s_pts[2 * j], s_pts[2 * j + 1], dB, cB, dist2, nthr);
+      }
+      // the rest of the slice, from global memory
+      for (int p = pc + threadIdx.x; p < p1; p += kFusedThreads) {
+        const float4 s = __ldg(L.model + 2 * p);
+        const float4 ns = __ldg(L.model + 2 * p + 1);
         if (s.w == 0.f || ns.w == 0.f) continue;
-        float3 sc = apply(s_w2c, make_float3(s.x, s.y, s.z));
-        if (sc.z >= -kEps) continue;
-        float rz = __frcp_rn(sc.z);
-        int pu = __float2int_rd(fmaf(L.cam.fx * sc.x, rz, L.cam.cx) + 0.5f);
-        int pv = __float2int_rd(fmaf(L.cam.fy * sc.y, rz, L.cam.cy) + 0.5f);
-        if ((unsigned)pu >= (unsigned)L.cam.w || (unsigned)pv >= (unsigned)L.cam.h) continue;
-        int q = pv * L.cam.w + pu;
-        float4 dc = __ldg(L.frame + 2 * q);
-        float4 nc = __ldg(L.frame + 2 * q + 1);
-        if (dc.w == 0.f || nc.w == 0.f) continue;
-        float3 d = apply(s_c2w, make_float3(dc.x, dc.y, dc.z));
-        float3 nd = rotate(s_c2w, make_float3(nc.x, nc.y, nc.z));
-        float ex = d.x - s.x, ey = d.y - s.y, ez = d.z - s.z;
-        if (!(fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < plan.dist_thresh * plan.dist_thresh)) continue;
-        float dn = nd.x * ns.x + nd.y * ns.y + nd.z * ns.z;
-        if (!(dn > plan.normal_thresh && dn < 1.f + kEps)) continue;
-        float a[6];
-        a[0] = ns.y * d.z - ns.z * d.y;
-        a[1] = ns.z * d.x - ns.x * d.z;
-        a[2] = ns.x * d.y - ns.y * d.x;
-        a[3] = ns.x; a[4] = ns.y; a[5] = ns.z;
-        float b = -(ns.x * ex + ns.y * ey + ns.z * ez);
-        int k = 0;
-#pragma unroll
-        for (int i = 0; i < 6; ++i)
-#pragma unroll
-          for (int j = i; j < 6; ++j) { acc[k] = fmaf(a[i], a[j], acc[k]); ++k; }
-#pragma unroll
-        for (int i = 0; i < 6; ++i) acc[21 + i] = fmaf(a[i], b, acc[21 + i]);
-        acc[27] = fmaf(b, b, acc[27]);
-        acc[28] += 1.f;
+        const int q = associate(s_w2c, L.cam, s);
+        if (q < 0) continue;
+        try_row(acc, s_c2w, s, ns, __ldg(L.frame + 2 * q), __ldg(L.frame + 2 * q + 1), dist2,
+                nthr);
       }
       // pairwise sums: a recursive-halving exchange across the warp (lanes
       // trade half of their remaining values each step, 31 shuffles for 32
@@ -511,7 +605,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
           for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
         ws->fused_partials[buf][blockIdx.x][lane] = lane < kVals ? y[0] : 0.f;
       }
-      grid_barrier(ws, nexpect);
+      grid_barrier(ws, nexpect * (unsigned)(iter_global + 1));
       // a barrier that gave up ends this frame's tracking in every block
       if (threadIdx.x == 0) s_err = *((volatile int *)&ws->error);
       __syncthreads();
@@ -548,12 +642,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
 #pragma unroll
           for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
         s_tot[threadIdx.x] = y[0];
-      }
-      __syncthreads();
-      if (warp == 0) {
-        double minpiv = 0.0;
-        bool ok = warp_solve_update(s_tot, s_pose, &minpiv);
-        if (lane == 0) {
+        __syncwarp();
+        if (threadIdx.x == 0) {
+          double minpiv = 0.0;
+          const bool ok = lane_solve_update(s_tot, s_pose, s_L, &minpiv);
           s_its += 1;
           s_inl = (int)s_tot[28];
           s_res = (double)s_tot[27];
@@ -562,6 +654,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
             for (int i = 0; i < 16; ++i) s_pose[i] = ws->pose_init[i];
             s_stop = 1;
           }
+          pose_to_rigid(s_pose, &s_c2w, &s_w2c);
         }
       }
       __syncthreads();
@@ -660,18 +753,41 @@ static bool icp_params_ok(const of_icp_params_t *p) {
   return p->dist_thresh_mm > 0.f;
 }
 
-// Grid of the fused kernel: every block co-resident (cooperative launch).
-static int fused_grid() {
-  static int grid = 0;
-  if (grid == 0) {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_icp_fused, kFusedThreads, 0);
-    int g = sms * (per_sm < 1 ? 1 : per_sm);
-    grid = g > kFusedMaxBlocks ? kFusedMaxBlocks : g;
+// Launch shape of the fused kernel on the current device: every block
+// co-resident (cooperative launch), with room in shared memory for the
+// block's slice of the finest level's model points (up to kMaxCachePts).
+constexpr int kMaxCachePts = 6144;  // 192 KiB of points per block
+struct FusedShape {
+  int grid;       // co-resident blocks (may exceed kFusedMaxBlocks: then refused)
+  int cache_pts;
+  size_t smem;
+};
+static of_status_t fused_shape(const of_camera_t *cam, FusedShape *fs) {
+  constexpr int kMaxDevices = 64;
+  static int grid_of[kMaxDevices] = {};
+  static std::mutex mu;
+  int dev = 0;
+  OF_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return OF_ERR_INVALID_ARGUMENT;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (grid_of[dev] == 0) {
+      const int max_smem = kMaxCachePts * 2 * (int)sizeof(float4);
+      OF_CUDA_TRY(cudaFuncSetAttribute((const void *)k_icp_fused,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+      int sms = 0, per_sm = 0;
+      OF_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      OF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_icp_fused,
+                                                                kFusedThreads, max_smem));
+      grid_of[dev] = sms * (per_sm < 1 ? 1 : per_sm);
+    }
+    fs->grid = grid_of[dev];
   }
-  return grid;
+  const long npx = (long)cam->width * cam->height;
+  const long chunk = (npx + fs->grid - 1) / fs->grid;
+  fs->cache_pts = (int)(chunk < kMaxCachePts ? chunk : kMaxCachePts);
+  fs->smem = (size_t)fs->cache_pts * 2 * sizeof(float4);
+  return OF_OK;
 }
 
 // Launches the whole coarse-to-fine ICP of one frame: a begin kernel and one
@@ -683,9 +799,14 @@ of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, con
   of_status_t st = of_pyramid_layout(cam, ip->levels, &lay);
   if (st != OF_OK) return st;
   IcpWorkspace *ws = (IcpWorkspace *)d_ws;
+  FusedShape fs;
+  st = fused_shape(cam, &fs);
+  if (st != OF_OK) return st;
+  if (fs.grid > kFusedMaxBlocks) return OF_ERR_TOO_LARGE;
   IcpPlan plan;
   memset(&plan, 0, sizeof(plan));
   plan.levels = ip->levels;
+  plan.cache_pts = fs.cache_pts;
   plan.dist_thresh = ip->dist_thresh_mm;
   plan.normal_thresh = ip->normal_thresh;
   for (int l = 0; l < ip->levels; ++l) {
@@ -701,8 +822,8 @@ of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, con
   st = of_launch_status();
   if (st != OF_OK) return st;
   void *args[] = {&plan, &pose, &ws, &stats};
-  OF_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)k_icp_fused, dim3(fused_grid()),
-                                          dim3(kFusedThreads), args, 0, s));
+  OF_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)k_icp_fused, dim3(fs.grid),
+                                          dim3(kFusedThreads), args, fs.smem, s));
   return OF_OK;
 }
 
@@ -788,11 +909,10 @@ extern "C" of_status_t of_icp_track_static(const of_camera_t *cam, const of_icp_
     return OF_ERR_INVALID_ARGUMENT;
   // the array holds partials for kFusedMaxBlocks blocks: a device whose
   // co-resident grid would need more is refused
-  int dev = 0, sms = 0, per_sm = 0;
-  OF_CUDA_TRY(cudaGetDevice(&dev));
-  OF_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  OF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_icp_fused, kFusedThreads, 0));
-  if ((long)sms * (per_sm < 1 ? 1 : per_sm) > kFusedMaxBlocks) return OF_ERR_TOO_LARGE;
+  FusedShape fs;
+  of_status_t sh = fused_shape(cam, &fs);
+  if (sh != OF_OK) return sh;
+  if (fs.grid > kFusedMaxBlocks) return OF_ERR_TOO_LARGE;
   void *ws = nullptr;
   of_status_t st = static_icp_workspace(&ws);
   if (st != OF_OK) return st;

@@ -15,6 +15,10 @@
 // z-consecutive voxels and touches memory with one 16-byte load and store,
 // only when one of them is updated. A whole brick is skipped before any
 // memory access when its 8 corner voxel centres lie outside one frustum plane.
+// of_integrate_tiled adds whole-brick decisions from per-tile bounds of the
+// depth frame: bricks that lie entirely behind the surface (beyond the
+// truncation band) are skipped, bricks that lie entirely in free space are
+// updated with +1 without projecting a voxel; the volume written is the same.
 // The SDF of voxels near the truncation band is evaluated with float-pair
 // arithmetic so that the stored int16 value matches an FP64 evaluation to
 // within one quantisation step.
@@ -34,6 +38,7 @@ struct IntegrateSetup {
   float oc_hi[3], oc_lo[3];  // (origin + vs/2 - c) per axis, float pair
   double mb[9];    // world-to-camera rotation scaled by 8 voxels (one brick), FP64
   double ob[3];    // camera-space centre of voxel (0,0,0), FP64
+  float cw[3];     // camera centre in world space
 };
 
 __device__ void make_setup(const double *P, const of_volume_desc_t &d, IntegrateSetup &S) {
@@ -53,6 +58,7 @@ __device__ void make_setup(const double *P, const of_volume_desc_t &d, Integrate
     double oc = org - c[a];
     S.oc_hi[a] = (float)oc;
     S.oc_lo[a] = (float)(oc - (double)S.oc_hi[a]);
+    S.cw[a] = (float)c[a];
   }
   S.vs_hi = (float)vs;
   S.vs_lo = (float)(vs - (double)S.vs_hi);
@@ -98,90 +104,220 @@ __device__ void make_planes(const double *P, const Cam &cam, Plane *pl) {
 }
 
 constexpr int kChunk = 32;  // bricks tested per batch (one warp ballot)
+constexpr int kTile = 8;    // depth-bound tiles are 8x8 pixels
+constexpr int kMaxTiles = 64;  // a brick whose footprint covers more tiles is evaluated per voxel
+// How a listed brick is integrated (of_integrate_tiled's work list).
+constexpr int kModeFull = 0;        // per-voxel test, with the frustum/border checks
+constexpr int kModeInside = 1;      // per-voxel test; every voxel is inside the frustum
+constexpr int kModeFront = 2;       // free space: +1 where the voxel's pixel holds a valid depth
+constexpr int kModeFrontDense = 3;  // free space, every pixel it reaches valid: +1 everywhere
 
-template <int STORAGE, bool CENSUS>
-__global__ void __launch_bounds__(256, 4) k_integrate(uint32_t *__restrict__ vol, of_volume_desc_t desc,
-                                                   Cam cam, const uint16_t *__restrict__ depth,
-                                                   int pitch, const double *__restrict__ pose,
-                                                   const float2 *__restrict__ lam,
-                                                   unsigned long long *count) {
-  __shared__ IntegrateSetup S;
-  __shared__ Plane planes[6];
-  __shared__ int s_list[kChunk][4];  // visible bricks of a batch: b, bx, by, bz
-  __shared__ int s_nvis;
-  __shared__ unsigned int s_count;
-  if (threadIdx.x == 0) {
-    make_setup(pose, desc, S);
-    make_planes(pose, cam, planes);
-    s_count = 0;
-  }
+// The per-frame constants of of_integrate_tiled, computed once (FP64) by its
+// first step and copied to shared memory by the next two.
+struct FrameSetup {
+  IntegrateSetup S;
+  Plane planes[6];
+};
+
+__device__ __forceinline__ void load_setup(const FrameSetup *g, FrameSetup *s) {
+  static_assert(sizeof(FrameSetup) % 4 == 0, "word copy");
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(g);
+  uint32_t *dst = reinterpret_cast<uint32_t *>(s);
+  for (int i = threadIdx.x; i < (int)(sizeof(FrameSetup) / 4); i += blockDim.x) dst[i] = src[i];
   __syncthreads();
-  const int nb = desc.resolution >> 3;
-  const int nbricks = nb * nb * nb;
-  const int half = threadIdx.x >> 7;
-  const int t = threadIdx.x & 127;
+}
+
+// of_integrate_tiled, step 1. Per 8x8 pixel tile of the raw depth frame, one
+// warp: x = min and |y| = max of L = lambda * D over the tile's valid pixels
+// (+inf and 0 if there is none); y carries a minus sign (-0 included) when a
+// pixel of the tile is invalid. L is the same FP32 product the integration
+// compares |p - c| with.
+__global__ void __launch_bounds__(256) k_depth_tiles(Cam cam, const uint16_t *__restrict__ depth,
+                                                     int pitch, const float2 *__restrict__ lam,
+                                                     float2 *__restrict__ tiles, int tiles_x,
+                                                     int ntiles, unsigned int *list_count,
+                                                     const double *__restrict__ pose,
+                                                     of_volume_desc_t desc, FrameSetup *setup) {
+  const int tile = blockIdx.x * 8 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  const int lx = t >> 4, ly = (t >> 1) & 7, lz0 = (t & 1) * 4;
-  const float T = desc.trunc_mm, inv_T = 1.0f / desc.trunc_mm;
-  const float dspan = cam.dmax - cam.dmin;
-  const unsigned uspan = (unsigned)(cam.w - 4), vspan = (unsigned)(cam.h - 4);
-  const float vs = S.vs_hi;
-  const float org = -0.5f * desc.size_mm;
-  const float hext = 3.5f * vs + 1e-3f;  // half extent of a brick's voxel centres
-  unsigned int my_count = 0;
-  const float cxh = cam.cx + 0.5f, cyh = cam.cy + 0.5f;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    // for the next two steps: an empty work list, the frame's setup
+    *list_count = 0;
+    make_setup(pose, desc, setup->S);
+    make_planes(pose, cam, setup->planes);
+  }
+  if (tile >= ntiles) return;  // warp-uniform
+  const int tx = tile % tiles_x, ty = tile / tiles_x;
   const float dlo = fmaxf(cam.dmin, 0.5f), dhi = cam.dmax;
-  const int nb2 = nb * nb;
-  uint8_t *flags = brick_flags(vol, desc.resolution);
-  // Bricks are dealt round-robin (brick b goes to CTA b mod grid), so every
-  // CTA gets a spatially spread, statistically equal share of the frustum.
-  // Per batch, warp 0 tests 32 of the CTA's bricks (one lane each) and
-  // compacts the visible ones into a shared list; the two 128-thread halves
-  // then take list entries alternately.
-  const int G = gridDim.x;
-  for (int q0 = 0; blockIdx.x + q0 * G < nbricks; q0 += kChunk) {
-    if (threadIdx.x < 32) {
-      int b = blockIdx.x + (q0 + lane) * G;
-      bool vis = false;
-      int bx = 0, by = 0, bz = 0;
-      if (b < nbricks) {
-        bz = b % nb; by = (b / nb) % nb; bx = b / nb2;
-        float cx = fmaf(vs, (float)(8 * bx) + 4.0f, org);
-        float cy = fmaf(vs, (float)(8 * by) + 4.0f, org);
-        float cz = fmaf(vs, (float)(8 * bz) + 4.0f, org);
-        vis = true;
+  float lmin = __int_as_float(0x7f800000), lmax = 0.f;
+  bool all_valid = true;
 #pragma unroll
-        for (int q = 0; q < 6; ++q) {
-          const Plane pl = planes[q];
-          float e = fmaf(pl.nx, cx, fmaf(pl.ny, cy, fmaf(pl.nz, cz, pl.d)));
-          float r = hext * (fabsf(pl.nx) + fabsf(pl.ny) + fabsf(pl.nz));
-          vis &= (e - r) <= 0.f;
-        }
+  for (int k = 0; k < 2; ++k) {
+    const int u = tx * kTile + (lane & 7), v = ty * kTile + (lane >> 3) + 4 * k;
+    if (u < cam.w && v < cam.h) {
+      const float D = (float)__ldg(depth + (size_t)v * pitch + u);
+      const float L = __ldg(reinterpret_cast<const float *>(lam) + 2 * (v * cam.w + u)) * D;
+      const bool valid = D >= dlo && D <= dhi;
+      all_valid &= valid;
+      if (valid) {
+        lmin = fminf(lmin, L);
+        lmax = fmaxf(lmax, L);
       }
-      unsigned m = __ballot_sync(0xffffffffu, vis);
-      if (vis) {
-        int slot = __popc(m & ((1u << lane) - 1u));
-        s_list[slot][0] = b; s_list[slot][1] = bx; s_list[slot][2] = by; s_list[slot][3] = bz;
-      }
-      if (lane == 0) s_nvis = __popc(m);
     }
-    __syncthreads();
-    const int nvis = s_nvis;
-    for (int e = half; e < nvis; e += 2) {
-      const int b = s_list[e][0], bx = s_list[e][1], by = s_list[e][2], bz = s_list[e][3];
-      // camera-space centre of the brick's voxel (0,0,0), FP64 then rounded:
-      // per-voxel offsets from it stay below 8 voxels, so the FP32 position
-      // error is about one rounding of the brick base.
-      const double fbx = (double)bx, fby = (double)by, fbz = (double)bz;
-      const float BX = (float)fma(S.mb[0], fbx, fma(S.mb[1], fby, fma(S.mb[2], fbz, S.ob[0])));
-      const float BY = (float)fma(S.mb[3], fbx, fma(S.mb[4], fby, fma(S.mb[5], fbz, S.ob[1])));
-      const float BZ = (float)fma(S.mb[6], fbx, fma(S.mb[7], fby, fma(S.mb[8], fbz, S.ob[2])));
-      float X0 = fmaf(S.m[0], (float)lx, fmaf(S.m[1], (float)ly, BX));
-      float Y0 = fmaf(S.m[3], (float)lx, fmaf(S.m[4], (float)ly, BY));
-      float Z0 = fmaf(S.m[6], (float)lx, fmaf(S.m[7], (float)ly, BZ));
-      float tnew[4];
-      unsigned upd = 0;
-      bool near = false;
+  }
+  all_valid = __all_sync(0xffffffffu, all_valid);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lmin = fminf(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
+    lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+  }
+  if (lane == 0) tiles[tile] = make_float2(lmin, all_valid ? lmax : -lmax);
+}
+
+// Whole-brick decision from the tile bounds (one thread per brick). Returns
+// -1 when no voxel of the brick can be updated, else the brick's mode:
+// kModeFront(Dense) when every voxel whose pixel holds a valid depth is
+// updated with tsdf' = +1 (free space), kModeInside / kModeFull when the
+// voxels must be evaluated one by one, with or without the per-voxel frustum
+// checks. Every verdict is conservative: each carries margins far above the
+// FP32 rounding of the per-voxel test, so the volume written is the one the
+// per-voxel test alone gives.
+//   skip:  for every voxel with a valid depth D in its pixel,
+//          |p - c| > L_max + T + slack >= L + T + slack  (the per-voxel skip);
+//   inside: every voxel projects inside the border and depth range;
+//   front: inside, and for every valid pixel it can reach
+//          |p - c| < L_min - T - slack; dense: every pixel it can reach is valid.
+// The pixel footprint is bounded by the projections of the 8 corner voxel
+// centres (a box projects inside the hull of its corners' projections), one
+// pixel wider on each side.
+__device__ int classify_brick(const IntegrateSetup &S, const Cam &cam, const float2 *tiles,
+                              int tiles_x, float T, float hext, float cx, float cy, float cz,
+                              int bx, int by, int bz) {
+  // distance range from the camera to the brick's voxel centres (world box)
+  const float ex = fabsf(cx - S.cw[0]), ey = fabsf(cy - S.cw[1]), ez = fabsf(cz - S.cw[2]);
+  const float ax = fmaxf(ex - hext, 0.f), ay = fmaxf(ey - hext, 0.f), az = fmaxf(ez - hext, 0.f);
+  const float fx_ = ex + hext, fy_ = ey + hext, fz_ = ez + hext;
+  const float rlo = sqrtf(fmaf(ax, ax, fmaf(ay, ay, az * az))) * (1.f - 1e-5f) - 0.01f;
+  const float rhi = sqrtf(fmaf(fx_, fx_, fmaf(fy_, fy_, fz_ * fz_))) * (1.f + 1e-5f) + 0.01f;
+  // camera-space corners: voxel (8b + 7i, 8b + 7j, 8b + 7k)
+  const float gx = (float)(8 * bx), gy = (float)(8 * by), gz = (float)(8 * bz);
+  const float X0 = fmaf(S.m[0], gx, fmaf(S.m[1], gy, fmaf(S.m[2], gz, S.o[0])));
+  const float Y0 = fmaf(S.m[3], gx, fmaf(S.m[4], gy, fmaf(S.m[5], gz, S.o[1])));
+  const float Z0 = fmaf(S.m[6], gx, fmaf(S.m[7], gy, fmaf(S.m[8], gz, S.o[2])));
+  float umin = 3.4e38f, umax = -3.4e38f, vmin = 3.4e38f, vmax = -3.4e38f;
+  float zmin = 3.4e38f, zmax = -3.4e38f;  // of -Z
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const float i = (c & 4) ? 7.f : 0.f, j = (c & 2) ? 7.f : 0.f, k = (c & 1) ? 7.f : 0.f;
+    const float X = fmaf(S.m[0], i, fmaf(S.m[1], j, fmaf(S.m[2], k, X0)));
+    const float Y = fmaf(S.m[3], i, fmaf(S.m[4], j, fmaf(S.m[5], k, Y0)));
+    const float Z = fmaf(S.m[6], i, fmaf(S.m[7], j, fmaf(S.m[8], k, Z0)));
+    const float rz = 1.0f / Z;
+    const float u = fmaf(cam.fx * X, rz, cam.cx), v = fmaf(cam.fy * Y, rz, cam.cy);
+    umin = fminf(umin, u); umax = fmaxf(umax, u);
+    vmin = fminf(vmin, v); vmax = fmaxf(vmax, v);
+    zmin = fminf(zmin, -Z); zmax = fmaxf(zmax, -Z);
+  }
+  if (!(zmin > 1.0f)) return kModeFull;  // reaches behind the camera: no bounded footprint
+  // (clamped so that the integer pixel bounds cannot overflow)
+  const int pu0 = __float2int_rd(fmaxf(umin + 0.5f, -1e8f)) - 1;
+  const int pu1 = __float2int_rd(fminf(umax + 0.5f, 1e8f)) + 1;
+  const int pv0 = __float2int_rd(fmaxf(vmin + 0.5f, -1e8f)) - 1;
+  const int pv1 = __float2int_rd(fminf(vmax + 0.5f, 1e8f)) + 1;
+  const int tx0 = max(pu0, 0) / kTile, tx1 = min(pu1, cam.w - 1) / kTile;
+  const int ty0 = max(pv0, 0) / kTile, ty1 = min(pv1, cam.h - 1) / kTile;
+  if (pu1 < 0 || pv1 < 0 || pu0 > cam.w - 1 || pv0 > cam.h - 1) return -1;  // off the image
+  if ((tx1 - tx0 + 1) * (ty1 - ty0 + 1) > kMaxTiles) return kModeFull;
+  float lmin = 3.4e38f, lmax = 0.f;
+  bool dense = true;
+  for (int ty = ty0; ty <= ty1; ++ty)
+    for (int tx = tx0; tx <= tx1; ++tx) {
+      const float2 tb = __ldg(tiles + ty * tiles_x + tx);
+      lmin = fminf(lmin, tb.x);
+      lmax = fmaxf(lmax, fabsf(tb.y));
+      dense &= !signbit(tb.y);
+    }
+  const float farb = fmaf(lmax, 1.f + 1e-5f, T + 0.05f) * (1.f + 2e-5f) + 0.02f;
+  if (rlo > farb) return -1;
+  const bool inside = pu0 >= 2 && pu1 <= cam.w - 3 && pv0 >= 2 && pv1 <= cam.h - 3 &&
+                      zmin >= fmaf(zmin, 1e-5f, cam.dmin + 0.05f) &&
+                      zmax <= cam.dmax - fmaf(zmax, 1e-5f, 0.05f);
+  if (!inside) return kModeFull;
+  const float nearb = (fmaf(lmin, 1.f - 1e-5f, -T) - 0.05f) * (1.f - 2e-5f) - 0.02f;
+  if (!(rhi < nearb)) return kModeInside;
+  return dense ? kModeFrontDense : kModeFront;
+}
+
+// Per-thread constants of the voxel loop.
+struct VoxelConsts {
+  float T, inv_T, dspan, cxh, cyh, dlo, dhi;
+  unsigned uspan, vspan;
+  int lx, ly, lz0, nb;
+};
+
+__device__ __forceinline__ VoxelConsts voxel_consts(const of_volume_desc_t &desc, const Cam &cam,
+                                                    int t) {
+  VoxelConsts K;
+  K.T = desc.trunc_mm;
+  K.inv_T = 1.0f / desc.trunc_mm;
+  K.dspan = cam.dmax - cam.dmin;
+  K.cxh = cam.cx + 0.5f;
+  K.cyh = cam.cy + 0.5f;
+  K.dlo = fmaxf(cam.dmin, 0.5f);
+  K.dhi = cam.dmax;
+  K.uspan = (unsigned)(cam.w - 4);
+  K.vspan = (unsigned)(cam.h - 4);
+  K.lx = t >> 4;
+  K.ly = (t >> 1) & 7;
+  K.lz0 = (t & 1) * 4;
+  K.nb = desc.resolution >> 3;
+  return K;
+}
+
+// Camera-space centre of brick (bx, by, bz)'s voxel (0,0,0), FP64 then
+// rounded: per-voxel offsets from it stay below 8 voxels, so the FP32
+// position error is about one rounding of the brick base.
+__device__ __forceinline__ float3 brick_base(const IntegrateSetup &S, int bx, int by, int bz) {
+  const double fbx = (double)bx, fby = (double)by, fbz = (double)bz;
+  return make_float3((float)fma(S.mb[0], fbx, fma(S.mb[1], fby, fma(S.mb[2], fbz, S.ob[0]))),
+                     (float)fma(S.mb[3], fbx, fma(S.mb[4], fby, fma(S.mb[5], fbz, S.ob[1]))),
+                     (float)fma(S.mb[6], fbx, fma(S.mb[7], fby, fma(S.mb[8], fbz, S.ob[2]))));
+}
+
+// One brick, 128 threads: thread t owns voxels (lx, ly, lz0 .. lz0 + 3) of
+// brick b, whose voxel (0,0,0) sits at camera-space `base`. `mode` (kMode*)
+// says what is known of the brick: in the free-space modes a voxel is updated
+// with tsdf' = +1 when its pixel holds a valid depth (always, when dense),
+// with no ray length or distance evaluated; kModeInside drops the per-voxel
+// frustum checks.
+template <int STORAGE, bool CENSUS, bool EARLY_LOAD = false>
+__device__ __forceinline__ void integrate_brick(
+    uint32_t *__restrict__ vol, uint8_t *__restrict__ flags, const of_volume_desc_t &desc,
+    const Cam &cam, const uint16_t *__restrict__ depth, int pitch,
+    const float2 *__restrict__ lam, const IntegrateSetup &S, const VoxelConsts &K, int t,
+    int lane, int b, int bx, int by, int bz, int mode, float3 base, unsigned &my_count) {
+  const float T = K.T, inv_T = K.inv_T, dspan = K.dspan, cxh = K.cxh, cyh = K.cyh;
+  const float dlo = K.dlo, dhi = K.dhi;
+  const unsigned uspan = K.uspan, vspan = K.vspan;
+  const int lx = K.lx, ly = K.ly, lz0 = K.lz0, nb = K.nb;
+  float tnew[4];
+  unsigned upd = 0;
+  bool near = false;
+  uint4 *p4 = reinterpret_cast<uint4 *>(vol + ((size_t)b << 9)) + t;
+  uint4 wv = make_uint4(0u, 0u, 0u, 0u);
+  // listed bricks are nearly always updated: their words are loaded before
+  // the depth gathers so that the two memory round trips overlap
+  if (EARLY_LOAD && !CENSUS) wv = *p4;
+  if (mode == kModeFrontDense) {
+    upd = 0xfu;
+    tnew[0] = tnew[1] = tnew[2] = tnew[3] = 1.0f;
+    goto brick_done;
+  }
+  {
+      const bool check = mode == kModeFull;
+      float X0 = fmaf(S.m[0], (float)lx, fmaf(S.m[1], (float)ly, base.x));
+      float Y0 = fmaf(S.m[3], (float)lx, fmaf(S.m[4], (float)ly, base.y));
+      float Z0 = fmaf(S.m[6], (float)lx, fmaf(S.m[7], (float)ly, base.z));
       // phase 1: project the four voxels; phase 2: issue every gather before
       // any result is used; phase 3: decide
       float Xv[4], Yv[4], Zv[4];
@@ -200,13 +336,26 @@ __global__ void __launch_bounds__(256, 4) k_integrate(uint32_t *__restrict__ vol
         int pu = __float2int_rd(fmaf(cam.fx * X, rz, cxh));
         int pv = __float2int_rd(fmaf(cam.fy * Y, rz, cyh));
         // -Z in [dmin, dmax] (and Z < 0), pixel outside the 2-pixel border
-        bool ok = (-Z - cam.dmin <= dspan) && (-Z >= cam.dmin) &&
-                  (unsigned)(pu - 2) < uspan && (unsigned)(pv - 2) < vspan;
+        // (known for the whole brick in every mode but kModeFull)
+        bool ok = true;
+        if (check)
+          ok = (-Z - cam.dmin <= dspan) && (-Z >= cam.dmin) && (unsigned)(pu - 2) < uspan &&
+               (unsigned)(pv - 2) < vspan;
         inb |= ok ? (1u << m) : 0u;
         pix[m] = ok ? pv * cam.w + pu : 0;
         dix[m] = ok ? pv * pitch + pu : 0;
       }
       if (!inb) goto brick_done;
+      if (mode == kModeFront) {
+        // free space: a voxel whose pixel holds a valid depth gets +1
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const float D = __int_as_float(0x4B000000 | (int)__ldg(depth + dix[m])) - 8388608.0f;
+          tnew[m] = 1.0f;
+          if (((inb >> m) & 1u) && D >= dlo && D <= dhi) upd |= 1u << m;
+        }
+        goto brick_done;
+      }
       {
         float Dv[4], Lh[4];
         bool have_xy = false;
@@ -250,12 +399,12 @@ __global__ void __launch_bounds__(256, 4) k_integrate(uint32_t *__restrict__ vol
           tnew[m] = sn;
         }
       }
+      }
     brick_done:
       if (CENSUS) {
         my_count += __popc(upd);
       } else if (upd) {
-        uint4 *p4 = reinterpret_cast<uint4 *>(vol + ((size_t)b << 9)) + t;
-        uint4 wv = *p4;
+        if (!EARLY_LOAD) wv = *p4;
         uint32_t w4[4] = {wv.x, wv.y, wv.z, wv.w};
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
@@ -271,7 +420,9 @@ __global__ void __launch_bounds__(256, 4) k_integrate(uint32_t *__restrict__ vol
           w4[m] = VoxelCodec<STORAGE>::pack(tn, wn);
           near |= (w4[m] & 0xffffu) != VoxelCodec<STORAGE>::kOneBits;
         }
-        *p4 = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+        // saturated free space (+1 at the maximum weight) stays as it is
+        if (w4[0] != wv.x || w4[1] != wv.y || w4[2] != wv.z || w4[3] != wv.w)
+          *p4 = make_uint4(w4[0], w4[1], w4[2], w4[3]);
       }
       // a warp that wrote a non-saturated voxel flags the brick and its 26
       // neighbours (idempotent byte stores, lanes 0..26)
@@ -281,6 +432,77 @@ __global__ void __launch_bounds__(256, 4) k_integrate(uint32_t *__restrict__ vol
         if ((unsigned)qx < (unsigned)nb && (unsigned)qy < (unsigned)nb && (unsigned)qz < (unsigned)nb)
           flags[(qx * nb + qy) * nb + qz] = 1;
       }
+}
+
+// The per-voxel integration over every brick of the volume (of_integrate,
+// of_integrate_census). Persistent grid; bricks are dealt round-robin (brick b
+// goes to CTA b mod grid), so every CTA gets a spatially spread, statistically
+// equal share of the frustum. Per batch, warp 0 tests 32 of the CTA's bricks
+// against the frustum (one lane each) and compacts the visible ones into a
+// shared list; the two 128-thread halves then take list entries alternately.
+template <int STORAGE, bool CENSUS>
+__global__ void __launch_bounds__(256, 4) k_integrate(uint32_t *__restrict__ vol, of_volume_desc_t desc,
+                                                   Cam cam, const uint16_t *__restrict__ depth,
+                                                   int pitch, const double *__restrict__ pose,
+                                                   const float2 *__restrict__ lam,
+                                                   unsigned long long *count) {
+  __shared__ IntegrateSetup S;
+  __shared__ Plane planes[6];
+  __shared__ int s_list[kChunk][4];  // visible bricks of a batch: b, bx, by, bz
+  __shared__ int s_nvis;
+  __shared__ unsigned int s_count;
+  if (threadIdx.x == 0) {
+    make_setup(pose, desc, S);
+    make_planes(pose, cam, planes);
+    s_count = 0;
+  }
+  __syncthreads();
+  const int nb = desc.resolution >> 3;
+  const int nbricks = nb * nb * nb;
+  const int half = threadIdx.x >> 7;
+  const int t = threadIdx.x & 127;
+  const int lane = threadIdx.x & 31;
+  const VoxelConsts K = voxel_consts(desc, cam, t);
+  const float vs = S.vs_hi;
+  const float org = -0.5f * desc.size_mm;
+  const float hext = 3.5f * vs + 1e-3f;  // half extent of a brick's voxel centres
+  unsigned int my_count = 0;
+  const int nb2 = nb * nb;
+  uint8_t *flags = brick_flags(vol, desc.resolution);
+  const int G = gridDim.x;
+  for (int q0 = 0; blockIdx.x + q0 * G < nbricks; q0 += kChunk) {
+    if (threadIdx.x < 32) {
+      int b = blockIdx.x + (q0 + lane) * G;
+      bool vis = false;
+      int bx = 0, by = 0, bz = 0;
+      if (b < nbricks) {
+        bz = b % nb; by = (b / nb) % nb; bx = b / nb2;
+        float cx = fmaf(vs, (float)(8 * bx) + 4.0f, org);
+        float cy = fmaf(vs, (float)(8 * by) + 4.0f, org);
+        float cz = fmaf(vs, (float)(8 * bz) + 4.0f, org);
+        vis = true;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          const Plane pl = planes[q];
+          float e = fmaf(pl.nx, cx, fmaf(pl.ny, cy, fmaf(pl.nz, cz, pl.d)));
+          float r = hext * (fabsf(pl.nx) + fabsf(pl.ny) + fabsf(pl.nz));
+          vis &= (e - r) <= 0.f;
+        }
+      }
+      unsigned m = __ballot_sync(0xffffffffu, vis);
+      if (vis) {
+        int slot = __popc(m & ((1u << lane) - 1u));
+        s_list[slot][0] = b; s_list[slot][1] = bx; s_list[slot][2] = by; s_list[slot][3] = bz;
+      }
+      if (lane == 0) s_nvis = __popc(m);
+    }
+    __syncthreads();
+    const int nvis = s_nvis;
+    for (int e = half; e < nvis; e += 2) {
+      const int bx = s_list[e][1], by = s_list[e][2], bz = s_list[e][3];
+      integrate_brick<STORAGE, CENSUS>(vol, flags, desc, cam, depth, pitch, lam, S, K, t, lane,
+                                       s_list[e][0], bx, by, bz, kModeFull,
+                                       brick_base(S, bx, by, bz), my_count);
     }
     __syncthreads();
   }
@@ -292,14 +514,129 @@ __global__ void __launch_bounds__(256, 4) k_integrate(uint32_t *__restrict__ vol
   }
 }
 
+// of_integrate_tiled, step 2: one thread per brick. Frustum test, then the
+// whole-brick decision from the tile bounds; kept bricks are appended to the
+// work list (one atomic per warp) as {bx | by << 8 | bz << 16 | mode << 24,
+// camera-space base of the brick (3 floats)}.
+__global__ void __launch_bounds__(256) k_classify_bricks(of_volume_desc_t desc, Cam cam,
+                                                         const double *__restrict__ pose,
+                                                         const float2 *__restrict__ tiles,
+                                                         int tiles_x, uint4 *__restrict__ list,
+                                                         unsigned int *__restrict__ list_count,
+                                                         const FrameSetup *__restrict__ setup) {
+  __shared__ FrameSetup F;
+  load_setup(setup, &F);
+  const IntegrateSetup &S = F.S;
+  const Plane *planes = F.planes;
+  const int nb = desc.resolution >> 3;
+  const int nbricks = nb * nb * nb;
+  const int lane = threadIdx.x & 31;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const float vs = S.vs_hi;
+  const float org = -0.5f * desc.size_mm;
+  const float hext = 3.5f * vs + 1e-3f;
+  bool keep = false;
+  uint4 entry = make_uint4(0u, 0u, 0u, 0u);
+  if (b < nbricks) {
+    const int bz = b % nb, by = (b / nb) % nb, bx = b / (nb * nb);
+    const float cx = fmaf(vs, (float)(8 * bx) + 4.0f, org);
+    const float cy = fmaf(vs, (float)(8 * by) + 4.0f, org);
+    const float cz = fmaf(vs, (float)(8 * bz) + 4.0f, org);
+    keep = true;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const Plane pl = planes[q];
+      float e = fmaf(pl.nx, cx, fmaf(pl.ny, cy, fmaf(pl.nz, cz, pl.d)));
+      float r = hext * (fabsf(pl.nx) + fabsf(pl.ny) + fabsf(pl.nz));
+      keep &= (e - r) <= 0.f;
+    }
+    if (keep) {
+      const int cls = classify_brick(S, cam, tiles, tiles_x, desc.trunc_mm, hext, cx, cy, cz, bx,
+                                     by, bz);
+      keep = cls >= 0;
+      const float3 base = brick_base(S, bx, by, bz);
+      entry = make_uint4((uint32_t)bx | (uint32_t)by << 8 | (uint32_t)bz << 16 |
+                             (uint32_t)max(cls, 0) << 24,
+                         __float_as_uint(base.x), __float_as_uint(base.y), __float_as_uint(base.z));
+    }
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, keep);
+  if (m) {
+    const int leader = __ffs(m) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(list_count, (unsigned)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (keep) list[base + __popc(m & ((1u << lane) - 1u))] = entry;
+  }
+}
+
+// of_integrate_tiled, step 3: persistent grid over the work list, each
+// 128-thread half of a CTA takes one listed brick at a time.
+template <int STORAGE>
+__global__ void __launch_bounds__(256, 4) k_integrate_list(uint32_t *__restrict__ vol,
+                                                        of_volume_desc_t desc, Cam cam,
+                                                        const uint16_t *__restrict__ depth,
+                                                        int pitch, const double *__restrict__ pose,
+                                                        const float2 *__restrict__ lam,
+                                                        const uint4 *__restrict__ list,
+                                                        const unsigned int *__restrict__ list_count,
+                                                        const FrameSetup *__restrict__ setup) {
+  __shared__ FrameSetup F;
+  load_setup(setup, &F);
+  const IntegrateSetup &S = F.S;
+  const int n = (int)*list_count;
+  const int half = threadIdx.x >> 7;
+  const int t = threadIdx.x & 127;
+  const int lane = threadIdx.x & 31;
+  const VoxelConsts K = voxel_consts(desc, cam, t);
+  const int nb = K.nb;
+  uint8_t *flags = brick_flags(vol, desc.resolution);
+  unsigned my_count = 0;
+  for (int e = blockIdx.x * 2 + half; e < n; e += gridDim.x * 2) {
+    const uint4 en = __ldg(list + e);
+    const int bx = (int)(en.x & 0xffu), by = (int)((en.x >> 8) & 0xffu);
+    const int bz = (int)((en.x >> 16) & 0xffu), mode = (int)(en.x >> 24);
+    const int b = (bx * nb + by) * nb + bz;
+    integrate_brick<STORAGE, false, true>(
+        vol, flags, desc, cam, depth, pitch, lam, S, K, t, lane, b, bx, by, bz, mode,
+        make_float3(__uint_as_float(en.y), __uint_as_float(en.z), __uint_as_float(en.w)), my_count);
+  }
+}
+
+int tiles_x_of(const of_camera_t *cam) { return (cam->width + kTile - 1) / kTile; }
+int tiles_of(const of_camera_t *cam) {
+  return tiles_x_of(cam) * ((cam->height + kTile - 1) / kTile);
+}
+
+// Scratch of of_integrate_tiled: [0, 256) work-list count, [256, 768) the
+// frame setup, then the tile bounds (float2 per tile), then the work list
+// (16 B per brick).
+struct ScratchLayout {
+  size_t setup, tiles, list, total;
+};
+static_assert(sizeof(FrameSetup) <= 512, "frame setup slot");
+ScratchLayout scratch_layout(const of_volume_desc_t *d, const of_camera_t *cam) {
+  const size_t nb = (size_t)(d->resolution / 8);
+  ScratchLayout L;
+  L.setup = 256;
+  L.tiles = 768;
+  L.list = L.tiles + (((size_t)tiles_of(cam) * sizeof(float2) + 255) & ~(size_t)255);
+  L.total = L.list + nb * nb * nb * sizeof(uint4);
+  return L;
+}
+
+unsigned persistent_blocks(const of_volume_desc_t *d) {
+  size_t nb = (size_t)(d->resolution / 8);
+  size_t nbr = nb * nb * nb;
+  // 4 resident CTAs of 256 threads per SM
+  return (unsigned)(nbr < (size_t)kSmCount * 4 ? nbr : (size_t)kSmCount * 4);
+}
+
 template <bool CENSUS>
 of_status_t launch_integrate(const of_volume_desc_t *d, void *vol, const of_camera_t *cam,
                              const uint16_t *depth, int pitch, const double *pose,
                              const float *lam, unsigned long long *count, cudaStream_t s) {
-  size_t nb = (size_t)(d->resolution / 8);
-  size_t nbr = nb * nb * nb;
-  // persistent grid: 4 resident CTAs of 256 threads per SM
-  unsigned blocks = (unsigned)(nbr < (size_t)kSmCount * 4 ? nbr : (size_t)kSmCount * 4);
+  const unsigned blocks = persistent_blocks(d);
   Cam c = make_cam(*cam);
   if (d->storage == OF_TSDF_I16)
     k_integrate<OF_TSDF_I16, CENSUS><<<blocks, 256, 0, s>>>(
@@ -307,6 +644,34 @@ of_status_t launch_integrate(const of_volume_desc_t *d, void *vol, const of_came
   else
     k_integrate<OF_TSDF_F16, CENSUS><<<blocks, 256, 0, s>>>(
         (uint32_t *)vol, *d, c, depth, pitch, pose, (const float2 *)lam, count);
+  return of_launch_status();
+}
+
+of_status_t launch_integrate_tiled(const of_volume_desc_t *d, void *vol, const of_camera_t *cam,
+                                   const uint16_t *depth, int pitch, const double *pose,
+                                   const float *lam, void *scratch, cudaStream_t s) {
+  const ScratchLayout L = scratch_layout(d, cam);
+  unsigned int *list_count = (unsigned int *)scratch;
+  float2 *tiles = (float2 *)((char *)scratch + L.tiles);
+  uint4 *list = (uint4 *)((char *)scratch + L.list);
+  FrameSetup *setup = (FrameSetup *)((char *)scratch + L.setup);
+  Cam c = make_cam(*cam);
+  const int tx = tiles_x_of(cam), nt = tiles_of(cam);
+  k_depth_tiles<<<(nt + 7) / 8, 256, 0, s>>>(c, depth, pitch, (const float2 *)lam, tiles, tx, nt,
+                                              list_count, pose, *d, setup);
+  const size_t nb = (size_t)(d->resolution / 8);
+  const unsigned nbr = (unsigned)(nb * nb * nb);
+  k_classify_bricks<<<(nbr + 255) / 256, 256, 0, s>>>(*d, c, pose, tiles, tx, list, list_count,
+                                                       setup);
+  const unsigned blocks = persistent_blocks(d);
+  if (d->storage == OF_TSDF_I16)
+    k_integrate_list<OF_TSDF_I16><<<blocks, 256, 0, s>>>((uint32_t *)vol, *d, c, depth, pitch, pose,
+                                                         (const float2 *)lam, list, list_count,
+                                                         setup);
+  else
+    k_integrate_list<OF_TSDF_F16><<<blocks, 256, 0, s>>>((uint32_t *)vol, *d, c, depth, pitch, pose,
+                                                         (const float2 *)lam, list, list_count,
+                                                         setup);
   return of_launch_status();
 }
 
@@ -319,6 +684,23 @@ extern "C" of_status_t of_integrate(const of_volume_desc_t *d, void *vol, const 
       pitch < cam->width)
     return OF_ERR_INVALID_ARGUMENT;
   return launch_integrate<false>(d, vol, cam, depth, pitch, pose, lam, nullptr, (cudaStream_t)s);
+}
+
+extern "C" of_status_t of_integrate_scratch_bytes(const of_volume_desc_t *d,
+                                                  const of_camera_t *cam, size_t *bytes) {
+  if (!of_volume_valid(d) || !of_camera_valid(cam) || !bytes) return OF_ERR_INVALID_ARGUMENT;
+  *bytes = scratch_layout(d, cam).total;
+  return OF_OK;
+}
+
+extern "C" of_status_t of_integrate_tiled(const of_volume_desc_t *d, void *vol,
+                                          const of_camera_t *cam, const uint16_t *depth,
+                                          int32_t pitch, const double *pose, const float *lam,
+                                          void *scratch, of_stream_t s) {
+  if (!of_volume_valid(d) || !of_camera_valid(cam) || !vol || !depth || !pose || !lam ||
+      !scratch || pitch < cam->width || ((uintptr_t)scratch & 255u))
+    return OF_ERR_INVALID_ARGUMENT;
+  return launch_integrate_tiled(d, vol, cam, depth, pitch, pose, lam, scratch, (cudaStream_t)s);
 }
 
 extern "C" of_status_t of_integrate_census(const of_volume_desc_t *d, const void *vol,

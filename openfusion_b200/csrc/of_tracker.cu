@@ -36,6 +36,7 @@ struct of_tracker {
   unsigned long long *hist_count = nullptr;
   uint16_t *depth = nullptr;
   float *lambda = nullptr;
+  void *scratch = nullptr;
   of_icp_stats_t *stats = nullptr;
   int hist_cap = 1024;
   int64_t frames = 0;
@@ -65,8 +66,8 @@ of_status_t enqueue_frame(of_tracker *t, bool track, cudaStream_t s) {
     st = of_icp_launch(&d.camera, &d.icp, t->frame, t->model, t->pose, t->icp_ws, t->stats, s);
     if (st != OF_OK) return st;
   }
-  st = of_integrate(&d.volume, t->volume, &d.camera, t->depth, d.camera.width, t->pose, t->lambda,
-                    s);
+  st = of_integrate_tiled(&d.volume, t->volume, &d.camera, t->depth, d.camera.width, t->pose,
+                          t->lambda, t->scratch, s);
   if (st != OF_OK) return st;
   st = of_raycast(&d.volume, t->volume, &d.camera, &d.raycast, d.icp.levels, t->pose, t->model,
                   nullptr, s);
@@ -110,7 +111,7 @@ void release(of_tracker *t) {
   if (t->g_first) cudaGraphExecDestroy(t->g_first);
   if (t->g_track) cudaGraphExecDestroy(t->g_track);
   void *bufs[] = {t->volume, t->frame, t->model, t->icp_ws, t->pose, t->hist, t->hist_count,
-                  t->depth, t->lambda, t->stats};
+                  t->depth, t->lambda, t->scratch, t->stats};
   for (void *b : bufs)
     if (b) cudaFree(b);
   if (t->cap) cudaStreamDestroy(t->cap);
@@ -134,9 +135,10 @@ extern "C" of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_track
   if (st != OF_OK) { release(t); return st; }
   cudaError_t e = cudaStreamCreateWithFlags(&t->cap, cudaStreamNonBlocking);
   if (e != cudaSuccess) { release(t); return of_set_cuda_error(e); }
-  size_t vol_bytes = 0, lam_bytes = 0;
+  size_t vol_bytes = 0, lam_bytes = 0, scratch_bytes = 0;
   of_volume_bytes(&desc->volume, &vol_bytes);
   of_lambda_bytes(&desc->camera, &lam_bytes);
+  of_integrate_scratch_bytes(&desc->volume, &desc->camera, &scratch_bytes);
   size_t px = (size_t)desc->camera.width * desc->camera.height;
   struct { void **p; size_t n; } allocs[] = {
       {&t->volume, vol_bytes},
@@ -148,6 +150,7 @@ extern "C" of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_track
       {(void **)&t->hist_count, sizeof(unsigned long long)},
       {(void **)&t->depth, px * sizeof(uint16_t)},
       {(void **)&t->lambda, lam_bytes},
+      {&t->scratch, scratch_bytes},
       {(void **)&t->stats, sizeof(of_icp_stats_t)},
   };
   for (auto &a : allocs) {

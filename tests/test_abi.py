@@ -70,3 +70,9 @@ def test_invalid_arguments_are_rejected(of):
     assert lib.of_pyramid_layout(C.byref(cam), 3, C.byref(lay)) == 1
     assert lib.of_integrate(None, None, None, None, 0, None, None, None) == 1
     assert lib.of_tracker_create(None, None) == 1
+
+
+def test_package_exports_resolve():
+    import openfusion_b200 as of
+    for name in of.__all__:
+        assert getattr(of, name) is not None, name

@@ -95,9 +95,12 @@ def test_preprocess_matches_oracle(of, ora, cuda, name, size):
 
 # ---------------------------------------------------------------- integrate
 
-@pytest.mark.parametrize("name,res,storage", [("c1", 128, "i16"), ("c2", 256, "i16"),
-                                              ("c2", 512, "i16"), ("c1", 128, "f16")])
-def test_integrate_matches_oracle(of, ora, cuda, name, res, storage):
+@pytest.mark.parametrize("name,res,storage,tiled", [("c1", 128, "i16", False),
+                                                    ("c2", 256, "i16", False),
+                                                    ("c2", 512, "i16", False),
+                                                    ("c2", 512, "i16", True),
+                                                    ("c1", 128, "f16", True)])
+def test_integrate_matches_oracle(of, ora, cuda, name, res, storage, tiled):
     import torch
     cfg = small(of, name, resolution=res, storage=storage)
     seq, vol, lam = build_state(of, cfg, 3, cuda)
@@ -110,7 +113,7 @@ def test_integrate_matches_oracle(of, ora, cuda, name, res, storage):
     dt = torch.from_numpy(d.astype(np.int16)).to(cuda)
     pt = dev_pose(pose, cuda)
     n_gpu = of.integrate_census(cfg, vol, dt, pt, lam)
-    of.integrate(cfg, vol, dt, pt, lam)
+    of.integrate(cfg, vol, dt, pt, lam, of.integrate_scratch(cfg, cuda) if tiled else None)
     torch.cuda.synchronize()
     q1, w1 = of.volume_to_linear(cfg, vol.cpu().numpy())
     qo = (words & 0xFFFF).astype(np.uint16).reshape(q1.shape)
@@ -128,6 +131,35 @@ def test_integrate_matches_oracle(of, ora, cuda, name, res, storage):
         o = qo[ok].view(np.float16).astype(np.float64)
         # fp16 of a value in [-1, 1]: one ulp is at most 2^-11
         assert np.abs(g - o).max() <= 2.0 ** -11 * 1.001
+
+
+@pytest.mark.parametrize("name,res,storage,geom", [("c2", 512, "i16", None),
+                                                   ("c1", 128, "f16", None),
+                                                   ("c2", 512, "i16", (1024.0, 10.0, 120, 50.0))])
+def test_integrate_tiled_equals_per_voxel(of, cuda, name, res, storage, geom):
+    """of_integrate_tiled decides whole bricks from per-tile depth bounds (skip
+    behind the surface, +1 in free space); over a run of frames the volume it
+    writes, brick flags included, is bit-identical to of_integrate's."""
+    import torch
+    kw = dict(resolution=res, storage=storage)
+    if geom:
+        # the reference's cube (1 m, 10 mm truncation): the scaled room sits
+        # 0.1-0.2 m from the camera
+        kw.update(size_mm=geom[0], trunc_mm=geom[1], max_weight=geom[2], min_depth_mm=geom[3])
+    cfg = small(of, name, **kw)
+    seq = of.make_sequence(cfg, frames=8)
+    lam, scratch = of.lambda_table(cfg, cuda), of.integrate_scratch(cfg, cuda)
+    va, vb = of.new_volume(cfg, cuda), of.new_volume(cfg, cuda)
+    for k in range(8):
+        d = torch.from_numpy(seq.depth[k].astype(np.int16)).to(cuda)
+        p = dev_pose(seq.poses[k], cuda)
+        of.integrate(cfg, va, d, p, lam)
+        of.integrate(cfg, vb, d, p, lam, scratch)
+        torch.cuda.synchronize()
+        assert torch.equal(va, vb), f"volumes differ after frame {k}"
+    # the run touched the volume
+    _, w = of.volume_to_linear(cfg, vb.cpu().numpy())
+    assert (w > 0).sum() > 10000
 
 
 # ---------------------------------------------------------------- raycast
