@@ -180,6 +180,14 @@ __host__ __device__ __forceinline__ size_t vox_index(int nb, int i, int j, int k
 __host__ __device__ __forceinline__ uint8_t *brick_flags(void *vol, int n) {
   return (uint8_t *)vol + (size_t)n * n * n * sizeof(uint32_t);
 }
+// One flag byte per super-brick of 4^3 bricks (32^3 voxels) after the brick
+// flags: set iff one of its bricks' flags is set (both are sticky).
+constexpr int kSuper = 4;
+__host__ __device__ __forceinline__ int super_count(int n) { return (n / 8 + kSuper - 1) / kSuper; }
+__host__ __device__ __forceinline__ uint8_t *super_flags(void *vol, int n) {
+  const size_t nb = (size_t)(n / 8);
+  return brick_flags(vol, n) + ((nb * nb * nb + 255) & ~(size_t)255);
+}
 
 template <int STORAGE>
 struct VoxelCodec;

@@ -101,8 +101,8 @@ extern "C" of_status_t of_pyramid_layout(const of_camera_t *cam, int32_t levels,
 extern "C" of_status_t of_volume_bytes(const of_volume_desc_t *d, size_t *bytes) {
   if (!of_volume_valid(d) || !bytes) return OF_ERR_INVALID_ARGUMENT;
   size_t n = (size_t)d->resolution;
-  size_t nb = n / kBrick;
-  *bytes = n * n * n * sizeof(uint32_t) + align256(nb * nb * nb);
+  size_t nb = n / kBrick, ns = (size_t)super_count((int)n);
+  *bytes = n * n * n * sizeof(uint32_t) + align256(nb * nb * nb) + align256(ns * ns * ns);
   return OF_OK;
 }
 
@@ -110,7 +110,7 @@ extern "C" of_status_t of_volume_reset(const of_volume_desc_t *d, void *vol, of_
   size_t bytes;
   if (of_volume_bytes(d, &bytes) != OF_OK || !vol) return OF_ERR_INVALID_ARGUMENT;
   // weight 0 everywhere: every voxel reads as +trunc (General.cu:27-50);
-  // every brick flag cleared.
+  // every brick and super-brick flag cleared.
   OF_CUDA_TRY(cudaMemsetAsync(vol, 0, bytes, (cudaStream_t)s));
   return OF_OK;
 }
@@ -174,10 +174,11 @@ extern "C" of_status_t of_volume_import(const of_volume_desc_t *d, void *vol, co
                                                                      weight);
   of_status_t st = of_launch_status();
   if (st != OF_OK) return st;
-  // imported content is unknown: mark every brick as near a surface
-  size_t n = (size_t)d->resolution, nb = n / kBrick;
-  OF_CUDA_TRY(cudaMemsetAsync((char *)vol + n * n * n * sizeof(uint32_t), 1, nb * nb * nb,
-                              (cudaStream_t)s));
+  // imported content is unknown: mark every brick (and super-brick) as near
+  // a surface
+  size_t n = (size_t)d->resolution, nb = n / kBrick, ns = (size_t)super_count((int)n);
+  OF_CUDA_TRY(cudaMemsetAsync(brick_flags(vol, (int)n), 1, nb * nb * nb, (cudaStream_t)s));
+  OF_CUDA_TRY(cudaMemsetAsync(super_flags(vol, (int)n), 1, ns * ns * ns, (cudaStream_t)s));
   return OF_OK;
 }
 

@@ -1,8 +1,10 @@
 // of_icp.cu -- multi-level point-to-plane ICP, entirely on the device.
 //
-// One launch per iteration. Each launch fuses what the reference spreads over
-// d_find_corresponding (Source/src/ICP.cu:116-251) and the host loop of
-// ICP::Iterate_ICP (Source/src/ICP.cpp:84-182):
+// The whole coarse-to-fine ICP of a frame runs in one cooperative launch
+// (k_icp_fused; k_icp_iter is the one-iteration form behind of_icp_system).
+// Together they do what the reference spreads over d_find_corresponding
+// (Source/src/ICP.cu:116-251) and the host loop of ICP::Iterate_ICP
+// (Source/src/ICP.cpp:84-182):
 //   for every model pixel with a valid world vertex s and normal n_s:
 //     s_c = T^-1 s; pixel = roundFloat(project(s_c)), rejected when outside
 //     the image or s_c.z >= -eps (ICP.cu:90-95, :152-167);
@@ -12,12 +14,12 @@
 //     inlier if |d - s| < dist and thresh < n_d . n_s < 1 + eps (ICP.cu:179-181);
 //     row A = [n_s x d, n_s], b = n_s . (s - d) (ICP.cu:186-201);
 //   sum the 21 upper A^T A entries, 6 A^T b entries, b^2 and the inlier count
-//   in FP32 (Kahan per thread, shuffle trees per warp and block);
-//   the last block to finish combines the per-block partials (Kahan + tree),
-//   solves A^T A x = A^T b by FP64 Cholesky, negates the rotation part
-//   (ICP.cpp:162-168), builds dT = [Rz(g) Ry(b) Rx(a) | t] and composes
-//   T <- dT T in FP64 (ICP.cu:266-305). A singular system restores the frame's
-//   starting pose and stops the remaining iterations (ICP.cpp:152-158).
+//   in FP32 (per-thread sums, pairwise shuffle trees per warp and block,
+//   Kahan over the blocks' partials);
+//   solve A^T A x = A^T b in FP64, negate the rotation part (ICP.cpp:162-168),
+//   build dT = [Rz(g) Ry(b) Rx(a) | t] and compose T <- dT T in FP64
+//   (ICP.cu:266-305). A singular system restores the frame's starting pose and
+//   stops the remaining iterations (ICP.cpp:152-158).
 #include "of_common.cuh"
 
 #include <mutex>
@@ -36,6 +38,7 @@ constexpr float kEps = 1e-6f;  // _EPSILON_ (Constants.h:14)
 
 constexpr int kFusedThreads = 1024;
 constexpr int kFusedMaxBlocks = 2 * kSmCount;
+constexpr int kSeqSlot = 31;  // word of a partial-sum row that carries its sequence number
 // A grid barrier gives up after about 0.15 s (this many 32 ns sleeps) and
 // reports status 2 instead of waiting forever.
 constexpr unsigned kSpinLimit = 1u << 22;
@@ -286,52 +289,66 @@ struct IcpPlan {
   int cache_pts;  // model points a block keeps in shared memory per level
 };
 
-// Grid-wide barrier for a co-resident grid. The arrival counter only grows
-// within a frame (the begin kernel zeroes it): barrier k of the frame is
-// passed once it reaches k * nexpect, so a barrier costs one atomic per block
-// plus the polling. The wait is bounded; on timeout the workspace error flag
-// is set.
-__device__ __forceinline__ void grid_barrier(IcpWorkspace *ws, unsigned target) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(&ws->bar_count, 1u);
-    volatile unsigned *cnt = &ws->bar_count;
-    unsigned spins = 0;
-    while ((int)(*cnt - target) < 0) {
-      if (++spins > kSpinLimit) {
-        atomicExch(&ws->error, 1);
-        break;
-      }
-      __nanosleep(32);
-    }
-    __threadfence();
+// Grid-wide exchange of a co-resident grid. Each block publishes its row of
+// partial sums and then, with a release store, the row's sequence number (the
+// iteration, counted from 1 within a frame; the begin kernel zeroes them);
+// a reader acquires a row's sequence number before it reads the row. A wait
+// is bounded; on timeout the workspace error flag is set.
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned *p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// Waits (acquire) until *p == v; gives up after kSpinLimit polls or as soon as
+// another block has reported a failed wait. Returns whether *p reached v.
+__device__ __forceinline__ bool wait_seq(IcpWorkspace *ws, const unsigned *p, unsigned v) {
+  unsigned spins = 0;
+  while (ld_acquire_gpu(p) != v) {
+    if (++spins > kSpinLimit) return false;
+    if ((spins & 255u) == 0u && ld_acquire_gpu(reinterpret_cast<unsigned *>(&ws->error)) != 0u)
+      return false;
+    __nanosleep(32);
   }
-  __syncthreads();
+  return true;
 }
 
-// 1 / d for a positive FP64 d by Newton's iteration r <- r + r (1 - d r)
-// from the FP32 reciprocal: each step squares the relative error
-// (2^-23 -> 2^-46 -> below FP64 rounding).
+// 1 / d for a positive FP64 d by one Newton step r <- r + r (1 - d r) from
+// the FP32 reciprocal: the step squares the relative error (2^-23 -> 2^-46),
+// seven orders of magnitude below the FP32 rounding of the summed system.
 __device__ __forceinline__ double recip_pos(double d) {
   const float df = (float)d;
   if (!(df > 1e-30f && df < 1e30f)) return 1.0 / d;
-  double r = (double)__frcp_rn(df);
-  double e = fma(-d, r, 1.0);
-  r = fma(r, e, r);
-  e = fma(-d, r, 1.0);
-  return fma(r, e, r);
+  const double r = (double)__frcp_rn(df);
+  return fma(r, fma(-d, r, 1.0), r);
 }
 
-// sin and cos from their Maclaurin series (Horner in x^2): through x^13 and
-// x^14 the truncation error for |x| <= 1/4 is below 1e-20, far under FP64
-// rounding. Larger angles use the library.
+// sin and cos from their Maclaurin series (Horner in x^2): through x^9 and
+// x^10 for |x| <= 1/32, through x^13 and x^14 for |x| <= 1/4; the truncation
+// error is below 1e-20 relative in both cases, far under FP64 rounding.
+// Larger angles use the library.
 __device__ __forceinline__ void sincos_small(double x, double *s, double *c) {
   if (!(fabs(x) <= 0.25)) {
     sincos(x, s, c);
     return;
   }
   const double x2 = x * x;
+  if (fabs(x) <= 0.03125) {
+    double ps = 1.0 / 362880.0;               // 1/9!
+    ps = fma(ps, x2, -1.0 / 5040.0);          // -1/7!
+    ps = fma(ps, x2, 1.0 / 120.0);            // 1/5!
+    ps = fma(ps, x2, -1.0 / 6.0);             // -1/3!
+    *s = fma(x * x2, ps, x);                  // x + x^3 (-1/3! + x^2/5! - ...)
+    double pc = -1.0 / 3628800.0;             // -1/10!
+    pc = fma(pc, x2, 1.0 / 40320.0);          // 1/8!
+    pc = fma(pc, x2, -1.0 / 720.0);           // -1/6!
+    pc = fma(pc, x2, 1.0 / 24.0);             // 1/4!
+    pc = fma(pc, x2, -0.5);                   // -1/2!
+    *c = fma(x2, pc, 1.0);                    // 1 + x^2 (-1/2! + x^2/4! - ...)
+    return;
+  }
   double ps = -1.0 / 6227020800.0;            // -1/13!
   ps = fma(ps, x2, 1.0 / 39916800.0);         // 1/11!
   ps = fma(ps, x2, -1.0 / 362880.0);          // -1/9!
@@ -351,79 +368,77 @@ __device__ __forceinline__ void sincos_small(double x, double *s, double *c) {
   *c = fma(-x2, pc, 1.0);
 }
 
-// One-thread FP64 solve of the 6x6 normal equations (21 upper entries and 6
-// right-hand sides in tot[0..26], inliers in tot[28]) and the SE(3) update of
-// P (row-major 4x4). LDL^T factorisation (its pivots d_j equal the squared
-// Cholesky pivots, so the singularity rule is the Cholesky solve's: a pivot
-// not above 1e-12 x the largest diagonal entry, a non-finite pivot, or fewer
-// than 6 inliers), forward and back substitution, rotation part negated
-// (ICP.cpp:162-168), dT = [Rz(g) Ry(b) Rx(a) | t] (ICP.cu:274-290), P <- dT P.
-// The unit-lower factor lives in `Ls` (36 doubles of shared memory) so that
-// the solve does not compete for the kernel's registers. Returns the success
-// flag; *minpiv gets min d_j / max H_ii.
+// Warp-parallel FP64 solve of the 6x6 normal equations (21 upper entries and
+// 6 right-hand sides in tot[0..26], inliers in tot[28]) and the SE(3) update
+// of P (row-major 4x4, shared memory); all 32 lanes of one warp call it.
+// Lane i < 6 holds row i of [H | g] and the rows are eliminated in order
+// (Gaussian elimination without pivoting, which on the symmetric system is the
+// LDL^T factorisation: its pivots d_j equal the squared Cholesky pivots, so
+// the singularity rule is the Cholesky solve's: a pivot not above 1e-12 x the
+// largest diagonal entry, a non-finite pivot, or fewer than 6 inliers). Back
+// substitution by one shuffle per unknown, rotation part negated
+// (ICP.cpp:162-168), dT = [Rz(g) Ry(b) Rx(a) | t] (ICP.cu:274-290) and
+// P <- dT P with one entry per lane. Returns the warp-uniform success flag;
+// *minpiv gets min d_j / max H_ii.
+__device__ __forceinline__ double shfl_d(double v, int src) {
+  return __shfl_sync(0xffffffffu, v, src);
+}
 __device__ __forceinline__ int upper_index(int i, int j) {  // i <= j
   return i * 6 - i * (i - 1) / 2 + (j - i);
 }
-__device__ __noinline__ bool lane_solve_update(const float *tot, double *P, double *Ls,
-                                               double *minpiv) {
+__device__ bool warp_solve_update(const float *tot, double *P, double *minpiv) {
+  const int lane = threadIdx.x & 31;
+  const int row = lane < 6 ? lane : 5;  // lanes 6.. shadow row 5
+  double a[7];
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+    a[k] = (double)tot[row <= k ? upper_index(row, k) : upper_index(k, row)];
+  a[6] = (double)tot[21 + row];
   double dmax = 0.0;
 #pragma unroll
   for (int i = 0; i < 6; ++i) dmax = fmax(dmax, (double)tot[upper_index(i, i)]);
   bool ok = tot[28] >= 6.f && dmax > 0.0 && isfinite(dmax);
-  const double inv_dmax = 1.0 / dmax;
-  double d[6], r[6];
-  double mp = 1e300;
+  const double thr = 1e-12 * dmax;
+  double dmin = 1e300, rmine = 0.0;
 #pragma unroll
   for (int j = 0; j < 6; ++j) {
-    // L_ij d_j = H_ij - sum_k L_ik L_jk d_k for i >= j (i = j gives d_j)
+    double pj[7];
 #pragma unroll
-    for (int i = j; i < 6; ++i) {
-      double t = (double)tot[upper_index(j, i)];
+    for (int k = j; k < 7; ++k) pj[k] = shfl_d(a[k], j);
+    const double dj = pj[j];
+    dmin = fmin(dmin, dj);
+    ok = ok && (dj > thr) && isfinite(dj);
+    const double rj = recip_pos(fmax(dj, 1e-300));
+    if (row == j) rmine = rj;
+    if (row > j) {
+      const double f = a[j] * rj;
 #pragma unroll
-      for (int k = 0; k < j; ++k) t = fma(-Ls[6 * i + k] * d[k], Ls[6 * j + k], t);
-      if (i == j) {
-        d[j] = t;
-        mp = fmin(mp, t * inv_dmax);
-        ok = ok && (t > 1e-12 * dmax) && isfinite(t);
-        r[j] = recip_pos(fmax(t, 1e-300));
-      } else {
-        Ls[6 * i + j] = t * r[j];
-      }
+      for (int k = j + 1; k < 7; ++k) a[k] = fma(-f, pj[k], a[k]);
     }
   }
-  *minpiv = ok ? mp : fmin(mp, 0.0);
+  *minpiv = ok ? dmin / dmax : fmin(dmin / dmax, 0.0);
   if (!ok) return false;
-  double z[6], x[6];
-#pragma unroll
-  for (int i = 0; i < 6; ++i) {
-    double t = (double)tot[21 + i];
-#pragma unroll
-    for (int k = 0; k < i; ++k) t = fma(-Ls[6 * i + k], z[k], t);
-    z[i] = t;
-  }
+  double x[6];
 #pragma unroll
   for (int i = 5; i >= 0; --i) {
-    double t = z[i] * r[i];
-#pragma unroll
-    for (int k = i + 1; k < 6; ++k) t = fma(-Ls[6 * k + i], x[k], t);
-    x[i] = t;
+    x[i] = shfl_d(a[6] * rmine, i);
+    if (row < i) a[6] = fma(-a[i], x[i], a[6]);
   }
-  double sa, ca, sb, cb, sg, cg;
-  sincos_small(-x[0], &sa, &ca);
-  sincos_small(-x[1], &sb, &cb);
-  sincos_small(-x[2], &sg, &cg);
-  const double D[12] = {cg * cb, -sg * ca + cg * sb * sa, sg * sa + cg * sb * ca, x[3],
-                        sg * cb, cg * ca + sg * sb * sa,  -cg * sa + sg * sb * ca, x[4],
-                        -sb,     cb * sa,                 cb * ca,                 x[5]};
-  // column j of dT P depends only on column j of P: update in place, rows
-  // 0..2 (row 3 of both is 0 0 0 1)
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const double p0 = P[j], p1 = P[4 + j], p2 = P[8 + j], p3 = P[12 + j];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-      P[4 * i + j] = fma(D[4 * i], p0, fma(D[4 * i + 1], p1, fma(D[4 * i + 2], p2, D[4 * i + 3] * p3)));
-  }
+  double sv = 0.0, cv = 1.0;
+  if (lane < 3) sincos_small(-x[lane], &sv, &cv);
+  const double sa = shfl_d(sv, 0), ca = shfl_d(cv, 0);
+  const double sb = shfl_d(sv, 1), cb = shfl_d(cv, 1);
+  const double sg = shfl_d(sv, 2), cg = shfl_d(cv, 2);
+  // lane l < 12 forms entry (l / 4, l % 4) of dT P; row 3 stays 0 0 0 1
+  const int r = (lane >> 2) % 3, c = lane & 3;
+  double D0, D1, D2, D3;
+  if (r == 0) { D0 = cg * cb; D1 = -sg * ca + cg * sb * sa; D2 = sg * sa + cg * sb * ca; D3 = x[3]; }
+  else if (r == 1) { D0 = sg * cb; D1 = cg * ca + sg * sb * sa; D2 = -cg * sa + sg * sb * ca; D3 = x[4]; }
+  else { D0 = -sb; D1 = cb * sa; D2 = cb * ca; D3 = x[5]; }
+  const double v = fma(D0, P[c], fma(D1, P[4 + c], fma(D2, P[8 + c], D3 * P[12 + c])));
+  __syncwarp();
+  if (lane < 12) P[lane] = v;
+  __syncwarp();
   return true;
 }
 
@@ -473,10 +488,10 @@ __device__ __forceinline__ void try_row(float *acc, const Rigid &c2w, float4 s, 
 }
 
 // The whole multi-level ICP of one frame in one cooperative launch. Each
-// block owns a contiguous slice of every level's model pixels; at the start
-// of a level it copies the slice's valid model points (vertex, normal) into
-// shared memory in pixel order, up to the dynamic shared-memory capacity (the
-// rest of the slice is read from global memory at every iteration). Per
+// block owns every grid-th 32-pixel chunk of every level's model; at the
+// start of a level it copies its chunks' valid model points (vertex, normal)
+// into shared memory in chunk order, up to the dynamic shared-memory capacity
+// (the rest is read from global memory at every iteration). Per
 // iteration: every block associates its points two at a time (both frame
 // gathers in flight together), accumulates the rows (tree sums), writes 29
 // partials, meets the others at one grid barrier, then reduces all blocks'
@@ -488,7 +503,6 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     k_icp_fused(IcpPlan plan, double *pose, IcpWorkspace *ws, of_icp_stats_t *stats) {
   extern __shared__ float4 s_pts[];  // 2 per cached model point
   __shared__ double s_pose[16];
-  __shared__ double s_L[36];
   __shared__ Rigid s_c2w, s_w2c;
   __shared__ float s_red[kFusedThreads / 32][32];
   __shared__ float s_tot[32];
@@ -503,25 +517,31 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     pose_to_rigid(pose, &s_c2w, &s_w2c);
   }
   __syncthreads();  // every thread reads s_stop / s_err / the pose below
-  // blocks a barrier waits for: the grid, plus any arrivals held back by the
-  // fault-injection hook (which then never come)
-  const unsigned nexpect = gridDim.x + (unsigned)max(0, ws->hold_barrier);
+  // the fault-injection hook holds every exchange for an arrival that never
+  // comes
+  const bool hold = ws->hold_barrier > 0;
   const float dist2 = plan.dist_thresh * plan.dist_thresh, nthr = plan.normal_thresh;
   int iter_global = 0;
   for (int l = plan.levels - 1; l >= 0 && !s_stop && !s_err; --l) {
     const IcpLevel L = plan.lv[l];
     const int npx = L.mw * L.mh;
-    const int chunk = (npx + (int)gridDim.x - 1) / (int)gridDim.x;
-    const int p0 = min((int)blockIdx.x * chunk, npx), p1 = min(p0 + chunk, npx);
-    const int pc = min(p1, p0 + plan.cache_pts);  // [p0, pc) cached, [pc, p1) not
-    // ---- cache this block's valid model points of the level, in pixel order
+    // model pixels are dealt to blocks in chunks of 32 (one warp), round
+    // robin, so every block gets an even, spatially spread share: chunk
+    // c_k = block + k * grid, k = 0 .. my_chunks - 1; the first kc chunks
+    // are kept in shared memory, the rest is read at every iteration
+    const int G = (int)gridDim.x;
+    const int nchunks = (npx + 31) >> 5;
+    const int my_chunks = nchunks > (int)blockIdx.x ? (nchunks - 1 - (int)blockIdx.x) / G + 1 : 0;
+    const int kc = min(my_chunks, plan.cache_pts >> 5);
+    // ---- cache this block's valid model points of the level, in chunk order
     if (threadIdx.x == 0) s_npts = 0;
     __syncthreads();
-    for (int base = p0; base < pc; base += kFusedThreads) {
-      const int p = base + threadIdx.x;
+    for (int k0 = 0; k0 < kc; k0 += kWarps) {
+      const int k = k0 + warp;
+      const int p = ((int)blockIdx.x + k * G) * 32 + lane;
       float4 s = make_float4(0.f, 0.f, 0.f, 0.f), ns = s;
       bool valid = false;
-      if (p < pc) {
+      if (k < kc && p < npx) {
         s = __ldg(L.model + 2 * p);
         ns = __ldg(L.model + 2 * p + 1);
         valid = s.w != 0.f && ns.w != 0.f;
@@ -563,8 +583,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         if (qA >= 0) try_row(acc, s_c2w, s_pts[2 * i], s_pts[2 * i + 1], dA, cA, dist2, nthr);
         if (qB >= 0) try_row(acc, s_c2w, s_pts[2 * j], s_pts[2 * j + 1], dB, cB, dist2, nthr);
       }
-      // the rest of the slice, from global memory
-      for (int p = pc + threadIdx.x; p < p1; p += kFusedThreads) {
+      // the rest of the block's chunks, from global memory
+      for (int k = kc + warp; k < my_chunks; k += kWarps) {
+        const int p = ((int)blockIdx.x + k * G) * 32 + lane;
+        if (p >= npx) continue;
         const float4 s = __ldg(L.model + 2 * p);
         const float4 ns = __ldg(L.model + 2 * p + 1);
         if (s.w == 0.f || ns.w == 0.f) continue;
@@ -595,6 +617,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       }
       __syncthreads();
       const int buf = iter_global & 1;
+      const unsigned seq = (unsigned)iter_global + 1u;
       if (warp == 0) {
         float y[kWarps];
 #pragma unroll
@@ -603,23 +626,42 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         for (int span = 1; span < kWarps; span *= 2)
 #pragma unroll
           for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
-        ws->fused_partials[buf][blockIdx.x][lane] = lane < kVals ? y[0] : 0.f;
+        // publish: the values, then (release) the row's sequence number
+        float *row = ws->fused_partials[buf][blockIdx.x];
+        if (lane < kSeqSlot) row[lane] = lane < kVals ? y[0] : 0.f;
+        __syncwarp();
+        if (lane == 0) st_release_gpu(reinterpret_cast<unsigned *>(row + kSeqSlot), seq);
+        // the fault-injection hook: an arrival that never comes
+        if (hold && lane == 0 && !wait_seq(ws, &ws->bar_gen, 0xffffffffu)) atomicExch(&ws->error, 1);
       }
-      grid_barrier(ws, nexpect * (unsigned)(iter_global + 1));
-      // a barrier that gave up ends this frame's tracking in every block
-      if (threadIdx.x == 0) s_err = *((volatile int *)&ws->error);
-      __syncthreads();
-      if (s_err) break;
-      // every block: Kahan over its strided share of the blocks' partials,
-      // then a tree over the groups, in a fixed order
+      // every block: wait for each block's row of this iteration (acquire),
+      // then Kahan over its strided share of the rows and a tree over the
+      // groups, in a fixed order. The acquire of a row's sequence number is
+      // this iteration's grid barrier.
       {
-        // all of this lane's loads are issued before the Kahan chain uses them
         constexpr int kPer = (kFusedMaxBlocks + kWarps - 1) / kWarps;
+        static_assert(kPer <= 32, "one polling lane per row");
         const int v = lane, grp = warp;
+        // lane q < kPer polls row grp + q * kWarps; all of the warp's rows are
+        // polled in parallel, then every lane reads its value of each row
+        const int rq = grp + lane * kWarps;
+        const unsigned *seq_q = reinterpret_cast<const unsigned *>(
+            ws->fused_partials[buf][lane < kPer && rq < (int)gridDim.x ? rq : 0] + kSeqSlot);
+        const bool need = lane < kPer && rq < (int)gridDim.x;
+        unsigned spins = 0;
+        while (!__all_sync(0xffffffffu, !need || ld_acquire_gpu(seq_q) == seq)) {
+          if (++spins > kSpinLimit ||
+              ((spins & 255u) == 0u && ld_acquire_gpu(reinterpret_cast<unsigned *>(&ws->error)))) {
+            if (lane == 0) atomicExch(&ws->error, 1);
+            break;
+          }
+          __nanosleep(32);
+        }
+        __syncwarp();  // the polling lanes' acquires precede every lane's reads
         float vals[kPer];
 #pragma unroll
         for (int q = 0; q < kPer; ++q) {
-          int r = grp + q * kWarps;
+          const int r = grp + q * kWarps;
           vals[q] = (v < kVals && r < (int)gridDim.x) ? __ldcg(&ws->fused_partials[buf][r][v]) : 0.f;
         }
         float sum = 0.f, c = 0.f;
@@ -633,6 +675,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         s_red[grp][v] = sum - c;
       }
       __syncthreads();
+      // a wait that gave up ends this frame's tracking in every block
+      if (threadIdx.x == 0) s_err = ld_acquire_gpu(reinterpret_cast<unsigned *>(&ws->error)) != 0u;
+      __syncthreads();
+      if (s_err) break;
       if (threadIdx.x < 32) {
         float y[kWarps];
 #pragma unroll
@@ -643,9 +689,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
           for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
         s_tot[threadIdx.x] = y[0];
         __syncwarp();
+        double minpiv = 0.0;
+        const bool ok = warp_solve_update(s_tot, s_pose, &minpiv);
         if (threadIdx.x == 0) {
-          double minpiv = 0.0;
-          const bool ok = lane_solve_update(s_tot, s_pose, s_L, &minpiv);
           s_its += 1;
           s_inl = (int)s_tot[28];
           s_res = (double)s_tot[27];
@@ -679,6 +725,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
 // Start of a frame's tracking: remember the starting pose, apply the
 // optional warm-start increment, clear the flags.
 __global__ void k_icp_begin(double *pose, IcpWorkspace *ws, of_icp_stats_t *stats) {
+  // no partial-sum row of this frame has been published yet
+  for (int i = threadIdx.x; i < 2 * kFusedMaxBlocks; i += blockDim.x)
+    reinterpret_cast<unsigned *>(ws->fused_partials[i / kFusedMaxBlocks][i % kFusedMaxBlocks])[kSeqSlot] = 0u;
   if (threadIdx.x != 0) return;
   if (ws->has_prior) {
     double O[16];
@@ -784,8 +833,8 @@ static of_status_t fused_shape(const of_camera_t *cam, FusedShape *fs) {
     fs->grid = grid_of[dev];
   }
   const long npx = (long)cam->width * cam->height;
-  const long chunk = (npx + fs->grid - 1) / fs->grid;
-  fs->cache_pts = (int)(chunk < kMaxCachePts ? chunk : kMaxCachePts);
+  const long per_block = ((npx + 31) / 32 + fs->grid - 1) / fs->grid * 32;
+  fs->cache_pts = (int)(per_block < kMaxCachePts ? per_block : kMaxCachePts);
   fs->smem = (size_t)fs->cache_pts * 2 * sizeof(float4);
   return OF_OK;
 }

@@ -425,12 +425,15 @@ __device__ __forceinline__ void integrate_brick(
           *p4 = make_uint4(w4[0], w4[1], w4[2], w4[3]);
       }
       // a warp that wrote a non-saturated voxel flags the brick and its 26
-      // neighbours (idempotent byte stores, lanes 0..26)
+      // neighbours, and their super-bricks (idempotent byte stores, lanes 0..26)
       if (!CENSUS && __any_sync(0xffffffffu, near) && lane < 27) {
         int ox = lane / 9 - 1, oy = (lane / 3) % 3 - 1, oz = lane % 3 - 1;
         int qx = bx + ox, qy = by + oy, qz = bz + oz;
-        if ((unsigned)qx < (unsigned)nb && (unsigned)qy < (unsigned)nb && (unsigned)qz < (unsigned)nb)
+        if ((unsigned)qx < (unsigned)nb && (unsigned)qy < (unsigned)nb && (unsigned)qz < (unsigned)nb) {
           flags[(qx * nb + qy) * nb + qz] = 1;
+          const int ns = super_count(desc.resolution);
+          super_flags(vol, desc.resolution)[((qx / kSuper) * ns + qy / kSuper) * ns + qz / kSuper] = 1;
+        }
       }
 }
 

@@ -142,29 +142,52 @@ __global__ void __launch_bounds__(256) k_raycast(const uint32_t *__restrict__ vo
     const float far_k = rp.far_step_frac * T;
     const uint8_t *__restrict__ flags = brick_flags((void *)vol, n);
     const float inv_vs = S.inv_vs;
-    // brick-region bounds: the cell base floor(g) of a position lies in brick
-    // b along an axis for g in [8b, 8b + 8), i.e. p in
-    // [org + vs (8b + 0.5), org + vs (8b + 8.5)).
-    const float bvs = 8.0f * vs;
     const float eps = 0.01f * vs;
+    const uint8_t *__restrict__ sflags = super_flags((void *)vol, n);
+    const int ns = super_count(n);
+    // per-axis reciprocal of the direction (0 where the ray is parallel to
+    // the axis planes: that axis bounds no jump)
+    const bool ux = fabsf(dir.x) > 1e-12f, uy = fabsf(dir.y) > 1e-12f, uz = fabsf(dir.z) > 1e-12f;
+    const float rdx = ux ? 1.0f / dir.x : 0.f, rdy = uy ? 1.0f / dir.y : 0.f, rdz = uz ? 1.0f / dir.z : 0.f;
     float t = t0;
     float fp = 1.0f;
     bool sampled = false;
+    int cur_b = -1, cur_s = -1;  // brick / super-brick the march is in, and their flags
+    bool cur_flag = false, cur_sflag = false;
     for (int it = 0; it < (1 << 16); ++it) {
       const float px = fmaf(t, dir.x, ox), py = fmaf(t, dir.y, oy), pz = fmaf(t, dir.z, oz);
       int bi = min(max(__float2int_rd(fmaf(px - org, inv_vs, -0.5f)), 0), n - 2) >> 3;
       int bj = min(max(__float2int_rd(fmaf(py - org, inv_vs, -0.5f)), 0), n - 2) >> 3;
       int bk = min(max(__float2int_rd(fmaf(pz - org, inv_vs, -0.5f)), 0), n - 2) >> 3;
-      if (!__ldg(flags + (bi * nb + bj) * nb + bk)) {
-        // every sample with its cell base in this brick reads exactly +1:
-        // jump just past the brick region; the landing cell is +1 as well
-        float ex = (dir.x > 0.f ? fmaf(bvs, (float)(bi + 1), org + 0.5f * vs) : fmaf(bvs, (float)bi, org + 0.5f * vs)) - ox;
-        float ey = (dir.y > 0.f ? fmaf(bvs, (float)(bj + 1), org + 0.5f * vs) : fmaf(bvs, (float)bj, org + 0.5f * vs)) - oy;
-        float ez = (dir.z > 0.f ? fmaf(bvs, (float)(bk + 1), org + 0.5f * vs) : fmaf(bvs, (float)bk, org + 0.5f * vs)) - oz;
+      const int si = bi / kSuper, sj = bj / kSuper, sk = bk / kSuper;
+      const int sidx = (si * ns + sj) * ns + sk;
+      if (sidx != cur_s) {
+        cur_s = sidx;
+        cur_sflag = __ldg(sflags + sidx) != 0;
+      }
+      bool skip = !cur_sflag;
+      if (!skip) {
+        const int b = (bi * nb + bj) * nb + bk;
+        if (b != cur_b) {
+          cur_b = b;
+          cur_flag = __ldg(flags + b) != 0;
+        }
+        skip = !cur_flag;
+      }
+      if (skip) {
+        // every sample with its cell base in this brick (or, when the
+        // super-brick's flag is clear, in this super-brick) reads exactly +1:
+        // jump just past the region; the landing cell is +1 as well. The
+        // region of cell bases [8b, 8b + 8) along an axis is
+        // p in [org + vs (8b + 0.5), org + vs (8b + 8.5)); R = 32 for a
+        // super-brick.
+        const float R = cur_sflag ? 8.0f : (float)(8 * kSuper);
+        const int ci = cur_sflag ? bi : si, cj = cur_sflag ? bj : sj, ck = cur_sflag ? bk : sk;
+        const float rvs = R * vs, h = org + 0.5f * vs;
         float te = 1e30f;
-        if (fabsf(dir.x) > 1e-12f) te = fminf(te, ex / dir.x);
-        if (fabsf(dir.y) > 1e-12f) te = fminf(te, ey / dir.y);
-        if (fabsf(dir.z) > 1e-12f) te = fminf(te, ez / dir.z);
+        if (ux) te = fminf(te, (fmaf(rvs, (float)(dir.x > 0.f ? ci + 1 : ci), h) - ox) * rdx);
+        if (uy) te = fminf(te, (fmaf(rvs, (float)(dir.y > 0.f ? cj + 1 : cj), h) - oy) * rdy);
+        if (uz) te = fminf(te, (fmaf(rvs, (float)(dir.z > 0.f ? ck + 1 : ck), h) - oz) * rdz);
         t = fmaxf(te, t) + eps;
         fp = 1.0f;
         sampled = true;

@@ -431,6 +431,17 @@ void ora_raycast(const ora_vol *v, const uint32_t *words, const uint8_t *flags, 
   const R min_step = (R)(p->min_step_vox * vs), far_k = (R)(p->far_step_frac * v->trunc);
   const R o[3] = {(R)P[3], (R)P[7], (R)P[11]};
   const R rvs = (R)vs;
+  /* super-brick flags (4^3 bricks): the OR of their bricks' flags, as the
+   * volume keeps them beside the brick flags */
+  const int nbk = n / 8, ns = (nbk + 3) / 4;
+  uint8_t *sflags = NULL;
+  if (flags) {
+    sflags = (uint8_t *)calloc((size_t)ns * ns * ns, 1);
+    for (int i = 0; i < nbk; ++i)
+      for (int j = 0; j < nbk; ++j)
+        for (int k = 0; k < nbk; ++k)
+          if (flags[((size_t)i * nbk + j) * nbk + k]) sflags[((size_t)(i / 4) * ns + j / 4) * ns + k / 4] = 1;
+  }
 #pragma omp parallel for schedule(dynamic, 4)
   for (int y = 0; y < c->h; ++y) {
     for (int x = 0; x < c->w; ++x) {
@@ -465,7 +476,8 @@ void ora_raycast(const ora_vol *v, const uint32_t *words, const uint8_t *flags, 
           if (flags) {
             /* empty-space skip: a brick whose flag is clear holds, with its
              * 26 neighbours, only +1 voxels; every sample whose cell base is
-             * in it reads +1, so the march jumps past its region */
+             * in it reads +1, so the march jumps past its region (past the
+             * region of the whole super-brick when its flag is clear) */
             int bi[3];
             R pp[3] = {px, py, pz};
             for (int a = 0; a < 3; ++a) {
@@ -474,13 +486,15 @@ void ora_raycast(const ora_vol *v, const uint32_t *words, const uint8_t *flags, 
               if (q > n - 2) q = n - 2;
               bi[a] = q >> 3;
             }
-            int nbk = n / 8;
-            if (!flags[((size_t)bi[0] * nbk + bi[1]) * nbk + bi[2]]) {
+            const int super_clear = !sflags[((size_t)(bi[0] / 4) * ns + bi[1] / 4) * ns + bi[2] / 4];
+            if (super_clear || !flags[((size_t)bi[0] * nbk + bi[1]) * nbk + bi[2]]) {
+              const int span = super_clear ? 32 : 8;
               R te = (R)1e30;
               for (int a = 0; a < 3; ++a) {
                 if (fabs((double)dir[a]) <= 1e-12) continue;
-                double edge = dir[a] > 0 ? V.org + vs * (8.0 * (bi[a] + 1) + 0.5)
-                                         : V.org + vs * (8.0 * bi[a] + 0.5);
+                const int ci = super_clear ? bi[a] / 4 : bi[a];
+                double edge = dir[a] > 0 ? V.org + vs * ((double)span * (ci + 1) + 0.5)
+                                         : V.org + vs * ((double)span * ci + 0.5);
                 R ta = (R)((edge - (double)o[a]) / (double)dir[a]);
                 if (ta < te) te = ta;
               }
@@ -558,6 +572,7 @@ void ora_raycast(const ora_vol *v, const uint32_t *words, const uint8_t *flags, 
       if (ambig) ambig[pix] = (uint8_t)amb;
     }
   }
+  free(sflags);
 }
 
 void ora_model_down(const R *src, int32_t sw, R *dst, int32_t dw, int32_t dh) {

@@ -177,6 +177,13 @@ def test_raycast_matches_oracle(of, ora, cuda, name, res):
     words = (q.astype(np.uint32) | (w.astype(np.uint32) << 16)).reshape(-1).copy()
     nb = cfg.resolution // 8
     flags = host.view(np.uint8)[4 * cfg.resolution ** 3:][: nb ** 3].copy()
+    # the volume keeps one super-brick flag per 4^3 bricks: the OR of theirs
+    ns = (nb + 3) // 4
+    soff = 4 * cfg.resolution ** 3 + (nb ** 3 + 255) // 256 * 256
+    sflags = host.view(np.uint8)[soff:soff + ns ** 3].reshape(ns, ns, ns)
+    pad = np.zeros((ns * 4,) * 3, np.uint8)
+    pad[:nb, :nb, :nb] = flags.reshape(nb, nb, nb)
+    assert np.array_equal(sflags != 0, pad.reshape(ns, 4, ns, 4, ns, 4).max(axis=(1, 3, 5)) != 0)
     opts, amb = ora.raycast(cfg, words, pose, ambig=True, flags=flags)
     # the skip is exact: the oracle without it finds the same surface
     plain, _ = ora.raycast(cfg, words, pose)
