@@ -137,7 +137,8 @@ of_status_t of_camera_level(const of_camera_t *cam, int32_t level, of_camera_t *
  * flag byte per brick (brick or a neighbour near a surface), padded to 256. */
 of_status_t of_volume_bytes(const of_volume_desc_t *desc, size_t *bytes);
 /* Resets every voxel to weight 0 (tsdf reads as +trunc), replacing
- * d_initVoxelArray (Source/src/General.cu:27-50). */
+ * d_initVoxelArray (Source/src/General.cu:27-50). An unobserved voxel's word
+ * holds the +1 tsdf pattern with weight 0. */
 of_status_t of_volume_reset(const of_volume_desc_t *desc, void *d_volume, of_stream_t stream);
 /* Writes the volume in the reference's layout: float tsdf in mm and the
  * weight, index x*N*N + y*N + z (Source/src/MainApp.cpp:181-276 dumps the

@@ -250,9 +250,12 @@ def volume_to_linear(cfg: Config, vol_words: np.ndarray):
 
 def linear_to_volume(cfg: Config, q: np.ndarray, weight: np.ndarray) -> np.ndarray:
     """(q, weight) in x,y,z order -> a whole volume buffer (int32 words) with
-    every brick flagged as near a surface."""
+    every brick flagged as near a surface; unobserved voxels (weight 0) hold
+    the +1 pattern, as the library's reset writes them."""
     n = cfg.resolution
     nb = n // 8
+    one = 0x7FFF if cfg.storage == "i16" else 0x3C00
+    q = np.where(np.asarray(weight) == 0, one, np.asarray(q).astype(np.int64) & 0xFFFF)
     words = (q.astype(np.uint32) & 0xFFFF) | (weight.astype(np.uint32) << 16)
     words = words.reshape(nb, 8, nb, 8, nb, 8).transpose(0, 2, 4, 1, 3, 5).reshape(-1)
     flags = np.ones(volume_bytes(cfg) - 4 * n ** 3, np.uint8)

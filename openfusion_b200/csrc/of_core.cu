@@ -106,12 +106,28 @@ extern "C" of_status_t of_volume_bytes(const of_volume_desc_t *d, size_t *bytes)
   return OF_OK;
 }
 
+// Every voxel word := value (the +1 bit pattern with weight 0).
+__global__ void k_volume_fill(uint4 *__restrict__ words, size_t n4, uint32_t value) {
+  const uint4 v = make_uint4(value, value, value, value);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4;
+       i += (size_t)gridDim.x * blockDim.x)
+    words[i] = v;
+}
+
 extern "C" of_status_t of_volume_reset(const of_volume_desc_t *d, void *vol, of_stream_t s) {
   size_t bytes;
   if (of_volume_bytes(d, &bytes) != OF_OK || !vol) return OF_ERR_INVALID_ARGUMENT;
-  // weight 0 everywhere: every voxel reads as +trunc (General.cu:27-50);
-  // every brick and super-brick flag cleared.
-  OF_CUDA_TRY(cudaMemsetAsync(vol, 0, bytes, (cudaStream_t)s));
+  // weight 0 everywhere: every voxel reads as +trunc (General.cu:27-50). The
+  // stored tsdf of an unobserved voxel is the +1 pattern, so readers need no
+  // weight test; every brick and super-brick flag cleared.
+  const size_t n = (size_t)d->resolution, words = n * n * n;
+  const uint32_t one = d->storage == OF_TSDF_I16 ? VoxelCodec<OF_TSDF_I16>::kOneBits
+                                                 : VoxelCodec<OF_TSDF_F16>::kOneBits;
+  k_volume_fill<<<kSmCount * 8, 256, 0, (cudaStream_t)s>>>((uint4 *)vol, words / 4, one);
+  of_status_t st = of_launch_status();
+  if (st != OF_OK) return st;
+  OF_CUDA_TRY(cudaMemsetAsync(brick_flags(vol, (int)n), 0, bytes - words * sizeof(uint32_t),
+                              (cudaStream_t)s));
   return OF_OK;
 }
 
@@ -142,7 +158,8 @@ __global__ void k_volume_import(uint32_t *__restrict__ vol, VolGeom g, const flo
     int j = (int)((idx / n) % n);
     int i = (int)(idx / (n * n));
     uint32_t wt = weight ? weight[idx] : 1u;
-    float t = tsdf ? tsdf[idx] * g.inv_trunc : 1.0f;
+    // an unobserved voxel keeps the +1 pattern (as after a reset)
+    float t = (tsdf && wt) ? tsdf[idx] * g.inv_trunc : 1.0f;
     vol[vox_index(g.nb, i, j, k)] = VoxelCodec<STORAGE>::pack(t, wt);
   }
 }

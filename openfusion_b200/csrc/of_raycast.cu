@@ -29,17 +29,21 @@ struct RaySetup {
   float inv_vs;
 };
 
-// Normalised tsdf of a voxel word for the raycast (weight 0 reads +1). The
-// int16 path converts without I2F: 2^23 + 2^22 + q is exact in FP32.
+// Stored tsdf of a voxel word, in storage units: q for int16 (q / 32767 is
+// the normalised tsdf), the value itself for fp16. An unobserved voxel
+// (weight 0) holds the +1 pattern (the reset and import write it), so no
+// weight test is needed. int16 without I2F: with u = q + 32768 (offset
+// binary, the low half XOR 0x8000), 1.5 * 2^23 + u is exact in FP32.
 template <int STORAGE>
 __device__ __forceinline__ float ray_value(uint32_t w) {
-  if (STORAGE == OF_TSDF_I16) {
-    int q = ((int)(w << 16)) >> 16;
-    float v = (__int_as_float(0x4B400000 + q) - 12582912.0f) * (1.0f / kQ);
-    return w < 65536u ? 1.0f : v;
-  } else {
-    return w < 65536u ? 1.0f : __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
-  }
+  if (STORAGE == OF_TSDF_I16)
+    return __int_as_float((w & 0xffffu) ^ 0x4B408000u) - 12615680.0f;  // 1.5 * 2^23 + 2^15
+  else
+    return __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
+}
+template <int STORAGE>
+constexpr float ray_scale() {
+  return STORAGE == OF_TSDF_I16 ? 1.0f / kQ : 1.0f;
 }
 
 // Trilinear tsdf at a world position. Corner (i0, j0, k0) is clamped to
@@ -76,7 +80,7 @@ __device__ __forceinline__ float trilinear(const uint32_t *__restrict__ vol, int
   float c11 = fmaf(fz, c111 - c110, c110);
   float c0 = fmaf(fy, c01 - c00, c00);
   float c1 = fmaf(fy, c11 - c10, c10);
-  return fmaf(fx, c1 - c0, c0);
+  return fmaf(fx, c1 - c0, c0) * ray_scale<STORAGE>();
 }
 
 __device__ __forceinline__ uint32_t rgba_pack(float x, float y, float z, float w) {
