@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define OF_ABI_VERSION 1
+#define OF_ABI_VERSION 2
 
 typedef int32_t of_status_t;
 #define OF_OK 0
@@ -96,6 +96,22 @@ typedef struct of_icp_params {
   int32_t iters[4];        /* iterations per level, finest level first: {10, 5, 4} */
   float dist_thresh_mm;    /* 25 */
   float normal_thresh;     /* cosine, 0.65 */
+  /* Early exit (no reference counterpart; 0 = always run every iteration):
+   * a level ends after an iteration whose increment rotates by less than
+   * stop_rot_rad about every axis and translates by less than stop_trans_mm
+   * along every axis. */
+  float stop_rot_rad;
+  float stop_trans_mm;
+  /* Judge of a warm-started result (of_icp_track_warm; no reference
+   * counterpart): it is replaced by plain ICP from the previous pose when the
+   * last iteration's RMS point-to-plane residual exceeds judge_max_rms_mm, its
+   * inliers are fewer than judge_min_inlier_frac of the examined model points,
+   * or it lies farther than judge_max_rot_rad / judge_max_trans_mm from the
+   * warm start (the disagreement with the prediction). */
+  float judge_max_rms_mm;
+  float judge_min_inlier_frac;
+  float judge_max_rot_rad;
+  float judge_max_trans_mm;
 } of_icp_params_t;
 
 /* Per-frame ICP result, written by the device. */
@@ -103,8 +119,8 @@ typedef struct of_icp_stats {
   int32_t status;        /* 0 = tracked; 1 = singular system, pose restored (ICP.cpp:152-158);
                             2 = a device-side wait gave up, pose restored */
   int32_t inliers;       /* correspondences of the last iteration run */
-  int32_t iterations;    /* iterations run */
-  int32_t reserved;
+  int32_t iterations;    /* iterations run (both passes of a replaced warm start) */
+  int32_t warm;          /* 0 = no warm start, 1 = warm start kept, 2 = replaced */
   double residual_sq;    /* sum of squared point-to-plane residuals, mm^2, last iteration */
   double min_pivot;      /* smallest Cholesky pivot / largest diagonal, last iteration */
 } of_icp_stats_t;
@@ -220,6 +236,14 @@ of_status_t of_icp_workspace_bytes(const of_camera_t *cam, size_t *bytes);
 of_status_t of_icp_track(const of_camera_t *cam, const of_icp_params_t *params,
                          const void *d_frame, const void *d_model, double *d_pose,
                          void *d_workspace, of_icp_stats_t *d_stats, of_stream_t stream);
+/* of_icp_track starting from a warm start (`d_warm_pose`, device FP64 4x4;
+ * e.g. of_cnn_warm_pose's). The result is judged (of_icp_params_t judge_*);
+ * a rejected one is replaced by plain ICP from `pose`. stats->warm tells
+ * which (1 kept, 2 replaced). No reference counterpart. */
+of_status_t of_icp_track_warm(const of_camera_t *cam, const of_icp_params_t *params,
+                              const void *d_frame, const void *d_model, double *d_pose,
+                              const double *d_warm_pose, void *d_workspace,
+                              of_icp_stats_t *d_stats, of_stream_t stream);
 /* of_icp_track without a workspace argument (no counterpart in the
  * reference): for callers that cannot allocate device memory once they run --
  * hosts that own every device allocation up front, such as plugin hosts with
@@ -262,6 +286,11 @@ typedef struct of_tracker_desc {
   double initial_pose[16]; /* camera-to-world of frame 0 */
   int32_t use_graph;       /* 1 = replay each frame as a captured CUDA graph */
   int32_t pose_history;    /* frames of pose history kept on the device (0 = 1024) */
+  /* Learned warm start: host FP32 weights of the warm-start CNN
+   * (of_cnn_param_count floats; NULL = plain ICP from the previous pose).
+   * Needs W = 80 k, H = 60 k. Each tracked frame then runs the CNN on the
+   * (previous, current) depth pair and of_icp_track_warm. */
+  const float *warm_start_weights;
 } of_tracker_desc_t;
 
 of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_tracker_t *out);
@@ -319,6 +348,65 @@ of_status_t of_pose_from_float(const float *d_pose_f32, double *d_pose, int32_t 
                                of_stream_t stream);
 of_status_t of_pose_to_float(const double *d_pose, float *d_pose_f32, float *d_inv_pose_f32,
                              float *d_camera_position3, of_stream_t stream);
+
+/* ---- learned ICP warm start (no reference counterpart: the reference
+ *      starts ICP at the previous pose, Source/src/ICP.cpp:84-182) -------- */
+
+/* A small BF16 CNN maps the pair (previous, current) of depth frames, block-
+ * averaged to 80x60, to the camera motion between them: 6 outputs, the
+ * rotation vector of R_prev^T R_cur times 10 (rad) and its translation
+ * R_prev^T (t_cur - t_prev) divided by 100 (mm). Parameters live twice on the
+ * device: FP32 master values (`d_master`, of_cnn_param_count floats; biases
+ * are read from them) and their BF16 copies (`d_params`, uint16 bit patterns,
+ * same count). Activations are stored in BF16, every sum runs in FP32, and
+ * every reduction in a fixed order, so results are reproducible. */
+of_status_t of_cnn_param_count(int64_t *count);
+/* Bytes of the per-batch workspace of of_cnn_forward / of_cnn_backward. */
+of_status_t of_cnn_workspace_bytes(int32_t batch, size_t *bytes);
+/* He-uniform weights and zero biases from a seed. */
+of_status_t of_cnn_init(float *d_master, uint16_t *d_params, uint64_t seed, of_stream_t stream);
+/* Network input (BF16, batch x 2 x 60 x 80) of `batch` pairs of uint16 depth
+ * frames of W x H (W = 80 k, H = 60 k): the mean of each k x k block's valid
+ * depths in metres, minus the mean over the previous frame's non-empty
+ * blocks; empty blocks are 0. Pair i is at d_prev + i * pair_stride and
+ * d_cur + i * pair_stride (pixels). */
+of_status_t of_cnn_input(const uint16_t *d_prev, const uint16_t *d_cur, int32_t width,
+                         int32_t height, int32_t batch, int64_t pair_stride, uint16_t *d_input,
+                         of_stream_t stream);
+/* Forward pass; `d_out` (may be NULL) receives batch x 6 floats. */
+of_status_t of_cnn_forward(const uint16_t *d_params, const float *d_master,
+                           const uint16_t *d_input, int32_t batch, void *d_workspace,
+                           float *d_out, of_stream_t stream);
+/* Forward and backward pass of the loss mean_b sum_k w_k (out_bk - target_bk)^2
+ * (`d_loss_weights`: 6 floats): writes the gradient of every parameter into
+ * `d_grad` (param-count floats) and the loss into `d_loss` (may be NULL). */
+of_status_t of_cnn_backward(const uint16_t *d_params, const float *d_master,
+                            const uint16_t *d_input, int32_t batch, const float *d_target,
+                            const float *d_loss_weights, void *d_workspace, float *d_grad,
+                            float *d_loss, of_stream_t stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8, bias-corrected; `step` counts
+ * from 1) on the master values; refreshes their BF16 copies. */
+of_status_t of_cnn_adam(float *d_master, uint16_t *d_params, const float *d_grad, float *d_m,
+                        float *d_v, int32_t step, float lr, of_stream_t stream);
+/* BF16 copies of (loaded) master values. */
+of_status_t of_cnn_load(const float *d_master, uint16_t *d_params, of_stream_t stream);
+/* Warm start from a prediction: d_warm_pose = d_prev_pose x [exp(w) | t] with
+ * w = out[0..2] / 10 (rad), t = 100 out[3..5] (mm); FP64 4x4 device poses. */
+of_status_t of_cnn_warm_pose(const float *d_out, const double *d_prev_pose, double *d_warm_pose,
+                             of_stream_t stream);
+
+/* ---- synthetic sequences on the device (test and training data) ------- */
+
+/* Renders `frames` uint16 depth frames (frame i at camera-to-world pose
+ * d_poses[16 i .. 16 i + 15], noise counter first_frame + i) of a scene built
+ * by of_synth_scene (`d_scene`: an of_synth_scene_t copied to the device), with
+ * the seeded renderer of libof_synth (of_synth_render); output frame i at
+ * d_depth + i * W * H. */
+of_status_t of_synth_render_device(const void *d_scene, int32_t width, int32_t height, float fx,
+                                   float fy, float cx, float cy, const double *d_poses,
+                                   int32_t frames, uint64_t noise_seed, int32_t first_frame,
+                                   float sigma_scale, float dropout, uint16_t *d_depth,
+                                   of_stream_t stream);
 
 #ifdef __cplusplus
 }

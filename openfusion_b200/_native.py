@@ -37,12 +37,15 @@ class RaycastParams(C.Structure):
 
 class IcpParams(C.Structure):
     _fields_ = [("levels", C.c_int32), ("iters", C.c_int32 * 4), ("dist_thresh_mm", C.c_float),
-                ("normal_thresh", C.c_float)]
+                ("normal_thresh", C.c_float), ("stop_rot_rad", C.c_float),
+                ("stop_trans_mm", C.c_float), ("judge_max_rms_mm", C.c_float),
+                ("judge_min_inlier_frac", C.c_float), ("judge_max_rot_rad", C.c_float),
+                ("judge_max_trans_mm", C.c_float)]
 
 
 class IcpStats(C.Structure):
     _fields_ = [("status", C.c_int32), ("inliers", C.c_int32), ("iterations", C.c_int32),
-                ("reserved", C.c_int32), ("residual_sq", C.c_double), ("min_pivot", C.c_double)]
+                ("warm", C.c_int32), ("residual_sq", C.c_double), ("min_pivot", C.c_double)]
 
 
 class PyramidLayout(C.Structure):
@@ -55,7 +58,7 @@ class TrackerDesc(C.Structure):
     _fields_ = [("camera", Camera), ("volume", VolumeDesc), ("filter", FilterParams),
                 ("raycast", RaycastParams), ("icp", IcpParams),
                 ("initial_pose", C.c_double * 16), ("use_graph", C.c_int32),
-                ("pose_history", C.c_int32)]
+                ("pose_history", C.c_int32), ("warm_start_weights", C.c_void_p)]
 
 
 class TrackerBuffers(C.Structure):
@@ -118,6 +121,20 @@ _SIGS = {
     "of_points_from_reference": (c_status, [C.POINTER(Camera), C.c_int32, P, P, P, c_stream]),
     "of_pose_from_float": (c_status, [P, P, C.c_int32, c_stream]),
     "of_pose_to_float": (c_status, [P, P, P, P, c_stream]),
+    "of_cnn_param_count": (c_status, [C.POINTER(C.c_int64)]),
+    "of_cnn_workspace_bytes": (c_status, [C.c_int32, C.POINTER(C.c_size_t)]),
+    "of_cnn_init": (c_status, [P, P, C.c_uint64, c_stream]),
+    "of_cnn_input": (c_status, [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int64, P, c_stream]),
+    "of_cnn_forward": (c_status, [P, P, P, C.c_int32, P, P, c_stream]),
+    "of_cnn_backward": (c_status, [P, P, P, C.c_int32, P, P, P, P, P, c_stream]),
+    "of_cnn_adam": (c_status, [P, P, P, P, P, C.c_int32, C.c_float, c_stream]),
+    "of_cnn_load": (c_status, [P, P, c_stream]),
+    "of_cnn_warm_pose": (c_status, [P, P, P, c_stream]),
+    "of_icp_track_warm": (c_status, [C.POINTER(Camera), C.POINTER(IcpParams), P, P, P, P, P, P,
+                                     c_stream]),
+    "of_synth_render_device": (c_status, [P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float,
+                                          C.c_float, P, C.c_int32, C.c_uint64, C.c_int32,
+                                          C.c_float, C.c_float, P, c_stream]),
 }
 
 _SYNTH_SIGS = {

@@ -43,6 +43,12 @@ class Config:
     iters: tuple = (10, 5, 4)
     dist_thresh_mm: float = 25.0
     normal_thresh: float = 0.65
+    stop_rot_rad: float = 0.0       # early exit (0 = every iteration)
+    stop_trans_mm: float = 0.0
+    judge_max_rms_mm: float = 10.0  # warm-start judge
+    judge_min_inlier_frac: float = 0.3
+    judge_max_rot_rad: float = 0.05
+    judge_max_trans_mm: float = 50.0
     min_step_vox: float = 0.75
     far_step_frac: float = 0.8
     refine_iters: int = 3
@@ -70,7 +76,10 @@ class Config:
 
     def icp(self) -> N.IcpParams:
         it = (C.c_int32 * 4)(*(list(self.iters) + [0] * (4 - len(self.iters))))
-        return N.IcpParams(self.levels, it, self.dist_thresh_mm, self.normal_thresh)
+        return N.IcpParams(self.levels, it, self.dist_thresh_mm, self.normal_thresh,
+                           self.stop_rot_rad, self.stop_trans_mm, self.judge_max_rms_mm,
+                           self.judge_min_inlier_frac, self.judge_max_rot_rad,
+                           self.judge_max_trans_mm)
 
     def radius(self) -> int:
         return self.radius_px if self.radius_px > 0 else int(np.ceil(2.0 * self.sigma_space_px))
@@ -269,7 +278,9 @@ class Tracker:
     frame loop (MainApp.cpp:786-964) as one CUDA graph per frame."""
 
     def __init__(self, cfg: Config, initial_pose: np.ndarray, use_graph: bool = True,
-                 pose_history: int = 1024):
+                 pose_history: int = 1024, warm_start_weights: np.ndarray | None = None):
+        """`warm_start_weights`: FP32 weights of the warm-start CNN (None =
+        plain ICP from the previous pose)."""
         self.cfg = cfg
         d = N.TrackerDesc()
         d.camera = cfg.camera()
@@ -280,6 +291,10 @@ class Tracker:
         d.initial_pose = (C.c_double * 16)(*np.asarray(initial_pose, np.float64).reshape(16))
         d.use_graph = 1 if use_graph else 0
         d.pose_history = pose_history
+        self._weights = None
+        if warm_start_weights is not None:
+            self._weights = np.ascontiguousarray(warm_start_weights, np.float32)
+            d.warm_start_weights = self._weights.ctypes.data
         h = C.c_void_p()
         N.check("of_tracker_create", N.lib().of_tracker_create(C.byref(d), C.byref(h)))
         self._h = h

@@ -30,6 +30,8 @@ CUDA_SOURCES = [
     "of_icp.cu",
     "of_tracker.cu",
     "of_adapters.cu",
+    "of_synth_gpu.cu",
+    "of_cnn.cu",
 ]
 SYNTH_SOURCES = ["of_synth.cpp"]
 
@@ -62,7 +64,8 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> dict[str, Path]
     BUILD.mkdir(exist_ok=True)
     LIBDIR.mkdir(exist_ok=True)
     nvcc = _nvcc()
-    headers = sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "openfusion_b200.h"]
+    headers = sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "openfusion_b200.h",
+                                           CSRC / "of_synth.h"]
     objs = []
     jobs = []
     for src in CUDA_SOURCES:

@@ -1,0 +1,566 @@
+// of_cnn.cu -- the learned ICP warm start: a small BF16 CNN that maps a pair
+// of 80x60 depth images (previous, current frame) to the 6-DoF motion between
+// them, with its own forward, backward and Adam kernels.
+//
+// No reference counterpart (the reference tracks with plain ICP only,
+// Source/src/ICP.cpp:84-182). Network (NCHW, batch b):
+//   in  2 x 60 x 80   depth (m) minus the previous frame's mean valid depth
+//   c1  conv 5x5 s2 p2  2 -> 16, ReLU    16 x 30 x 40
+//   c2  conv 3x3 s2 p1 16 -> 32, ReLU    32 x 15 x 20
+//   c3  conv 3x3 s2 p1 32 -> 64, ReLU    64 x  8 x 10
+//   c4  conv 3x3 s2 p1 64 -> 128, ReLU  128 x  4 x  5
+//   f1  2560 -> 160, ReLU
+//   f2  160 -> 6   (rotation vector x 10 rad^-1, translation / 100 mm)
+// 508,534 parameters. Mixed precision: weights and stored activations in
+// BF16, every sum in FP32, gradients, master weights and Adam moments in
+// FP32. Every reduction runs in a fixed order (no atomics), so a training run
+// is reproducible bit for bit.
+#include <cuda_bf16.h>
+
+#include "of_common.cuh"
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+struct ConvSpec {
+  int ci, co, k, s, p, hi, wi, ho, wo;
+};
+constexpr int kLayers = 6;
+constexpr ConvSpec kConv[4] = {{2, 16, 5, 2, 2, 60, 80, 30, 40},
+                               {16, 32, 3, 2, 1, 30, 40, 15, 20},
+                               {32, 64, 3, 2, 1, 15, 20, 8, 10},
+                               {64, 128, 3, 2, 1, 8, 10, 4, 5}};
+constexpr int kF1In = 128 * 4 * 5, kF1Out = 160, kF2Out = 6;
+constexpr int kInH = 60, kInW = 80;
+
+constexpr long conv_w(int l) { return (long)kConv[l].co * kConv[l].ci * kConv[l].k * kConv[l].k; }
+// parameter offsets (floats): [w0 b0 w1 b1 w2 b2 w3 b3 wf1 bf1 wf2 bf2]
+constexpr long kOffW0 = 0, kOffB0 = kOffW0 + conv_w(0);
+constexpr long kOffW1 = kOffB0 + 16, kOffB1 = kOffW1 + conv_w(1);
+constexpr long kOffW2 = kOffB1 + 32, kOffB2 = kOffW2 + conv_w(2);
+constexpr long kOffW3 = kOffB2 + 64, kOffB3 = kOffW3 + conv_w(3);
+constexpr long kOffF1 = kOffB3 + 128, kOffBF1 = kOffF1 + (long)kF1In * kF1Out;
+constexpr long kOffF2 = kOffBF1 + kF1Out, kOffBF2 = kOffF2 + (long)kF1Out * kF2Out;
+constexpr long kParams = kOffBF2 + kF2Out;
+static_assert(kParams == 508534, "parameter count");
+
+// per-sample activation sizes: input, c1..c4, f1 (BF16) and the output (FP32)
+constexpr long kActIn = 2L * kInH * kInW;
+constexpr long kAct[4] = {16L * 30 * 40, 32L * 15 * 20, 64L * 8 * 10, 128L * 4 * 5};
+
+// Workspace (per batch b): BF16 activations a1..a4, f1; FP32 output; FP32
+// gradients g1..g4, gf1, gout (activation-sized).
+struct CnnWs {
+  bf16 *a[4];
+  bf16 *f1;
+  float *out;
+  float *g[4];
+  float *gf1;
+  float *gout;
+  float *loss;  // [b] per-sample losses, then their sum at [b]
+  size_t total;
+};
+inline size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
+CnnWs ws_layout(void *base, int b) {
+  CnnWs w;
+  char *p = (char *)base;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { char *q = p ? p + off : nullptr; off += a256(bytes); return q; };
+  for (int l = 0; l < 4; ++l) w.a[l] = (bf16 *)take((size_t)b * kAct[l] * sizeof(bf16));
+  w.f1 = (bf16 *)take((size_t)b * kF1Out * sizeof(bf16));
+  w.out = (float *)take((size_t)b * kF2Out * sizeof(float));
+  for (int l = 0; l < 4; ++l) w.g[l] = (float *)take((size_t)b * kAct[l] * sizeof(float));
+  w.gf1 = (float *)take((size_t)b * kF1Out * sizeof(float));
+  w.gout = (float *)take((size_t)b * kF2Out * sizeof(float));
+  w.loss = (float *)take((size_t)(b + 1) * sizeof(float));
+  w.total = off;
+  return w;
+}
+
+__device__ __forceinline__ float bf(bf16 x) { return __bfloat162float(x); }
+
+// ---------------------------------------------------------------- input --
+
+// One block per pair: 8x8 (in general (W/80) x (H/60)) block means of the
+// valid depths of both frames, in metres, minus the mean of the previous
+// frame's valid block means; empty blocks are 0.
+__global__ void __launch_bounds__(256) k_cnn_input(const uint16_t *__restrict__ prev,
+                                                   const uint16_t *__restrict__ cur, int w,
+                                                   int h, long pair_stride,
+                                                   bf16 *__restrict__ in) {
+  __shared__ float s_val[2][kInH * kInW];
+  __shared__ float s_sum[256];
+  __shared__ int s_cnt[256];
+  const int b = blockIdx.x;
+  const int bx = w / kInW, by = h / kInH;
+  const uint16_t *src[2] = {prev + (size_t)b * pair_stride, cur + (size_t)b * pair_stride};
+  float lsum = 0.f;
+  int lcnt = 0;
+  for (int f = 0; f < 2; ++f)
+    for (int c = threadIdx.x; c < kInH * kInW; c += blockDim.x) {
+      const int cy = c / kInW, cx = c % kInW;
+      float acc = 0.f;
+      int n = 0;
+      for (int y = 0; y < by; ++y)
+        for (int x = 0; x < bx; ++x) {
+          const uint16_t d = src[f][(size_t)(cy * by + y) * w + cx * bx + x];
+          if (d) { acc += (float)d; ++n; }
+        }
+      const float v = n ? acc / (1000.f * n) : 0.f;
+      s_val[f][c] = v;
+      if (f == 0 && n) { lsum += v; ++lcnt; }
+    }
+  s_sum[threadIdx.x] = lsum;
+  s_cnt[threadIdx.x] = lcnt;
+  __syncthreads();
+  for (int span = blockDim.x / 2; span > 0; span >>= 1) {
+    if (threadIdx.x < span) {
+      s_sum[threadIdx.x] += s_sum[threadIdx.x + span];
+      s_cnt[threadIdx.x] += s_cnt[threadIdx.x + span];
+    }
+    __syncthreads();
+  }
+  const float mu = s_cnt[0] ? s_sum[0] / (float)s_cnt[0] : 0.f;
+  for (int f = 0; f < 2; ++f)
+    for (int c = threadIdx.x; c < kInH * kInW; c += blockDim.x) {
+      const float v = s_val[f][c];
+      in[(size_t)b * kActIn + (size_t)f * kInH * kInW + c] = __float2bfloat16_rn(v > 0.f ? v - mu : 0.f);
+    }
+}
+
+// ---------------------------------------------------------------- convs --
+
+// out[b, co, oy, ox] = relu(bias[co] + sum_{ci, ky, kx} w[co, ci, ky, kx] in[b, ci, iy, ix])
+template <int K, int S, int P>
+__global__ void __launch_bounds__(256) k_conv_fwd(const bf16 *__restrict__ in,
+                                                  const bf16 *__restrict__ wt,
+                                                  const float *__restrict__ bias, ConvSpec c,
+                                                  int batch, bf16 *__restrict__ out) {
+  const long total = (long)batch * c.co * c.ho * c.wo;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const int ox = (int)(i % c.wo), oy = (int)((i / c.wo) % c.ho);
+    const int co = (int)((i / ((long)c.wo * c.ho)) % c.co), b = (int)(i / ((long)c.wo * c.ho * c.co));
+    float acc = bias[co];
+    const bf16 *ib = in + (size_t)b * c.ci * c.hi * c.wi;
+    const bf16 *wb = wt + (size_t)co * c.ci * K * K;
+    for (int ci = 0; ci < c.ci; ++ci) {
+#pragma unroll
+      for (int ky = 0; ky < K; ++ky) {
+        const int iy = oy * S - P + ky;
+        if ((unsigned)iy >= (unsigned)c.hi) continue;
+#pragma unroll
+        for (int kx = 0; kx < K; ++kx) {
+          const int ix = ox * S - P + kx;
+          if ((unsigned)ix >= (unsigned)c.wi) continue;
+          acc = fmaf(bf(wb[(ci * K + ky) * K + kx]), bf(ib[((size_t)ci * c.hi + iy) * c.wi + ix]), acc);
+        }
+      }
+    }
+    out[i] = __float2bfloat16_rn(fmaxf(acc, 0.f));
+  }
+}
+
+// gin[b, ci, iy, ix] = sum_{co, ky, kx: iy = oy S - P + ky} w[co, ci, ky, kx] gout[b, co, oy, ox],
+// with gout the gradient at the pre-activation (masked by this layer's ReLU).
+template <int K, int S, int P>
+__global__ void __launch_bounds__(256) k_conv_bwd_data(const float *__restrict__ gpost,
+                                                       const bf16 *__restrict__ act,
+                                                       const bf16 *__restrict__ wt, ConvSpec c,
+                                                       int batch, float *__restrict__ gin) {
+  const long total = (long)batch * c.ci * c.hi * c.wi;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const int ix = (int)(i % c.wi), iy = (int)((i / c.wi) % c.hi);
+    const int ci = (int)((i / ((long)c.wi * c.hi)) % c.ci), b = (int)(i / ((long)c.wi * c.hi * c.ci));
+    float acc = 0.f;
+    for (int co = 0; co < c.co; ++co) {
+      const size_t gb = ((size_t)b * c.co + co) * c.ho * c.wo;
+      const bf16 *wb = wt + ((size_t)co * c.ci + ci) * K * K;
+#pragma unroll
+      for (int ky = 0; ky < K; ++ky) {
+        const int ny = iy + P - ky;
+        if (ny < 0 || ny % S) continue;
+        const int oy = ny / S;
+        if (oy >= c.ho) continue;
+#pragma unroll
+        for (int kx = 0; kx < K; ++kx) {
+          const int nx = ix + P - kx;
+          if (nx < 0 || nx % S) continue;
+          const int ox = nx / S;
+          if (ox >= c.wo) continue;
+          const size_t o = gb + (size_t)oy * c.wo + ox;
+          const float g = bf(act[o]) > 0.f ? gpost[o] : 0.f;
+          acc = fmaf(bf(wb[ky * K + kx]), g, acc);
+        }
+      }
+    }
+    gin[i] = acc;
+  }
+}
+
+// gw[co, ci, ky, kx] = sum_{b, oy, ox} gpre[b, co, oy, ox] in[b, ci, oy S - P + ky, ox S - P + kx];
+// gb[co] = sum gpre[b, co, ., .]. One block per (co, ci): each thread sums a
+// fixed strided share of (b, oy, ox) for all K*K taps, then a tree.
+template <int K, int S, int P>
+__global__ void __launch_bounds__(256) k_conv_bwd_weight(const float *__restrict__ gpost,
+                                                         const bf16 *__restrict__ act,
+                                                         const bf16 *__restrict__ in, ConvSpec c,
+                                                         int batch, float *__restrict__ gw,
+                                                         float *__restrict__ gbias) {
+  __shared__ float s_red[256][K * K + 1];
+  const int co = blockIdx.x / c.ci, ci = blockIdx.x % c.ci;
+  float acc[K * K + 1];
+#pragma unroll
+  for (int t = 0; t <= K * K; ++t) acc[t] = 0.f;
+  const long n = (long)batch * c.ho * c.wo;
+  for (long q = threadIdx.x; q < n; q += blockDim.x) {
+    const int ox = (int)(q % c.wo), oy = (int)((q / c.wo) % c.ho), b = (int)(q / ((long)c.wo * c.ho));
+    const size_t o = (((size_t)b * c.co + co) * c.ho + oy) * c.wo + ox;
+    const float g = bf(act[o]) > 0.f ? gpost[o] : 0.f;
+    if (g == 0.f) continue;
+    const bf16 *ib = in + ((size_t)b * c.ci + ci) * c.hi * c.wi;
+#pragma unroll
+    for (int ky = 0; ky < K; ++ky) {
+      const int iy = oy * S - P + ky;
+      if ((unsigned)iy >= (unsigned)c.hi) continue;
+#pragma unroll
+      for (int kx = 0; kx < K; ++kx) {
+        const int ix = ox * S - P + kx;
+        if ((unsigned)ix >= (unsigned)c.wi) continue;
+        acc[ky * K + kx] = fmaf(g, bf(ib[(size_t)iy * c.wi + ix]), acc[ky * K + kx]);
+      }
+    }
+    acc[K * K] += g;
+  }
+#pragma unroll
+  for (int t = 0; t <= K * K; ++t) s_red[threadIdx.x][t] = acc[t];
+  __syncthreads();
+  for (int span = 128; span > 0; span >>= 1) {
+    if ((int)threadIdx.x < span)
+      for (int t = 0; t <= K * K; ++t) s_red[threadIdx.x][t] += s_red[threadIdx.x + span][t];
+    __syncthreads();
+  }
+  if ((int)threadIdx.x < K * K) gw[((size_t)co * c.ci + ci) * K * K + threadIdx.x] = s_red[0][threadIdx.x];
+  if (ci == 0 && threadIdx.x == 0) gbias[co] = s_red[0][K * K];
+}
+
+// ------------------------------------------------------------------- fc --
+
+// out[b, j] = act(bias[j] + sum_i w[j, i] in[b, i]); one warp per (b, j).
+template <bool RELU, typename TOut>
+__global__ void __launch_bounds__(256) k_fc_fwd(const bf16 *__restrict__ in,
+                                                const bf16 *__restrict__ wt,
+                                                const float *__restrict__ bias, int nin, int nout,
+                                                int batch, TOut *__restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (warp >= (long)batch * nout) return;  // warp-uniform
+  const int j = (int)(warp % nout), b = (int)(warp / nout);
+  float acc = 0.f;
+  for (int i = lane; i < nin; i += 32)
+    acc = fmaf(bf(wt[(size_t)j * nin + i]), bf(in[(size_t)b * nin + i]), acc);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) {
+    float v = acc + bias[j];
+    if (RELU) v = fmaxf(v, 0.f);
+    if constexpr (sizeof(TOut) == 2) out[warp] = __float2bfloat16_rn(v);
+    else out[warp] = v;
+  }
+}
+
+// gin[b, i] = sum_j w[j, i] gpre[b, j] (gpre masked by the ReLU of `act`
+// when given); one thread per (b, i).
+__global__ void __launch_bounds__(256) k_fc_bwd_data(const float *__restrict__ gpost,
+                                                     const bf16 *__restrict__ act,
+                                                     const bf16 *__restrict__ wt, int nin,
+                                                     int nout, int batch,
+                                                     float *__restrict__ gin) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)batch * nin) return;
+  const int i = (int)(t % nin), b = (int)(t / nin);
+  float acc = 0.f;
+  for (int j = 0; j < nout; ++j) {
+    const size_t o = (size_t)b * nout + j;
+    const float g = (!act || bf(act[o]) > 0.f) ? gpost[o] : 0.f;
+    acc = fmaf(bf(wt[(size_t)j * nin + i]), g, acc);
+  }
+  gin[t] = acc;
+}
+
+// gw[j, i] = sum_b gpre[b, j] in[b, i]; gb[j] = sum_b gpre[b, j]; one thread
+// per (j, i) (i == nin: the bias).
+__global__ void __launch_bounds__(256) k_fc_bwd_weight(const float *__restrict__ gpost,
+                                                       const bf16 *__restrict__ act,
+                                                       const bf16 *__restrict__ in, int nin,
+                                                       int nout, int batch,
+                                                       float *__restrict__ gw,
+                                                       float *__restrict__ gbias) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)nout * (nin + 1)) return;
+  const int i = (int)(t % (nin + 1)), j = (int)(t / (nin + 1));
+  float acc = 0.f;
+  for (int b = 0; b < batch; ++b) {
+    const size_t o = (size_t)b * nout + j;
+    const float g = (!act || bf(act[o]) > 0.f) ? gpost[o] : 0.f;
+    acc = fmaf(g, i < nin ? bf(in[(size_t)b * nin + i]) : 1.f, acc);
+  }
+  if (i < nin) gw[(size_t)j * nin + i] = acc;
+  else gbias[j] = acc;
+}
+
+// ----------------------------------------------------------------- loss --
+
+// Mean over the batch of sum_k wk (out - target)^2; gout = d loss / d out.
+// loss[b] per sample, loss[batch] the mean (fixed-order sum, one thread).
+__global__ void k_loss(const float *__restrict__ out, const float *__restrict__ target,
+                       const float *__restrict__ wk, int batch, float *__restrict__ gout,
+                       float *__restrict__ loss) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < batch) {
+    float l = 0.f;
+    for (int k = 0; k < kF2Out; ++k) {
+      const float e = out[b * kF2Out + k] - target[b * kF2Out + k];
+      l = fmaf(wk[k] * e, e, l);
+      gout[b * kF2Out + k] = 2.f * wk[k] * e / (float)batch;
+    }
+    loss[b] = l;
+  }
+}
+__global__ void k_loss_sum(float *loss, int batch) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  float s = 0.f;
+  for (int b = 0; b < batch; ++b) s += loss[b];
+  loss[batch] = s / (float)batch;
+}
+
+// ---------------------------------------------------------- init / adam --
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// He-uniform weights (bound sqrt(6 / fan_in)), zero biases.
+__global__ void k_cnn_init(float *__restrict__ master, bf16 *__restrict__ mirror, uint64_t seed) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kParams) return;
+  long fan = 0;  // 0 for a bias
+  if (i >= kOffW0 && i < kOffB0) fan = 2 * 5 * 5;
+  else if (i >= kOffW1 && i < kOffB1) fan = 16 * 3 * 3;
+  else if (i >= kOffW2 && i < kOffB2) fan = 32 * 3 * 3;
+  else if (i >= kOffW3 && i < kOffB3) fan = 64 * 3 * 3;
+  else if (i >= kOffF1 && i < kOffBF1) fan = kF1In;
+  else if (i >= kOffF2 && i < kOffBF2) fan = kF1Out;
+  const bool bias = fan == 0;
+  float v = 0.f;
+  if (!bias) {
+    const double u = ((mix64(seed ^ mix64((uint64_t)i)) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+    v = (float)((2.0 * u - 1.0) * sqrt(6.0 / (double)fan));
+  }
+  master[i] = v;
+  mirror[i] = __float2bfloat16_rn(v);
+}
+
+__global__ void k_adam(float *__restrict__ master, bf16 *__restrict__ mirror,
+                       const float *__restrict__ grad, float *__restrict__ m, float *__restrict__ v,
+                       float lr, float b1, float b2, float eps, float c1, float c2) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kParams) return;
+  const float g = grad[i];
+  const float mi = fmaf(b1, m[i], (1.f - b1) * g);
+  const float vi = fmaf(b2, v[i], (1.f - b2) * g * g);
+  m[i] = mi;
+  v[i] = vi;
+  const float p = master[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+  master[i] = p;
+  mirror[i] = __float2bfloat16_rn(p);
+}
+
+unsigned blocks_for(long n) { return (unsigned)((n + 255) / 256 < 148L * 64 ? (n + 255) / 256 : 148L * 64); }
+
+template <int K, int S, int P>
+void conv_fwd(const bf16 *in, const bf16 *w, const float *b, const ConvSpec &c, int batch, bf16 *out,
+              cudaStream_t s) {
+  k_conv_fwd<K, S, P><<<blocks_for((long)batch * c.co * c.ho * c.wo), 256, 0, s>>>(in, w, b, c, batch, out);
+}
+
+void forward(const bf16 *pw, const float *pm, const bf16 *in, int batch, const CnnWs &w,
+             cudaStream_t s) {
+  const bf16 *x = in;
+  conv_fwd<5, 2, 2>(x, pw + kOffW0, pm + kOffB0, kConv[0], batch, w.a[0], s);
+  conv_fwd<3, 2, 1>(w.a[0], pw + kOffW1, pm + kOffB1, kConv[1], batch, w.a[1], s);
+  conv_fwd<3, 2, 1>(w.a[1], pw + kOffW2, pm + kOffB2, kConv[2], batch, w.a[2], s);
+  conv_fwd<3, 2, 1>(w.a[2], pw + kOffW3, pm + kOffB3, kConv[3], batch, w.a[3], s);
+  const long w1 = (long)batch * kF1Out * 32, w2 = (long)batch * kF2Out * 32;
+  k_fc_fwd<true, bf16><<<(unsigned)((w1 + 255) / 256), 256, 0, s>>>(w.a[3], pw + kOffF1, pm + kOffBF1,
+                                                                   kF1In, kF1Out, batch, w.f1);
+  k_fc_fwd<false, float><<<(unsigned)((w2 + 255) / 256), 256, 0, s>>>(w.f1, pw + kOffF2, pm + kOffBF2,
+                                                                     kF1Out, kF2Out, batch, w.out);
+}
+
+template <int K, int S, int P>
+void conv_bwd(const float *gpost, const bf16 *act, const bf16 *in, const bf16 *wt, const ConvSpec &c,
+              int batch, float *gin, float *gw, float *gb, cudaStream_t s) {
+  k_conv_bwd_weight<K, S, P><<<c.co * c.ci, 256, 0, s>>>(gpost, act, in, c, batch, gw, gb);
+  if (gin)
+    k_conv_bwd_data<K, S, P><<<blocks_for((long)batch * c.ci * c.hi * c.wi), 256, 0, s>>>(
+        gpost, act, wt, c, batch, gin);
+}
+
+}  // namespace
+
+extern "C" of_status_t of_cnn_param_count(int64_t *count) {
+  if (!count) return OF_ERR_INVALID_ARGUMENT;
+  *count = kParams;
+  return OF_OK;
+}
+
+extern "C" of_status_t of_cnn_workspace_bytes(int32_t batch, size_t *bytes) {
+  if (batch < 1 || batch > 65536 || !bytes) return OF_ERR_INVALID_ARGUMENT;
+  *bytes = ws_layout(nullptr, batch).total;
+  return OF_OK;
+}
+
+extern "C" of_status_t of_cnn_init(float *d_master, uint16_t *d_params, uint64_t seed,
+                                   of_stream_t s) {
+  if (!d_master || !d_params) return OF_ERR_INVALID_ARGUMENT;
+  k_cnn_init<<<(unsigned)((kParams + 255) / 256), 256, 0, (cudaStream_t)s>>>(d_master, (bf16 *)d_params, seed);
+  return of_launch_status();
+}
+
+extern "C" of_status_t of_cnn_input(const uint16_t *d_prev, const uint16_t *d_cur, int32_t width,
+                                    int32_t height, int32_t batch, int64_t pair_stride,
+                                    uint16_t *d_input, of_stream_t s) {
+  if (!d_prev || !d_cur || !d_input || batch < 1 || batch > 65535 || width < kInW ||
+      height < kInH || width % kInW || height % kInH || width / kInW != height / kInH ||
+      (batch > 1 && pair_stride < (int64_t)width * height))
+    return OF_ERR_INVALID_ARGUMENT;
+  k_cnn_input<<<batch, 256, 0, (cudaStream_t)s>>>(d_prev, d_cur, width, height, (long)pair_stride,
+                                                  (bf16 *)d_input);
+  return of_launch_status();
+}
+
+extern "C" of_status_t of_cnn_forward(const uint16_t *d_params, const float *d_master,
+                                      const uint16_t *d_input, int32_t batch, void *d_ws,
+                                      float *d_out, of_stream_t s) {
+  if (!d_params || !d_master || !d_input || !d_ws || batch < 1 || batch > 65536)
+    return OF_ERR_INVALID_ARGUMENT;
+  CnnWs w = ws_layout(d_ws, batch);
+  forward((const bf16 *)d_params, d_master, (const bf16 *)d_input, batch, w, (cudaStream_t)s);
+  if (d_out)
+    OF_CUDA_TRY(cudaMemcpyAsync(d_out, w.out, (size_t)batch * kF2Out * sizeof(float),
+                                cudaMemcpyDeviceToDevice, (cudaStream_t)s));
+  return of_launch_status();
+}
+
+extern "C" of_status_t of_cnn_backward(const uint16_t *d_params, const float *d_master,
+                                       const uint16_t *d_input, int32_t batch,
+                                       const float *d_target, const float *d_loss_weights,
+                                       void *d_ws, float *d_grad, float *d_loss, of_stream_t st) {
+  if (!d_params || !d_master || !d_input || !d_target || !d_loss_weights || !d_ws || !d_grad ||
+      batch < 1 || batch > 65536)
+    return OF_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = (cudaStream_t)st;
+  const bf16 *pw = (const bf16 *)d_params;
+  const bf16 *in = (const bf16 *)d_input;
+  CnnWs w = ws_layout(d_ws, batch);
+  forward(pw, d_master, in, batch, w, s);
+  k_loss<<<(batch + 255) / 256, 256, 0, s>>>(w.out, d_target, d_loss_weights, batch, w.gout, w.loss);
+  k_loss_sum<<<1, 32, 0, s>>>(w.loss, batch);
+  // f2 (linear): gradients of its weights and of f1's output
+  k_fc_bwd_weight<<<(unsigned)(((long)kF2Out * (kF1Out + 1) + 255) / 256), 256, 0, s>>>(
+      w.gout, nullptr, w.f1, kF1Out, kF2Out, batch, d_grad + kOffF2, d_grad + kOffBF2);
+  k_fc_bwd_data<<<(unsigned)(((long)batch * kF1Out + 255) / 256), 256, 0, s>>>(
+      w.gout, nullptr, pw + kOffF2, kF1Out, kF2Out, batch, w.gf1);
+  // f1 (ReLU)
+  k_fc_bwd_weight<<<(unsigned)(((long)kF1Out * (kF1In + 1) + 255) / 256), 256, 0, s>>>(
+      w.gf1, w.f1, w.a[3], kF1In, kF1Out, batch, d_grad + kOffF1, d_grad + kOffBF1);
+  k_fc_bwd_data<<<(unsigned)(((long)batch * kF1In + 255) / 256), 256, 0, s>>>(
+      w.gf1, w.f1, pw + kOffF1, kF1In, kF1Out, batch, w.g[3]);
+  // convs (ReLU), last to first; the first has no input gradient
+  conv_bwd<3, 2, 1>(w.g[3], w.a[3], w.a[2], pw + kOffW3, kConv[3], batch, w.g[2], d_grad + kOffW3,
+                    d_grad + kOffB3, s);
+  conv_bwd<3, 2, 1>(w.g[2], w.a[2], w.a[1], pw + kOffW2, kConv[2], batch, w.g[1], d_grad + kOffW2,
+                    d_grad + kOffB2, s);
+  conv_bwd<3, 2, 1>(w.g[1], w.a[1], w.a[0], pw + kOffW1, kConv[1], batch, w.g[0], d_grad + kOffW1,
+                    d_grad + kOffB1, s);
+  conv_bwd<5, 2, 2>(w.g[0], w.a[0], in, pw + kOffW0, kConv[0], batch, nullptr, d_grad + kOffW0,
+                    d_grad + kOffB0, s);
+  if (d_loss)
+    OF_CUDA_TRY(cudaMemcpyAsync(d_loss, w.loss + batch, sizeof(float), cudaMemcpyDeviceToDevice, s));
+  return of_launch_status();
+}
+
+extern "C" of_status_t of_cnn_adam(float *d_master, uint16_t *d_params, const float *d_grad,
+                                   float *d_m, float *d_v, int32_t step, float lr,
+                                   of_stream_t s) {
+  if (!d_master || !d_params || !d_grad || !d_m || !d_v || step < 1 || !(lr > 0.f))
+    return OF_ERR_INVALID_ARGUMENT;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = (float)(1.0 / (1.0 - pow((double)b1, step)));
+  const float c2 = (float)(1.0 / (1.0 - pow((double)b2, step)));
+  k_adam<<<(unsigned)((kParams + 255) / 256), 256, 0, (cudaStream_t)s>>>(
+      d_master, (bf16 *)d_params, d_grad, d_m, d_v, lr, b1, b2, 1e-8f, c1, c2);
+  return of_launch_status();
+}
+
+namespace {
+
+__global__ void k_cnn_mirror(const float *__restrict__ master, bf16 *__restrict__ mirror) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < kParams) mirror[i] = __float2bfloat16_rn(master[i]);
+}
+
+// warm = prev x [R | t] with R = exp(w) (Rodrigues; series for small angles),
+// w = out[0..2] / 10 rad, t = 100 out[3..5] mm: the predicted motion applied
+// in the previous camera's frame.
+__global__ void k_cnn_warm_pose(const float *__restrict__ out, const double *__restrict__ prev,
+                                double *__restrict__ warm) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double wx = out[0] * 0.1, wy = out[1] * 0.1, wz = out[2] * 0.1;
+  const double th2 = wx * wx + wy * wy + wz * wz;
+  double a, b;  // sin(th)/th, (1 - cos(th))/th^2
+  if (th2 < 1e-8) {
+    a = 1.0 - th2 / 6.0;
+    b = 0.5 - th2 / 24.0;
+  } else {
+    const double th = sqrt(th2);
+    a = sin(th) / th;
+    b = (1.0 - cos(th)) / th2;
+  }
+  const double K[9] = {0.0, -wz, wy, wz, 0.0, -wx, -wy, wx, 0.0};
+  double D[16] = {0};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double k2 = 0.0;
+      for (int m = 0; m < 3; ++m) k2 += K[3 * i + m] * K[3 * m + j];
+      D[4 * i + j] = (i == j ? 1.0 : 0.0) + a * K[3 * i + j] + b * k2;
+    }
+  D[3] = out[3] * 100.0; D[7] = out[4] * 100.0; D[11] = out[5] * 100.0; D[15] = 1.0;
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) {
+      double s = 0.0;
+      for (int m = 0; m < 4; ++m) s += prev[4 * i + m] * D[4 * m + j];
+      warm[4 * i + j] = s;
+    }
+}
+
+}  // namespace
+
+extern "C" of_status_t of_cnn_load(const float *d_master, uint16_t *d_params, of_stream_t s) {
+  if (!d_master || !d_params) return OF_ERR_INVALID_ARGUMENT;
+  k_cnn_mirror<<<(unsigned)((kParams + 255) / 256), 256, 0, (cudaStream_t)s>>>(d_master, (bf16 *)d_params);
+  return of_launch_status();
+}
+
+extern "C" of_status_t of_cnn_warm_pose(const float *d_out, const double *d_prev_pose,
+                                        double *d_warm_pose, of_stream_t s) {
+  if (!d_out || !d_prev_pose || !d_warm_pose) return OF_ERR_INVALID_ARGUMENT;
+  k_cnn_warm_pose<<<1, 32, 0, (cudaStream_t)s>>>(d_out, d_prev_pose, d_warm_pose);
+  return of_launch_status();
+}

@@ -53,6 +53,12 @@ extern "C" void of_default_params(of_filter_params_t *f, of_raycast_params_t *r,
     i->iters[0] = 10; i->iters[1] = 5; i->iters[2] = 4; i->iters[3] = 0;
     i->dist_thresh_mm = 25.0f;
     i->normal_thresh = 0.65f;
+    i->stop_rot_rad = 0.0f;
+    i->stop_trans_mm = 0.0f;
+    i->judge_max_rms_mm = 10.0f;
+    i->judge_min_inlier_frac = 0.3f;
+    i->judge_max_rot_rad = 0.05f;
+    i->judge_max_trans_mm = 50.0f;
   }
 }
 

@@ -53,9 +53,11 @@ struct IcpWorkspace {
   int pad0[2];
   double pose_init[16];
   double prior[16];
+  double warm_pose[16];  // this frame's warm start (of_icp_track_warm)
   int has_prior;
   int hold_barrier;  // fault injection: arrivals a grid barrier waits for that never come
-  int pad2[2];
+  int has_warm;
+  int pad2;
   float partials[kIcpMaxBlocks][32];
   float fused_partials[2][kFusedMaxBlocks][32];
 };
@@ -287,6 +289,8 @@ struct IcpPlan {
   int levels;
   float dist_thresh, normal_thresh;
   int cache_pts;  // model points a block keeps in shared memory per level
+  float stop_rot, stop_trans;  // early exit (0: every iteration)
+  float judge_rms, judge_frac, judge_rot, judge_trans;
 };
 
 // Grid-wide exchange of a co-resident grid. Each block publishes its row of
@@ -379,14 +383,16 @@ __device__ __forceinline__ void sincos_small(double x, double *s, double *c) {
 // substitution by one shuffle per unknown, rotation part negated
 // (ICP.cpp:162-168), dT = [Rz(g) Ry(b) Rx(a) | t] (ICP.cu:274-290) and
 // P <- dT P with one entry per lane. Returns the warp-uniform success flag;
-// *minpiv gets min d_j / max H_ii.
+// *minpiv gets min d_j / max H_ii, *inc_rot / *inc_trans the largest
+// rotation (rad) / translation (mm) component of the increment.
 __device__ __forceinline__ double shfl_d(double v, int src) {
   return __shfl_sync(0xffffffffu, v, src);
 }
 __device__ __forceinline__ int upper_index(int i, int j) {  // i <= j
   return i * 6 - i * (i - 1) / 2 + (j - i);
 }
-__device__ bool warp_solve_update(const float *tot, double *P, double *minpiv) {
+__device__ bool warp_solve_update(const float *tot, double *P, double *minpiv, float *inc_rot,
+                                  float *inc_trans) {
   const int lane = threadIdx.x & 31;
   const int row = lane < 6 ? lane : 5;  // lanes 6.. shadow row 5
   double a[7];
@@ -424,6 +430,8 @@ __device__ bool warp_solve_update(const float *tot, double *P, double *minpiv) {
     x[i] = shfl_d(a[6] * rmine, i);
     if (row < i) a[6] = fma(-a[i], x[i], a[6]);
   }
+  *inc_rot = (float)fmax(fabs(x[0]), fmax(fabs(x[1]), fabs(x[2])));
+  *inc_trans = (float)fmax(fabs(x[3]), fmax(fabs(x[4]), fabs(x[5])));
   double sv = 0.0, cv = 1.0;
   if (lane < 3) sincos_small(-x[lane], &sv, &cv);
   const double sa = shfl_d(sv, 0), ca = shfl_d(cv, 0);
@@ -487,6 +495,25 @@ __device__ __forceinline__ void try_row(float *acc, const Rigid &c2w, float4 s, 
   add_row(acc, s, ns, d);
 }
 
+// Judge of a warm-started ICP result P (warm start W): kept when the last
+// iteration's RMS point-to-plane residual, its inlier fraction among the
+// examined model points, and its rotation / translation away from W are all
+// within the thresholds.
+__device__ __forceinline__ bool judge_keep(const IcpPlan &plan, const double *W, const double *P,
+                                        double res_sq, int inliers, int examined) {
+  double tr = 0.0, dt2 = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    for (int k = 0; k < 3; ++k) tr += W[4 * k + i] * P[4 * k + i];
+    const double d = P[4 * i + 3] - W[4 * i + 3];
+    dt2 += d * d;
+  }
+  const double rot = acos(fmin(1.0, fmax(-1.0, 0.5 * (tr - 1.0))));
+  const double rms = sqrt(res_sq / (double)max(inliers, 1));
+  const double frac = (double)inliers / (double)max(examined, 1);
+  return rms <= plan.judge_rms && frac >= plan.judge_frac && rot <= plan.judge_rot &&
+         sqrt(dt2) <= plan.judge_trans;
+}
+
 // The whole multi-level ICP of one frame in one cooperative launch. Each
 // block owns every grid-th 32-pixel chunk of every level's model; at the
 // start of a level it copies its chunks' valid model points (vertex, normal)
@@ -507,206 +534,240 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   __shared__ float s_red[kFusedThreads / 32][32];
   __shared__ float s_tot[32];
   __shared__ int s_warp_n[kFusedThreads / 32];
-  __shared__ int s_stop, s_inl, s_its, s_err, s_npts;
+  __shared__ int s_stop, s_inl, s_its, s_err, s_npts, s_conv, s_warm, s_examined;
   __shared__ double s_res, s_piv;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int kWarps = kFusedThreads / 32;
-  if (threadIdx.x < 16) s_pose[threadIdx.x] = pose[threadIdx.x];
+  // pass 0 starts from the warm start when this frame has one, else from the
+  // frame's starting pose (pose == ws->pose_init); pass 1, from the starting
+  // pose, runs only when the judge replaces the warm-started result
+  const bool warm = ws->has_warm != 0;
+  if (threadIdx.x < 16) s_pose[threadIdx.x] = warm ? ws->warm_pose[threadIdx.x] : pose[threadIdx.x];
   if (threadIdx.x == 0) {
-    s_stop = 0; s_err = 0; s_its = 0; s_inl = 0; s_res = 0.0; s_piv = 0.0;
-    pose_to_rigid(pose, &s_c2w, &s_w2c);
+    s_stop = 0; s_err = 0; s_its = 0; s_inl = 0; s_res = 0.0; s_piv = 0.0; s_examined = 0;
+    s_warm = warm ? 1 : 0;
   }
-  __syncthreads();  // every thread reads s_stop / s_err / the pose below
+  __syncthreads();  // every thread reads the flags and the pose below
+  if (threadIdx.x == 0) pose_to_rigid(s_pose, &s_c2w, &s_w2c);
   // the fault-injection hook holds every exchange for an arrival that never
   // comes
   const bool hold = ws->hold_barrier > 0;
   const float dist2 = plan.dist_thresh * plan.dist_thresh, nthr = plan.normal_thresh;
   int iter_global = 0;
-  for (int l = plan.levels - 1; l >= 0 && !s_stop && !s_err; --l) {
-    const IcpLevel L = plan.lv[l];
-    const int npx = L.mw * L.mh;
-    // model pixels are dealt to blocks in chunks of 32 (one warp), round
-    // robin, so every block gets an even, spatially spread share: chunk
-    // c_k = block + k * grid, k = 0 .. my_chunks - 1; the first kc chunks
-    // are kept in shared memory, the rest is read at every iteration
-    const int G = (int)gridDim.x;
-    const int nchunks = (npx + 31) >> 5;
-    const int my_chunks = nchunks > (int)blockIdx.x ? (nchunks - 1 - (int)blockIdx.x) / G + 1 : 0;
-    const int kc = min(my_chunks, plan.cache_pts >> 5);
-    // ---- cache this block's valid model points of the level, in chunk order
-    if (threadIdx.x == 0) s_npts = 0;
-    __syncthreads();
-    for (int k0 = 0; k0 < kc; k0 += kWarps) {
-      const int k = k0 + warp;
-      const int p = ((int)blockIdx.x + k * G) * 32 + lane;
-      float4 s = make_float4(0.f, 0.f, 0.f, 0.f), ns = s;
-      bool valid = false;
-      if (k < kc && p < npx) {
-        s = __ldg(L.model + 2 * p);
-        ns = __ldg(L.model + 2 * p + 1);
-        valid = s.w != 0.f && ns.w != 0.f;
-      }
-      const unsigned m = __ballot_sync(0xffffffffu, valid);
-      if (lane == 0) s_warp_n[warp] = __popc(m);
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int l = plan.levels - 1; l >= 0 && !s_stop && !s_err; --l) {
+      const IcpLevel L = plan.lv[l];
+      const int npx = L.mw * L.mh;
+      // model pixels are dealt to blocks in chunks of 32 (one warp), round
+      // robin, so every block gets an even, spatially spread share: chunk
+      // c_k = block + k * grid, k = 0 .. my_chunks - 1; the first kc chunks
+      // are kept in shared memory, the rest is read at every iteration
+      const int G = (int)gridDim.x;
+      const int nchunks = (npx + 31) >> 5;
+      const int my_chunks = nchunks > (int)blockIdx.x ? (nchunks - 1 - (int)blockIdx.x) / G + 1 : 0;
+      const int kc = min(my_chunks, plan.cache_pts >> 5);
+      // ---- cache this block's valid model points of the level, in chunk order
+      if (threadIdx.x == 0) { s_npts = 0; s_conv = 0; }
       __syncthreads();
-      int off = s_npts;
-      for (int w = 0; w < warp; ++w) off += s_warp_n[w];
-      if (valid) {
-        const int slot = off + __popc(m & ((1u << lane) - 1u));
-        s_pts[2 * slot] = s;
-        s_pts[2 * slot + 1] = ns;
-      }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        int tot = 0;
-        for (int w = 0; w < kWarps; ++w) tot += s_warp_n[w];
-        s_npts += tot;
-      }
-      __syncthreads();
-    }
-    const int n = s_npts;
-    for (int it = 0; it < L.iters; ++it) {
-      float acc[kVals];
-#pragma unroll
-      for (int v = 0; v < kVals; ++v) acc[v] = 0.f;
-      // cached points, two per step
-      for (int i = threadIdx.x; i < n; i += 2 * kFusedThreads) {
-        const int j = i + kFusedThreads;
-        const int qA = associate(s_w2c, L.cam, s_pts[2 * i]);
-        const int qB = j < n ? associate(s_w2c, L.cam, s_pts[2 * j]) : -1;
-        float4 dA = make_float4(0.f, 0.f, 0.f, 0.f), cA = dA, dB = dA, cB = dA;
-        if (qA >= 0) { dA = __ldg(L.frame + 2 * qA); cA = __ldg(L.frame + 2 * qA + 1); }
-        if (qB >= 0) { dB = __ldg(L.frame + 2 * qB); cB = __ldg(L.frame + 2 * qB + 1); }
-        // the model points are read again from shared memory rather than
-        // held in registers across the gathers
-        asm volatile("" ::: "memory");
-        if (qA >= 0) try_row(acc, s_c2w, s_pts[2 * i], s_pts[2 * i + 1], dA, cA, dist2, nthr);
-        if (qB >= 0) try_row(acc, s_c2w, s_pts[2 * j], s_pts[2 * j + 1], dB, cB, dist2, nthr);
-      }
-      // the rest of the block's chunks, from global memory
-      for (int k = kc + warp; k < my_chunks; k += kWarps) {
+      for (int k0 = 0; k0 < kc; k0 += kWarps) {
+        const int k = k0 + warp;
         const int p = ((int)blockIdx.x + k * G) * 32 + lane;
-        if (p >= npx) continue;
-        const float4 s = __ldg(L.model + 2 * p);
-        const float4 ns = __ldg(L.model + 2 * p + 1);
-        if (s.w == 0.f || ns.w == 0.f) continue;
-        const int q = associate(s_w2c, L.cam, s);
-        if (q < 0) continue;
-        try_row(acc, s_c2w, s, ns, __ldg(L.frame + 2 * q), __ldg(L.frame + 2 * q + 1), dist2,
-                nthr);
-      }
-      // pairwise sums: a recursive-halving exchange across the warp (lanes
-      // trade half of their remaining values each step, 31 shuffles for 32
-      // values) leaves lane v with the warp's sum of value v; then a tree
-      // over the block's warps.
-      {
-        float r[32];
-#pragma unroll
-        for (int v = 0; v < 32; ++v) r[v] = v < kVals ? acc[v] : 0.f;
-#pragma unroll
-        for (int sft = 16; sft >= 1; sft >>= 1) {
-          const bool upper = (lane & sft) != 0;
-#pragma unroll
-          for (int i = 0; i < sft; ++i) {
-            float send = upper ? r[i] : r[i + sft];
-            float keep = upper ? r[i + sft] : r[i];
-            r[i] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
-          }
+        float4 s = make_float4(0.f, 0.f, 0.f, 0.f), ns = s;
+        bool valid = false;
+        if (k < kc && p < npx) {
+          s = __ldg(L.model + 2 * p);
+          ns = __ldg(L.model + 2 * p + 1);
+          valid = s.w != 0.f && ns.w != 0.f;
         }
-        s_red[warp][lane] = r[0];
-      }
-      __syncthreads();
-      const int buf = iter_global & 1;
-      const unsigned seq = (unsigned)iter_global + 1u;
-      if (warp == 0) {
-        float y[kWarps];
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) y[w] = s_red[w][lane];
-#pragma unroll
-        for (int span = 1; span < kWarps; span *= 2)
-#pragma unroll
-          for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
-        // publish: the values, then (release) the row's sequence number
-        float *row = ws->fused_partials[buf][blockIdx.x];
-        if (lane < kSeqSlot) row[lane] = lane < kVals ? y[0] : 0.f;
-        __syncwarp();
-        if (lane == 0) st_release_gpu(reinterpret_cast<unsigned *>(row + kSeqSlot), seq);
-        // the fault-injection hook: an arrival that never comes
-        if (hold && lane == 0 && !wait_seq(ws, &ws->bar_gen, 0xffffffffu)) atomicExch(&ws->error, 1);
-      }
-      // every block: wait for each block's row of this iteration (acquire),
-      // then Kahan over its strided share of the rows and a tree over the
-      // groups, in a fixed order. The acquire of a row's sequence number is
-      // this iteration's grid barrier.
-      {
-        constexpr int kPer = (kFusedMaxBlocks + kWarps - 1) / kWarps;
-        static_assert(kPer <= 32, "one polling lane per row");
-        const int v = lane, grp = warp;
-        // lane q < kPer polls row grp + q * kWarps; all of the warp's rows are
-        // polled in parallel, then every lane reads its value of each row
-        const int rq = grp + lane * kWarps;
-        const unsigned *seq_q = reinterpret_cast<const unsigned *>(
-            ws->fused_partials[buf][lane < kPer && rq < (int)gridDim.x ? rq : 0] + kSeqSlot);
-        const bool need = lane < kPer && rq < (int)gridDim.x;
-        unsigned spins = 0;
-        while (!__all_sync(0xffffffffu, !need || ld_acquire_gpu(seq_q) == seq)) {
-          if (++spins > kSpinLimit ||
-              ((spins & 255u) == 0u && ld_acquire_gpu(reinterpret_cast<unsigned *>(&ws->error)))) {
-            if (lane == 0) atomicExch(&ws->error, 1);
-            break;
-          }
-          __nanosleep(32);
+        const unsigned m = __ballot_sync(0xffffffffu, valid);
+        if (lane == 0) s_warp_n[warp] = __popc(m);
+        __syncthreads();
+        int off = s_npts;
+        for (int w = 0; w < warp; ++w) off += s_warp_n[w];
+        if (valid) {
+          const int slot = off + __popc(m & ((1u << lane) - 1u));
+          s_pts[2 * slot] = s;
+          s_pts[2 * slot + 1] = ns;
         }
-        __syncwarp();  // the polling lanes' acquires precede every lane's reads
-        float vals[kPer];
-#pragma unroll
-        for (int q = 0; q < kPer; ++q) {
-          const int r = grp + q * kWarps;
-          vals[q] = (v < kVals && r < (int)gridDim.x) ? __ldcg(&ws->fused_partials[buf][r][v]) : 0.f;
-        }
-        float sum = 0.f, c = 0.f;
-#pragma unroll
-        for (int q = 0; q < kPer; ++q) {
-          float y = vals[q] - c;
-          float t = sum + y;
-          c = (t - sum) - y;
-          sum = t;
-        }
-        s_red[grp][v] = sum - c;
-      }
-      __syncthreads();
-      // a wait that gave up ends this frame's tracking in every block
-      if (threadIdx.x == 0) s_err = ld_acquire_gpu(reinterpret_cast<unsigned *>(&ws->error)) != 0u;
-      __syncthreads();
-      if (s_err) break;
-      if (threadIdx.x < 32) {
-        float y[kWarps];
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) y[w] = s_red[w][threadIdx.x];
-#pragma unroll
-        for (int span = 1; span < kWarps; span *= 2)
-#pragma unroll
-          for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
-        s_tot[threadIdx.x] = y[0];
-        __syncwarp();
-        double minpiv = 0.0;
-        const bool ok = warp_solve_update(s_tot, s_pose, &minpiv);
+        __syncthreads();
         if (threadIdx.x == 0) {
-          s_its += 1;
-          s_inl = (int)s_tot[28];
-          s_res = (double)s_tot[27];
-          s_piv = minpiv;
-          if (!ok) {
-            for (int i = 0; i < 16; ++i) s_pose[i] = ws->pose_init[i];
-            s_stop = 1;
-          }
-          pose_to_rigid(s_pose, &s_c2w, &s_w2c);
+          int tot = 0;
+          for (int w = 0; w < kWarps; ++w) tot += s_warp_n[w];
+          s_npts += tot;
         }
+        __syncthreads();
       }
-      __syncthreads();
-      ++iter_global;
-      if (s_stop) break;
+      const int n = s_npts;
+      for (int it = 0; it < L.iters; ++it) {
+        float acc[kVals];
+        float examined = 0.f;  // model points that project into the frame
+#pragma unroll
+        for (int v = 0; v < kVals; ++v) acc[v] = 0.f;
+        // cached points, two per step
+        for (int i = threadIdx.x; i < n; i += 2 * kFusedThreads) {
+          const int j = i + kFusedThreads;
+          const int qA = associate(s_w2c, L.cam, s_pts[2 * i]);
+          const int qB = j < n ? associate(s_w2c, L.cam, s_pts[2 * j]) : -1;
+          float4 dA = make_float4(0.f, 0.f, 0.f, 0.f), cA = dA, dB = dA, cB = dA;
+          if (qA >= 0) { dA = __ldg(L.frame + 2 * qA); cA = __ldg(L.frame + 2 * qA + 1); }
+          if (qB >= 0) { dB = __ldg(L.frame + 2 * qB); cB = __ldg(L.frame + 2 * qB + 1); }
+          // the model points are read again from shared memory rather than
+          // held in registers across the gathers
+          asm volatile("" ::: "memory");
+          if (qA >= 0) {
+            examined += 1.f;
+            try_row(acc, s_c2w, s_pts[2 * i], s_pts[2 * i + 1], dA, cA, dist2, nthr);
+          }
+          if (qB >= 0) {
+            examined += 1.f;
+            try_row(acc, s_c2w, s_pts[2 * j], s_pts[2 * j + 1], dB, cB, dist2, nthr);
+          }
+        }
+        // the rest of the block's chunks, from global memory
+        for (int k = kc + warp; k < my_chunks; k += kWarps) {
+          const int p = ((int)blockIdx.x + k * G) * 32 + lane;
+          if (p >= npx) continue;
+          const float4 s = __ldg(L.model + 2 * p);
+          const float4 ns = __ldg(L.model + 2 * p + 1);
+          if (s.w == 0.f || ns.w == 0.f) continue;
+          const int q = associate(s_w2c, L.cam, s);
+          if (q < 0) continue;
+          examined += 1.f;
+          try_row(acc, s_c2w, s, ns, __ldg(L.frame + 2 * q), __ldg(L.frame + 2 * q + 1), dist2,
+                  nthr);
+        }
+        // pairwise sums: a recursive-halving exchange across the warp (lanes
+        // trade half of their remaining values each step, 31 shuffles for 32
+        // values) leaves lane v with the warp's sum of value v; then a tree
+        // over the block's warps. Value kVals is the examined-point count.
+        {
+          float r[32];
+#pragma unroll
+          for (int v = 0; v < 32; ++v) r[v] = v < kVals ? acc[v] : (v == kVals ? examined : 0.f);
+#pragma unroll
+          for (int sft = 16; sft >= 1; sft >>= 1) {
+            const bool upper = (lane & sft) != 0;
+#pragma unroll
+            for (int i = 0; i < sft; ++i) {
+              float send = upper ? r[i] : r[i + sft];
+              float keep = upper ? r[i + sft] : r[i];
+              r[i] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
+            }
+          }
+          s_red[warp][lane] = r[0];
+        }
+        __syncthreads();
+        const int buf = iter_global & 1;
+        const unsigned seq = (unsigned)iter_global + 1u;
+        if (warp == 0) {
+          float y[kWarps];
+#pragma unroll
+          for (int w = 0; w < kWarps; ++w) y[w] = s_red[w][lane];
+#pragma unroll
+          for (int span = 1; span < kWarps; span *= 2)
+#pragma unroll
+            for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
+          // publish: the values, then (release) the row's sequence number
+          float *row = ws->fused_partials[buf][blockIdx.x];
+          if (lane < kSeqSlot) row[lane] = lane <= kVals ? y[0] : 0.f;
+          __syncwarp();
+          if (lane == 0) st_release_gpu(reinterpret_cast<unsigned *>(row + kSeqSlot), seq);
+          // the fault-injection hook: an arrival that never comes
+          if (hold && lane == 0 && !wait_seq(ws, &ws->bar_gen, 0xffffffffu))
+            atomicExch(&ws->error, 1);
+        }
+        // every block: wait for each block's row of this iteration (acquire),
+        // then Kahan over its strided share of the rows and a tree over the
+        // groups, in a fixed order. The acquire of a row's sequence number is
+        // this iteration's grid barrier.
+        {
+          constexpr int kPer = (kFusedMaxBlocks + kWarps - 1) / kWarps;
+          static_assert(kPer <= 32, "one polling lane per row");
+          const int v = lane, grp = warp;
+          // lane q < kPer polls row grp + q * kWarps; all of the warp's rows
+          // are polled in parallel, then every lane reads its value of each row
+          const int rq = grp + lane * kWarps;
+          const unsigned *seq_q = reinterpret_cast<const unsigned *>(
+              ws->fused_partials[buf][lane < kPer && rq < (int)gridDim.x ? rq : 0] + kSeqSlot);
+          const bool need = lane < kPer && rq < (int)gridDim.x;
+          unsigned spins = 0;
+          while (!__all_sync(0xffffffffu, !need || ld_acquire_gpu(seq_q) == seq)) {
+            if (++spins > kSpinLimit ||
+                ((spins & 255u) == 0u && ld_acquire_gpu(reinterpret_cast<unsigned *>(&ws->error)))) {
+              if (lane == 0) atomicExch(&ws->error, 1);
+              break;
+            }
+            __nanosleep(32);
+          }
+          __syncwarp();  // the polling lanes' acquires precede every lane's reads
+          float vals[kPer];
+#pragma unroll
+          for (int q = 0; q < kPer; ++q) {
+            const int r = grp + q * kWarps;
+            vals[q] = (v <= kVals && r < (int)gridDim.x) ? __ldcg(&ws->fused_partials[buf][r][v]) : 0.f;
+          }
+          float sum = 0.f, c = 0.f;
+#pragma unroll
+          for (int q = 0; q < kPer; ++q) {
+            float y = vals[q] - c;
+            float t = sum + y;
+            c = (t - sum) - y;
+            sum = t;
+          }
+          s_red[grp][v] = sum - c;
+        }
+        __syncthreads();
+        // a wait that gave up ends this frame's tracking in every block
+        if (threadIdx.x == 0) s_err = ld_acquire_gpu(reinterpret_cast<unsigned *>(&ws->error)) != 0u;
+        __syncthreads();
+        if (s_err) break;
+        if (threadIdx.x < 32) {
+          float y[kWarps];
+#pragma unroll
+          for (int w = 0; w < kWarps; ++w) y[w] = s_red[w][threadIdx.x];
+#pragma unroll
+          for (int span = 1; span < kWarps; span *= 2)
+#pragma unroll
+            for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
+          s_tot[threadIdx.x] = y[0];
+          __syncwarp();
+          double minpiv = 0.0;
+          float inc_rot = 0.f, inc_trans = 0.f;
+          const bool ok = warp_solve_update(s_tot, s_pose, &minpiv, &inc_rot, &inc_trans);
+          if (threadIdx.x == 0) {
+            s_its += 1;
+            s_inl = (int)s_tot[28];
+            s_examined = (int)s_tot[kVals];
+            s_res = (double)s_tot[27];
+            s_piv = minpiv;
+            if (!ok) {
+              for (int i = 0; i < 16; ++i) s_pose[i] = ws->pose_init[i];
+              s_stop = 1;
+            } else if (plan.stop_rot > 0.f && inc_rot < plan.stop_rot &&
+                       inc_trans < plan.stop_trans) {
+              s_conv = 1;  // converged at this level
+            }
+            pose_to_rigid(s_pose, &s_c2w, &s_w2c);
+          }
+        }
+        __syncthreads();
+        ++iter_global;
+        if (s_stop || s_conv) break;
+      }
     }
+    // ---- judge a warm-started result; replace it by plain ICP if it fails
+    if (pass == 1 || !warm || s_err) break;
+    if (threadIdx.x == 0) {
+      const bool keep = !s_stop && judge_keep(plan, ws->warm_pose, s_pose, s_res, s_inl, s_examined);
+      s_warm = keep ? 1 : 2;
+      if (!keep) {
+        s_stop = 0;
+        for (int i = 0; i < 16; ++i) s_pose[i] = ws->pose_init[i];
+        pose_to_rigid(s_pose, &s_c2w, &s_w2c);
+      }
+    }
+    __syncthreads();
+    if (s_warm == 1) break;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     int err = *((volatile int *)&ws->error);
@@ -716,6 +777,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       stats->status = err ? 2 : (s_stop ? 1 : 0);
       stats->inliers = s_inl;
       stats->iterations = s_its;
+      stats->warm = warm ? s_warm : 0;
       stats->residual_sq = s_res;
       stats->min_pivot = s_piv;
     }
@@ -723,8 +785,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
 }
 
 // Start of a frame's tracking: remember the starting pose, apply the
-// optional warm-start increment, clear the flags.
-__global__ void k_icp_begin(double *pose, IcpWorkspace *ws, of_icp_stats_t *stats) {
+// optional prior increment, take the optional warm start (`warm`, a device
+// FP64 pose), clear the flags.
+__global__ void k_icp_begin(double *pose, IcpWorkspace *ws, of_icp_stats_t *stats,
+                            const double *warm) {
   // no partial-sum row of this frame has been published yet
   for (int i = threadIdx.x; i < 2 * kFusedMaxBlocks; i += blockDim.x)
     reinterpret_cast<unsigned *>(ws->fused_partials[i / kFusedMaxBlocks][i % kFusedMaxBlocks])[kSeqSlot] = 0u;
@@ -741,6 +805,9 @@ __global__ void k_icp_begin(double *pose, IcpWorkspace *ws, of_icp_stats_t *stat
     ws->has_prior = 0;  // a prior applies to one frame
   }
   for (int i = 0; i < 16; ++i) ws->pose_init[i] = pose[i];
+  ws->has_warm = warm != nullptr;
+  if (warm)
+    for (int i = 0; i < 16; ++i) ws->warm_pose[i] = warm[i];
   ws->ticket = 0;
   ws->stop = 0;
   ws->iterations = 0;
@@ -750,6 +817,7 @@ __global__ void k_icp_begin(double *pose, IcpWorkspace *ws, of_icp_stats_t *stat
     stats->status = 0;
     stats->inliers = 0;
     stats->iterations = 0;
+    stats->warm = 0;
     stats->residual_sq = 0.0;
     stats->min_pivot = 0.0;
   }
@@ -843,7 +911,7 @@ static of_status_t fused_shape(const of_camera_t *cam, FusedShape *fs) {
 // cooperative launch of the fused kernel.
 of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, const void *d_frame,
                           const void *d_model, double *pose, void *d_ws, of_icp_stats_t *stats,
-                          cudaStream_t s) {
+                          cudaStream_t s, const double *d_warm) {
   of_pyramid_layout_t lay;
   of_status_t st = of_pyramid_layout(cam, ip->levels, &lay);
   if (st != OF_OK) return st;
@@ -858,6 +926,12 @@ of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, con
   plan.cache_pts = fs.cache_pts;
   plan.dist_thresh = ip->dist_thresh_mm;
   plan.normal_thresh = ip->normal_thresh;
+  plan.stop_rot = ip->stop_rot_rad;
+  plan.stop_trans = ip->stop_trans_mm;
+  plan.judge_rms = ip->judge_max_rms_mm;
+  plan.judge_frac = ip->judge_min_inlier_frac;
+  plan.judge_rot = ip->judge_max_rot_rad;
+  plan.judge_trans = ip->judge_max_trans_mm;
   for (int l = 0; l < ip->levels; ++l) {
     of_camera_t cl = camera_level(*cam, l);
     plan.lv[l].cam = make_cam(cl);
@@ -867,7 +941,7 @@ of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, con
     plan.lv[l].mh = cl.height;
     plan.lv[l].iters = ip->iters[l];
   }
-  k_icp_begin<<<1, 32, 0, s>>>(pose, ws, stats);
+  k_icp_begin<<<1, 32, 0, s>>>(pose, ws, stats, d_warm);
   st = of_launch_status();
   if (st != OF_OK) return st;
   void *args[] = {&plan, &pose, &ws, &stats};
@@ -881,7 +955,17 @@ extern "C" of_status_t of_icp_track(const of_camera_t *cam, const of_icp_params_
                                     void *d_ws, of_icp_stats_t *stats, of_stream_t s) {
   if (!of_camera_valid(cam) || !icp_params_ok(ip) || !d_frame || !d_model || !pose || !d_ws)
     return OF_ERR_INVALID_ARGUMENT;
-  return of_icp_launch(cam, ip, d_frame, d_model, pose, d_ws, stats, (cudaStream_t)s);
+  return of_icp_launch(cam, ip, d_frame, d_model, pose, d_ws, stats, (cudaStream_t)s, nullptr);
+}
+
+extern "C" of_status_t of_icp_track_warm(const of_camera_t *cam, const of_icp_params_t *ip,
+                                         const void *d_frame, const void *d_model, double *pose,
+                                         const double *d_warm_pose, void *d_ws,
+                                         of_icp_stats_t *stats, of_stream_t s) {
+  if (!of_camera_valid(cam) || !icp_params_ok(ip) || !d_frame || !d_model || !pose ||
+      !d_warm_pose || !d_ws)
+    return OF_ERR_INVALID_ARGUMENT;
+  return of_icp_launch(cam, ip, d_frame, d_model, pose, d_ws, stats, (cudaStream_t)s, d_warm_pose);
 }
 
 extern "C" of_status_t of_icp_system(const of_camera_t *cam, const of_icp_params_t *ip,
@@ -965,5 +1049,5 @@ extern "C" of_status_t of_icp_track_static(const of_camera_t *cam, const of_icp_
   void *ws = nullptr;
   of_status_t st = static_icp_workspace(&ws);
   if (st != OF_OK) return st;
-  return of_icp_launch(cam, ip, d_frame, d_model, pose, ws, stats, (cudaStream_t)stream);
+  return of_icp_launch(cam, ip, d_frame, d_model, pose, ws, stats, (cudaStream_t)stream, nullptr);
 }

@@ -20,7 +20,7 @@ bool of_volume_valid(const of_volume_desc_t *d);
 size_t of_icp_workspace_size();
 of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, const void *d_frame,
                           const void *d_model, double *pose, void *d_ws, of_icp_stats_t *stats,
-                          cudaStream_t s);
+                          cudaStream_t s, const double *d_warm);
 of_status_t of_icp_set_prior(void *d_workspace, const double *prior_host, cudaStream_t s);
 
 struct of_tracker {
@@ -38,6 +38,15 @@ struct of_tracker {
   float *lambda = nullptr;
   void *scratch = nullptr;
   of_icp_stats_t *stats = nullptr;
+  // learned warm start (desc.warm_start_weights != NULL)
+  bool warm = false;
+  float *cnn_master = nullptr;
+  uint16_t *cnn_params = nullptr;
+  void *cnn_ws = nullptr;
+  uint16_t *cnn_in = nullptr;
+  float *cnn_out = nullptr;
+  double *warm_pose = nullptr;
+  uint16_t *prev_depth = nullptr;
   int hist_cap = 1024;
   int64_t frames = 0;
   int kernels_first = 0;
@@ -63,7 +72,16 @@ of_status_t enqueue_frame(of_tracker *t, bool track, cudaStream_t s) {
   if (track) {
     st = of_preprocess(&d.camera, &d.filter, t->depth, d.camera.width, t->frame, s);
     if (st != OF_OK) return st;
-    st = of_icp_launch(&d.camera, &d.icp, t->frame, t->model, t->pose, t->icp_ws, t->stats, s);
+    if (t->warm) {
+      // the CNN's motion estimate between the previous and this depth frame
+      st = of_cnn_input(t->prev_depth, t->depth, d.camera.width, d.camera.height, 1, 0, t->cnn_in, s);
+      if (st == OF_OK)
+        st = of_cnn_forward(t->cnn_params, t->cnn_master, t->cnn_in, 1, t->cnn_ws, t->cnn_out, s);
+      if (st == OF_OK) st = of_cnn_warm_pose(t->cnn_out, t->pose, t->warm_pose, s);
+      if (st != OF_OK) return st;
+    }
+    st = of_icp_launch(&d.camera, &d.icp, t->frame, t->model, t->pose, t->icp_ws, t->stats, s,
+                       t->warm ? t->warm_pose : nullptr);
     if (st != OF_OK) return st;
   }
   st = of_integrate_tiled(&d.volume, t->volume, &d.camera, t->depth, d.camera.width, t->pose,
@@ -73,7 +91,12 @@ of_status_t enqueue_frame(of_tracker *t, bool track, cudaStream_t s) {
                   nullptr, s);
   if (st != OF_OK) return st;
   k_record_pose<<<1, 32, 0, s>>>(t->pose, t->hist, t->hist_count, t->hist_cap);
-  return of_launch_status();
+  st = of_launch_status();
+  if (st == OF_OK && t->warm)  // the next frame's pair
+    OF_CUDA_TRY(cudaMemcpyAsync(t->prev_depth, t->depth,
+                                (size_t)d.camera.width * d.camera.height * sizeof(uint16_t),
+                                cudaMemcpyDeviceToDevice, s));
+  return st;
 }
 
 int count_kernel_nodes(cudaGraph_t g) {
@@ -111,7 +134,8 @@ void release(of_tracker *t) {
   if (t->g_first) cudaGraphExecDestroy(t->g_first);
   if (t->g_track) cudaGraphExecDestroy(t->g_track);
   void *bufs[] = {t->volume, t->frame, t->model, t->icp_ws, t->pose, t->hist, t->hist_count,
-                  t->depth, t->lambda, t->scratch, t->stats};
+                  t->depth, t->lambda, t->scratch, t->stats, t->cnn_master, t->cnn_params,
+                  t->cnn_ws, t->cnn_in, t->cnn_out, t->warm_pose, t->prev_depth};
   for (void *b : bufs)
     if (b) cudaFree(b);
   if (t->cap) cudaStreamDestroy(t->cap);
@@ -140,6 +164,15 @@ extern "C" of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_track
   of_lambda_bytes(&desc->camera, &lam_bytes);
   of_integrate_scratch_bytes(&desc->volume, &desc->camera, &scratch_bytes);
   size_t px = (size_t)desc->camera.width * desc->camera.height;
+  int64_t np = 0;
+  size_t cnn_ws = 0;
+  t->warm = desc->warm_start_weights != nullptr;
+  if (t->warm) {
+    const int w = desc->camera.width, h = desc->camera.height;
+    if (w % 80 || h % 60 || w / 80 != h / 60) { release(t); return OF_ERR_INVALID_ARGUMENT; }
+    of_cnn_param_count(&np);
+    of_cnn_workspace_bytes(1, &cnn_ws);
+  }
   struct { void **p; size_t n; } allocs[] = {
       {&t->volume, vol_bytes},
       {&t->frame, t->lay.total_bytes},
@@ -152,8 +185,16 @@ extern "C" of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_track
       {(void **)&t->lambda, lam_bytes},
       {&t->scratch, scratch_bytes},
       {(void **)&t->stats, sizeof(of_icp_stats_t)},
+      {(void **)&t->cnn_master, (size_t)np * sizeof(float)},
+      {(void **)&t->cnn_params, (size_t)np * sizeof(uint16_t)},
+      {&t->cnn_ws, cnn_ws},
+      {(void **)&t->cnn_in, t->warm ? 2 * 60 * 80 * sizeof(uint16_t) : 0},
+      {(void **)&t->cnn_out, t->warm ? 6 * sizeof(float) : 0},
+      {(void **)&t->warm_pose, t->warm ? 16 * sizeof(double) : 0},
+      {(void **)&t->prev_depth, t->warm ? px * sizeof(uint16_t) : 0},
   };
   for (auto &a : allocs) {
+    if (a.n == 0) continue;
     e = cudaMalloc(a.p, a.n);
     if (e != cudaSuccess) {
       cudaGetLastError();
@@ -169,6 +210,10 @@ extern "C" of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_track
             cudaMemsetAsync(t->frame, 0, t->lay.total_bytes, s) == cudaSuccess &&
             cudaMemcpyAsync(t->pose, desc->initial_pose, 16 * sizeof(double),
                             cudaMemcpyHostToDevice, s) == cudaSuccess;
+  if (ok && t->warm)
+    ok = cudaMemcpyAsync(t->cnn_master, desc->warm_start_weights, (size_t)np * sizeof(float),
+                         cudaMemcpyHostToDevice, s) == cudaSuccess &&
+         of_cnn_load(t->cnn_master, t->cnn_params, s) == OF_OK;
   if (!ok) { release(t); return of_set_cuda_error(cudaGetLastError()); }
   st = of_volume_reset(&desc->volume, t->volume, s);
   if (st == OF_OK) st = of_lambda_table(&desc->camera, t->lambda, s);
