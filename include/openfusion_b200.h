@@ -112,6 +112,10 @@ typedef struct of_icp_params {
   float judge_min_inlier_frac;
   float judge_max_rot_rad;
   float judge_max_trans_mm;
+  /* Pyramid levels a warm-started pass uses, finest first (0 = all): the
+   * coarse levels exist to pull in a large initial misalignment, which a
+   * good warm start does not have; the judge still guards the result. */
+  int32_t warm_levels;
 } of_icp_params_t;
 
 /* Per-frame ICP result, written by the device. */
@@ -366,13 +370,15 @@ of_status_t of_cnn_workspace_bytes(int32_t batch, size_t *bytes);
 /* He-uniform weights and zero biases from a seed. */
 of_status_t of_cnn_init(float *d_master, uint16_t *d_params, uint64_t seed, of_stream_t stream);
 /* Network input (BF16, batch x 2 x 60 x 80) of `batch` pairs of uint16 depth
- * frames of W x H (W = 80 k, H = 60 k): the mean of each k x k block's valid
- * depths in metres, minus the mean over the previous frame's non-empty
- * blocks; empty blocks are 0. Pair i is at d_prev + i * pair_stride and
- * d_cur + i * pair_stride (pixels). */
+ * frames of W x H (W = 80 k, H = 60 k), from the mean of each k x k block's
+ * valid depths in metres: channel 0 the previous frame's block means minus
+ * their mean over its non-empty blocks, channel 1 current minus previous
+ * block mean; empty blocks give 0. Pair i is at d_prev + i * pair_stride and
+ * d_cur + i * pair_stride (pixels). `d_cells`: scratch of batch x 2 x 60 x 80
+ * floats. */
 of_status_t of_cnn_input(const uint16_t *d_prev, const uint16_t *d_cur, int32_t width,
-                         int32_t height, int32_t batch, int64_t pair_stride, uint16_t *d_input,
-                         of_stream_t stream);
+                         int32_t height, int32_t batch, int64_t pair_stride, float *d_cells,
+                         uint16_t *d_input, of_stream_t stream);
 /* Forward pass; `d_out` (may be NULL) receives batch x 6 floats. */
 of_status_t of_cnn_forward(const uint16_t *d_params, const float *d_master,
                            const uint16_t *d_input, int32_t batch, void *d_workspace,

@@ -40,7 +40,7 @@ class IcpParams(C.Structure):
                 ("normal_thresh", C.c_float), ("stop_rot_rad", C.c_float),
                 ("stop_trans_mm", C.c_float), ("judge_max_rms_mm", C.c_float),
                 ("judge_min_inlier_frac", C.c_float), ("judge_max_rot_rad", C.c_float),
-                ("judge_max_trans_mm", C.c_float)]
+                ("judge_max_trans_mm", C.c_float), ("warm_levels", C.c_int32)]
 
 
 class IcpStats(C.Structure):
@@ -124,7 +124,8 @@ _SIGS = {
     "of_cnn_param_count": (c_status, [C.POINTER(C.c_int64)]),
     "of_cnn_workspace_bytes": (c_status, [C.c_int32, C.POINTER(C.c_size_t)]),
     "of_cnn_init": (c_status, [P, P, C.c_uint64, c_stream]),
-    "of_cnn_input": (c_status, [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int64, P, c_stream]),
+    "of_cnn_input": (c_status, [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int64, P, P,
+                                c_stream]),
     "of_cnn_forward": (c_status, [P, P, P, C.c_int32, P, P, c_stream]),
     "of_cnn_backward": (c_status, [P, P, P, C.c_int32, P, P, P, P, P, c_stream]),
     "of_cnn_adam": (c_status, [P, P, P, P, P, C.c_int32, C.c_float, c_stream]),

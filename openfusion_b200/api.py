@@ -49,6 +49,7 @@ class Config:
     judge_min_inlier_frac: float = 0.3
     judge_max_rot_rad: float = 0.05
     judge_max_trans_mm: float = 50.0
+    warm_levels: int = 0            # pyramid levels of a warm-started pass (0 = all)
     min_step_vox: float = 0.75
     far_step_frac: float = 0.8
     refine_iters: int = 3
@@ -79,7 +80,7 @@ class Config:
         return N.IcpParams(self.levels, it, self.dist_thresh_mm, self.normal_thresh,
                            self.stop_rot_rad, self.stop_trans_mm, self.judge_max_rms_mm,
                            self.judge_min_inlier_frac, self.judge_max_rot_rad,
-                           self.judge_max_trans_mm)
+                           self.judge_max_trans_mm, self.warm_levels)
 
     def radius(self) -> int:
         return self.radius_px if self.radius_px > 0 else int(np.ceil(2.0 * self.sigma_space_px))

@@ -4,7 +4,7 @@
 //
 // No reference counterpart (the reference tracks with plain ICP only,
 // Source/src/ICP.cpp:84-182). Network (NCHW, batch b):
-//   in  2 x 60 x 80   depth (m) minus the previous frame's mean valid depth
+//   in  2 x 60 x 80   previous depth (m) minus its mean; current - previous
 //   c1  conv 5x5 s2 p2  2 -> 16, ReLU    16 x 30 x 40
 //   c2  conv 3x3 s2 p1 16 -> 32, ReLU    32 x 15 x 20
 //   c3  conv 3x3 s2 p1 32 -> 64, ReLU    64 x  8 x 10
@@ -82,51 +82,63 @@ __device__ __forceinline__ float bf(bf16 x) { return __bfloat162float(x); }
 
 // ---------------------------------------------------------------- input --
 
-// One block per pair: 8x8 (in general (W/80) x (H/60)) block means of the
-// valid depths of both frames, in metres, minus the mean of the previous
-// frame's valid block means; empty blocks are 0.
-__global__ void __launch_bounds__(256) k_cnn_input(const uint16_t *__restrict__ prev,
+// Step 1 of the network input, one thread per (pair, frame, cell): the mean
+// of the valid depths of the cell's k x k pixels (k = W / 80 = H / 60), in
+// metres (0 for an empty cell).
+__global__ void __launch_bounds__(256) k_cnn_cells(const uint16_t *__restrict__ prev,
                                                    const uint16_t *__restrict__ cur, int w,
-                                                   int h, long pair_stride,
-                                                   bf16 *__restrict__ in) {
-  __shared__ float s_val[2][kInH * kInW];
+                                                   int h, long pair_stride, int batch,
+                                                   float *__restrict__ cells) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long)batch * kActIn) return;
+  const int c = (int)(i % (kInH * kInW)), f = (int)((i / (kInH * kInW)) % 2);
+  const int b = (int)(i / kActIn);
+  const int k = w / kInW;
+  const int cy = c / kInW, cx = c % kInW;
+  const uint16_t *src = (f ? cur : prev) + (size_t)b * pair_stride;
+  float acc = 0.f;
+  int n = 0;
+  for (int y = 0; y < k; ++y)
+    for (int x = 0; x < k; ++x) {
+      const uint16_t d = __ldg(src + (size_t)(cy * k + y) * w + cx * k + x);
+      if (d) { acc += (float)d; ++n; }
+    }
+  cells[i] = n ? acc / (1000.f * n) : 0.f;
+}
+
+// Step 2, one block per pair: channel 0 = previous cell minus the mean of
+// the previous frame's non-empty cells (fixed-order tree), channel 1 =
+// current cell minus previous cell (where both are non-empty); 0 elsewhere.
+// Stored in BF16: the difference channel keeps the small motion signal at
+// full relative precision (a depth near 2 m is only good to ~8 mm in BF16).
+__global__ void __launch_bounds__(256) k_cnn_center(const float *__restrict__ cells,
+                                                    bf16 *__restrict__ in) {
   __shared__ float s_sum[256];
   __shared__ int s_cnt[256];
   const int b = blockIdx.x;
-  const int bx = w / kInW, by = h / kInH;
-  const uint16_t *src[2] = {prev + (size_t)b * pair_stride, cur + (size_t)b * pair_stride};
+  const float *cp = cells + (size_t)b * kActIn;
   float lsum = 0.f;
   int lcnt = 0;
-  for (int f = 0; f < 2; ++f)
-    for (int c = threadIdx.x; c < kInH * kInW; c += blockDim.x) {
-      const int cy = c / kInW, cx = c % kInW;
-      float acc = 0.f;
-      int n = 0;
-      for (int y = 0; y < by; ++y)
-        for (int x = 0; x < bx; ++x) {
-          const uint16_t d = src[f][(size_t)(cy * by + y) * w + cx * bx + x];
-          if (d) { acc += (float)d; ++n; }
-        }
-      const float v = n ? acc / (1000.f * n) : 0.f;
-      s_val[f][c] = v;
-      if (f == 0 && n) { lsum += v; ++lcnt; }
-    }
+  for (int c = threadIdx.x; c < kInH * kInW; c += blockDim.x) {
+    const float v = cp[c];
+    if (v > 0.f) { lsum += v; ++lcnt; }
+  }
   s_sum[threadIdx.x] = lsum;
   s_cnt[threadIdx.x] = lcnt;
   __syncthreads();
   for (int span = blockDim.x / 2; span > 0; span >>= 1) {
-    if (threadIdx.x < span) {
+    if ((int)threadIdx.x < span) {
       s_sum[threadIdx.x] += s_sum[threadIdx.x + span];
       s_cnt[threadIdx.x] += s_cnt[threadIdx.x + span];
     }
     __syncthreads();
   }
   const float mu = s_cnt[0] ? s_sum[0] / (float)s_cnt[0] : 0.f;
-  for (int f = 0; f < 2; ++f)
-    for (int c = threadIdx.x; c < kInH * kInW; c += blockDim.x) {
-      const float v = s_val[f][c];
-      in[(size_t)b * kActIn + (size_t)f * kInH * kInW + c] = __float2bfloat16_rn(v > 0.f ? v - mu : 0.f);
-    }
+  for (int c = threadIdx.x; c < kInH * kInW; c += blockDim.x) {
+    const float p = cp[c], q = cp[kInH * kInW + c];
+    in[(size_t)b * kActIn + c] = __float2bfloat16_rn(p > 0.f ? p - mu : 0.f);
+    in[(size_t)b * kActIn + kInH * kInW + c] = __float2bfloat16_rn(p > 0.f && q > 0.f ? q - p : 0.f);
+  }
 }
 
 // ---------------------------------------------------------------- convs --
@@ -160,6 +172,33 @@ __global__ void __launch_bounds__(256) k_conv_fwd(const bf16 *__restrict__ in,
     }
     out[i] = __float2bfloat16_rn(fmaxf(acc, 0.f));
   }
+}
+
+// The same convolution for small batches (inference): one warp per output,
+// the ci x K x K taps dealt to the lanes in a fixed order, then a shuffle
+// tree; enough parallelism for a single pair.
+template <int K, int S, int P>
+__global__ void __launch_bounds__(256) k_conv_fwd_warp(const bf16 *__restrict__ in,
+                                                       const bf16 *__restrict__ wt,
+                                                       const float *__restrict__ bias, ConvSpec c,
+                                                       int batch, bf16 *__restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const long i = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= (long)batch * c.co * c.ho * c.wo) return;  // warp-uniform
+  const int ox = (int)(i % c.wo), oy = (int)((i / c.wo) % c.ho);
+  const int co = (int)((i / ((long)c.wo * c.ho)) % c.co), b = (int)(i / ((long)c.wo * c.ho * c.co));
+  const bf16 *ib = in + (size_t)b * c.ci * c.hi * c.wi;
+  const bf16 *wb = wt + (size_t)co * c.ci * K * K;
+  float acc = 0.f;
+  for (int tap = lane; tap < c.ci * K * K; tap += 32) {
+    const int ci = tap / (K * K), ky = (tap / K) % K, kx = tap % K;
+    const int iy = oy * S - P + ky, ix = ox * S - P + kx;
+    if ((unsigned)iy < (unsigned)c.hi && (unsigned)ix < (unsigned)c.wi)
+      acc = fmaf(bf(wb[tap]), bf(ib[((size_t)ci * c.hi + iy) * c.wi + ix]), acc);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) out[i] = __float2bfloat16_rn(fmaxf(acc + bias[co], 0.f));
 }
 
 // gin[b, ci, iy, ix] = sum_{co, ky, kx: iy = oy S - P + ky} w[co, ci, ky, kx] gout[b, co, oy, ox],
@@ -383,10 +422,16 @@ __global__ void k_adam(float *__restrict__ master, bf16 *__restrict__ mirror,
 
 unsigned blocks_for(long n) { return (unsigned)((n + 255) / 256 < 148L * 64 ? (n + 255) / 256 : 148L * 64); }
 
+constexpr int kSmallBatch = 16;  // up to this batch, one warp per conv output
+
 template <int K, int S, int P>
 void conv_fwd(const bf16 *in, const bf16 *w, const float *b, const ConvSpec &c, int batch, bf16 *out,
               cudaStream_t s) {
-  k_conv_fwd<K, S, P><<<blocks_for((long)batch * c.co * c.ho * c.wo), 256, 0, s>>>(in, w, b, c, batch, out);
+  const long n = (long)batch * c.co * c.ho * c.wo;
+  if (batch <= kSmallBatch)
+    k_conv_fwd_warp<K, S, P><<<(unsigned)((n * 32 + 255) / 256), 256, 0, s>>>(in, w, b, c, batch, out);
+  else
+    k_conv_fwd<K, S, P><<<blocks_for(n), 256, 0, s>>>(in, w, b, c, batch, out);
 }
 
 void forward(const bf16 *pw, const float *pm, const bf16 *in, int batch, const CnnWs &w,
@@ -435,13 +480,15 @@ extern "C" of_status_t of_cnn_init(float *d_master, uint16_t *d_params, uint64_t
 
 extern "C" of_status_t of_cnn_input(const uint16_t *d_prev, const uint16_t *d_cur, int32_t width,
                                     int32_t height, int32_t batch, int64_t pair_stride,
-                                    uint16_t *d_input, of_stream_t s) {
-  if (!d_prev || !d_cur || !d_input || batch < 1 || batch > 65535 || width < kInW ||
+                                    float *d_cells, uint16_t *d_input, of_stream_t s) {
+  if (!d_prev || !d_cur || !d_cells || !d_input || batch < 1 || batch > 65535 || width < kInW ||
       height < kInH || width % kInW || height % kInH || width / kInW != height / kInH ||
       (batch > 1 && pair_stride < (int64_t)width * height))
     return OF_ERR_INVALID_ARGUMENT;
-  k_cnn_input<<<batch, 256, 0, (cudaStream_t)s>>>(d_prev, d_cur, width, height, (long)pair_stride,
-                                                  (bf16 *)d_input);
+  const long n = (long)batch * kActIn;
+  k_cnn_cells<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)s>>>(
+      d_prev, d_cur, width, height, (long)pair_stride, batch, d_cells);
+  k_cnn_center<<<batch, 256, 0, (cudaStream_t)s>>>(d_cells, (bf16 *)d_input);
   return of_launch_status();
 }
 

@@ -59,6 +59,7 @@ extern "C" void of_default_params(of_filter_params_t *f, of_raycast_params_t *r,
     i->judge_min_inlier_frac = 0.3f;
     i->judge_max_rot_rad = 0.05f;
     i->judge_max_trans_mm = 50.0f;
+    i->warm_levels = 0;
   }
 }
 

@@ -291,6 +291,7 @@ struct IcpPlan {
   int cache_pts;  // model points a block keeps in shared memory per level
   float stop_rot, stop_trans;  // early exit (0: every iteration)
   float judge_rms, judge_frac, judge_rot, judge_trans;
+  int warm_levels;  // levels of a warm-started pass (<= levels)
 };
 
 // Grid-wide exchange of a co-resident grid. Each block publishes its row of
@@ -555,7 +556,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   const float dist2 = plan.dist_thresh * plan.dist_thresh, nthr = plan.normal_thresh;
   int iter_global = 0;
   for (int pass = 0; pass < 2; ++pass) {
-    for (int l = plan.levels - 1; l >= 0 && !s_stop && !s_err; --l) {
+    const int top = (pass == 0 && warm) ? plan.warm_levels - 1 : plan.levels - 1;
+    for (int l = top; l >= 0 && !s_stop && !s_err; --l) {
       const IcpLevel L = plan.lv[l];
       const int npx = L.mw * L.mh;
       // model pixels are dealt to blocks in chunks of 32 (one warp), round
@@ -932,6 +934,8 @@ of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, con
   plan.judge_frac = ip->judge_min_inlier_frac;
   plan.judge_rot = ip->judge_max_rot_rad;
   plan.judge_trans = ip->judge_max_trans_mm;
+  plan.warm_levels = (ip->warm_levels > 0 && ip->warm_levels < ip->levels) ? ip->warm_levels
+                                                                          : ip->levels;
   for (int l = 0; l < ip->levels; ++l) {
     of_camera_t cl = camera_level(*cam, l);
     plan.lv[l].cam = make_cam(cl);

@@ -44,6 +44,7 @@ struct of_tracker {
   uint16_t *cnn_params = nullptr;
   void *cnn_ws = nullptr;
   uint16_t *cnn_in = nullptr;
+  float *cnn_cells = nullptr;
   float *cnn_out = nullptr;
   double *warm_pose = nullptr;
   uint16_t *prev_depth = nullptr;
@@ -74,7 +75,8 @@ of_status_t enqueue_frame(of_tracker *t, bool track, cudaStream_t s) {
     if (st != OF_OK) return st;
     if (t->warm) {
       // the CNN's motion estimate between the previous and this depth frame
-      st = of_cnn_input(t->prev_depth, t->depth, d.camera.width, d.camera.height, 1, 0, t->cnn_in, s);
+      st = of_cnn_input(t->prev_depth, t->depth, d.camera.width, d.camera.height, 1, 0,
+                        t->cnn_cells, t->cnn_in, s);
       if (st == OF_OK)
         st = of_cnn_forward(t->cnn_params, t->cnn_master, t->cnn_in, 1, t->cnn_ws, t->cnn_out, s);
       if (st == OF_OK) st = of_cnn_warm_pose(t->cnn_out, t->pose, t->warm_pose, s);
@@ -135,7 +137,7 @@ void release(of_tracker *t) {
   if (t->g_track) cudaGraphExecDestroy(t->g_track);
   void *bufs[] = {t->volume, t->frame, t->model, t->icp_ws, t->pose, t->hist, t->hist_count,
                   t->depth, t->lambda, t->scratch, t->stats, t->cnn_master, t->cnn_params,
-                  t->cnn_ws, t->cnn_in, t->cnn_out, t->warm_pose, t->prev_depth};
+                  t->cnn_ws, t->cnn_in, t->cnn_cells, t->cnn_out, t->warm_pose, t->prev_depth};
   for (void *b : bufs)
     if (b) cudaFree(b);
   if (t->cap) cudaStreamDestroy(t->cap);
@@ -189,6 +191,7 @@ extern "C" of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_track
       {(void **)&t->cnn_params, (size_t)np * sizeof(uint16_t)},
       {&t->cnn_ws, cnn_ws},
       {(void **)&t->cnn_in, t->warm ? 2 * 60 * 80 * sizeof(uint16_t) : 0},
+      {(void **)&t->cnn_cells, t->warm ? 2 * 60 * 80 * sizeof(float) : 0},
       {(void **)&t->cnn_out, t->warm ? 6 * sizeof(float) : 0},
       {(void **)&t->warm_pose, t->warm ? 16 * sizeof(double) : 0},
       {(void **)&t->prev_depth, t->warm ? px * sizeof(uint16_t) : 0},

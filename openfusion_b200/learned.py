@@ -137,8 +137,9 @@ class WarmStartNet:
         b, h, w = prev.shape
         assert prev.is_contiguous() and cur.is_contiguous()
         out = torch.empty((b, IN_ELEMS), dtype=torch.int16, device=prev.device) if out is None else out
+        cells = torch.empty((b, IN_ELEMS), dtype=torch.float32, device=prev.device)
         N.check("of_cnn_input", N.lib().of_cnn_input(_ptr(prev), _ptr(cur), w, h, b, h * w,
-                                                    _ptr(out), _stream()))
+                                                    _ptr(cells), _ptr(out), _stream()))
         return out
 
     def forward(self, inp):
@@ -170,11 +171,12 @@ class WarmStartNet:
 
 # ------------------------------------------------------------ training data --
 
-def icp_labelled_pairs(cfg: Config, seed: int, frames: int, device="cuda"):
+def icp_labelled_pairs(cfg: Config, seed: int, frames: int, device="cuda", swap: bool = False):
     """One seeded trajectory: network inputs of its consecutive depth pairs
     and their targets, the motion between each frame's ground-truth pose and
     the pose this library's ICP finds for the next frame (frame-to-frame,
-    started at the ground truth, against the previous frame's own maps)."""
+    started at the ground truth, against the previous frame's own maps).
+    With `swap` the reversed pairs follow, with the inverse motions."""
     import torch
     import dataclasses
     c = dataclasses.replace(cfg, seed=seed)
@@ -209,6 +211,10 @@ def icp_labelled_pairs(cfg: Config, seed: int, frames: int, device="cuda"):
         out[k - 1].copy_(pose)
     icp_poses = out.cpu().numpy().reshape(-1, 4, 4)
     target = np.stack([motion_target(poses[k - 1], icp_poses[k - 1]) for k in range(1, frames)])
+    if swap:
+        inp = torch.cat([inp, WarmStartNet.inputs(depth[1:].contiguous(), depth[:-1].contiguous())])
+        back = np.stack([motion_target(icp_poses[k - 1], poses[k - 1]) for k in range(1, frames)])
+        target = np.concatenate([target, back])
     return inp, torch.from_numpy(target.astype(np.float32)).to(device), poses, icp_poses
 
 
@@ -219,11 +225,11 @@ def _icp_ws_bytes(cfg: Config) -> int:
     return b.value
 
 
-def training_set(cfg: Config, seeds, frames: int, device="cuda"):
+def training_set(cfg: Config, seeds, frames: int, device="cuda", swap: bool = False):
     import torch
     xs, ys = [], []
     for s in seeds:
-        x, y, _, _ = icp_labelled_pairs(cfg, int(s), frames, device)
+        x, y, _, _ = icp_labelled_pairs(cfg, int(s), frames, device, swap)
         xs.append(x)
         ys.append(y)
     return torch.cat(xs), torch.cat(ys)

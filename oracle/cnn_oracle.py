@@ -68,6 +68,27 @@ def bf16_bits_to_f64(bits: np.ndarray) -> np.ndarray:
     return (np.asarray(bits, np.uint16).astype(np.uint32) << 16).view(np.float32).astype(np.float64)
 
 
+def network_input(prev: np.ndarray, cur: np.ndarray) -> np.ndarray:
+    """Input of one pair of uint16 depth frames (H = 60 k, W = 80 k), before
+    BF16 rounding: block means of the valid depths in metres (0 if empty);
+    channel 0 the previous block means minus their mean over the non-empty
+    blocks, channel 1 current minus previous where both are non-empty."""
+    h, w = prev.shape
+    k = w // 80
+
+    def cells(d):
+        b = np.asarray(d, np.float64).reshape(60, k, 80, k)
+        n = (b > 0).sum(axis=(1, 3))
+        s = b.sum(axis=(1, 3))
+        return np.where(n > 0, s / (1000.0 * np.maximum(n, 1)), 0.0)
+
+    p, q = cells(prev), cells(cur)
+    mu = p[p > 0].mean() if (p > 0).any() else 0.0
+    x0 = np.where(p > 0, p - mu, 0.0)
+    x1 = np.where((p > 0) & (q > 0), q - p, 0.0)
+    return np.stack([x0, x1])
+
+
 def _im2col(x, k, s, p):
     b, c, h, w = x.shape
     ho, wo = (h + 2 * p - k) // s + 1, (w + 2 * p - k) // s + 1

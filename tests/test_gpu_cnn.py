@@ -50,6 +50,23 @@ def test_device_renderer_matches_host(of, cuda):
         assert (host > 0).mean() > 0.9
 
 
+def test_network_input_matches_oracle(of, cuda):
+    import torch
+    from openfusion_b200 import learned
+    cfg = of.CONFIGS["c2"]
+    seq = of.make_sequence(cfg, frames=3)
+    d = torch.from_numpy(seq.depth.astype(np.int16)).to(cuda)
+    bits = learned.WarmStartNet.inputs(d[:-1].contiguous(), d[1:].contiguous()).cpu().numpy()
+    got = co.bf16_bits_to_f64(bits.view(np.uint16)).reshape(2, 2, 60, 80)
+    for i in range(2):
+        ref = co.network_input(seq.depth[i], seq.depth[i + 1])
+        # BF16 rounding (at most one spacing, 2^-7 relative) of FP32 sums
+        # that differ from the FP64 ones by ~1e-7 m
+        tol = np.abs(ref) * 2.0 ** -7 + 1e-6
+        assert np.all(np.abs(got[i] - ref) <= tol), np.abs(got[i] - ref).max()
+        assert (np.abs(ref[1]) > 0).mean() > 0.5
+
+
 def test_forward_matches_oracle(of, cuda):
     from openfusion_b200 import learned
     net = learned.WarmStartNet(cuda, seed=3)
