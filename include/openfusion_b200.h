@@ -394,6 +394,17 @@ of_status_t of_cnn_backward(const uint16_t *d_params, const float *d_master,
  * from 1) on the master values; refreshes their BF16 copies. */
 of_status_t of_cnn_adam(float *d_master, uint16_t *d_params, const float *d_grad, float *d_m,
                         float *d_v, int32_t step, float lr, of_stream_t stream);
+/* The prediction for one pair in one launch (one cluster of 16 CTAs, one per
+ * SM, each staging its slice of the weights in shared memory and sharing the
+ * activations through distributed shared memory): of_cnn_input,
+ * of_cnn_forward and of_cnn_warm_pose fused, with the same arithmetic up to
+ * the order of each output's sums. `d_out` (6 floats) and `d_warm_pose` (with
+ * `d_prev_pose`) may each be NULL. W / 80 = H / 60 must be 1, 2, 4 or 8;
+ * `d_params` and both depth frames 16-byte aligned. No scratch memory. */
+of_status_t of_cnn_predict(const uint16_t *d_params, const float *d_master,
+                           const uint16_t *d_prev, const uint16_t *d_cur, int32_t width,
+                           int32_t height, const double *d_prev_pose, float *d_out,
+                           double *d_warm_pose, of_stream_t stream);
 /* BF16 copies of (loaded) master values. */
 of_status_t of_cnn_load(const float *d_master, uint16_t *d_params, of_stream_t stream);
 /* Warm start from a prediction: d_warm_pose = d_prev_pose x [exp(w) | t] with

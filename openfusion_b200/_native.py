@@ -130,6 +130,7 @@ _SIGS = {
     "of_cnn_backward": (c_status, [P, P, P, C.c_int32, P, P, P, P, P, c_stream]),
     "of_cnn_adam": (c_status, [P, P, P, P, P, C.c_int32, C.c_float, c_stream]),
     "of_cnn_load": (c_status, [P, P, c_stream]),
+    "of_cnn_predict": (c_status, [P, P, P, P, C.c_int32, C.c_int32, P, P, P, c_stream]),
     "of_cnn_warm_pose": (c_status, [P, P, P, c_stream]),
     "of_icp_track_warm": (c_status, [C.POINTER(Camera), C.POINTER(IcpParams), P, P, P, P, P, P,
                                      c_stream]),

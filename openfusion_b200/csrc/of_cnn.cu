@@ -15,9 +15,12 @@
 // BF16, every sum in FP32, gradients, master weights and Adam moments in
 // FP32. Every reduction runs in a fixed order (no atomics), so a training run
 // is reproducible bit for bit.
+#include <cooperative_groups.h>
 #include <cuda_bf16.h>
 
 #include "of_common.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -26,7 +29,6 @@ using bf16 = __nv_bfloat16;
 struct ConvSpec {
   int ci, co, k, s, p, hi, wi, ho, wo;
 };
-constexpr int kLayers = 6;
 constexpr ConvSpec kConv[4] = {{2, 16, 5, 2, 2, 60, 80, 30, 40},
                                {16, 32, 3, 2, 1, 30, 40, 15, 20},
                                {32, 64, 3, 2, 1, 15, 20, 8, 10},
@@ -566,9 +568,8 @@ __global__ void k_cnn_mirror(const float *__restrict__ master, bf16 *__restrict_
 // warm = prev x [R | t] with R = exp(w) (Rodrigues; series for small angles),
 // w = out[0..2] / 10 rad, t = 100 out[3..5] mm: the predicted motion applied
 // in the previous camera's frame.
-__global__ void k_cnn_warm_pose(const float *__restrict__ out, const double *__restrict__ prev,
-                                double *__restrict__ warm) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// D = [exp(w) | t] of a prediction (the motion in the previous camera's frame)
+__device__ void motion_matrix(const float *out, double *D) {
   const double wx = out[0] * 0.1, wy = out[1] * 0.1, wz = out[2] * 0.1;
   const double th2 = wx * wx + wy * wy + wz * wz;
   double a, b;  // sin(th)/th, (1 - cos(th))/th^2
@@ -581,14 +582,19 @@ __global__ void k_cnn_warm_pose(const float *__restrict__ out, const double *__r
     b = (1.0 - cos(th)) / th2;
   }
   const double K[9] = {0.0, -wz, wy, wz, 0.0, -wx, -wy, wx, 0.0};
-  double D[16] = {0};
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) {
       double k2 = 0.0;
       for (int m = 0; m < 3; ++m) k2 += K[3 * i + m] * K[3 * m + j];
       D[4 * i + j] = (i == j ? 1.0 : 0.0) + a * K[3 * i + j] + b * k2;
     }
-  D[3] = out[3] * 100.0; D[7] = out[4] * 100.0; D[11] = out[5] * 100.0; D[15] = 1.0;
+  D[3] = out[3] * 100.0; D[7] = out[4] * 100.0; D[11] = out[5] * 100.0;
+  D[12] = 0.0; D[13] = 0.0; D[14] = 0.0; D[15] = 1.0;
+}
+
+__device__ void warm_pose_of(const float *out, const double *prev, double *warm) {
+  double D[16];
+  motion_matrix(out, D);
   for (int i = 0; i < 4; ++i)
     for (int j = 0; j < 4; ++j) {
       double s = 0.0;
@@ -597,7 +603,451 @@ __global__ void k_cnn_warm_pose(const float *__restrict__ out, const double *__r
     }
 }
 
+__global__ void k_cnn_warm_pose(const float *__restrict__ out, const double *__restrict__ prev,
+                                double *__restrict__ warm) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) warm_pose_of(out, prev, warm);
+}
+
+// ------------------------------------------- fused single-pair inference --
+//
+// The whole prediction for one (previous, current) pair in one launch: one
+// cluster of kCluCtas CTAs, one per SM. CTA r owns 1/kCluCtas of the block
+// means and of every layer's output channels, and holds a full copy of every
+// activation in its shared memory. A layer runs in three steps: the CTA
+// computes its channel slice from its local copy of the layer input, pushes
+// the slice (a contiguous run of the NCHW activation) into the other CTAs'
+// copies with 16-byte distributed-shared-memory stores, and one cluster
+// barrier publishes every slice. The CTA's weight slice of every layer is
+// staged into shared memory at launch, while the block means are summed:
+// convolution weights converted to FP32 and stored tap-major
+// ([ci][ky][kx][channel], one vector load feeds all of the CTA's channels),
+// FC weights copied as BF16 with cp.async. Arithmetic is the batched
+// kernels': BF16 weights and activations, FP32 sums (in another order), BF16
+// storage.
+constexpr int kCluCtas = 16;  // the non-portable cluster maximum (opted in at set-up)
+constexpr int kInferThreads = 512;
+constexpr int kInferWarps = kInferThreads / 32;
+constexpr int kCellsPerCta = 2 * kInH * kInW / kCluCtas;
+constexpr int kF1PerCta = kF1Out / kCluCtas;
+constexpr int conv_per(int l) { return kConv[l].co / kCluCtas; }
+constexpr int conv_taps(int l) { return kConv[l].ci * kConv[l].k * kConv[l].k; }
+// bias slots in shared memory: b0..b3 (this CTA's channels), bf1 (its FC1
+// outputs), bf2
+constexpr int bias_at(int i) {
+  return i == 0 ? 0 : i <= 4 ? bias_at(i - 1) + conv_per(i - 1) : bias_at(4) + kF1PerCta;
+}
+constexpr int kBiasN = bias_at(5) + kF2Out;
+static_assert(kCellsPerCta * kCluCtas == 2 * kInH * kInW && kCellsPerCta % 4 == 0, "cell slices");
+static_assert(kF1PerCta * kCluCtas == kF1Out && kF1PerCta <= kInferWarps, "FC1 slices");
+static_assert(kBiasN <= 32 && conv_taps(0) * conv_per(0) <= kInferThreads, "staging");
+// 16-byte vector staging of the conv1..3 and FC weight slices
+static_assert(kOffW1 % 8 == 0 && kOffW2 % 8 == 0 && kOffW3 % 8 == 0 && kOffF1 % 8 == 0 &&
+                  kOffF2 % 8 == 0, "16-byte aligned weight blocks");
+static_assert((conv_taps(1) * conv_per(1)) % 8 == 0 && (conv_taps(2) * conv_per(2)) % 8 == 0 &&
+                  (conv_taps(3) * conv_per(3)) % 8 == 0 && (kF1PerCta * kF1In) % 8 == 0 &&
+                  (kF2Out * kF1Out) % 8 == 0, "16-byte weight slices");
+// 16-byte slice pushes
+static_assert((kAct[0] / kCluCtas) % 8 == 0 && (kAct[1] / kCluCtas) % 8 == 0 &&
+                  (kAct[2] / kCluCtas) % 8 == 0 && (kAct[3] / kCluCtas) % 8 == 0,
+              "16-byte activation slices");
+
+constexpr int kV1 = conv_taps(1) * conv_per(1) / 8, kV2 = conv_taps(2) * conv_per(2) / 8,
+              kV3 = conv_taps(3) * conv_per(3) / 8;
+constexpr int kConvVecs = kV1 + kV2 + kV3;
+constexpr int kConvVecRounds = (kConvVecs + kInferThreads - 1) / kInferThreads;
+
+struct InferSmem {
+  alignas(16) float cells[2 * kInH * kInW];
+  alignas(16) bf16 in[kActIn];
+  alignas(16) bf16 a1[kAct[0]];
+  alignas(16) bf16 a2[kAct[1]];
+  alignas(16) bf16 a3[kAct[2]];
+  alignas(16) bf16 a4[kAct[3]];
+  alignas(16) bf16 wf1[kF1PerCta * kF1In];
+  alignas(16) bf16 wf2[kF2Out * kF1Out];
+  alignas(16) float w0[conv_taps(0) * conv_per(0)];
+  alignas(16) float w1[conv_taps(1) * conv_per(1)];
+  alignas(16) float w2[conv_taps(2) * conv_per(2)];
+  alignas(16) float w3[conv_taps(3) * conv_per(3)];
+  float bias[32];
+  alignas(16) bf16 f1[kF1Out];
+  float out[8];
+  float wsum[kInferWarps];
+  int wcnt[kInferWarps];
+  float psum[kCluCtas];
+  int pcnt[kCluCtas];
+};
+static_assert(sizeof(InferSmem) <= 227 * 1024, "shared memory");
+
+__device__ __forceinline__ float bf_bits(uint32_t b16) { return __uint_as_float(b16 << 16); }
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// source of staging vector v (8 BF16) of this CTA's conv1..3 weight slices
+__device__ __forceinline__ const uint4 *conv_vec_src(const bf16 *pw, int rank, int v) {
+  if (v < kV1) return reinterpret_cast<const uint4 *>(pw + kOffW1) + rank * kV1 + v;
+  if (v < kV1 + kV2) return reinterpret_cast<const uint4 *>(pw + kOffW2) + rank * kV2 + (v - kV1);
+  return reinterpret_cast<const uint4 *>(pw + kOffW3) + rank * kV3 + (v - kV1 - kV2);
+}
+
+// element e of a CTA's slice of conv layer L ([channel][tap], as in global
+// memory) -> its tap-major FP32 place ([tap][channel])
+template <int L>
+__device__ __forceinline__ void put_tap_major(float *w, int e, float x) {
+  constexpr int T = conv_taps(L), PER = conv_per(L);
+  w[(e % T) * PER + e / T] = x;
+}
+
+__device__ __forceinline__ void store_conv_vec(InferSmem &S, int v, const uint4 q) {
+  const uint32_t u[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const float x = bf_bits(i & 1 ? u[i >> 1] >> 16 : u[i >> 1] & 0xffffu);
+    if (v < kV1) put_tap_major<1>(S.w1, v * 8 + i, x);
+    else if (v < kV1 + kV2) put_tap_major<2>(S.w2, (v - kV1) * 8 + i, x);
+    else put_tap_major<3>(S.w3, (v - kV1 - kV2) * 8 + i, x);
+  }
+}
+
+// bias slot s of this CTA (FP32 master values)
+__device__ __forceinline__ float bias_of(const float *pm, int rank, int s) {
+  if (s < bias_at(1)) return pm[kOffB0 + rank * conv_per(0) + s];
+  if (s < bias_at(2)) return pm[kOffB1 + rank * conv_per(1) + s - bias_at(1)];
+  if (s < bias_at(3)) return pm[kOffB2 + rank * conv_per(2) + s - bias_at(2)];
+  if (s < bias_at(4)) return pm[kOffB3 + rank * conv_per(3) + s - bias_at(3)];
+  if (s < bias_at(5)) return pm[kOffBF1 + rank * kF1PerCta + s - bias_at(4)];
+  return pm[kOffBF2 + s - bias_at(5)];
+}
+
+// a row of K depth pixels as one load
+template <int K> struct RowVec;
+template <> struct RowVec<8> { using T = uint4; };
+template <> struct RowVec<4> { using T = uint2; };
+template <> struct RowVec<2> { using T = uint32_t; };
+template <> struct RowVec<1> { using T = uint16_t; };
+
+template <int K>
+__device__ __forceinline__ void row_sum(const typename RowVec<K>::T &q, float &s, int &n) {
+  uint32_t u[(K + 1) / 2];
+  if constexpr (K == 8) { u[0] = q.x; u[1] = q.y; u[2] = q.z; u[3] = q.w; }
+  else if constexpr (K == 4) { u[0] = q.x; u[1] = q.y; }
+  else u[0] = q;
+  s = 0.f;
+  n = 0;
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    const uint32_t d = i & 1 ? u[i >> 1] >> 16 : u[i >> 1] & 0xffffu;
+    if (d) { s += (float)d; ++n; }
+  }
+}
+
+// This CTA's block means (cells rank * kCellsPerCta ..), K lanes per cell
+// (one K-pixel row each, all loads in flight at once); sums of <= 64 uint16
+// depths are exact in FP32, so the means equal the batched kernel's. Also
+// returns this thread's share of the sum and count of the non-empty cells of
+// the previous frame.
+template <int K>
+__device__ __forceinline__ void infer_cells(const uint16_t *prev, const uint16_t *cur, int w,
+                                            InferSmem &S, int rank, float &psum, int &pcnt) {
+  using V = typename RowVec<K>::T;
+  constexpr int T = kCellsPerCta * K, R = (T + kInferThreads - 1) / kInferThreads;
+  static_assert(kInferThreads % K == 0, "cell lanes");
+  V q[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int t = r * kInferThreads + threadIdx.x;
+    q[r] = V{};
+    if (t < T) {
+      const int c = rank * kCellsPerCta + t / K, y = t % K;
+      const int f = c / (kInH * kInW), cy = (c / kInW) % kInH, cx = c % kInW;
+      const uint16_t *row = (f ? cur : prev) + (size_t)(cy * K + y) * w + cx * K;
+      q[r] = __ldg(reinterpret_cast<const V *>(row));
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    float s;
+    int n;
+    row_sum<K>(q[r], s, n);
+#pragma unroll
+    for (int o = 1; o < K; o <<= 1) {
+      s += __shfl_xor_sync(0xffffffffu, s, o);
+      n += __shfl_xor_sync(0xffffffffu, n, o);
+    }
+    const int t = r * kInferThreads + threadIdx.x;
+    if (t < T && t % K == 0) {
+      const int c = rank * kCellsPerCta + t / K;
+      const float v = n ? s / (1000.f * n) : 0.f;
+      S.cells[c] = v;
+      if (c < kInH * kInW && v > 0.f) { psum += v; ++pcnt; }
+    }
+  }
+}
+
+// copy this CTA's slice [off, off + bytes) of a shared buffer into the same
+// place of every other CTA's copy (16-byte stores)
+__device__ __forceinline__ void push_slice(cg::cluster_group &cluster, void *buf, int off, int bytes,
+                                           int rank) {
+  const int nv = bytes / 16;
+  const uint4 *src = reinterpret_cast<const uint4 *>(static_cast<char *>(buf) + off);
+  for (int i = threadIdx.x; i < nv * (kCluCtas - 1); i += kInferThreads) {
+    const int p = i / nv, v = i - p * nv;
+    const int r = p + (p >= rank);
+    uint4 *dst = reinterpret_cast<uint4 *>(cluster.map_shared_rank(static_cast<char *>(buf), r) + off);
+    dst[v] = src[v];
+  }
+}
+
+// this CTA's channels of conv layer L from the local input copy into the
+// local output copy: each thread one output pixel for all of the CTA's
+// channels (register tile), the input channels split among G adjacent lanes
+// (ci = g, g + G, ...) and summed by shuffles
+template <int L, int G>
+__device__ __forceinline__ void infer_conv(const bf16 *in, const float *w, const float *bias,
+                                           bf16 *out, int rank) {
+  constexpr int CI = kConv[L].ci, K = kConv[L].k, STR = kConv[L].s, P = kConv[L].p;
+  constexpr int HI = kConv[L].hi, WI = kConv[L].wi, HO = kConv[L].ho, WO = kConv[L].wo;
+  constexpr int PER = conv_per(L), T = HO * WO * G;
+  static_assert(CI % G == 0 && 32 % G == 0 && (G == 1 || T % 32 == 0), "lane groups");
+  for (int base = 0; base < T; base += kInferThreads) {
+    if (base + (int)(threadIdx.x & ~31u) >= T) break;  // warp-uniform
+    const int t = base + threadIdx.x;
+    const bool live = t < T;
+    const int p = live ? t / G : 0, g = t % G;
+    const int oy = p / WO, ox = p % WO;
+    float acc[PER];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) acc[j] = 0.f;
+#pragma unroll 2
+    for (int ci = g; ci < CI; ci += G) {
+#pragma unroll
+      for (int ky = 0; ky < K; ++ky) {
+        const int iy = oy * STR - P + ky;
+        if ((unsigned)iy >= (unsigned)HI) continue;
+#pragma unroll
+        for (int kx = 0; kx < K; ++kx) {
+          const int ix = ox * STR - P + kx;
+          if ((unsigned)ix >= (unsigned)WI) continue;
+          const float x = bf(in[(ci * HI + iy) * WI + ix]);
+          const float *wp = w + ((ci * K + ky) * K + kx) * PER;
+          if constexpr (PER % 4 == 0) {
+#pragma unroll
+            for (int j = 0; j < PER; j += 4) {
+              const float4 q = *reinterpret_cast<const float4 *>(wp + j);
+              acc[j] = fmaf(q.x, x, acc[j]);
+              acc[j + 1] = fmaf(q.y, x, acc[j + 1]);
+              acc[j + 2] = fmaf(q.z, x, acc[j + 2]);
+              acc[j + 3] = fmaf(q.w, x, acc[j + 3]);
+            }
+          } else if constexpr (PER == 2) {
+            const float2 q = *reinterpret_cast<const float2 *>(wp);
+            acc[0] = fmaf(q.x, x, acc[0]);
+            acc[1] = fmaf(q.y, x, acc[1]);
+          } else {
+#pragma unroll
+            for (int j = 0; j < PER; ++j) acc[j] = fmaf(wp[j], x, acc[j]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 1; o < G; o <<= 1)
+#pragma unroll
+      for (int j = 0; j < PER; ++j) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+    if (live) {
+#pragma unroll
+      for (int j = 0; j < PER; ++j)
+        if (j % G == g)
+          out[((rank * PER + j) * HO + oy) * WO + ox] = __float2bfloat16_rn(fmaxf(acc[j] + bias[j], 0.f));
+    }
+  }
+}
+
+// a conv layer's slice push: this CTA's PER channels of the NCHW output
+template <int L>
+__device__ __forceinline__ void push_conv(cg::cluster_group &cluster, bf16 *out, int rank) {
+  constexpr int bytes = (int)(kAct[L] / kCluCtas * sizeof(bf16));
+  push_slice(cluster, out, rank * bytes, bytes, rank);
+}
+
+// entry (i, j) of the warm start (the expression warm_pose_of evaluates)
+__device__ double warm_pose_entry(const float *out, const double *prev, int i, int j) {
+  double D[16];
+  motion_matrix(out, D);
+  double s = 0.0;
+  for (int m = 0; m < 4; ++m) s += prev[4 * i + m] * D[4 * m + j];
+  return s;
+}
+
+__global__ void __cluster_dims__(kCluCtas, 1, 1) __launch_bounds__(kInferThreads)
+    k_cnn_infer(const bf16 *__restrict__ pw, const float *__restrict__ pm,
+                const uint16_t *__restrict__ prev, const uint16_t *__restrict__ cur, int w,
+                const double *__restrict__ prev_pose, float *__restrict__ out6,
+                double *__restrict__ warm) {
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  InferSmem &S = *reinterpret_cast<InferSmem *>(s_raw);
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // every CTA of the cluster is running before any distributed store (the
+  // matching wait comes before the first push)
+  asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
+  // weight staging: conv slices into registers, FC slices by cp.async
+  uint4 wv[kConvVecRounds];
+#pragma unroll
+  for (int r = 0; r < kConvVecRounds; ++r) {
+    const int v = r * kInferThreads + threadIdx.x;
+    if (v < kConvVecs) wv[r] = __ldg(conv_vec_src(pw, rank, v));
+  }
+  float w0v = 0.f, bv = 0.f;
+  if (threadIdx.x < conv_taps(0) * conv_per(0))
+    w0v = bf(pw[kOffW0 + rank * conv_taps(0) * conv_per(0) + threadIdx.x]);
+  if (threadIdx.x < kBiasN) bv = bias_of(pm, rank, threadIdx.x);
+  {
+    const uint4 *f1src = reinterpret_cast<const uint4 *>(pw + kOffF1) + rank * (kF1PerCta * kF1In / 8);
+    for (int v = threadIdx.x; v < kF1PerCta * kF1In / 8; v += kInferThreads)
+      cp_async16(reinterpret_cast<uint4 *>(S.wf1) + v, f1src + v);
+    if (rank == 0)
+      for (int v = threadIdx.x; v < kF2Out * kF1Out / 8; v += kInferThreads)
+        cp_async16(reinterpret_cast<uint4 *>(S.wf2) + v, reinterpret_cast<const uint4 *>(pw + kOffF2) + v);
+  }
+  // block means of both frames (this CTA's cells)
+  float psum = 0.f;
+  int pcnt = 0;
+  const int k = w / kInW;
+  if (k == 8) infer_cells<8>(prev, cur, w, S, rank, psum, pcnt);
+  else if (k == 4) infer_cells<4>(prev, cur, w, S, rank, psum, pcnt);
+  else if (k == 2) infer_cells<2>(prev, cur, w, S, rank, psum, pcnt);
+  else infer_cells<1>(prev, cur, w, S, rank, psum, pcnt);
+  // staged conv weights and biases to shared memory
+#pragma unroll
+  for (int r = 0; r < kConvVecRounds; ++r) {
+    const int v = r * kInferThreads + threadIdx.x;
+    if (v < kConvVecs) store_conv_vec(S, v, wv[r]);
+  }
+  if (threadIdx.x < conv_taps(0) * conv_per(0)) put_tap_major<0>(S.w0, threadIdx.x, w0v);
+  if (threadIdx.x < kBiasN) S.bias[threadIdx.x] = bv;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    psum += __shfl_xor_sync(0xffffffffu, psum, o);
+    pcnt += __shfl_xor_sync(0xffffffffu, pcnt, o);
+  }
+  if (lane == 0) { S.wsum[warp] = psum; S.wcnt[warp] = pcnt; }
+  __syncthreads();
+  asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
+  constexpr int kCellBytes = kCellsPerCta * (int)sizeof(float);
+  push_slice(cluster, S.cells, rank * kCellBytes, kCellBytes, rank);
+  if (warp == 0) {
+    float s = 0.f;
+    int n = 0;
+    for (int i = 0; i < kInferWarps; ++i) { s += S.wsum[i]; n += S.wcnt[i]; }
+    if (lane < kCluCtas) {
+      cluster.map_shared_rank(S.psum, lane)[rank] = s;
+      cluster.map_shared_rank(S.pcnt, lane)[rank] = n;
+    }
+  }
+  cluster.sync();
+  // network input, in every CTA: centred previous block means, difference
+  {
+    float s = 0.f;
+    int n = 0;
+#pragma unroll
+    for (int r = 0; r < kCluCtas; ++r) { s += S.psum[r]; n += S.pcnt[r]; }
+    const float mu = n ? s / (float)n : 0.f;
+    for (int c = threadIdx.x; c < kInH * kInW; c += kInferThreads) {
+      const float p = S.cells[c], q = S.cells[kInH * kInW + c];
+      S.in[c] = __float2bfloat16_rn(p > 0.f ? p - mu : 0.f);
+      S.in[kInH * kInW + c] = __float2bfloat16_rn(p > 0.f && q > 0.f ? q - p : 0.f);
+    }
+  }
+  __syncthreads();
+  infer_conv<0, 1>(S.in, S.w0, S.bias + bias_at(0), S.a1, rank);
+  __syncthreads();
+  push_conv<0>(cluster, S.a1, rank);
+  cluster.sync();
+  infer_conv<1, 1>(S.a1, S.w1, S.bias + bias_at(1), S.a2, rank);
+  __syncthreads();
+  push_conv<1>(cluster, S.a2, rank);
+  cluster.sync();
+  infer_conv<2, 4>(S.a2, S.w2, S.bias + bias_at(2), S.a3, rank);
+  __syncthreads();
+  push_conv<2>(cluster, S.a3, rank);
+  cluster.sync();
+  infer_conv<3, 16>(S.a3, S.w3, S.bias + bias_at(3), S.a4, rank);
+  cp_async_wait_all();
+  __syncthreads();
+  push_conv<3>(cluster, S.a4, rank);
+  cluster.sync();
+  // f1: this CTA's outputs, one warp each, into CTA 0's copy
+  if (warp < kF1PerCta) {
+    const __nv_bfloat162 *wr = reinterpret_cast<const __nv_bfloat162 *>(S.wf1 + warp * kF1In);
+    const __nv_bfloat162 *xa = reinterpret_cast<const __nv_bfloat162 *>(S.a4);
+    float s0 = 0.f, s1 = 0.f;
+#pragma unroll 4
+    for (int i = lane; i < kF1In / 2; i += 32) {
+      const float2 a = __bfloat1622float2(wr[i]), x = __bfloat1622float2(xa[i]);
+      s0 = fmaf(a.x, x.x, s0);
+      s1 = fmaf(a.y, x.y, s1);
+    }
+    float acc = s0 + s1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0)
+      cluster.map_shared_rank(S.f1, 0)[rank * kF1PerCta + warp] =
+          __float2bfloat16_rn(fmaxf(acc + S.bias[bias_at(4) + warp], 0.f));
+  }
+  cluster.sync();
+  if (rank != 0) return;
+  // f2 and the warm start, in CTA 0
+  if (warp < kF2Out) {
+    const __nv_bfloat162 *wr = reinterpret_cast<const __nv_bfloat162 *>(S.wf2 + warp * kF1Out);
+    const __nv_bfloat162 *xa = reinterpret_cast<const __nv_bfloat162 *>(S.f1);
+    float acc = 0.f;
+    for (int i = lane; i < kF1Out / 2; i += 32) {
+      const float2 a = __bfloat1622float2(wr[i]), x = __bfloat1622float2(xa[i]);
+      acc = fmaf(a.x, x.x, acc);
+      acc = fmaf(a.y, x.y, acc);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) S.out[warp] = acc + S.bias[bias_at(5) + warp];
+  }
+  __syncthreads();
+  if (threadIdx.x < kF2Out && out6) out6[threadIdx.x] = S.out[threadIdx.x];
+  if (threadIdx.x < 16 && warm)
+    warm[threadIdx.x] = warm_pose_entry(S.out, prev_pose, threadIdx.x >> 2, threadIdx.x & 3);
+}
+
 }  // namespace
+
+extern "C" of_status_t of_cnn_predict(const uint16_t *d_params, const float *d_master,
+                                      const uint16_t *d_prev, const uint16_t *d_cur, int32_t width,
+                                      int32_t height, const double *d_prev_pose, float *d_out,
+                                      double *d_warm_pose, of_stream_t s) {
+  if (!d_params || !d_master || !d_prev || !d_cur || (d_warm_pose && !d_prev_pose) ||
+      ((uintptr_t)d_params & 15u) || width % kInW || height % kInH || width / kInW != height / kInH ||
+      (width / kInW != 1 && width / kInW != 2 && width / kInW != 4 && width / kInW != 8) ||
+      ((uintptr_t)d_prev & 15u) || ((uintptr_t)d_cur & 15u))
+    return OF_ERR_INVALID_ARGUMENT;
+  static bool attr_set[64] = {};
+  int dev = 0;
+  OF_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    OF_CUDA_TRY(cudaFuncSetAttribute((const void *)k_cnn_infer,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(InferSmem)));
+    OF_CUDA_TRY(cudaFuncSetAttribute((const void *)k_cnn_infer,
+                                     cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    attr_set[dev] = true;
+  }
+  k_cnn_infer<<<kCluCtas, kInferThreads, sizeof(InferSmem), (cudaStream_t)s>>>(
+      (const bf16 *)d_params, d_master, d_prev, d_cur, width, d_prev_pose, d_out, d_warm_pose);
+  return of_launch_status();
+}
 
 extern "C" of_status_t of_cnn_load(const float *d_master, uint16_t *d_params, of_stream_t s) {
   if (!d_master || !d_params) return OF_ERR_INVALID_ARGUMENT;

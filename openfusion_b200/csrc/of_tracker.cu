@@ -27,6 +27,9 @@ struct of_tracker {
   of_tracker_desc_t desc;
   of_pyramid_layout_t lay;
   cudaStream_t cap;
+  // the warm-start CNN runs on a branch beside pre-processing (fork / join)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   void *volume = nullptr;
   void *frame = nullptr;
   void *model = nullptr;
@@ -71,17 +74,22 @@ of_status_t enqueue_frame(of_tracker *t, bool track, cudaStream_t s) {
   const of_tracker_desc_t &d = t->desc;
   of_status_t st;
   if (track) {
-    st = of_preprocess(&d.camera, &d.filter, t->depth, d.camera.width, t->frame, s);
-    if (st != OF_OK) return st;
     if (t->warm) {
-      // the CNN's motion estimate between the previous and this depth frame
-      st = of_cnn_input(t->prev_depth, t->depth, d.camera.width, d.camera.height, 1, 0,
-                        t->cnn_cells, t->cnn_in, s);
-      if (st == OF_OK)
-        st = of_cnn_forward(t->cnn_params, t->cnn_master, t->cnn_in, 1, t->cnn_ws, t->cnn_out, s);
-      if (st == OF_OK) st = of_cnn_warm_pose(t->cnn_out, t->pose, t->warm_pose, s);
-      if (st != OF_OK) return st;
+      // the CNN's motion estimate between the previous and this depth frame,
+      // on a branch that runs beside pre-processing and joins before ICP
+      OF_CUDA_TRY(cudaEventRecord(t->ev_fork, s));
+      OF_CUDA_TRY(cudaStreamWaitEvent(t->side, t->ev_fork, 0));
+      st = of_cnn_predict(t->cnn_params, t->cnn_master, t->prev_depth, t->depth, d.camera.width,
+                          d.camera.height, t->pose, t->cnn_out, t->warm_pose, t->side);
+      OF_CUDA_TRY(cudaEventRecord(t->ev_join, t->side));
+      if (st != OF_OK) {
+        cudaStreamWaitEvent(s, t->ev_join, 0);
+        return st;
+      }
     }
+    st = of_preprocess(&d.camera, &d.filter, t->depth, d.camera.width, t->frame, s);
+    if (t->warm) OF_CUDA_TRY(cudaStreamWaitEvent(s, t->ev_join, 0));
+    if (st != OF_OK) return st;
     st = of_icp_launch(&d.camera, &d.icp, t->frame, t->model, t->pose, t->icp_ws, t->stats, s,
                        t->warm ? t->warm_pose : nullptr);
     if (st != OF_OK) return st;
@@ -126,7 +134,7 @@ of_status_t capture(of_tracker *t, bool track, cudaGraphExec_t *out) {
   }
   if (e != cudaSuccess) return of_set_cuda_error(e);
   (track ? t->kernels_track : t->kernels_first) = count_kernel_nodes(g);
-  e = cudaGraphInstantiate(out, g, 0);
+  e = cudaGraphInstantiateWithFlags(out, g, cudaGraphInstantiateFlagUseNodePriority);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return of_set_cuda_error(e);
   return OF_OK;
@@ -141,6 +149,9 @@ void release(of_tracker *t) {
   for (void *b : bufs)
     if (b) cudaFree(b);
   if (t->cap) cudaStreamDestroy(t->cap);
+  if (t->side) cudaStreamDestroy(t->side);
+  if (t->ev_fork) cudaEventDestroy(t->ev_fork);
+  if (t->ev_join) cudaEventDestroy(t->ev_join);
   delete t;
 }
 
@@ -160,6 +171,16 @@ extern "C" of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_track
   of_status_t st = of_pyramid_layout(&desc->camera, desc->icp.levels, &t->lay);
   if (st != OF_OK) { release(t); return st; }
   cudaError_t e = cudaStreamCreateWithFlags(&t->cap, cudaStreamNonBlocking);
+  if (e == cudaSuccess && desc->warm_start_weights) {
+    // the CNN branch at the greatest priority: its cluster of whole SMs is
+    // placed before pre-processing blocks fill them (kept in the graphs by
+    // cudaGraphInstantiateFlagUseNodePriority)
+    int least = 0, greatest = 0;
+    e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&t->side, cudaStreamNonBlocking, greatest);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_join, cudaEventDisableTiming);
+  }
   if (e != cudaSuccess) { release(t); return of_set_cuda_error(e); }
   size_t vol_bytes = 0, lam_bytes = 0, scratch_bytes = 0;
   of_volume_bytes(&desc->volume, &vol_bytes);

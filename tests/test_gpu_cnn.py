@@ -136,3 +136,33 @@ def test_training_is_reproducible_and_reduces_the_loss(of, cuda):
     losses, w = runs[0]
     assert losses[-1] < 0.5 * losses[0], losses
     assert np.array_equal(w, runs[1][1])
+
+
+def test_fused_prediction_matches_the_staged_path(of, cuda):
+    """of_cnn_predict (one cluster launch) against of_cnn_input +
+    of_cnn_forward + of_cnn_warm_pose on the trained weights: outputs within
+    1% of their norm (same arithmetic, other summation order), warm pose
+    within the same tolerance carried through the exponential map."""
+    import torch
+    from openfusion_b200 import _native as N, learned
+    net = learned.WarmStartNet(cuda, weights=learned.load_weights())
+    cfg = of.CONFIGS["c5"]
+    seq = of.make_sequence(cfg, frames=3)
+    d = torch.from_numpy(seq.depth.astype(np.int16)).to(cuda)
+    lib, st = N.lib(), torch.cuda.current_stream().cuda_stream
+    for k in (1, 2):
+        ref = net.forward(net.inputs(d[k - 1].contiguous(), d[k].contiguous()))
+        prev = torch.tensor(seq.poses[k - 1].reshape(16), dtype=torch.float64, device=cuda)
+        w_ref = torch.empty(16, dtype=torch.float64, device=cuda)
+        assert lib.of_cnn_warm_pose(ref.data_ptr(), prev.data_ptr(), w_ref.data_ptr(), st) == 0
+        out = torch.zeros(6, dtype=torch.float32, device=cuda)
+        warm = torch.zeros(16, dtype=torch.float64, device=cuda)
+        assert lib.of_cnn_predict(net.params.data_ptr(), net.master.data_ptr(), d[k - 1].data_ptr(),
+                                  d[k].data_ptr(), cfg.width, cfg.height, prev.data_ptr(),
+                                  out.data_ptr(), warm.data_ptr(), st) == 0
+        torch.cuda.synchronize()
+        r, o = ref.cpu().numpy()[0], out.cpu().numpy()
+        assert _rel(o, r) < 1e-2, (o, r)
+        W, Wr = warm.cpu().numpy().reshape(4, 4), w_ref.cpu().numpy().reshape(4, 4)
+        assert np.abs(W[:3, :3] - Wr[:3, :3]).max() < 1e-3 * max(1.0, np.abs(r).max())
+        assert np.abs(W[:3, 3] - Wr[:3, 3]).max() < 2.0
