@@ -220,6 +220,15 @@ def icp_track(cfg: Config, frame, model, pose, ws, stats=None):
                                                  _ptr(stats), _stream()))
 
 
+def icp_track_warm(cfg: Config, frame, model, pose, warm_pose, ws, stats=None):
+    """icp_track from a warm start (FP64 device 4x4), judged against the
+    previous pose in `pose`; a rejected result is replaced by plain ICP."""
+    N.check("of_icp_track_warm",
+            N.lib().of_icp_track_warm(C.byref(cfg.camera()), C.byref(cfg.icp()), _ptr(frame),
+                                      _ptr(model), _ptr(pose), _ptr(warm_pose), _ptr(ws),
+                                      _ptr(stats), _stream()))
+
+
 def icp_system(cfg: Config, level: int, frame, model, pose, ws):
     """One correspondence + reduction pass (ICP::FindCorresponding): 29 floats."""
     import torch
