@@ -15,6 +15,10 @@ Multi-GPU: the path does not shard a single sequence; N GPUs run N independent
 sequences (different seeds), one process per GPU, no collective on the frame
 path (weak scaling); timing is the max over ranks.
 
+`warm_start` compares the learned warm start with plain ICP on the
+large-motion workload (same frames, same early exit, device-timed frames/s,
+ICP iterations and per-frame pose error against the ground truth).
+
 `--impl reference` runs the CPU implementation of the same equations (the
 FP32 OpenMP build of the oracle restatement) on the host cores.
 """
@@ -47,6 +51,8 @@ def parse():
     ap.add_argument("--config", default="c2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--warm-frames", type=int, default=121,
+                    help="frames of the warm-start comparison (0 = skip it)")
     return ap.parse_args()
 
 
@@ -290,6 +296,9 @@ def run_ours(args, cfg, world, rank, local):
     # ---- per-stage kernel times (stage-wise launches with CUDA events)
     stages = stage_times(of, cfg, seq, depth_dev, order, args, dev)
 
+    # ---- the learned warm start against plain ICP (large-motion workload)
+    warm = warm_start_comparison(of, args, dev, world, rank) if args.warm_frames > 1 else None
+
     fps = world * args.steps / (ms_max / 1e3)
     e2e_fps = world * args.steps / (e2e_ms / 1e3)
     if rank != 0:
@@ -330,12 +339,47 @@ def run_ours(args, cfg, world, rank, local):
         "gpu_launches": kernels,
         "clocks": sampler.summary(),
     }
+    if warm is not None:
+        line["warm_start"] = warm
     if world == 1 and not args.no_cpu_baseline:
         cps, n, dt, cores = cpu_frames_per_s(cfg, seq, args.cpu_seconds)
         line["cpu_baseline"] = {"value": cps, "unit": "frames/s", "cores": cores, "kind": "port",
                                 "sample": f"{n} consecutive frames ({dt:.1f} s) of the same "
                                           "sequence, FP32 OpenMP restatement"}
     print(json.dumps(line), flush=True)
+
+
+def warm_start_comparison(of, args, dev, world, rank):
+    """The learned warm start against plain ICP on the large-motion workload
+    (640x480, 512^3 over 3 m, inter-frame motion up to 10 cm / 5 deg, held-out
+    seed): both trackers with the same early exit over the same rendered
+    frames, device-timed (CUDA events, max over ranks), with ICP iterations
+    and per-frame pose error against the ground truth."""
+    import dataclasses
+    from openfusion_b200 import learned
+    from openfusion_b200.train_warm_start import eval_config, pose_errors, run_tracker
+    cfg = dataclasses.replace(eval_config(of), seed=910000 + rank)
+    scene = of.make_scene(cfg.scene_kind, cfg.seed, cfg.size_mm)
+    poses = of.make_trajectory(cfg.motion, cfg.seed + 1, cfg.size_mm, args.warm_frames)
+    depth = learned.render_device(cfg, scene, poses, device=dev)
+    out = {"workload": "c5: 640x480, 512^3 over 3 m, motion U[0,10] cm / U[0,5] deg per frame; "
+                       "early exit 2e-5 rad / 0.02 mm in both arms; warm passes on the 2 finest levels",
+           "frames": args.warm_frames - 1, "data": "synthetic (held-out seed, device renderer)"}
+    weights = learned.load_weights()
+    for arm, w in (("plain", None), ("warm", weights)):
+        hist, its, kept, _ = run_tracker(of, cfg, depth, poses, w, timed=False)
+        barrier(world)
+        _, _, _, ms = run_tracker(of, cfg, depth, poses, w, timed=True)
+        ms = max_over_ranks(ms, world)
+        r, t = pose_errors(hist[1:], poses[1:])
+        out[arm] = {"frames_per_s": world * 1e3 / ms, "ms_per_frame": ms,
+                    "mean_icp_iterations": float(np.mean(its)),
+                    "max_rot_err_deg": float(np.max(r)), "mean_rot_err_deg": float(np.mean(r)),
+                    "max_trans_err_mm": float(np.max(t)), "mean_trans_err_mm": float(np.mean(t))}
+        if arm == "warm":
+            out[arm]["warm_start_kept_frac"] = float(np.mean(kept == 1))
+    out["warm_over_plain_frames_per_s"] = out["warm"]["frames_per_s"] / out["plain"]["frames_per_s"]
+    return out
 
 
 def stage_times(of, cfg, seq, depth_dev, order, args, dev):

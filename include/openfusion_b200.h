@@ -299,12 +299,20 @@ typedef struct of_tracker_desc {
 
 of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_tracker_t *out);
 of_status_t of_tracker_destroy(of_tracker_t tracker);
-/* Processes one depth frame: frame 0 is fused at the initial pose; every
- * later frame is tracked against the model of the previous one, then fused
- * and raycast. `depth_is_host` != 0: `depth` is host memory (pinned for an
- * asynchronous copy) and is copied on `stream`. */
+/* Processes one depth frame in the reference's order (RunApp::display,
+ * MainApp.cpp:786-964): the previous frame is fused at its tracked pose and
+ * the model raycast there, while this frame is pre-processed (graph
+ * branches); then this frame is tracked against that model. Frame 0 only
+ * sets the pose (its initial pose). The pose is this frame's when the call's
+ * work completes; the volume and model hold the frames before it until the
+ * next call or of_tracker_flush. `depth_is_host` != 0: `depth` is host memory
+ * (pinned for an asynchronous copy) and is copied on `stream`. */
 of_status_t of_tracker_process(of_tracker_t tracker, const uint16_t *depth, int32_t depth_is_host,
                                of_stream_t stream);
+/* Fuses the last processed frame at its pose and raycasts the model there
+ * now (before reading the volume or the model); the next
+ * of_tracker_process then skips that fusion. No effect when already done. */
+of_status_t of_tracker_flush(of_tracker_t tracker, of_stream_t stream);
 /* Sets the starting pose of the next frame's ICP to `pose_delta` x previous
  * pose (host FP64 4x4, world frame); used for a warm start. NULL clears it. */
 of_status_t of_tracker_set_prior(of_tracker_t tracker, const double *pose_delta);
@@ -328,7 +336,7 @@ typedef struct of_tracker_buffers {
   of_icp_stats_t *stats;
   int64_t frames;
   int32_t kernels_first;  /* kernel launches of frame 0's graph */
-  int32_t kernels_track;  /* kernel launches of every later frame's graph */
+  int32_t kernels_track;  /* kernel launches of every later step's graph */
 } of_tracker_buffers_t;
 of_status_t of_tracker_buffers(of_tracker_t tracker, of_tracker_buffers_t *out);
 

@@ -113,6 +113,7 @@ _SIGS = {
     "of_tracker_create": (c_status, [C.POINTER(TrackerDesc), C.POINTER(C.c_void_p)]),
     "of_tracker_destroy": (c_status, [P]),
     "of_tracker_process": (c_status, [P, P, C.c_int32, c_stream]),
+    "of_tracker_flush": (c_status, [P, c_stream]),
     "of_tracker_set_prior": (c_status, [P, P]),
     "of_tracker_pose": (c_status, [P, P, P, c_stream]),
     "of_tracker_pose_history": (c_status, [P, P, C.c_int32, c_stream]),

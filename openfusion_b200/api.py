@@ -328,6 +328,11 @@ class Tracker:
                 N.lib().of_tracker_process(self._h, depth.data_ptr(), on_host, _stream(stream)))
         self.frames += 1
 
+    def flush(self, stream=None):
+        """Fuses the last processed frame now (each process() call fuses the
+        frame before it); call before reading the volume or the model."""
+        N.check("of_tracker_flush", N.lib().of_tracker_flush(self._h, _stream(stream)))
+
     def set_prior(self, delta: np.ndarray | None):
         arr = None if delta is None else (C.c_double * 16)(*np.asarray(delta, np.float64).reshape(16))
         N.check("of_tracker_set_prior", N.lib().of_tracker_set_prior(self._h, arr))

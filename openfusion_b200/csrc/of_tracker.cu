@@ -1,13 +1,17 @@
 // of_tracker.cu -- the whole per-frame pipeline, owned state and CUDA graphs.
 //
 // Replaces RunApp::display (Source/src/MainApp.cpp:786-964) without its host
-// round trips: frame k is pre-processed, tracked against the model raycast
-// after frame k-1, fused at the tracked pose and raycast at that pose for
-// frame k+1. The reference's order (integrate(k-1) -> raycast(k-1) ->
-// convert(k) -> ICP(k) -> UpdateTransforms) is the same sequence rotated by
-// one stage. The state the reference allocates in RunApp::initCudaPointers
-// (MainApp.cpp:591-647) lives here; the per-frame launch sequence is captured
-// once as a CUDA graph and replayed.
+// round trips and in its order: the step that receives depth frame k fuses
+// frame k-1 at its tracked pose and raycasts the model there
+// (integrate(k-1) -> raycast(k-1)), pre-processes frame k, and tracks frame k
+// against that model (convert(k) -> ICP(k)). Pre-processing (and the
+// warm-start CNN) depend only on the new depth frame, so they run on graph
+// branches beside integrate -> raycast and join before ICP; the last frame is
+// fused by the next step or by of_tracker_flush. The depth input is double
+// buffered (frame k-1 is fused while frame k is pre-processed). The state the
+// reference allocates in RunApp::initCudaPointers (MainApp.cpp:591-647) lives
+// here; each step's launch sequence is captured once as a CUDA graph (one per
+// depth-buffer parity) and replayed.
 #include "of_common.cuh"
 
 #include <new>
@@ -27,9 +31,11 @@ struct of_tracker {
   of_tracker_desc_t desc;
   of_pyramid_layout_t lay;
   cudaStream_t cap;
-  // the warm-start CNN runs on a branch beside pre-processing (fork / join)
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // branches of a step: pre-processing, and the warm-start CNN at the
+  // greatest stream priority (its cluster of whole SMs is placed before other
+  // blocks fill them; kept in the graphs by cudaGraphInstantiateFlagUseNodePriority)
+  cudaStream_t pre = nullptr, side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_pre = nullptr, ev_cnn = nullptr;
   void *volume = nullptr;
   void *frame = nullptr;
   void *model = nullptr;
@@ -37,7 +43,7 @@ struct of_tracker {
   double *pose = nullptr;
   double *hist = nullptr;
   unsigned long long *hist_count = nullptr;
-  uint16_t *depth = nullptr;
+  uint16_t *depth[2] = {nullptr, nullptr};  // frame k in depth[k & 1]
   float *lambda = nullptr;
   void *scratch = nullptr;
   of_icp_stats_t *stats = nullptr;
@@ -45,18 +51,15 @@ struct of_tracker {
   bool warm = false;
   float *cnn_master = nullptr;
   uint16_t *cnn_params = nullptr;
-  void *cnn_ws = nullptr;
-  uint16_t *cnn_in = nullptr;
-  float *cnn_cells = nullptr;
   float *cnn_out = nullptr;
   double *warm_pose = nullptr;
-  uint16_t *prev_depth = nullptr;
   int hist_cap = 1024;
   int64_t frames = 0;
+  bool last_fused = false;  // of_tracker_flush fused the last frame already
   int kernels_first = 0;
   int kernels_track = 0;
   cudaGraphExec_t g_first = nullptr;
-  cudaGraphExec_t g_track = nullptr;
+  cudaGraphExec_t g_track[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -70,43 +73,51 @@ __global__ void k_record_pose(const double *pose, double *hist, unsigned long lo
   *count = c + 1;
 }
 
-of_status_t enqueue_frame(of_tracker *t, bool track, cudaStream_t s) {
+// Frame 0 of a tracker: its pose is the initial pose (fused by the next step).
+of_status_t enqueue_first(of_tracker *t, cudaStream_t s) {
+  k_record_pose<<<1, 32, 0, s>>>(t->pose, t->hist, t->hist_count, t->hist_cap);
+  return of_launch_status();
+}
+
+// fuse the frame in `depth` at the current pose and raycast the model there
+of_status_t enqueue_fuse(of_tracker *t, const uint16_t *depth, cudaStream_t s) {
   const of_tracker_desc_t &d = t->desc;
-  of_status_t st;
-  if (track) {
-    if (t->warm) {
-      // the CNN's motion estimate between the previous and this depth frame,
-      // on a branch that runs beside pre-processing and joins before ICP
-      OF_CUDA_TRY(cudaEventRecord(t->ev_fork, s));
-      OF_CUDA_TRY(cudaStreamWaitEvent(t->side, t->ev_fork, 0));
-      st = of_cnn_predict(t->cnn_params, t->cnn_master, t->prev_depth, t->depth, d.camera.width,
-                          d.camera.height, t->pose, t->cnn_out, t->warm_pose, t->side);
-      OF_CUDA_TRY(cudaEventRecord(t->ev_join, t->side));
-      if (st != OF_OK) {
-        cudaStreamWaitEvent(s, t->ev_join, 0);
-        return st;
-      }
-    }
-    st = of_preprocess(&d.camera, &d.filter, t->depth, d.camera.width, t->frame, s);
-    if (t->warm) OF_CUDA_TRY(cudaStreamWaitEvent(s, t->ev_join, 0));
-    if (st != OF_OK) return st;
-    st = of_icp_launch(&d.camera, &d.icp, t->frame, t->model, t->pose, t->icp_ws, t->stats, s,
-                       t->warm ? t->warm_pose : nullptr);
-    if (st != OF_OK) return st;
-  }
-  st = of_integrate_tiled(&d.volume, t->volume, &d.camera, t->depth, d.camera.width, t->pose,
-                          t->lambda, t->scratch, s);
+  of_status_t st = of_integrate_tiled(&d.volume, t->volume, &d.camera, depth, d.camera.width,
+                                      t->pose, t->lambda, t->scratch, s);
   if (st != OF_OK) return st;
-  st = of_raycast(&d.volume, t->volume, &d.camera, &d.raycast, d.icp.levels, t->pose, t->model,
-                  nullptr, s);
+  return of_raycast(&d.volume, t->volume, &d.camera, &d.raycast, d.icp.levels, t->pose, t->model,
+                    nullptr, s);
+}
+
+// The step of frame k >= 1 (depth[cur]): integrate(k-1) -> raycast(k-1) on
+// `s`, beside pre-process(k) and the CNN(k-1, k) on their branches; ICP(k)
+// after the join. `fuse` = false when of_tracker_flush fused frame k-1.
+of_status_t enqueue_track(of_tracker *t, int cur, bool fuse, cudaStream_t s) {
+  const of_tracker_desc_t &d = t->desc;
+  const uint16_t *now = t->depth[cur], *before = t->depth[cur ^ 1];
+  OF_CUDA_TRY(cudaEventRecord(t->ev_fork, s));
+  OF_CUDA_TRY(cudaStreamWaitEvent(t->pre, t->ev_fork, 0));
+  of_status_t st = OF_OK;
+  if (t->warm) {
+    OF_CUDA_TRY(cudaStreamWaitEvent(t->side, t->ev_fork, 0));
+    st = of_cnn_predict(t->cnn_params, t->cnn_master, before, now, d.camera.width,
+                        d.camera.height, t->pose, t->cnn_out, t->warm_pose, t->side);
+    OF_CUDA_TRY(cudaEventRecord(t->ev_cnn, t->side));
+  }
+  of_status_t sp = of_preprocess(&d.camera, &d.filter, now, d.camera.width, t->frame, t->pre);
+  OF_CUDA_TRY(cudaEventRecord(t->ev_pre, t->pre));
+  of_status_t sf = fuse ? enqueue_fuse(t, before, s) : OF_OK;
+  // every branch joins before an error returns (a capture must end joined)
+  OF_CUDA_TRY(cudaStreamWaitEvent(s, t->ev_pre, 0));
+  if (t->warm) OF_CUDA_TRY(cudaStreamWaitEvent(s, t->ev_cnn, 0));
+  if (st != OF_OK) return st;
+  if (sp != OF_OK) return sp;
+  if (sf != OF_OK) return sf;
+  st = of_icp_launch(&d.camera, &d.icp, t->frame, t->model, t->pose, t->icp_ws, t->stats, s,
+                     t->warm ? t->warm_pose : nullptr);
   if (st != OF_OK) return st;
   k_record_pose<<<1, 32, 0, s>>>(t->pose, t->hist, t->hist_count, t->hist_cap);
-  st = of_launch_status();
-  if (st == OF_OK && t->warm)  // the next frame's pair
-    OF_CUDA_TRY(cudaMemcpyAsync(t->prev_depth, t->depth,
-                                (size_t)d.camera.width * d.camera.height * sizeof(uint16_t),
-                                cudaMemcpyDeviceToDevice, s));
-  return st;
+  return of_launch_status();
 }
 
 int count_kernel_nodes(cudaGraph_t g) {
@@ -123,17 +134,18 @@ int count_kernel_nodes(cudaGraph_t g) {
   return k;
 }
 
-of_status_t capture(of_tracker *t, bool track, cudaGraphExec_t *out) {
+// graph of frame 0 (cur < 0) or of a tracking step with depth[cur]
+of_status_t capture(of_tracker *t, int cur, cudaGraphExec_t *out) {
   cudaGraph_t g = nullptr;
   OF_CUDA_TRY(cudaStreamBeginCapture(t->cap, cudaStreamCaptureModeThreadLocal));
-  of_status_t st = enqueue_frame(t, track, t->cap);
+  of_status_t st = cur < 0 ? enqueue_first(t, t->cap) : enqueue_track(t, cur, true, t->cap);
   cudaError_t e = cudaStreamEndCapture(t->cap, &g);
   if (st != OF_OK) {
     if (g) cudaGraphDestroy(g);
     return st;
   }
   if (e != cudaSuccess) return of_set_cuda_error(e);
-  (track ? t->kernels_track : t->kernels_first) = count_kernel_nodes(g);
+  (cur >= 0 ? t->kernels_track : t->kernels_first) = count_kernel_nodes(g);
   e = cudaGraphInstantiateWithFlags(out, g, cudaGraphInstantiateFlagUseNodePriority);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return of_set_cuda_error(e);
@@ -142,16 +154,17 @@ of_status_t capture(of_tracker *t, bool track, cudaGraphExec_t *out) {
 
 void release(of_tracker *t) {
   if (t->g_first) cudaGraphExecDestroy(t->g_first);
-  if (t->g_track) cudaGraphExecDestroy(t->g_track);
+  for (cudaGraphExec_t g : t->g_track)
+    if (g) cudaGraphExecDestroy(g);
   void *bufs[] = {t->volume, t->frame, t->model, t->icp_ws, t->pose, t->hist, t->hist_count,
-                  t->depth, t->lambda, t->scratch, t->stats, t->cnn_master, t->cnn_params,
-                  t->cnn_ws, t->cnn_in, t->cnn_cells, t->cnn_out, t->warm_pose, t->prev_depth};
+                  t->depth[0], t->depth[1], t->lambda, t->scratch, t->stats, t->cnn_master,
+                  t->cnn_params, t->cnn_out, t->warm_pose};
   for (void *b : bufs)
     if (b) cudaFree(b);
-  if (t->cap) cudaStreamDestroy(t->cap);
-  if (t->side) cudaStreamDestroy(t->side);
-  if (t->ev_fork) cudaEventDestroy(t->ev_fork);
-  if (t->ev_join) cudaEventDestroy(t->ev_join);
+  for (cudaStream_t q : {t->cap, t->pre, t->side})
+    if (q) cudaStreamDestroy(q);
+  for (cudaEvent_t ev : {t->ev_fork, t->ev_pre, t->ev_cnn})
+    if (ev) cudaEventDestroy(ev);
   delete t;
 }
 
@@ -171,15 +184,14 @@ extern "C" of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_track
   of_status_t st = of_pyramid_layout(&desc->camera, desc->icp.levels, &t->lay);
   if (st != OF_OK) { release(t); return st; }
   cudaError_t e = cudaStreamCreateWithFlags(&t->cap, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&t->pre, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_pre, cudaEventDisableTiming);
   if (e == cudaSuccess && desc->warm_start_weights) {
-    // the CNN branch at the greatest priority: its cluster of whole SMs is
-    // placed before pre-processing blocks fill them (kept in the graphs by
-    // cudaGraphInstantiateFlagUseNodePriority)
     int least = 0, greatest = 0;
     e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
     if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&t->side, cudaStreamNonBlocking, greatest);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_fork, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_cnn, cudaEventDisableTiming);
   }
   if (e != cudaSuccess) { release(t); return of_set_cuda_error(e); }
   size_t vol_bytes = 0, lam_bytes = 0, scratch_bytes = 0;
@@ -188,13 +200,11 @@ extern "C" of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_track
   of_integrate_scratch_bytes(&desc->volume, &desc->camera, &scratch_bytes);
   size_t px = (size_t)desc->camera.width * desc->camera.height;
   int64_t np = 0;
-  size_t cnn_ws = 0;
   t->warm = desc->warm_start_weights != nullptr;
   if (t->warm) {
     const int w = desc->camera.width, h = desc->camera.height;
     if (w % 80 || h % 60 || w / 80 != h / 60) { release(t); return OF_ERR_INVALID_ARGUMENT; }
     of_cnn_param_count(&np);
-    of_cnn_workspace_bytes(1, &cnn_ws);
   }
   struct { void **p; size_t n; } allocs[] = {
       {&t->volume, vol_bytes},
@@ -204,18 +214,15 @@ extern "C" of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_track
       {(void **)&t->pose, 16 * sizeof(double)},
       {(void **)&t->hist, (size_t)t->hist_cap * 16 * sizeof(double)},
       {(void **)&t->hist_count, sizeof(unsigned long long)},
-      {(void **)&t->depth, px * sizeof(uint16_t)},
+      {(void **)&t->depth[0], px * sizeof(uint16_t)},
+      {(void **)&t->depth[1], px * sizeof(uint16_t)},
       {(void **)&t->lambda, lam_bytes},
       {&t->scratch, scratch_bytes},
       {(void **)&t->stats, sizeof(of_icp_stats_t)},
       {(void **)&t->cnn_master, (size_t)np * sizeof(float)},
       {(void **)&t->cnn_params, (size_t)np * sizeof(uint16_t)},
-      {&t->cnn_ws, cnn_ws},
-      {(void **)&t->cnn_in, t->warm ? 2 * 60 * 80 * sizeof(uint16_t) : 0},
-      {(void **)&t->cnn_cells, t->warm ? 2 * 60 * 80 * sizeof(float) : 0},
       {(void **)&t->cnn_out, t->warm ? 6 * sizeof(float) : 0},
       {(void **)&t->warm_pose, t->warm ? 16 * sizeof(double) : 0},
-      {(void **)&t->prev_depth, t->warm ? px * sizeof(uint16_t) : 0},
   };
   for (auto &a : allocs) {
     if (a.n == 0) continue;
@@ -243,8 +250,9 @@ extern "C" of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_track
   if (st == OF_OK) st = of_lambda_table(&desc->camera, t->lambda, s);
   if (st == OF_OK && cudaStreamSynchronize(s) != cudaSuccess) st = of_set_cuda_error(cudaGetLastError());
   if (st == OF_OK && desc->use_graph) {
-    st = capture(t, false, &t->g_first);
-    if (st == OF_OK) st = capture(t, true, &t->g_track);
+    st = capture(t, -1, &t->g_first);
+    if (st == OF_OK) st = capture(t, 0, &t->g_track[0]);
+    if (st == OF_OK) st = capture(t, 1, &t->g_track[1]);
   }
   if (st != OF_OK) { release(t); return st; }
   *out = t;
@@ -262,20 +270,31 @@ extern "C" of_status_t of_tracker_process(of_tracker_t t, const uint16_t *depth,
                                           of_stream_t stream) {
   if (!t || !depth) return OF_ERR_INVALID_ARGUMENT;
   cudaStream_t s = (cudaStream_t)stream;
+  const int cur = (int)(t->frames & 1);
   size_t bytes = (size_t)t->desc.camera.width * t->desc.camera.height * sizeof(uint16_t);
   if (on_host) {
-    OF_CUDA_TRY(cudaMemcpyAsync(t->depth, depth, bytes, cudaMemcpyHostToDevice, s));
-  } else if (depth != t->depth) {
-    OF_CUDA_TRY(cudaMemcpyAsync(t->depth, depth, bytes, cudaMemcpyDeviceToDevice, s));
+    OF_CUDA_TRY(cudaMemcpyAsync(t->depth[cur], depth, bytes, cudaMemcpyHostToDevice, s));
+  } else if (depth != t->depth[cur]) {
+    OF_CUDA_TRY(cudaMemcpyAsync(t->depth[cur], depth, bytes, cudaMemcpyDeviceToDevice, s));
   }
-  bool track = t->frames > 0;
-  if (t->desc.use_graph) {
-    OF_CUDA_TRY(cudaGraphLaunch(track ? t->g_track : t->g_first, s));
+  const bool track = t->frames > 0;
+  if (t->desc.use_graph && !(track && t->last_fused)) {
+    OF_CUDA_TRY(cudaGraphLaunch(track ? t->g_track[cur] : t->g_first, s));
   } else {
-    of_status_t st = enqueue_frame(t, track, s);
+    of_status_t st = track ? enqueue_track(t, cur, !t->last_fused, s) : enqueue_first(t, s);
     if (st != OF_OK) return st;
   }
+  t->last_fused = false;
   t->frames += 1;
+  return OF_OK;
+}
+
+extern "C" of_status_t of_tracker_flush(of_tracker_t t, of_stream_t stream) {
+  if (!t) return OF_ERR_INVALID_ARGUMENT;
+  if (t->frames == 0 || t->last_fused) return OF_OK;
+  of_status_t st = enqueue_fuse(t, t->depth[(t->frames - 1) & 1], (cudaStream_t)stream);
+  if (st != OF_OK) return st;
+  t->last_fused = true;
   return OF_OK;
 }
 
@@ -318,7 +337,7 @@ extern "C" of_status_t of_tracker_buffers(of_tracker_t t, of_tracker_buffers_t *
   out->frame = t->frame;
   out->model = t->model;
   out->pose = t->pose;
-  out->depth = t->depth;
+  out->depth = t->frames > 0 ? t->depth[(t->frames - 1) & 1] : t->depth[0];
   out->lambda = t->lambda;
   out->stats = t->stats;
   out->frames = t->frames;

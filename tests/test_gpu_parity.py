@@ -301,6 +301,70 @@ def test_tracker_graph_equals_eager(of, cuda):
     assert np.array_equal(poses[0], poses[1])
 
 
+def test_tracker_equals_stagewise_pipeline(of, cuda):
+    """The tracker's step (fuse k-1 and raycast beside pre-process k, then
+    ICP k) gives bit for bit the poses of the stage-by-stage sequence
+    integrate(k-1) -> raycast(k-1) -> preprocess(k) -> ICP(k) through the
+    public per-stage calls."""
+    import torch
+    cfg = small(of, "c1")
+    n = 6
+    seq = of.make_sequence(cfg, frames=n)
+    depth = [torch.from_numpy(seq.depth[k].astype(np.int16)).to(cuda) for k in range(n)]
+    tr = of.Tracker(cfg, seq.poses[0], use_graph=True)
+    for k in range(n):
+        tr.process(depth[k])
+    hist = tr.pose_history(n)
+    tr.close()
+    vol, lam = of.new_volume(cfg, cuda), of.lambda_table(cfg, cuda)
+    scratch = of.integrate_scratch(cfg, cuda)
+    frame, model = of.new_pyramid(cfg, cuda), of.new_pyramid(cfg, cuda)
+    ws = of.icp_workspace(cfg, cuda)
+    pose = dev_pose(seq.poses[0], cuda)
+    ref = [seq.poses[0]]
+    for k in range(1, n):
+        of.integrate(cfg, vol, depth[k - 1], pose, lam, scratch)
+        of.raycast(cfg, vol, pose, model)
+        of.preprocess(cfg, depth[k], frame)
+        of.icp_track(cfg, frame, model, pose, ws)
+        ref.append(pose.cpu().numpy().reshape(4, 4).copy())
+    assert np.array_equal(hist, np.array(ref))
+
+
+def test_tracker_flush_fuses_the_last_frame_once(of, cuda):
+    """of_tracker_flush fuses the last frame early; later steps skip that
+    fusion, so poses and the final volume equal those of a tracker that never
+    flushed (and then flushes once)."""
+    import ctypes as C
+    import torch
+    cfg = small(of, "c1", resolution=64)
+    n = 8
+    seq = of.make_sequence(cfg, frames=n)
+    depth = [torch.from_numpy(seq.depth[k].astype(np.int16)).to(cuda) for k in range(n)]
+    lib, stream = of._native.lib(), torch.cuda.current_stream().cuda_stream
+    out = []
+    for flush_at in ((), (2, 3, 5)):
+        tr = of.Tracker(cfg, seq.poses[0], use_graph=True)
+        for k in range(n):
+            tr.process(depth[k])
+            if k in flush_at:
+                tr.flush()
+                tr.flush()  # a second flush has no effect
+        tr.flush()
+        hist = tr.pose_history(n)
+        m = cfg.resolution ** 3
+        tsdf = torch.empty(m, dtype=torch.float32, device=cuda)
+        wgt = torch.empty(m, dtype=torch.int16, device=cuda)
+        assert lib.of_volume_export(C.byref(cfg.volume()), C.c_void_p(tr.buffers().volume),
+                                    tsdf.data_ptr(), wgt.data_ptr(), stream) == 0
+        torch.cuda.synchronize()
+        out.append((hist, tsdf.cpu().numpy(), wgt.cpu().numpy()))
+        tr.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
+    assert out[0][2].view(np.uint16).max() == n  # every frame fused exactly once
+
+
 def test_tracker_follows_ground_truth(of, cuda):
     import torch
     cfg = small(of, "c1")
