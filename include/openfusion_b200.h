@@ -340,6 +340,65 @@ typedef struct of_tracker_buffers {
 } of_tracker_buffers_t;
 of_status_t of_tracker_buffers(of_tracker_t tracker, of_tracker_buffers_t *out);
 
+/* ---- many independent streams (batched) ------------------------------- */
+
+/* One depth stream of a batch: its camera, volume and initial pose. */
+typedef struct of_batch_stream {
+  of_camera_t camera;
+  of_volume_desc_t volume;  /* all streams of a batch use the same storage */
+  double initial_pose[16];  /* camera-to-world of its frame 0 */
+} of_batch_stream_t;
+
+/* Tuning knobs of the batched stages; none changes a result. */
+typedef struct of_batch_tuning {
+  int32_t ray_tile;      /* raycast block: 0 = 16x16, 1 = 32x8, 2 = 8x32, 3 = 32x4 */
+  int32_t list_div;      /* integration blocks per stream = bricks / {16,32,64,128,256}[list_div] */
+  int32_t icp_clusters;  /* resident 8-CTA clusters of the batched ICP (0 = as many as fit) */
+  int32_t tuned;         /* (of_batch_tuning) 1 = chosen by measurement */
+} of_batch_tuning_t;
+
+typedef struct of_batch_desc {
+  int32_t count;                     /* streams */
+  const of_batch_stream_t *streams;  /* count entries (copied) */
+  of_filter_params_t filter;         /* shared by all streams */
+  of_raycast_params_t raycast;
+  of_icp_params_t icp;
+  int32_t use_graph;  /* 1 = replay each step as a captured CUDA graph */
+  int32_t tune;       /* 1 = choose the knobs online by timing candidates on the first steps */
+  of_batch_tuning_t tuning;  /* the knobs when tune == 0 (start values otherwise) */
+} of_batch_desc_t;
+
+typedef struct of_batch *of_batch_t;
+
+/* Many independent streams tracked and fused together, one launch per stage
+ * for all of them (the tracker's step order for every stream): batched
+ * filter + pyramid + maps, integration, raycast, and one persistent launch of
+ * thread-block clusters for every stream's ICP. Per stream, every stage but
+ * ICP writes what the single-stream stage writes; ICP sums in another order.
+ * No reference counterpart (the reference runs one camera). */
+of_status_t of_batch_create(const of_batch_desc_t *desc, of_batch_t *out);
+of_status_t of_batch_destroy(of_batch_t batch);
+/* One frame of every stream: `depth[i]` (count pointers; host memory when
+ * `depth_is_host`, copied on `stream`) is stream i's next frame. */
+of_status_t of_batch_process(of_batch_t batch, const uint16_t *const *depth, int32_t depth_is_host,
+                             of_stream_t stream);
+/* Fuses every stream's last frame now (see of_tracker_flush). */
+of_status_t of_batch_flush(of_batch_t batch, of_stream_t stream);
+/* Current poses (count x 16 FP64, host) and optionally each stream's last
+ * ICP statistics (count entries), copied on `stream`. */
+of_status_t of_batch_poses(of_batch_t batch, double *poses, of_icp_stats_t *stats,
+                           of_stream_t stream);
+/* The knobs in use (after tuning: the measured winners). */
+of_status_t of_batch_tuning(of_batch_t batch, of_batch_tuning_t *out);
+/* Device pointers of stream i's state (volume, pyramids, pose, ...). */
+of_status_t of_batch_stream_buffers(of_batch_t batch, int32_t i, of_tracker_buffers_t *out);
+/* Host-only planning: a stream's per-frame work in voxel-visit units, and a
+ * longest-first greedy assignment of streams to `ranks` GPUs. */
+of_status_t of_batch_stream_cost(const of_batch_stream_t *stream, const of_icp_params_t *icp,
+                                 double *cost);
+of_status_t of_batch_shard(const double *cost, int32_t count, int32_t ranks,
+                           int32_t *rank_of_stream);
+
 /* ---- reference-layout adapters (for the reference's PointInfo /
  *      CameraData: AoS float3, BAD_VERTEX = FLT_MAX, BasicTypes.h:40-49) --- */
 

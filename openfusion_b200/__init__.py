@@ -6,17 +6,17 @@ CUDA kernels behind the C-ABI of include/openfusion_b200.h; this package is the
 Python mirror of the reference's per-frame interfaces over that ABI.
 """
 from . import _native
-from .api import (CONFIGS, Config, Sequence, Tracker, integrate_scratch, icp_system, icp_track,
+from .api import (CONFIGS, Batch, Config, c4_configs, Sequence, Tracker, integrate_scratch, icp_system, icp_track,
                   icp_track_warm,
                   icp_workspace, integrate, integrate_census, lambda_table, level_camera, linear_to_volume,
                   make_scene, make_sequence, make_trajectory, new_pyramid, new_volume,
                   preprocess, pyramid_layout, raycast, render, unpack_depth, unpack_points,
-                  volume_bytes, volume_to_linear)
+                  volume_bytes, volume_to_linear, shard, stream_cost)
 
 __all__ = [
-    "CONFIGS", "Config", "Sequence", "Tracker", "integrate_scratch", "icp_system", "icp_track", "icp_track_warm", "icp_workspace",
+    "CONFIGS", "Batch", "Config", "c4_configs", "Sequence", "Tracker", "integrate_scratch", "icp_system", "icp_track", "icp_track_warm", "icp_workspace",
     "integrate", "integrate_census", "lambda_table", "level_camera", "linear_to_volume",
     "make_scene", "make_sequence", "make_trajectory", "new_pyramid", "new_volume", "preprocess",
     "pyramid_layout", "raycast", "render", "unpack_depth", "unpack_points", "volume_bytes",
-    "volume_to_linear",
+    "volume_to_linear", "shard", "stream_cost",
 ]

@@ -68,6 +68,21 @@ class TrackerBuffers(C.Structure):
                 ("kernels_track", C.c_int32)]
 
 
+class BatchStream(C.Structure):
+    _fields_ = [("camera", Camera), ("volume", VolumeDesc), ("initial_pose", C.c_double * 16)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("ray_tile", C.c_int32), ("list_div", C.c_int32), ("icp_clusters", C.c_int32),
+                ("tuned", C.c_int32)]
+
+
+class BatchDesc(C.Structure):
+    _fields_ = [("count", C.c_int32), ("streams", C.POINTER(BatchStream)),
+                ("filter", FilterParams), ("raycast", RaycastParams), ("icp", IcpParams),
+                ("use_graph", C.c_int32), ("tune", C.c_int32), ("tuning", BatchTuning)]
+
+
 class SynthPrim(C.Structure):
     _fields_ = [("kind", C.c_int32), ("p", C.c_float * 10)]
 
@@ -114,6 +129,16 @@ _SIGS = {
     "of_tracker_destroy": (c_status, [P]),
     "of_tracker_process": (c_status, [P, P, C.c_int32, c_stream]),
     "of_tracker_flush": (c_status, [P, c_stream]),
+    "of_batch_create": (c_status, [C.POINTER(BatchDesc), C.POINTER(C.c_void_p)]),
+    "of_batch_destroy": (c_status, [P]),
+    "of_batch_process": (c_status, [P, C.POINTER(C.c_void_p), C.c_int32, c_stream]),
+    "of_batch_flush": (c_status, [P, c_stream]),
+    "of_batch_poses": (c_status, [P, P, P, c_stream]),
+    "of_batch_tuning": (c_status, [P, C.POINTER(BatchTuning)]),
+    "of_batch_stream_buffers": (c_status, [P, C.c_int32, C.POINTER(TrackerBuffers)]),
+    "of_batch_stream_cost": (c_status, [C.POINTER(BatchStream), C.POINTER(IcpParams),
+                                        C.POINTER(C.c_double)]),
+    "of_batch_shard": (c_status, [P, C.c_int32, C.c_int32, P]),
     "of_tracker_set_prior": (c_status, [P, P]),
     "of_tracker_pose": (c_status, [P, P, P, c_stream]),
     "of_tracker_pose_history": (c_status, [P, P, C.c_int32, c_stream]),

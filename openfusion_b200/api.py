@@ -102,6 +102,25 @@ CONFIGS = {
 }
 
 
+def c4_configs(count: int = 64, seed: int = 4000, frames: int = 100) -> list[Config]:
+    """The batched-streams workload: `count` independent seeded scenes (room
+    of 20 boxes and spheres), each with a resolution drawn uniformly from
+    {160x120, 320x240, 640x480} (intrinsics scaled from 640x480 / 525 px) and
+    a volume drawn from {128^3, 256^3, 512^3} over U[2, 3] m (truncation the
+    larger of 30 mm and 4 voxels). Stream i: scene seed seed + i."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        w, h = [(160, 120), (320, 240), (640, 480)][int(rng.integers(0, 3))]
+        res = [128, 256, 512][int(rng.integers(0, 3))]
+        size = float(rng.uniform(2000.0, 3000.0))
+        f = 525.0 * w / 640.0
+        out.append(Config(f"c4_s{i}_{w}x{h}_{res}^3", w, h, f, f, (w - 1) / 2.0, (h - 1) / 2.0,
+                          res, size, max(30.0, 4.0 * size / res), max_weight=128, scene_kind=1,
+                          frames=frames, seed=seed + i, dropout=0.02))
+    return out
+
+
 def _stream(stream=None) -> int:
     import torch
     s = stream if stream is not None else torch.cuda.current_stream()
@@ -411,3 +430,104 @@ def make_sequence(cfg: Config, frames: int | None = None, render_depth: bool = T
     if render_depth:
         seq.depth = np.stack([render(cfg, scene, poses[k], k) for k in range(f)])
     return seq
+
+
+# ------------------------------------------------------------------ batched --
+
+def stream_cost(cfg: Config) -> float:
+    """Per-frame work of one stream (voxel-visit units), of_batch_stream_cost."""
+    st = N.BatchStream()
+    st.camera = cfg.camera()
+    st.volume = cfg.volume()
+    c = C.c_double()
+    N.check("of_batch_stream_cost", N.lib().of_batch_stream_cost(C.byref(st), C.byref(cfg.icp()),
+                                                                 C.byref(c)))
+    return c.value
+
+
+def shard(costs, ranks: int) -> list[int]:
+    """Longest-first greedy assignment of streams to ranks (of_batch_shard)."""
+    n = len(costs)
+    arr = (C.c_double * max(n, 1))(*costs)
+    out = (C.c_int32 * max(n, 1))()
+    N.check("of_batch_shard", N.lib().of_batch_shard(C.cast(arr, C.c_void_p), n, ranks,
+                                                     C.cast(out, C.c_void_p)))
+    return [int(out[i]) for i in range(n)]
+
+
+class Batch:
+    """Many independent streams (each its own Config: camera, volume) tracked
+    and fused together, one launch per stage for all streams (of_batch_*).
+    The filter, raycast and ICP parameters are `common`'s (default: the first
+    stream's)."""
+
+    def __init__(self, cfgs: list[Config], initial_poses, common: Config | None = None,
+                 use_graph: bool = True, tune: bool = False, tuning: tuple | None = None):
+        common = common or cfgs[0]
+        self.cfgs = list(cfgs)
+        n = len(cfgs)
+        self._streams = (N.BatchStream * n)()
+        for i, (c, P) in enumerate(zip(cfgs, initial_poses)):
+            self._streams[i].camera = c.camera()
+            self._streams[i].volume = c.volume()
+            self._streams[i].initial_pose = (C.c_double * 16)(*np.asarray(P, np.float64).reshape(16))
+        d = N.BatchDesc()
+        d.count = n
+        d.streams = C.cast(self._streams, C.POINTER(N.BatchStream))
+        d.filter = common.filter()
+        d.raycast = common.raycast()
+        d.icp = common.icp()
+        d.use_graph = 1 if use_graph else 0
+        d.tune = 1 if tune else 0
+        t = tuning or (0, 2, 0)
+        d.tuning = N.BatchTuning(t[0], t[1], t[2], 0)
+        h = C.c_void_p()
+        N.check("of_batch_create", N.lib().of_batch_create(C.byref(d), C.byref(h)))
+        self._h = h
+        self.frames = 0
+
+    def close(self):
+        if self._h:
+            N.lib().of_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def process(self, depths, stream=None):
+        """One frame of every stream: CUDA uint16 tensors, or (pinned) CPU tensors."""
+        assert len(depths) == len(self.cfgs)
+        on_host = 0 if depths[0].is_cuda else 1
+        ptrs = (C.c_void_p * len(depths))(*[d.data_ptr() for d in depths])
+        N.check("of_batch_process", N.lib().of_batch_process(self._h, ptrs, on_host,
+                                                             _stream(stream)))
+        self.frames += 1
+
+    def flush(self, stream=None):
+        N.check("of_batch_flush", N.lib().of_batch_flush(self._h, _stream(stream)))
+
+    def poses(self, with_stats: bool = False):
+        """(n, 4, 4) current poses (synchronous), and the ICP statistics."""
+        import torch
+        n = len(self.cfgs)
+        out = np.zeros((n, 16), np.float64)
+        stats = (N.IcpStats * n)()
+        N.check("of_batch_poses", N.lib().of_batch_poses(self._h, out.ctypes.data,
+                                                         C.cast(stats, C.c_void_p), _stream()))
+        torch.cuda.current_stream().synchronize()
+        P = out.reshape(n, 4, 4)
+        return (P, list(stats)) if with_stats else P
+
+    def tuning(self) -> N.BatchTuning:
+        t = N.BatchTuning()
+        N.check("of_batch_tuning", N.lib().of_batch_tuning(self._h, C.byref(t)))
+        return t
+
+    def buffers(self, i: int) -> N.TrackerBuffers:
+        b = N.TrackerBuffers()
+        N.check("of_batch_stream_buffers", N.lib().of_batch_stream_buffers(self._h, i, C.byref(b)))
+        return b
+

@@ -32,6 +32,7 @@ CUDA_SOURCES = [
     "of_adapters.cu",
     "of_synth_gpu.cu",
     "of_cnn.cu",
+    "of_batch.cu",
 ]
 SYNTH_SOURCES = ["of_synth.cpp"]
 

@@ -20,7 +20,7 @@
 //   build dT = [Rz(g) Ry(b) Rx(a) | t] and compose T <- dT T in FP64
 //   (ICP.cu:266-305). A singular system restores the frame's starting pose and
 //   stops the remaining iterations (ICP.cpp:152-158).
-#include "of_common.cuh"
+#include "of_batch.cuh"
 
 #include <mutex>
 #include <string.h>
@@ -1055,3 +1055,294 @@ extern "C" of_status_t of_icp_track_static(const of_camera_t *cam, const of_icp_
   if (st != OF_OK) return st;
   return of_icp_launch(cam, ip, d_frame, d_model, pose, ws, stats, (cudaStream_t)stream, nullptr);
 }
+
+// ------------------------------------------------------------ batched ICP --
+//
+// Multi-level ICP of many independent streams in one persistent launch: each
+// thread-block cluster of kBatchCtas CTAs tracks one stream at a time and
+// takes the next stream from an atomic ticket over a longest-first order.
+// Per iteration every CTA associates its share of the level's model pixels
+// (thread g of the cluster takes pixels g, g + kBatchCtas * kBatchThreads,
+// ...), reduces its rows (warp recursive halving, then a tree over warps),
+// and pushes its 30-value row into every CTA's shared memory
+// (double-buffered by iteration parity); after one cluster barrier every CTA
+// sums the kBatchCtas rows in the same order and solves the same 6x6 system,
+// so all hold the same pose. The only waits are hardware cluster barriers.
+// The per-pixel arithmetic (association, inlier tests, rows, FP64 solve and
+// composition) is the single-stream kernel's; the summation order differs.
+#include <cooperative_groups.h>
+
+namespace {
+
+namespace cg = cooperative_groups;
+
+constexpr int kBatchCtas = 8;
+constexpr int kBatchThreads = 512;
+constexpr int kBatchWarps = kBatchThreads / 32;
+
+struct IcpJob {
+  IcpLevel lv[kMaxLevels];
+  int levels;
+  double *pose;
+  of_icp_stats_t *stats;
+};
+
+__global__ void __cluster_dims__(kBatchCtas, 1, 1) __launch_bounds__(kBatchThreads, 1)
+    k_icp_batch(const IcpJob *__restrict__ jobs, const int *__restrict__ order, int njobs,
+                unsigned int *ticket, float dist_thresh, float normal_thresh, float stop_rot,
+                float stop_trans) {
+  __shared__ double s_pose[16], s_init[16];
+  __shared__ Rigid s_c2w, s_w2c;
+  __shared__ float s_red[kBatchWarps][32];
+  __shared__ float s_part[2][kBatchCtas][32];
+  __shared__ float s_tot[32];
+  __shared__ int s_job, s_stop, s_conv, s_its, s_inl;
+  __shared__ double s_res, s_piv;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const float dist2 = dist_thresh * dist_thresh;
+  for (;;) {
+    if (rank == 0 && threadIdx.x == 0) {
+      const unsigned t = atomicAdd(ticket, 1u);
+      const int job = t < (unsigned)njobs ? __ldg(order + t) : -1;
+      for (int r = 0; r < kBatchCtas; ++r) *cluster.map_shared_rank(&s_job, r) = job;
+    }
+    cluster.sync();
+    const int job = s_job;
+    // every CTA has read the job before CTA 0 may hand out the next one
+    cluster.sync();
+    if (job < 0) break;
+    const IcpJob &J = jobs[job];
+    if (threadIdx.x < 16) {
+      s_pose[threadIdx.x] = J.pose[threadIdx.x];
+      s_init[threadIdx.x] = J.pose[threadIdx.x];
+    }
+    if (threadIdx.x == 0) {
+      s_stop = 0; s_conv = 0; s_its = 0; s_inl = 0; s_res = 0.0; s_piv = 0.0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) pose_to_rigid(s_pose, &s_c2w, &s_w2c);
+    __syncthreads();
+    int iter = 0;
+    for (int l = J.levels - 1; l >= 0 && !s_stop; --l) {
+      const IcpLevel L = J.lv[l];
+      const int npx = L.mw * L.mh;
+      if (threadIdx.x == 0) s_conv = 0;
+      __syncthreads();
+      for (int it = 0; it < L.iters; ++it) {
+        float acc[kVals];
+        float examined = 0.f;
+#pragma unroll
+        for (int v = 0; v < kVals; ++v) acc[v] = 0.f;
+        constexpr int kStride = kBatchCtas * kBatchThreads;
+        for (int p = rank * kBatchThreads + threadIdx.x; p < npx; p += 2 * kStride) {
+          const int p2 = p + kStride;
+          const float4 sA = __ldg(L.model + 2 * p), nA = __ldg(L.model + 2 * p + 1);
+          float4 sB = make_float4(0.f, 0.f, 0.f, 0.f), nB = sB;
+          if (p2 < npx) { sB = __ldg(L.model + 2 * p2); nB = __ldg(L.model + 2 * p2 + 1); }
+          const int qA = (sA.w != 0.f && nA.w != 0.f) ? associate(s_w2c, L.cam, sA) : -1;
+          const int qB = (sB.w != 0.f && nB.w != 0.f) ? associate(s_w2c, L.cam, sB) : -1;
+          float4 dA = make_float4(0.f, 0.f, 0.f, 0.f), cA = dA, dB = dA, cB = dA;
+          if (qA >= 0) { dA = __ldg(L.frame + 2 * qA); cA = __ldg(L.frame + 2 * qA + 1); }
+          if (qB >= 0) { dB = __ldg(L.frame + 2 * qB); cB = __ldg(L.frame + 2 * qB + 1); }
+          if (qA >= 0) {
+            examined += 1.f;
+            try_row(acc, s_c2w, sA, nA, dA, cA, dist2, normal_thresh);
+          }
+          if (qB >= 0) {
+            examined += 1.f;
+            try_row(acc, s_c2w, sB, nB, dB, cB, dist2, normal_thresh);
+          }
+        }
+        // this CTA's row: recursive halving across the warp, a tree over warps
+        {
+          float r[32];
+#pragma unroll
+          for (int v = 0; v < 32; ++v) r[v] = v < kVals ? acc[v] : (v == kVals ? examined : 0.f);
+#pragma unroll
+          for (int sft = 16; sft >= 1; sft >>= 1) {
+            const bool upper = (lane & sft) != 0;
+#pragma unroll
+            for (int i = 0; i < sft; ++i) {
+              float send = upper ? r[i] : r[i + sft];
+              float keep = upper ? r[i + sft] : r[i];
+              r[i] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
+            }
+          }
+          s_red[warp][lane] = r[0];
+        }
+        __syncthreads();
+        const int buf = iter & 1;
+        if (warp == 0) {
+          float y[kBatchWarps];
+#pragma unroll
+          for (int w = 0; w < kBatchWarps; ++w) y[w] = s_red[w][lane];
+#pragma unroll
+          for (int span = 1; span < kBatchWarps; span *= 2)
+#pragma unroll
+            for (int w = 0; w + span < kBatchWarps; w += 2 * span) y[w] += y[w + span];
+#pragma unroll
+          for (int r = 0; r < kBatchCtas; ++r) cluster.map_shared_rank(&s_part[buf][rank][0], r)[lane] = y[0];
+        }
+        cluster.sync();
+        if (warp == 0) {
+          float y[kBatchCtas];
+#pragma unroll
+          for (int r = 0; r < kBatchCtas; ++r) y[r] = s_part[buf][r][lane];
+#pragma unroll
+          for (int span = 1; span < kBatchCtas; span *= 2)
+#pragma unroll
+            for (int r = 0; r + span < kBatchCtas; r += 2 * span) y[r] += y[r + span];
+          s_tot[lane] = y[0];
+          __syncwarp();
+          double minpiv = 0.0;
+          float inc_rot = 0.f, inc_trans = 0.f;
+          const bool ok = warp_solve_update(s_tot, s_pose, &minpiv, &inc_rot, &inc_trans);
+          if (lane == 0) {
+            s_its += 1;
+            s_inl = (int)s_tot[28];
+            s_res = (double)s_tot[27];
+            s_piv = minpiv;
+            if (!ok) {
+              for (int i = 0; i < 16; ++i) s_pose[i] = s_init[i];
+              s_stop = 1;
+            } else if (stop_rot > 0.f && inc_rot < stop_rot && inc_trans < stop_trans) {
+              s_conv = 1;
+            }
+            pose_to_rigid(s_pose, &s_c2w, &s_w2c);
+          }
+        }
+        __syncthreads();
+        ++iter;
+        if (s_stop || s_conv) break;
+      }
+    }
+    if (rank == 0 && threadIdx.x == 0) {
+      for (int i = 0; i < 16; ++i) J.pose[i] = s_pose[i];
+      if (J.stats) {
+        J.stats->status = s_stop ? 1 : 0;
+        J.stats->inliers = s_inl;
+        J.stats->iterations = s_its;
+        J.stats->warm = 0;
+        J.stats->residual_sq = s_res;
+        J.stats->min_pivot = s_piv;
+      }
+    }
+  }
+}
+
+}  // namespace
+
+namespace of {
+
+struct IcpBatch {
+  int n = 0;
+  float dist, nthr, stop_rot, stop_trans;
+  IcpJob *jobs = nullptr;
+  int *order = nullptr;
+  unsigned int *ticket = nullptr;
+};
+
+void icp_batch_destroy(IcpBatch *b) {
+  if (!b) return;
+  cudaFree(b->jobs);
+  cudaFree(b->order);
+  cudaFree(b->ticket);
+  delete b;
+}
+
+// Clusters of the batched ICP that fit on the device at once.
+int icp_batch_max_clusters() {
+  static int cached = 0;
+  if (cached > 0) return cached;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(kBatchCtas * kSmCount / kBatchCtas);
+  cfg.blockDim = dim3(kBatchThreads);
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeClusterDimension;
+  attr.val.clusterDim.x = kBatchCtas;
+  attr.val.clusterDim.y = 1;
+  attr.val.clusterDim.z = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, (void *)k_icp_batch, &cfg) != cudaSuccess || n < 1) {
+    cudaGetLastError();
+    n = kSmCount / kBatchCtas;
+  }
+  cached = n;
+  return n;
+}
+
+of_status_t icp_batch_create(const BatchStream *s, int n, const BatchParams &p, IcpBatch **out) {
+  const of_icp_params_t *ip = &p.icp;
+  if (n < 1 || !icp_params_ok(ip)) return OF_ERR_INVALID_ARGUMENT;
+  IcpBatch *b = new IcpBatch();
+  b->n = n;
+  b->dist = ip->dist_thresh_mm;
+  b->nthr = ip->normal_thresh;
+  b->stop_rot = ip->stop_rot_rad;
+  b->stop_trans = ip->stop_trans_mm;
+  IcpJob *jobs = new IcpJob[n];
+  int *order = new int[n + 1];
+  double *cost = new double[n];
+  of_status_t st = OF_OK;
+  for (int i = 0; i < n && st == OF_OK; ++i) {
+    of_pyramid_layout_t lay;
+    st = of_pyramid_layout(&s[i].cam, ip->levels, &lay);
+    memset(&jobs[i], 0, sizeof(IcpJob));
+    jobs[i].levels = ip->levels;
+    jobs[i].pose = s[i].pose;
+    jobs[i].stats = s[i].stats;
+    cost[i] = 0.0;
+    for (int l = 0; l < ip->levels; ++l) {
+      const of_camera_t cl = camera_level(s[i].cam, l);
+      IcpLevel &L = jobs[i].lv[l];
+      L.cam = make_cam(cl);
+      L.frame = (const float4 *)((const char *)s[i].frame + lay.points_offset[l]);
+      L.model = (const float4 *)((const char *)s[i].model + lay.points_offset[l]);
+      L.mw = cl.width;
+      L.mh = cl.height;
+      L.iters = ip->iters[l];
+      cost[i] += (double)cl.width * cl.height * ip->iters[l];
+    }
+  }
+  // longest first (ties by index), so the last streams taken are the shortest
+  for (int i = 0; i < n; ++i) order[i] = i;
+  for (int i = 1; i < n; ++i)
+    for (int k = i; k > 0 && (cost[order[k]] > cost[order[k - 1]] ||
+                              (cost[order[k]] == cost[order[k - 1]] && order[k] < order[k - 1]));
+         --k) {
+      const int t = order[k]; order[k] = order[k - 1]; order[k - 1] = t;
+    }
+  order[n] = 0;
+  if (st == OF_OK) st = upload_jobs(jobs, order, n, &b->jobs, &b->order);
+  if (st == OF_OK) {
+    cudaError_t e = cudaMalloc(&b->ticket, sizeof(unsigned int));
+    if (e != cudaSuccess) st = of_set_cuda_error(e);
+  }
+  delete[] jobs;
+  delete[] order;
+  delete[] cost;
+  if (st != OF_OK) {
+    icp_batch_destroy(b);
+    return st;
+  }
+  *out = b;
+  return OF_OK;
+}
+
+of_status_t icp_batch_launch(const IcpBatch *b, const BatchKnobs &k, cudaStream_t s) {
+  const int maxc = icp_batch_max_clusters();
+  int clusters = k.icp_clusters > 0 ? k.icp_clusters : maxc;
+  if (clusters > maxc) clusters = maxc;
+  if (clusters > b->n) clusters = b->n;
+  OF_CUDA_TRY(cudaMemsetAsync(b->ticket, 0, sizeof(unsigned int), s));
+  k_icp_batch<<<clusters * kBatchCtas, kBatchThreads, 0, s>>>(b->jobs, b->order, b->n, b->ticket,
+                                                            b->dist, b->nthr, b->stop_rot,
+                                                            b->stop_trans);
+  return of_launch_status();
+}
+
+}  // namespace of

@@ -22,7 +22,7 @@
 // The SDF of voxels near the truncation band is evaluated with float-pair
 // arithmetic so that the stored int16 value matches an FP64 evaluation to
 // within one quantisation step.
-#include "of_common.cuh"
+#include "of_batch.cuh"
 
 using namespace of;
 
@@ -132,15 +132,16 @@ __device__ __forceinline__ void load_setup(const FrameSetup *g, FrameSetup *s) {
 // (+inf and 0 if there is none); y carries a minus sign (-0 included) when a
 // pixel of the tile is invalid. L is the same FP32 product the integration
 // compares |p - c| with.
-__global__ void __launch_bounds__(256) k_depth_tiles(Cam cam, const uint16_t *__restrict__ depth,
-                                                     int pitch, const float2 *__restrict__ lam,
-                                                     float2 *__restrict__ tiles, int tiles_x,
-                                                     int ntiles, unsigned int *list_count,
-                                                     const double *__restrict__ pose,
-                                                     of_volume_desc_t desc, FrameSetup *setup) {
-  const int tile = blockIdx.x * 8 + (threadIdx.x >> 5);
+__device__ __forceinline__ void depth_tiles_block(const Cam &cam, const uint16_t *__restrict__ depth,
+                                                  int pitch, const float2 *__restrict__ lam,
+                                                  float2 *__restrict__ tiles, int tiles_x,
+                                                  int ntiles, unsigned int *list_count,
+                                                  const double *__restrict__ pose,
+                                                  const of_volume_desc_t &desc, FrameSetup *setup,
+                                                  int bx) {
+  const int tile = bx * 8 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (bx == 0 && threadIdx.x == 0) {
     // for the next two steps: an empty work list, the frame's setup
     *list_count = 0;
     make_setup(pose, desc, setup->S);
@@ -172,6 +173,15 @@ __global__ void __launch_bounds__(256) k_depth_tiles(Cam cam, const uint16_t *__
     lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
   }
   if (lane == 0) tiles[tile] = make_float2(lmin, all_valid ? lmax : -lmax);
+}
+__global__ void __launch_bounds__(256) k_depth_tiles(Cam cam, const uint16_t *__restrict__ depth,
+                                                     int pitch, const float2 *__restrict__ lam,
+                                                     float2 *__restrict__ tiles, int tiles_x,
+                                                     int ntiles, unsigned int *list_count,
+                                                     const double *__restrict__ pose,
+                                                     of_volume_desc_t desc, FrameSetup *setup) {
+  depth_tiles_block(cam, depth, pitch, lam, tiles, tiles_x, ntiles, list_count, pose, desc, setup,
+                    blockIdx.x);
 }
 
 // Whole-brick decision from the tile bounds (one thread per brick). Returns
@@ -521,12 +531,11 @@ __global__ void __launch_bounds__(256, 4) k_integrate(uint32_t *__restrict__ vol
 // whole-brick decision from the tile bounds; kept bricks are appended to the
 // work list (one atomic per warp) as {bx | by << 8 | bz << 16 | mode << 24,
 // camera-space base of the brick (3 floats)}.
-__global__ void __launch_bounds__(256) k_classify_bricks(of_volume_desc_t desc, Cam cam,
-                                                         const double *__restrict__ pose,
-                                                         const float2 *__restrict__ tiles,
-                                                         int tiles_x, uint4 *__restrict__ list,
-                                                         unsigned int *__restrict__ list_count,
-                                                         const FrameSetup *__restrict__ setup) {
+__device__ __forceinline__ void classify_block(const of_volume_desc_t &desc, const Cam &cam,
+                                               const float2 *__restrict__ tiles, int tiles_x,
+                                               uint4 *__restrict__ list,
+                                               unsigned int *__restrict__ list_count,
+                                               const FrameSetup *__restrict__ setup, int bx) {
   __shared__ FrameSetup F;
   load_setup(setup, &F);
   const IntegrateSetup &S = F.S;
@@ -534,7 +543,7 @@ __global__ void __launch_bounds__(256) k_classify_bricks(of_volume_desc_t desc, 
   const int nb = desc.resolution >> 3;
   const int nbricks = nb * nb * nb;
   const int lane = threadIdx.x & 31;
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = bx * blockDim.x + threadIdx.x;
   const float vs = S.vs_hi;
   const float org = -0.5f * desc.size_mm;
   const float hext = 3.5f * vs + 1e-3f;
@@ -572,18 +581,26 @@ __global__ void __launch_bounds__(256) k_classify_bricks(of_volume_desc_t desc, 
     if (keep) list[base + __popc(m & ((1u << lane) - 1u))] = entry;
   }
 }
+__global__ void __launch_bounds__(256) k_classify_bricks(of_volume_desc_t desc, Cam cam,
+                                                         const double *__restrict__ pose,
+                                                         const float2 *__restrict__ tiles,
+                                                         int tiles_x, uint4 *__restrict__ list,
+                                                         unsigned int *__restrict__ list_count,
+                                                         const FrameSetup *__restrict__ setup) {
+  classify_block(desc, cam, tiles, tiles_x, list, list_count, setup, blockIdx.x);
+}
 
 // of_integrate_tiled, step 3: persistent grid over the work list, each
 // 128-thread half of a CTA takes one listed brick at a time.
 template <int STORAGE>
-__global__ void __launch_bounds__(256, 4) k_integrate_list(uint32_t *__restrict__ vol,
-                                                        of_volume_desc_t desc, Cam cam,
-                                                        const uint16_t *__restrict__ depth,
-                                                        int pitch, const double *__restrict__ pose,
-                                                        const float2 *__restrict__ lam,
-                                                        const uint4 *__restrict__ list,
-                                                        const unsigned int *__restrict__ list_count,
-                                                        const FrameSetup *__restrict__ setup) {
+__device__ __forceinline__ void integrate_list_block(uint32_t *__restrict__ vol,
+                                                     const of_volume_desc_t &desc, const Cam &cam,
+                                                     const uint16_t *__restrict__ depth, int pitch,
+                                                     const float2 *__restrict__ lam,
+                                                     const uint4 *__restrict__ list,
+                                                     const unsigned int *__restrict__ list_count,
+                                                     const FrameSetup *__restrict__ setup, int bx,
+                                                     int gx) {
   __shared__ FrameSetup F;
   load_setup(setup, &F);
   const IntegrateSetup &S = F.S;
@@ -595,7 +612,7 @@ __global__ void __launch_bounds__(256, 4) k_integrate_list(uint32_t *__restrict_
   const int nb = K.nb;
   uint8_t *flags = brick_flags(vol, desc.resolution);
   unsigned my_count = 0;
-  for (int e = blockIdx.x * 2 + half; e < n; e += gridDim.x * 2) {
+  for (int e = bx * 2 + half; e < n; e += gx * 2) {
     const uint4 en = __ldg(list + e);
     const int bx = (int)(en.x & 0xffu), by = (int)((en.x >> 8) & 0xffu);
     const int bz = (int)((en.x >> 16) & 0xffu), mode = (int)(en.x >> 24);
@@ -604,6 +621,18 @@ __global__ void __launch_bounds__(256, 4) k_integrate_list(uint32_t *__restrict_
         vol, flags, desc, cam, depth, pitch, lam, S, K, t, lane, b, bx, by, bz, mode,
         make_float3(__uint_as_float(en.y), __uint_as_float(en.z), __uint_as_float(en.w)), my_count);
   }
+}
+template <int STORAGE>
+__global__ void __launch_bounds__(256, 4) k_integrate_list(uint32_t *__restrict__ vol,
+                                                        of_volume_desc_t desc, Cam cam,
+                                                        const uint16_t *__restrict__ depth,
+                                                        int pitch, const double *__restrict__ pose,
+                                                        const float2 *__restrict__ lam,
+                                                        const uint4 *__restrict__ list,
+                                                        const unsigned int *__restrict__ list_count,
+                                                        const FrameSetup *__restrict__ setup) {
+  integrate_list_block<STORAGE>(vol, desc, cam, depth, pitch, lam, list, list_count, setup,
+                                blockIdx.x, gridDim.x);
 }
 
 int tiles_x_of(const of_camera_t *cam) { return (cam->width + kTile - 1) / kTile; }
@@ -678,7 +707,159 @@ of_status_t launch_integrate_tiled(const of_volume_desc_t *d, void *vol, const o
   return of_launch_status();
 }
 
+// ---------------------------------------------------------------- batched --
+// One stream of the batched of_integrate_tiled: its three steps run as three
+// launches over all streams.
+struct IntJob {
+  uint32_t *vol;
+  of_volume_desc_t desc;
+  Cam cam;
+  const uint16_t *depth[2];
+  int pitch;
+  const double *pose;
+  const float2 *lam;
+  float2 *tiles;
+  uint4 *list;
+  unsigned int *count;
+  FrameSetup *setup;
+  int tiles_x, ntiles;
+};
+
+__global__ void __launch_bounds__(256) k_depth_tiles_batch(const IntJob *__restrict__ jobs,
+                                                           const int *__restrict__ first, int n,
+                                                           int parity) {
+  const int j = batch_job(first, n, blockIdx.x);
+  const IntJob &J = jobs[j];
+  depth_tiles_block(J.cam, J.depth[parity], J.pitch, J.lam, J.tiles, J.tiles_x, J.ntiles, J.count,
+                    J.pose, J.desc, J.setup, blockIdx.x - __ldg(first + j));
+}
+__global__ void __launch_bounds__(256) k_classify_batch(const IntJob *__restrict__ jobs,
+                                                        const int *__restrict__ first, int n) {
+  const int j = batch_job(first, n, blockIdx.x);
+  const IntJob &J = jobs[j];
+  classify_block(J.desc, J.cam, J.tiles, J.tiles_x, J.list, J.count, J.setup,
+                 blockIdx.x - __ldg(first + j));
+}
+template <int STORAGE>
+__global__ void __launch_bounds__(256, 4) k_integrate_list_batch(const IntJob *__restrict__ jobs,
+                                                              const int *__restrict__ first, int n,
+                                                              int parity) {
+  const int j = batch_job(first, n, blockIdx.x);
+  const IntJob &J = jobs[j];
+  const int b0 = __ldg(first + j);
+  integrate_list_block<STORAGE>(J.vol, J.desc, J.cam, J.depth[parity], J.pitch, J.lam, J.list,
+                                J.count, J.setup, blockIdx.x - b0, __ldg(first + j + 1) - b0);
+}
+
+// list_div candidates of the batched integration (blocks per stream =
+// ceil(bricks / list_div), at most the single-stream persistent grid)
+constexpr int kListDivs[] = {16, 32, 64, 128, 256};
+constexpr int kNumListDivs = (int)(sizeof(kListDivs) / sizeof(kListDivs[0]));
+
 }  // namespace
+
+namespace of {
+
+struct IntegrateBatch {
+  int n = 0, storage = OF_TSDF_I16;
+  IntJob *jobs = nullptr;
+  int *tiles_first = nullptr, tiles_blocks = 0;
+  int *classify_first = nullptr, classify_blocks = 0;
+  int *list_first[kNumListDivs] = {}, list_blocks[kNumListDivs] = {};
+};
+
+void integrate_batch_destroy(IntegrateBatch *b) {
+  if (!b) return;
+  cudaFree(b->jobs);
+  cudaFree(b->tiles_first);
+  cudaFree(b->classify_first);
+  for (int i = 0; i < kNumListDivs; ++i) cudaFree(b->list_first[i]);
+  delete b;
+}
+
+int integrate_list_div(int knob) { return kListDivs[knob < 0 ? 0 : knob % kNumListDivs]; }
+
+of_status_t integrate_batch_create(const BatchStream *s, int n, IntegrateBatch **out) {
+  if (n < 1) return OF_ERR_INVALID_ARGUMENT;
+  for (int i = 0; i < n; ++i)
+    if (s[i].vol_desc.storage != s[0].vol_desc.storage || !s[i].scratch ||
+        ((uintptr_t)s[i].scratch & 255u))
+      return OF_ERR_INVALID_ARGUMENT;
+  IntegrateBatch *b = new IntegrateBatch();
+  b->n = n;
+  b->storage = s[0].vol_desc.storage;
+  IntJob *jobs = new IntJob[n];
+  int *ft = new int[n + 1], *fc = new int[n + 1], *fl = new int[n + 1];
+  ft[0] = fc[0] = 0;
+  for (int i = 0; i < n; ++i) {
+    const ScratchLayout L = scratch_layout(&s[i].vol_desc, &s[i].cam);
+    char *sc = (char *)s[i].scratch;
+    IntJob &J = jobs[i];
+    J.vol = (uint32_t *)s[i].volume;
+    J.desc = s[i].vol_desc;
+    J.cam = make_cam(s[i].cam);
+    J.depth[0] = s[i].depth[0];
+    J.depth[1] = s[i].depth[1];
+    J.pitch = s[i].cam.width;
+    J.pose = s[i].pose;
+    J.lam = (const float2 *)s[i].lambda;
+    J.tiles = (float2 *)(sc + L.tiles);
+    J.list = (uint4 *)(sc + L.list);
+    J.count = (unsigned int *)sc;
+    J.setup = (FrameSetup *)(sc + L.setup);
+    J.tiles_x = tiles_x_of(&s[i].cam);
+    J.ntiles = tiles_of(&s[i].cam);
+    const int nb = s[i].vol_desc.resolution / 8;
+    ft[i + 1] = ft[i] + (J.ntiles + 7) / 8;
+    fc[i + 1] = fc[i] + (nb * nb * nb + 255) / 256;
+  }
+  b->tiles_blocks = ft[n];
+  b->classify_blocks = fc[n];
+  of_status_t st = upload_jobs(jobs, ft, n, &b->jobs, &b->tiles_first);
+  IntJob *tmp = nullptr;
+  if (st == OF_OK) {
+    st = upload_jobs(jobs, fc, n, &tmp, &b->classify_first);
+    cudaFree(tmp);
+  }
+  for (int k = 0; k < kNumListDivs && st == OF_OK; ++k) {
+    fl[0] = 0;
+    for (int i = 0; i < n; ++i) {
+      const size_t nb = (size_t)(s[i].vol_desc.resolution / 8);
+      const size_t want = (nb * nb * nb + kListDivs[k] - 1) / kListDivs[k];
+      const size_t cap = persistent_blocks(&s[i].vol_desc);
+      fl[i + 1] = fl[i] + (int)(want < cap ? want : cap);
+    }
+    b->list_blocks[k] = fl[n];
+    st = upload_jobs(jobs, fl, n, &tmp, &b->list_first[k]);
+    cudaFree(tmp);
+  }
+  delete[] jobs;
+  delete[] ft;
+  delete[] fc;
+  delete[] fl;
+  if (st != OF_OK) {
+    integrate_batch_destroy(b);
+    return st;
+  }
+  *out = b;
+  return OF_OK;
+}
+
+of_status_t integrate_batch_launch(const IntegrateBatch *b, int parity, const BatchKnobs &k,
+                                   cudaStream_t s) {
+  const int d = k.list_div < 0 ? 0 : k.list_div % kNumListDivs;
+  k_depth_tiles_batch<<<b->tiles_blocks, 256, 0, s>>>(b->jobs, b->tiles_first, b->n, parity);
+  k_classify_batch<<<b->classify_blocks, 256, 0, s>>>(b->jobs, b->classify_first, b->n);
+  if (b->storage == OF_TSDF_I16)
+    k_integrate_list_batch<OF_TSDF_I16><<<b->list_blocks[d], 256, 0, s>>>(b->jobs, b->list_first[d],
+                                                                        b->n, parity);
+  else
+    k_integrate_list_batch<OF_TSDF_F16><<<b->list_blocks[d], 256, 0, s>>>(b->jobs, b->list_first[d],
+                                                                        b->n, parity);
+  return of_launch_status();
+}
+
+}  // namespace of
 
 extern "C" of_status_t of_integrate(const of_volume_desc_t *d, void *vol, const of_camera_t *cam,
                                     const uint16_t *depth, int32_t pitch, const double *pose,

@@ -9,7 +9,7 @@
 // row/column, where a neighbour is invalid, or where the cross product is zero.
 // The world transform the reference applies at every ICP iteration
 // (ICP.cpp:174) is applied on the fly inside the ICP kernel instead.
-#include "of_common.cuh"
+#include "of_batch.cuh"
 
 using namespace of;
 
@@ -81,15 +81,16 @@ __device__ __forceinline__ float ex2_approx(float x) {
 // Invalid depths are stored as -1e30 in the tile: their squared range
 // difference overflows to +inf and their weight 2^-inf is exactly 0, so no
 // per-tap select is needed. One ex2 per tap.
+// (tile (bx, by) of the image; the kernels below pass their block index)
 template <int R>
-__global__ void __launch_bounds__(256) k_bilateral_r(const uint16_t *__restrict__ depth, int pitch,
-                                                     int w, int h, float dmin, float dmax,
-                                                     float ks, float kr, float *__restrict__ out) {
+__device__ __forceinline__ void bilateral_tile(const uint16_t *__restrict__ depth, int pitch,
+                                               int w, int h, float dmin, float dmax, float ks,
+                                               float kr, float *__restrict__ out, int bx, int by) {
   constexpr int TW = kTileX + 2 * R;
   constexpr int TH = kTileY + 2 * R;
   __shared__ float tile[TH * TW];
-  const int x0 = blockIdx.x * kTileX - R;
-  const int y0 = blockIdx.y * kTileY - R;
+  const int x0 = bx * kTileX - R;
+  const int y0 = by * kTileY - R;
   for (int i = threadIdx.x; i < TW * TH; i += blockDim.x) {
     int tx = i % TW, ty = i / TW;
     int gx = x0 + tx, gy = y0 + ty;
@@ -102,7 +103,7 @@ __global__ void __launch_bounds__(256) k_bilateral_r(const uint16_t *__restrict_
   }
   __syncthreads();
   const int lx = threadIdx.x % kTileX, ly = threadIdx.x / kTileX;
-  const int x = blockIdx.x * kTileX + lx, y = blockIdx.y * kTileY + ly;
+  const int x = bx * kTileX + lx, y = by * kTileY + ly;
   if (x >= w || y >= h) return;
   const float *ctr = tile + (ly + R) * TW + lx + R;
   const float c = *ctr;
@@ -128,24 +129,37 @@ __global__ void __launch_bounds__(256) k_bilateral_r(const uint16_t *__restrict_
   out[(size_t)y * w + x] = result;
 }
 
+template <int R>
+__global__ void __launch_bounds__(256) k_bilateral_r(const uint16_t *__restrict__ depth, int pitch,
+                                                     int w, int h, float dmin, float dmax,
+                                                     float ks, float kr, float *__restrict__ out) {
+  bilateral_tile<R>(depth, pitch, w, h, dmin, dmax, ks, kr, out, blockIdx.x, blockIdx.y);
+}
+
 // No filter: the raw depth as float, invalid -> 0 (the reference converts the
 // raw depth, CameraHandler.cu:65-89).
-__global__ void k_depth_raw(const uint16_t *__restrict__ depth, int pitch, int w, int h,
-                            float dmin, float dmax, float *__restrict__ out) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x;
-  int y = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void depth_raw_tile(const uint16_t *__restrict__ depth, int pitch,
+                                               int w, int h, float dmin, float dmax,
+                                               float *__restrict__ out, int bx, int by) {
+  int x = bx * blockDim.x + threadIdx.x;
+  int y = by * blockDim.y + threadIdx.y;
   if (x >= w || y >= h) return;
   float d = (float)depth[(size_t)y * pitch + x];
   out[(size_t)y * w + x] = depth_valid(d, dmin, dmax) ? d : 0.f;
+}
+__global__ void k_depth_raw(const uint16_t *__restrict__ depth, int pitch, int w, int h,
+                            float dmin, float dmax, float *__restrict__ out) {
+  depth_raw_tile(depth, pitch, w, h, dmin, dmax, out, blockIdx.x, blockIdx.y);
 }
 
 // Level l -> l+1: pixel (x, y) averages the valid pixels of the 2x2 block
 // {2x, 2x+1} x {2y, 2y+1} that lie within 3 sigma_r of the block's first
 // valid pixel (row-major order); 0 if the block has none.
-__global__ void k_pyr_down(const float *__restrict__ src, int sw, int sh, float *__restrict__ dst,
-                           int dw, int dh, float guard) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x;
-  int y = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void pyr_down_tile(const float *__restrict__ src, int sw, int sh,
+                                              float *__restrict__ dst, int dw, int dh, float guard,
+                                              int bx, int by) {
+  int x = bx * blockDim.x + threadIdx.x;
+  int y = by * blockDim.y + threadIdx.y;
   if (x >= dw || y >= dh) return;
   float ref = 0.f, sum = 0.f;
   int cnt = 0;
@@ -167,14 +181,19 @@ __global__ void k_pyr_down(const float *__restrict__ src, int sw, int sh, float 
     }
   dst[(size_t)y * dw + x] = cnt ? sum / (float)cnt : 0.f;
 }
+__global__ void k_pyr_down(const float *__restrict__ src, int sw, int sh, float *__restrict__ dst,
+                           int dw, int dh, float guard) {
+  pyr_down_tile(src, sw, sh, dst, dw, dh, guard, blockIdx.x, blockIdx.y);
+}
 
 // Camera-space vertex and normal of every pixel of one level. Differences
 // of neighbouring vertices are formed from depth differences (no
 // cancellation between large coordinates).
-__global__ void k_vertex_normal(const float *__restrict__ depth, int w, int h, float cx, float cy,
-                                float ifx, float ify, float4 *__restrict__ pts) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x;
-  int y = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void vertex_normal_tile(const float *__restrict__ depth, int w, int h,
+                                                   float cx, float cy, float ifx, float ify,
+                                                   float4 *__restrict__ pts, int bx, int by) {
+  int x = bx * blockDim.x + threadIdx.x;
+  int y = by * blockDim.y + threadIdx.y;
   if (x >= w || y >= h) return;
   size_t p = (size_t)y * w + x;
   float d = depth[p];
@@ -203,8 +222,209 @@ __global__ void k_vertex_normal(const float *__restrict__ depth, int w, int h, f
   pts[2 * p] = v;
   pts[2 * p + 1] = n;
 }
+__global__ void k_vertex_normal(const float *__restrict__ depth, int w, int h, float cx, float cy,
+                                float ifx, float ify, float4 *__restrict__ pts) {
+  vertex_normal_tile(depth, w, h, cx, cy, ifx, ify, pts, blockIdx.x, blockIdx.y);
+}
+
+// ---------------------------------------------------------------- batched --
+// Jobs of the batched launches (one per stream, or per stream and level);
+// gx = tiles per image row.
+struct FilterJob {
+  const uint16_t *depth[2];
+  int pitch, w, h, gx;
+  float dmin, dmax;
+  float *out;
+};
+struct PyrJob {
+  const float *src;
+  float *dst;
+  int sw, sh, dw, dh, gx;
+};
+struct VnJob {
+  const float *depth;
+  float4 *pts;
+  int w, h, gx;
+  float cx, cy, ifx, ify;
+};
+
+template <int R>
+__global__ void __launch_bounds__(256) k_bilateral_batch(const FilterJob *__restrict__ jobs,
+                                                         const int *__restrict__ first, int n,
+                                                         int parity, float ks, float kr) {
+  const int j = batch_job(first, n, blockIdx.x);
+  const FilterJob &J = jobs[j];
+  const int b = blockIdx.x - __ldg(first + j);
+  bilateral_tile<R>(J.depth[parity], J.pitch, J.w, J.h, J.dmin, J.dmax, ks, kr, J.out, b % J.gx,
+                    b / J.gx);
+}
+__global__ void k_depth_raw_batch(const FilterJob *__restrict__ jobs, const int *__restrict__ first,
+                                  int n, int parity) {
+  const int j = batch_job(first, n, blockIdx.x);
+  const FilterJob &J = jobs[j];
+  const int b = blockIdx.x - __ldg(first + j);
+  depth_raw_tile(J.depth[parity], J.pitch, J.w, J.h, J.dmin, J.dmax, J.out, b % J.gx, b / J.gx);
+}
+__global__ void k_pyr_down_batch(const PyrJob *__restrict__ jobs, const int *__restrict__ first,
+                                 int n, float guard) {
+  const int j = batch_job(first, n, blockIdx.x);
+  const PyrJob &J = jobs[j];
+  const int b = blockIdx.x - __ldg(first + j);
+  pyr_down_tile(J.src, J.sw, J.sh, J.dst, J.dw, J.dh, guard, b % J.gx, b / J.gx);
+}
+__global__ void k_vertex_normal_batch(const VnJob *__restrict__ jobs, const int *__restrict__ first,
+                                      int n) {
+  const int j = batch_job(first, n, blockIdx.x);
+  const VnJob &J = jobs[j];
+  const int b = blockIdx.x - __ldg(first + j);
+  vertex_normal_tile(J.depth, J.w, J.h, J.cx, J.cy, J.ifx, J.ify, J.pts, b % J.gx, b / J.gx);
+}
+
+int filter_radius(const of_filter_params_t *fp) {
+  return fp->radius_px > 0 ? fp->radius_px : (int)ceilf(2.0f * fp->sigma_space_px);
+}
 
 }  // namespace
+
+namespace of {
+
+// Level-0 filter of every stream in one launch, then one launch per pyramid
+// level, then the vertex/normal maps of every (stream, level) in one launch.
+struct PreprocessBatch {
+  int n = 0, levels = 0, radius = 0;
+  float ks = 0.f, kr = 0.f, guard = 0.f;
+  FilterJob *filter = nullptr;
+  int *filter_first = nullptr, filter_blocks = 0;
+  PyrJob *pyr[kMaxLevels] = {};
+  int *pyr_first[kMaxLevels] = {}, pyr_blocks[kMaxLevels] = {};
+  VnJob *vn = nullptr;
+  int *vn_first = nullptr, vn_jobs = 0, vn_blocks = 0;
+};
+
+void preprocess_batch_destroy(PreprocessBatch *b) {
+  if (!b) return;
+  cudaFree(b->filter);
+  cudaFree(b->filter_first);
+  for (int l = 0; l < kMaxLevels; ++l) {
+    cudaFree(b->pyr[l]);
+    cudaFree(b->pyr_first[l]);
+  }
+  cudaFree(b->vn);
+  cudaFree(b->vn_first);
+  delete b;
+}
+
+of_status_t preprocess_batch_create(const BatchStream *s, int n, const BatchParams &p,
+                                    PreprocessBatch **out) {
+  const of_filter_params_t *fp = &p.filter;
+  if (n < 1 || fp->levels < 1 || fp->levels > kMaxLevels || fp->sigma_space_px <= 0.f ||
+      fp->sigma_range_mm <= 0.f || fp->radius_px < -1)
+    return OF_ERR_INVALID_ARGUMENT;
+  const int R = filter_radius(fp);
+  const bool raw = fp->radius_px == -1;
+  if (!raw && !(R >= 3 && R <= 10) && R != 12) return OF_ERR_INVALID_ARGUMENT;
+  PreprocessBatch *b = new PreprocessBatch();
+  b->n = n;
+  b->levels = fp->levels;
+  b->radius = raw ? -1 : R;
+  const double log2e = 1.4426950408889634;
+  b->ks = (float)(log2e / (2.0 * (double)fp->sigma_space_px * fp->sigma_space_px));
+  b->kr = (float)(log2e / (2.0 * (double)fp->sigma_range_mm * fp->sigma_range_mm));
+  b->guard = 3.0f * fp->sigma_range_mm;
+  FilterJob *fj = new FilterJob[n];
+  PyrJob *pj = new PyrJob[n];
+  VnJob *vj = new VnJob[(size_t)n * fp->levels];
+  int *first = new int[(size_t)n * fp->levels + 1];
+  of_status_t st = OF_OK;
+  // level-0 filter (32x8 tiles either way)
+  first[0] = 0;
+  for (int i = 0; i < n && st == OF_OK; ++i) {
+    of_pyramid_layout_t lay;
+    st = of_pyramid_layout(&s[i].cam, fp->levels, &lay);
+    const int w = s[i].cam.width, h = s[i].cam.height;
+    fj[i] = {{s[i].depth[0], s[i].depth[1]}, w, w, h, (w + kTileX - 1) / kTileX,
+             s[i].cam.min_depth_mm, s[i].cam.max_depth_mm,
+             (float *)((char *)s[i].frame + lay.depth_offset[0])};
+    first[i + 1] = first[i] + fj[i].gx * ((h + kTileY - 1) / kTileY);
+  }
+  if (st == OF_OK) {
+    b->filter_blocks = first[n];
+    st = upload_jobs(fj, first, n, &b->filter, &b->filter_first);
+  }
+  for (int l = 1; l < fp->levels && st == OF_OK; ++l) {
+    first[0] = 0;
+    for (int i = 0; i < n; ++i) {
+      of_pyramid_layout_t lay;
+      of_pyramid_layout(&s[i].cam, fp->levels, &lay);
+      char *base = (char *)s[i].frame;
+      pj[i] = {(const float *)(base + lay.depth_offset[l - 1]), (float *)(base + lay.depth_offset[l]),
+               lay.width[l - 1], lay.height[l - 1], lay.width[l], lay.height[l],
+               (lay.width[l] + 31) / 32};
+      first[i + 1] = first[i] + pj[i].gx * ((lay.height[l] + 7) / 8);
+    }
+    b->pyr_blocks[l] = first[n];
+    st = upload_jobs(pj, first, n, &b->pyr[l], &b->pyr_first[l]);
+  }
+  if (st == OF_OK) {
+    int k = 0;
+    first[0] = 0;
+    for (int i = 0; i < n; ++i) {
+      of_pyramid_layout_t lay;
+      of_pyramid_layout(&s[i].cam, fp->levels, &lay);
+      char *base = (char *)s[i].frame;
+      for (int l = 0; l < fp->levels; ++l, ++k) {
+        const of_camera_t c = camera_level(s[i].cam, l);
+        vj[k] = {(const float *)(base + lay.depth_offset[l]), (float4 *)(base + lay.points_offset[l]),
+                 c.width, c.height, (c.width + 31) / 32, c.cx, c.cy,
+                 (float)(1.0 / (double)c.fx), (float)(1.0 / (double)c.fy)};
+        first[k + 1] = first[k] + vj[k].gx * ((c.height + 7) / 8);
+      }
+    }
+    b->vn_jobs = k;
+    b->vn_blocks = first[k];
+    st = upload_jobs(vj, first, k, &b->vn, &b->vn_first);
+  }
+  delete[] fj;
+  delete[] pj;
+  delete[] vj;
+  delete[] first;
+  if (st != OF_OK) {
+    preprocess_batch_destroy(b);
+    return st;
+  }
+  *out = b;
+  return OF_OK;
+}
+
+of_status_t preprocess_batch_launch(const PreprocessBatch *b, int parity, cudaStream_t s) {
+  if (b->radius < 0) {
+    k_depth_raw_batch<<<b->filter_blocks, dim3(32, 8), 0, s>>>(b->filter, b->filter_first, b->n,
+                                                               parity);
+  } else {
+#define OF_BILATERAL_BATCH(RR)                                                                 case RR:                                                                                       k_bilateral_batch<RR><<<b->filter_blocks, kTileX * kTileY, 0, s>>>(                              b->filter, b->filter_first, b->n, parity, b->ks, b->kr);                                 break;
+    switch (b->radius) {
+      OF_BILATERAL_BATCH(3)
+      OF_BILATERAL_BATCH(4)
+      OF_BILATERAL_BATCH(5)
+      OF_BILATERAL_BATCH(6)
+      OF_BILATERAL_BATCH(7)
+      OF_BILATERAL_BATCH(8)
+      OF_BILATERAL_BATCH(9)
+      OF_BILATERAL_BATCH(10)
+      OF_BILATERAL_BATCH(12)
+      default:
+        return OF_ERR_INVALID_ARGUMENT;
+    }
+#undef OF_BILATERAL_BATCH
+  }
+  for (int l = 1; l < b->levels; ++l)
+    k_pyr_down_batch<<<b->pyr_blocks[l], dim3(32, 8), 0, s>>>(b->pyr[l], b->pyr_first[l], b->n,
+                                                              b->guard);
+  k_vertex_normal_batch<<<b->vn_blocks, dim3(32, 8), 0, s>>>(b->vn, b->vn_first, b->vn_jobs);
+  return of_launch_status();
+}
+
+}  // namespace of
 
 extern "C" of_status_t of_preprocess(const of_camera_t *cam, const of_filter_params_t *fp,
                                      const uint16_t *d_depth, int32_t pitch, void *d_frame,
