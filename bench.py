@@ -19,6 +19,11 @@ path (weak scaling); timing is the max over ranks.
 large-motion workload (same frames, same early exit, device-timed frames/s,
 ICP iterations and per-frame pose error against the ground truth).
 
+`batched_streams` runs 64 independent streams of mixed resolution and volume
+(the batched-streams workload) through one Batch (one launch per stage, one
+graph per step, knobs tuned online) and, beside it, through one single-stream
+tracker per stream; with N GPUs the streams are sharded longest-first.
+
 `--impl reference` runs the CPU implementation of the same equations (the
 FP32 OpenMP build of the oracle restatement) on the host cores.
 """
@@ -53,6 +58,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--warm-frames", type=int, default=121,
                     help="frames of the warm-start comparison (0 = skip it)")
+    ap.add_argument("--c4-streams", type=int, default=64,
+                    help="streams of the batched-streams measurement (0 = skip it)")
+    ap.add_argument("--c4-frames", type=int, default=32, help="rendered frames per stream")
+    ap.add_argument("--c4-steps", type=int, default=40, help="timed steps of the batch")
     return ap.parse_args()
 
 
@@ -298,6 +307,8 @@ def run_ours(args, cfg, world, rank, local):
 
     # ---- the learned warm start against plain ICP (large-motion workload)
     warm = warm_start_comparison(of, args, dev, world, rank) if args.warm_frames > 1 else None
+    # ---- many independent streams batched
+    batched = batched_streams(of, args, dev, world, rank) if args.c4_streams > 0 else None
 
     fps = world * args.steps / (ms_max / 1e3)
     e2e_fps = world * args.steps / (e2e_ms / 1e3)
@@ -341,6 +352,8 @@ def run_ours(args, cfg, world, rank, local):
     }
     if warm is not None:
         line["warm_start"] = warm
+    if batched is not None:
+        line["batched_streams"] = batched
     if world == 1 and not args.no_cpu_baseline:
         cps, n, dt, cores = cpu_frames_per_s(cfg, seq, args.cpu_seconds)
         line["cpu_baseline"] = {"value": cps, "unit": "frames/s", "cores": cores, "kind": "port",
@@ -379,6 +392,89 @@ def warm_start_comparison(of, args, dev, world, rank):
         if arm == "warm":
             out[arm]["warm_start_kept_frac"] = float(np.mean(kept == 1))
     out["warm_over_plain_frames_per_s"] = out["warm"]["frames_per_s"] / out["plain"]["frames_per_s"]
+    return out
+
+
+def batched_streams(of, args, dev, world, rank):
+    """The batched-streams workload: 64 independent seeded streams of mixed
+    resolution and volume (c4_configs), sharded over the ranks longest-first,
+    one frame of every stream per step through one Batch (one launch per
+    stage, CUDA graph per step, knobs tuned online during the warm-up).
+    Beside it: the same streams through one single-stream Tracker each, run
+    one after another on the same device (the per-stream path). Device time,
+    max over ranks; frames/s counts every stream's frames."""
+    import torch
+    from openfusion_b200 import learned
+    cfgs = of.c4_configs(count=args.c4_streams, frames=args.c4_frames)
+    plan = of.shard([of.stream_cost(c) for c in cfgs], world)
+    mine = [c for c, r in zip(cfgs, plan) if r == rank]
+    seqs = []
+    for c in mine:
+        scene = of.make_scene(c.scene_kind, c.seed, c.size_mm)
+        poses = of.make_trajectory(c.motion, c.seed + 1, c.size_mm, c.frames)
+        seqs.append((poses, learned.render_device(c, scene, poses, device=dev)))
+    n_seq = args.c4_frames
+    tune_steps = 30
+    warm = max(args.warmup, tune_steps)
+    total = 1 + warm + args.c4_steps
+    order = [frame_index(i, n_seq) for i in range(total)]
+    stream = torch.cuda.current_stream(dev)
+    out = {"workload": f"c4: {args.c4_streams} streams, resolution U{{160x120, 320x240, 640x480}}, "
+                       "volume U{128^3, 256^3, 512^3} over U[2, 3] m, seeded rooms; one frame of "
+                       "every stream per step",
+           "streams": args.c4_streams, "streams_this_rank": len(mine), "steps": args.c4_steps,
+           "data": "synthetic (device renderer)", "parallelism": f"shard{world}"}
+    # ---- batched
+    batch = of.Batch(mine, [p[0] for p, _ in seqs], use_graph=True, tune=True)
+    for i in range(1 + warm):
+        batch.process([d[order[i]] for _, d in seqs])
+    torch.cuda.synchronize()
+    tun = batch.tuning()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for i in range(1 + warm, total):
+        batch.process([d[order[i]] for _, d in seqs])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    P = batch.poses()
+    err = [pose_errors([P[k]], [seqs[k][0][order[-1]]]) for k in range(len(mine))]
+    launches = batch.buffers(0).kernels_track
+    batch.close()
+    del batch
+    torch.cuda.empty_cache()
+    # ---- the same streams, one single-stream tracker each
+    trackers = [of.Tracker(c, p[0], use_graph=True, pose_history=8) for c, (p, _) in zip(mine, seqs)]
+    for i in range(1 + warm):
+        for t, (_, d) in zip(trackers, seqs):
+            t.process(d[order[i]])
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for i in range(1 + warm, total):
+        for t, (_, d) in zip(trackers, seqs):
+            t.process(d[order[i]])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_seq = max_over_ranks(e0.elapsed_time(e1), world)
+    for t in trackers:
+        t.close()
+    del trackers
+    torch.cuda.empty_cache()
+    frames = args.c4_streams * args.c4_steps
+    out.update({
+        "frames_per_s": frames / (ms / 1e3), "ms_per_step": ms / args.c4_steps,
+        "single_stream_trackers_frames_per_s": frames / (ms_seq / 1e3),
+        "batched_over_single_stream": ms_seq / ms,
+        "gpu_launches_per_step": launches,
+        "tuning": {"ray_tile": int(tun.ray_tile), "list_div": int(tun.list_div),
+                   "icp_clusters": int(tun.icp_clusters), "tuned": int(tun.tuned)},
+        "max_rot_err_deg_last_step": float(np.degrees(max(e[0][0] for e in err))),
+        "max_trans_err_mm_last_step": float(max(e[1][0] for e in err)),
+    })
     return out
 
 
