@@ -340,7 +340,8 @@ def run_ours(args, cfg, world, rank, local):
                        "max_trans_mm": float(max(trans)),
                        "mean_trans_mm": float(np.mean(trans)),
                        "last_icp_status": int(st.status), "last_inliers": int(st.inliers)},
-        "roofline": {"kernel": "k_integrate", "bound": "hbm", "achieved": achieved,
+        "roofline": {"kernel": "integrate stage (k_depth_tiles + k_classify_bricks + "
+                               "k_integrate_list)", "bound": "hbm", "achieved": achieved,
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "alg_bytes_per_launch": integ_bytes,
