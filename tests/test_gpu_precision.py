@@ -1,0 +1,24 @@
+"""The large-volume precision study (tests/precision_c3.py) on its first
+frames: 1024^3 FP16 volume over 4 m, every stage against the FP64 oracle on
+the GPU's own state at one checkpoint. Tolerances: TSDF within one FP16 ulp
+of tsdf/trunc, vertices within 0.1 mm, pose within 1e-5 rad / 0.01 mm, ICP
+sums within 2e-5 of their Cauchy-Schwarz scale."""
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_large_volume_fp16_stages_match_oracle(cuda):
+    from precision_c3 import run_study
+    res = run_study(frames=4, checkpoints=[3], log=lambda m: None)
+    cp = res["checkpoints"][0]
+    assert cp["integrate"]["weights_equal"]
+    assert cp["integrate"]["flagged_frac"] < 5e-3
+    assert cp["integrate"]["voxels_updated_oracle"] > 1_000_000
+    assert cp["integrate"]["max_tsdf_err_fp16_ulp"] <= 1.001
+    assert cp["raycast"]["hit_frac"] > 0.5 and cp["raycast"]["hit_mismatch_frac"] < 1e-3
+    assert cp["raycast"]["vertex_err_mm_q999"] < 0.1
+    assert cp["icp"]["oracle_status"] == 0
+    assert cp["icp"]["rot_err_rad"] < 1e-5 and cp["icp"]["trans_err_mm"] < 1e-2
+    assert cp["icp_sums"]["sum_err_rel_scale_max"] < 2e-5
+    assert res["summary"]["gt_max_trans_mm"] < 10.0
