@@ -43,6 +43,8 @@ typedef int32_t of_status_t;
 #define OF_ERR_OUT_OF_MEMORY 3    /* the tracker could not allocate device memory */
 #define OF_ERR_NOT_READY 4        /* called in the wrong order (e.g. track before the first frame) */
 #define OF_ERR_TOO_LARGE 5        /* a size beyond a fixed maximum of the entry point */
+#define OF_ERR_IO 6               /* a file could not be opened, read or written */
+#define OF_END_OF_SEQUENCE 7      /* a recorded sequence has no more frames */
 
 typedef void *of_stream_t; /* cudaStream_t */
 
@@ -339,6 +341,43 @@ typedef struct of_tracker_buffers {
   int32_t kernels_track;  /* kernel launches of every later step's graph */
 } of_tracker_buffers_t;
 of_status_t of_tracker_buffers(of_tracker_t tracker, of_tracker_buffers_t *out);
+
+/* ---- recorded sequences (the reference's on-disk format) -------------- */
+
+/* A recording directory holds `Parameters.txt` and raw frames `recorded1`,
+ * `recorded2`, ... (W x H uint16 depth in mm, row major): the format of
+ * Source/data/ParametersFileFormat.txt:1-11, as CameraFromFile reads it
+ * (Source/src/CameraSupport/CameraFromFile.cpp:22-98) and WriteToFile writes
+ * it (WriteToFile.cpp:18-145). */
+typedef struct of_recording_info {
+  of_camera_t camera;   /* width, height, fx, fy, cx, cy, min/max depth (mm) */
+  float z_offset_mm;    /* "Z offset in mm (for GIP, otherwise 0)" */
+  int32_t frames;       /* "Number of frames" (0 if absent) */
+  char name[256];
+  char date[64];
+  char camera_type[64];
+} of_recording_info_t;
+of_status_t of_recording_read_info(const char *dir, of_recording_info_t *info);
+of_status_t of_recording_write_info(const char *dir, const of_recording_info_t *info);
+/* Frame `number` (1-based, as the reference counts) to / from host memory;
+ * the writer also takes device memory (`depth_is_device`, copied on `stream`). */
+of_status_t of_recording_read_frame(const char *dir, int32_t number, int32_t width,
+                                    int32_t height, uint16_t *depth);
+of_status_t of_recording_write_frame(const char *dir, int32_t number, int32_t width,
+                                     int32_t height, const uint16_t *depth,
+                                     int32_t depth_is_device, of_stream_t stream);
+
+/* A recording as a frame source: one background thread reads `prefetch`
+ * frames ahead into pinned host buffers; of_reader_next copies the next frame
+ * to device memory with one asynchronous copy on `stream` (the buffer is
+ * reused only after that copy completes) and returns OF_END_OF_SEQUENCE after
+ * the last frame. Replaces CameraFromFile::GetDepthFrame's synchronous read
+ * and cudaMemcpy (CameraFromFile.cpp:73-98). */
+typedef struct of_reader *of_reader_t;
+of_status_t of_reader_open(const char *dir, int32_t prefetch, of_reader_t *out);
+of_status_t of_reader_info(of_reader_t reader, int32_t *width, int32_t *height, int32_t *frames);
+of_status_t of_reader_next(of_reader_t reader, uint16_t *d_depth, of_stream_t stream);
+of_status_t of_reader_close(of_reader_t reader);
 
 /* ---- many independent streams (batched) ------------------------------- */
 

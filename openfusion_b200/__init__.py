@@ -6,7 +6,8 @@ CUDA kernels behind the C-ABI of include/openfusion_b200.h; this package is the
 Python mirror of the reference's per-frame interfaces over that ABI.
 """
 from . import _native
-from .api import (CONFIGS, Batch, Config, c4_configs, Sequence, Tracker, integrate_scratch, icp_system, icp_track,
+from .api import (CONFIGS, Batch, Config, Reader, c4_configs, read_recording_frame,
+                  read_recording_info, write_recording, Sequence, Tracker, integrate_scratch, icp_system, icp_track,
                   icp_track_warm,
                   icp_workspace, integrate, integrate_census, lambda_table, level_camera, linear_to_volume,
                   make_scene, make_sequence, make_trajectory, new_pyramid, new_volume,
@@ -14,7 +15,8 @@ from .api import (CONFIGS, Batch, Config, c4_configs, Sequence, Tracker, integra
                   volume_bytes, volume_to_linear, shard, stream_cost)
 
 __all__ = [
-    "CONFIGS", "Batch", "Config", "c4_configs", "Sequence", "Tracker", "integrate_scratch", "icp_system", "icp_track", "icp_track_warm", "icp_workspace",
+    "CONFIGS", "Batch", "Config", "Reader", "c4_configs", "read_recording_frame",
+    "read_recording_info", "write_recording", "Sequence", "Tracker", "integrate_scratch", "icp_system", "icp_track", "icp_track_warm", "icp_workspace",
     "integrate", "integrate_census", "lambda_table", "level_camera", "linear_to_volume",
     "make_scene", "make_sequence", "make_trajectory", "new_pyramid", "new_volume", "preprocess",
     "pyramid_layout", "raycast", "render", "unpack_depth", "unpack_points", "volume_bytes",

@@ -83,6 +83,11 @@ class BatchDesc(C.Structure):
                 ("use_graph", C.c_int32), ("tune", C.c_int32), ("tuning", BatchTuning)]
 
 
+class RecordingInfo(C.Structure):
+    _fields_ = [("camera", Camera), ("z_offset_mm", C.c_float), ("frames", C.c_int32),
+                ("name", C.c_char * 256), ("date", C.c_char * 64), ("camera_type", C.c_char * 64)]
+
+
 class SynthPrim(C.Structure):
     _fields_ = [("kind", C.c_int32), ("p", C.c_float * 10)]
 
@@ -129,6 +134,16 @@ _SIGS = {
     "of_tracker_destroy": (c_status, [P]),
     "of_tracker_process": (c_status, [P, P, C.c_int32, c_stream]),
     "of_tracker_flush": (c_status, [P, c_stream]),
+    "of_recording_read_info": (c_status, [C.c_char_p, C.POINTER(RecordingInfo)]),
+    "of_recording_write_info": (c_status, [C.c_char_p, C.POINTER(RecordingInfo)]),
+    "of_recording_read_frame": (c_status, [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, P]),
+    "of_recording_write_frame": (c_status, [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, P,
+                                            C.c_int32, c_stream]),
+    "of_reader_open": (c_status, [C.c_char_p, C.c_int32, C.POINTER(C.c_void_p)]),
+    "of_reader_info": (c_status, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                  C.POINTER(C.c_int32)]),
+    "of_reader_next": (c_status, [P, P, c_stream]),
+    "of_reader_close": (c_status, [P]),
     "of_batch_create": (c_status, [C.POINTER(BatchDesc), C.POINTER(C.c_void_p)]),
     "of_batch_destroy": (c_status, [P]),
     "of_batch_process": (c_status, [P, C.POINTER(C.c_void_p), C.c_int32, c_stream]),

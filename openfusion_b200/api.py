@@ -432,6 +432,89 @@ def make_sequence(cfg: Config, frames: int | None = None, render_depth: bool = T
     return seq
 
 
+# --------------------------------------------------------------- recordings --
+
+END_OF_SEQUENCE = 7  # of_reader_next after the last frame
+
+
+def read_recording_info(path) -> N.RecordingInfo:
+    """Parameters.txt of a recording directory (CameraFromFile::Init)."""
+    info = N.RecordingInfo()
+    N.check("of_recording_read_info", N.lib().of_recording_read_info(str(path).encode(),
+                                                                     C.byref(info)))
+    return info
+
+
+def write_recording(path, cfg: Config, depth_frames, name: str = "", date: str = "",
+                    camera_type: str = "Synthetic", z_offset_mm: float = 0.0) -> None:
+    """A recording directory in the reference's format (WriteToFile): host
+    uint16 frames [F, H, W] (numpy) or CUDA tensors."""
+    import os
+    os.makedirs(path, exist_ok=True)
+    info = N.RecordingInfo()
+    info.camera = cfg.camera()
+    info.z_offset_mm = z_offset_mm
+    info.frames = len(depth_frames)
+    info.name = (name or str(path)).encode()[:255]
+    info.date = date.encode()[:63]
+    info.camera_type = camera_type.encode()[:63]
+    N.check("of_recording_write_info", N.lib().of_recording_write_info(str(path).encode(),
+                                                                       C.byref(info)))
+    for k, d in enumerate(depth_frames):
+        on_dev = hasattr(d, "is_cuda") and d.is_cuda
+        if on_dev:
+            ptr = d.data_ptr()
+        else:
+            d = np.ascontiguousarray(d, np.uint16)
+            ptr = d.ctypes.data
+        N.check("of_recording_write_frame",
+                N.lib().of_recording_write_frame(str(path).encode(), k + 1, cfg.width, cfg.height,
+                                                 ptr, 1 if on_dev else 0,
+                                                 _stream() if on_dev else None))
+
+
+def read_recording_frame(path, number: int, width: int, height: int) -> np.ndarray:
+    out = np.zeros((height, width), np.uint16)
+    N.check("of_recording_read_frame", N.lib().of_recording_read_frame(
+        str(path).encode(), number, width, height, out.ctypes.data))
+    return out
+
+
+class Reader:
+    """A recording as a prefetching frame source (of_reader_*): next() copies
+    the next frame into a CUDA tensor asynchronously; None after the last."""
+
+    def __init__(self, path, prefetch: int = 4):
+        h = C.c_void_p()
+        N.check("of_reader_open", N.lib().of_reader_open(str(path).encode(), prefetch, C.byref(h)))
+        self._h = h
+        w, hh, f = C.c_int32(), C.c_int32(), C.c_int32()
+        N.check("of_reader_info", N.lib().of_reader_info(self._h, C.byref(w), C.byref(hh),
+                                                         C.byref(f)))
+        self.width, self.height, self.frames = w.value, hh.value, f.value
+
+    def next(self, out=None, stream=None):
+        import torch
+        if out is None:
+            out = torch.empty((self.height, self.width), dtype=torch.int16, device="cuda")
+        st = N.lib().of_reader_next(self._h, out.data_ptr(), _stream(stream))
+        if st == END_OF_SEQUENCE:
+            return None
+        N.check("of_reader_next", st)
+        return out
+
+    def close(self):
+        if self._h:
+            N.lib().of_reader_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # ------------------------------------------------------------------ batched --
 
 def stream_cost(cfg: Config) -> float:

@@ -33,6 +33,7 @@ CUDA_SOURCES = [
     "of_synth_gpu.cu",
     "of_cnn.cu",
     "of_batch.cu",
+    "of_recording.cu",
 ]
 SYNTH_SOURCES = ["of_synth.cpp"]
 

@@ -30,6 +30,8 @@ extern "C" const char *of_status_string(of_status_t s) {
     case OF_ERR_OUT_OF_MEMORY: return "out of device memory";
     case OF_ERR_NOT_READY: return "not ready";
     case OF_ERR_TOO_LARGE: return "size beyond the entry point's fixed maximum";
+    case OF_ERR_IO: return "file could not be opened, read or written";
+    case OF_END_OF_SEQUENCE: return "end of the recorded sequence";
     default: return "unknown status";
   }
 }
