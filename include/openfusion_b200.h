@@ -342,6 +342,30 @@ typedef struct of_tracker_buffers {
 } of_tracker_buffers_t;
 of_status_t of_tracker_buffers(of_tracker_t tracker, of_tracker_buffers_t *out);
 
+/* ---- surface mesh and volume file (no GL) ----------------------------- */
+
+/* Triangle mesh of the tsdf = 0 surface of the observed voxels (marching
+ * tetrahedra: 6 tetrahedra per cell of 8 voxels; no cracks; triangles face
+ * the free space). The reference's own extraction is commented out
+ * (Source/src/MainApp.cpp:277-328). Writes up to `max_triangles` triangles as
+ * 9 floats (3 vertices, world mm) to `d_triangles` and, if `d_ids` is not
+ * NULL, one id each (cell * 12 + 2 * tetrahedron + k, cell = (i n + j) n + k
+ * of its lowest voxel); `d_count` (device) receives the surface's triangle
+ * count, which may exceed `max_triangles` (call again with room for all).
+ * Triangle order is not fixed; ids identify them. */
+of_status_t of_mesh_extract(const of_volume_desc_t *desc, const void *d_volume, float *d_triangles,
+                            uint64_t *d_ids, uint32_t max_triangles, uint32_t *d_count,
+                            of_stream_t stream);
+/* Host triangles (9 floats each) as a Wavefront OBJ file (vertices and
+ * 1-based faces). */
+of_status_t of_mesh_write_obj(const char *path, const float *triangles, uint32_t count);
+/* The volume as the reference's SavedVolume.raw: N^3 float tsdf in mm, index
+ * x N^2 + y N + z, unobserved voxels +truncation (RunApp::saveVolumeToFile,
+ * Source/src/MainApp.cpp:181-276). Allocates N^3 x 6 bytes of device memory
+ * and N^3 x 4 bytes of host memory for the call. */
+of_status_t of_volume_save_raw(const of_volume_desc_t *desc, const void *d_volume, const char *path,
+                               of_stream_t stream);
+
 /* ---- recorded sequences (the reference's on-disk format) -------------- */
 
 /* A recording directory holds `Parameters.txt` and raw frames `recorded1`,

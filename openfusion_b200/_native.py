@@ -134,6 +134,9 @@ _SIGS = {
     "of_tracker_destroy": (c_status, [P]),
     "of_tracker_process": (c_status, [P, P, C.c_int32, c_stream]),
     "of_tracker_flush": (c_status, [P, c_stream]),
+    "of_mesh_extract": (c_status, [C.POINTER(VolumeDesc), P, P, P, C.c_uint32, P, c_stream]),
+    "of_mesh_write_obj": (c_status, [C.c_char_p, P, C.c_uint32]),
+    "of_volume_save_raw": (c_status, [C.POINTER(VolumeDesc), P, C.c_char_p, c_stream]),
     "of_recording_read_info": (c_status, [C.c_char_p, C.POINTER(RecordingInfo)]),
     "of_recording_write_info": (c_status, [C.c_char_p, C.POINTER(RecordingInfo)]),
     "of_recording_read_frame": (c_status, [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, P]),

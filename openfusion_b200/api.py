@@ -432,6 +432,42 @@ def make_sequence(cfg: Config, frames: int | None = None, render_depth: bool = T
     return seq
 
 
+# ------------------------------------------------------------------- mesh --
+
+def extract_mesh(cfg: Config, vol, max_triangles: int | None = None, with_ids: bool = False):
+    """Triangles [T, 3, 3] (CUDA float32, world mm) of the volume's surface
+    (of_mesh_extract); grows the buffer once if the first guess is short."""
+    import torch
+    cap = max_triangles or 1 << 20
+    count = torch.zeros(1, dtype=torch.int32, device=vol.device)
+    for _ in range(2):
+        tris = torch.empty((cap, 9), dtype=torch.float32, device=vol.device)
+        ids = torch.empty(cap, dtype=torch.int64, device=vol.device) if with_ids else None
+        N.check("of_mesh_extract", N.lib().of_mesh_extract(
+            C.byref(cfg.volume()), _ptr(vol), _ptr(tris), _ptr(ids), cap, _ptr(count), _stream()))
+        n = int(count.item())
+        if n <= cap or max_triangles:
+            break
+        cap = n
+    n = min(n, cap)
+    out = tris[:n].view(n, 3, 3)
+    return (out, ids[:n]) if with_ids else out
+
+
+def write_obj(path, triangles) -> None:
+    """Triangles [T, 3, 3] (host or CUDA) as a Wavefront OBJ file."""
+    t = np.ascontiguousarray(triangles.cpu().numpy() if hasattr(triangles, "cpu") else triangles,
+                             np.float32)
+    N.check("of_mesh_write_obj", N.lib().of_mesh_write_obj(str(path).encode(), t.ctypes.data,
+                                                           t.shape[0]))
+
+
+def save_volume_raw(cfg: Config, vol, path) -> None:
+    """The volume as the reference's SavedVolume.raw (N^3 float tsdf mm)."""
+    N.check("of_volume_save_raw", N.lib().of_volume_save_raw(C.byref(cfg.volume()), _ptr(vol),
+                                                             str(path).encode(), _stream()))
+
+
 # --------------------------------------------------------------- recordings --
 
 END_OF_SEQUENCE = 7  # of_reader_next after the last frame

@@ -34,6 +34,7 @@ CUDA_SOURCES = [
     "of_cnn.cu",
     "of_batch.cu",
     "of_recording.cu",
+    "of_mesh.cu",
 ]
 SYNTH_SOURCES = ["of_synth.cpp"]
 

@@ -98,6 +98,8 @@ class Oracle:
         L.ora_tracker_pose.argtypes = [P, P]
         L.ora_tracker_volume.argtypes = [P]
         L.ora_tracker_volume.restype = C.c_void_p
+        L.ora_mesh.argtypes = [C.POINTER(Vol), P, P, P, C.c_int64]
+        L.ora_mesh.restype = C.c_int64
 
     # ----------------------------------------------------------- parameters
     @staticmethod
@@ -229,6 +231,17 @@ class Oracle:
         mp = C.c_double()
         st = self.lib.ora_icp_step(s.ctypes.data, P_.ctypes.data, C.byref(mp))
         return st, P_, mp.value
+
+    def mesh(self, cfg, words: np.ndarray):
+        """(triangles [T, 3, 3] mm, ids [T]) of linear-layout uint32 `words`, id order."""
+        w = np.ascontiguousarray(words, np.uint32)
+        n = self.lib.ora_mesh(C.byref(self.vol(cfg)), w.ctypes.data, None, None, 0)
+        tris = np.zeros((max(n, 1), 9), self.real)
+        ids = np.zeros(max(n, 1), np.uint64)
+        m = self.lib.ora_mesh(C.byref(self.vol(cfg)), w.ctypes.data, tris.ctypes.data,
+                              ids.ctypes.data, n)
+        assert m == n
+        return tris[:n].reshape(n, 3, 3), ids[:n]
 
     def icp_track(self, cfg, frame_buf: np.ndarray, model_buf: np.ndarray, pose: np.ndarray):
         P_ = np.array(pose, np.float64, copy=True)

@@ -1148,3 +1148,105 @@ void ora_ref_compose(const double *xopt, double *T, double *full) {
   matmul4(D, T, T);
   matmul4(full, D, full);
 }
+
+/* ------------------------------------------------------------------ mesh */
+
+/* Marching tetrahedra (Doi & Koide 1991; Bloomenthal's tetrahedral
+ * polygonizer) over Kuhn's split of each cell into the 6 tetrahedra around
+ * its main diagonal: corners 0, e_a, e_a + e_b, 7 (corner index dx | dy << 1 |
+ * dz << 2) for each axis order. A corner with tsdf < 0 is inside; one corner
+ * against three gives the triangle on its three edges, two against two the
+ * quadrilateral e(p,r) e(q,r) e(q,s) e(p,s) as (epr, eqr, eqs) + (epr, eqs,
+ * eps). Vertex = linear zero crossing, interpolated from the edge's voxel of
+ * lower brick-major address. Triangles face from the inside corners to the
+ * outside ones. Only cells whose 8 voxels are observed produce triangles. */
+static const int ora_tets[6][4] = {{0, 1, 3, 7}, {0, 1, 5, 7}, {0, 2, 3, 7},
+                                   {0, 2, 6, 7}, {0, 4, 5, 7}, {0, 4, 6, 7}};
+
+static uint64_t brick_address(int n, int i, int j, int k) {
+  const uint64_t nb = (uint64_t)(n / 8);
+  const uint64_t b = ((uint64_t)(i >> 3) * nb + (uint64_t)(j >> 3)) * nb + (uint64_t)(k >> 3);
+  return (b << 9) | (uint64_t)(((i & 7) << 6) | ((j & 7) << 3) | (k & 7));
+}
+
+typedef struct {
+  R v, p[3];
+  uint64_t a;
+} mesh_corner;
+
+static void mesh_edge(const mesh_corner *x, const mesh_corner *y, R *out) {
+  const mesh_corner *lo = x->a < y->a ? x : y, *hi = x->a < y->a ? y : x;
+  const R t = lo->v / (lo->v - hi->v);
+  for (int d = 0; d < 3; ++d) out[d] = lo->p[d] + t * (hi->p[d] - lo->p[d]);
+}
+
+static void mesh_put(R *out, const R *a, const R *b, const R *c, const R *dir) {
+  R u[3], w[3];
+  for (int d = 0; d < 3; ++d) { u[d] = b[d] - a[d]; w[d] = c[d] - a[d]; }
+  const R nx = u[1] * w[2] - u[2] * w[1], ny = u[2] * w[0] - u[0] * w[2], nz = u[0] * w[1] - u[1] * w[0];
+  const int flip = nx * dir[0] + ny * dir[1] + nz * dir[2] < 0;
+  for (int d = 0; d < 3; ++d) {
+    out[d] = a[d];
+    out[3 + d] = flip ? c[d] : b[d];
+    out[6 + d] = flip ? b[d] : c[d];
+  }
+}
+
+int64_t ora_mesh(const ora_vol *v, const uint32_t *words, R *tris, uint64_t *ids, int64_t max_tris) {
+  const int n = v->n;
+  int64_t cnt = 0;
+  for (int i = 0; i < n - 1; ++i)
+    for (int j = 0; j < n - 1; ++j)
+      for (int k = 0; k < n - 1; ++k) {
+        mesh_corner C[8];
+        int live = 1;
+        for (int c = 0; c < 8 && live; ++c) {
+          const int ci = i + (c & 1), cj = j + ((c >> 1) & 1), ck = k + (c >> 2);
+          const uint32_t w = words[((size_t)ci * n + cj) * n + ck];
+          if ((w >> 16) == 0) live = 0;
+          C[c].v = vox_value(w, v->storage);
+          C[c].p[0] = (R)voxel_centre(v->size, n, ci);
+          C[c].p[1] = (R)voxel_centre(v->size, n, cj);
+          C[c].p[2] = (R)voxel_centre(v->size, n, ck);
+          C[c].a = brick_address(n, ci, cj, ck);
+        }
+        if (!live) continue;
+        const uint64_t cell = ((uint64_t)i * n + j) * n + k;
+        for (int q = 0; q < 6; ++q) {
+          int in[4], outc[4], ni = 0, no = 0;
+          for (int r = 0; r < 4; ++r) {
+            const int t = ora_tets[q][r];
+            if (C[t].v < 0) in[ni++] = t;
+            else outc[no++] = t;
+          }
+          if (ni == 0 || ni == 4) continue;
+          R dir[3] = {0, 0, 0};
+          for (int r = 0; r < no; ++r)
+            for (int d = 0; d < 3; ++d) dir[d] += C[outc[r]].p[d] * ni;
+          for (int r = 0; r < ni; ++r)
+            for (int d = 0; d < 3; ++d) dir[d] -= C[in[r]].p[d] * no;
+          if (ni == 2) {
+            R epr[3], eqr[3], eqs[3], eps[3];
+            mesh_edge(&C[in[0]], &C[outc[0]], epr);
+            mesh_edge(&C[in[1]], &C[outc[0]], eqr);
+            mesh_edge(&C[in[1]], &C[outc[1]], eqs);
+            mesh_edge(&C[in[0]], &C[outc[1]], eps);
+            if (cnt < max_tris) { mesh_put(tris + 9 * cnt, epr, eqr, eqs, dir); ids[cnt] = cell * 12 + 2 * q; }
+            ++cnt;
+            if (cnt < max_tris) { mesh_put(tris + 9 * cnt, epr, eqs, eps, dir); ids[cnt] = cell * 12 + 2 * q + 1; }
+            ++cnt;
+          } else {
+            const int s = ni == 1 ? in[0] : outc[0];
+            const int *rest = ni == 1 ? outc : in;
+            R a[3], b[3], c[3];
+            mesh_edge(&C[s], &C[rest[0]], a);
+            mesh_edge(&C[s], &C[rest[1]], b);
+            mesh_edge(&C[s], &C[rest[2]], c);
+            if (cnt < max_tris) { mesh_put(tris + 9 * cnt, a, b, c, dir); ids[cnt] = cell * 12 + 2 * q; }
+            ++cnt;
+          }
+        }
+      }
+  return cnt;
+}
+

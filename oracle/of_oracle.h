@@ -130,6 +130,13 @@ void ora_ref_icp_system(const ora_refcam *c, const uint16_t *new_depth, const do
                         double *out6, double *amb36, double *amb6);
 void ora_ref_compose(const double *xopt, double *T, double *full);
 
+/* Mesh of the tsdf = 0 surface by marching tetrahedra (Kuhn's 6 tetrahedra
+ * per cell, cells of 8 observed voxels), linear-layout words. Writes up to
+ * `max_tris` triangles (9 reals each) and their ids (cell * 12 + 2 tet + k,
+ * cell = (i n + j) n + k), in id order; returns the number of triangles. */
+int64_t ora_mesh(const ora_vol *v, const uint32_t *words, ora_real *tris, uint64_t *ids,
+                 int64_t max_tris);
+
 /* CPU tracker: the whole frame loop (used as the CPU baseline) */
 typedef struct ora_tracker ora_tracker;
 ora_tracker *ora_tracker_create(const ora_cam *c, const ora_vol *v, const ora_params *p,
