@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define OF_ABI_VERSION 2
+#define OF_ABI_VERSION 3
 
 typedef int32_t of_status_t;
 #define OF_OK 0
@@ -279,6 +279,37 @@ of_status_t of_icp_system(const of_camera_t *cam, const of_icp_params_t *params,
                           const void *d_frame, const void *d_model, const double *d_pose,
                           void *d_workspace, float *d_system, of_stream_t stream);
 
+/* ---- camera-side depth filters ---------------------------------------- */
+
+/* The filters the reference's cameras run on raw depth
+ * (Source/src/CameraSupport/CameraAbstract.cu:9-229; chained by
+ * GIPCam.cpp:173-177 and SoftKineticCamera.cpp:424-430), with the intended
+ * border handling (neighbours outside the image left out or clamped, not
+ * wrapped around). */
+#define OF_DEPTH_FILTER_MEDIAN5 1   /* median of the 5x5 window's non-null pixels */
+#define OF_DEPTH_FILTER_GRADIENT 2  /* Prewitt: 0 where |gradient| / 6 > threshold */
+#define OF_DEPTH_FILTER_AVERAGE 4   /* 8-neighbour mean; null where it differs from the pixel by more than the threshold */
+#define OF_DEPTH_FILTER_UNDISTORT 8 /* Brown k1, k2, p1, p2 from the camera's intrinsics */
+typedef struct of_depth_filter_params {
+  int32_t steps;           /* OF_DEPTH_FILTER_* bits; applied as undistort, median, gradient, average */
+  int32_t null_value;      /* depth of an invalid pixel (depthNullValue; 0 for most cameras) */
+  int32_t average_passes;  /* average applied this many times (GIPCam: 2) */
+  float average_threshold_mm;   /* 15 */
+  float gradient_threshold_mm;  /* 10 */
+  float k1, k2, p1, p2;
+} of_depth_filter_params_t;
+void of_depth_filter_defaults(of_depth_filter_params_t *params);
+/* The chain `params->steps` from d_in to d_out (may be equal); `d_scratch`
+ * (W x H uint16, distinct from both) is needed for more than one step or in
+ * place. Runs on `stream` without synchronising. */
+of_status_t of_depth_filter(const of_camera_t *cam, const of_depth_filter_params_t *params,
+                            const uint16_t *d_in, uint16_t *d_out, uint16_t *d_scratch,
+                            of_stream_t stream);
+/* One filter (`kind` = one OF_DEPTH_FILTER_* bit) from d_in to d_out (distinct). */
+of_status_t of_depth_filter_step(const of_camera_t *cam, int32_t kind,
+                                 const of_depth_filter_params_t *params, const uint16_t *d_in,
+                                 uint16_t *d_out, of_stream_t stream);
+
 /* ---- tracker: the whole frame (RunApp::display, MainApp.cpp:786-964) ---- */
 
 typedef struct of_tracker *of_tracker_t;
@@ -297,6 +328,9 @@ typedef struct of_tracker_desc {
    * Needs W = 80 k, H = 60 k. Each tracked frame then runs the CNN on the
    * (previous, current) depth pair and of_icp_track_warm. */
   const float *warm_start_weights;
+  /* Camera-side filters applied in place to each depth frame before it is
+   * used (steps = 0: none). */
+  of_depth_filter_params_t depth_filter;
 } of_tracker_desc_t;
 
 of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_tracker_t *out);

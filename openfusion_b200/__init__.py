@@ -6,7 +6,8 @@ CUDA kernels behind the C-ABI of include/openfusion_b200.h; this package is the
 Python mirror of the reference's per-frame interfaces over that ABI.
 """
 from . import _native
-from .api import (CONFIGS, Batch, Config, Reader, c4_configs, extract_mesh, read_recording_frame,
+from .api import (CONFIGS, Batch, Config, Reader, c4_configs, depth_filter, depth_filter_params,
+                  extract_mesh, read_recording_frame,
                   save_volume_raw, write_obj,
                   read_recording_info, write_recording, Sequence, Tracker, integrate_scratch, icp_system, icp_track,
                   icp_track_warm,
@@ -16,7 +17,8 @@ from .api import (CONFIGS, Batch, Config, Reader, c4_configs, extract_mesh, read
                   volume_bytes, volume_to_linear, shard, stream_cost)
 
 __all__ = [
-    "CONFIGS", "Batch", "Config", "Reader", "c4_configs", "extract_mesh", "read_recording_frame",
+    "CONFIGS", "Batch", "Config", "Reader", "c4_configs", "depth_filter", "depth_filter_params",
+    "extract_mesh", "read_recording_frame",
     "save_volume_raw", "write_obj",
     "read_recording_info", "write_recording", "Sequence", "Tracker", "integrate_scratch", "icp_system", "icp_track", "icp_track_warm", "icp_workspace",
     "integrate", "integrate_census", "lambda_table", "level_camera", "linear_to_volume",

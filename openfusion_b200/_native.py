@@ -54,11 +54,18 @@ class PyramidLayout(C.Structure):
                 ("total_bytes", C.c_size_t)]
 
 
+class DepthFilterParams(C.Structure):
+    _fields_ = [("steps", C.c_int32), ("null_value", C.c_int32), ("average_passes", C.c_int32),
+                ("average_threshold_mm", C.c_float), ("gradient_threshold_mm", C.c_float),
+                ("k1", C.c_float), ("k2", C.c_float), ("p1", C.c_float), ("p2", C.c_float)]
+
+
 class TrackerDesc(C.Structure):
     _fields_ = [("camera", Camera), ("volume", VolumeDesc), ("filter", FilterParams),
                 ("raycast", RaycastParams), ("icp", IcpParams),
                 ("initial_pose", C.c_double * 16), ("use_graph", C.c_int32),
-                ("pose_history", C.c_int32), ("warm_start_weights", C.c_void_p)]
+                ("pose_history", C.c_int32), ("warm_start_weights", C.c_void_p),
+                ("depth_filter", DepthFilterParams)]
 
 
 class TrackerBuffers(C.Structure):
@@ -134,6 +141,11 @@ _SIGS = {
     "of_tracker_destroy": (c_status, [P]),
     "of_tracker_process": (c_status, [P, P, C.c_int32, c_stream]),
     "of_tracker_flush": (c_status, [P, c_stream]),
+    "of_depth_filter_defaults": (None, [C.POINTER(DepthFilterParams)]),
+    "of_depth_filter": (c_status, [C.POINTER(Camera), C.POINTER(DepthFilterParams), P, P, P,
+                                   c_stream]),
+    "of_depth_filter_step": (c_status, [C.POINTER(Camera), C.c_int32,
+                                        C.POINTER(DepthFilterParams), P, P, c_stream]),
     "of_mesh_extract": (c_status, [C.POINTER(VolumeDesc), P, P, P, C.c_uint32, P, c_stream]),
     "of_mesh_write_obj": (c_status, [C.c_char_p, P, C.c_uint32]),
     "of_volume_save_raw": (c_status, [C.POINTER(VolumeDesc), P, C.c_char_p, c_stream]),

@@ -307,7 +307,8 @@ class Tracker:
     frame loop (MainApp.cpp:786-964) as one CUDA graph per frame."""
 
     def __init__(self, cfg: Config, initial_pose: np.ndarray, use_graph: bool = True,
-                 pose_history: int = 1024, warm_start_weights: np.ndarray | None = None):
+                 pose_history: int = 1024, warm_start_weights: np.ndarray | None = None,
+                 depth_filter: N.DepthFilterParams | None = None):
         """`warm_start_weights`: FP32 weights of the warm-start CNN (None =
         plain ICP from the previous pose)."""
         self.cfg = cfg
@@ -320,6 +321,8 @@ class Tracker:
         d.initial_pose = (C.c_double * 16)(*np.asarray(initial_pose, np.float64).reshape(16))
         d.use_graph = 1 if use_graph else 0
         d.pose_history = pose_history
+        if depth_filter is not None:
+            d.depth_filter = depth_filter
         self._weights = None
         if warm_start_weights is not None:
             self._weights = np.ascontiguousarray(warm_start_weights, np.float32)
@@ -430,6 +433,35 @@ def make_sequence(cfg: Config, frames: int | None = None, render_depth: bool = T
     if render_depth:
         seq.depth = np.stack([render(cfg, scene, poses[k], k) for k in range(f)])
     return seq
+
+
+# ------------------------------------------------------- camera-side filters --
+
+DEPTH_FILTER = {"median5": 1, "gradient": 2, "average": 4, "undistort": 8}
+
+
+def depth_filter_params(steps=(), null_value: int = 0, average_passes: int = 1,
+                        average_threshold_mm: float = 15.0, gradient_threshold_mm: float = 10.0,
+                        k1=0.0, k2=0.0, p1=0.0, p2=0.0) -> N.DepthFilterParams:
+    p = N.DepthFilterParams()
+    N.lib().of_depth_filter_defaults(C.byref(p))
+    p.steps = sum(DEPTH_FILTER[s] for s in steps)
+    p.null_value, p.average_passes = null_value, average_passes
+    p.average_threshold_mm, p.gradient_threshold_mm = average_threshold_mm, gradient_threshold_mm
+    p.k1, p.k2, p.p1, p.p2 = k1, k2, p1, p2
+    return p
+
+
+def depth_filter(cfg: Config, depth, steps=(), out=None, **kw):
+    """The camera-side filter chain on a CUDA uint16 (int16-typed) depth image."""
+    import torch
+    p = depth_filter_params(steps, **kw)
+    out = torch.empty_like(depth) if out is None else out
+    scratch = torch.empty_like(depth)
+    N.check("of_depth_filter", N.lib().of_depth_filter(C.byref(cfg.camera()), C.byref(p),
+                                                       _ptr(depth), _ptr(out), _ptr(scratch),
+                                                       _stream()))
+    return out
 
 
 # ------------------------------------------------------------------- mesh --

@@ -35,6 +35,7 @@ CUDA_SOURCES = [
     "of_batch.cu",
     "of_recording.cu",
     "of_mesh.cu",
+    "of_filters.cu",
 ]
 SYNTH_SOURCES = ["of_synth.cpp"]
 

@@ -44,6 +44,7 @@ struct of_tracker {
   double *hist = nullptr;
   unsigned long long *hist_count = nullptr;
   uint16_t *depth[2] = {nullptr, nullptr};  // frame k in depth[k & 1]
+  uint16_t *filter_scratch = nullptr;       // camera-side filters (desc.depth_filter)
   float *lambda = nullptr;
   void *scratch = nullptr;
   of_icp_stats_t *stats = nullptr;
@@ -73,8 +74,17 @@ __global__ void k_record_pose(const double *pose, double *hist, unsigned long lo
   *count = c + 1;
 }
 
+// the camera-side filters of the new frame, in place (none when steps = 0)
+of_status_t enqueue_filters(of_tracker *t, int cur, cudaStream_t s) {
+  if (t->desc.depth_filter.steps == 0) return OF_OK;
+  return of_depth_filter(&t->desc.camera, &t->desc.depth_filter, t->depth[cur], t->depth[cur],
+                         t->filter_scratch, s);
+}
+
 // Frame 0 of a tracker: its pose is the initial pose (fused by the next step).
 of_status_t enqueue_first(of_tracker *t, cudaStream_t s) {
+  of_status_t st = enqueue_filters(t, 0, s);
+  if (st != OF_OK) return st;
   k_record_pose<<<1, 32, 0, s>>>(t->pose, t->hist, t->hist_count, t->hist_cap);
   return of_launch_status();
 }
@@ -95,6 +105,8 @@ of_status_t enqueue_fuse(of_tracker *t, const uint16_t *depth, cudaStream_t s) {
 of_status_t enqueue_track(of_tracker *t, int cur, bool fuse, cudaStream_t s) {
   const of_tracker_desc_t &d = t->desc;
   const uint16_t *now = t->depth[cur], *before = t->depth[cur ^ 1];
+  of_status_t sflt = enqueue_filters(t, cur, s);
+  if (sflt != OF_OK) return sflt;
   OF_CUDA_TRY(cudaEventRecord(t->ev_fork, s));
   OF_CUDA_TRY(cudaStreamWaitEvent(t->pre, t->ev_fork, 0));
   of_status_t st = OF_OK;
@@ -157,7 +169,7 @@ void release(of_tracker *t) {
   for (cudaGraphExec_t g : t->g_track)
     if (g) cudaGraphExecDestroy(g);
   void *bufs[] = {t->volume, t->frame, t->model, t->icp_ws, t->pose, t->hist, t->hist_count,
-                  t->depth[0], t->depth[1], t->lambda, t->scratch, t->stats, t->cnn_master,
+                  t->depth[0], t->depth[1], t->filter_scratch, t->lambda, t->scratch, t->stats, t->cnn_master,
                   t->cnn_params, t->cnn_out, t->warm_pose};
   for (void *b : bufs)
     if (b) cudaFree(b);
@@ -216,6 +228,7 @@ extern "C" of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_track
       {(void **)&t->hist_count, sizeof(unsigned long long)},
       {(void **)&t->depth[0], px * sizeof(uint16_t)},
       {(void **)&t->depth[1], px * sizeof(uint16_t)},
+      {(void **)&t->filter_scratch, desc->depth_filter.steps ? px * sizeof(uint16_t) : 0},
       {(void **)&t->lambda, lam_bytes},
       {&t->scratch, scratch_bytes},
       {(void **)&t->stats, sizeof(of_icp_stats_t)},

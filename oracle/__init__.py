@@ -98,6 +98,11 @@ class Oracle:
         L.ora_tracker_pose.argtypes = [P, P]
         L.ora_tracker_volume.argtypes = [P]
         L.ora_tracker_volume.restype = C.c_void_p
+        L.ora_depth_median5.argtypes = [C.c_int32, C.c_int32, C.c_int32, P, P]
+        L.ora_depth_average.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_double, P, P]
+        L.ora_depth_gradient.argtypes = [C.c_int32, C.c_int32, C.c_double, P, P, P]
+        L.ora_depth_undistort.argtypes = [C.c_int32, C.c_int32] + [C.c_double] * 8 + [
+            C.c_int32, P, P, P]
         L.ora_mesh.argtypes = [C.POINTER(Vol), P, P, P, C.c_int64]
         L.ora_mesh.restype = C.c_int64
 
@@ -231,6 +236,28 @@ class Oracle:
         mp = C.c_double()
         st = self.lib.ora_icp_step(s.ctypes.data, P_.ctypes.data, C.byref(mp))
         return st, P_, mp.value
+
+    def depth_filter(self, kind: str, depth: np.ndarray, null_value: int = 0, thr: float = 0.0,
+                     undistort=None):
+        """Camera-side filter of uint16 depth [H, W]: "median5", "average"
+        (thr mm), "gradient" (thr mm) or "undistort" (undistort = (fx, fy, cx,
+        cy, k1, k2, p1, p2)). Returns (out, ambiguity mask or None)."""
+        d = np.ascontiguousarray(depth, np.uint16)
+        h, w = d.shape
+        out = np.zeros_like(d)
+        amb = np.zeros(d.shape, np.uint8)
+        if kind == "median5":
+            self.lib.ora_depth_median5(w, h, null_value, d.ctypes.data, out.ctypes.data)
+            return out, None
+        if kind == "average":
+            self.lib.ora_depth_average(w, h, null_value, thr, d.ctypes.data, out.ctypes.data)
+            return out, None
+        if kind == "gradient":
+            self.lib.ora_depth_gradient(w, h, thr, d.ctypes.data, out.ctypes.data, amb.ctypes.data)
+            return out, amb
+        self.lib.ora_depth_undistort(w, h, *[float(x) for x in undistort], null_value,
+                                     d.ctypes.data, out.ctypes.data, amb.ctypes.data)
+        return out, amb
 
     def mesh(self, cfg, words: np.ndarray):
         """(triangles [T, 3, 3] mm, ids [T]) of linear-layout uint32 `words`, id order."""

@@ -1250,3 +1250,105 @@ int64_t ora_mesh(const ora_vol *v, const uint32_t *words, R *tris, uint64_t *ids
   return cnt;
 }
 
+/* -------------------------------------------------------- depth filters */
+
+static int cmp_u16(const void *a, const void *b) {
+  return (int)*(const uint16_t *)a - (int)*(const uint16_t *)b;
+}
+
+/* d_MedianFilter (CameraAbstract.cu:103-124) with in-image windows */
+void ora_depth_median5(int32_t w, int32_t h, int32_t null_value, const uint16_t *in, uint16_t *out) {
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      uint16_t v[25];
+      int n = 0, win = 0;
+      for (int j = -2; j <= 2; ++j)
+        for (int i = -2; i <= 2; ++i) {
+          const int xx = x + i, yy = y + j;
+          if (xx < 0 || xx >= w || yy < 0 || yy >= h) continue;
+          ++win;
+          const uint16_t d = in[(size_t)yy * w + xx];
+          if (d != (uint16_t)null_value) v[n++] = d;
+        }
+      uint16_t r = (uint16_t)null_value;
+      if (n > win / 2) {
+        qsort(v, (size_t)n, sizeof(uint16_t), cmp_u16);
+        r = (n & 1) ? v[n / 2] : (uint16_t)(((int)v[n / 2 - 1] + (int)v[n / 2]) / 2);
+      }
+      out[(size_t)y * w + x] = r;
+    }
+}
+
+/* d_AverageFilter (CameraAbstract.cu:9-34): mean of the 8-neighbours (the
+ * in-image ones), compared with the pixel */
+void ora_depth_average(int32_t w, int32_t h, int32_t null_value, double thr, const uint16_t *in,
+                       uint16_t *out) {
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      double s = 0;
+      int n = 0;
+      for (int j = -1; j <= 1; ++j)
+        for (int i = -1; i <= 1; ++i) {
+          const int xx = x + i, yy = y + j;
+          if ((i == 0 && j == 0) || xx < 0 || xx >= w || yy < 0 || yy >= h) continue;
+          s += in[(size_t)yy * w + xx];
+          ++n;
+        }
+      const double avg = s / n;
+      const double v = in[(size_t)y * w + x];
+      out[(size_t)y * w + x] = fabs(avg - v) > thr ? (uint16_t)null_value : (uint16_t)avg;
+    }
+}
+
+/* d_GradientFilter (CameraAbstract.cu:36-71): Prewitt sums with clamped
+ * coordinates; gradient / 6 against the threshold */
+void ora_depth_gradient(int32_t w, int32_t h, double thr, const uint16_t *in, uint16_t *out,
+                        uint8_t *ambig) {
+#define CL(a, m) ((a) < 0 ? 0 : ((a) >= (m) ? (m) - 1 : (a)))
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      long gx = 0, gy = 0;
+      for (int j = -1; j <= 1; ++j)
+        gx += (long)in[(size_t)CL(y + j, h) * w + CL(x + 1, w)] - in[(size_t)CL(y + j, h) * w + CL(x - 1, w)];
+      for (int i = -1; i <= 1; ++i)
+        gy += (long)in[(size_t)CL(y + 1, h) * w + CL(x + i, w)] - in[(size_t)CL(y - 1, h) * w + CL(x + i, w)];
+      const double g2 = (double)(gx * gx + gy * gy), t2 = 36.0 * thr * thr;
+      out[(size_t)y * w + x] = g2 > t2 ? 0 : in[(size_t)y * w + x];
+      if (ambig) ambig[(size_t)y * w + x] = fabs(g2 - t2) <= 1e-3 * t2;
+    }
+#undef CL
+}
+
+/* d_undistort (CameraAbstract.cu:170-221): the Brown model of the raw image
+ * evaluated at the ideal pixel's normalised coordinates (the y term from the
+ * undistorted x), bilinear sample of the raw depth */
+void ora_depth_undistort(int32_t w, int32_t h, double fx, double fy, double cx, double cy,
+                         double k1, double k2, double p1, double p2, int32_t null_value,
+                         const uint16_t *in, uint16_t *out, uint8_t *ambig) {
+  const uint16_t nv = (uint16_t)null_value;
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      const double xn = (x - cx) / fx, yn = (y - cy) / fy;
+      const double r2 = xn * xn + yn * yn, rad = 1 + k1 * r2 + k2 * r2 * r2;
+      const double xd = xn * rad + 2 * p1 * xn * yn + p2 * (r2 + 2 * xn * xn);
+      const double yd = yn * rad + p1 * (r2 + 2 * yn * yn) + 2 * p2 * xn * yn;
+      const double u = fx * xd + cx, v = fy * yd + cy;
+      const double u0f = floor(u), v0f = floor(v);
+      const size_t o = (size_t)y * w + x;
+      if (ambig) {
+        const double fu = u - u0f, fv = v - v0f;
+        ambig[o] = fu < 1e-4 || fu > 1 - 1e-4 || fv < 1e-4 || fv > 1 - 1e-4;
+      }
+      if (u0f < 0 || u0f > w - 1 || v0f < 0 || v0f > h - 1) { out[o] = nv; continue; }
+      const int u0 = (int)u0f, v0 = (int)v0f;
+      const int u1 = u0 + 1 < w ? u0 + 1 : u0, v1 = v0 + 1 < h ? v0 + 1 : v0;
+      const uint16_t a = in[(size_t)v0 * w + u0], b = in[(size_t)v0 * w + u1];
+      const uint16_t c = in[(size_t)v1 * w + u0], d = in[(size_t)v1 * w + u1];
+      if (a == nv || b == nv || c == nv || d == nv) { out[o] = nv; continue; }
+      const double fu = u - u0f, fv = v - v0f;
+      const uint16_t f1 = u1 == u0 ? a : (uint16_t)((1 - fu) * a + fu * b);
+      const uint16_t f2 = v1 == v0 ? f1 : (u1 == u0 ? c : (uint16_t)((1 - fu) * c + fu * d));
+      out[o] = (uint16_t)((1 - fv) * f1 + fv * f2);
+    }
+}
+

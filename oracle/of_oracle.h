@@ -137,6 +137,28 @@ void ora_ref_compose(const double *xopt, double *T, double *full);
 int64_t ora_mesh(const ora_vol *v, const uint32_t *words, ora_real *tris, uint64_t *ids,
                  int64_t max_tris);
 
+/* Camera-side depth filters (Source/src/CameraSupport/CameraAbstract.cu:9-229)
+ * on uint16 depth, with the intended border handling: neighbours outside the
+ * image are left out (median, average) or clamped (gradient).
+ *   median5:  median of the window's non-null pixels (mean of the middle two,
+ *             truncated, for an even count); null unless more than half of the
+ *             window's in-image pixels are non-null
+ *   average:  mean of the in-image 8-neighbours; null when it differs from the
+ *             pixel by more than `thr`, else the mean truncated
+ *   gradient: Prewitt sums gx, gy; 0 where (gx/6)^2 + (gy/6)^2 > thr^2
+ *   undistort: Brown model (k1, k2 radial, p1, p2 tangential) from the ideal
+ *             pixel to the raw image, bilinear with truncated row values;
+ *             null outside the image or where a tap is null. `ambig` flags
+ *             pixels whose source lies within 1e-4 px of a tap boundary. */
+void ora_depth_median5(int32_t w, int32_t h, int32_t null_value, const uint16_t *in, uint16_t *out);
+void ora_depth_average(int32_t w, int32_t h, int32_t null_value, double thr, const uint16_t *in,
+                       uint16_t *out);
+void ora_depth_gradient(int32_t w, int32_t h, double thr, const uint16_t *in, uint16_t *out,
+                        uint8_t *ambig);
+void ora_depth_undistort(int32_t w, int32_t h, double fx, double fy, double cx, double cy,
+                         double k1, double k2, double p1, double p2, int32_t null_value,
+                         const uint16_t *in, uint16_t *out, uint8_t *ambig);
+
 /* CPU tracker: the whole frame loop (used as the CPU baseline) */
 typedef struct ora_tracker ora_tracker;
 ora_tracker *ora_tracker_create(const ora_cam *c, const ora_vol *v, const ora_params *p,

@@ -15,7 +15,7 @@ HERE = Path(__file__).resolve().parent
 OUT = HERE.parent / "_ref"
 REF = Path("/root/reference/Source")
 TUS = ["ref_camera.cu", "ref_volume.cu", "ref_general.cu", "ref_raycast.cu", "ref_icp.cu",
-       "ref_pipeline.cu"]
+       "ref_pipeline.cu", "ref_filters.cu"]
 
 
 def build() -> Path | None:
