@@ -499,6 +499,17 @@ of_status_t of_batch_shard(const double *cost, int32_t count, int32_t ranks,
 /* ---- reference-layout adapters (for the reference's PointInfo /
  *      CameraData: AoS float3, BAD_VERTEX = FLT_MAX, BasicTypes.h:40-49) --- */
 
+/* Headless views (RGBA8 words, as the reference packs them for its
+ * windows, rgbaFloatToIntCamera, Source/src/CameraSupport/CameraHandler.cu:55-62):
+ * depth as gray depth / max depth, opaque (CameraHandler.cu:75-78); level-0
+ * normals of a frame or model as (n + 1) / 2 with alpha `alpha`
+ * (CameraHandler.cu:128-131: 1; the raycast's show-normals mode,
+ * Raycaster.cu:214-218: 0), world space when `d_pose` (frame maps) is given.
+ * The raycast's shaded view is of_raycast's `rgba` output. */
+of_status_t of_depth_to_rgba(const of_camera_t *cam, const uint16_t *d_depth, uint32_t *d_rgba,
+                             of_stream_t stream);
+of_status_t of_normals_to_rgba(const of_camera_t *cam, const void *d_pyramid, const double *d_pose,
+                               float alpha, uint32_t *d_rgba, of_stream_t stream);
 /* Level 0 of a model/frame -> AoS float3 maps; invalid vertex = FLT_MAX,
  * invalid normal = 0. If `d_pose` is not NULL the points are camera-space
  * and are transformed to world space first (frame maps). */

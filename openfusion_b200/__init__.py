@@ -7,6 +7,7 @@ Python mirror of the reference's per-frame interfaces over that ABI.
 """
 from . import _native
 from .api import (CONFIGS, Batch, Config, Reader, c4_configs, depth_filter, depth_filter_params,
+                  depth_rgba, normals_rgba,
                   extract_mesh, read_recording_frame,
                   save_volume_raw, write_obj,
                   read_recording_info, write_recording, Sequence, Tracker, integrate_scratch, icp_system, icp_track,
@@ -18,6 +19,7 @@ from .api import (CONFIGS, Batch, Config, Reader, c4_configs, depth_filter, dept
 
 __all__ = [
     "CONFIGS", "Batch", "Config", "Reader", "c4_configs", "depth_filter", "depth_filter_params",
+    "depth_rgba", "normals_rgba",
     "extract_mesh", "read_recording_frame",
     "save_volume_raw", "write_obj",
     "read_recording_info", "write_recording", "Sequence", "Tracker", "integrate_scratch", "icp_system", "icp_track", "icp_track_warm", "icp_workspace",

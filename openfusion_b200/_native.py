@@ -146,6 +146,8 @@ _SIGS = {
                                    c_stream]),
     "of_depth_filter_step": (c_status, [C.POINTER(Camera), C.c_int32,
                                         C.POINTER(DepthFilterParams), P, P, c_stream]),
+    "of_depth_to_rgba": (c_status, [C.POINTER(Camera), P, P, c_stream]),
+    "of_normals_to_rgba": (c_status, [C.POINTER(Camera), P, P, C.c_float, P, c_stream]),
     "of_mesh_extract": (c_status, [C.POINTER(VolumeDesc), P, P, P, C.c_uint32, P, c_stream]),
     "of_mesh_write_obj": (c_status, [C.c_char_p, P, C.c_uint32]),
     "of_volume_save_raw": (c_status, [C.POINTER(VolumeDesc), P, C.c_char_p, c_stream]),

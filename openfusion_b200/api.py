@@ -464,6 +464,26 @@ def depth_filter(cfg: Config, depth, steps=(), out=None, **kw):
     return out
 
 
+# ----------------------------------------------------------- headless views --
+
+def depth_rgba(cfg: Config, depth):
+    """RGBA8 words [H, W] (int32 CUDA tensor): gray depth / max depth."""
+    import torch
+    out = torch.empty((cfg.height, cfg.width), dtype=torch.int32, device=depth.device)
+    N.check("of_depth_to_rgba", N.lib().of_depth_to_rgba(C.byref(cfg.camera()), _ptr(depth),
+                                                         _ptr(out), _stream()))
+    return out
+
+
+def normals_rgba(cfg: Config, pyramid, pose=None, alpha: float = 1.0):
+    """RGBA8 words [H, W] of level-0 normals, (n + 1) / 2 (world space with `pose`)."""
+    import torch
+    out = torch.empty((cfg.height, cfg.width), dtype=torch.int32, device=pyramid.device)
+    N.check("of_normals_to_rgba", N.lib().of_normals_to_rgba(
+        C.byref(cfg.camera()), _ptr(pyramid), _ptr(pose), alpha, _ptr(out), _stream()))
+    return out
+
+
 # ------------------------------------------------------------------- mesh --
 
 def extract_mesh(cfg: Config, vol, max_triangles: int | None = None, with_ids: bool = False):

@@ -30,6 +30,38 @@ __global__ void k_points_to_ref(const float4 *__restrict__ pts, int npx, const d
   if (n3) { n3[3 * p] = no.x; n3[3 * p + 1] = no.y; n3[3 * p + 2] = no.z; }
 }
 
+// rgbaFloatToIntCamera (Source/src/CameraSupport/CameraHandler.cu:55-62)
+__device__ __forceinline__ uint32_t pack_rgba(float x, float y, float z, float w) {
+  x = __saturatef(x); y = __saturatef(y); z = __saturatef(z); w = __saturatef(w);
+  return ((uint32_t)(w * 255.f) << 24) | ((uint32_t)(z * 255.f) << 16) |
+         ((uint32_t)(y * 255.f) << 8) | (uint32_t)(x * 255.f);
+}
+
+// gray depth / max depth, opaque (d_convertDepthToWorldVertices, CameraHandler.cu:75-78)
+__global__ void k_depth_rgba(const uint16_t *__restrict__ depth, int npx, float inv_max,
+                             uint32_t *__restrict__ rgba) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npx) return;
+  const float g = (float)depth[p] * inv_max;
+  rgba[p] = pack_rgba(g, g, g, 1.f);
+}
+
+// (n + 1) / 2 per channel (d_convertDepthToWorldNormals, CameraHandler.cu:128-131;
+// the raycast's show-normals mode, Raycaster.cu:214-218); an invalid normal is 0
+__global__ void k_normal_rgba(const float4 *__restrict__ pts, int npx, const double *pose,
+                              float alpha, uint32_t *__restrict__ rgba) {
+  __shared__ Rigid T;
+  if (threadIdx.x == 0 && pose) pose_to_rigid(pose, &T, nullptr);
+  __syncthreads();
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npx) return;
+  const float4 v = pts[2 * p], n = pts[2 * p + 1];
+  float3 no = make_float3(0.f, 0.f, 0.f);
+  if (v.w != 0.f && n.w != 0.f)
+    no = pose ? rotate(T, make_float3(n.x, n.y, n.z)) : make_float3(n.x, n.y, n.z);
+  rgba[p] = pack_rgba((no.x + 1.f) * 0.5f, (no.y + 1.f) * 0.5f, (no.z + 1.f) * 0.5f, alpha);
+}
+
 __global__ void k_points_from_ref(const float *__restrict__ v3, const float *__restrict__ n3,
                                   int npx, float4 *pts) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -72,3 +104,27 @@ extern "C" of_status_t of_points_from_reference(const of_camera_t *cam, int32_t 
   if (st != OF_OK) return st;
   return of_model_pyramid(cam, levels, d_model, (cudaStream_t)s);
 }
+
+extern "C" of_status_t of_depth_to_rgba(const of_camera_t *cam, const uint16_t *d_depth,
+                                        uint32_t *d_rgba, of_stream_t s) {
+  if (!of_camera_valid(cam) || !d_depth || !d_rgba || cam->max_depth_mm <= 0.f)
+    return OF_ERR_INVALID_ARGUMENT;
+  const int npx = cam->width * cam->height;
+  k_depth_rgba<<<(npx + 255) / 256, 256, 0, (cudaStream_t)s>>>(d_depth, npx,
+                                                               1.f / cam->max_depth_mm, d_rgba);
+  return of_launch_status();
+}
+
+extern "C" of_status_t of_normals_to_rgba(const of_camera_t *cam, const void *d_pyramid,
+                                          const double *d_pose, float alpha, uint32_t *d_rgba,
+                                          of_stream_t s) {
+  if (!of_camera_valid(cam) || !d_pyramid || !d_rgba) return OF_ERR_INVALID_ARGUMENT;
+  of_pyramid_layout_t lay;
+  of_status_t st = of_pyramid_layout(cam, 1, &lay);
+  if (st != OF_OK) return st;
+  const int npx = cam->width * cam->height;
+  k_normal_rgba<<<(npx + 255) / 256, 256, 0, (cudaStream_t)s>>>(
+      (const float4 *)((const char *)d_pyramid + lay.points_offset[0]), npx, d_pose, alpha, d_rgba);
+  return of_launch_status();
+}
+

@@ -146,3 +146,31 @@ def test_raw_depth_mode_matches_reference_conversion(of, ora, cuda):
     assert np.array_equal(d0, np.where(valid, raw, 0.0).astype(np.float32))
     levels, _ = ora.preprocess(cfg, seq.depth[0])
     assert np.array_equal(levels[0][0], np.where(valid, raw, 0.0))
+
+
+def _pack(x, y, z, w):
+    """rgbaFloatToIntCamera in float32 (saturate, scale, truncate)."""
+    c = [np.clip(np.asarray(a, np.float32), 0, 1) for a in (x, y, z, w)]
+    q = [(a * np.float32(255)).astype(np.uint32) for a in c]
+    return (q[3] << 24) | (q[2] << 16) | (q[1] << 8) | q[0]
+
+
+def test_headless_views(of, cuda):
+    """Depth and normal RGBA views packed as the reference packs them."""
+    import torch
+    cfg = c1(of)
+    seq = of.make_sequence(cfg, frames=1)
+    d = torch.from_numpy(seq.depth[0].astype(np.int16)).to(cuda)
+    g = of.depth_rgba(cfg, d).cpu().numpy().view(np.uint32)
+    gray = seq.depth[0].astype(np.float32) * np.float32(1.0 / cfg.max_depth_mm)
+    assert np.array_equal(g, _pack(gray, gray, gray, np.float32(1)))
+    frame = of.preprocess(cfg, d)
+    v, n = of.unpack_points(cfg, frame, 0)
+    nn = n.cpu().numpy()
+    ok = (v.cpu().numpy()[..., 3] != 0) & (nn[..., 3] != 0)
+    nv = np.where(ok[..., None], nn[..., :3], 0).astype(np.float32)
+    r = of.normals_rgba(cfg, frame, alpha=0.0).cpu().numpy().view(np.uint32)
+    h = np.float32(0.5)
+    exp = _pack((nv[..., 0] + 1) * h, (nv[..., 1] + 1) * h, (nv[..., 2] + 1) * h, np.float32(0))
+    assert np.array_equal(r, exp)
+    assert (r != _pack(h, h, h, np.float32(0))).mean() > 0.5
