@@ -296,8 +296,14 @@ def linear_to_volume(cfg: Config, q: np.ndarray, weight: np.ndarray) -> np.ndarr
     q = np.where(np.asarray(weight) == 0, one, np.asarray(q).astype(np.int64) & 0xFFFF)
     words = (q.astype(np.uint32) & 0xFFFF) | (weight.astype(np.uint32) << 16)
     words = words.reshape(nb, 8, nb, 8, nb, 8).transpose(0, 2, 4, 1, 3, 5).reshape(-1)
-    flags = np.ones(volume_bytes(cfg) - 4 * n ** 3, np.uint8)
-    return np.concatenate([words.view(np.uint8), flags]).view(np.int32)
+    # brick and super-brick flags set (near a surface), saturated-brick bytes clear
+    nbr = nb ** 3
+    ns = (nb + 3) // 4
+    tail = np.zeros(volume_bytes(cfg) - 4 * n ** 3, np.uint8)
+    tail[:nbr] = 1
+    soff = (nbr + 255) // 256 * 256
+    tail[soff:soff + ns ** 3] = 1
+    return np.concatenate([words.view(np.uint8), tail]).view(np.int32)
 
 
 # ----------------------------------------------------------------- tracker --

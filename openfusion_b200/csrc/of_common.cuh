@@ -189,6 +189,16 @@ __host__ __device__ __forceinline__ uint8_t *super_flags(void *vol, int n) {
   return brick_flags(vol, n) + ((nb * nb * nb + 255) & ~(size_t)255);
 }
 
+// One byte per brick after the super-brick flags: bit w (w = 0..3) set when,
+// after the last integration that processed the brick, its voxels 128 w ..
+// 128 w + 127 were all +1 at the maximum weight; 0xF = saturated free space.
+// Updating a saturated brick with +1 leaves every word as it is, so the tiled
+// integration does not list it for its free-space modes.
+__host__ __device__ __forceinline__ uint8_t *saturated_flags(void *vol, int n) {
+  const size_t ns = (size_t)super_count(n);
+  return super_flags(vol, n) + ((ns * ns * ns + 255) & ~(size_t)255);
+}
+
 template <int STORAGE>
 struct VoxelCodec;
 

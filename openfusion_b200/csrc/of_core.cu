@@ -111,7 +111,9 @@ extern "C" of_status_t of_volume_bytes(const of_volume_desc_t *d, size_t *bytes)
   if (!of_volume_valid(d) || !bytes) return OF_ERR_INVALID_ARGUMENT;
   size_t n = (size_t)d->resolution;
   size_t nb = n / kBrick, ns = (size_t)super_count((int)n);
-  *bytes = n * n * n * sizeof(uint32_t) + align256(nb * nb * nb) + align256(ns * ns * ns);
+  // voxel words, brick flags, super-brick flags, saturated-brick bytes
+  *bytes = n * n * n * sizeof(uint32_t) + align256(nb * nb * nb) + align256(ns * ns * ns) +
+           align256(nb * nb * nb);
   return OF_OK;
 }
 
@@ -205,6 +207,7 @@ extern "C" of_status_t of_volume_import(const of_volume_desc_t *d, void *vol, co
   size_t n = (size_t)d->resolution, nb = n / kBrick, ns = (size_t)super_count((int)n);
   OF_CUDA_TRY(cudaMemsetAsync(brick_flags(vol, (int)n), 1, nb * nb * nb, (cudaStream_t)s));
   OF_CUDA_TRY(cudaMemsetAsync(super_flags(vol, (int)n), 1, ns * ns * ns, (cudaStream_t)s));
+  OF_CUDA_TRY(cudaMemsetAsync(saturated_flags(vol, (int)n), 0, nb * nb * nb, (cudaStream_t)s));
   return OF_OK;
 }
 

@@ -305,7 +305,8 @@ __device__ __forceinline__ void integrate_brick(
     uint32_t *__restrict__ vol, uint8_t *__restrict__ flags, const of_volume_desc_t &desc,
     const Cam &cam, const uint16_t *__restrict__ depth, int pitch,
     const float2 *__restrict__ lam, const IntegrateSetup &S, const VoxelConsts &K, int t,
-    int lane, int b, int bx, int by, int bz, int mode, float3 base, unsigned &my_count) {
+    int lane, int b, int bx, int by, int bz, int mode, float3 base, unsigned &my_count,
+    int sat_old = -1) {
   const float T = K.T, inv_T = K.inv_T, dspan = K.dspan, cxh = K.cxh, cyh = K.cyh;
   const float dlo = K.dlo, dhi = K.dhi;
   const unsigned uspan = K.uspan, vspan = K.vspan;
@@ -315,6 +316,7 @@ __device__ __forceinline__ void integrate_brick(
   bool near = false;
   uint4 *p4 = reinterpret_cast<uint4 *>(vol + ((size_t)b << 9)) + t;
   uint4 wv = make_uint4(0u, 0u, 0u, 0u);
+  uint4 wfin;  // the thread's words after the update
   // listed bricks are nearly always updated: their words are loaded before
   // the depth gathers so that the two memory round trips overlap
   if (EARLY_LOAD && !CENSUS) wv = *p4;
@@ -413,7 +415,10 @@ __device__ __forceinline__ void integrate_brick(
     brick_done:
       if (CENSUS) {
         my_count += __popc(upd);
-      } else if (upd) {
+      } else if (!upd) {
+        if (!EARLY_LOAD) wv = *p4;
+        wfin = wv;
+      } else {
         if (!EARLY_LOAD) wv = *p4;
         uint32_t w4[4] = {wv.x, wv.y, wv.z, wv.w};
 #pragma unroll
@@ -431,8 +436,27 @@ __device__ __forceinline__ void integrate_brick(
           near |= (w4[m] & 0xffffu) != VoxelCodec<STORAGE>::kOneBits;
         }
         // saturated free space (+1 at the maximum weight) stays as it is
-        if (w4[0] != wv.x || w4[1] != wv.y || w4[2] != wv.z || w4[3] != wv.w)
-          *p4 = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+        wfin = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+        if (w4[0] != wv.x || w4[1] != wv.y || w4[2] != wv.z || w4[3] != wv.w) *p4 = wfin;
+      }
+      if (!CENSUS) {
+        // the brick's saturated byte: bit w belongs to the brick's warp w
+        // (voxels 128 w .. 128 w + 127), set while that warp's voxels are all
+        // +1 at the maximum weight; only a change of the warp's own state
+        // touches memory (one word atomic; the byte shares its word with three
+        // other bricks)
+        const uint32_t satw = VoxelCodec<STORAGE>::kOneBits | ((uint32_t)desc.max_weight << 16);
+        const bool sat = wfin.x == satw && wfin.y == satw && wfin.z == satw && wfin.w == satw;
+        const bool vote = __all_sync(0xffffffffu, sat);
+        if (lane == 0) {
+          unsigned *word = reinterpret_cast<unsigned *>(saturated_flags(vol, desc.resolution)) + (b >> 2);
+          const unsigned m = 1u << ((t >> 5) + 8 * (b & 3));
+          // the brick's byte as its work-list entry carries it, else from memory
+          const bool had = sat_old >= 0 ? ((sat_old >> (t >> 5)) & 1) != 0
+                                        : (*reinterpret_cast<volatile unsigned *>(word) & m) != 0u;
+          if (vote && !had) atomicOr(word, m);
+          if (!vote && had) atomicAnd(word, ~m);
+        }
       }
       // a warp that wrote a non-saturated voxel flags the brick and its 26
       // neighbours, and their super-bricks (idempotent byte stores, lanes 0..26)
@@ -529,10 +553,13 @@ __global__ void __launch_bounds__(256, 4) k_integrate(uint32_t *__restrict__ vol
 
 // of_integrate_tiled, step 2: one thread per brick. Frustum test, then the
 // whole-brick decision from the tile bounds; kept bricks are appended to the
-// work list (one atomic per warp) as {bx | by << 8 | bz << 16 | mode << 24,
-// camera-space base of the brick (3 floats)}.
+// work list (one atomic per warp) as {bx | by << 8 | bz << 16 | mode << 24 |
+// saturated-brick bits << 26, camera-space base of the brick (3 floats)}.
+// Free-space bricks whose voxels are all saturated (+1 at the maximum weight)
+// are left out: updating them would write nothing.
 __device__ __forceinline__ void classify_block(const of_volume_desc_t &desc, const Cam &cam,
                                                const float2 *__restrict__ tiles, int tiles_x,
+                                               const uint8_t *__restrict__ sat,
                                                uint4 *__restrict__ list,
                                                unsigned int *__restrict__ list_count,
                                                const FrameSetup *__restrict__ setup, int bx) {
@@ -565,10 +592,12 @@ __device__ __forceinline__ void classify_block(const of_volume_desc_t &desc, con
     if (keep) {
       const int cls = classify_brick(S, cam, tiles, tiles_x, desc.trunc_mm, hext, cx, cy, cz, bx,
                                      by, bz);
-      keep = cls >= 0;
+      // free space over saturated free space changes no word
+      const bool noop = (cls == kModeFront || cls == kModeFrontDense) && __ldg(sat + b) == 0xF;
+      keep = cls >= 0 && !noop;
       const float3 base = brick_base(S, bx, by, bz);
       entry = make_uint4((uint32_t)bx | (uint32_t)by << 8 | (uint32_t)bz << 16 |
-                             (uint32_t)max(cls, 0) << 24,
+                             (uint32_t)max(cls, 0) << 24 | (uint32_t)(__ldg(sat + b) & 0xF) << 26,
                          __float_as_uint(base.x), __float_as_uint(base.y), __float_as_uint(base.z));
     }
   }
@@ -584,10 +613,12 @@ __device__ __forceinline__ void classify_block(const of_volume_desc_t &desc, con
 __global__ void __launch_bounds__(256) k_classify_bricks(of_volume_desc_t desc, Cam cam,
                                                          const double *__restrict__ pose,
                                                          const float2 *__restrict__ tiles,
-                                                         int tiles_x, uint4 *__restrict__ list,
+                                                         int tiles_x,
+                                                         const uint8_t *__restrict__ sat,
+                                                         uint4 *__restrict__ list,
                                                          unsigned int *__restrict__ list_count,
                                                          const FrameSetup *__restrict__ setup) {
-  classify_block(desc, cam, tiles, tiles_x, list, list_count, setup, blockIdx.x);
+  classify_block(desc, cam, tiles, tiles_x, sat, list, list_count, setup, blockIdx.x);
 }
 
 // of_integrate_tiled, step 3: persistent grid over the work list, each
@@ -615,11 +646,13 @@ __device__ __forceinline__ void integrate_list_block(uint32_t *__restrict__ vol,
   for (int e = bx * 2 + half; e < n; e += gx * 2) {
     const uint4 en = __ldg(list + e);
     const int bx = (int)(en.x & 0xffu), by = (int)((en.x >> 8) & 0xffu);
-    const int bz = (int)((en.x >> 16) & 0xffu), mode = (int)(en.x >> 24);
+    const int bz = (int)((en.x >> 16) & 0xffu), mode = (int)((en.x >> 24) & 3u);
+    const int sat_old = (int)((en.x >> 26) & 0xfu);
     const int b = (bx * nb + by) * nb + bz;
     integrate_brick<STORAGE, false, true>(
         vol, flags, desc, cam, depth, pitch, lam, S, K, t, lane, b, bx, by, bz, mode,
-        make_float3(__uint_as_float(en.y), __uint_as_float(en.z), __uint_as_float(en.w)), my_count);
+        make_float3(__uint_as_float(en.y), __uint_as_float(en.z), __uint_as_float(en.w)), my_count,
+        sat_old);
   }
 }
 template <int STORAGE>
@@ -693,8 +726,8 @@ of_status_t launch_integrate_tiled(const of_volume_desc_t *d, void *vol, const o
                                               list_count, pose, *d, setup);
   const size_t nb = (size_t)(d->resolution / 8);
   const unsigned nbr = (unsigned)(nb * nb * nb);
-  k_classify_bricks<<<(nbr + 255) / 256, 256, 0, s>>>(*d, c, pose, tiles, tx, list, list_count,
-                                                       setup);
+  k_classify_bricks<<<(nbr + 255) / 256, 256, 0, s>>>(
+      *d, c, pose, tiles, tx, saturated_flags(vol, d->resolution), list, list_count, setup);
   const unsigned blocks = persistent_blocks(d);
   if (d->storage == OF_TSDF_I16)
     k_integrate_list<OF_TSDF_I16><<<blocks, 256, 0, s>>>((uint32_t *)vol, *d, c, depth, pitch, pose,
@@ -737,8 +770,8 @@ __global__ void __launch_bounds__(256) k_classify_batch(const IntJob *__restrict
                                                         const int *__restrict__ first, int n) {
   const int j = batch_job(first, n, blockIdx.x);
   const IntJob &J = jobs[j];
-  classify_block(J.desc, J.cam, J.tiles, J.tiles_x, J.list, J.count, J.setup,
-                 blockIdx.x - __ldg(first + j));
+  classify_block(J.desc, J.cam, J.tiles, J.tiles_x, saturated_flags(J.vol, J.desc.resolution),
+                 J.list, J.count, J.setup, blockIdx.x - __ldg(first + j));
 }
 template <int STORAGE>
 __global__ void __launch_bounds__(256, 4) k_integrate_list_batch(const IntJob *__restrict__ jobs,

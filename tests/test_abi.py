@@ -54,8 +54,9 @@ def test_layout_and_sizes(of):
     assert list(lay.width)[:3] == [640, 320, 160] and list(lay.height)[:3] == [480, 240, 120]
     for l in range(3):
         assert lay.depth_offset[l] % 256 == 0 and lay.points_offset[l] % 256 == 0
-    # voxels + brick flags + super-brick flags (4^3 bricks), each flag block padded to 256 B
-    assert of.volume_bytes(cfg) == 512 ** 3 * 4 + 64 ** 3 + 16 ** 3 + (256 - 16 ** 3 % 256) % 256
+    # voxels + brick flags + super-brick flags (4^3 bricks) + saturated-brick
+    # bytes, each byte block padded to 256 B
+    assert of.volume_bytes(cfg) == 512 ** 3 * 4 + 64 ** 3 + 16 ** 3 + (256 - 16 ** 3 % 256) % 256 + 64 ** 3
     c1 = of.level_camera(cfg, 1)
     assert (c1.fx, c1.cx, c1.cy) == (262.5, 159.5, 119.5)
 

@@ -162,6 +162,36 @@ def test_integrate_tiled_equals_per_voxel(of, cuda, name, res, storage, geom):
     assert (w > 0).sum() > 10000
 
 
+def test_saturated_free_space_is_skipped_exactly(of, cuda):
+    """With a maximum weight of 3, free space saturates (+1 at weight 3) after
+    three frames; the tiled integration then leaves those bricks unlisted.
+    Over 12 frames the volume, brick flags and saturated-brick bytes stay bit
+    for bit those of the per-voxel path, and saturated bricks exist."""
+    import torch
+    cfg = small(of, "c2", resolution=256, max_weight=3)
+    seq = of.make_sequence(cfg, frames=12)
+    lam, scratch = of.lambda_table(cfg, cuda), of.integrate_scratch(cfg, cuda)
+    va, vb = of.new_volume(cfg, cuda), of.new_volume(cfg, cuda)
+    for k in range(12):
+        d = torch.from_numpy(seq.depth[k].astype(np.int16)).to(cuda)
+        p = dev_pose(seq.poses[k], cuda)
+        of.integrate(cfg, va, d, p, lam)
+        of.integrate(cfg, vb, d, p, lam, scratch)
+        torch.cuda.synchronize()
+        assert torch.equal(va, vb), f"volumes differ after frame {k}"
+    host = vb.cpu().numpy().view(np.uint8)
+    n, nb = cfg.resolution, cfg.resolution // 8
+    ns = (nb + 3) // 4
+    off = 4 * n ** 3 + (nb ** 3 + 255) // 256 * 256 + (ns ** 3 + 255) // 256 * 256
+    sat = host[off:off + nb ** 3] == 0xF
+    assert 100 < int(sat.sum()) < nb ** 3
+    # a saturated brick holds only +1 at the maximum weight
+    q, w = of.volume_to_linear(cfg, vb.cpu().numpy())
+    qb = q.reshape(nb, 8, nb, 8, nb, 8).transpose(0, 2, 4, 1, 3, 5).reshape(-1, 512)
+    wb = w.reshape(nb, 8, nb, 8, nb, 8).transpose(0, 2, 4, 1, 3, 5).reshape(-1, 512)
+    assert np.all(qb[sat] == 0x7FFF) and np.all(wb[sat] == 3)
+
+
 # ---------------------------------------------------------------- raycast
 
 @pytest.mark.parametrize("name,res", [("c1", 128), ("c2", 512)])
