@@ -360,6 +360,16 @@ of_status_t of_tracker_pose(of_tracker_t tracker, double *pose, of_icp_stats_t *
 /* Copies the poses of the last `count` frames (oldest first) to host memory. */
 of_status_t of_tracker_pose_history(of_tracker_t tracker, double *poses, int32_t count,
                                     of_stream_t stream);
+/* Checkpoint / resume: the tracker's state (volume with its brick bytes,
+ * pose, pose history, frame count and the last depth frame, which the next
+ * step fuses) to one file with a header, and back into a tracker created
+ * with the same camera, volume and pose_history (else
+ * OF_ERR_INVALID_ARGUMENT). A resumed tracker continues bit for bit as the
+ * saved one would have. Synchronises `stream`; host memory for one copy of
+ * the volume is allocated during the call. The reference saves only the raw
+ * float volume (Source/src/MainApp.cpp:259-268) and the pose (:430-451). */
+of_status_t of_tracker_save(of_tracker_t tracker, const char *path, of_stream_t stream);
+of_status_t of_tracker_load(of_tracker_t tracker, const char *path, of_stream_t stream);
 /* Raw device pointers of the tracker's state, for inspection and for the
  * reference-shaped C++ wrappers. */
 typedef struct of_tracker_buffers {

@@ -141,6 +141,8 @@ _SIGS = {
     "of_tracker_destroy": (c_status, [P]),
     "of_tracker_process": (c_status, [P, P, C.c_int32, c_stream]),
     "of_tracker_flush": (c_status, [P, c_stream]),
+    "of_tracker_save": (c_status, [P, C.c_char_p, c_stream]),
+    "of_tracker_load": (c_status, [P, C.c_char_p, c_stream]),
     "of_depth_filter_defaults": (None, [C.POINTER(DepthFilterParams)]),
     "of_depth_filter": (c_status, [C.POINTER(Camera), C.POINTER(DepthFilterParams), P, P, P,
                                    c_stream]),

@@ -361,6 +361,18 @@ class Tracker:
         frame before it); call before reading the volume or the model."""
         N.check("of_tracker_flush", N.lib().of_tracker_flush(self._h, _stream(stream)))
 
+    def save(self, path, stream=None):
+        """Checkpoint: volume, pose, history, frame count, last frame (of_tracker_save)."""
+        N.check("of_tracker_save", N.lib().of_tracker_save(self._h, str(path).encode(),
+                                                           _stream(stream)))
+
+    def load(self, path, stream=None):
+        """Resume from a checkpoint of the same configuration (of_tracker_load)."""
+        N.check("of_tracker_load", N.lib().of_tracker_load(self._h, str(path).encode(),
+                                                           _stream(stream)))
+        b = self.buffers()
+        self.frames = int(b.frames)
+
     def set_prior(self, delta: np.ndarray | None):
         arr = None if delta is None else (C.c_double * 16)(*np.asarray(delta, np.float64).reshape(16))
         N.check("of_tracker_set_prior", N.lib().of_tracker_set_prior(self._h, arr))

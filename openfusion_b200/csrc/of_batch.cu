@@ -319,6 +319,7 @@ extern "C" of_status_t of_batch_destroy(of_batch_t b) {
 
 extern "C" of_status_t of_batch_process(of_batch_t b, const uint16_t *const *depth,
                                         int32_t depth_is_host, of_stream_t stream) {
+  OF_RANGE("of_batch_process");
   if (!b || !depth) return OF_ERR_INVALID_ARGUMENT;
   const int n = b->desc.count;
   for (int i = 0; i < n; ++i)

@@ -1028,6 +1028,7 @@ extern "C" of_status_t of_cnn_predict(const uint16_t *d_params, const float *d_m
                                       const uint16_t *d_prev, const uint16_t *d_cur, int32_t width,
                                       int32_t height, const double *d_prev_pose, float *d_out,
                                       double *d_warm_pose, of_stream_t s) {
+  OF_RANGE("of_cnn_predict");
   if (!d_params || !d_master || !d_prev || !d_cur || (d_warm_pose && !d_prev_pose) ||
       ((uintptr_t)d_params & 15u) || width % kInW || height % kInH || width / kInW != height / kInH ||
       (width / kInW != 1 && width / kInW != 2 && width / kInW != 4 && width / kInW != 8) ||

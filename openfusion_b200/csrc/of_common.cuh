@@ -14,6 +14,17 @@
 
 #include "openfusion_b200.h"
 
+#include <nvtx3/nvToolsExt.h>
+
+// An NVTX range around a C-ABI call (visible in Nsight timelines; near-zero
+// cost when no tool is attached). Host-side only: a graph replay shows the
+// call that launched it, not the captured stages.
+struct OfNvtxRange {
+  explicit OfNvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~OfNvtxRange() { nvtxRangePop(); }
+};
+#define OF_RANGE(name) OfNvtxRange of_nvtx_range_(name)
+
 #define OF_CUDA_TRY(expr)                                   \
   do {                                                      \
     cudaError_t _e = (expr);                                \

@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(kFx * kFy) k_undistort(const uint16_t *__restr
 dim3 grid_of(int w, int h) { return dim3((w + kFx - 1) / kFx, (h + kFy - 1) / kFy); }
 
 bool filter_params_ok(const of_depth_filter_params_t *p) {
-  return p && (p->steps & ~0x1F) == 0 && p->null_value >= 0 && p->null_value <= 0xFFFF &&
+  return p && (p->steps & ~0xF) == 0 && p->null_value >= 0 && p->null_value <= 0xFFFF &&
          p->average_passes >= 0 && p->average_passes <= 4 && p->average_threshold_mm >= 0.f &&
          p->gradient_threshold_mm >= 0.f;
 }
@@ -194,6 +194,7 @@ extern "C" of_status_t of_depth_filter_step(const of_camera_t *cam, int32_t kind
 extern "C" of_status_t of_depth_filter(const of_camera_t *cam, const of_depth_filter_params_t *p,
                                        const uint16_t *d_in, uint16_t *d_out, uint16_t *d_scratch,
                                        of_stream_t stream) {
+  OF_RANGE("of_depth_filter");
   if (!of_camera_valid(cam) || !filter_params_ok(p) || !d_in || !d_out) return OF_ERR_INVALID_ARGUMENT;
   cudaStream_t s = (cudaStream_t)stream;
   const size_t bytes = (size_t)cam->width * cam->height * sizeof(uint16_t);

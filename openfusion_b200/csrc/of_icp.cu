@@ -957,6 +957,7 @@ of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, con
 extern "C" of_status_t of_icp_track(const of_camera_t *cam, const of_icp_params_t *ip,
                                     const void *d_frame, const void *d_model, double *pose,
                                     void *d_ws, of_icp_stats_t *stats, of_stream_t s) {
+  OF_RANGE("of_icp_track");
   if (!of_camera_valid(cam) || !icp_params_ok(ip) || !d_frame || !d_model || !pose || !d_ws)
     return OF_ERR_INVALID_ARGUMENT;
   return of_icp_launch(cam, ip, d_frame, d_model, pose, d_ws, stats, (cudaStream_t)s, nullptr);
@@ -966,6 +967,7 @@ extern "C" of_status_t of_icp_track_warm(const of_camera_t *cam, const of_icp_pa
                                          const void *d_frame, const void *d_model, double *pose,
                                          const double *d_warm_pose, void *d_ws,
                                          of_icp_stats_t *stats, of_stream_t s) {
+  OF_RANGE("of_icp_track_warm");
   if (!of_camera_valid(cam) || !icp_params_ok(ip) || !d_frame || !d_model || !pose ||
       !d_warm_pose || !d_ws)
     return OF_ERR_INVALID_ARGUMENT;

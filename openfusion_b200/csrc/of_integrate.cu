@@ -897,6 +897,7 @@ of_status_t integrate_batch_launch(const IntegrateBatch *b, int parity, const Ba
 extern "C" of_status_t of_integrate(const of_volume_desc_t *d, void *vol, const of_camera_t *cam,
                                     const uint16_t *depth, int32_t pitch, const double *pose,
                                     const float *lam, of_stream_t s) {
+  OF_RANGE("of_integrate");
   if (!of_volume_valid(d) || !of_camera_valid(cam) || !vol || !depth || !pose || !lam ||
       pitch < cam->width)
     return OF_ERR_INVALID_ARGUMENT;
@@ -914,6 +915,7 @@ extern "C" of_status_t of_integrate_tiled(const of_volume_desc_t *d, void *vol,
                                           const of_camera_t *cam, const uint16_t *depth,
                                           int32_t pitch, const double *pose, const float *lam,
                                           void *scratch, of_stream_t s) {
+  OF_RANGE("of_integrate_tiled");
   if (!of_volume_valid(d) || !of_camera_valid(cam) || !vol || !depth || !pose || !lam ||
       !scratch || pitch < cam->width || ((uintptr_t)scratch & 255u))
     return OF_ERR_INVALID_ARGUMENT;

@@ -177,6 +177,7 @@ __global__ void __launch_bounds__(kMeshThreads) k_mesh(const uint32_t *__restric
 extern "C" of_status_t of_mesh_extract(const of_volume_desc_t *d, const void *vol, float *d_tris,
                                        uint64_t *d_ids, uint32_t max_triangles, uint32_t *d_count,
                                        of_stream_t stream) {
+  OF_RANGE("of_mesh_extract");
   if (!of_volume_valid(d) || !vol || !d_count || (max_triangles > 0 && !d_tris))
     return OF_ERR_INVALID_ARGUMENT;
   cudaStream_t s = (cudaStream_t)stream;

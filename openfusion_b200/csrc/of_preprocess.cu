@@ -429,6 +429,7 @@ of_status_t preprocess_batch_launch(const PreprocessBatch *b, int parity, cudaSt
 extern "C" of_status_t of_preprocess(const of_camera_t *cam, const of_filter_params_t *fp,
                                      const uint16_t *d_depth, int32_t pitch, void *d_frame,
                                      of_stream_t stream) {
+  OF_RANGE("of_preprocess");
   if (!of_camera_valid(cam) || !fp || !d_depth || !d_frame || pitch < cam->width)
     return OF_ERR_INVALID_ARGUMENT;
   if (fp->levels < 1 || fp->levels > kMaxLevels || fp->sigma_space_px <= 0.f ||

@@ -460,6 +460,7 @@ extern "C" of_status_t of_raycast(const of_volume_desc_t *d, const void *vol,
                                   const of_camera_t *cam, const of_raycast_params_t *rp,
                                   int32_t levels, const double *pose, void *d_model,
                                   uint32_t *rgba, of_stream_t stream) {
+  OF_RANGE("of_raycast");
   if (!of_volume_valid(d) || !of_camera_valid(cam) || !rp || !vol || !pose || !d_model)
     return OF_ERR_INVALID_ARGUMENT;
   if (levels < 1 || levels > kMaxLevels || rp->min_step_vox <= 0.f || rp->far_step_frac < 0.f ||

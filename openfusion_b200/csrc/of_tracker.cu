@@ -15,7 +15,9 @@
 #include "of_common.cuh"
 
 #include <new>
+#include <stdio.h>
 #include <string.h>
+#include <vector>
 
 using namespace of;
 
@@ -281,6 +283,7 @@ extern "C" of_status_t of_tracker_destroy(of_tracker_t t) {
 
 extern "C" of_status_t of_tracker_process(of_tracker_t t, const uint16_t *depth, int32_t on_host,
                                           of_stream_t stream) {
+  OF_RANGE("of_tracker_process");
   if (!t || !depth) return OF_ERR_INVALID_ARGUMENT;
   cudaStream_t s = (cudaStream_t)stream;
   const int cur = (int)(t->frames & 1);
@@ -358,3 +361,130 @@ extern "C" of_status_t of_tracker_buffers(of_tracker_t t, of_tracker_buffers_t *
   out->kernels_track = t->kernels_track;
   return OF_OK;
 }
+
+// ---------------------------------------------------------- checkpoints --
+//
+// A tracker's state as one file: a header (what the state belongs to and the
+// scalars), then the pose history, the last depth frame (the next step fuses
+// it) and the whole volume buffer (voxel words and the brick bytes). The
+// frame and model pyramids are not saved: the next step recomputes both.
+// The reference saves the raw float volume only (SavedVolume.raw,
+// Source/src/MainApp.cpp:259-268) and the pose on a key press (:430-451).
+
+namespace {
+
+struct CheckpointHeader {
+  char magic[8];  // "OFCKPT1\0"
+  int32_t abi_version;
+  int32_t width, height;
+  int32_t resolution, storage;
+  float size_mm, trunc_mm;
+  int32_t max_weight;
+  int32_t last_fused;
+  int64_t frames;
+  int32_t hist_cap;
+  int32_t pad;
+  uint64_t hist_count;
+  uint64_t volume_bytes;
+  double pose[16];
+};
+
+const char kCheckpointMagic[8] = {'O', 'F', 'C', 'K', 'P', 'T', '1', 0};
+
+of_status_t write_all(FILE *f, const void *p, size_t n) {
+  return fwrite(p, 1, n, f) == n ? OF_OK : OF_ERR_IO;
+}
+of_status_t read_all(FILE *f, void *p, size_t n) {
+  return fread(p, 1, n, f) == n ? OF_OK : OF_ERR_IO;
+}
+
+}  // namespace
+
+extern "C" of_status_t of_tracker_save(of_tracker_t t, const char *path, of_stream_t stream) {
+  if (!t || !path) return OF_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = (cudaStream_t)stream;
+  OF_CUDA_TRY(cudaStreamSynchronize(s));
+  const of_tracker_desc_t &d = t->desc;
+  size_t vol_bytes = 0;
+  of_volume_bytes(&d.volume, &vol_bytes);
+  const size_t px = (size_t)d.camera.width * d.camera.height;
+  CheckpointHeader h;
+  memset(&h, 0, sizeof(h));
+  memcpy(h.magic, kCheckpointMagic, 8);
+  h.abi_version = OF_ABI_VERSION;
+  h.width = d.camera.width;
+  h.height = d.camera.height;
+  h.resolution = d.volume.resolution;
+  h.storage = d.volume.storage;
+  h.size_mm = d.volume.size_mm;
+  h.trunc_mm = d.volume.trunc_mm;
+  h.max_weight = d.volume.max_weight;
+  h.last_fused = t->last_fused ? 1 : 0;
+  h.frames = t->frames;
+  h.hist_cap = t->hist_cap;
+  h.volume_bytes = vol_bytes;
+  std::vector<double> hist((size_t)t->hist_cap * 16);
+  std::vector<uint16_t> depth(px);
+  std::vector<char> vol(vol_bytes);
+  OF_CUDA_TRY(cudaMemcpy(h.pose, t->pose, sizeof(h.pose), cudaMemcpyDeviceToHost));
+  OF_CUDA_TRY(cudaMemcpy(&h.hist_count, t->hist_count, sizeof(h.hist_count), cudaMemcpyDeviceToHost));
+  OF_CUDA_TRY(cudaMemcpy(hist.data(), t->hist, hist.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  if (t->frames > 0)
+    OF_CUDA_TRY(cudaMemcpy(depth.data(), t->depth[(t->frames - 1) & 1], px * sizeof(uint16_t),
+                           cudaMemcpyDeviceToHost));
+  OF_CUDA_TRY(cudaMemcpy(vol.data(), t->volume, vol_bytes, cudaMemcpyDeviceToHost));
+  FILE *f = fopen(path, "wb");
+  if (!f) return OF_ERR_IO;
+  of_status_t st = write_all(f, &h, sizeof(h));
+  if (st == OF_OK) st = write_all(f, hist.data(), hist.size() * sizeof(double));
+  if (st == OF_OK) st = write_all(f, depth.data(), px * sizeof(uint16_t));
+  if (st == OF_OK) st = write_all(f, vol.data(), vol_bytes);
+  if (fclose(f) != 0 && st == OF_OK) st = OF_ERR_IO;
+  return st;
+}
+
+extern "C" of_status_t of_tracker_load(of_tracker_t t, const char *path, of_stream_t stream) {
+  if (!t || !path) return OF_ERR_INVALID_ARGUMENT;
+  const of_tracker_desc_t &d = t->desc;
+  FILE *f = fopen(path, "rb");
+  if (!f) return OF_ERR_IO;
+  CheckpointHeader h;
+  of_status_t st = read_all(f, &h, sizeof(h));
+  size_t vol_bytes = 0;
+  of_volume_bytes(&d.volume, &vol_bytes);
+  const size_t px = (size_t)d.camera.width * d.camera.height;
+  if (st == OF_OK &&
+      (memcmp(h.magic, kCheckpointMagic, 8) != 0 || h.abi_version != OF_ABI_VERSION ||
+       h.width != d.camera.width || h.height != d.camera.height ||
+       h.resolution != d.volume.resolution || h.storage != d.volume.storage ||
+       h.size_mm != d.volume.size_mm || h.trunc_mm != d.volume.trunc_mm ||
+       h.max_weight != d.volume.max_weight || h.volume_bytes != vol_bytes ||
+       h.hist_cap != t->hist_cap || h.frames < 0))
+    st = OF_ERR_INVALID_ARGUMENT;  // a checkpoint of another configuration
+  std::vector<double> hist;
+  std::vector<uint16_t> depth;
+  std::vector<char> vol;
+  if (st == OF_OK) {
+    hist.resize((size_t)t->hist_cap * 16);
+    depth.resize(px);
+    vol.resize(vol_bytes);
+    st = read_all(f, hist.data(), hist.size() * sizeof(double));
+    if (st == OF_OK) st = read_all(f, depth.data(), px * sizeof(uint16_t));
+    if (st == OF_OK) st = read_all(f, vol.data(), vol_bytes);
+  }
+  fclose(f);
+  if (st != OF_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  OF_CUDA_TRY(cudaStreamSynchronize(s));
+  OF_CUDA_TRY(cudaMemcpy(t->pose, h.pose, sizeof(h.pose), cudaMemcpyHostToDevice));
+  OF_CUDA_TRY(cudaMemcpy(t->hist_count, &h.hist_count, sizeof(h.hist_count), cudaMemcpyHostToDevice));
+  OF_CUDA_TRY(cudaMemcpy(t->hist, hist.data(), hist.size() * sizeof(double), cudaMemcpyHostToDevice));
+  if (h.frames > 0)
+    OF_CUDA_TRY(cudaMemcpy(t->depth[(h.frames - 1) & 1], depth.data(), px * sizeof(uint16_t),
+                           cudaMemcpyHostToDevice));
+  OF_CUDA_TRY(cudaMemcpy(t->volume, vol.data(), vol_bytes, cudaMemcpyHostToDevice));
+  t->frames = h.frames;
+  t->last_fused = h.last_fused != 0;
+  return OF_OK;
+}
+

@@ -408,3 +408,74 @@ def test_tracker_follows_ground_truth(of, cuda):
     errs = [pose_error(hist[k], seq.poses[k]) for k in range(30)]
     assert max(e[1] for e in errs) < 5.0, errs
     assert max(e[0] for e in errs) < np.radians(0.5)
+
+
+def test_tracker_checkpoint_resume(of, cuda, tmp_path):
+    """A tracker saved after 5 frames and loaded into a fresh tracker (graph
+    or eager) continues bit for bit as the saved one: poses of frames 5..9,
+    the pose history, and the final volume."""
+    import ctypes as C
+    import torch
+    cfg = small(of, "c1", resolution=64)
+    seq = of.make_sequence(cfg, frames=10)
+    depth = [torch.from_numpy(seq.depth[k].astype(np.int16)).to(cuda) for k in range(10)]
+    a = of.Tracker(cfg, seq.poses[0])
+    for k in range(5):
+        a.process(depth[k])
+    a.save(tmp_path / "t.ofck")
+    b = of.Tracker(cfg, np.eye(4), use_graph=False)
+    b.load(tmp_path / "t.ofck")
+    assert b.frames == 5
+    for k in range(5, 10):
+        a.process(depth[k])
+        b.process(depth[k])
+    assert np.array_equal(a.pose_history(10), b.pose_history(10))
+    a.flush()
+    b.flush()
+    torch.cuda.synchronize()
+    lib, st = of._native.lib(), torch.cuda.current_stream().cuda_stream
+    m = cfg.resolution ** 3
+    outs = []
+    for tr in (a, b):
+        t_ = torch.empty(m, dtype=torch.float32, device=cuda)
+        w_ = torch.empty(m, dtype=torch.int16, device=cuda)
+        assert lib.of_volume_export(C.byref(cfg.volume()), C.c_void_p(tr.buffers().volume),
+                                    t_.data_ptr(), w_.data_ptr(), st) == 0
+        torch.cuda.synchronize()
+        outs.append((t_.cpu().numpy(), w_.cpu().numpy()))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    # a checkpoint of another volume is refused
+    other = of.Tracker(small(of, "c1", resolution=32), seq.poses[0])
+    from openfusion_b200._native import OpenFusionError
+    with pytest.raises(OpenFusionError) as e:
+        other.load(tmp_path / "t.ofck")
+    assert e.value.status == 1
+    for tr in (a, b, other):
+        tr.close()
+
+
+def test_tracker_survives_corrupt_frames(of, cuda):
+    """Faults injected on the host: an empty frame (no depth at all) makes ICP
+    singular, so the pose of the frame before stays and the status says so; a
+    frame of uniform noise is tracked without error and the pose stays finite;
+    good frames after them are processed as usual."""
+    import torch
+    cfg = small(of, "c1")
+    seq = of.make_sequence(cfg, frames=8)
+    tr = of.Tracker(cfg, seq.poses[0])
+    for k in range(4):
+        tr.process(torch.from_numpy(seq.depth[k].astype(np.int16)).to(cuda))
+    tr.process(torch.zeros((cfg.height, cfg.width), dtype=torch.int16, device=cuda))
+    _, st4 = tr.pose()
+    assert st4.status == 1  # singular system: no correspondences
+    rng = np.random.default_rng(3)
+    noise = rng.integers(0, 65536, (cfg.height, cfg.width)).astype(np.uint16).view(np.int16)
+    tr.process(torch.from_numpy(noise).to(cuda))
+    _, st5 = tr.pose()
+    assert st5.status in (0, 1)
+    for k in range(6, 8):
+        tr.process(torch.from_numpy(seq.depth[k].astype(np.int16)).to(cuda))
+    hist = tr.pose_history(8)
+    tr.close()
+    assert np.array_equal(hist[4], hist[3])  # singular: the pose stays
+    assert np.all(np.isfinite(hist))
