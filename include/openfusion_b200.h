@@ -256,7 +256,7 @@ of_status_t of_icp_track_warm(const of_camera_t *cam, const of_icp_params_t *par
  * a fixed memory budget, or real-time loops where cudaMalloc's implicit
  * synchronisation and a possible failure mid-session are not acceptable. It
  * allocates nothing: its scratch is one file-scope device array of about
- * 115 KB (per-block partial sums for at most 296 cooperating blocks) that every
+ * 186 KB (per-block partial sums for at most 296 cooperating blocks) that every
  * GPU loading the library holds until the process exits; a device that would
  * need more blocks gets OF_ERR_TOO_LARGE. The first call on a device looks up
  * and zeroes that array (with the device current) and should come before any

@@ -38,7 +38,11 @@ constexpr float kEps = 1e-6f;  // _EPSILON_ (Constants.h:14)
 
 constexpr int kFusedThreads = 1024;
 constexpr int kFusedMaxBlocks = 2 * kSmCount;
-constexpr int kSeqSlot = 31;  // word of a partial-sum row that carries its sequence number
+// A partial-sum row slot of the fused kernel is one 64-bit word: the value's
+// bits, and above them the slot's sequence number (the frame's epoch << 13 |
+// the iteration + 1), so a reader that sees the number sees the value with it.
+constexpr int kIterBits = 13;  // up to 2 passes x 4 levels x 1000 iterations
+constexpr unsigned kEpochMask = (1u << (32 - kIterBits)) - 1u;
 // A grid barrier gives up after about 0.15 s (this many 32 ns sleeps) and
 // reports status 2 instead of waiting forever.
 constexpr unsigned kSpinLimit = 1u << 22;
@@ -59,8 +63,11 @@ struct IcpWorkspace {
   int has_warm;
   int pad2;
   float partials[kIcpMaxBlocks][32];
-  float fused_partials[2][kFusedMaxBlocks][32];
+  unsigned long long fused_rows[2][kFusedMaxBlocks][32];
+  unsigned int epoch;  // frames begun on this workspace (k_icp_begin), mod 2^19
+  unsigned int magic;  // kWorkspaceMagic once k_icp_begin has cleared the rows
 };
+constexpr unsigned kWorkspaceMagic = 0x4F46494Bu;
 
 enum IcpMode { kModeUpdate = 0, kModeSystem = 1 };
 
@@ -307,6 +314,14 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
 __device__ __forceinline__ void st_release_gpu(unsigned *p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ unsigned long long ld_relaxed_gpu(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_gpu(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
 // Waits (acquire) until *p == v; gives up after kSpinLimit polls or as soon as
 // another block has reported a failed wait. Returns whether *p reached v.
 __device__ __forceinline__ bool wait_seq(IcpWorkspace *ws, const unsigned *p, unsigned v) {
@@ -543,6 +558,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   // frame's starting pose (pose == ws->pose_init); pass 1, from the starting
   // pose, runs only when the judge replaces the warm-started result
   const bool warm = ws->has_warm != 0;
+  const unsigned epoch = ws->epoch;
   if (threadIdx.x < 16) s_pose[threadIdx.x] = warm ? ws->warm_pose[threadIdx.x] : pose[threadIdx.x];
   if (threadIdx.x == 0) {
     s_stop = 0; s_err = 0; s_its = 0; s_inl = 0; s_res = 0.0; s_piv = 0.0; s_examined = 0;
@@ -660,7 +676,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         }
         __syncthreads();
         const int buf = iter_global & 1;
-        const unsigned seq = (unsigned)iter_global + 1u;
+        const unsigned seq = (epoch << kIterBits) | (unsigned)(iter_global + 1);
         if (warp == 0) {
           float y[kWarps];
 #pragma unroll
@@ -669,44 +685,55 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
           for (int span = 1; span < kWarps; span *= 2)
 #pragma unroll
             for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
-          // publish: the values, then (release) the row's sequence number
-          float *row = ws->fused_partials[buf][blockIdx.x];
-          if (lane < kSeqSlot) row[lane] = lane <= kVals ? y[0] : 0.f;
-          __syncwarp();
-          if (lane == 0) st_release_gpu(reinterpret_cast<unsigned *>(row + kSeqSlot), seq);
+          // publish: each value with this iteration's sequence number in one
+          // 64-bit store (no fence: a slot validates itself)
+          if (lane <= kVals)
+            st_relaxed_gpu(&ws->fused_rows[buf][blockIdx.x][lane],
+                           (unsigned long long)__float_as_uint(y[0]) |
+                               ((unsigned long long)seq << 32));
           // the fault-injection hook: an arrival that never comes
-          if (hold && lane == 0 && !wait_seq(ws, &ws->bar_gen, 0xffffffffu))
+          if (hold && lane == 0 && !wait_seq(ws, &ws->bar_gen, 0xffffffffu)) {
             atomicExch(&ws->error, 1);
+            s_err = 1;
+          }
         }
-        // every block: wait for each block's row of this iteration (acquire),
-        // then Kahan over its strided share of the rows and a tree over the
-        // groups, in a fixed order. The acquire of a row's sequence number is
-        // this iteration's grid barrier.
+        // every block: wait for each block's row of this iteration, then
+        // Kahan over its strided share of the rows and a tree over the
+        // groups, in a fixed order. Seeing every slot of this iteration is
+        // this iteration's grid barrier. Lane v of warp g reads value v of
+        // rows g, g + 32, ...; a round re-reads only the slots not yet seen.
         {
           constexpr int kPer = (kFusedMaxBlocks + kWarps - 1) / kWarps;
-          static_assert(kPer <= 32, "one polling lane per row");
           const int v = lane, grp = warp;
-          // lane q < kPer polls row grp + q * kWarps; all of the warp's rows
-          // are polled in parallel, then every lane reads its value of each row
-          const int rq = grp + lane * kWarps;
-          const unsigned *seq_q = reinterpret_cast<const unsigned *>(
-              ws->fused_partials[buf][lane < kPer && rq < (int)gridDim.x ? rq : 0] + kSeqSlot);
-          const bool need = lane < kPer && rq < (int)gridDim.x;
+          float vals[kPer];
+          unsigned pending = 0;
+#pragma unroll
+          for (int q = 0; q < kPer; ++q) {
+            vals[q] = 0.f;
+            if (v <= kVals && grp + q * kWarps < (int)gridDim.x) pending |= 1u << q;
+          }
           unsigned spins = 0;
-          while (!__all_sync(0xffffffffu, !need || ld_acquire_gpu(seq_q) == seq)) {
+          for (;;) {
+#pragma unroll
+            for (int q = 0; q < kPer; ++q) {
+              if (!((pending >> q) & 1u)) continue;
+              const unsigned long long w =
+                  ld_relaxed_gpu(&ws->fused_rows[buf][grp + q * kWarps][v]);
+              if ((unsigned)(w >> 32) == seq) {
+                vals[q] = __uint_as_float((unsigned)w);
+                pending &= ~(1u << q);
+              }
+            }
+            if (__all_sync(0xffffffffu, pending == 0u)) break;
             if (++spins > kSpinLimit ||
                 ((spins & 255u) == 0u && ld_acquire_gpu(reinterpret_cast<unsigned *>(&ws->error)))) {
-              if (lane == 0) atomicExch(&ws->error, 1);
+              if (lane == 0) {
+                atomicExch(&ws->error, 1);
+                s_err = 1;
+              }
               break;
             }
             __nanosleep(32);
-          }
-          __syncwarp();  // the polling lanes' acquires precede every lane's reads
-          float vals[kPer];
-#pragma unroll
-          for (int q = 0; q < kPer; ++q) {
-            const int r = grp + q * kWarps;
-            vals[q] = (v <= kVals && r < (int)gridDim.x) ? __ldcg(&ws->fused_partials[buf][r][v]) : 0.f;
           }
           float sum = 0.f, c = 0.f;
 #pragma unroll
@@ -718,9 +745,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
           }
           s_red[grp][v] = sum - c;
         }
-        __syncthreads();
-        // a wait that gave up ends this frame's tracking in every block
-        if (threadIdx.x == 0) s_err = ld_acquire_gpu(reinterpret_cast<unsigned *>(&ws->error)) != 0u;
+        // a wait that gave up (here or, later, in every other block) ends this
+        // frame's tracking; the final status reads the workspace's flag
         __syncthreads();
         if (s_err) break;
         if (threadIdx.x < 32) {
@@ -791,10 +817,20 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
 // FP64 pose), clear the flags.
 __global__ void k_icp_begin(double *pose, IcpWorkspace *ws, of_icp_stats_t *stats,
                             const double *warm) {
-  // no partial-sum row of this frame has been published yet
-  for (int i = threadIdx.x; i < 2 * kFusedMaxBlocks; i += blockDim.x)
-    reinterpret_cast<unsigned *>(ws->fused_partials[i / kFusedMaxBlocks][i % kFusedMaxBlocks])[kSeqSlot] = 0u;
+  // a new epoch: no slot carries this frame's sequence numbers yet. Slots are
+  // cleared when the epoch wraps (every 2^19 frames), so an old slot never
+  // matches a new number.
+  // (and on a workspace's first use, whatever its memory held)
+  const bool fresh = ws->magic != kWorkspaceMagic;
+  const unsigned epoch = fresh ? 1u : (ws->epoch + 1u) & kEpochMask;
+  if (epoch == 0u || fresh) {
+    unsigned long long *rows = &ws->fused_rows[0][0][0];
+    for (int i = threadIdx.x; i < 2 * kFusedMaxBlocks * 32; i += blockDim.x) rows[i] = 0ull;
+  }
+  __syncthreads();
   if (threadIdx.x != 0) return;
+  ws->epoch = epoch == 0u ? 1u : epoch;
+  ws->magic = kWorkspaceMagic;
   if (ws->has_prior) {
     double O[16];
     for (int i = 0; i < 16; ++i) O[i] = pose[i];
@@ -1006,7 +1042,7 @@ extern "C" of_status_t of_icp_system(const of_camera_t *cam, const of_icp_params
 // budget or real-time loops where cudaMalloc's implicit synchronisation and a
 // possible failure mid-session are not acceptable), of_icp_track_static uses a
 // workspace that lives in this file-scope array instead. Every GPU that loads
-// the library holds it (sizeof(IcpWorkspace), about 115 KB) until the process
+// the library holds it (sizeof(IcpWorkspace), about 186 KB) until the process
 // exits. It holds the per-block partial sums of at most kFusedMaxBlocks
 // cooperating blocks.
 static __device__ __align__(256) unsigned char g_static_icp_ws[sizeof(IcpWorkspace)];
