@@ -114,7 +114,7 @@ __device__ inline void pose_to_rigid(const double *P, Rigid *c2w, Rigid *w2c) {
       double acc = 0.0;
       for (int j = 0; j < 3; ++j) {
         w2c->r[3 * i + j] = (float)P[4 * j + i];
-        acc -= P[4 * j + i] * P[4 * j + 3];
+        acc = fma(-P[4 * j + i], P[4 * j + 3], acc);
       }
       w2c->t[i] = (float)acc;
     }

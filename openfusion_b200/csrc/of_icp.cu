@@ -299,6 +299,11 @@ struct IcpPlan {
   float stop_rot, stop_trans;  // early exit (0: every iteration)
   float judge_rms, judge_frac, judge_rot, judge_trans;
   int warm_levels;  // levels of a warm-started pass (<= levels)
+  // optional pose history (a ring of hist_cap row-major poses and its running
+  // count): the final pose is appended by the kernel's last store
+  double *hist;
+  unsigned long long *hist_count;
+  int hist_cap;
 };
 
 // Grid-wide exchange of a co-resident grid. Each block publishes its row of
@@ -335,13 +340,15 @@ __device__ __forceinline__ bool wait_seq(IcpWorkspace *ws, const unsigned *p, un
   return true;
 }
 
-// 1 / d for a positive FP64 d by one Newton step r <- r + r (1 - d r) from
-// the FP32 reciprocal: the step squares the relative error (2^-23 -> 2^-46),
-// seven orders of magnitude below the FP32 rounding of the summed system.
+// 1 / d for a positive normal FP64 d: the approximate FP64 reciprocal of the
+// PTX ISA (rcp.approx.ftz.f64, a relative error of at most about 2^-20)
+// refined by two Newton-Raphson steps r <- r + r (1 - d r), each of which
+// squares the relative error (to below 2^-80, under FP64 rounding). It stays
+// on the FP64 pipe (no conversion to FP32 and back).
 __device__ __forceinline__ double recip_pos(double d) {
-  const float df = (float)d;
-  if (!(df > 1e-30f && df < 1e30f)) return 1.0 / d;
-  const double r = (double)__frcp_rn(df);
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+  r = fma(r, fma(-d, r, 1.0), r);
   return fma(r, fma(-d, r, 1.0), r);
 }
 
@@ -400,7 +407,9 @@ __device__ __forceinline__ void sincos_small(double x, double *s, double *c) {
 // (ICP.cpp:162-168), dT = [Rz(g) Ry(b) Rx(a) | t] (ICP.cu:274-290) and
 // P <- dT P with one entry per lane. Returns the warp-uniform success flag;
 // *minpiv gets min d_j / max H_ii, *inc_rot / *inc_trans the largest
-// rotation (rad) / translation (mm) component of the increment.
+// rotation (rad) / translation (mm) component of the increment. With c2w /
+// w2c given, the lanes also write the FP32 rigid transforms of the new pose
+// (pose_to_rigid's values) on success.
 __device__ __forceinline__ double shfl_d(double v, int src) {
   return __shfl_sync(0xffffffffu, v, src);
 }
@@ -408,7 +417,7 @@ __device__ __forceinline__ int upper_index(int i, int j) {  // i <= j
   return i * 6 - i * (i - 1) / 2 + (j - i);
 }
 __device__ bool warp_solve_update(const float *tot, double *P, double *minpiv, float *inc_rot,
-                                  float *inc_trans) {
+                                  float *inc_trans, Rigid *c2w = nullptr, Rigid *w2c = nullptr) {
   const int lane = threadIdx.x & 31;
   const int row = lane < 6 ? lane : 5;  // lanes 6.. shadow row 5
   double a[7];
@@ -462,6 +471,28 @@ __device__ bool warp_solve_update(const float *tot, double *P, double *minpiv, f
   const double v = fma(D0, P[c], fma(D1, P[4 + c], fma(D2, P[8 + c], D3 * P[12 + c])));
   __syncwarp();
   if (lane < 12) P[lane] = v;
+  if (c2w) {
+    // entry (r, c) of the new pose is v on lane 4 r + c (lanes 0..11)
+    if (lane < 12) {
+      if (c < 3) {
+        c2w->r[3 * r + c] = (float)v;
+        w2c->r[3 * c + r] = (float)v;
+      } else {
+        c2w->t[r] = (float)v;
+      }
+    }
+    // w2c.t[i] = -(column i of R) . t, lane i < 3
+    const int ci = lane < 3 ? lane : 0;
+    const double r0 = shfl_d(v, ci), r1 = shfl_d(v, 4 + ci), r2 = shfl_d(v, 8 + ci);
+    const double t0 = shfl_d(v, 3), t1 = shfl_d(v, 7), t2 = shfl_d(v, 11);
+    if (lane < 3) {
+      double acc = 0.0;
+      acc = fma(-r0, t0, acc);
+      acc = fma(-r1, t1, acc);
+      acc = fma(-r2, t2, acc);
+      w2c->t[lane] = (float)acc;
+    }
+  }
   __syncwarp();
   return true;
 }
@@ -657,8 +688,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         // pairwise sums: a recursive-halving exchange across the warp (lanes
         // trade half of their remaining values each step, 31 shuffles for 32
         // values) leaves lane v with the warp's sum of value v; then a tree
-        // over the block's warps. Value kVals is the examined-point count.
-        {
+        // over the block's warps. Value kVals is the examined-point count. A
+        // warp that examined no point (the coarse levels leave most warps
+        // idle) holds only +0 and writes its zeros directly.
+        if (!__any_sync(0xffffffffu, examined > 0.f)) {
+          s_red[warp][lane] = 0.f;
+        } else {
           float r[32];
 #pragma unroll
           for (int v = 0; v < 32; ++v) r[v] = v < kVals ? acc[v] : (v == kVals ? examined : 0.f);
@@ -761,7 +796,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
           __syncwarp();
           double minpiv = 0.0;
           float inc_rot = 0.f, inc_trans = 0.f;
-          const bool ok = warp_solve_update(s_tot, s_pose, &minpiv, &inc_rot, &inc_trans);
+          // (on success the warp also writes the new pose's rigid transforms)
+          const bool ok =
+              warp_solve_update(s_tot, s_pose, &minpiv, &inc_rot, &inc_trans, &s_c2w, &s_w2c);
           if (threadIdx.x == 0) {
             s_its += 1;
             s_inl = (int)s_tot[28];
@@ -771,11 +808,11 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
             if (!ok) {
               for (int i = 0; i < 16; ++i) s_pose[i] = ws->pose_init[i];
               s_stop = 1;
+              pose_to_rigid(s_pose, &s_c2w, &s_w2c);
             } else if (plan.stop_rot > 0.f && inc_rot < plan.stop_rot &&
                        inc_trans < plan.stop_trans) {
               s_conv = 1;  // converged at this level
             }
-            pose_to_rigid(s_pose, &s_c2w, &s_w2c);
           }
         }
         __syncthreads();
@@ -800,6 +837,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     int err = *((volatile int *)&ws->error);
     for (int i = 0; i < 16; ++i) pose[i] = err ? ws->pose_init[i] : s_pose[i];
+    if (plan.hist) {
+      const unsigned long long c = *plan.hist_count;
+      double *dst = plan.hist + (size_t)(c % (unsigned long long)plan.hist_cap) * 16;
+      for (int i = 0; i < 16; ++i) dst[i] = err ? ws->pose_init[i] : s_pose[i];
+      *plan.hist_count = c + 1;
+    }
     ws->iterations = s_its;
     if (stats) {
       stats->status = err ? 2 : (s_stop ? 1 : 0);
@@ -949,7 +992,8 @@ static of_status_t fused_shape(const of_camera_t *cam, FusedShape *fs) {
 // cooperative launch of the fused kernel.
 of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, const void *d_frame,
                           const void *d_model, double *pose, void *d_ws, of_icp_stats_t *stats,
-                          cudaStream_t s, const double *d_warm) {
+                          cudaStream_t s, const double *d_warm, double *d_hist,
+                          unsigned long long *d_hist_count, int hist_cap) {
   of_pyramid_layout_t lay;
   of_status_t st = of_pyramid_layout(cam, ip->levels, &lay);
   if (st != OF_OK) return st;
@@ -972,6 +1016,11 @@ of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, con
   plan.judge_trans = ip->judge_max_trans_mm;
   plan.warm_levels = (ip->warm_levels > 0 && ip->warm_levels < ip->levels) ? ip->warm_levels
                                                                           : ip->levels;
+  if (d_hist && d_hist_count && hist_cap > 0) {
+    plan.hist = d_hist;
+    plan.hist_count = d_hist_count;
+    plan.hist_cap = hist_cap;
+  }
   for (int l = 0; l < ip->levels; ++l) {
     of_camera_t cl = camera_level(*cam, l);
     plan.lv[l].cam = make_cam(cl);
@@ -996,7 +1045,8 @@ extern "C" of_status_t of_icp_track(const of_camera_t *cam, const of_icp_params_
   OF_RANGE("of_icp_track");
   if (!of_camera_valid(cam) || !icp_params_ok(ip) || !d_frame || !d_model || !pose || !d_ws)
     return OF_ERR_INVALID_ARGUMENT;
-  return of_icp_launch(cam, ip, d_frame, d_model, pose, d_ws, stats, (cudaStream_t)s, nullptr);
+  return of_icp_launch(cam, ip, d_frame, d_model, pose, d_ws, stats, (cudaStream_t)s, nullptr,
+                       nullptr, nullptr, 0);
 }
 
 extern "C" of_status_t of_icp_track_warm(const of_camera_t *cam, const of_icp_params_t *ip,
@@ -1007,7 +1057,8 @@ extern "C" of_status_t of_icp_track_warm(const of_camera_t *cam, const of_icp_pa
   if (!of_camera_valid(cam) || !icp_params_ok(ip) || !d_frame || !d_model || !pose ||
       !d_warm_pose || !d_ws)
     return OF_ERR_INVALID_ARGUMENT;
-  return of_icp_launch(cam, ip, d_frame, d_model, pose, d_ws, stats, (cudaStream_t)s, d_warm_pose);
+  return of_icp_launch(cam, ip, d_frame, d_model, pose, d_ws, stats, (cudaStream_t)s, d_warm_pose,
+                       nullptr, nullptr, 0);
 }
 
 extern "C" of_status_t of_icp_system(const of_camera_t *cam, const of_icp_params_t *ip,
@@ -1091,7 +1142,8 @@ extern "C" of_status_t of_icp_track_static(const of_camera_t *cam, const of_icp_
   void *ws = nullptr;
   of_status_t st = static_icp_workspace(&ws);
   if (st != OF_OK) return st;
-  return of_icp_launch(cam, ip, d_frame, d_model, pose, ws, stats, (cudaStream_t)stream, nullptr);
+  return of_icp_launch(cam, ip, d_frame, d_model, pose, ws, stats, (cudaStream_t)stream, nullptr,
+                       nullptr, nullptr, 0);
 }
 
 // ------------------------------------------------------------ batched ICP --

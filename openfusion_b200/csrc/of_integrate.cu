@@ -134,6 +134,7 @@ __device__ __forceinline__ void load_setup(const FrameSetup *g, FrameSetup *s) {
 // compares |p - c| with.
 __device__ __forceinline__ void depth_tiles_block(const Cam &cam, const uint16_t *__restrict__ depth,
                                                   int pitch, const float2 *__restrict__ lam,
+                                                  float2 *__restrict__ lmap,
                                                   float2 *__restrict__ tiles, int tiles_x,
                                                   int ntiles, unsigned int *list_count,
                                                   const double *__restrict__ pose,
@@ -143,7 +144,8 @@ __device__ __forceinline__ void depth_tiles_block(const Cam &cam, const uint16_t
   const int lane = threadIdx.x & 31;
   if (bx == 0 && threadIdx.x == 0) {
     // for the next two steps: an empty work list, the frame's setup
-    *list_count = 0;
+    list_count[0] = 0;
+    list_count[1] = 0;  // the work counter of step 3
     make_setup(pose, desc, setup->S);
     make_planes(pose, cam, setup->planes);
   }
@@ -157,9 +159,14 @@ __device__ __forceinline__ void depth_tiles_block(const Cam &cam, const uint16_t
     const int u = tx * kTile + (lane & 7), v = ty * kTile + (lane >> 3) + 4 * k;
     if (u < cam.w && v < cam.h) {
       const float D = (float)__ldg(depth + (size_t)v * pitch + u);
-      const float L = __ldg(reinterpret_cast<const float *>(lam) + 2 * (v * cam.w + u)) * D;
+      const float2 lp = __ldg(lam + v * cam.w + u);
+      const float2 Lp = two_prod(lp.x, D);
+      const float L = Lp.x;
       const bool valid = D >= dlo && D <= dhi;
       all_valid &= valid;
+      // the pixel's L = lambda D as a float pair (hi = the FP32 product), or
+      // -1 where the depth is invalid
+      lmap[v * cam.w + u] = valid ? make_float2(L, __fmaf_rn(lp.y, D, Lp.y)) : make_float2(-1.f, 0.f);
       if (valid) {
         lmin = fminf(lmin, L);
         lmax = fmaxf(lmax, L);
@@ -176,12 +183,13 @@ __device__ __forceinline__ void depth_tiles_block(const Cam &cam, const uint16_t
 }
 __global__ void __launch_bounds__(256) k_depth_tiles(Cam cam, const uint16_t *__restrict__ depth,
                                                      int pitch, const float2 *__restrict__ lam,
+                                                     float2 *__restrict__ lmap,
                                                      float2 *__restrict__ tiles, int tiles_x,
                                                      int ntiles, unsigned int *list_count,
                                                      const double *__restrict__ pose,
                                                      of_volume_desc_t desc, FrameSetup *setup) {
-  depth_tiles_block(cam, depth, pitch, lam, tiles, tiles_x, ntiles, list_count, pose, desc, setup,
-                    blockIdx.x);
+  depth_tiles_block(cam, depth, pitch, lam, lmap, tiles, tiles_x, ntiles, list_count, pose, desc,
+                    setup, blockIdx.x);
 }
 
 // Whole-brick decision from the tile bounds (one thread per brick). Returns
@@ -300,13 +308,13 @@ __device__ __forceinline__ float3 brick_base(const IntegrateSetup &S, int bx, in
 // with tsdf' = +1 when its pixel holds a valid depth (always, when dense),
 // with no ray length or distance evaluated; kModeInside drops the per-voxel
 // frustum checks.
-template <int STORAGE, bool CENSUS, bool EARLY_LOAD = false>
+template <int STORAGE, bool CENSUS, bool EARLY_LOAD = false, bool LMAP = false>
 __device__ __forceinline__ void integrate_brick(
     uint32_t *__restrict__ vol, uint8_t *__restrict__ flags, const of_volume_desc_t &desc,
     const Cam &cam, const uint16_t *__restrict__ depth, int pitch,
     const float2 *__restrict__ lam, const IntegrateSetup &S, const VoxelConsts &K, int t,
     int lane, int b, int bx, int by, int bz, int mode, float3 base, unsigned &my_count,
-    int sat_old = -1) {
+    int sat_old = -1, const float2 *__restrict__ lmap = nullptr) {
   const float T = K.T, inv_T = K.inv_T, dspan = K.dspan, cxh = K.cxh, cyh = K.cyh;
   const float dlo = K.dlo, dhi = K.dhi;
   const unsigned uspan = K.uspan, vspan = K.vspan;
@@ -362,31 +370,45 @@ __device__ __forceinline__ void integrate_brick(
         // free space: a voxel whose pixel holds a valid depth gets +1
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-          const float D = __int_as_float(0x4B000000 | (int)__ldg(depth + dix[m])) - 8388608.0f;
+          bool valid;
+          if (LMAP) {
+            valid = __ldg(reinterpret_cast<const float *>(lmap) + 2 * pix[m]) > 0.f;
+          } else {
+            const float D = __int_as_float(0x4B000000 | (int)__ldg(depth + dix[m])) - 8388608.0f;
+            valid = D >= dlo && D <= dhi;
+          }
           tnew[m] = 1.0f;
-          if (((inb >> m) & 1u) && D >= dlo && D <= dhi) upd |= 1u << m;
+          if (((inb >> m) & 1u) && valid) upd |= 1u << m;
         }
         goto brick_done;
       }
       {
-        float Dv[4], Lh[4];
+        // per voxel: L = lambda D of its pixel as a float pair (hi = the
+        // rounded FP32 product), hi < 0 where the depth is invalid
+        float2 Lv[4];
         bool have_xy = false;
         float2 sxy = make_float2(0.f, 0.f);
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-          // uint16 -> float without I2F: 2^23 + d is exact
-          Dv[m] = __int_as_float(0x4B000000 | (int)__ldg(depth + dix[m])) - 8388608.0f;
-          Lh[m] = __ldg(reinterpret_cast<const float *>(lam) + 2 * pix[m]);
+          if (LMAP) {
+            Lv[m] = __ldg(lmap + pix[m]);
+          } else {
+            // uint16 -> float without I2F: 2^23 + d is exact
+            const float D = __int_as_float(0x4B000000 | (int)__ldg(depth + dix[m])) - 8388608.0f;
+            const float2 lp = __ldg(lam + pix[m]);
+            const float2 Lp = two_prod(lp.x, D);
+            Lv[m] = (D >= dlo && D <= dhi) ? make_float2(Lp.x, __fmaf_rn(lp.y, D, Lp.y))
+                                           : make_float2(-1.f, 0.f);
+          }
         }
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
           tnew[m] = 0.f;
-          const float D = Dv[m];
-          if (!((inb >> m) & 1u) || !(D >= dlo && D <= dhi)) continue;
+          if (!((inb >> m) & 1u) || !(Lv[m].x > 0.f)) continue;
           const float X = Xv[m], Y = Yv[m], Z = Zv[m];
           // SDF = L - r with L = lambda D, r = |p_c|; decide on squares first
           float r2 = fmaf(X, X, fmaf(Y, Y, Z * Z));
-          float L = Lh[m] * D;
+          const float L = Lv[m].x;
           const float slack = fmaf(1e-5f, L, 0.05f);
           float far = L + T + slack;            // SDF < -T - slack  <=>  r > far
           if (r2 > far * far) continue;
@@ -400,9 +422,7 @@ __device__ __forceinline__ void integrate_brick(
               have_xy = true;
             }
             float2 rr = df_sqrt(df_add(sxy, axis_sq(S, 2, bz * 8 + lz0 + m)));
-            float llo = __ldg(reinterpret_cast<const float *>(lam) + 2 * pix[m] + 1);
-            float2 Lp = two_prod(Lh[m], D);
-            Lp.y = __fmaf_rn(llo, D, Lp.y);
+            const float2 Lp = Lv[m];
             float sdf2 = __fadd_rn(__fsub_rn(Lp.x, rr.x), __fsub_rn(Lp.y, rr.y));
             if (sdf2 < -T) continue;
             sn = fminf(sdf2, T) * inv_T;
@@ -621,38 +641,60 @@ __global__ void __launch_bounds__(256) k_classify_bricks(of_volume_desc_t desc, 
   classify_block(desc, cam, tiles, tiles_x, sat, list, list_count, setup, blockIdx.x);
 }
 
-// of_integrate_tiled, step 3: persistent grid over the work list, each
-// 128-thread half of a CTA takes one listed brick at a time.
+// of_integrate_tiled, step 3: persistent grid over the work list. The work
+// unit is a quarter of a listed brick (the 128 voxels of 2 x-slices, one warp
+// of 32 threads with 4 voxels each): unit u is quarter u & 3 of entry u >> 2.
+// A block works on chunks of kListChunk consecutive units (16 bricks), warp w
+// on the units u = w mod 8 of the chunk, so the four quarters of a brick run
+// side by side. Block b starts with chunk b; every further chunk comes from a
+// counter (one atomic per chunk, requested when the current chunk starts and
+// published at its closing barrier), so a block that starts late (its SM
+// held by a concurrent branch of the frame graph) takes less work instead of
+// delaying the stage by a fixed share.
+constexpr unsigned kListChunk = 64;
 template <int STORAGE>
 __device__ __forceinline__ void integrate_list_block(uint32_t *__restrict__ vol,
                                                      const of_volume_desc_t &desc, const Cam &cam,
                                                      const uint16_t *__restrict__ depth, int pitch,
                                                      const float2 *__restrict__ lam,
+                                                     const float2 *__restrict__ lmap,
                                                      const uint4 *__restrict__ list,
-                                                     const unsigned int *__restrict__ list_count,
-                                                     const FrameSetup *__restrict__ setup, int bx,
-                                                     int gx) {
+                                                     unsigned int *__restrict__ list_count,
+                                                     const FrameSetup *__restrict__ setup,
+                                                     unsigned bx, unsigned gx) {
+  static_assert(kListChunk % 8 == 0, "whole units per warp");
   __shared__ FrameSetup F;
+  __shared__ unsigned s_chunk[2];
   load_setup(setup, &F);
   const IntegrateSetup &S = F.S;
-  const int n = (int)*list_count;
-  const int half = threadIdx.x >> 7;
-  const int t = threadIdx.x & 127;
+  const unsigned units = 4u * *reinterpret_cast<volatile unsigned *>(list_count);
+  unsigned *next = list_count + 1;
   const int lane = threadIdx.x & 31;
+  const unsigned warp = threadIdx.x >> 5;  // 8 warps
+  const int t = (int)((warp & 3u) << 5) + lane;
   const VoxelConsts K = voxel_consts(desc, cam, t);
-  const int nb = K.nb;
   uint8_t *flags = brick_flags(vol, desc.resolution);
+  const int nb = K.nb;
   unsigned my_count = 0;
-  for (int e = bx * 2 + half; e < n; e += gx * 2) {
-    const uint4 en = __ldg(list + e);
-    const int bx = (int)(en.x & 0xffu), by = (int)((en.x >> 8) & 0xffu);
-    const int bz = (int)((en.x >> 16) & 0xffu), mode = (int)((en.x >> 24) & 3u);
-    const int sat_old = (int)((en.x >> 26) & 0xfu);
-    const int b = (bx * nb + by) * nb + bz;
-    integrate_brick<STORAGE, false, true>(
-        vol, flags, desc, cam, depth, pitch, lam, S, K, t, lane, b, bx, by, bz, mode,
-        make_float3(__uint_as_float(en.y), __uint_as_float(en.z), __uint_as_float(en.w)), my_count,
-        sat_old);
+  int buf = 0;
+  for (unsigned c = bx; c * kListChunk < units; buf ^= 1) {
+    unsigned nxt = 0;
+    if (threadIdx.x == 0) nxt = gx + atomicAdd(next, 1u);
+    const unsigned u1 = min((c + 1) * kListChunk, units);
+    for (unsigned u = c * kListChunk + warp; u < u1; u += 8) {
+      const uint4 en = __ldg(list + (u >> 2));
+      const int bx = (int)(en.x & 0xffu), by = (int)((en.x >> 8) & 0xffu);
+      const int bz = (int)((en.x >> 16) & 0xffu), mode = (int)((en.x >> 24) & 3u);
+      const int sat_old = (int)((en.x >> 26) & 0xfu);
+      const int b = (bx * nb + by) * nb + bz;
+      integrate_brick<STORAGE, false, true, true>(
+          vol, flags, desc, cam, depth, pitch, lam, S, K, t, lane, b, bx, by, bz, mode,
+          make_float3(__uint_as_float(en.y), __uint_as_float(en.z), __uint_as_float(en.w)),
+          my_count, sat_old, lmap);
+    }
+    if (threadIdx.x == 0) s_chunk[buf] = nxt;
+    __syncthreads();
+    c = s_chunk[buf];
   }
 }
 template <int STORAGE>
@@ -661,10 +703,11 @@ __global__ void __launch_bounds__(256, 4) k_integrate_list(uint32_t *__restrict_
                                                         const uint16_t *__restrict__ depth,
                                                         int pitch, const double *__restrict__ pose,
                                                         const float2 *__restrict__ lam,
+                                                        const float2 *__restrict__ lmap,
                                                         const uint4 *__restrict__ list,
-                                                        const unsigned int *__restrict__ list_count,
+                                                        unsigned int *__restrict__ list_count,
                                                         const FrameSetup *__restrict__ setup) {
-  integrate_list_block<STORAGE>(vol, desc, cam, depth, pitch, lam, list, list_count, setup,
+  integrate_list_block<STORAGE>(vol, desc, cam, depth, pitch, lam, lmap, list, list_count, setup,
                                 blockIdx.x, gridDim.x);
 }
 
@@ -673,11 +716,12 @@ int tiles_of(const of_camera_t *cam) {
   return tiles_x_of(cam) * ((cam->height + kTile - 1) / kTile);
 }
 
-// Scratch of of_integrate_tiled: [0, 256) work-list count, [256, 768) the
-// frame setup, then the tile bounds (float2 per tile), then the work list
-// (16 B per brick).
+// Scratch of of_integrate_tiled: [0, 256) the work-list count and step 3's
+// work counter, [256, 768) the frame setup, then the tile bounds (float2 per
+// tile), the work list (16 B per brick) and the per-pixel L = lambda D map
+// (float2 per pixel).
 struct ScratchLayout {
-  size_t setup, tiles, list, total;
+  size_t setup, tiles, list, lmap, total;
 };
 static_assert(sizeof(FrameSetup) <= 512, "frame setup slot");
 ScratchLayout scratch_layout(const of_volume_desc_t *d, const of_camera_t *cam) {
@@ -686,7 +730,8 @@ ScratchLayout scratch_layout(const of_volume_desc_t *d, const of_camera_t *cam) 
   L.setup = 256;
   L.tiles = 768;
   L.list = L.tiles + (((size_t)tiles_of(cam) * sizeof(float2) + 255) & ~(size_t)255);
-  L.total = L.list + nb * nb * nb * sizeof(uint4);
+  L.lmap = L.list + ((nb * nb * nb * sizeof(uint4) + 255) & ~(size_t)255);
+  L.total = L.lmap + (((size_t)cam->width * cam->height * sizeof(float2) + 255) & ~(size_t)255);
   return L;
 }
 
@@ -719,11 +764,12 @@ of_status_t launch_integrate_tiled(const of_volume_desc_t *d, void *vol, const o
   unsigned int *list_count = (unsigned int *)scratch;
   float2 *tiles = (float2 *)((char *)scratch + L.tiles);
   uint4 *list = (uint4 *)((char *)scratch + L.list);
+  float2 *lmap = (float2 *)((char *)scratch + L.lmap);
   FrameSetup *setup = (FrameSetup *)((char *)scratch + L.setup);
   Cam c = make_cam(*cam);
   const int tx = tiles_x_of(cam), nt = tiles_of(cam);
-  k_depth_tiles<<<(nt + 7) / 8, 256, 0, s>>>(c, depth, pitch, (const float2 *)lam, tiles, tx, nt,
-                                              list_count, pose, *d, setup);
+  k_depth_tiles<<<(nt + 7) / 8, 256, 0, s>>>(c, depth, pitch, (const float2 *)lam, lmap, tiles, tx,
+                                              nt, list_count, pose, *d, setup);
   const size_t nb = (size_t)(d->resolution / 8);
   const unsigned nbr = (unsigned)(nb * nb * nb);
   k_classify_bricks<<<(nbr + 255) / 256, 256, 0, s>>>(
@@ -731,12 +777,12 @@ of_status_t launch_integrate_tiled(const of_volume_desc_t *d, void *vol, const o
   const unsigned blocks = persistent_blocks(d);
   if (d->storage == OF_TSDF_I16)
     k_integrate_list<OF_TSDF_I16><<<blocks, 256, 0, s>>>((uint32_t *)vol, *d, c, depth, pitch, pose,
-                                                         (const float2 *)lam, list, list_count,
-                                                         setup);
+                                                         (const float2 *)lam, lmap, list,
+                                                         list_count, setup);
   else
     k_integrate_list<OF_TSDF_F16><<<blocks, 256, 0, s>>>((uint32_t *)vol, *d, c, depth, pitch, pose,
-                                                         (const float2 *)lam, list, list_count,
-                                                         setup);
+                                                         (const float2 *)lam, lmap, list,
+                                                         list_count, setup);
   return of_launch_status();
 }
 
@@ -753,6 +799,7 @@ struct IntJob {
   const float2 *lam;
   float2 *tiles;
   uint4 *list;
+  float2 *lmap;
   unsigned int *count;
   FrameSetup *setup;
   int tiles_x, ntiles;
@@ -763,8 +810,8 @@ __global__ void __launch_bounds__(256) k_depth_tiles_batch(const IntJob *__restr
                                                            int parity) {
   const int j = batch_job(first, n, blockIdx.x);
   const IntJob &J = jobs[j];
-  depth_tiles_block(J.cam, J.depth[parity], J.pitch, J.lam, J.tiles, J.tiles_x, J.ntiles, J.count,
-                    J.pose, J.desc, J.setup, blockIdx.x - __ldg(first + j));
+  depth_tiles_block(J.cam, J.depth[parity], J.pitch, J.lam, J.lmap, J.tiles, J.tiles_x, J.ntiles,
+                    J.count, J.pose, J.desc, J.setup, blockIdx.x - __ldg(first + j));
 }
 __global__ void __launch_bounds__(256) k_classify_batch(const IntJob *__restrict__ jobs,
                                                         const int *__restrict__ first, int n) {
@@ -780,8 +827,9 @@ __global__ void __launch_bounds__(256, 4) k_integrate_list_batch(const IntJob *_
   const int j = batch_job(first, n, blockIdx.x);
   const IntJob &J = jobs[j];
   const int b0 = __ldg(first + j);
-  integrate_list_block<STORAGE>(J.vol, J.desc, J.cam, J.depth[parity], J.pitch, J.lam, J.list,
-                                J.count, J.setup, blockIdx.x - b0, __ldg(first + j + 1) - b0);
+  integrate_list_block<STORAGE>(J.vol, J.desc, J.cam, J.depth[parity], J.pitch, J.lam, J.lmap,
+                                J.list, J.count, J.setup, blockIdx.x - b0,
+                                __ldg(first + j + 1) - b0);
 }
 
 // list_div candidates of the batched integration (blocks per stream =
@@ -838,6 +886,7 @@ of_status_t integrate_batch_create(const BatchStream *s, int n, IntegrateBatch *
     J.lam = (const float2 *)s[i].lambda;
     J.tiles = (float2 *)(sc + L.tiles);
     J.list = (uint4 *)(sc + L.list);
+    J.lmap = (float2 *)(sc + L.lmap);
     J.count = (unsigned int *)sc;
     J.setup = (FrameSetup *)(sc + L.setup);
     J.tiles_x = tiles_x_of(&s[i].cam);

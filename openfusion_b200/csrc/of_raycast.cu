@@ -52,7 +52,8 @@ constexpr float ray_scale() {
 // indices fit in 32 bits (n <= 1024).
 template <int STORAGE>
 __device__ __forceinline__ float trilinear(const uint32_t *__restrict__ vol, int n, int nb,
-                                           float org, float inv_vs, float px, float py, float pz) {
+                                           float org, float inv_vs, float px, float py, float pz,
+                                           int3 *cell = nullptr) {
   float gx = fmaf(px - org, inv_vs, -0.5f);
   float gy = fmaf(py - org, inv_vs, -0.5f);
   float gz = fmaf(pz - org, inv_vs, -0.5f);
@@ -60,6 +61,7 @@ __device__ __forceinline__ float trilinear(const uint32_t *__restrict__ vol, int
   int iy = min(max(__float2int_rd(gy), 0), n - 2);
   int iz = min(max(__float2int_rd(gz), 0), n - 2);
   float fx = gx - (float)ix, fy = gy - (float)iy, fz = gz - (float)iz;
+  if (cell) *cell = make_int3(ix, iy, iz);
   unsigned base = ((((unsigned)(ix >> 3) * nb + (unsigned)(iy >> 3)) * nb + (unsigned)(iz >> 3)) << 9) |
                   (unsigned)(((ix & 7) << 6) | ((iy & 7) << 3) | (iz & 7));
   unsigned dx = (ix & 7) == 7 ? (unsigned)nb * nb * 512u - 448u : 64u;
@@ -90,13 +92,34 @@ __device__ __forceinline__ uint32_t rgba_pack(float x, float y, float z, float w
          ((uint32_t)(y * 255.f) << 8) | (uint32_t)(x * 255.f);
 }
 
+// Levels 1 .. levels-1 of the model pyramid written by the raycast itself:
+// pixel (x, y) of level l is the ray of level-0 pixel (2^l x, 2^l y), the
+// value the chain of 2x subsamplings (k_model_down) gives.
+struct ModelLevels {
+  float4 *pts[kMaxLevels];
+  int w[kMaxLevels];
+  int levels;
+};
+
+// (out of line: the kernel keeps its registers for the march)
+__device__ __noinline__ void write_coarse(const ModelLevels &coarse, int x, int y, float4 vtx,
+                                          float4 nrm) {
+  for (int l = 1; l < coarse.levels; ++l) {
+    const int m = (1 << l) - 1;
+    if ((x & m) | (y & m)) break;
+    const size_t q = (size_t)(y >> l) * coarse.w[l] + (x >> l);
+    coarse.pts[l][2 * q] = vtx;
+    coarse.pts[l][2 * q + 1] = nrm;
+  }
+}
+
 template <int STORAGE>
 __device__ __forceinline__ void raycast_tile(const uint32_t *__restrict__ vol,
                                              const of_volume_desc_t &desc, const Cam &cam,
                                              const of_raycast_params_t &rp,
                                              const double *__restrict__ pose,
                                              float4 *__restrict__ pts, uint32_t *rgba, int bx,
-                                             int by) {
+                                             int by, const ModelLevels *coarse = nullptr) {
   __shared__ RaySetup S;
   if (threadIdx.x == 0 && threadIdx.y == 0) {
     pose_to_rigid(pose, &S.c2w, nullptr);
@@ -159,11 +182,19 @@ __device__ __forceinline__ void raycast_tile(const uint32_t *__restrict__ vol,
     bool sampled = false;
     int cur_b = -1, cur_s = -1;  // brick / super-brick the march is in, and their flags
     bool cur_flag = false, cur_sflag = false;
+    // the clamped cell base of the position at t when the last sample was
+    // taken there (the same expression as below, so the same brick)
+    int3 cell = make_int3(0, 0, 0);
+    bool have_cell = false;
     for (int it = 0; it < (1 << 16); ++it) {
-      const float px = fmaf(t, dir.x, ox), py = fmaf(t, dir.y, oy), pz = fmaf(t, dir.z, oz);
-      int bi = min(max(__float2int_rd(fmaf(px - org, inv_vs, -0.5f)), 0), n - 2) >> 3;
-      int bj = min(max(__float2int_rd(fmaf(py - org, inv_vs, -0.5f)), 0), n - 2) >> 3;
-      int bk = min(max(__float2int_rd(fmaf(pz - org, inv_vs, -0.5f)), 0), n - 2) >> 3;
+      if (!have_cell) {
+        const float px = fmaf(t, dir.x, ox), py = fmaf(t, dir.y, oy), pz = fmaf(t, dir.z, oz);
+        cell.x = min(max(__float2int_rd(fmaf(px - org, inv_vs, -0.5f)), 0), n - 2);
+        cell.y = min(max(__float2int_rd(fmaf(py - org, inv_vs, -0.5f)), 0), n - 2);
+        cell.z = min(max(__float2int_rd(fmaf(pz - org, inv_vs, -0.5f)), 0), n - 2);
+      }
+      have_cell = false;
+      const int bi = cell.x >> 3, bj = cell.y >> 3, bk = cell.z >> 3;
       const int si = bi / kSuper, sj = bj / kSuper, sk = bk / kSuper;
       const int sidx = (si * ns + sj) * ns + sk;
       if (sidx != cur_s) {
@@ -200,14 +231,15 @@ __device__ __forceinline__ void raycast_tile(const uint32_t *__restrict__ vol,
         continue;
       }
       if (!sampled) {
-        fp = trilinear<STORAGE>(vol, n, nb, org, inv_vs, px, py, pz);
+        fp = trilinear<STORAGE>(vol, n, nb, org, inv_vs, fmaf(t, dir.x, ox), fmaf(t, dir.y, oy),
+                                fmaf(t, dir.z, oz));
         sampled = true;
       }
       float step = fp > 0.f ? fmaxf(min_step, far_k * fp) : min_step;
       float tn = t + step;
       if (tn > t1) break;
       float fn = trilinear<STORAGE>(vol, n, nb, org, inv_vs, fmaf(tn, dir.x, ox),
-                                    fmaf(tn, dir.y, oy), fmaf(tn, dir.z, oz));
+                                    fmaf(tn, dir.y, oy), fmaf(tn, dir.z, oz), &cell);
       if (fp > 0.f && fn <= 0.f) {
         float ta = t, fa = fp, tb = tn, fb = fn;
         // shrink a long bracket with minimum steps from its positive end, so
@@ -241,6 +273,7 @@ __device__ __forceinline__ void raycast_tile(const uint32_t *__restrict__ vol,
       if (fp < 0.f && fn > 0.f) break;  // back face
       t = tn;
       fp = fn;
+      have_cell = true;
     }
   }
   const size_t p = (size_t)y * cam.w + x;
@@ -267,6 +300,7 @@ __device__ __forceinline__ void raycast_tile(const uint32_t *__restrict__ vol,
   }
   pts[2 * p] = vtx;
   pts[2 * p + 1] = nrm;
+  if (coarse && ((x | y) & 1) == 0) write_coarse(*coarse, x, y, vtx, nrm);
   if (rgba) {
     // shaded output of Raycaster.cu:221-227 (showNormal == false)
     float dd = -(dir.x * nrm.x + dir.y * nrm.y + dir.z * nrm.z);
@@ -280,8 +314,9 @@ __global__ void __launch_bounds__(256) k_raycast(const uint32_t *__restrict__ vo
                                                  of_volume_desc_t desc, Cam cam,
                                                  of_raycast_params_t rp,
                                                  const double *__restrict__ pose,
-                                                 float4 *__restrict__ pts, uint32_t *rgba) {
-  raycast_tile<STORAGE>(vol, desc, cam, rp, pose, pts, rgba, blockIdx.x, blockIdx.y);
+                                                 float4 *__restrict__ pts, uint32_t *rgba,
+                                                 ModelLevels coarse) {
+  raycast_tile<STORAGE>(vol, desc, cam, rp, pose, pts, rgba, blockIdx.x, blockIdx.y, &coarse);
 }
 
 // Model level l -> l+1 by subsampling pixel (2x, 2y): model points are used
@@ -474,11 +509,18 @@ extern "C" of_status_t of_raycast(const of_volume_desc_t *d, const void *vol,
   dim3 grid((cam->width + 15) / 16, (cam->height + 15) / 16);
   Cam c = make_cam(*cam);
   float4 *pts = (float4 *)((char *)d_model + lay.points_offset[0]);
+  ModelLevels coarse;
+  memset(&coarse, 0, sizeof(coarse));
+  coarse.levels = levels;
+  for (int l = 0; l < levels; ++l) {
+    coarse.pts[l] = (float4 *)((char *)d_model + lay.points_offset[l]);
+    coarse.w[l] = lay.width[l];
+  }
   if (d->storage == OF_TSDF_I16)
-    k_raycast<OF_TSDF_I16><<<grid, blk, 0, s>>>((const uint32_t *)vol, *d, c, *rp, pose, pts, rgba);
+    k_raycast<OF_TSDF_I16><<<grid, blk, 0, s>>>((const uint32_t *)vol, *d, c, *rp, pose, pts, rgba,
+                                                coarse);
   else
-    k_raycast<OF_TSDF_F16><<<grid, blk, 0, s>>>((const uint32_t *)vol, *d, c, *rp, pose, pts, rgba);
-  st = of_launch_status();
-  if (st != OF_OK) return st;
-  return of_model_pyramid(cam, levels, d_model, s);
+    k_raycast<OF_TSDF_F16><<<grid, blk, 0, s>>>((const uint32_t *)vol, *d, c, *rp, pose, pts, rgba,
+                                                coarse);
+  return of_launch_status();
 }

@@ -26,7 +26,8 @@ bool of_volume_valid(const of_volume_desc_t *d);
 size_t of_icp_workspace_size();
 of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, const void *d_frame,
                           const void *d_model, double *pose, void *d_ws, of_icp_stats_t *stats,
-                          cudaStream_t s, const double *d_warm);
+                          cudaStream_t s, const double *d_warm, double *d_hist,
+                          unsigned long long *d_hist_count, int hist_cap);
 of_status_t of_icp_set_prior(void *d_workspace, const double *prior_host, cudaStream_t s);
 
 struct of_tracker {
@@ -127,11 +128,9 @@ of_status_t enqueue_track(of_tracker *t, int cur, bool fuse, cudaStream_t s) {
   if (st != OF_OK) return st;
   if (sp != OF_OK) return sp;
   if (sf != OF_OK) return sf;
-  st = of_icp_launch(&d.camera, &d.icp, t->frame, t->model, t->pose, t->icp_ws, t->stats, s,
-                     t->warm ? t->warm_pose : nullptr);
-  if (st != OF_OK) return st;
-  k_record_pose<<<1, 32, 0, s>>>(t->pose, t->hist, t->hist_count, t->hist_cap);
-  return of_launch_status();
+  // the ICP kernel appends the frame's pose to the history itself
+  return of_icp_launch(&d.camera, &d.icp, t->frame, t->model, t->pose, t->icp_ws, t->stats, s,
+                       t->warm ? t->warm_pose : nullptr, t->hist, t->hist_count, t->hist_cap);
 }
 
 int count_kernel_nodes(cudaGraph_t g) {

@@ -27,9 +27,11 @@ import numpy as np
 
 def eval_config(of):
     """C5 with the early exit both arms use in the comparison; a warm-started
-    pass skips the coarsest pyramid level."""
+    pass runs on the finest pyramid level only (the prediction already lies
+    within the finest level's convergence basin on most frames; the judge sends
+    the others back to plain ICP over every level)."""
     return dataclasses.replace(of.CONFIGS["c5"], stop_rot_rad=2e-5, stop_trans_mm=0.02,
-                               warm_levels=2)
+                               warm_levels=1)
 
 
 def pose_errors(P, G):
@@ -87,7 +89,7 @@ def evaluate(of, learned, weights, seqs: int, frames: int, device):
             if arm == "warm":
                 res[arm]["kept"] += (warm == 1).tolist()
     out = {"workload": "C5 640x480, 512^3 over 3 m, large motion; early exit 2e-5 rad / "
-                       "0.02 mm; warm passes on the 2 finest levels",
+                       "0.02 mm; warm pass on the finest level",
            "sequences": seqs, "frames_per_sequence": frames}
     for arm, d in res.items():
         out[arm] = {"frames_per_s": 1e3 / float(np.mean(d["ms"])),

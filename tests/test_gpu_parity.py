@@ -233,6 +233,14 @@ def test_raycast_matches_oracle(of, ora, cuda, name, res):
     nb = both & (gn[..., 3] > 0) & (opts[..., 7] > 0)
     nerr = np.linalg.norm(gn[..., :3][nb] - opts[..., 4:7][nb], axis=-1)
     assert np.median(nerr) < 1e-3
+    # the coarser model levels written by the raycast: pixel (x, y) of level l
+    # is level 0's pixel (2^l x, 2^l y), exactly
+    v0, n0 = (t.cpu().numpy() for t in of.unpack_points(cfg, model, 0))
+    for l in range(1, cfg.levels):
+        vl, nl = (t.cpu().numpy() for t in of.unpack_points(cfg, model, l))
+        s = 1 << l
+        assert vl.shape[:2] == ((cfg.height + s - 1) // s, (cfg.width + s - 1) // s)
+        assert np.array_equal(vl, v0[::s, ::s]) and np.array_equal(nl, n0[::s, ::s])
 
 
 # ---------------------------------------------------------------- ICP
