@@ -643,15 +643,17 @@ __global__ void __launch_bounds__(256) k_classify_bricks(of_volume_desc_t desc, 
 
 // of_integrate_tiled, step 3: persistent grid over the work list. The work
 // unit is a quarter of a listed brick (the 128 voxels of 2 x-slices, one warp
-// of 32 threads with 4 voxels each): unit u is quarter u & 3 of entry u >> 2.
-// A block works on chunks of kListChunk consecutive units (16 bricks), warp w
-// on the units u = w mod 8 of the chunk, so the four quarters of a brick run
-// side by side. Block b starts with chunk b; every further chunk comes from a
-// counter (one atomic per chunk, requested when the current chunk starts and
-// published at its closing barrier), so a block that starts late (its SM
-// held by a concurrent branch of the frame graph) takes less work instead of
-// delaying the stage by a fixed share.
-constexpr unsigned kListChunk = 64;
+// of 32 threads with 4 voxels each). The list is cut into N chunks of up to
+// kChunkBricks bricks, chunk c holding entries c, c + N, c + 2N, ...: a sample
+// of the whole list, so chunks cost about the same although the cost of a
+// brick varies by region. Warp w of a block takes quarter w & 3 of every
+// other brick of the chunk, so the four quarters of a brick run side by side.
+// Block b starts with chunk b; every further chunk comes from a counter (one
+// atomic per chunk, requested when the current chunk starts and published at
+// its closing barrier), so a block that starts late (its SM held by a
+// concurrent branch of the frame graph) takes less work instead of delaying
+// the stage by a fixed share.
+constexpr unsigned kChunkBricks = 8;
 template <int STORAGE>
 __device__ __forceinline__ void integrate_list_block(uint32_t *__restrict__ vol,
                                                      const of_volume_desc_t &desc, const Cam &cam,
@@ -662,12 +664,13 @@ __device__ __forceinline__ void integrate_list_block(uint32_t *__restrict__ vol,
                                                      unsigned int *__restrict__ list_count,
                                                      const FrameSetup *__restrict__ setup,
                                                      unsigned bx, unsigned gx) {
-  static_assert(kListChunk % 8 == 0, "whole units per warp");
+  static_assert(kChunkBricks % 2 == 0, "two bricks per step of the 8 warps");
   __shared__ FrameSetup F;
   __shared__ unsigned s_chunk[2];
   load_setup(setup, &F);
   const IntegrateSetup &S = F.S;
-  const unsigned units = 4u * *reinterpret_cast<volatile unsigned *>(list_count);
+  const unsigned n = *reinterpret_cast<volatile unsigned *>(list_count);
+  const unsigned nchunks = (n + kChunkBricks - 1) / kChunkBricks;
   unsigned *next = list_count + 1;
   const int lane = threadIdx.x & 31;
   const unsigned warp = threadIdx.x >> 5;  // 8 warps
@@ -677,12 +680,13 @@ __device__ __forceinline__ void integrate_list_block(uint32_t *__restrict__ vol,
   const int nb = K.nb;
   unsigned my_count = 0;
   int buf = 0;
-  for (unsigned c = bx; c * kListChunk < units; buf ^= 1) {
+  for (unsigned c = bx; c < nchunks; buf ^= 1) {
     unsigned nxt = 0;
     if (threadIdx.x == 0) nxt = gx + atomicAdd(next, 1u);
-    const unsigned u1 = min((c + 1) * kListChunk, units);
-    for (unsigned u = c * kListChunk + warp; u < u1; u += 8) {
-      const uint4 en = __ldg(list + (u >> 2));
+    for (unsigned k = warp >> 2; k < kChunkBricks; k += 2) {
+      const unsigned e = c + k * nchunks;
+      if (e >= n) break;
+      const uint4 en = __ldg(list + e);
       const int bx = (int)(en.x & 0xffu), by = (int)((en.x >> 8) & 0xffu);
       const int bz = (int)((en.x >> 16) & 0xffu), mode = (int)((en.x >> 24) & 3u);
       const int sat_old = (int)((en.x >> 26) & 0xfu);
