@@ -446,6 +446,13 @@ __device__ __forceinline__ void integrate_brick(
           if (!(upd & (1u << m))) continue;
           uint32_t word = w4[m];
           uint32_t wt = word >> 16;
+          if (tnew[m] == 1.0f && (word & 0xffffu) == VoxelCodec<STORAGE>::kOneBits) {
+            // +1 (or unobserved) averaged with +1: the quotient below lies
+            // within a few ulp of 1 and packs to the +1 bits again, so only
+            // the weight changes
+            w4[m] = VoxelCodec<STORAGE>::kOneBits | (min(wt + 1u, (uint32_t)desc.max_weight) << 16);
+            continue;
+          }
           // weight as float without I2F (2^23 + w is exact)
           float wf = __int_as_float(0x4B000000 | (int)wt) - 8388608.0f;
           float told = wt ? VoxelCodec<STORAGE>::tsdf(word) : 0.f;

@@ -85,6 +85,66 @@ __device__ __forceinline__ float trilinear(const uint32_t *__restrict__ vol, int
   return fmaf(fx, c1 - c0, c0) * ray_scale<STORAGE>();
 }
 
+// Central differences of the trilinear field one voxel apart along each axis
+// at p: (f(p + vs e_a) - f(p - vs e_a)) for a = x, y, z. The six samples take
+// p's cell fractions (equal to their own up to FP32 rounding of the shifted
+// position), so their 48 corner reads come from the 32 voxels of p's cell
+// widened by one voxel along each axis in turn. Each sample is interpolated
+// in trilinear()'s order (z, then y, then x). p's cell base must lie in
+// [1, n-3] on every axis (the caller keeps p one voxel inside the box).
+template <int STORAGE>
+__device__ __forceinline__ float3 central_gradient(const uint32_t *__restrict__ vol, int n, int nb,
+                                                   float org, float inv_vs, float px, float py,
+                                                   float pz) {
+  const float gx = fmaf(px - org, inv_vs, -0.5f);
+  const float gy = fmaf(py - org, inv_vs, -0.5f);
+  const float gz = fmaf(pz - org, inv_vs, -0.5f);
+  const int ix = min(max(__float2int_rd(gx), 1), n - 3);
+  const int iy = min(max(__float2int_rd(gy), 1), n - 3);
+  const int iz = min(max(__float2int_rd(gz), 1), n - 3);
+  const float fx = gx - (float)ix, fy = gy - (float)iy, fz = gz - (float)iz;
+  // word offset of index i-1 .. i+2 along each axis (brick part + local part)
+  unsigned ox[4], oy[4], oz[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const unsigned a = (unsigned)(ix - 1 + k), b = (unsigned)(iy - 1 + k), c = (unsigned)(iz - 1 + k);
+    ox[k] = (((a >> 3) * (unsigned)nb * (unsigned)nb) << 9) + ((a & 7u) << 6);
+    oy[k] = (((b >> 3) * (unsigned)nb) << 9) + ((b & 7u) << 3);
+    oz[k] = ((c >> 3) << 9) + (c & 7u);
+  }
+  auto v = [&](int kx, int ky, int kz) {
+    return ray_value<STORAGE>(__ldg(vol + ox[kx] + oy[ky] + oz[kz]));
+  };
+  auto lerp = [](float a, float b, float f) { return fmaf(f, b - a, a); };
+  // z-interpolated rows at x = kx, y = ky, over the cell's own z pair (1, 2)
+  float Lz[4][4];
+#pragma unroll
+  for (int kx = 0; kx < 4; ++kx)
+#pragma unroll
+    for (int ky = 0; ky < 4; ++ky) {
+      const bool need = (ky == 1 || ky == 2) || (kx == 1 || kx == 2);
+      Lz[kx][ky] = need ? lerp(v(kx, ky, 1), v(kx, ky, 2), fz) : 0.f;
+    }
+  // x: cells (ix - 1) and (ix + 1)
+  const float xm = lerp(lerp(Lz[0][1], Lz[0][2], fy), lerp(Lz[1][1], Lz[1][2], fy), fx);
+  const float xp = lerp(lerp(Lz[2][1], Lz[2][2], fy), lerp(Lz[3][1], Lz[3][2], fy), fx);
+  // y: cells (iy - 1) and (iy + 1)
+  const float ym = lerp(lerp(Lz[1][0], Lz[1][1], fy), lerp(Lz[2][0], Lz[2][1], fy), fx);
+  const float yp = lerp(lerp(Lz[1][2], Lz[1][3], fy), lerp(Lz[2][2], Lz[2][3], fy), fx);
+  // z: cells (iz - 1) and (iz + 1), over the cell's own x and y pairs
+  float zm, zp;
+  {
+    const float m11 = lerp(v(1, 1, 0), v(1, 1, 1), fz), m12 = lerp(v(1, 2, 0), v(1, 2, 1), fz);
+    const float m21 = lerp(v(2, 1, 0), v(2, 1, 1), fz), m22 = lerp(v(2, 2, 0), v(2, 2, 1), fz);
+    const float p11 = lerp(v(1, 1, 2), v(1, 1, 3), fz), p12 = lerp(v(1, 2, 2), v(1, 2, 3), fz);
+    const float p21 = lerp(v(2, 1, 2), v(2, 1, 3), fz), p22 = lerp(v(2, 2, 2), v(2, 2, 3), fz);
+    zm = lerp(lerp(m11, m12, fy), lerp(m21, m22, fy), fx);
+    zp = lerp(lerp(p11, p12, fy), lerp(p21, p22, fy), fx);
+  }
+  const float sc = ray_scale<STORAGE>();
+  return make_float3(xp * sc - xm * sc, yp * sc - ym * sc, zp * sc - zm * sc);
+}
+
 __device__ __forceinline__ uint32_t rgba_pack(float x, float y, float z, float w) {
   // rgbaFloatToInt (Raycaster.cu:26-33)
   x = __saturatef(x); y = __saturatef(y); z = __saturatef(z); w = __saturatef(w);
@@ -284,12 +344,8 @@ __device__ __forceinline__ void raycast_tile(const uint32_t *__restrict__ vol,
     float lo = S.lo, hi = S.hi;
     if (px - vs >= lo && px + vs <= hi && py - vs >= lo && py + vs <= hi && pz - vs >= lo &&
         pz + vs <= hi) {
-      float gx = trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, px + vs, py, pz) -
-                 trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, px - vs, py, pz);
-      float gy = trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, px, py + vs, pz) -
-                 trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, px, py - vs, pz);
-      float gz = trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, px, py, pz + vs) -
-                 trilinear<STORAGE>(vol, n, nb, org, S.inv_vs, px, py, pz - vs);
+      const float3 g = central_gradient<STORAGE>(vol, n, nb, org, S.inv_vs, px, py, pz);
+      const float gx = g.x, gy = g.y, gz = g.z;
       float l2 = gx * gx + gy * gy + gz * gz;
       if (l2 > 0.f) {
         float inv = rsqrtf(l2);
