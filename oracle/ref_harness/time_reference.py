@@ -101,8 +101,43 @@ def main(frames: int):
                   for P, G in zip(Ps, poses))
         tra = max(float(np.linalg.norm(P[:3, 3] - G[:3, 3])) for P, G in zip(Ps, poses))
         return rot, tra
+    def stages(cfg):
+        # the tracker's stages launched one by one in its order (integrate k-1,
+        # raycast k-1, pre-process k, ICP k), each timed with CUDA events; mean
+        # over frames 4..60 (before free space saturates) and after frame 130
+        vol, lam = of.new_volume(cfg, dev), of.lambda_table(cfg, dev)
+        scr = of.integrate_scratch(cfg, dev)
+        frame, model, ws = of.new_pyramid(cfg, dev), of.new_pyramid(cfg, dev), of.icp_workspace(cfg, dev)
+        pose = torch.tensor(np.asarray(poses[0]).reshape(16), dtype=torch.float64, device=dev)
+        names = ["integrate", "raycast", "preprocess", "icp"]
+        early, late = [], []
+        s = torch.cuda.current_stream()
+        for k in range(1, frames):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+            ev[0].record(s)
+            of.integrate(cfg, vol, dd[k - 1], pose, lam, scr)
+            ev[1].record(s)
+            of.raycast(cfg, vol, pose, model)
+            ev[2].record(s)
+            of.preprocess(cfg, dd[k], frame)
+            ev[3].record(s)
+            of.icp_track(cfg, frame, model, pose, ws)
+            ev[4].record(s)
+            s.synchronize()
+            t = [ev[i].elapsed_time(ev[i + 1]) * 1e3 for i in range(4)]
+            if 3 < k <= 60:
+                early.append(t)
+            elif k > 130:
+                late.append(t)
+        out = {}
+        for key, rows in (("frames_4_60", early), ("after_frame_130", late)):
+            if rows:
+                out[key] = dict(zip(names, np.round(np.mean(rows, axis=0), 1).tolist()))
+        return out
+
     ours_ms, hist = run(base)
     exit_ms, hist_exit = run(dataclasses.replace(base, stop_rot_rad=2e-5, stop_trans_mm=0.02))
+    stage_us = stages(base)
     print(json.dumps({
         "workload": "640x480, 512^3 over 1024 mm (reference constants), %d frames" % frames,
         "reference_kernels_sm100a": {"ms_per_frame": ref_ms, "frames_per_s": 1e3 / ref_ms,
@@ -116,7 +151,8 @@ def main(frames: int):
                                        "max_pose_err_deg_mm": err(hist_exit),
                                        "icp": "3 levels, at most 10/5/4, a level ends when an "
                                               "increment is below 2e-5 rad and 0.02 mm"},
-        "speedup_convergence_exit": ref_ms / exit_ms}))
+        "speedup_convergence_exit": ref_ms / exit_ms,
+        "stages_us": stage_us}))
 
 
 if __name__ == "__main__":
