@@ -275,6 +275,16 @@ def run_ours(args, cfg, world, rank, local):
     kernels = bufs.kernels_track * args.steps
     hist = tr.pose_history(total)
     _, st = tr.pose()
+    # ---- per-frame times: CUDA events between the steps of the same tracker,
+    # continuing the sequence (every frame is past frame 10)
+    nf = min(args.steps, 300)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(nf + 1)]
+    evs[0].record(stream)
+    for i in range(nf):
+        tr.process(depth_dev[frame_index(total + i, n_seq)])
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize()
+    per_frame = np.array([evs[i].elapsed_time(evs[i + 1]) for i in range(nf)])
     tr.close()
     rots, trans = pose_errors(hist, [seq.poses[j] for j in order])
 
@@ -316,6 +326,11 @@ def run_ours(args, cfg, world, rank, local):
         return
     peak, peak_kind = peaks()
     integ_bytes = stages["integrate_alg_bytes"]
+    # the traffic of a kernel that visits every voxel (the reference's), over
+    # this stage's time: above the HBM peak because whole bricks are decided
+    # from tile bounds and skipped
+    sweep_bytes = 8.0 * cfg.resolution ** 3 + 2.0 * cfg.width * cfg.height
+    sweep_gbps = sweep_bytes / (stages["integrate_ms"] / 1e3) / 1e9
     achieved = integ_bytes / (stages["integrate_ms"] / 1e3) / 1e9
     traffic = None
     tf = ROOT / "profiles" / "integrate_traffic.json"
@@ -346,6 +361,13 @@ def run_ours(args, cfg, world, rank, local):
                      "frac": achieved / peak, "traffic": traffic,
                      "alg_bytes_per_launch": integ_bytes,
                      "updated_voxels_per_launch": stages["integrate_updated_voxels"]},
+        "frame_ms": {"median": float(np.median(per_frame)), "p10": float(np.percentile(per_frame, 10)),
+                     "p90": float(np.percentile(per_frame, 90)), "frames": int(nf),
+                     "how": "CUDA events between graph-replayed steps (rank 0)"},
+        "integrate_full_sweep": {"bytes_per_frame": sweep_bytes, "equivalent_GBps": sweep_gbps,
+                                 "note": "8 B x N^3 + depth (a kernel visiting every voxel, as the "
+                                         "reference's does) over this stage's time; not a roofline "
+                                         "fraction: whole bricks are skipped"},
         "e2e": {"value": e2e_fps, "unit": "frames/s",
                 "h2d_bytes_per_step": cfg.width * cfg.height * 2, "d2h_bytes_per_step": 128},
         "gpu_launches": kernels,

@@ -209,8 +209,9 @@ of_status_t of_integrate_tiled(const of_volume_desc_t *desc, void *d_volume,
                                const of_camera_t *cam, const uint16_t *d_depth, int32_t pitch_px,
                                const double *d_pose, const float *d_lambda, void *d_scratch,
                                of_stream_t stream);
-/* Bytes of of_integrate_tiled's scratch: 768 + 8 B per 8x8 pixel tile
- * (rounded up to 256) + 16 B per 8^3 brick. */
+/* Bytes of of_integrate_tiled's scratch: 768 + 8 B per 8x8 pixel tile + 16 B
+ * per 8^3 brick + 8 B per pixel (the frame's lambda * D map), each part
+ * rounded up to 256. */
 of_status_t of_integrate_scratch_bytes(const of_volume_desc_t *desc, const of_camera_t *cam,
                                        size_t *bytes);
 /* Counts the voxels one of_integrate call would update (same decisions, no
@@ -224,8 +225,9 @@ of_status_t of_integrate_census(const of_volume_desc_t *desc, const void *d_volu
 
 /* Casts one ray per pixel of level 0 from pose `d_pose` and writes world-space
  * vertex/normal maps into `d_model` (of_pyramid_layout; only points_offset
- * is used), then fills levels 1.. by guarded 2x2 averaging. `d_rgba` (may be
- * NULL) receives the reference's shaded image (Raycaster.cu:214-228). */
+ * is used); pixel (x, y) of level l = 1 .. levels-1 is the ray of level-0
+ * pixel (2^l x, 2^l y), written by the same launch. `d_rgba` (may be NULL)
+ * receives the reference's shaded image (Raycaster.cu:214-228). */
 of_status_t of_raycast(const of_volume_desc_t *desc, const void *d_volume, const of_camera_t *cam,
                        const of_raycast_params_t *params, int32_t levels, const double *d_pose,
                        void *d_model, uint32_t *d_rgba, of_stream_t stream);
