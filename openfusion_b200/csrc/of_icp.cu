@@ -341,10 +341,10 @@ __device__ __forceinline__ bool wait_seq(IcpWorkspace *ws, const unsigned *p, un
 }
 
 // 1 / d for a positive normal FP64 d: the approximate FP64 reciprocal of the
-// PTX ISA (rcp.approx.ftz.f64, a relative error of at most about 2^-20)
-// refined by two Newton-Raphson steps r <- r + r (1 - d r), each of which
-// squares the relative error (to below 2^-80, under FP64 rounding). It stays
-// on the FP64 pipe (no conversion to FP32 and back).
+// PTX ISA (rcp.approx.ftz.f64; measured on B200 at most 9.8e-7 relative,
+// about 2^-20) refined by two Newton-Raphson steps r <- r + r (1 - d r), each
+// of which squares the relative error (to below 2^-80, under FP64 rounding).
+// No conversion to FP32 and back is needed.
 __device__ __forceinline__ double recip_pos(double d) {
   double r;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
@@ -569,7 +569,7 @@ __device__ __forceinline__ bool judge_keep(const IcpPlan &plan, const double *W,
 // iteration: every block associates its points two at a time (both frame
 // gathers in flight together), accumulates the rows (tree sums), writes 29
 // partials, meets the others at one grid barrier, then reduces all blocks'
-// partials in the same fixed order and one thread solves the 6x6 system, so
+// partials in the same fixed order and one warp solves the 6x6 system, so
 // every block holds the same new pose without a second barrier. Partials
 // alternate between two buffers: a block can only overwrite buffer i%2 after
 // the barrier of iteration i+1, which every block reaches only after reading it.
