@@ -360,7 +360,12 @@ def run_ours(args, cfg, world, rank, local):
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "alg_bytes_per_launch": integ_bytes,
-                     "updated_voxels_per_launch": stages["integrate_updated_voxels"]},
+                     "alg_units": "8 B per voxel in view (centre inside the 2-pixel border, "
+                                  "depth in [min, max]) + 2 B per depth pixel",
+                     "visible_voxels_per_launch": stages["integrate_visible_voxels"],
+                     "updated_voxels_per_launch": stages["integrate_updated_voxels"],
+                     "frac_updated_voxels": stages["integrate_updated_bytes"] /
+                                            (stages["integrate_ms"] / 1e3) / 1e9 / peak},
         "frame_ms": {"median": float(np.median(per_frame)), "p10": float(np.percentile(per_frame, 10)),
                      "p90": float(np.percentile(per_frame, 90)), "frames": int(nf),
                      "how": "CUDA events between graph-replayed steps (rank 0)"},
@@ -540,18 +545,23 @@ def stage_times(of, cfg, seq, depth_dev, order, args, dev):
                 acc[name] += ev[j].elapsed_time(ev[j + 1])
             n += 1
     # Algorithmic bytes of one integration launch: 4 B read + 4 B write per
-    # updated voxel plus 2 B per depth pixel. The census launch counts the
-    # updated voxels with the same decisions and no writes; it replays the
-    # same frames at the same poses on a second volume, outside any timing.
+    # voxel in view (centre inside the 2-pixel border, depth in [min, max])
+    # plus 2 B per depth pixel; beside it the stricter count of the voxels the
+    # launch actually changes. The census launches count both with the
+    # integration's own tests and no writes; they replay the same frames at
+    # the same poses on a second volume, outside any timing.
     vol2 = of.new_volume(cfg, dev)
-    upd = []
+    upd, vis = [], []
     for i in range(total):
         d = depth_dev[order[i]]
         if i > args.warmup and (i - args.warmup) % 10 == 0:
             upd.append(of.integrate_census(cfg, vol2, d, poses[i], lam))
+            vis.append(of.integrate_visible_census(cfg, vol2, d, poses[i], lam))
         of.integrate(cfg, vol2, d, poses[i], lam, scratch)
     out = {f"{k}_ms": v / max(n, 1) for k, v in acc.items()}
-    out["integrate_alg_bytes"] = 8.0 * float(np.mean(upd)) + 2.0 * cfg.width * cfg.height
+    out["integrate_alg_bytes"] = 8.0 * float(np.mean(vis)) + 2.0 * cfg.width * cfg.height
+    out["integrate_visible_voxels"] = float(np.mean(vis))
+    out["integrate_updated_bytes"] = 8.0 * float(np.mean(upd)) + 2.0 * cfg.width * cfg.height
     out["integrate_updated_voxels"] = float(np.mean(upd))
     del vol, vol2
     torch.cuda.empty_cache()

@@ -220,6 +220,14 @@ of_status_t of_integrate_census(const of_volume_desc_t *desc, const void *d_volu
                                 const of_camera_t *cam, const uint16_t *d_depth,
                                 int32_t pitch_px, const double *d_pose, const float *d_lambda,
                                 unsigned long long *d_count, of_stream_t stream);
+/* Counts the voxels in view at `d_pose`: those whose centre projects inside the
+ * 2-pixel image border with a depth in [min, max] (the frustum test of
+ * VolumeIntegrator.cu:12-16, :131), adding to the device uint64 `d_count`. */
+of_status_t of_integrate_visible_census(const of_volume_desc_t *desc, const void *d_volume,
+                                        const of_camera_t *cam, const uint16_t *d_depth,
+                                        int32_t pitch_px, const double *d_pose,
+                                        const float *d_lambda, unsigned long long *d_count,
+                                        of_stream_t stream);
 
 /* ---- raycast (replaces Raycaster::Raycast, Source/src/Raycaster.cu:97-242) */
 

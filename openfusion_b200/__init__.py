@@ -12,7 +12,7 @@ from .api import (CONFIGS, Batch, Config, Reader, c4_configs, depth_filter, dept
                   save_volume_raw, write_obj,
                   read_recording_info, write_recording, Sequence, Tracker, integrate_scratch, icp_system, icp_track,
                   icp_track_warm,
-                  icp_workspace, integrate, integrate_census, lambda_table, level_camera, linear_to_volume,
+                  icp_workspace, integrate, integrate_census, integrate_visible_census, lambda_table, level_camera, linear_to_volume,
                   make_scene, make_sequence, make_trajectory, new_pyramid, new_volume,
                   preprocess, pyramid_layout, raycast, render, unpack_depth, unpack_points,
                   volume_bytes, volume_to_linear, shard, stream_cost)
@@ -23,7 +23,7 @@ __all__ = [
     "extract_mesh", "read_recording_frame",
     "save_volume_raw", "write_obj",
     "read_recording_info", "write_recording", "Sequence", "Tracker", "integrate_scratch", "icp_system", "icp_track", "icp_track_warm", "icp_workspace",
-    "integrate", "integrate_census", "lambda_table", "level_camera", "linear_to_volume",
+    "integrate", "integrate_census", "integrate_visible_census", "lambda_table", "level_camera", "linear_to_volume",
     "make_scene", "make_sequence", "make_trajectory", "new_pyramid", "new_volume", "preprocess",
     "pyramid_layout", "raycast", "render", "unpack_depth", "unpack_points", "volume_bytes",
     "volume_to_linear", "shard", "stream_cost",

@@ -127,6 +127,8 @@ _SIGS = {
     "of_lambda_table": (c_status, [C.POINTER(Camera), P, c_stream]),
     "of_integrate_census": (c_status, [C.POINTER(VolumeDesc), P, C.POINTER(Camera), P, C.c_int32,
                                        P, P, P, c_stream]),
+    "of_integrate_visible_census": (c_status, [C.POINTER(VolumeDesc), P, C.POINTER(Camera), P,
+                                               C.c_int32, P, P, P, c_stream]),
     "of_raycast": (c_status, [C.POINTER(VolumeDesc), P, C.POINTER(Camera),
                               C.POINTER(RaycastParams), C.c_int32, P, P, P, c_stream]),
     "of_icp_workspace_bytes": (c_status, [C.POINTER(Camera), C.POINTER(C.c_size_t)]),

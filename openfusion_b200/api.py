@@ -213,6 +213,17 @@ def integrate_census(cfg: Config, vol, depth, pose, lam) -> int:
                                         _stream()))
     return int(cnt.item())
 
+def integrate_visible_census(cfg: Config, vol, depth, pose, lam) -> int:
+    """Voxels in view at `pose`: centre inside the 2-pixel image border with a
+    depth in [min, max] (the integration's frustum test)."""
+    import torch
+    cnt = torch.zeros(1, dtype=torch.int64, device=vol.device)
+    N.check("of_integrate_visible_census",
+            N.lib().of_integrate_visible_census(C.byref(cfg.volume()), _ptr(vol),
+                                                C.byref(cfg.camera()), _ptr(depth), cfg.width,
+                                                _ptr(pose), _ptr(lam), _ptr(cnt), _stream()))
+    return int(cnt.item())
+
 
 def raycast(cfg: Config, vol, pose, model=None, rgba=None):
     """Raycaster::Raycast: world vertex/normal pyramid of the volume at `pose`."""

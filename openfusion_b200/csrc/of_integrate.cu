@@ -266,6 +266,11 @@ __device__ int classify_brick(const IntegrateSetup &S, const Cam &cam, const flo
   return dense ? kModeFrontDense : kModeFront;
 }
 
+// What of_integrate's census counts instead of writing the volume.
+constexpr int kCensusUpdated = 1;  // voxels the integration would update
+constexpr int kCensusVisible = 2;  // voxels whose centre projects inside the
+                                   // 2-pixel border within [min, max] depth
+
 // Per-thread constants of the voxel loop.
 struct VoxelConsts {
   float T, inv_T, dspan, cxh, cyh, dlo, dhi;
@@ -308,7 +313,7 @@ __device__ __forceinline__ float3 brick_base(const IntegrateSetup &S, int bx, in
 // with tsdf' = +1 when its pixel holds a valid depth (always, when dense),
 // with no ray length or distance evaluated; kModeInside drops the per-voxel
 // frustum checks.
-template <int STORAGE, bool CENSUS, bool EARLY_LOAD = false, bool LMAP = false>
+template <int STORAGE, int CENSUS, bool EARLY_LOAD = false, bool LMAP = false>
 __device__ __forceinline__ void integrate_brick(
     uint32_t *__restrict__ vol, uint8_t *__restrict__ flags, const of_volume_desc_t &desc,
     const Cam &cam, const uint16_t *__restrict__ depth, int pitch,
@@ -321,6 +326,7 @@ __device__ __forceinline__ void integrate_brick(
   const int lx = K.lx, ly = K.ly, lz0 = K.lz0, nb = K.nb;
   float tnew[4];
   unsigned upd = 0;
+  unsigned inb = 0;  // voxels inside the 2-pixel border and the depth range (kModeFull)
   bool near = false;
   uint4 *p4 = reinterpret_cast<uint4 *>(vol + ((size_t)b << 9)) + t;
   uint4 wv = make_uint4(0u, 0u, 0u, 0u);
@@ -342,7 +348,6 @@ __device__ __forceinline__ void integrate_brick(
       // any result is used; phase 3: decide
       float Xv[4], Yv[4], Zv[4];
       int pix[4], dix[4];
-      unsigned inb = 0;
 #pragma unroll
       for (int m = 0; m < 4; ++m) {
         const float lz = (float)(lz0 + m);
@@ -434,7 +439,7 @@ __device__ __forceinline__ void integrate_brick(
       }
     brick_done:
       if (CENSUS) {
-        my_count += __popc(upd);
+        my_count += __popc(CENSUS == kCensusVisible ? inb : upd);
       } else if (!upd) {
         if (!EARLY_LOAD) wv = *p4;
         wfin = wv;
@@ -504,7 +509,7 @@ __device__ __forceinline__ void integrate_brick(
 // equal share of the frustum. Per batch, warp 0 tests 32 of the CTA's bricks
 // against the frustum (one lane each) and compacts the visible ones into a
 // shared list; the two 128-thread halves then take list entries alternately.
-template <int STORAGE, bool CENSUS>
+template <int STORAGE, int CENSUS>
 __global__ void __launch_bounds__(256, 4) k_integrate(uint32_t *__restrict__ vol, of_volume_desc_t desc,
                                                    Cam cam, const uint16_t *__restrict__ depth,
                                                    int pitch, const double *__restrict__ pose,
@@ -698,7 +703,7 @@ __device__ __forceinline__ void integrate_list_block(uint32_t *__restrict__ vol,
       const int bz = (int)((en.x >> 16) & 0xffu), mode = (int)((en.x >> 24) & 3u);
       const int sat_old = (int)((en.x >> 26) & 0xfu);
       const int b = (bx * nb + by) * nb + bz;
-      integrate_brick<STORAGE, false, true, true>(
+      integrate_brick<STORAGE, 0, true, true>(
           vol, flags, desc, cam, depth, pitch, lam, S, K, t, lane, b, bx, by, bz, mode,
           make_float3(__uint_as_float(en.y), __uint_as_float(en.z), __uint_as_float(en.w)),
           my_count, sat_old, lmap);
@@ -753,7 +758,7 @@ unsigned persistent_blocks(const of_volume_desc_t *d) {
   return (unsigned)(nbr < (size_t)kSmCount * 4 ? nbr : (size_t)kSmCount * 4);
 }
 
-template <bool CENSUS>
+template <int CENSUS>
 of_status_t launch_integrate(const of_volume_desc_t *d, void *vol, const of_camera_t *cam,
                              const uint16_t *depth, int pitch, const double *pose,
                              const float *lam, unsigned long long *count, cudaStream_t s) {
@@ -961,7 +966,7 @@ extern "C" of_status_t of_integrate(const of_volume_desc_t *d, void *vol, const 
   if (!of_volume_valid(d) || !of_camera_valid(cam) || !vol || !depth || !pose || !lam ||
       pitch < cam->width)
     return OF_ERR_INVALID_ARGUMENT;
-  return launch_integrate<false>(d, vol, cam, depth, pitch, pose, lam, nullptr, (cudaStream_t)s);
+  return launch_integrate<0>(d, vol, cam, depth, pitch, pose, lam, nullptr, (cudaStream_t)s);
 }
 
 extern "C" of_status_t of_integrate_scratch_bytes(const of_volume_desc_t *d,
@@ -989,6 +994,18 @@ extern "C" of_status_t of_integrate_census(const of_volume_desc_t *d, const void
   if (!of_volume_valid(d) || !of_camera_valid(cam) || !vol || !depth || !pose || !lam ||
       !count || pitch < cam->width)
     return OF_ERR_INVALID_ARGUMENT;
-  return launch_integrate<true>(d, (void *)vol, cam, depth, pitch, pose, lam, count,
+  return launch_integrate<kCensusUpdated>(d, (void *)vol, cam, depth, pitch, pose, lam, count,
                                 (cudaStream_t)s);
+}
+
+extern "C" of_status_t of_integrate_visible_census(const of_volume_desc_t *d, const void *vol,
+                                                   const of_camera_t *cam, const uint16_t *depth,
+                                                   int32_t pitch, const double *pose,
+                                                   const float *lam, unsigned long long *count,
+                                                   of_stream_t s) {
+  if (!of_volume_valid(d) || !of_camera_valid(cam) || !vol || !depth || !pose || !lam ||
+      !count || pitch < cam->width)
+    return OF_ERR_INVALID_ARGUMENT;
+  return launch_integrate<kCensusVisible>(d, (void *)vol, cam, depth, pitch, pose, lam, count,
+                                          (cudaStream_t)s);
 }

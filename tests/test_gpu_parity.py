@@ -95,6 +95,40 @@ def test_preprocess_matches_oracle(of, ora, cuda, name, size):
 
 # ---------------------------------------------------------------- integrate
 
+def test_visible_census_counts_the_voxels_in_view(of, cuda):
+    """of_integrate_visible_census against an FP64 count of the same test:
+    voxel centre inside the 2-pixel border (roundFloat pixel) with a depth in
+    [min, max] (VolumeIntegrator.cu:12-16, :131)."""
+    import torch
+    cfg = small(of, "c1", resolution=128)
+    seq = of.make_sequence(cfg, frames=3)
+    vol, lam = of.new_volume(cfg, cuda), of.lambda_table(cfg, cuda)
+    counts = []
+    for k in (1, 2):
+        d = torch.from_numpy(seq.depth[k].astype(np.int16)).to(cuda)
+        n_gpu = of.integrate_visible_census(cfg, vol, d, dev_pose(seq.poses[k], cuda), lam)
+        P = np.asarray(seq.poses[k], np.float64)
+        n = cfg.resolution
+        vs = cfg.size_mm / n
+        g = -0.5 * cfg.size_mm + 0.5 * vs + vs * np.arange(n)
+        X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+        pc = (np.stack([X, Y, Z], -1).reshape(-1, 3) - P[:3, 3]) @ P[:3, :3]
+        with np.errstate(all="ignore"):
+            u = np.floor(cfg.fx * pc[:, 0] / pc[:, 2] + cfg.cx + 0.5)
+            v = np.floor(cfg.fy * pc[:, 1] / pc[:, 2] + cfg.cy + 0.5)
+        z = -pc[:, 2]
+        ok = ((z >= cfg.min_depth_mm) & (z <= cfg.max_depth_mm) & (u >= 2) & (u <= cfg.width - 3)
+              & (v >= 2) & (v <= cfg.height - 3))
+        n_np = int(ok.sum())
+        counts.append(n_gpu)
+        assert n_np > 0.1 * n ** 3, "the view should cover a good part of the cube"
+        # FP32 pixel rounding moves only voxels within ~1e-4 px of the border
+        assert abs(n_gpu - n_np) <= 20 + 1e-4 * n_np, (k, n_gpu, n_np)
+    # the count does not depend on the volume's contents
+    of.integrate(cfg, vol, d, dev_pose(seq.poses[2], cuda), lam)
+    assert of.integrate_visible_census(cfg, vol, d, dev_pose(seq.poses[2], cuda), lam) == counts[1]
+
+
 @pytest.mark.parametrize("name,res,storage,tiled", [("c1", 128, "i16", False),
                                                     ("c2", 256, "i16", False),
                                                     ("c2", 512, "i16", False),
