@@ -137,11 +137,13 @@ def frame_index(i: int, n: int) -> int:
     return j if j < n else period - j
 
 
-def dist_setup():
+def dist_setup(init: bool = True):
+    """World size and ranks from torchrun's environment; the NCCL process
+    group only when the ranks exchange anything (`init`)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
+    if world > 1 and init:
         import datetime
         import torch
         import torch.distributed as dist
@@ -570,7 +572,9 @@ def stage_times(of, cfg, seq, depth_dev, order, args, dev):
 
 def main():
     args = parse()
-    world, rank, local = dist_setup()
+    # the reference arm runs on rank 0 alone and exchanges nothing
+    grouped = args.impl != "reference"
+    world, rank, local = dist_setup(init=grouped)
     import openfusion_b200 as of
     cfg = of.CONFIGS[args.config]
     try:
@@ -579,7 +583,7 @@ def main():
         else:
             run_ours(args, cfg, world, rank, local)
     finally:
-        if world > 1:
+        if world > 1 and grouped:
             import torch.distributed as dist
             dist.destroy_process_group()
 

@@ -31,3 +31,23 @@ def test_reference_arm_prints_one_contract_line():
     assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
     assert d["config"]["workload"].startswith("c2_640x480_512")
+
+
+def test_reference_arm_under_torchrun_prints_from_rank_0_only():
+    """Two ranks launched the way the multi-GPU runs are (torchrun, one node,
+    127.0.0.1): rank 0 alone measures and prints; the other exits 0."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    out = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+                          "--nproc-per-node", "2", "--master-addr", "127.0.0.1",
+                          "--master-port", str(port), str(ROOT / "bench.py"), "--impl",
+                          "reference", "--gpus", "2", "--steps", "1", "--warmup", "1",
+                          "--frames", "6"],
+                         cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.lstrip().startswith("{")]
+    assert len(lines) == 1, out.stdout
+    d = json.loads(lines[0].strip())
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
