@@ -196,6 +196,52 @@ def test_integrate_tiled_equals_per_voxel(of, cuda, name, res, storage, geom):
     assert (w > 0).sum() > 10000
 
 
+@pytest.mark.parametrize("size", [(161, 121), (203, 157)])
+def test_ragged_frame_sizes(of, ora, cuda, size):
+    """Frames whose sides are not multiples of the 8x8 depth tiles or of the
+    16x16 ray blocks: the tiled integration (partial tiles, the per-pixel L
+    map) still writes the per-voxel path's volume bit for bit, the raycast's
+    level 0 matches the oracle, and its coarser levels are the 2^l subsamples."""
+    import torch
+    w, h = size
+    f = 262.5 * w / 320.0
+    cfg = small(of, "c1", width=w, height=h, fx=f, fy=f, cx=(w - 1) / 2, cy=(h - 1) / 2)
+    seq = of.make_sequence(cfg, frames=5)
+    lam, scratch = of.lambda_table(cfg, cuda), of.integrate_scratch(cfg, cuda)
+    va, vb = of.new_volume(cfg, cuda), of.new_volume(cfg, cuda)
+    for k in range(4):
+        d = torch.from_numpy(seq.depth[k].astype(np.int16)).to(cuda)
+        p = dev_pose(seq.poses[k], cuda)
+        of.integrate(cfg, va, d, p, lam)
+        of.integrate(cfg, vb, d, p, lam, scratch)
+        torch.cuda.synchronize()
+        assert torch.equal(va, vb), f"volumes differ after frame {k}"
+    pose = seq.poses[4]
+    model = of.raycast(cfg, vb, dev_pose(pose, cuda))
+    torch.cuda.synchronize()
+    host = vb.cpu().numpy()
+    q, wt = of.volume_to_linear(cfg, host)
+    assert (wt > 0).sum() > 10000
+    words = (q.astype(np.uint32) | (wt.astype(np.uint32) << 16)).reshape(-1).copy()
+    nb = cfg.resolution // 8
+    flags = host.view(np.uint8)[4 * cfg.resolution ** 3:][: nb ** 3].copy()
+    opts, amb = ora.raycast(cfg, words, pose, ambig=True, flags=flags)
+    v0, n0 = (t.cpu().numpy() for t in of.unpack_points(cfg, model, 0))
+    gv = v0.astype(np.float64)
+    ok = amb == 0
+    hit_g, hit_o = gv[..., 3] > 0, opts[..., 3] > 0
+    assert hit_o.mean() > 0.3, "the scene should be mostly visible"
+    assert (hit_g != hit_o)[ok].mean() < 1e-3
+    both = hit_g & hit_o & ok
+    verr = np.linalg.norm(gv[..., :3][both] - opts[..., :3][both], axis=-1)
+    assert np.quantile(verr, 0.999) < 0.1, f"vertex err q99.9 {np.quantile(verr, 0.999)} mm"
+    for l in range(1, cfg.levels):
+        vl, nl = (t.cpu().numpy() for t in of.unpack_points(cfg, model, l))
+        s = 1 << l
+        assert vl.shape[:2] == ((h + s - 1) // s, (w + s - 1) // s)
+        assert np.array_equal(vl, v0[::s, ::s]) and np.array_equal(nl, n0[::s, ::s])
+
+
 def test_saturated_free_space_is_skipped_exactly(of, cuda):
     """With a maximum weight of 3, free space saturates (+1 at weight 3) after
     three frames; the tiled integration then leaves those bricks unlisted.
