@@ -24,6 +24,12 @@ ICP iterations and per-frame pose error against the ground truth).
 graph per step, knobs tuned online) and, beside it, through one single-stream
 tracker per stream; with N GPUs the streams are sharded longest-first.
 
+`ref_kernels_b200` (a baseline leg, N = 1): the reference's own CUDA kernels
+rebuilt for sm_100a with this workload's volume geometry, driven in the
+reference's frame order on the same frames as the timed region.
+
+`roofline` is the integration stage's, `roofline_raycast` the raycast's.
+
 `--impl reference` runs the CPU implementation of the same equations (the
 FP32 OpenMP build of the oracle restatement) on the host cores.
 """
@@ -55,6 +61,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-kernels", action="store_true",
+                    help="skip the reference's kernels rebuilt for sm_100a (baseline leg)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--warm-frames", type=int, default=121,
                     help="frames of the warm-start comparison (0 = skip it)")
@@ -130,6 +138,15 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
+def profile_figure(name: str, key: str = "dram_bytes_per_launch"):
+    """A figure from an ncu summary under profiles/ (DRAM bytes per launch)."""
+    f = ROOT / "profiles" / name
+    try:
+        return json.loads(f.read_text()).get(key)
+    except (OSError, ValueError):
+        return None
+
+
 def frame_index(i: int, n: int) -> int:
     """Ping-pong through n rendered frames: consecutive steps stay adjacent poses."""
     period = 2 * (n - 1)
@@ -168,6 +185,30 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
+def workload_config(cfg, n_frames: int, world: int) -> dict:
+    """The `config` of both arms' JSON lines: the same workload, worded once."""
+    store = "int16" if cfg.storage == "i16" else "fp16"
+    return {"workload": cfg.name, "width": cfg.width, "height": cfg.height,
+            "volume": f"{cfg.resolution}^3 {store}+uint16 over {cfg.size_mm / 1000:g} m, "
+                      f"truncation {cfg.trunc_mm:g} mm, max weight {cfg.max_weight}",
+            "icp": f"{cfg.levels} levels, {'/'.join(str(i) for i in cfg.iters)} iterations, "
+                   "plain (no warm start)",
+            "frames": f"{n_frames} rendered frames (seed {cfg.seed}), traversed forward and back",
+            "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (512 MiB volume)"}
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def pose_errors(hist, gt):
     rots, trans = [], []
     for P, G in zip(hist, gt):
@@ -193,6 +234,91 @@ def cpu_frames_per_s(cfg, seq, seconds: float):
     dt = time.perf_counter() - t0
     tr.close()
     return n / dt, n, dt, o.threads()
+
+
+# ------------------------------------------------ reference kernels (R1)
+
+def ref_kernels_b200(cfg, seq, order, warmup: int, steps: int) -> dict:
+    """Baseline leg: the reference's own CUDA kernels, rebuilt for sm_100a
+    from its sources with this workload's volume geometry (512^3 over 3 m,
+    truncation 30 mm, max weight 128; raycast step 0.75 voxel), driven in
+    RunApp::display order (Source/src/MainApp.cpp:786-964: integrate ->
+    raycast -> depth upload + updateCameraData -> 15 single-level ICP
+    iterations with the host solve -> UpdateTransforms) on the same frames in
+    the same order as the timed region, after the same warm-up. Frame time is
+    the host wall time of each synchronous frame (the reference synchronises
+    between its stages)."""
+    import ctypes as C
+    lib_path = ROOT / "oracle" / "_ref" / "libref_kernels_c2.so"
+    if not lib_path.exists():
+        return {"unavailable": "oracle/_ref/libref_kernels_c2.so not built (the reference "
+                               "sources were absent at build time)"}
+    lib = C.CDLL(str(lib_path))
+    lib.ref_world_volume.restype = C.c_float
+    lib.ref_truncation.restype = C.c_float
+    geom = (lib.ref_volume_size(), float(lib.ref_world_volume()), float(lib.ref_truncation()),
+            lib.ref_max_weight())
+    if geom != (cfg.resolution, cfg.size_mm, cfg.trunc_mm, cfg.max_weight):
+        return {"unavailable": f"reference kernels built for {geom}, not this workload"}
+
+    class RefCam(C.Structure):
+        _fields_ = [(k, C.c_int32) for k in ("w", "h")] + [
+            (k, C.c_float) for k in ("fx", "fy", "cx", "cy", "ifx", "ify", "icx", "icy",
+                                     "dmin", "dmax")]
+    # inverse intrinsics as CameraFromFile.cpp:42-51 forms them (inverse of K)
+    cam = RefCam(cfg.width, cfg.height, cfg.fx, cfg.fy, cfg.cx, cfg.cy, 1.0 / cfg.fx,
+                 1.0 / cfg.fy, -cfg.cx / cfg.fx, -cfg.cy / cfg.fy, cfg.min_depth_mm,
+                 cfg.max_depth_mm)
+    P = C.c_void_p
+    lib.ref_pipeline_create.argtypes = [P, P]
+    lib.ref_pipeline_frame.argtypes = [P, P, P]
+    pose0 = np.asarray(seq.poses[order[0]], np.float32).reshape(16).copy()
+    if lib.ref_pipeline_create(C.byref(cam), pose0.ctypes.data) != 0:
+        return {"unavailable": "ref_pipeline_create failed"}
+    depth = [np.ascontiguousarray(seq.depth[j], np.uint16) for j in order]
+    po = np.zeros(16, np.float32)
+    t = C.c_double()
+    ms, hist = [], []
+    for i in range(len(order)):
+        rc = lib.ref_pipeline_frame(depth[i].ctypes.data, po.ctypes.data, C.byref(t))
+        if rc != 0:
+            return {"unavailable": f"ref_pipeline_frame returned {rc} at frame {i}"}
+        if i > warmup:
+            ms.append(t.value)
+            hist.append(po.reshape(4, 4).astype(np.float64))
+    rots, trans = pose_errors(hist, [seq.poses[j] for j in order[1 + warmup:]])
+    total_ms = float(np.sum(ms))
+    return {"frames_per_s": len(ms) / (total_ms / 1e3), "ms_per_frame": total_ms / len(ms),
+            "frames": len(ms), "warmup": warmup,
+            "how": "host wall time per synchronous frame (std::chrono), same frames as the "
+                   "timed region",
+            "geometry": "512^3 over 3000 mm, truncation 30 mm, max weight 128 (generated "
+                        "Constants.h); raycast step 1.5 mm x 3000/1024 = 0.75 voxel",
+            "icp": "1 level x 15 iterations, FP32 host solve (ICP.cpp:84-182)",
+            "max_rot_err_deg": float(np.degrees(max(rots))), "max_trans_err_mm": float(max(trans))}
+
+
+def cpp_shim_leg(frames: int) -> dict:
+    """The same workload through the reference-shaped C++ classes
+    (include/openfusion_b200.hpp) with the reference's own call lines and
+    order: Integrate -> Raycast -> synchronous depth upload +
+    CameraHandler::updateCameraData -> ICP::Iterate_ICP ->
+    General::Instance()->UpdateTransforms, one call per stage per frame on the
+    legacy default stream, no graph (tests/cpp/shim_track.cpp; CUDA events
+    around the frame loop after two warm-up frames). The drop-in path a
+    reference host gets by linking the shim."""
+    exe = ROOT / "tests" / "cpp" / "_build" / "shim_track"
+    if not exe.exists():
+        return {"unavailable": "tests/cpp/_build/shim_track not built"}
+    try:
+        out = subprocess.run([str(exe), str(frames), "c2"], capture_output=True, text=True,
+                             timeout=600)
+        res = json.loads(out.stdout.strip().splitlines()[-1])
+    except Exception as e:  # report, never fail the bench line
+        return {"unavailable": f"shim run failed: {e}"}
+    res["how"] = ("reference call lines through include/openfusion_b200.hpp, per-stage calls, "
+                  "synchronous pageable depth upload per frame, CUDA events")
+    return res
 
 
 # ------------------------------------------------------------------- arms
@@ -225,11 +351,11 @@ def run_reference(args, cfg, world, rank):
         "impl": "reference", "metric": METRIC, "value": fps, "unit": "frames/s",
         "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * dt / steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded analytic room scene)",
-        "config": {"workload": cfg.name, "width": cfg.width, "height": cfg.height,
-                   "volume": f"{cfg.resolution}^3 over {cfg.size_mm / 1000:g} m",
-                   "icp_iters": list(cfg.iters), "frames_requested": args.steps},
-        "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": o.threads(), "kind": "port",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded analytic room scene, axial noise + 2% dropout)",
+        "config": workload_config(cfg, n_seq, args.gpus),
+        "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": o.threads(),
+                         "cpu_model": cpu_model(), "kind": "port",
                          "sample": f"{steps} consecutive frames after {args.warmup} warm-up "
                                    "frames (FP32 OpenMP restatement of the same equations)"},
         "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0,
@@ -334,24 +460,13 @@ def run_ours(args, cfg, world, rank, local):
     sweep_bytes = 8.0 * cfg.resolution ** 3 + 2.0 * cfg.width * cfg.height
     sweep_gbps = sweep_bytes / (stages["integrate_ms"] / 1e3) / 1e9
     achieved = integ_bytes / (stages["integrate_ms"] / 1e3) / 1e9
-    traffic = None
-    tf = ROOT / "profiles" / "integrate_traffic.json"
-    if tf.exists():
-        try:
-            traffic = json.loads(tf.read_text()).get("dram_bytes_per_launch")
-        except Exception:
-            traffic = None
+    traffic = profile_figure("integrate_traffic.json")
     line = {
         "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded analytic room scene, axial noise + 2% dropout)",
-        "config": {"workload": cfg.name, "width": cfg.width, "height": cfg.height,
-                   "volume": f"{cfg.resolution}^3 int16+uint16 over {cfg.size_mm / 1000:g} m",
-                   "icp": "3 levels, 10/5/4 iterations, plain (no warm start)",
-                   "frames": f"{n_seq} rendered frames, traversed forward and back",
-                   "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (512 MiB volume)"},
+        "config": workload_config(cfg, n_seq, world),
         "stages_ms": {k: v for k, v in stages.items() if k.endswith("_ms")},
         "pose_error": {"max_rot_deg": float(np.degrees(max(rots))),
                        "max_trans_mm": float(max(trans)),
@@ -368,6 +483,17 @@ def run_ours(args, cfg, world, rank, local):
                      "updated_voxels_per_launch": stages["integrate_updated_voxels"],
                      "frac_updated_voxels": stages["integrate_updated_bytes"] /
                                             (stages["integrate_ms"] / 1e3) / 1e9 / peak},
+        "roofline_raycast": {
+            "kernel": "k_raycast", "bound": "hbm",
+            "achieved": stages["raycast_alg_bytes"] / (stages["raycast_ms"] / 1e3) / 1e9,
+            "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+            "frac": stages["raycast_alg_bytes"] / (stages["raycast_ms"] / 1e3) / 1e9 / peak,
+            "traffic": profile_figure("raycast_traffic.json"),
+            "alg_bytes_per_launch": stages["raycast_alg_bytes"],
+            "alg_samples_per_launch": stages["raycast_samples"],
+            "alg_units": "2 B per sample of a plain march at 0.75 voxel from the ray's entry "
+                         "(box of voxel centres, depth range) to its surface or exit, 8 samples "
+                         "per hit for the trilinear refinement, + 24 B per pixel out"},
         "frame_ms": {"median": float(np.median(per_frame)), "p10": float(np.percentile(per_frame, 10)),
                      "p90": float(np.percentile(per_frame, 90)), "frames": int(nf),
                      "how": "CUDA events between graph-replayed steps (rank 0)"},
@@ -384,9 +510,18 @@ def run_ours(args, cfg, world, rank, local):
         line["warm_start"] = warm
     if batched is not None:
         line["batched_streams"] = batched
+    if world == 1:
+        line["e2e_cpp_shim"] = cpp_shim_leg(args.steps + 3)
+    if world == 1 and not args.no_ref_kernels:
+        ref = ref_kernels_b200(cfg, seq, order, args.warmup, args.steps)
+        if "frames_per_s" in ref:
+            ref["value_over_reference_kernels"] = fps / ref["frames_per_s"]
+            ref["e2e_over_reference_kernels"] = e2e_fps / ref["frames_per_s"]
+        line["ref_kernels_b200"] = ref
     if world == 1 and not args.no_cpu_baseline:
         cps, n, dt, cores = cpu_frames_per_s(cfg, seq, args.cpu_seconds)
-        line["cpu_baseline"] = {"value": cps, "unit": "frames/s", "cores": cores, "kind": "port",
+        line["cpu_baseline"] = {"value": cps, "unit": "frames/s", "cores": cores,
+                                "cpu_model": cpu_model(), "kind": "port",
                                 "sample": f"{n} consecutive frames ({dt:.1f} s) of the same "
                                           "sequence, FP32 OpenMP restatement"}
     print(json.dumps(line), flush=True)
@@ -490,6 +625,7 @@ def batched_streams(of, args, dev, world, rank):
     e1.record(stream)
     torch.cuda.synchronize()
     ms_seq = max_over_ranks(e0.elapsed_time(e1), world)
+    err_seq = [pose_errors([t.pose()[0]], [seqs[k][0][order[-1]]]) for k, t in enumerate(trackers)]
     for t in trackers:
         t.close()
     del trackers
@@ -504,8 +640,24 @@ def batched_streams(of, args, dev, world, rank):
                    "icp_clusters": int(tun.icp_clusters), "tuned": int(tun.tuned)},
         "max_rot_err_deg_last_step": float(np.degrees(max(e[0][0] for e in err))),
         "max_trans_err_mm_last_step": float(max(e[1][0] for e in err)),
+        # the same streams through single-stream trackers: the drift against
+        # the ground truth is the method's on that stream, not the batching's
+        "single_stream_max_rot_err_deg_last_step": float(np.degrees(max(e[0][0] for e in err_seq))),
+        "single_stream_max_trans_err_mm_last_step": float(max(e[1][0] for e in err_seq)),
+        "worst_stream": worst_stream(mine, err, err_seq),
     })
     return out
+
+
+def worst_stream(cfgs, err_batch, err_single):
+    """The stream with the largest last-step translation error of the batch,
+    with both paths' errors against the ground truth."""
+    k = int(np.argmax([e[1][0] for e in err_batch]))
+    return {"name": cfgs[k].name, "size_mm": cfgs[k].size_mm, "trunc_mm": cfgs[k].trunc_mm,
+            "batched_rot_deg": float(np.degrees(err_batch[k][0][0])),
+            "batched_trans_mm": float(err_batch[k][1][0]),
+            "single_stream_rot_deg": float(np.degrees(err_single[k][0][0])),
+            "single_stream_trans_mm": float(err_single[k][1][0])}
 
 
 def stage_times(of, cfg, seq, depth_dev, order, args, dev):
@@ -526,6 +678,7 @@ def stage_times(of, cfg, seq, depth_dev, order, args, dev):
     poses = [pose.clone()]
     n = 0
     total = len(order)
+    ray_samples, ray_pixels = [], []
     for i in range(1, total):
         d = depth_dev[order[i]]
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
@@ -546,6 +699,16 @@ def stage_times(of, cfg, seq, depth_dev, order, args, dev):
             for j, name in enumerate(acc):
                 acc[name] += ev[j].elapsed_time(ev[j + 1])
             n += 1
+            if (i - args.warmup) % 10 == 1:
+                # the raycast's algorithmic samples at this frame's pose, from
+                # the surface distances the launch found (outside the timing)
+                v, _ = of.unpack_points(cfg, model, 0)
+                v = v.cpu().numpy().astype(np.float64)
+                P = pose.cpu().numpy().reshape(4, 4)
+                dist = np.linalg.norm(v[..., :3] - P[:3, 3], axis=-1)
+                smp, _ = of.raycast_march_samples(cfg, P, v[..., 3] > 0, dist)
+                ray_samples.append(smp)
+                ray_pixels.append(cfg.width * cfg.height)
     # Algorithmic bytes of one integration launch: 4 B read + 4 B write per
     # voxel in view (centre inside the 2-pixel border, depth in [min, max])
     # plus 2 B per depth pixel; beside it the stricter count of the voxels the
@@ -561,6 +724,10 @@ def stage_times(of, cfg, seq, depth_dev, order, args, dev):
             vis.append(of.integrate_visible_census(cfg, vol2, d, poses[i], lam))
         of.integrate(cfg, vol2, d, poses[i], lam, scratch)
     out = {f"{k}_ms": v / max(n, 1) for k, v in acc.items()}
+    # raycast: 2 B (one int16 tsdf) per algorithmic sample + 24 B (vertex and
+    # normal, 3 floats each) per pixel written
+    out["raycast_samples"] = float(np.mean(ray_samples))
+    out["raycast_alg_bytes"] = 2.0 * float(np.mean(ray_samples)) + 24.0 * float(np.mean(ray_pixels))
     out["integrate_alg_bytes"] = 8.0 * float(np.mean(vis)) + 2.0 * cfg.width * cfg.height
     out["integrate_visible_voxels"] = float(np.mean(vis))
     out["integrate_updated_bytes"] = 8.0 * float(np.mean(upd)) + 2.0 * cfg.width * cfg.height

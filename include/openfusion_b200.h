@@ -268,11 +268,14 @@ of_status_t of_icp_track_warm(const of_camera_t *cam, const of_icp_params_t *par
  * allocates nothing: its scratch is one file-scope device array of about
  * 186 KB (per-block partial sums for at most 296 cooperating blocks) that every
  * GPU loading the library holds until the process exits; a device that would
- * need more blocks gets OF_ERR_TOO_LARGE. The first call on a device looks up
- * and zeroes that array (with the device current) and should come before any
- * stream capture. All calls share the one array and each starts by clearing
- * the state it needs cleared; calls whose executions overlap on the GPU race
- * with each other -- order them on one stream. Results equal of_icp_track's. */
+ * need more blocks gets OF_ERR_TOO_LARGE. Every call looks up the array's
+ * device address in the current context with cudaGetSymbolAddress (no
+ * allocation, no synchronisation); on a device's first call that lookup may
+ * load the library's device code, so make that first call before any stream
+ * capture. The array starts zeroed when the device code loads. All calls
+ * share the one array and each starts by clearing the state it needs
+ * cleared; calls whose executions overlap on the GPU race with each other --
+ * order them on one stream. Results equal of_icp_track's bit for bit. */
 of_status_t of_icp_track_static(const of_camera_t *cam, const of_icp_params_t *params,
                                 const void *d_frame, const void *d_model, double *d_pose,
                                 of_icp_stats_t *d_stats, of_stream_t stream);
@@ -288,6 +291,16 @@ of_status_t of_icp_workspace_hold_barrier(void *d_workspace, int32_t extra, of_s
 of_status_t of_icp_system(const of_camera_t *cam, const of_icp_params_t *params, int32_t level,
                           const void *d_frame, const void *d_model, const double *d_pose,
                           void *d_workspace, float *d_system, of_stream_t stream);
+/* One solve-and-compose step on a system of_icp_system wrote: replaces the
+ * host half of an ICP::Iterate_ICP iteration (ICP.cpp:142-168: symmetrise,
+ * singularity test, LLT solve, rotation part negated) and
+ * ICP::BuildNewTransformMatrix (ICP.cu:320-340: dT = [Rz Ry Rx | t],
+ * T <- dT T), in FP64 on the device with the tracking kernels' own solve.
+ * A singular system (a pivot not above 1e-12 x the largest diagonal entry, or
+ * fewer than 6 inliers) leaves `d_pose` unchanged and reports status 1 in
+ * `d_stats` (device, may be NULL; iterations = 1). */
+of_status_t of_icp_solve_step(const float *d_system, double *d_pose, of_icp_stats_t *d_stats,
+                              of_stream_t stream);
 
 /* ---- camera-side depth filters ---------------------------------------- */
 

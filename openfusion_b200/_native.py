@@ -139,6 +139,7 @@ _SIGS = {
                                        c_stream]),
     "of_icp_system": (c_status, [C.POINTER(Camera), C.POINTER(IcpParams), C.c_int32, P, P, P, P,
                                  P, c_stream]),
+    "of_icp_solve_step": (c_status, [P, P, P, c_stream]),
     "of_tracker_create": (c_status, [C.POINTER(TrackerDesc), C.POINTER(C.c_void_p)]),
     "of_tracker_destroy": (c_status, [P]),
     "of_tracker_process": (c_status, [P, P, C.c_int32, c_stream]),

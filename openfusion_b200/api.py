@@ -235,6 +235,43 @@ def raycast(cfg: Config, vol, pose, model=None, rgba=None):
     return model
 
 
+def raycast_march_samples(cfg: Config, pose: np.ndarray, hit: np.ndarray,
+                          hit_dist: np.ndarray) -> tuple[int, int]:
+    """The algorithmic sample count of one raycast launch: for every pixel's
+    ray (through the pixel at z = -1, Raycaster.cu:112-125), the volume reads
+    of a plain march at 0.75 voxel from where the ray enters the box of voxel
+    centres within the depth range to its surface (`hit`, at distance
+    `hit_dist` mm from the camera) or to where it leaves, counting the sample
+    at the start, plus 8 reads for the trilinear refinement of a hit. This is
+    what a kernel without empty-space skipping reads; it is the roofline's
+    unit, not what this library's raycast reads. Host arithmetic in FP64.
+    Returns (samples, rays that enter the box)."""
+    P = np.asarray(pose, np.float64).reshape(4, 4)
+    ys, xs = np.mgrid[0:cfg.height, 0:cfg.width].astype(np.float64)
+    dc = np.stack([-(xs - cfg.cx) / cfg.fx, -(ys - cfg.cy) / cfg.fy, -np.ones_like(xs)], -1)
+    lam = np.linalg.norm(dc, axis=-1)
+    d = (dc @ P[:3, :3].T) / lam[..., None]
+    o = P[:3, 3]
+    vs = cfg.size_mm / cfg.resolution
+    lo, hi = -0.5 * cfg.size_mm + 0.5 * vs, 0.5 * cfg.size_mm - 0.5 * vs
+    with np.errstate(divide="ignore", invalid="ignore"):
+        t_a = (lo - o) / d
+        t_b = (hi - o) / d
+    par = np.abs(d) < 1e-12
+    inside = (o >= lo) & (o <= hi)
+    t_near = np.where(par, np.where(inside, -np.inf, np.inf), np.minimum(t_a, t_b)).max(-1)
+    t_far = np.where(par, np.where(inside, np.inf, -np.inf), np.maximum(t_a, t_b)).min(-1)
+    t0 = np.maximum(t_near, cfg.min_depth_mm * lam)
+    t1 = np.minimum(t_far, cfg.max_depth_mm * lam)
+    enters = t0 < t1
+    hit = np.asarray(hit, bool) & enters
+    t_end = np.where(hit, np.asarray(hit_dist, np.float64), t1)
+    step = 0.75 * vs
+    n = np.where(enters & (t_end >= t0), np.floor((t_end - t0) / step) + 1.0, 0.0)
+    n += np.where(hit, 8.0, 0.0)
+    return int(n.sum()), int(enters.sum())
+
+
 def icp_workspace(cfg: Config, device="cuda"):
     import torch
     n = C.c_size_t()
@@ -267,6 +304,23 @@ def icp_system(cfg: Config, level: int, frame, model, pose, ws):
                                                    level, _ptr(frame), _ptr(model), _ptr(pose),
                                                    _ptr(ws), _ptr(out), _stream()))
     return out
+
+
+class _DeviceBytes:
+    """A device range described by the CUDA array interface (no copy)."""
+
+    def __init__(self, ptr: int, nbytes: int):
+        self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1",
+                                         "data": (int(ptr), False), "version": 3}
+
+
+def copy_pyramid(cfg: Config, ptr: int, device="cuda"):
+    """A copy (uint8 CUDA tensor) of the frame or model pyramid at device
+    address `ptr`, e.g. a Tracker's or a Batch stream's `buffers().frame` /
+    `.model`, ordered on the current stream."""
+    import torch
+    src = torch.as_tensor(_DeviceBytes(ptr, int(pyramid_layout(cfg).total_bytes)), device=device)
+    return src.clone()
 
 
 def unpack_points(cfg: Config, pyr, level: int = 0):

@@ -110,21 +110,32 @@ of_status_t enqueue_track(of_tracker *t, int cur, bool fuse, cudaStream_t s) {
   const uint16_t *now = t->depth[cur], *before = t->depth[cur ^ 1];
   of_status_t sflt = enqueue_filters(t, cur, s);
   if (sflt != OF_OK) return sflt;
-  OF_CUDA_TRY(cudaEventRecord(t->ev_fork, s));
-  OF_CUDA_TRY(cudaStreamWaitEvent(t->pre, t->ev_fork, 0));
-  of_status_t st = OF_OK;
-  if (t->warm) {
-    OF_CUDA_TRY(cudaStreamWaitEvent(t->side, t->ev_fork, 0));
+  OF_CUDA_TRY(cudaEventRecord(t->ev_fork, s));  // nothing has forked before this
+  // From the fork on, a failed call is remembered rather than returned at
+  // once, so that every branch that forked also joins `s` before the error is
+  // returned (a capture must end joined).
+  cudaError_t first = cudaSuccess;
+  auto ok = [&first](cudaError_t e) {
+    if (e != cudaSuccess && first == cudaSuccess) first = e;
+    return e == cudaSuccess;
+  };
+  const bool pre_forked = ok(cudaStreamWaitEvent(t->pre, t->ev_fork, 0));
+  const bool side_forked = t->warm && ok(cudaStreamWaitEvent(t->side, t->ev_fork, 0));
+  of_status_t st = OF_OK, sp = OF_OK;
+  bool cnn_recorded = false, pre_recorded = false;
+  if (side_forked) {
     st = of_cnn_predict(t->cnn_params, t->cnn_master, before, now, d.camera.width,
                         d.camera.height, t->pose, t->cnn_out, t->warm_pose, t->side);
-    OF_CUDA_TRY(cudaEventRecord(t->ev_cnn, t->side));
+    cnn_recorded = ok(cudaEventRecord(t->ev_cnn, t->side));
   }
-  of_status_t sp = of_preprocess(&d.camera, &d.filter, now, d.camera.width, t->frame, t->pre);
-  OF_CUDA_TRY(cudaEventRecord(t->ev_pre, t->pre));
+  if (pre_forked) {
+    sp = of_preprocess(&d.camera, &d.filter, now, d.camera.width, t->frame, t->pre);
+    pre_recorded = ok(cudaEventRecord(t->ev_pre, t->pre));
+  }
   of_status_t sf = fuse ? enqueue_fuse(t, before, s) : OF_OK;
-  // every branch joins before an error returns (a capture must end joined)
-  OF_CUDA_TRY(cudaStreamWaitEvent(s, t->ev_pre, 0));
-  if (t->warm) OF_CUDA_TRY(cudaStreamWaitEvent(s, t->ev_cnn, 0));
+  if (pre_recorded) ok(cudaStreamWaitEvent(s, t->ev_pre, 0));
+  if (cnn_recorded) ok(cudaStreamWaitEvent(s, t->ev_cnn, 0));
+  if (first != cudaSuccess) return of_set_cuda_error(first);
   if (st != OF_OK) return st;
   if (sp != OF_OK) return sp;
   if (sf != OF_OK) return sf;

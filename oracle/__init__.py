@@ -28,6 +28,18 @@ class Vol(C.Structure):
                 ("trunc", C.c_double), ("max_w", C.c_int32), ("pad", C.c_int32)]
 
 
+class IcpOpts(C.Structure):
+    _fields_ = [("stop_rot", C.c_double), ("stop_trans", C.c_double), ("warm_levels", C.c_int32),
+                ("pad", C.c_int32), ("judge_rms", C.c_double), ("judge_frac", C.c_double),
+                ("judge_rot", C.c_double), ("judge_trans", C.c_double)]
+
+
+class IcpResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("warm", C.c_int32),
+                ("inliers", C.c_int32), ("examined", C.c_int32), ("decisions_near", C.c_int32),
+                ("residual_sq", C.c_double)]
+
+
 class RefCam(C.Structure):
     _fields_ = [("w", C.c_int32), ("h", C.c_int32), ("fx", C.c_double), ("fy", C.c_double),
                 ("cx", C.c_double), ("cy", C.c_double), ("ifx", C.c_double), ("ify", C.c_double),
@@ -83,6 +95,9 @@ class Oracle:
         L.ora_icp_step.restype = C.c_int32
         L.ora_icp_track.argtypes = [C.POINTER(Cam), C.POINTER(Params), P, P, P, P]
         L.ora_icp_track.restype = C.c_int32
+        L.ora_icp_track_ex.argtypes = [C.POINTER(Cam), C.POINTER(Params), C.POINTER(IcpOpts), P,
+                                       P, P, P, C.POINTER(IcpResult)]
+        L.ora_icp_track_ex.restype = C.c_int32
         L.ora_ref_convert.argtypes = [C.POINTER(RefCam), P, P, P, P]
         L.ora_ref_integrate_voxels.argtypes = [C.POINTER(RefVol), C.POINTER(RefCam), P, P, P, P,
                                                C.c_int64, P, P, P, P, P]
@@ -210,6 +225,26 @@ class Oracle:
                              None if am is None else am.ctypes.data)
         return pts, am
 
+    @staticmethod
+    def shade_rgba(cfg, pose: np.ndarray, normals: np.ndarray) -> np.ndarray:
+        """The raycast's shaded view (showNormal false) in FP64, from world
+        normals [H, W, 3] (zero where the ray missed): the ray of pixel (x, y)
+        through the pixel at z = -1, rotated by the pose and normalised
+        (Raycaster.cu:112-125); g = 0.6 (-d . n) + 0.2, black where |d . n| is
+        below epsilon (Raycaster.cu:219-227); packed by rgbaFloatToInt
+        (Raycaster.cu:26-33): each channel saturated to [0, 1], times 255,
+        truncated; alpha 0. Returns uint32 [H, W]."""
+        P = np.asarray(pose, np.float64)
+        ys, xs = np.mgrid[0:cfg.height, 0:cfg.width].astype(np.float64)
+        dc = np.stack([-(xs - cfg.cx) / cfg.fx, -(ys - cfg.cy) / cfg.fy,
+                       -np.ones_like(xs)], -1)
+        dw = dc @ P[:3, :3].T
+        d = dw / np.linalg.norm(dw, axis=-1, keepdims=True)
+        dot = -(d * np.asarray(normals, np.float64)).sum(-1)
+        g = np.where(np.abs(dot) < 1e-6, 0.0, 0.6 * dot + 0.2)
+        q = np.floor(np.clip(g, 0.0, 1.0) * 255.0).astype(np.uint32)
+        return (q << 16) | (q << 8) | q
+
     def model_pyramid(self, cfg, pts0: np.ndarray):
         lv = [np.ascontiguousarray(pts0, self.real)]
         for (w, h) in self.level_dims(cfg)[1:]:
@@ -277,6 +312,20 @@ class Oracle:
                                     frame_buf.ctypes.data, model_buf.ctypes.data, P_.ctypes.data,
                                     C.byref(its))
         return st, P_, its.value
+
+    def icp_track_ex(self, cfg, frame_buf: np.ndarray, model_buf: np.ndarray, pose: np.ndarray,
+                     warm: np.ndarray | None = None):
+        """ora_icp_track_ex with cfg's early exit (stop_rot_rad, stop_trans_mm),
+        warm_levels and judge thresholds; returns (pose, IcpResult)."""
+        P_ = np.array(pose, np.float64, copy=True)
+        W = None if warm is None else np.ascontiguousarray(warm, np.float64)
+        o = IcpOpts(cfg.stop_rot_rad, cfg.stop_trans_mm, cfg.warm_levels, 0, cfg.judge_max_rms_mm,
+                    cfg.judge_min_inlier_frac, cfg.judge_max_rot_rad, cfg.judge_max_trans_mm)
+        r = IcpResult()
+        self.lib.ora_icp_track_ex(C.byref(self.cam(cfg)), C.byref(self.params(cfg)), C.byref(o),
+                                  frame_buf.ctypes.data, model_buf.ctypes.data, P_.ctypes.data,
+                                  None if W is None else W.ctypes.data, C.byref(r))
+        return P_, r
 
     def threads(self) -> int:
         return self.lib.ora_threads()

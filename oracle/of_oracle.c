@@ -590,7 +590,7 @@ void ora_model_down(const R *src, int32_t sw, R *dst, int32_t dw, int32_t dh) {
  * the projected coordinate is used on the axes whose bit is set. */
 static int icp_row(const ora_cam *lc, const R *frame, const R *s, const R *ns, const double *P,
                    const double *W, double dist, double nthr, int alt, R *a, R *b, int *gate_amb,
-                   int *round_amb) {
+                   int *round_amb, int *projected) {
   R sc[3];
   for (int r = 0; r < 3; ++r)
     sc[r] = (R)W[4 * r] * s[0] + (R)W[4 * r + 1] * s[1] + (R)W[4 * r + 2] * s[2] + (R)W[4 * r + 3];
@@ -602,6 +602,7 @@ static int icp_row(const ora_cam *lc, const R *frame, const R *s, const R *ns, c
   if (alt & 1) pu = (uf - floor(uf) < 0.5) ? pu + 1 : pu - 1;
   if (alt & 2) pv = (vf - floor(vf) < 0.5) ? pv + 1 : pv - 1;
   if (pu < 0 || pu >= lc->w || pv < 0 || pv >= lc->h) return 0;
+  if (projected) *projected = 1;  /* the model point lands in the frame: examined */
   const R *f = frame + 8 * ((size_t)pv * lc->w + pu);
   if (f[3] == 0 || f[7] == 0) return 0;
   R d[3], nd[3];
@@ -649,25 +650,29 @@ static void rigid_inverse(const double *P, double *W) {
   W[15] = 1.0;
 }
 
-void ora_icp_system(const ora_cam *lc, const R *frame, int32_t mw, int32_t mh, const R *model,
-                    const double *P, double dist, double nthr, double *out, double *amb) {
+/* One correspondence pass (see ora_icp_system); `examined` (may be NULL)
+ * gets the number of model points that project into the frame. */
+static void icp_system_impl(const ora_cam *lc, const R *frame, int32_t mw, int32_t mh,
+                            const R *model, const double *P, double dist, double nthr,
+                            double *out, double *amb, double *examined) {
   double W[16];
   rigid_inverse(P, W);
   const int npx = mw * mh;
-  double acc[29] = {0}, am[29] = {0};
+  double acc[29] = {0}, am[29] = {0}, ex = 0.0;
   /* rows accumulate per image row, rows combine in order: deterministic */
-  double *rows = (double *)calloc((size_t)mh * 58, sizeof(double));
+  double *rows = (double *)calloc((size_t)mh * 59, sizeof(double));
 #pragma omp parallel for schedule(static)
   for (int y = 0; y < mh; ++y) {
-    double *ra = rows + (size_t)y * 58, *rm = ra + 29;
+    double *ra = rows + (size_t)y * 59, *rm = ra + 29;
     for (int x = 0; x < mw; ++x) {
       size_t p = (size_t)y * mw + x;
       const R *s = model + 8 * p;
       if (s[3] == 0 || s[7] == 0) continue;
       R a[6], b;
-      int gamb = 0, ramb = 0;
+      int gamb = 0, ramb = 0, proj = 0;
       double v[29];
-      int ok = icp_row(lc, frame, s, s + 4, P, W, dist, nthr, 0, a, &b, &gamb, &ramb);
+      int ok = icp_row(lc, frame, s, s + 4, P, W, dist, nthr, 0, a, &b, &gamb, &ramb, &proj);
+      ra[58] += proj;
       if (ok) row_products(a, b, v);
       if (ok == 1)
         for (int q = 0; q < 29; ++q) ra[q] += v[q];
@@ -677,7 +682,8 @@ void ora_icp_system(const ora_cam *lc, const R *frame, int32_t mw, int32_t mh, c
         for (int alt = 1; alt < 4; ++alt) {
           if ((alt & ramb) != alt) continue;
           R a2[6], b2;
-          if (icp_row(lc, frame, s, s + 4, P, W, dist, nthr, alt, a2, &b2, NULL, NULL) == 1) {
+          if (icp_row(lc, frame, s, s + 4, P, W, dist, nthr, alt, a2, &b2, NULL, NULL, NULL) ==
+              1) {
             row_products(a2, b2, v);
             for (int q = 0; q < 29; ++q) rm[q] += fabs(v[q]);
           }
@@ -686,15 +692,23 @@ void ora_icp_system(const ora_cam *lc, const R *frame, int32_t mw, int32_t mh, c
     }
   }
   (void)npx;
-  for (int y = 0; y < mh; ++y)
+  for (int y = 0; y < mh; ++y) {
     for (int q = 0; q < 29; ++q) {
-      acc[q] += rows[(size_t)y * 58 + q];
-      am[q] += rows[(size_t)y * 58 + 29 + q];
+      acc[q] += rows[(size_t)y * 59 + q];
+      am[q] += rows[(size_t)y * 59 + 29 + q];
     }
+    ex += rows[(size_t)y * 59 + 58];
+  }
   free(rows);
   for (int q = 0; q < 29; ++q) out[q] = acc[q];
   if (amb)
     for (int q = 0; q < 29; ++q) amb[q] = am[q];
+  if (examined) *examined = ex;
+}
+
+void ora_icp_system(const ora_cam *lc, const R *frame, int32_t mw, int32_t mh, const R *model,
+                    const double *P, double dist, double nthr, double *out, double *amb) {
+  icp_system_impl(lc, frame, mw, mh, model, P, dist, nthr, out, amb, NULL);
 }
 
 /* FP64 Cholesky solve of the 6x6 normal equations and the SE(3) update:
@@ -703,7 +717,15 @@ void ora_icp_system(const ora_cam *lc, const R *frame, int32_t mw, int32_t mh, c
  * (Source/src/ICP.cu:266-305: dT = [Rz(g) Ry(b) Rx(a) | t], T <- dT T). The
  * singularity test is a pivot below 1e-12 x the largest diagonal entry or
  * fewer than 6 inliers, in place of |det| < 1e-6 in FP32. */
+static int32_t icp_solve_step(const double *sys, double *P, double *minpiv, double *x_out);
+
 int32_t ora_icp_step(const double *sys, double *P, double *minpiv) {
+  return icp_solve_step(sys, P, minpiv, NULL);
+}
+
+/* as ora_icp_step; x_out (may be NULL) gets the solution x of H x = g before
+ * the rotation part is negated */
+static int32_t icp_solve_step(const double *sys, double *P, double *minpiv, double *x_out) {
   double H[6][6], L[6][6] = {{0}}, g[6], y[6], x[6];
   int q = 0;
   for (int i = 0; i < 6; ++i)
@@ -737,6 +759,8 @@ int32_t ora_icp_step(const double *sys, double *P, double *minpiv) {
     for (int k = i + 1; k < 6; ++k) t -= L[k][i] * x[k];
     x[i] = t / L[i][i];
   }
+  if (x_out)
+    for (int i = 0; i < 6; ++i) x_out[i] = x[i];
   double xo[6] = {-x[0], -x[1], -x[2], x[3], x[4], x[5]};
   double D[16];
   euler_increment(xo, D);
@@ -783,6 +807,100 @@ int32_t ora_icp_track(const ora_cam *c, const ora_params *p, const R *frame, con
   }
   if (iterations) *iterations = its;
   return 0;
+}
+
+/* Multi-level ICP with the device path's options, in FP64: the early exit, a
+ * warm-started first pass and the judge that keeps or replaces its result.
+ * Neither has a reference counterpart (the reference starts from the
+ * previous pose and runs every iteration, Source/src/ICP.cpp:84-182); this
+ * restates the project's own method so the device kernel can be checked
+ * against it step by step:
+ *   - a level ends early once the increment's rotation components are all
+ *     below stop_rot (rad) and its translation components all below
+ *     stop_trans (mm), when stop_rot > 0;
+ *   - with a warm start W, pass 0 starts from W and runs only the
+ *     warm_levels finest levels; its result is kept when the system did not
+ *     become singular, the last iteration's RMS point-to-plane residual is at
+ *     most judge_rms, its inliers are at least judge_frac of the model points
+ *     that landed in the frame, and the result lies within judge_rot (rad,
+ *     angle of W^T P) and judge_trans (mm) of W; otherwise pass 1 runs plain
+ *     ICP from the starting pose over every level;
+ *   - a singular system restores the starting pose and ends the pass
+ *     (ICP.cpp:152-158).
+ * res->decisions_near counts exit and judge decisions whose quantity lies
+ * within 1 % of its threshold (where FP32 and FP64 may decide differently). */
+static int near_threshold(double q, double thr) { return fabs(q - thr) <= 0.01 * fabs(thr); }
+
+int32_t ora_icp_track_ex(const ora_cam *c, const ora_params *p, const ora_icp_opts *o,
+                         const R *frame, const R *model, double *P, const double *warm,
+                         ora_icp_result *res) {
+  const R *fd[4], *fp[4], *md[4], *mp[4];
+  ora_cam lc[4];
+  pyramid_levels(c, p->levels, frame, fd, fp, lc);
+  pyramid_levels(c, p->levels, model, md, mp, lc);
+  double P0[16];
+  memcpy(P0, P, sizeof(P0));
+  const int warm_levels = (o->warm_levels > 0 && o->warm_levels < p->levels) ? o->warm_levels
+                                                                             : p->levels;
+  int its = 0, stop = 0, warm_status = 0, near = 0, inl = 0, examined = 0;
+  double res_sq = 0.0;
+  if (warm) memcpy(P, warm, 16 * sizeof(double));
+  for (int pass = 0; pass < 2; ++pass) {
+    const int top = (pass == 0 && warm) ? warm_levels - 1 : p->levels - 1;
+    for (int l = top; l >= 0 && !stop; --l) {
+      for (int it = 0; it < p->iters[l]; ++it) {
+        double sys[29], ex = 0.0, x[6], mp_ = 0.0;
+        icp_system_impl(&lc[l], fp[l], lc[l].w, lc[l].h, mp[l], P, p->dist_thresh,
+                        p->normal_thresh, sys, NULL, &ex);
+        ++its;
+        inl = (int)sys[28];
+        examined = (int)ex;
+        res_sq = sys[27];
+        if (icp_solve_step(sys, P, &mp_, x) != 0) {
+          memcpy(P, P0, sizeof(P0));
+          stop = 1;
+          break;
+        }
+        if (o->stop_rot > 0.0) {
+          const double ir = fmax(fabs(x[0]), fmax(fabs(x[1]), fabs(x[2])));
+          const double it_ = fmax(fabs(x[3]), fmax(fabs(x[4]), fabs(x[5])));
+          near += near_threshold(ir, o->stop_rot) || near_threshold(it_, o->stop_trans);
+          if (ir < o->stop_rot && it_ < o->stop_trans) break;
+        }
+      }
+    }
+    if (pass == 1 || !warm) break;
+    int keep = !stop;
+    if (keep) {
+      double tr = 0.0, dt2 = 0.0;
+      for (int i = 0; i < 3; ++i) {
+        for (int k = 0; k < 3; ++k) tr += warm[4 * k + i] * P[4 * k + i];
+        const double d = P[4 * i + 3] - warm[4 * i + 3];
+        dt2 += d * d;
+      }
+      const double rot = acos(fmin(1.0, fmax(-1.0, 0.5 * (tr - 1.0))));
+      const double rms = sqrt(res_sq / (double)(inl > 1 ? inl : 1));
+      const double frac = (double)inl / (double)(examined > 1 ? examined : 1);
+      near += near_threshold(rms, o->judge_rms) || near_threshold(frac, o->judge_frac) ||
+              near_threshold(rot, o->judge_rot) || near_threshold(sqrt(dt2), o->judge_trans);
+      keep = rms <= o->judge_rms && frac >= o->judge_frac && rot <= o->judge_rot &&
+             sqrt(dt2) <= o->judge_trans;
+    }
+    warm_status = keep ? 1 : 2;
+    if (keep) break;
+    stop = 0;
+    memcpy(P, P0, sizeof(P0));
+  }
+  if (res) {
+    res->status = stop ? 1 : 0;
+    res->iterations = its;
+    res->warm = warm ? warm_status : 0;
+    res->inliers = inl;
+    res->examined = examined;
+    res->decisions_near = near;
+    res->residual_sq = res_sq;
+  }
+  return stop ? 1 : 0;
 }
 
 /* ------------------------------------------------------------ CPU tracker */

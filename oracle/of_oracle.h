@@ -97,6 +97,28 @@ int32_t ora_icp_step(const double *sys, double *pose, double *min_pivot);
 int32_t ora_icp_track(const ora_cam *c, const ora_params *p, const ora_real *frame,
                       const ora_real *model, double *pose, int32_t *iterations);
 
+/* options and result of ora_icp_track_ex: early exit, warm start, judge */
+typedef struct ora_icp_opts {
+  double stop_rot, stop_trans;  /* early exit thresholds (rad, mm); stop_rot 0 = off */
+  int32_t warm_levels;          /* finest levels of a warm-started pass (0 = all) */
+  int32_t pad;
+  double judge_rms, judge_frac, judge_rot, judge_trans;
+} ora_icp_opts;
+typedef struct ora_icp_result {
+  int32_t status;          /* 0 tracked, 1 singular (starting pose restored) */
+  int32_t iterations;      /* both passes */
+  int32_t warm;            /* 0 no warm start, 1 kept, 2 replaced by plain ICP */
+  int32_t inliers;         /* last iteration */
+  int32_t examined;        /* model points of the last iteration that landed in the frame */
+  int32_t decisions_near;  /* exit/judge decisions within 1 % of a threshold */
+  double residual_sq;      /* last iteration */
+} ora_icp_result;
+/* ora_icp_track with the early exit and an optional warm start (`warm`, FP64
+ * 4x4, or NULL) judged as the device path judges it. Returns status. */
+int32_t ora_icp_track_ex(const ora_cam *c, const ora_params *p, const ora_icp_opts *o,
+                         const ora_real *frame, const ora_real *model, double *pose,
+                         const double *warm, ora_icp_result *res);
+
 /* ---- reference semantics (pinned against the reference's own kernels) ---- */
 typedef struct ora_refcam {
   int32_t w, h;

@@ -32,12 +32,48 @@ def test_cpp_reference_shaped_classes_track(of, cuda):
     sys.path.insert(0, str(ROOT / "tests" / "cpp"))
     import build_shim
     exe = build_shim.build()
-    out = subprocess.run([str(exe), "20"], capture_output=True, text=True, timeout=300)
-    assert out.returncode == 0, out.stderr
-    res = json.loads(out.stdout.strip().splitlines()[-1])
-    assert res["cuda"] == "no error"
-    assert res["bad_status"] == 0
-    assert res["max_trans_mm"] < 5.0 and res["max_rot_rad"] < np.radians(0.5), res
+    for args, max_mm in ((["20"], 5.0), (["8", "c2"], 5.0)):
+        out = subprocess.run([str(exe), *args], capture_output=True, text=True, timeout=300)
+        assert out.returncode == 0, out.stderr
+        res = json.loads(out.stdout.strip().splitlines()[-1])
+        assert res["cuda"] == "no error"
+        assert res["bad_status"] == 0
+        assert res["frames_per_s"] > 0
+        assert res["max_trans_mm"] < max_mm and res["max_rot_rad"] < np.radians(0.5), res
+
+
+def test_cpp_reference_icp_steps_equal_the_tracking_solve(of, ora, cuda):
+    """The public ICP steps of the shim's C-ABI: of_icp_system then
+    of_icp_solve_step (ICP::FindCorresponding + ICP::BuildNewTransformMatrix)
+    equal the FP64 oracle's correspondence pass and solve on the same maps
+    within the pose tolerance; a singular system leaves the pose unchanged."""
+    import torch
+    from test_gpu_parity import gpu_pyramid_to_oracle, icp_inputs
+    cfg = c1(of)
+    seq, vol, lam, model, frame = icp_inputs(of, None, cfg, cuda)
+    ws = of.icp_workspace(cfg, cuda)
+    lib = of._native.lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    P0 = seq.poses[3]
+    pose = dev_pose(P0, cuda)
+    sys0 = of.icp_system(cfg, 0, frame, model, pose, ws)
+    stats = torch.zeros(32, dtype=torch.uint8, device=cuda)
+    assert lib.of_icp_solve_step(sys0.data_ptr(), pose.data_ptr(), stats.data_ptr(), stream) == 0
+    torch.cuda.synchronize()
+    _, fpts = gpu_pyramid_to_oracle(of, ora, cfg, frame)
+    _, mpts = gpu_pyramid_to_oracle(of, ora, cfg, model, with_depth=False)
+    o, _ = ora.icp_system(cfg, 0, fpts[0], mpts[0], P0)
+    st_o, Po, _ = ora.icp_step(o, P0)
+    assert st_o == 0
+    st = stats.cpu().numpy().view(np.int32)
+    assert st[0] == 0 and st[2] == 1 and abs(st[1] - o[28]) <= 2
+    rot, trans = pose_error(pose.cpu().numpy().reshape(4, 4), Po)
+    assert rot < 1e-5 and trans < 1e-2, (rot, trans)
+    zero = torch.zeros(32, dtype=torch.float32, device=cuda)
+    before = pose.clone()
+    assert lib.of_icp_solve_step(zero.data_ptr(), pose.data_ptr(), stats.data_ptr(), stream) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(before, pose) and stats.cpu().numpy().view(np.int32)[0] == 1
 
 
 def test_icp_barrier_timeout_reports_status(of, cuda):
@@ -174,3 +210,43 @@ def test_headless_views(of, cuda):
     exp = _pack((nv[..., 0] + 1) * h, (nv[..., 1] + 1) * h, (nv[..., 2] + 1) * h, np.float32(0))
     assert np.array_equal(r, exp)
     assert (r != _pack(h, h, h, np.float32(0))).mean() > 0.5
+
+
+def test_shaded_raycast_view_matches_oracle(of, ora, cuda):
+    """The raycast's shaded RGBA (Raycaster.cu:212-228, showNormal false):
+    0.6 (-d . n) + 0.2 in grey, black where d . n vanishes, alpha 0, packed
+    by rgbaFloatToInt. Stepwise against the FP64 restatement on the GPU's own
+    normals: every channel within 1 LSB (FP32 against FP64 before the
+    truncation to 8 bits), almost every pixel exact; and end to end against
+    the FP64 oracle's own raycast normals on the rays both hit."""
+    import torch
+    from test_gpu_parity import build_state
+    cfg = c1(of)
+    seq, vol, lam = build_state(of, cfg, 4, cuda)
+    pose = seq.poses[3]
+    rgba = torch.zeros((cfg.height, cfg.width), dtype=torch.int32, device=cuda)
+    model = of.raycast(cfg, vol, dev_pose(pose, cuda), rgba=rgba)
+    torch.cuda.synchronize()
+    g = rgba.cpu().numpy().view(np.uint32)
+    v, n = (t.cpu().numpy().astype(np.float64) for t in of.unpack_points(cfg, model, 0))
+    nrm = np.where(n[..., 3:4] > 0, n[..., :3], 0.0)
+    exp = ora.shade_rgba(cfg, pose, nrm)
+    assert np.all(g >> 24 == 0), "alpha is 0"
+    ch = [(g >> s) & 0xFF for s in (0, 8, 16)]
+    assert np.array_equal(ch[0], ch[1]) and np.array_equal(ch[0], ch[2]), "grey"
+    diff = np.abs(ch[0].astype(np.int64) - (exp & 0xFF).astype(np.int64))
+    assert diff.max() <= 1, diff.max()
+    assert (diff == 0).mean() > 0.999, (diff == 0).mean()
+    hit = n[..., 3] > 0
+    assert hit.mean() > 0.5 and np.all(ch[0][~hit] == 0)
+    lit = ch[0][hit]
+    assert lit.max() > 150 and np.median(lit) > 60, "surfaces facing the camera are lit"
+    # end to end: the oracle's own normals of the same volume
+    host = vol.cpu().numpy()
+    q, w = of.volume_to_linear(cfg, host)
+    words = (q.astype(np.uint32) | (w.astype(np.uint32) << 16)).reshape(-1).copy()
+    opts, amb = ora.raycast(cfg, words, pose, ambig=True)
+    both = hit & (opts[..., 7] > 0) & (amb == 0)
+    e2e = ora.shade_rgba(cfg, pose, np.where(opts[..., 7:8] > 0, opts[..., 4:7], 0.0))
+    d2 = np.abs(ch[0][both].astype(np.int64) - (e2e[both] & 0xFF).astype(np.int64))
+    assert np.quantile(d2, 0.99) <= 1 and np.median(d2) == 0, (np.quantile(d2, 0.99), d2.max())

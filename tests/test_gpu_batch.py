@@ -144,3 +144,51 @@ def test_tuned_and_graph_batches_equal_the_eager_one(of, cuda):
     for r in runs[1:]:
         assert np.array_equal(r[0], runs[0][0])
         assert np.array_equal(r[1], runs[0][1]) and np.array_equal(r[2], runs[0][2])
+
+
+def all_shapes_configs(of):
+    """Six streams covering every resolution {160x120, 320x240, 640x480} and
+    every volume {128^3, 256^3, 512^3} of the batched-streams workload."""
+    base = of.c4_configs(count=6, seed=4300, frames=4)
+    shapes = [((160, 120), 128, 2000.0), ((320, 240), 256, 2500.0), ((640, 480), 512, 3000.0),
+              ((160, 120), 512, 2400.0), ((640, 480), 128, 2800.0), ((320, 240), 512, 2200.0)]
+    out = []
+    for c, ((w, h), res, size) in zip(base, shapes):
+        f = 525.0 * w / 640.0
+        out.append(dataclasses.replace(c, width=w, height=h, fx=f, fy=f, cx=(w - 1) / 2.0,
+                                       cy=(h - 1) / 2.0, resolution=res, size_mm=size,
+                                       trunc_mm=max(30.0, 4.0 * size / res)))
+    return out
+
+
+def test_batched_icp_matches_oracle_per_stream(of, ora, cuda):
+    """Stepwise parity of the batched ICP (k_icp_batch) at the pose
+    tolerance (1e-5 rad, 0.01 mm): after the third step of a batch of six
+    streams of every resolution and volume, each stream's pose equals the FP64
+    oracle's multi-level ICP (10/5/4 iterations) run on that stream's own
+    frame and model pyramids from the pose it started the step at."""
+    import torch
+    from test_gpu_parity import gpu_pyramid_to_oracle
+    cfgs = all_shapes_configs(of)
+    seqs, depth = sequences(of, cfgs, 3, cuda)
+    batch = of.Batch(cfgs, [s.poses[0] for s in seqs])
+    for k in range(2):
+        batch.process(depth[k])
+    start = batch.poses()
+    batch.process(depth[2])
+    P, stats = batch.poses(with_stats=True)
+    for i, c in enumerate(cfgs):
+        b = batch.buffers(i)
+        frame = of.copy_pyramid(c, b.frame, cuda)
+        model = of.copy_pyramid(c, b.model, cuda)
+        torch.cuda.synchronize()
+        fbuf, _ = gpu_pyramid_to_oracle(of, ora, c, frame)
+        mbuf, _ = gpu_pyramid_to_oracle(of, ora, c, model, with_depth=False)
+        st, opose, its = ora.icp_track(c, fbuf, mbuf, start[i])
+        assert st == 0 and stats[i].status == 0, (c.name, st, stats[i].status)
+        assert stats[i].iterations == its == sum(c.iters), (c.name, stats[i].iterations, its)
+        rot, trans = pose_error(P[i], opose)
+        assert rot < 1e-5 and trans < 1e-2, (c.name, rot, trans)
+        rot_gt, trans_gt = pose_error(P[i], seqs[i].poses[2])
+        assert rot_gt < np.radians(1.0) and trans_gt < 20.0, (c.name, rot_gt, trans_gt)
+    batch.close()
