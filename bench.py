@@ -541,7 +541,8 @@ def warm_start_comparison(of, args, dev, world, rank):
     poses = of.make_trajectory(cfg.motion, cfg.seed + 1, cfg.size_mm, args.warm_frames)
     depth = learned.render_device(cfg, scene, poses, device=dev)
     out = {"workload": "c5: 640x480, 512^3 over 3 m, motion U[0,10] cm / U[0,5] deg per frame; "
-                       "early exit 2e-5 rad / 0.02 mm in both arms; warm pass on the finest level",
+                       f"early exit {cfg.stop_rot_rad:g} rad / {cfg.stop_trans_mm:g} mm in both "
+                       "arms; warm pass on the finest level",
            "frames": args.warm_frames - 1, "data": "synthetic (held-out seed, device renderer)"}
     weights = learned.load_weights()
     for arm, w in (("plain", None), ("warm", weights)):

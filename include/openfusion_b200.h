@@ -88,7 +88,8 @@ typedef struct of_raycast_params {
   float min_step_vox;    /* smallest march step, voxels (0.75) */
   float far_step_frac;   /* step as a fraction of tsdf*trunc when far from the surface (0.8) */
   int32_t refine_iters;  /* regula-falsi refinements of the zero crossing (3) */
-  int32_t reserved;
+  int32_t tile;          /* pixel block of one CTA (no result depends on it):
+                            0 = 16x16, 1 = 32x8, 2 = 8x32, 3 = 32x4 */
 } of_raycast_params_t;
 
 /* ICP (replaces ICP_ITERATIONS, DISTANCE_THRESHOLD, NORMAL_THRESHOLD,

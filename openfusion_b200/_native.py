@@ -32,7 +32,7 @@ class FilterParams(C.Structure):
 
 class RaycastParams(C.Structure):
     _fields_ = [("min_step_vox", C.c_float), ("far_step_frac", C.c_float),
-                ("refine_iters", C.c_int32), ("reserved", C.c_int32)]
+                ("refine_iters", C.c_int32), ("tile", C.c_int32)]
 
 
 class IcpParams(C.Structure):

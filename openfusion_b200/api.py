@@ -53,6 +53,7 @@ class Config:
     min_step_vox: float = 0.75
     far_step_frac: float = 0.8
     refine_iters: int = 3
+    ray_tile: int = 0               # raycast block shape (0 16x16, 1 32x8, 2 8x32, 3 32x4)
     scene_kind: int = 1
     motion: int = 0
     noise: float = 1.0
@@ -73,7 +74,8 @@ class Config:
                               self.levels)
 
     def raycast(self) -> N.RaycastParams:
-        return N.RaycastParams(self.min_step_vox, self.far_step_frac, self.refine_iters, 0)
+        return N.RaycastParams(self.min_step_vox, self.far_step_frac, self.refine_iters,
+                               self.ray_tile)
 
     def icp(self) -> N.IcpParams:
         it = (C.c_int32 * 4)(*(list(self.iters) + [0] * (4 - len(self.iters))))

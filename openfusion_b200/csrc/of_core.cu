@@ -48,7 +48,7 @@ extern "C" void of_default_params(of_filter_params_t *f, of_raycast_params_t *r,
     r->min_step_vox = 0.75f;
     r->far_step_frac = 0.8f;
     r->refine_iters = 3;
-    r->reserved = 0;
+    r->tile = 0;
   }
   if (i) {
     i->levels = 3;

@@ -22,12 +22,10 @@
 //   stops the remaining iterations (ICP.cpp:152-158).
 #include "of_batch.cuh"
 
-#include <cooperative_groups.h>
 #include <mutex>
 #include <string.h>
 
 using namespace of;
-namespace cg = cooperative_groups;
 
 bool of_camera_valid(const of_camera_t *c);
 
@@ -68,10 +66,6 @@ struct IcpWorkspace {
   unsigned long long fused_rows[2][kFusedMaxBlocks][32];
   unsigned int epoch;  // frames begun on this workspace (k_icp_begin), mod 2^19
   unsigned int magic;  // kWorkspaceMagic once k_icp_begin has cleared the rows
-  // the coarse levels' result (k_icp_coarse), where k_icp_fused continues
-  double coarse_pose[16];
-  double coarse_res, coarse_piv;
-  int coarse_its, coarse_stop, coarse_inl, coarse_examined;
 };
 constexpr unsigned kWorkspaceMagic = 0x4F46494Bu;
 
@@ -305,7 +299,6 @@ struct IcpPlan {
   float stop_rot, stop_trans;  // early exit (0: every iteration)
   float judge_rms, judge_frac, judge_rot, judge_trans;
   int warm_levels;  // levels of a warm-started pass (<= levels)
-  int coarse;       // k_icp_coarse ran the levels above 0 of this (plain) frame
   // optional pose history (a ring of hist_cap row-major poses and its running
   // count): the final pose is appended by the kernel's last store
   double *hist;
@@ -597,23 +590,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   // pose, runs only when the judge replaces the warm-started result
   const bool warm = ws->has_warm != 0;
   const unsigned epoch = ws->epoch;
-  // a plain frame whose coarse levels k_icp_coarse ran continues from its
-  // result at level 0
-  const bool coarse = plan.coarse && !warm;
-  if (threadIdx.x < 16)
-    s_pose[threadIdx.x] = warm ? ws->warm_pose[threadIdx.x]
-                               : (coarse ? ws->coarse_pose[threadIdx.x] : pose[threadIdx.x]);
+  if (threadIdx.x < 16) s_pose[threadIdx.x] = warm ? ws->warm_pose[threadIdx.x] : pose[threadIdx.x];
   if (threadIdx.x == 0) {
     s_stop = 0; s_err = 0; s_its = 0; s_inl = 0; s_res = 0.0; s_piv = 0.0; s_examined = 0;
     s_warm = warm ? 1 : 0;
-    if (coarse) {
-      s_its = ws->coarse_its;
-      s_stop = ws->coarse_stop;
-      s_inl = ws->coarse_inl;
-      s_examined = ws->coarse_examined;
-      s_res = ws->coarse_res;
-      s_piv = ws->coarse_piv;
-    }
   }
   __syncthreads();  // every thread reads the flags and the pose below
   if (threadIdx.x == 0) pose_to_rigid(s_pose, &s_c2w, &s_w2c);
@@ -623,8 +603,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   const float dist2 = plan.dist_thresh * plan.dist_thresh, nthr = plan.normal_thresh;
   int iter_global = 0;
   for (int pass = 0; pass < 2; ++pass) {
-    const int top = (pass == 0 && warm) ? plan.warm_levels - 1
-                                         : ((pass == 0 && coarse) ? 0 : plan.levels - 1);
+    const int top = (pass == 0 && warm) ? plan.warm_levels - 1 : plan.levels - 1;
     for (int l = top; l >= 0 && !s_stop && !s_err; --l) {
       const IcpLevel L = plan.lv[l];
       const int npx = L.mw * L.mh;
@@ -876,40 +855,24 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   }
 }
 
-// A new epoch for a frame begun on `ws`: no slot carries this frame's
-// sequence numbers yet. Slots must be cleared (*clear) when the epoch wraps
-// (every 2^19 frames), so an old slot never matches a new number, and on a
-// workspace's first use, whatever its memory held.
-__device__ __forceinline__ unsigned next_epoch(const IcpWorkspace *ws, bool *clear) {
-  const bool fresh = ws->magic != kWorkspaceMagic;
-  const unsigned epoch = fresh ? 1u : (ws->epoch + 1u) & kEpochMask;
-  *clear = epoch == 0u || fresh;
-  return epoch == 0u ? 1u : epoch;
-}
-
-__device__ void begin_state(double *pose, IcpWorkspace *ws, of_icp_stats_t *stats,
-                            const double *warm, unsigned epoch);
-
 // Start of a frame's tracking: remember the starting pose, apply the
 // optional prior increment, take the optional warm start (`warm`, a device
 // FP64 pose), clear the flags.
 __global__ void k_icp_begin(double *pose, IcpWorkspace *ws, of_icp_stats_t *stats,
                             const double *warm) {
-  bool clear;
-  const unsigned epoch = next_epoch(ws, &clear);
-  if (clear) {
+  // a new epoch: no slot carries this frame's sequence numbers yet. Slots are
+  // cleared when the epoch wraps (every 2^19 frames), so an old slot never
+  // matches a new number.
+  // (and on a workspace's first use, whatever its memory held)
+  const bool fresh = ws->magic != kWorkspaceMagic;
+  const unsigned epoch = fresh ? 1u : (ws->epoch + 1u) & kEpochMask;
+  if (epoch == 0u || fresh) {
     unsigned long long *rows = &ws->fused_rows[0][0][0];
     for (int i = threadIdx.x; i < 2 * kFusedMaxBlocks * 32; i += blockDim.x) rows[i] = 0ull;
   }
   __syncthreads();
   if (threadIdx.x != 0) return;
-  begin_state(pose, ws, stats, warm, epoch);
-}
-
-// k_icp_begin's single-thread part, with the epoch of next_epoch.
-__device__ void begin_state(double *pose, IcpWorkspace *ws, of_icp_stats_t *stats,
-                            const double *warm, unsigned epoch) {
-  ws->epoch = epoch;
+  ws->epoch = epoch == 0u ? 1u : epoch;
   ws->magic = kWorkspaceMagic;
   if (ws->has_prior) {
     double O[16];
@@ -938,182 +901,6 @@ __device__ void begin_state(double *pose, IcpWorkspace *ws, of_icp_stats_t *stat
     stats->warm = 0;
     stats->residual_sq = 0.0;
     stats->min_pivot = 0.0;
-  }
-}
-
-// The coarse pyramid levels of a plain frame on one thread-block cluster.
-//
-// The levels above 0 hold a quarter and a sixteenth of the pixels; a
-// full-grid exchange per iteration costs them as much as level 0. Here one
-// cluster of kCoarseCtas CTAs runs them, and k_icp_fused continues at level 0
-// from the result (ws->coarse_*). The kernel also does k_icp_begin's work, so
-// a plain frame needs no separate begin launch.
-//
-// Per iteration every CTA associates its share of the level's model pixels
-// (thread g of the cluster takes pixels g, g + kCoarseCtas * kCoarseThreads,
-// ..., four at a time with every gather in flight together), reduces its rows (recursive halving across each warp, then a tree over
-// the warps) and pushes its 30-value row into every CTA's shared memory,
-// double-buffered by iteration parity. After one hardware cluster barrier
-// every CTA sums the kCoarseCtas rows in the same order and solves the same
-// FP64 system, so all hold the same pose with no second barrier; a CTA can
-// only overwrite buffer i % 2 after barrier i + 1, which every CTA passes only
-// after reading it. The per-pixel arithmetic, the solve, the early exit and the
-// singular-system rule are k_icp_fused's.
-constexpr int kCoarseCtas = 16;  // a non-portable cluster size (8 where 16 cannot be resident)
-constexpr int kCoarseThreads = 512;
-constexpr int kCoarsePts = 4;    // model points per thread and step
-
-__global__ void __launch_bounds__(kCoarseThreads, 1)
-    k_icp_coarse(IcpPlan plan, double *pose, IcpWorkspace *ws, of_icp_stats_t *stats) {
-  __shared__ double s_pose[16];
-  __shared__ Rigid s_c2w, s_w2c;
-  __shared__ float s_red[kCoarseThreads / 32][32];
-  __shared__ float s_part[2][kCoarseCtas][32];
-  __shared__ float s_tot[32];
-  __shared__ int s_stop, s_conv, s_its, s_inl, s_examined;
-  __shared__ double s_res, s_piv;
-  cg::cluster_group cluster = cg::this_cluster();
-  const int rank = (int)cluster.block_rank();
-  const int nctas = (int)cluster.num_blocks();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int kWarps = kCoarseThreads / 32;
-  // ---- the frame's start (k_icp_begin): every thread reads the epoch before
-  // CTA 0 advances it
-  bool clear;
-  const unsigned epoch = next_epoch(ws, &clear);
-  cluster.sync();
-  if (clear) {
-    unsigned long long *rows = &ws->fused_rows[0][0][0];
-    for (int i = rank * kCoarseThreads + threadIdx.x; i < 2 * kFusedMaxBlocks * 32;
-         i += nctas * kCoarseThreads)
-      rows[i] = 0ull;
-  }
-  if (rank == 0 && threadIdx.x == 0) {
-    begin_state(pose, ws, stats, nullptr, epoch);
-    // the starting pose into every CTA
-    for (int r = 0; r < nctas; ++r) {
-      double *dst = cluster.map_shared_rank(&s_pose[0], r);
-      for (int i = 0; i < 16; ++i) dst[i] = ws->pose_init[i];
-    }
-  }
-  if (threadIdx.x == 0) {
-    s_stop = 0; s_its = 0; s_inl = 0; s_examined = 0; s_res = 0.0; s_piv = 0.0;
-  }
-  cluster.sync();
-  if (threadIdx.x == 0) pose_to_rigid(s_pose, &s_c2w, &s_w2c);
-  __syncthreads();
-  const float dist2 = plan.dist_thresh * plan.dist_thresh, nthr = plan.normal_thresh;
-  int iter = 0;
-  for (int l = plan.levels - 1; l >= 1 && !s_stop; --l) {
-    const IcpLevel L = plan.lv[l];
-    const int npx = L.mw * L.mh;
-    if (threadIdx.x == 0) s_conv = 0;
-    __syncthreads();
-    for (int it = 0; it < L.iters; ++it) {
-      float acc[kVals];
-      float examined = 0.f;
-#pragma unroll
-      for (int v = 0; v < kVals; ++v) acc[v] = 0.f;
-      const int stride = nctas * kCoarseThreads;
-      for (int p = rank * kCoarseThreads + threadIdx.x; p < npx; p += kCoarsePts * stride) {
-        float4 sv[kCoarsePts], nv[kCoarsePts], dv[kCoarsePts], cv[kCoarsePts];
-        int q[kCoarsePts];
-#pragma unroll
-        for (int k = 0; k < kCoarsePts; ++k) {
-          const int pk = p + k * stride;
-          sv[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-          nv[k] = sv[k];
-          if (pk < npx) { sv[k] = __ldg(L.model + 2 * pk); nv[k] = __ldg(L.model + 2 * pk + 1); }
-        }
-#pragma unroll
-        for (int k = 0; k < kCoarsePts; ++k) {
-          q[k] = (sv[k].w != 0.f && nv[k].w != 0.f) ? associate(s_w2c, L.cam, sv[k]) : -1;
-          dv[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-          cv[k] = dv[k];
-          if (q[k] >= 0) { dv[k] = __ldg(L.frame + 2 * q[k]); cv[k] = __ldg(L.frame + 2 * q[k] + 1); }
-        }
-#pragma unroll
-        for (int k = 0; k < kCoarsePts; ++k) {
-          if (q[k] < 0) continue;
-          examined += 1.f;
-          try_row(acc, s_c2w, sv[k], nv[k], dv[k], cv[k], dist2, nthr);
-        }
-      }
-      // this CTA's row: recursive halving across the warp, a tree over warps
-      if (!__any_sync(0xffffffffu, examined > 0.f)) {
-        s_red[warp][lane] = 0.f;
-      } else {
-        float r[32];
-#pragma unroll
-        for (int v = 0; v < 32; ++v) r[v] = v < kVals ? acc[v] : (v == kVals ? examined : 0.f);
-#pragma unroll
-        for (int sft = 16; sft >= 1; sft >>= 1) {
-          const bool upper = (lane & sft) != 0;
-#pragma unroll
-          for (int i = 0; i < sft; ++i) {
-            float send = upper ? r[i] : r[i + sft];
-            float keep = upper ? r[i + sft] : r[i];
-            r[i] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
-          }
-        }
-        s_red[warp][lane] = r[0];
-      }
-      __syncthreads();
-      const int buf = iter & 1;
-      if (warp == 0) {
-        float y[kWarps];
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) y[w] = s_red[w][lane];
-#pragma unroll
-        for (int span = 1; span < kWarps; span *= 2)
-#pragma unroll
-          for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
-        for (int r = 0; r < nctas; ++r) cluster.map_shared_rank(&s_part[buf][rank][0], r)[lane] = y[0];
-      }
-      cluster.sync();
-      if (warp == 0) {
-        // the CTAs' rows in a fixed order (a tree over the ranks)
-        float y[kCoarseCtas];
-#pragma unroll
-        for (int r = 0; r < kCoarseCtas; ++r) y[r] = r < nctas ? s_part[buf][r][lane] : 0.f;
-#pragma unroll
-        for (int span = 1; span < kCoarseCtas; span *= 2)
-#pragma unroll
-          for (int r = 0; r + span < kCoarseCtas; r += 2 * span) y[r] += y[r + span];
-        s_tot[lane] = y[0];
-        __syncwarp();
-        double minpiv = 0.0;
-        float inc_rot = 0.f, inc_trans = 0.f;
-        const bool ok =
-            warp_solve_update(s_tot, s_pose, &minpiv, &inc_rot, &inc_trans, &s_c2w, &s_w2c);
-        if (lane == 0) {
-          s_its += 1;
-          s_inl = (int)s_tot[28];
-          s_examined = (int)s_tot[kVals];
-          s_res = (double)s_tot[27];
-          s_piv = minpiv;
-          if (!ok) {
-            for (int i = 0; i < 16; ++i) s_pose[i] = ws->pose_init[i];
-            s_stop = 1;
-          } else if (plan.stop_rot > 0.f && inc_rot < plan.stop_rot &&
-                     inc_trans < plan.stop_trans) {
-            s_conv = 1;
-          }
-        }
-      }
-      __syncthreads();
-      ++iter;
-      if (s_stop || s_conv) break;
-    }
-  }
-  if (rank == 0 && threadIdx.x == 0) {
-    for (int i = 0; i < 16; ++i) ws->coarse_pose[i] = s_pose[i];
-    ws->coarse_its = s_its;
-    ws->coarse_stop = s_stop;
-    ws->coarse_inl = s_inl;
-    ws->coarse_examined = s_examined;
-    ws->coarse_res = s_res;
-    ws->coarse_piv = s_piv;
   }
 }
 
@@ -1204,47 +991,8 @@ static of_status_t fused_shape(const of_camera_t *cam, FusedShape *fs) {
   return OF_OK;
 }
 
-// CTAs of k_icp_coarse's cluster on the current device: kCoarseCtas (a
-// non-portable cluster size) when such a cluster of 1024-thread CTAs fits,
-// else the portable 8. The attribute is set on every call (see fused_shape).
-static of_status_t coarse_ctas(int *out) {
-  constexpr int kMaxDevices = 64;
-  static int ctas_of[kMaxDevices] = {};
-  static std::mutex mu;
-  int dev = 0;
-  OF_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) return OF_ERR_INVALID_ARGUMENT;
-  OF_CUDA_TRY(cudaFuncSetAttribute((const void *)k_icp_coarse,
-                                   cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-  std::lock_guard<std::mutex> lock(mu);
-  if (ctas_of[dev] == 0) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(kCoarseCtas);
-    cfg.blockDim = dim3(kCoarseThreads);
-    cudaLaunchAttribute attr;
-    attr.id = cudaLaunchAttributeClusterDimension;
-    attr.val.clusterDim.x = kCoarseCtas;
-    attr.val.clusterDim.y = 1;
-    attr.val.clusterDim.z = 1;
-    cfg.attrs = &attr;
-    cfg.numAttrs = 1;
-    int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, (void *)k_icp_coarse, &cfg) != cudaSuccess || n < 1) {
-      cudaGetLastError();
-      n = 0;
-    }
-    ctas_of[dev] = n >= 1 ? kCoarseCtas : 8;
-  }
-  *out = ctas_of[dev];
-  return OF_OK;
-}
-
-// Launches the whole coarse-to-fine ICP of one frame. A plain frame with
-// more than one level: k_icp_coarse (the frame's start and the coarse levels
-// on one cluster), then one cooperative launch of the fused kernel for level
-// 0. A warm-started frame (whose judge may send it back to the coarse levels
-// in a second pass) or a single-level one: the begin kernel, then the fused
-// kernel for every level.
+// Launches the whole coarse-to-fine ICP of one frame: a begin kernel and one
+// cooperative launch of the fused kernel.
 of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, const void *d_frame,
                           const void *d_model, double *pose, void *d_ws, of_icp_stats_t *stats,
                           cudaStream_t s, const double *d_warm, double *d_hist,
@@ -1285,29 +1033,9 @@ of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, con
     plan.lv[l].mh = cl.height;
     plan.lv[l].iters = ip->iters[l];
   }
-  plan.coarse = (d_warm == nullptr && ip->levels > 1) ? 1 : 0;
-  if (plan.coarse) {
-    int ctas = 0;
-    st = coarse_ctas(&ctas);
-    if (st != OF_OK) return st;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(ctas);
-    cfg.blockDim = dim3(kCoarseThreads);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = s;
-    cudaLaunchAttribute attr;
-    attr.id = cudaLaunchAttributeClusterDimension;
-    attr.val.clusterDim.x = ctas;
-    attr.val.clusterDim.y = 1;
-    attr.val.clusterDim.z = 1;
-    cfg.attrs = &attr;
-    cfg.numAttrs = 1;
-    OF_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_icp_coarse, plan, pose, ws, stats));
-  } else {
-    k_icp_begin<<<1, 32, 0, s>>>(pose, ws, stats, d_warm);
-    st = of_launch_status();
-    if (st != OF_OK) return st;
-  }
+  k_icp_begin<<<1, 32, 0, s>>>(pose, ws, stats, d_warm);
+  st = of_launch_status();
+  if (st != OF_OK) return st;
   void *args[] = {&plan, &pose, &ws, &stats};
   OF_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)k_icp_fused, dim3(fs.grid),
                                           dim3(kFusedThreads), args, fs.smem, s));
@@ -1455,7 +1183,11 @@ extern "C" of_status_t of_icp_track_static(const of_camera_t *cam, const of_icp_
 // so all hold the same pose. The only waits are hardware cluster barriers.
 // The per-pixel arithmetic (association, inlier tests, rows, FP64 solve and
 // composition) is the single-stream kernel's; the summation order differs.
+#include <cooperative_groups.h>
+
 namespace {
+
+namespace cg = cooperative_groups;
 
 constexpr int kBatchCtas = 8;
 constexpr int kBatchThreads = 512;

@@ -405,7 +405,7 @@ struct DownJob {
   int sw, dw, dh, step, gx;
 };
 
-// block shapes of the batched raycast (a tuning knob; every ray is the same)
+// block shapes of the raycast (a tuning knob; every ray is the same)
 constexpr int kRayTiles = 4;
 constexpr int kRayTileX[kRayTiles] = {16, 32, 8, 32};
 constexpr int kRayTileY[kRayTiles] = {16, 8, 32, 4};
@@ -555,14 +555,15 @@ extern "C" of_status_t of_raycast(const of_volume_desc_t *d, const void *vol,
   if (!of_volume_valid(d) || !of_camera_valid(cam) || !rp || !vol || !pose || !d_model)
     return OF_ERR_INVALID_ARGUMENT;
   if (levels < 1 || levels > kMaxLevels || rp->min_step_vox <= 0.f || rp->far_step_frac < 0.f ||
-      rp->refine_iters < 0 || rp->refine_iters > 16)
+      rp->refine_iters < 0 || rp->refine_iters > 16 || rp->tile < 0 || rp->tile >= kRayTiles)
     return OF_ERR_INVALID_ARGUMENT;
   of_pyramid_layout_t lay;
   of_status_t st = of_pyramid_layout(cam, levels, &lay);
   if (st != OF_OK) return st;
   cudaStream_t s = (cudaStream_t)stream;
-  dim3 blk(16, 16);
-  dim3 grid((cam->width + 15) / 16, (cam->height + 15) / 16);
+  const int tx = kRayTileX[rp->tile], ty = kRayTileY[rp->tile];
+  dim3 blk(tx, ty);
+  dim3 grid((cam->width + tx - 1) / tx, (cam->height + ty - 1) / ty);
   Cam c = make_cam(*cam);
   float4 *pts = (float4 *)((char *)d_model + lay.points_offset[0]);
   ModelLevels coarse;

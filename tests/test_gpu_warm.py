@@ -90,7 +90,8 @@ def test_kept_warm_start_lands_on_the_plain_result(of, ora, cuda, name):
 def test_rejected_warm_start_is_replaced_by_plain_icp(of, ora, cuda, name):
     """A warm start 200 mm / 6 deg off is rejected (disagreement beyond the
     judge's 50 mm / 0.05 rad), as the oracle's judge rejects it, and the
-    result is plain ICP's, bit for bit."""
+    result is plain ICP's from the previous pose, bit for bit, and the
+    oracle's within 1e-5 rad / 0.01 mm."""
     cfg = small(of, name)
     seq, plain, sp, warm, sw, W, frame, model = run_plain_and_warm(
         of, cfg, cuda, lambda G: perturbed(G, np.radians(6.0), 200.0))
