@@ -380,8 +380,11 @@ def run_ours(args, cfg, world, rank, local):
     depth_host = torch.from_numpy(seq.depth.astype(np.int16)).pin_memory()
     stream = torch.cuda.current_stream(dev)
 
+    # the tracker tunes its raycast block shape online at a warm-up step, before
+    # its step graphs are captured (never inside the timed region)
+    tune = min(3, args.warmup) if args.warmup >= 1 else 0
     # ---- device-resident loop: value
-    tr = of.Tracker(cfg, seq.poses[0], use_graph=True, pose_history=total)
+    tr = of.Tracker(cfg, seq.poses[0], use_graph=True, pose_history=total, tune=tune)
     tr.process(depth_dev[order[0]])
     for i in range(1, 1 + args.warmup):
         tr.process(depth_dev[order[i]])
@@ -401,6 +404,7 @@ def run_ours(args, cfg, world, rank, local):
     ms_max = max_over_ranks(ms, world)
     bufs = tr.buffers()
     kernels = bufs.kernels_track * args.steps
+    ray_tile, tuned = tr.tuning()
     hist = tr.pose_history(total)
     _, st = tr.pose()
     # ---- per-frame times: CUDA events between the steps of the same tracker,
@@ -417,7 +421,7 @@ def run_ours(args, cfg, world, rank, local):
     rots, trans = pose_errors(hist, [seq.poses[j] for j in order])
 
     # ---- end to end through the C-ABI: pinned host depth in, pose out
-    tr = of.Tracker(cfg, seq.poses[0], use_graph=True, pose_history=total)
+    tr = of.Tracker(cfg, seq.poses[0], use_graph=True, pose_history=total, tune=tune)
     pose_out = torch.zeros((total, 16), dtype=torch.float64).pin_memory()
     tr.process(depth_host[order[0]])
     for i in range(1, 1 + args.warmup):
@@ -440,8 +444,11 @@ def run_ours(args, cfg, world, rank, local):
         "end-to-end poses differ from the device-resident run"
     tr.close()
 
-    # ---- per-stage kernel times (stage-wise launches with CUDA events)
-    stages = stage_times(of, cfg, seq, depth_dev, order, args, dev)
+    # ---- per-stage kernel times (stage-wise launches with CUDA events), with
+    # the block shape the tracker chose
+    import dataclasses
+    stages = stage_times(of, dataclasses.replace(cfg, ray_tile=ray_tile), seq, depth_dev, order,
+                         args, dev)
 
     # ---- the learned warm start against plain ICP (large-motion workload)
     warm = warm_start_comparison(of, args, dev, world, rank) if args.warm_frames > 1 else None
@@ -504,6 +511,8 @@ def run_ours(args, cfg, world, rank, local):
         "e2e": {"value": e2e_fps, "unit": "frames/s",
                 "h2d_bytes_per_step": cfg.width * cfg.height * 2, "d2h_bytes_per_step": 128},
         "gpu_launches": kernels,
+        "tuning": {"raycast_block": ["16x16", "32x8", "8x32", "32x4"][ray_tile],
+                   "tuned_online": tuned, "at_warmup_step": tune},
         "clocks": sampler.summary(),
     }
     if warm is not None:

@@ -381,9 +381,12 @@ class Tracker:
 
     def __init__(self, cfg: Config, initial_pose: np.ndarray, use_graph: bool = True,
                  pose_history: int = 1024, warm_start_weights: np.ndarray | None = None,
-                 depth_filter: N.DepthFilterParams | None = None):
+                 depth_filter: N.DepthFilterParams | None = None, tune: int = 0):
         """`warm_start_weights`: FP32 weights of the warm-start CNN (None =
-        plain ICP from the previous pose)."""
+        plain ICP from the previous pose). `tune` = k >= 1: step k times the
+        step shapes (raycast and ICP in one launch, or separately with each
+        raycast block shape) and keeps the fastest before the step graphs are
+        captured (of_tracker_desc_t.tune); 0: the one-launch step."""
         self.cfg = cfg
         d = N.TrackerDesc()
         d.camera = cfg.camera()
@@ -394,6 +397,7 @@ class Tracker:
         d.initial_pose = (C.c_double * 16)(*np.asarray(initial_pose, np.float64).reshape(16))
         d.use_graph = 1 if use_graph else 0
         d.pose_history = pose_history
+        d.tune = tune
         if depth_filter is not None:
             d.depth_filter = depth_filter
         self._weights = None
@@ -469,6 +473,14 @@ class Tracker:
         b = N.TrackerBuffers()
         N.check("of_tracker_buffers", N.lib().of_tracker_buffers(self._h, C.byref(b)))
         return b
+
+    def tuning(self) -> tuple[bool, int, bool]:
+        """(raycast and ICP in one launch?, raycast block shape when not,
+        whether the online tuning has run)."""
+        comb, tile, tuned = C.c_int32(), C.c_int32(), C.c_int32()
+        N.check("of_tracker_tuning", N.lib().of_tracker_tuning(self._h, C.byref(comb),
+                                                               C.byref(tile), C.byref(tuned)))
+        return bool(comb.value), tile.value, bool(tuned.value)
 
 
 # --------------------------------------------------------------- synthetic --

@@ -61,8 +61,10 @@ struct CnnWs {
   float *gf1;
   float *gout;
   float *loss;  // [b] per-sample losses, then their sum at [b]
+  float *part;  // split-K partial tiles of the tensor-core GEMMs
   size_t total;
 };
+size_t mma_part_floats(int b);
 inline size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 CnnWs ws_layout(void *base, int b) {
   CnnWs w;
@@ -76,6 +78,7 @@ CnnWs ws_layout(void *base, int b) {
   w.gf1 = (float *)take((size_t)b * kF1Out * sizeof(float));
   w.gout = (float *)take((size_t)b * kF2Out * sizeof(float));
   w.loss = (float *)take((size_t)(b + 1) * sizeof(float));
+  w.part = (float *)take(mma_part_floats(b) * sizeof(float));
   w.total = off;
   return w;
 }
@@ -146,37 +149,7 @@ __global__ void __launch_bounds__(256) k_cnn_center(const float *__restrict__ ce
 // ---------------------------------------------------------------- convs --
 
 // out[b, co, oy, ox] = relu(bias[co] + sum_{ci, ky, kx} w[co, ci, ky, kx] in[b, ci, iy, ix])
-template <int K, int S, int P>
-__global__ void __launch_bounds__(256) k_conv_fwd(const bf16 *__restrict__ in,
-                                                  const bf16 *__restrict__ wt,
-                                                  const float *__restrict__ bias, ConvSpec c,
-                                                  int batch, bf16 *__restrict__ out) {
-  const long total = (long)batch * c.co * c.ho * c.wo;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (long)gridDim.x * blockDim.x) {
-    const int ox = (int)(i % c.wo), oy = (int)((i / c.wo) % c.ho);
-    const int co = (int)((i / ((long)c.wo * c.ho)) % c.co), b = (int)(i / ((long)c.wo * c.ho * c.co));
-    float acc = bias[co];
-    const bf16 *ib = in + (size_t)b * c.ci * c.hi * c.wi;
-    const bf16 *wb = wt + (size_t)co * c.ci * K * K;
-    for (int ci = 0; ci < c.ci; ++ci) {
-#pragma unroll
-      for (int ky = 0; ky < K; ++ky) {
-        const int iy = oy * S - P + ky;
-        if ((unsigned)iy >= (unsigned)c.hi) continue;
-#pragma unroll
-        for (int kx = 0; kx < K; ++kx) {
-          const int ix = ox * S - P + kx;
-          if ((unsigned)ix >= (unsigned)c.wi) continue;
-          acc = fmaf(bf(wb[(ci * K + ky) * K + kx]), bf(ib[((size_t)ci * c.hi + iy) * c.wi + ix]), acc);
-        }
-      }
-    }
-    out[i] = __float2bfloat16_rn(fmaxf(acc, 0.f));
-  }
-}
-
-// The same convolution for small batches (inference): one warp per output,
+// for small batches (inference): one warp per output,
 // the ci x K x K taps dealt to the lanes in a fixed order, then a shuffle
 // tree; enough parallelism for a single pair.
 template <int K, int S, int P>
@@ -201,90 +174,6 @@ __global__ void __launch_bounds__(256) k_conv_fwd_warp(const bf16 *__restrict__ 
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
   if (lane == 0) out[i] = __float2bfloat16_rn(fmaxf(acc + bias[co], 0.f));
-}
-
-// gin[b, ci, iy, ix] = sum_{co, ky, kx: iy = oy S - P + ky} w[co, ci, ky, kx] gout[b, co, oy, ox],
-// with gout the gradient at the pre-activation (masked by this layer's ReLU).
-template <int K, int S, int P>
-__global__ void __launch_bounds__(256) k_conv_bwd_data(const float *__restrict__ gpost,
-                                                       const bf16 *__restrict__ act,
-                                                       const bf16 *__restrict__ wt, ConvSpec c,
-                                                       int batch, float *__restrict__ gin) {
-  const long total = (long)batch * c.ci * c.hi * c.wi;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (long)gridDim.x * blockDim.x) {
-    const int ix = (int)(i % c.wi), iy = (int)((i / c.wi) % c.hi);
-    const int ci = (int)((i / ((long)c.wi * c.hi)) % c.ci), b = (int)(i / ((long)c.wi * c.hi * c.ci));
-    float acc = 0.f;
-    for (int co = 0; co < c.co; ++co) {
-      const size_t gb = ((size_t)b * c.co + co) * c.ho * c.wo;
-      const bf16 *wb = wt + ((size_t)co * c.ci + ci) * K * K;
-#pragma unroll
-      for (int ky = 0; ky < K; ++ky) {
-        const int ny = iy + P - ky;
-        if (ny < 0 || ny % S) continue;
-        const int oy = ny / S;
-        if (oy >= c.ho) continue;
-#pragma unroll
-        for (int kx = 0; kx < K; ++kx) {
-          const int nx = ix + P - kx;
-          if (nx < 0 || nx % S) continue;
-          const int ox = nx / S;
-          if (ox >= c.wo) continue;
-          const size_t o = gb + (size_t)oy * c.wo + ox;
-          const float g = bf(act[o]) > 0.f ? gpost[o] : 0.f;
-          acc = fmaf(bf(wb[ky * K + kx]), g, acc);
-        }
-      }
-    }
-    gin[i] = acc;
-  }
-}
-
-// gw[co, ci, ky, kx] = sum_{b, oy, ox} gpre[b, co, oy, ox] in[b, ci, oy S - P + ky, ox S - P + kx];
-// gb[co] = sum gpre[b, co, ., .]. One block per (co, ci): each thread sums a
-// fixed strided share of (b, oy, ox) for all K*K taps, then a tree.
-template <int K, int S, int P>
-__global__ void __launch_bounds__(256) k_conv_bwd_weight(const float *__restrict__ gpost,
-                                                         const bf16 *__restrict__ act,
-                                                         const bf16 *__restrict__ in, ConvSpec c,
-                                                         int batch, float *__restrict__ gw,
-                                                         float *__restrict__ gbias) {
-  __shared__ float s_red[256][K * K + 1];
-  const int co = blockIdx.x / c.ci, ci = blockIdx.x % c.ci;
-  float acc[K * K + 1];
-#pragma unroll
-  for (int t = 0; t <= K * K; ++t) acc[t] = 0.f;
-  const long n = (long)batch * c.ho * c.wo;
-  for (long q = threadIdx.x; q < n; q += blockDim.x) {
-    const int ox = (int)(q % c.wo), oy = (int)((q / c.wo) % c.ho), b = (int)(q / ((long)c.wo * c.ho));
-    const size_t o = (((size_t)b * c.co + co) * c.ho + oy) * c.wo + ox;
-    const float g = bf(act[o]) > 0.f ? gpost[o] : 0.f;
-    if (g == 0.f) continue;
-    const bf16 *ib = in + ((size_t)b * c.ci + ci) * c.hi * c.wi;
-#pragma unroll
-    for (int ky = 0; ky < K; ++ky) {
-      const int iy = oy * S - P + ky;
-      if ((unsigned)iy >= (unsigned)c.hi) continue;
-#pragma unroll
-      for (int kx = 0; kx < K; ++kx) {
-        const int ix = ox * S - P + kx;
-        if ((unsigned)ix >= (unsigned)c.wi) continue;
-        acc[ky * K + kx] = fmaf(g, bf(ib[(size_t)iy * c.wi + ix]), acc[ky * K + kx]);
-      }
-    }
-    acc[K * K] += g;
-  }
-#pragma unroll
-  for (int t = 0; t <= K * K; ++t) s_red[threadIdx.x][t] = acc[t];
-  __syncthreads();
-  for (int span = 128; span > 0; span >>= 1) {
-    if ((int)threadIdx.x < span)
-      for (int t = 0; t <= K * K; ++t) s_red[threadIdx.x][t] += s_red[threadIdx.x + span][t];
-    __syncthreads();
-  }
-  if ((int)threadIdx.x < K * K) gw[((size_t)co * c.ci + ci) * K * K + threadIdx.x] = s_red[0][threadIdx.x];
-  if (ci == 0 && threadIdx.x == 0) gbias[co] = s_red[0][K * K];
 }
 
 // ------------------------------------------------------------------- fc --
@@ -312,45 +201,301 @@ __global__ void __launch_bounds__(256) k_fc_fwd(const bf16 *__restrict__ in,
   }
 }
 
-// gin[b, i] = sum_j w[j, i] gpre[b, j] (gpre masked by the ReLU of `act`
-// when given); one thread per (b, i).
-__global__ void __launch_bounds__(256) k_fc_bwd_data(const float *__restrict__ gpost,
-                                                     const bf16 *__restrict__ act,
-                                                     const bf16 *__restrict__ wt, int nin,
-                                                     int nout, int batch,
-                                                     float *__restrict__ gin) {
-  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long)batch * nin) return;
-  const int i = (int)(t % nin), b = (int)(t / nin);
-  float acc = 0.f;
-  for (int j = 0; j < nout; ++j) {
-    const size_t o = (size_t)b * nout + j;
-    const float g = (!act || bf(act[o]) > 0.f) ? gpost[o] : 0.f;
-    acc = fmaf(bf(wt[(size_t)j * nin + i]), g, acc);
-  }
-  gin[t] = acc;
+// ------------------------------------------------- tensor-core GEMMs --
+//
+// The training contractions as implicit GEMMs on the tensor cores:
+// D[m, n] = sum_k A(m, k) B(k, n) with A and B read through a problem
+// functor that gathers them from the layer's tensors (im2col on the fly, the
+// padding and the ReLU masks included). One warp computes a 16 x 32 tile of
+// D, four mma n8 subtiles sharing each A fragment, over a K range:
+//   - forward (BF16 weights and activations): mma.sync m16n8k16 BF16 x BF16
+//     with FP32 accumulation, the products the scalar kernels form, summed in
+//     another fixed order;
+//   - backward (FP32 gradients): mma.sync m16n8k8 TF32 x TF32 with FP32
+//     accumulation; BF16 operands are exact in TF32, an FP32 gradient is
+//     rounded to TF32 (cvt.rna, relative error below 2^-11).
+// Large reductions (the weight gradients sum over batch x pixels) are split
+// along K over blockIdx.y; each slice writes its partial tile and a second
+// kernel sums the slices in index order, so every result is reproducible bit
+// for bit. Fragment layouts (PTX ISA, mma.m16n8k16 / m16n8k8, g = lane / 4,
+// t = lane % 4): A row-major, B column-major, accumulators c0..c3 at
+// (g, 2t), (g, 2t + 1), (g + 8, 2t), (g + 8, 2t + 1).
+
+constexpr int kMmaWarps = 4;      // warps per CTA, one 16 x 32 tile each
+constexpr int kMmaNt = 4;         // n8 subtiles per warp tile
+constexpr int kMmaTileN = 8 * kMmaNt;
+constexpr long kMmaSliceK = 2048; // K per split slice of a long reduction
+constexpr int kMmaMaxSlices = 256;
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t *>(&v);
+}
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void mma_bf16(float *c, const uint32_t *a, const uint32_t *b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+      "{%8, %9}, {%0, %1, %2, %3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+__device__ __forceinline__ void mma_tf32(float *c, const uint32_t *a, const uint32_t *b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+      "{%8, %9}, {%0, %1, %2, %3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-// gw[j, i] = sum_b gpre[b, j] in[b, i]; gb[j] = sum_b gpre[b, j]; one thread
-// per (j, i) (i == nin: the bias).
-__global__ void __launch_bounds__(256) k_fc_bwd_weight(const float *__restrict__ gpost,
-                                                       const bf16 *__restrict__ act,
-                                                       const bf16 *__restrict__ in, int nin,
-                                                       int nout, int batch,
-                                                       float *__restrict__ gw,
-                                                       float *__restrict__ gbias) {
-  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long)nout * (nin + 1)) return;
-  const int i = (int)(t % (nin + 1)), j = (int)(t / (nin + 1));
-  float acc = 0.f;
-  for (int b = 0; b < batch; ++b) {
-    const size_t o = (size_t)b * nout + j;
-    const float g = (!act || bf(act[o]) > 0.f) ? gpost[o] : 0.f;
-    acc = fmaf(g, i < nin ? bf(in[(size_t)b * nin + i]) : 1.f, acc);
+// Warp tile (m0, n0) over k in [k0, k1): BF16 (KS = 16) or TF32 (KS = 8).
+// Elements outside [0, M) x [0, Kd) or [0, Kd) x [0, N) read as 0 (Kd: the
+// reduction length of the problem).
+template <class P, bool BF16>
+__device__ __forceinline__ void mma_tile(const P &p, int m0, int n0, long k0, long k1,
+                                         float (&c)[kMmaNt][4]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  constexpr int KS = BF16 ? 16 : 8;
+  const int ma = m0 + g, mb = m0 + g + 8;
+  for (long k = k0; k < k1; k += KS) {
+    uint32_t a[4];
+    if (BF16) {
+      const long ka = k + 2 * t, kb = k + 2 * t + 8;
+      a[0] = pack_bf16x2(p.a(ma, ka), p.a(ma, ka + 1));
+      a[1] = pack_bf16x2(p.a(mb, ka), p.a(mb, ka + 1));
+      a[2] = pack_bf16x2(p.a(ma, kb), p.a(ma, kb + 1));
+      a[3] = pack_bf16x2(p.a(mb, kb), p.a(mb, kb + 1));
+    } else {
+      a[0] = to_tf32(p.a(ma, k + t));
+      a[1] = to_tf32(p.a(mb, k + t));
+      a[2] = to_tf32(p.a(ma, k + t + 4));
+      a[3] = to_tf32(p.a(mb, k + t + 4));
+    }
+#pragma unroll
+    for (int j = 0; j < kMmaNt; ++j) {
+      const int n = n0 + 8 * j + g;
+      uint32_t b[2];
+      if (BF16) {
+        b[0] = pack_bf16x2(p.b(k + 2 * t, n), p.b(k + 2 * t + 1, n));
+        b[1] = pack_bf16x2(p.b(k + 2 * t + 8, n), p.b(k + 2 * t + 9, n));
+        mma_bf16(c[j], a, b);
+      } else {
+        b[0] = to_tf32(p.b(k + t, n));
+        b[1] = to_tf32(p.b(k + t + 4, n));
+        mma_tf32(c[j], a, b);
+      }
+    }
   }
-  if (i < nin) gw[(size_t)j * nin + i] = acc;
-  else gbias[j] = acc;
 }
+
+// Grid: x over the warp tiles (kMmaWarps per CTA), y over the K slices.
+// With one slice the tile goes through p.store(m, n, value); with several,
+// slice s writes part[(s * M + m) * N + n] and k_mma_reduce sums them.
+template <class P, bool BF16>
+__global__ void __launch_bounds__(32 * kMmaWarps) k_mma(P p, float *__restrict__ part) {
+  const int tiles_n = (p.N + kMmaTileN - 1) / kMmaTileN;
+  const int tiles = ((p.M + 15) / 16) * tiles_n;
+  const int tile = blockIdx.x * kMmaWarps + (threadIdx.x >> 5);
+  if (tile >= tiles) return;  // warp-uniform
+  const int m0 = (tile / tiles_n) * 16, n0 = (tile % tiles_n) * kMmaTileN;
+  const long slice = (p.Kd + gridDim.y - 1) / gridDim.y;
+  const long KS = BF16 ? 16 : 8;
+  const long k0 = ((long)blockIdx.y * slice) / KS * KS;
+  const long k1 = blockIdx.y + 1 == gridDim.y ? p.Kd : (((long)blockIdx.y + 1) * slice) / KS * KS;
+  float c[kMmaNt][4] = {};
+  mma_tile<P, BF16>(p, m0, n0, k0, k1, c);
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int j = 0; j < kMmaNt; ++j)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int m = m0 + g + (r >= 2 ? 8 : 0), n = n0 + 8 * j + 2 * t + (r & 1);
+      if (m >= p.M || n >= p.N) continue;
+      if (gridDim.y == 1) p.store(m, n, c[j][r]);
+      else part[((size_t)blockIdx.y * p.M + m) * p.N + n] = c[j][r];
+    }
+}
+
+template <class P>
+__global__ void __launch_bounds__(256) k_mma_reduce(P p, const float *__restrict__ part,
+                                                    int slices) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long)p.M * p.N) return;
+  float acc = 0.f;
+  for (int s = 0; s < slices; ++s) acc += part[(size_t)s * p.M * p.N + i];
+  p.store((int)(i / p.N), (int)(i % p.N), acc);
+}
+
+// K slices of a reduction of length K (1 when it is short).
+inline int mma_slices(long K) {
+  const long s = (K + kMmaSliceK - 1) / kMmaSliceK;
+  return (int)(s < 1 ? 1 : (s > kMmaMaxSlices ? kMmaMaxSlices : s));
+}
+
+// Launches D = A B of problem p; `part` holds slices x M x N floats when the
+// reduction is split.
+template <class P, bool BF16>
+void mma_launch(const P &p, float *part, int slices, cudaStream_t s) {
+  const long tiles = (long)((p.M + 15) / 16) * ((p.N + kMmaTileN - 1) / kMmaTileN);
+  dim3 grid((unsigned)((tiles + kMmaWarps - 1) / kMmaWarps), (unsigned)slices);
+  k_mma<P, BF16><<<grid, 32 * kMmaWarps, 0, s>>>(p, part);
+  if (slices > 1)
+    k_mma_reduce<P><<<(unsigned)(((long)p.M * p.N + 255) / 256), 256, 0, s>>>(p, part, slices);
+}
+
+// Convolution forward: m = co, k = (ci, ky, kx), n = (b, oy, ox);
+// out = relu(bias + acc) in BF16.
+template <int K, int S, int P>
+struct ConvFwdProb {
+  const bf16 *in, *wt;
+  const float *bias;
+  bf16 *out;
+  ConvSpec c;
+  int M, N;
+  long Kd;
+  __device__ float a(int m, long k) const {
+    return (m < M && k < Kd) ? bf(wt[(size_t)m * Kd + k]) : 0.f;
+  }
+  __device__ float b(long k, int n) const {
+    if (n >= N || k >= Kd) return 0.f;
+    const int ci = (int)(k / (K * K)), ky = (int)((k / K) % K), kx = (int)(k % K);
+    const int hw = c.ho * c.wo, bb = n / hw, p = n % hw, oy = p / c.wo, ox = p % c.wo;
+    const int iy = oy * S - P + ky, ix = ox * S - P + kx;
+    if ((unsigned)iy >= (unsigned)c.hi || (unsigned)ix >= (unsigned)c.wi) return 0.f;
+    return bf(in[(((size_t)bb * c.ci + ci) * c.hi + iy) * c.wi + ix]);
+  }
+  __device__ void store(int m, int n, float v) const {
+    const int hw = c.ho * c.wo, bb = n / hw, p = n % hw;
+    out[((size_t)bb * c.co + m) * hw + p] = __float2bfloat16_rn(fmaxf(v + bias[m], 0.f));
+  }
+};
+
+// The gradient at a ReLU layer's pre-activation: gpost where act > 0.
+__device__ __forceinline__ float relu_grad(const float *gpost, const bf16 *act, size_t o) {
+  return (!act || bf(act[o]) > 0.f) ? gpost[o] : 0.f;
+}
+
+// Convolution input gradient: m = ci, k = (co, ky, kx), n = (b, iy, ix).
+template <int K, int S, int P>
+struct ConvBwdDataProb {
+  const float *gpost;
+  const bf16 *act, *wt;
+  float *gin;
+  ConvSpec c;
+  int M, N;
+  long Kd;
+  __device__ float a(int m, long k) const {
+    if (m >= M || k >= Kd) return 0.f;
+    const int co = (int)(k / (K * K)), tap = (int)(k % (K * K));
+    return bf(wt[((size_t)co * c.ci + m) * K * K + tap]);
+  }
+  __device__ float b(long k, int n) const {
+    if (n >= N || k >= Kd) return 0.f;
+    const int co = (int)(k / (K * K)), ky = (int)((k / K) % K), kx = (int)(k % K);
+    const int hw = c.hi * c.wi, bb = n / hw, q = n % hw, iy = q / c.wi, ix = q % c.wi;
+    const int ny = iy + P - ky, nx = ix + P - kx;
+    if (ny < 0 || nx < 0 || ny % S || nx % S) return 0.f;
+    const int oy = ny / S, ox = nx / S;
+    if (oy >= c.ho || ox >= c.wo) return 0.f;
+    return relu_grad(gpost, act, (((size_t)bb * c.co + co) * c.ho + oy) * c.wo + ox);
+  }
+  __device__ void store(int m, int n, float v) const {
+    const int hw = c.hi * c.wi, bb = n / hw, q = n % hw;
+    gin[((size_t)bb * c.ci + m) * hw + q] = v;
+  }
+};
+
+// Convolution weight (and bias) gradient: m = co, k = (b, oy, ox),
+// n = (ci, ky, kx), and n = ci K K is the bias (B = 1).
+template <int K, int S, int P>
+struct ConvBwdWeightProb {
+  const float *gpost;
+  const bf16 *act, *in;
+  float *gw, *gbias;
+  ConvSpec c;
+  int M, N;
+  long Kd;
+  __device__ float a(int m, long k) const {
+    if (m >= M || k >= Kd) return 0.f;
+    const int hw = c.ho * c.wo, bb = (int)(k / hw), p = (int)(k % hw);
+    return relu_grad(gpost, act, ((size_t)bb * c.co + m) * hw + p);
+  }
+  __device__ float b(long k, int n) const {
+    if (n >= N || k >= Kd) return 0.f;
+    if (n == N - 1) return 1.f;
+    const int ci = n / (K * K), ky = (n / K) % K, kx = n % K;
+    const int hw = c.ho * c.wo, bb = (int)(k / hw), p = (int)(k % hw), oy = p / c.wo, ox = p % c.wo;
+    const int iy = oy * S - P + ky, ix = ox * S - P + kx;
+    if ((unsigned)iy >= (unsigned)c.hi || (unsigned)ix >= (unsigned)c.wi) return 0.f;
+    return bf(in[(((size_t)bb * c.ci + ci) * c.hi + iy) * c.wi + ix]);
+  }
+  __device__ void store(int m, int n, float v) const {
+    if (n == N - 1) gbias[m] = v;
+    else gw[(size_t)m * (N - 1) + n] = v;
+  }
+};
+
+// Fully connected forward: m = j, k = i, n = b; out = act(bias + acc).
+template <bool RELU, typename TOut>
+struct FcFwdProb {
+  const bf16 *in, *wt;
+  const float *bias;
+  TOut *out;
+  int M, N;
+  long Kd;
+  __device__ float a(int m, long k) const {
+    return (m < M && k < Kd) ? bf(wt[(size_t)m * Kd + k]) : 0.f;
+  }
+  __device__ float b(long k, int n) const {
+    return (n < N && k < Kd) ? bf(in[(size_t)n * Kd + k]) : 0.f;
+  }
+  __device__ void store(int m, int n, float v) const {
+    v += bias[m];
+    if (RELU) v = fmaxf(v, 0.f);
+    if constexpr (sizeof(TOut) == 2) out[(size_t)n * M + m] = __float2bfloat16_rn(v);
+    else out[(size_t)n * M + m] = v;
+  }
+};
+
+// Fully connected input gradient: m = i, k = j, n = b.
+struct FcBwdDataProb {
+  const float *gpost;
+  const bf16 *act, *wt;
+  float *gin;
+  int M, N;  // M = nin, N = batch
+  long Kd;   // nout
+  __device__ float a(int m, long k) const {
+    return (m < M && k < Kd) ? bf(wt[(size_t)k * M + m]) : 0.f;
+  }
+  __device__ float b(long k, int n) const {
+    return (n < N && k < Kd) ? relu_grad(gpost, act, (size_t)n * Kd + k) : 0.f;
+  }
+  __device__ void store(int m, int n, float v) const { gin[(size_t)n * M + m] = v; }
+};
+
+// Fully connected weight (and bias) gradient: m = j, k = b, n = i, and
+// n = nin is the bias (B = 1).
+struct FcBwdWeightProb {
+  const float *gpost;
+  const bf16 *act, *in;
+  float *gw, *gbias;
+  int M, N;  // M = nout, N = nin + 1
+  long Kd;   // batch
+  __device__ float a(int m, long k) const {
+    return (m < M && k < Kd) ? relu_grad(gpost, act, (size_t)k * M + m) : 0.f;
+  }
+  __device__ float b(long k, int n) const {
+    if (n >= N || k >= Kd) return 0.f;
+    return n == N - 1 ? 1.f : bf(in[(size_t)k * (N - 1) + n]);
+  }
+  __device__ void store(int m, int n, float v) const {
+    if (n == N - 1) gbias[m] = v;
+    else gw[(size_t)m * (N - 1) + n] = v;
+  }
+};
 
 // ----------------------------------------------------------------- loss --
 
@@ -424,39 +569,82 @@ __global__ void k_adam(float *__restrict__ master, bf16 *__restrict__ mirror,
 
 unsigned blocks_for(long n) { return (unsigned)((n + 255) / 256 < 148L * 64 ? (n + 255) / 256 : 148L * 64); }
 
-constexpr int kSmallBatch = 16;  // up to this batch, one warp per conv output
+constexpr int kSmallBatch = 16;  // up to this batch, one warp per conv / fc output
+
+// Partial-tile floats the split reductions of a batch need (the weight
+// gradients, whose K = batch x output pixels).
+size_t mma_part_floats(int b) {
+  size_t m = 0;
+  for (int l = 0; l < 4; ++l) {
+    const ConvSpec &c = kConv[l];
+    const int sl = mma_slices((long)b * c.ho * c.wo);
+    const int taps = (l == 0 ? 25 : 9) * c.ci;
+    if (sl > 1) m = m > (size_t)sl * c.co * (taps + 1) ? m : (size_t)sl * c.co * (taps + 1);
+  }
+  const int sl = mma_slices(b);
+  if (sl > 1) {
+    const size_t f1 = (size_t)sl * kF1Out * (kF1In + 1), f2 = (size_t)sl * kF2Out * (kF1Out + 1);
+    m = m > f1 ? m : f1;
+    m = m > f2 ? m : f2;
+  }
+  return m;
+}
 
 template <int K, int S, int P>
 void conv_fwd(const bf16 *in, const bf16 *w, const float *b, const ConvSpec &c, int batch, bf16 *out,
-              cudaStream_t s) {
+              float *part, cudaStream_t s) {
   const long n = (long)batch * c.co * c.ho * c.wo;
-  if (batch <= kSmallBatch)
+  if (batch <= kSmallBatch) {
     k_conv_fwd_warp<K, S, P><<<(unsigned)((n * 32 + 255) / 256), 256, 0, s>>>(in, w, b, c, batch, out);
-  else
-    k_conv_fwd<K, S, P><<<blocks_for(n), 256, 0, s>>>(in, w, b, c, batch, out);
+  } else {
+    ConvFwdProb<K, S, P> p{in, w, b, out, c, c.co, batch * c.ho * c.wo, (long)c.ci * K * K};
+    mma_launch<ConvFwdProb<K, S, P>, true>(p, part, 1, s);
+  }
 }
 
 void forward(const bf16 *pw, const float *pm, const bf16 *in, int batch, const CnnWs &w,
              cudaStream_t s) {
   const bf16 *x = in;
-  conv_fwd<5, 2, 2>(x, pw + kOffW0, pm + kOffB0, kConv[0], batch, w.a[0], s);
-  conv_fwd<3, 2, 1>(w.a[0], pw + kOffW1, pm + kOffB1, kConv[1], batch, w.a[1], s);
-  conv_fwd<3, 2, 1>(w.a[1], pw + kOffW2, pm + kOffB2, kConv[2], batch, w.a[2], s);
-  conv_fwd<3, 2, 1>(w.a[2], pw + kOffW3, pm + kOffB3, kConv[3], batch, w.a[3], s);
-  const long w1 = (long)batch * kF1Out * 32, w2 = (long)batch * kF2Out * 32;
-  k_fc_fwd<true, bf16><<<(unsigned)((w1 + 255) / 256), 256, 0, s>>>(w.a[3], pw + kOffF1, pm + kOffBF1,
-                                                                   kF1In, kF1Out, batch, w.f1);
-  k_fc_fwd<false, float><<<(unsigned)((w2 + 255) / 256), 256, 0, s>>>(w.f1, pw + kOffF2, pm + kOffBF2,
-                                                                     kF1Out, kF2Out, batch, w.out);
+  conv_fwd<5, 2, 2>(x, pw + kOffW0, pm + kOffB0, kConv[0], batch, w.a[0], w.part, s);
+  conv_fwd<3, 2, 1>(w.a[0], pw + kOffW1, pm + kOffB1, kConv[1], batch, w.a[1], w.part, s);
+  conv_fwd<3, 2, 1>(w.a[1], pw + kOffW2, pm + kOffB2, kConv[2], batch, w.a[2], w.part, s);
+  conv_fwd<3, 2, 1>(w.a[2], pw + kOffW3, pm + kOffB3, kConv[3], batch, w.a[3], w.part, s);
+  if (batch <= kSmallBatch) {
+    const long w1 = (long)batch * kF1Out * 32, w2 = (long)batch * kF2Out * 32;
+    k_fc_fwd<true, bf16><<<(unsigned)((w1 + 255) / 256), 256, 0, s>>>(
+        w.a[3], pw + kOffF1, pm + kOffBF1, kF1In, kF1Out, batch, w.f1);
+    k_fc_fwd<false, float><<<(unsigned)((w2 + 255) / 256), 256, 0, s>>>(
+        w.f1, pw + kOffF2, pm + kOffBF2, kF1Out, kF2Out, batch, w.out);
+  } else {
+    FcFwdProb<true, bf16> f1{w.a[3], pw + kOffF1, pm + kOffBF1, w.f1, kF1Out, batch, kF1In};
+    mma_launch<FcFwdProb<true, bf16>, true>(f1, w.part, 1, s);
+    FcFwdProb<false, float> f2{w.f1, pw + kOffF2, pm + kOffBF2, w.out, kF2Out, batch, kF1Out};
+    mma_launch<FcFwdProb<false, float>, true>(f2, w.part, 1, s);
+  }
 }
 
+// A convolution's weight and bias gradients and, when gin is given, its
+// input gradient, from the gradient at its output (masked by its ReLU).
 template <int K, int S, int P>
 void conv_bwd(const float *gpost, const bf16 *act, const bf16 *in, const bf16 *wt, const ConvSpec &c,
-              int batch, float *gin, float *gw, float *gb, cudaStream_t s) {
-  k_conv_bwd_weight<K, S, P><<<c.co * c.ci, 256, 0, s>>>(gpost, act, in, c, batch, gw, gb);
-  if (gin)
-    k_conv_bwd_data<K, S, P><<<blocks_for((long)batch * c.ci * c.hi * c.wi), 256, 0, s>>>(
-        gpost, act, wt, c, batch, gin);
+              int batch, float *gin, float *gw, float *gb, float *part, cudaStream_t s) {
+  ConvBwdWeightProb<K, S, P> pw{gpost, act, in, gw, gb, c, c.co, c.ci * K * K + 1,
+                                (long)batch * c.ho * c.wo};
+  mma_launch<ConvBwdWeightProb<K, S, P>, false>(pw, part, mma_slices(pw.Kd), s);
+  if (gin) {
+    ConvBwdDataProb<K, S, P> pd{gpost, act, wt, gin, c, c.ci, batch * c.hi * c.wi,
+                                (long)c.co * K * K};
+    mma_launch<ConvBwdDataProb<K, S, P>, false>(pd, part, 1, s);
+  }
+}
+
+// A fully connected layer's weight and bias gradients and its input gradient.
+void fc_bwd(const float *gpost, const bf16 *act, const bf16 *in, const bf16 *wt, int nin, int nout,
+            int batch, float *gin, float *gw, float *gb, float *part, cudaStream_t s) {
+  FcBwdWeightProb pw{gpost, act, in, gw, gb, nout, nin + 1, batch};
+  mma_launch<FcBwdWeightProb, false>(pw, part, mma_slices(batch), s);
+  FcBwdDataProb pd{gpost, act, wt, gin, nin, batch, nout};
+  mma_launch<FcBwdDataProb, false>(pd, part, 1, s);
 }
 
 }  // namespace
@@ -522,24 +710,20 @@ extern "C" of_status_t of_cnn_backward(const uint16_t *d_params, const float *d_
   k_loss<<<(batch + 255) / 256, 256, 0, s>>>(w.out, d_target, d_loss_weights, batch, w.gout, w.loss);
   k_loss_sum<<<1, 32, 0, s>>>(w.loss, batch);
   // f2 (linear): gradients of its weights and of f1's output
-  k_fc_bwd_weight<<<(unsigned)(((long)kF2Out * (kF1Out + 1) + 255) / 256), 256, 0, s>>>(
-      w.gout, nullptr, w.f1, kF1Out, kF2Out, batch, d_grad + kOffF2, d_grad + kOffBF2);
-  k_fc_bwd_data<<<(unsigned)(((long)batch * kF1Out + 255) / 256), 256, 0, s>>>(
-      w.gout, nullptr, pw + kOffF2, kF1Out, kF2Out, batch, w.gf1);
+  fc_bwd(w.gout, nullptr, w.f1, pw + kOffF2, kF1Out, kF2Out, batch, w.gf1, d_grad + kOffF2,
+         d_grad + kOffBF2, w.part, s);
   // f1 (ReLU)
-  k_fc_bwd_weight<<<(unsigned)(((long)kF1Out * (kF1In + 1) + 255) / 256), 256, 0, s>>>(
-      w.gf1, w.f1, w.a[3], kF1In, kF1Out, batch, d_grad + kOffF1, d_grad + kOffBF1);
-  k_fc_bwd_data<<<(unsigned)(((long)batch * kF1In + 255) / 256), 256, 0, s>>>(
-      w.gf1, w.f1, pw + kOffF1, kF1In, kF1Out, batch, w.g[3]);
+  fc_bwd(w.gf1, w.f1, w.a[3], pw + kOffF1, kF1In, kF1Out, batch, w.g[3], d_grad + kOffF1,
+         d_grad + kOffBF1, w.part, s);
   // convs (ReLU), last to first; the first has no input gradient
   conv_bwd<3, 2, 1>(w.g[3], w.a[3], w.a[2], pw + kOffW3, kConv[3], batch, w.g[2], d_grad + kOffW3,
-                    d_grad + kOffB3, s);
+                    d_grad + kOffB3, w.part, s);
   conv_bwd<3, 2, 1>(w.g[2], w.a[2], w.a[1], pw + kOffW2, kConv[2], batch, w.g[1], d_grad + kOffW2,
-                    d_grad + kOffB2, s);
+                    d_grad + kOffB2, w.part, s);
   conv_bwd<3, 2, 1>(w.g[1], w.a[1], w.a[0], pw + kOffW1, kConv[1], batch, w.g[0], d_grad + kOffW1,
-                    d_grad + kOffB1, s);
+                    d_grad + kOffB1, w.part, s);
   conv_bwd<5, 2, 2>(w.g[0], w.a[0], in, pw + kOffW0, kConv[0], batch, nullptr, d_grad + kOffW0,
-                    d_grad + kOffB0, s);
+                    d_grad + kOffB0, w.part, s);
   if (d_loss)
     OF_CUDA_TRY(cudaMemcpyAsync(d_loss, w.loss + batch, sizeof(float), cudaMemcpyDeviceToDevice, s));
   return of_launch_status();

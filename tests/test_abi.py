@@ -34,7 +34,7 @@ def test_binding_table_matches_header(of):
 
 def test_abi_version_and_status_strings(of):
     lib = of._native.lib()
-    assert lib.of_abi_version() == 3
+    assert lib.of_abi_version() == 4
     assert lib.of_status_string(0) == b"ok"
     assert b"invalid" in lib.of_status_string(1)
 

@@ -419,6 +419,36 @@ def test_tracker_graph_equals_eager(of, cuda):
     assert np.array_equal(poses[0], poses[1])
 
 
+@pytest.mark.parametrize("name", ["c1", "c2"])
+def test_tracker_online_tuning_changes_no_result(of, cuda, name):
+    """A tracker that tunes the raycast block shape online (step 2 times
+    every shape, then the step graphs are captured) tracks bit for bit like
+    one with the default shape, and every shape gives the same model."""
+    import dataclasses
+    import torch
+    cfg = small(of, name)
+    seq = of.make_sequence(cfg, frames=6)
+    depth = [torch.from_numpy(seq.depth[k].astype(np.int16)).to(cuda) for k in range(6)]
+    runs = []
+    for tune in (0, 2):
+        tr = of.Tracker(cfg, seq.poses[0], use_graph=True, tune=tune)
+        for d in depth:
+            tr.process(d)
+        runs.append((tr.pose_history(6), tr.tuning()))
+        tr.close()
+    assert runs[0][1] == (0, False)
+    assert runs[1][1][1] and 0 <= runs[1][1][0] < 4, runs[1][1]
+    assert np.array_equal(runs[0][0], runs[1][0])
+    vol, lam = of.new_volume(cfg, cuda), of.lambda_table(cfg, cuda)
+    for k in range(3):
+        of.integrate(cfg, vol, depth[k], dev_pose(seq.poses[k], cuda), lam)
+    models = [of.raycast(dataclasses.replace(cfg, ray_tile=t), vol, dev_pose(seq.poses[2], cuda))
+              for t in range(4)]
+    torch.cuda.synchronize()
+    for m in models[1:]:
+        assert torch.equal(m, models[0])
+
+
 def test_tracker_equals_stagewise_pipeline(of, cuda):
     """The tracker's step (fuse k-1 and raycast beside pre-process k, then
     ICP k) gives bit for bit the poses of the stage-by-stage sequence
