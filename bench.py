@@ -380,8 +380,8 @@ def run_ours(args, cfg, world, rank, local):
     depth_host = torch.from_numpy(seq.depth.astype(np.int16)).pin_memory()
     stream = torch.cuda.current_stream(dev)
 
-    # the tracker tunes its raycast block shape online at a warm-up step, before
-    # its step graphs are captured (never inside the timed region)
+    # the tracker tunes its raycast block shape online at a warm-up step,
+    # before its step graphs are captured (never inside the timed region)
     tune = min(3, args.warmup) if args.warmup >= 1 else 0
     # ---- device-resident loop: value
     tr = of.Tracker(cfg, seq.poses[0], use_graph=True, pose_history=total, tune=tune)
@@ -445,7 +445,7 @@ def run_ours(args, cfg, world, rank, local):
     tr.close()
 
     # ---- per-stage kernel times (stage-wise launches with CUDA events), with
-    # the block shape the tracker chose
+    # the raycast block shape the tracker chose
     import dataclasses
     stages = stage_times(of, dataclasses.replace(cfg, ray_tile=ray_tile), seq, depth_dev, order,
                          args, dev)

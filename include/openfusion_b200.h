@@ -355,15 +355,12 @@ typedef struct of_tracker_desc {
   /* Camera-side filters applied in place to each depth frame before it is
    * used (steps = 0: none). */
   of_depth_filter_params_t depth_filter;
-  /* Online tuning of the step shape, which changes no result (no reference
-   * counterpart). A step raycasts the model and tracks the new frame either
-   * in one launch (the default) or as a raycast launch with the block shape
-   * raycast.tile followed by the ICP launch. 0: the default. k >= 1: step k
-   * times the five candidates (the combined launch, and the separate launches
-   * with each raycast block shape) on the volume it has just fused, at its
-   * tracked pose, into scratch buffers, keeps the fastest (of_tracker_tuning)
-   * and only then captures the step graphs; the steps before it run without
-   * graphs and step k synchronises its stream. */
+  /* Online tuning of the launch shapes that change no result (no reference
+   * counterpart). 0: raycast.tile is used as given. k >= 1: step k times
+   * every raycast block shape (of_raycast_params_t.tile) on the volume it has
+   * just fused, at its tracked pose, into a scratch model, keeps the fastest
+   * (of_tracker_tuning), and only then captures the step graphs; the steps
+   * before it run without graphs and step k synchronises its stream. */
   int32_t tune;
 } of_tracker_desc_t;
 
@@ -419,11 +416,9 @@ typedef struct of_tracker_buffers {
   int32_t kernels_track;  /* kernel launches of every later step's graph */
 } of_tracker_buffers_t;
 of_status_t of_tracker_buffers(of_tracker_t tracker, of_tracker_buffers_t *out);
-/* The step shape in use (combined = 1: raycast and ICP in one launch; else
- * the raycast's block shape, of_raycast_params_t.tile) and whether the online
- * tuning has run (of_tracker_desc_t.tune). */
-of_status_t of_tracker_tuning(of_tracker_t tracker, int32_t *combined, int32_t *ray_tile,
-                              int32_t *tuned);
+/* The raycast block shape in use (of_raycast_params_t.tile) and whether the
+ * online tuning has run (of_tracker_desc_t.tune). */
+of_status_t of_tracker_tuning(of_tracker_t tracker, int32_t *ray_tile, int32_t *tuned);
 
 /* ---- surface mesh and volume file (no GL) ----------------------------- */
 

@@ -180,7 +180,7 @@ _SIGS = {
     "of_tracker_pose": (c_status, [P, P, P, c_stream]),
     "of_tracker_pose_history": (c_status, [P, P, C.c_int32, c_stream]),
     "of_tracker_buffers": (c_status, [P, C.POINTER(TrackerBuffers)]),
-    "of_tracker_tuning": (c_status, [P, P, P, P]),
+    "of_tracker_tuning": (c_status, [P, P, P]),
     "of_points_to_reference": (c_status, [C.POINTER(Camera), P, P, P, P, c_stream]),
     "of_points_from_reference": (c_status, [C.POINTER(Camera), C.c_int32, P, P, P, c_stream]),
     "of_pose_from_float": (c_status, [P, P, C.c_int32, c_stream]),

@@ -383,10 +383,9 @@ class Tracker:
                  pose_history: int = 1024, warm_start_weights: np.ndarray | None = None,
                  depth_filter: N.DepthFilterParams | None = None, tune: int = 0):
         """`warm_start_weights`: FP32 weights of the warm-start CNN (None =
-        plain ICP from the previous pose). `tune` = k >= 1: step k times the
-        step shapes (raycast and ICP in one launch, or separately with each
-        raycast block shape) and keeps the fastest before the step graphs are
-        captured (of_tracker_desc_t.tune); 0: the one-launch step."""
+        plain ICP from the previous pose). `tune` = k >= 1: step k times every
+        raycast block shape and keeps the fastest before the step graphs are
+        captured (of_tracker_desc_t.tune); 0: cfg.ray_tile as given."""
         self.cfg = cfg
         d = N.TrackerDesc()
         d.camera = cfg.camera()
@@ -474,13 +473,12 @@ class Tracker:
         N.check("of_tracker_buffers", N.lib().of_tracker_buffers(self._h, C.byref(b)))
         return b
 
-    def tuning(self) -> tuple[bool, int, bool]:
-        """(raycast and ICP in one launch?, raycast block shape when not,
-        whether the online tuning has run)."""
-        comb, tile, tuned = C.c_int32(), C.c_int32(), C.c_int32()
-        N.check("of_tracker_tuning", N.lib().of_tracker_tuning(self._h, C.byref(comb),
-                                                               C.byref(tile), C.byref(tuned)))
-        return bool(comb.value), tile.value, bool(tuned.value)
+    def tuning(self) -> tuple[int, bool]:
+        """(raycast block shape in use, whether the online tuning has run)."""
+        tile, tuned = C.c_int32(), C.c_int32()
+        N.check("of_tracker_tuning", N.lib().of_tracker_tuning(self._h, C.byref(tile),
+                                                               C.byref(tuned)))
+        return tile.value, bool(tuned.value)
 
 
 # --------------------------------------------------------------- synthetic --

@@ -20,7 +20,7 @@
 //   build dT = [Rz(g) Ry(b) Rx(a) | t] and compose T <- dT T in FP64
 //   (ICP.cu:266-305). A singular system restores the frame's starting pose and
 //   stops the remaining iterations (ICP.cpp:152-158).
-#include "of_raycast.cuh"
+#include "of_batch.cuh"
 
 #include <mutex>
 #include <string.h>
@@ -66,12 +66,6 @@ struct IcpWorkspace {
   unsigned long long fused_rows[2][kFusedMaxBlocks][32];
   unsigned int epoch;  // frames begun on this workspace (k_icp_begin), mod 2^19
   unsigned int magic;  // kWorkspaceMagic once k_icp_begin has cleared the rows
-  unsigned int ray_next;     // k_track_step: next ray chunk
-  unsigned int coarse_done;  // k_track_step: coarse ray chunks written
-  // the group's state after the coarse levels, for every block
-  double coarse_pose[16];
-  double coarse_res, coarse_piv;
-  int coarse_its, coarse_stop, coarse_inl, coarse_examined;
 };
 constexpr unsigned kWorkspaceMagic = 0x4F46494Bu;
 
@@ -305,7 +299,6 @@ struct IcpPlan {
   float stop_rot, stop_trans;  // early exit (0: every iteration)
   float judge_rms, judge_frac, judge_rot, judge_trans;
   int warm_levels;  // levels of a warm-started pass (<= levels)
-  int group;        // blocks that run the coarse levels (0: every block)
   // optional pose history (a ring of hist_cap row-major poses and its running
   // count): the final pose is appended by the kernel's last store
   double *hist;
@@ -568,518 +561,307 @@ __device__ __forceinline__ bool judge_keep(const IcpPlan &plan, const double *W,
          sqrt(dt2) <= plan.judge_trans;
 }
 
-// ---------------------------------------------------------------------------
-// The fused tracking kernel: the whole multi-level ICP of one frame in one
-// cooperative launch (k_icp_fused), and the same preceded by the frame's
-// raycast (k_track_step).
-//
-// Reduction topology. A level's iterations run on G co-resident blocks: the
-// coarse pyramid levels (l >= 1) on a group of kGroupBlocks blocks, the finest
-// level on every block. Within a level each block owns every G-th 32-pixel
-// chunk of the level's model; at the start of the level it copies its chunks'
-// valid model points (vertex, normal) into shared memory in chunk order, up to
-// the dynamic shared-memory capacity (the rest is read from global memory at
-// every iteration). Per iteration every participating block associates its
-// points two at a time (both frame gathers in flight together), accumulates
-// the rows (pairwise tree sums), writes its 29 partials as self-validating
-// 64-bit slots, reads the G blocks' rows (seeing every slot of this iteration
-// is the iteration's barrier), sums them in a fixed order, and one warp solves
-// the 6x6 system, so every block holds the same new pose without a second
-// barrier. Partials alternate between two buffers: a block can only overwrite
-// buffer i % 2 after the exchange of iteration i + 1, which every block
-// reaches only after reading it. Between the group's levels and level 0 one
-// grid barrier hands the group's state (pose, counters) to every block. The
-// coarse levels hold a quarter and a sixteenth of the pixels: on the whole
-// grid most blocks would idle through an exchange among 148 rows; on the group
-// the exchange is among 16.
-//
-// k_track_step first raycasts the model (the tracker step's raycast of frame
-// k - 1) with the same per-ray code as of_raycast, the rays taken by warps
-// from a queue of 32-ray chunks: the coarse-level rays (pixels (2x, 2y), whose
-// points are levels 1 and 2) first, then the others. Once the coarse rays are
-// written, the group runs the coarse ICP levels while the other blocks march
-// the remaining rays; the group then takes rays again, and after one grid
-// barrier (every ray written) all blocks run level 0. The raycast and the ICP
-// are those of the separate launches, bit for bit.
-
-constexpr int kGroupBlocks = 16;
-
-// Per-block state of the fused kernel (shared memory).
-struct FusedState {
-  double pose[16];
-  Rigid c2w, w2c;
-  double res, piv;
-  int stop, inl, its, err, conv, warm, examined;
-};
-
-// Waits until the relaxed-loaded counter `*p` reaches `target` (thread 0 of a
-// block); bounded like every wait here: on timeout or another block's
-// failure the workspace error flag is set and false returned.
-__device__ bool wait_count(IcpWorkspace *ws, const unsigned *p, unsigned target) {
-  unsigned spins = 0;
-  while (ld_acquire_gpu(p) < target) {
-    if (++spins > kSpinLimit ||
-        ((spins & 255u) == 0u && ld_acquire_gpu(reinterpret_cast<unsigned *>(&ws->error)))) {
-      atomicExch(&ws->error, 1);
-      return false;
-    }
-    __nanosleep(32);
-  }
-  return true;
-}
-
-// Grid barrier number k (1, 2, ... within a frame) of the co-resident grid,
-// over a monotonic arrival counter zeroed by the frame's begin step. Writes
-// before it (fenced by each block's thread 0 after its block barrier) are
-// seen after it.
-__device__ void grid_barrier(IcpWorkspace *ws, unsigned k, FusedState &S) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(&ws->bar_count, 1u);
-    if (!wait_count(ws, &ws->bar_count, k * gridDim.x)) S.err = 1;
-  }
-  __syncthreads();
-}
-
-// The group's result (block 0 of the group writes it; read after a barrier).
-__device__ void put_group_state(IcpWorkspace *ws, const FusedState &S) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  for (int i = 0; i < 16; ++i) ws->coarse_pose[i] = S.pose[i];
-  ws->coarse_its = S.its;
-  ws->coarse_stop = S.stop;
-  ws->coarse_inl = S.inl;
-  ws->coarse_examined = S.examined;
-  ws->coarse_res = S.res;
-  ws->coarse_piv = S.piv;
-}
-__device__ void get_group_state(IcpWorkspace *ws, FusedState &S) {
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < 16; ++i) S.pose[i] = __ldcg(&ws->coarse_pose[i]);
-    S.its = __ldcg(&ws->coarse_its);
-    S.stop = __ldcg(&ws->coarse_stop);
-    S.inl = __ldcg(&ws->coarse_inl);
-    S.examined = __ldcg(&ws->coarse_examined);
-    S.res = __ldcg(&ws->coarse_res);
-    S.piv = __ldcg(&ws->coarse_piv);
-    pose_to_rigid(S.pose, &S.c2w, &S.w2c);
-  }
-  __syncthreads();
-}
-
-// The iterations of level l on blocks [0, G) (the caller calls it on those
-// only). The model is read with L2 loads: k_track_step writes it in the same
-// launch.
-__device__ void icp_level(const IcpPlan &plan, int l, int G, IcpWorkspace *ws, FusedState &S,
-                          float4 *s_pts, bool hold, unsigned epoch) {
-  __shared__ float s_red[kFusedThreads / 32][32];
-  __shared__ float s_tot[32];
-  __shared__ int s_warp_n[kFusedThreads / 32];
-  __shared__ int s_npts;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int kWarps = kFusedThreads / 32;
-  const float dist2 = plan.dist_thresh * plan.dist_thresh, nthr = plan.normal_thresh;
-  const IcpLevel L = plan.lv[l];
-  const int npx = L.mw * L.mh;
-  // model pixels are dealt to blocks in chunks of 32 (one warp), round
-  // robin, so every block gets an even, spatially spread share: chunk
-  // c_k = block + k * G, k = 0 .. my_chunks - 1; the first kc chunks
-  // are kept in shared memory, the rest is read at every iteration
-  const int nchunks = (npx + 31) >> 5;
-  const int my_chunks = nchunks > (int)blockIdx.x ? (nchunks - 1 - (int)blockIdx.x) / G + 1 : 0;
-  const int kc = min(my_chunks, plan.cache_pts >> 5);
-  // ---- cache this block's valid model points of the level, in chunk order
-  if (threadIdx.x == 0) { s_npts = 0; S.conv = 0; }
-  __syncthreads();
-  for (int k0 = 0; k0 < kc; k0 += kWarps) {
-    const int k = k0 + warp;
-    const int p = ((int)blockIdx.x + k * G) * 32 + lane;
-    float4 s = make_float4(0.f, 0.f, 0.f, 0.f), ns = s;
-    bool valid = false;
-    if (k < kc && p < npx) {
-      s = __ldcg(L.model + 2 * p);
-      ns = __ldcg(L.model + 2 * p + 1);
-      valid = s.w != 0.f && ns.w != 0.f;
-    }
-    const unsigned m = __ballot_sync(0xffffffffu, valid);
-    if (lane == 0) s_warp_n[warp] = __popc(m);
-    __syncthreads();
-    int off = s_npts;
-    for (int w = 0; w < warp; ++w) off += s_warp_n[w];
-    if (valid) {
-      const int slot = off + __popc(m & ((1u << lane) - 1u));
-      s_pts[2 * slot] = s;
-      s_pts[2 * slot + 1] = ns;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int tot = 0;
-      for (int w = 0; w < kWarps; ++w) tot += s_warp_n[w];
-      s_npts += tot;
-    }
-    __syncthreads();
-  }
-  const int n = s_npts;
-  for (int it = 0; it < L.iters; ++it) {
-    float acc[kVals];
-    float examined = 0.f;  // model points that project into the frame
-#pragma unroll
-    for (int v = 0; v < kVals; ++v) acc[v] = 0.f;
-    // cached points, two per step
-    for (int i = threadIdx.x; i < n; i += 2 * kFusedThreads) {
-      const int j = i + kFusedThreads;
-      const int qA = associate(S.w2c, L.cam, s_pts[2 * i]);
-      const int qB = j < n ? associate(S.w2c, L.cam, s_pts[2 * j]) : -1;
-      float4 dA = make_float4(0.f, 0.f, 0.f, 0.f), cA = dA, dB = dA, cB = dA;
-      if (qA >= 0) { dA = __ldg(L.frame + 2 * qA); cA = __ldg(L.frame + 2 * qA + 1); }
-      if (qB >= 0) { dB = __ldg(L.frame + 2 * qB); cB = __ldg(L.frame + 2 * qB + 1); }
-      // the model points are read again from shared memory rather than
-      // held in registers across the gathers
-      asm volatile("" ::: "memory");
-      if (qA >= 0) {
-        examined += 1.f;
-        try_row(acc, S.c2w, s_pts[2 * i], s_pts[2 * i + 1], dA, cA, dist2, nthr);
-      }
-      if (qB >= 0) {
-        examined += 1.f;
-        try_row(acc, S.c2w, s_pts[2 * j], s_pts[2 * j + 1], dB, cB, dist2, nthr);
-      }
-    }
-    // the rest of the block's chunks, from global memory
-    for (int k = kc + warp; k < my_chunks; k += kWarps) {
-      const int p = ((int)blockIdx.x + k * G) * 32 + lane;
-      if (p >= npx) continue;
-      const float4 s = __ldcg(L.model + 2 * p);
-      const float4 ns = __ldcg(L.model + 2 * p + 1);
-      if (s.w == 0.f || ns.w == 0.f) continue;
-      const int q = associate(S.w2c, L.cam, s);
-      if (q < 0) continue;
-      examined += 1.f;
-      try_row(acc, S.c2w, s, ns, __ldg(L.frame + 2 * q), __ldg(L.frame + 2 * q + 1), dist2, nthr);
-    }
-    // pairwise sums: a recursive-halving exchange across the warp (lanes
-    // trade half of their remaining values each step, 31 shuffles for 32
-    // values) leaves lane v with the warp's sum of value v; then a tree
-    // over the block's warps. Value kVals is the examined-point count. A
-    // warp that examined no point (the coarse levels leave most warps
-    // idle) holds only +0 and writes its zeros directly.
-    if (!__any_sync(0xffffffffu, examined > 0.f)) {
-      s_red[warp][lane] = 0.f;
-    } else {
-      float r[32];
-#pragma unroll
-      for (int v = 0; v < 32; ++v) r[v] = v < kVals ? acc[v] : (v == kVals ? examined : 0.f);
-#pragma unroll
-      for (int sft = 16; sft >= 1; sft >>= 1) {
-        const bool upper = (lane & sft) != 0;
-#pragma unroll
-        for (int i = 0; i < sft; ++i) {
-          float send = upper ? r[i] : r[i + sft];
-          float keep = upper ? r[i + sft] : r[i];
-          r[i] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
-        }
-      }
-      s_red[warp][lane] = r[0];
-    }
-    __syncthreads();
-    // (S.its: the iterations this frame has run, on every block alike)
-    const int buf = S.its & 1;
-    const unsigned seq = (epoch << kIterBits) | (unsigned)(S.its + 1);
-    if (warp == 0) {
-      float y[kWarps];
-#pragma unroll
-      for (int w = 0; w < kWarps; ++w) y[w] = s_red[w][lane];
-#pragma unroll
-      for (int span = 1; span < kWarps; span *= 2)
-#pragma unroll
-        for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
-      // publish: each value with this iteration's sequence number in one
-      // 64-bit store (no fence: a slot validates itself)
-      if (lane <= kVals)
-        st_relaxed_gpu(&ws->fused_rows[buf][blockIdx.x][lane],
-                       (unsigned long long)__float_as_uint(y[0]) | ((unsigned long long)seq << 32));
-      // the fault-injection hook: an arrival that never comes
-      if (hold && lane == 0 && !wait_seq(ws, &ws->bar_gen, 0xffffffffu)) {
-        atomicExch(&ws->error, 1);
-        S.err = 1;
-      }
-    }
-    // every block: wait for each block's row of this iteration, then
-    // Kahan over its strided share of the rows and a tree over the
-    // groups, in a fixed order. Lane v of warp g reads value v of rows
-    // g, g + 32, ...; a round re-reads only the slots not yet seen.
-    {
-      constexpr int kPer = (kFusedMaxBlocks + kWarps - 1) / kWarps;
-      const int v = lane, grp = warp;
-      float vals[kPer];
-      unsigned pending = 0;
-#pragma unroll
-      for (int q = 0; q < kPer; ++q) {
-        vals[q] = 0.f;
-        if (v <= kVals && grp + q * kWarps < G) pending |= 1u << q;
-      }
-      unsigned spins = 0;
-      for (;;) {
-#pragma unroll
-        for (int q = 0; q < kPer; ++q) {
-          if (!((pending >> q) & 1u)) continue;
-          const unsigned long long w = ld_relaxed_gpu(&ws->fused_rows[buf][grp + q * kWarps][v]);
-          if ((unsigned)(w >> 32) == seq) {
-            vals[q] = __uint_as_float((unsigned)w);
-            pending &= ~(1u << q);
-          }
-        }
-        if (__all_sync(0xffffffffu, pending == 0u)) break;
-        if (++spins > kSpinLimit ||
-            ((spins & 255u) == 0u && ld_acquire_gpu(reinterpret_cast<unsigned *>(&ws->error)))) {
-          if (lane == 0) {
-            atomicExch(&ws->error, 1);
-            S.err = 1;
-          }
-          break;
-        }
-        __nanosleep(32);
-      }
-      float sum = 0.f, c = 0.f;
-#pragma unroll
-      for (int q = 0; q < kPer; ++q) {
-        float y = vals[q] - c;
-        float t = sum + y;
-        c = (t - sum) - y;
-        sum = t;
-      }
-      s_red[grp][v] = sum - c;
-    }
-    // a wait that gave up (here or, later, in every other block) ends this
-    // frame's tracking; the final status reads the workspace's flag
-    __syncthreads();
-    if (S.err) break;
-    if (threadIdx.x < 32) {
-      float y[kWarps];
-#pragma unroll
-      for (int w = 0; w < kWarps; ++w) y[w] = s_red[w][threadIdx.x];
-#pragma unroll
-      for (int span = 1; span < kWarps; span *= 2)
-#pragma unroll
-        for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
-      s_tot[threadIdx.x] = y[0];
-      __syncwarp();
-      double minpiv = 0.0;
-      float inc_rot = 0.f, inc_trans = 0.f;
-      // (on success the warp also writes the new pose's rigid transforms)
-      const bool ok =
-          warp_solve_update(s_tot, S.pose, &minpiv, &inc_rot, &inc_trans, &S.c2w, &S.w2c);
-      if (threadIdx.x == 0) {
-        S.its += 1;
-        S.inl = (int)s_tot[28];
-        S.examined = (int)s_tot[kVals];
-        S.res = (double)s_tot[27];
-        S.piv = minpiv;
-        if (!ok) {
-          for (int i = 0; i < 16; ++i) S.pose[i] = ws->pose_init[i];
-          S.stop = 1;
-          pose_to_rigid(S.pose, &S.c2w, &S.w2c);
-        } else if (plan.stop_rot > 0.f && inc_rot < plan.stop_rot && inc_trans < plan.stop_trans) {
-          S.conv = 1;  // converged at this level
-        }
-      }
-    }
-    __syncthreads();
-    if (S.stop || S.conv) break;
-  }
-}
-
-// The levels top .. 0 of one pass from the current state: the coarse ones
-// on the group when the plan has one (then a grid barrier hands the group's
-// state over), level 0 on every block. `*barriers` counts the grid barriers.
-__device__ void icp_pass(const IcpPlan &plan, int top, IcpWorkspace *ws, FusedState &S,
-                         float4 *s_pts, bool hold, unsigned epoch, unsigned *barriers,
-                         bool group_done = false) {
-  const int G = (int)gridDim.x;
-  const bool grouped = plan.group > 0 && top >= 1;
-  if (grouped && !group_done) {
-    if ((int)blockIdx.x < plan.group)
-      for (int l = top; l >= 1 && !S.stop && !S.err; --l) icp_level(plan, l, plan.group, ws, S, s_pts, hold, epoch);
-    if ((int)blockIdx.x < plan.group) put_group_state(ws, S);
-  }
-  if (grouped) {
-    grid_barrier(ws, ++*barriers, S);
-    const int err = S.err;
-    get_group_state(ws, S);
-    if (threadIdx.x == 0) S.err = err;
-    __syncthreads();
-  }
-  for (int l = grouped ? 0 : top; l >= 0 && !S.stop && !S.err; --l)
-    icp_level(plan, l, G, ws, S, s_pts, hold, epoch);
-}
-
-// The queue of the raycast's rays in k_track_step: 32-ray chunks, the
-// coarse-level rays (pixel (2x, 2y) for the level-1 pixel (x, y)) first,
-// then the three other pixels of every 2 x 2 quad.
-struct RayQueue {
-  const uint32_t *vol;
-  of_volume_desc_t desc;
-  Cam cam;
-  of_raycast_params_t rp;
-  float4 *pts;
-  ModelLevels coarse;
-  int w1, h1;  // level-1 size
-};
-
-__device__ __forceinline__ bool chunk_pixel(const RayQueue &R, int c, int ncc, int lane, int *x,
-                                            int *y) {
-  if (c < ncc) {
-    const int i = c * 32 + lane;
-    if (i >= R.w1 * R.h1) return false;
-    *x = 2 * (i % R.w1);
-    *y = 2 * (i / R.w1);
-  } else {
-    const int f = (c - ncc) * 32 + lane;
-    if (f >= 3 * R.w1 * R.h1) return false;
-    const int q = f / 3, sub = f - 3 * q, qx = q % R.w1, qy = q / R.w1;
-    *x = 2 * qx + (sub != 1 ? 1 : 0);
-    *y = 2 * qy + (sub != 0 ? 1 : 0);
-  }
-  return *x < R.cam.w && *y < R.cam.h;
-}
-
-// Warps take chunks until the queue is empty (or, with `coarse_only`, until
-// the coarse chunks are all taken); each finished coarse chunk is counted
-// after its points are written and fenced.
-template <int STORAGE>
-__device__ void ray_chunks(const RayQueue &R, const RaySetup &setup, IcpWorkspace *ws,
-                           bool coarse_only) {
-  const int lane = threadIdx.x & 31;
-  const int ncc = (R.w1 * R.h1 + 31) / 32, nfc = (3 * R.w1 * R.h1 + 31) / 32;
-  const int nch = ncc + nfc;
-  for (;;) {
-    int c = nch;
-    if (lane == 0 && !(coarse_only && ld_acquire_gpu(&ws->ray_next) >= (unsigned)ncc))
-      c = (int)min(atomicAdd(&ws->ray_next, 1u), (unsigned)nch);
-    c = __shfl_sync(0xffffffffu, c, 0);
-    if (c >= nch) break;
-    int x = 0, y = 0;
-    if (chunk_pixel(R, c, ncc, lane, &x, &y))
-      raycast_pixel<STORAGE>(R.vol, R.desc, R.cam, R.rp, setup, x, y, R.pts, nullptr, &R.coarse);
-    if (c < ncc) {
-      __threadfence();
-      __syncwarp();
-      if (lane == 0) atomicAdd(&ws->coarse_done, 1u);
-    }
-  }
-}
-
-// Initial per-block state: pass 0 starts from the warm start when this frame
-// has one, else from the frame's starting pose (ws->pose_init, the begin
-// step's, with any prior applied).
-__device__ void fused_start(IcpWorkspace *ws, FusedState &S) {
-  const bool warm = ws->has_warm != 0;
-  if (threadIdx.x < 16) S.pose[threadIdx.x] = warm ? ws->warm_pose[threadIdx.x] : ws->pose_init[threadIdx.x];
-  if (threadIdx.x == 0) {
-    S.stop = 0; S.err = 0; S.its = 0; S.inl = 0; S.res = 0.0; S.piv = 0.0; S.examined = 0;
-    S.conv = 0;
-    S.warm = warm ? 1 : 0;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) pose_to_rigid(S.pose, &S.c2w, &S.w2c);
-  __syncthreads();
-}
-
-// Both passes (warm start, judge, replacement) and the final writes.
-__device__ void fused_finish(const IcpPlan &plan, double *pose, IcpWorkspace *ws,
-                             of_icp_stats_t *stats, FusedState &S, float4 *s_pts,
-                             unsigned *barriers, bool group_done) {
-  const bool warm = S.warm != 0;
-  const unsigned epoch = ws->epoch;
-  const bool hold = ws->hold_barrier > 0;
-  for (int pass = 0; pass < 2; ++pass) {
-    const int top = (pass == 0 && warm) ? plan.warm_levels - 1 : plan.levels - 1;
-    icp_pass(plan, top, ws, S, s_pts, hold, epoch, barriers, pass == 0 && group_done);
-    // ---- judge a warm-started result; replace it by plain ICP if it fails
-    if (pass == 1 || !warm || S.err) break;
-    if (threadIdx.x == 0) {
-      const bool keep = !S.stop && judge_keep(plan, ws->warm_pose, S.pose, S.res, S.inl, S.examined);
-      S.warm = keep ? 1 : 2;
-      if (!keep) {
-        S.stop = 0;
-        for (int i = 0; i < 16; ++i) S.pose[i] = ws->pose_init[i];
-        pose_to_rigid(S.pose, &S.c2w, &S.w2c);
-      }
-    }
-    __syncthreads();
-    if (S.warm == 1) break;
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    int err = *((volatile int *)&ws->error);
-    for (int i = 0; i < 16; ++i) pose[i] = err ? ws->pose_init[i] : S.pose[i];
-    if (plan.hist) {
-      const unsigned long long c = *plan.hist_count;
-      double *dst = plan.hist + (size_t)(c % (unsigned long long)plan.hist_cap) * 16;
-      for (int i = 0; i < 16; ++i) dst[i] = err ? ws->pose_init[i] : S.pose[i];
-      *plan.hist_count = c + 1;
-    }
-    ws->iterations = S.its;
-    if (stats) {
-      stats->status = err ? 2 : (S.stop ? 1 : 0);
-      stats->inliers = S.inl;
-      stats->iterations = S.its;
-      stats->warm = warm ? S.warm : 0;
-      stats->residual_sq = S.res;
-      stats->min_pivot = S.piv;
-    }
-  }
-}
-
+// The whole multi-level ICP of one frame in one cooperative launch. Each
+// block owns every grid-th 32-pixel chunk of every level's model; at the
+// start of a level it copies its chunks' valid model points (vertex, normal)
+// into shared memory in chunk order, up to the dynamic shared-memory capacity
+// (the rest is read from global memory at every iteration). Per
+// iteration: every block associates its points two at a time (both frame
+// gathers in flight together), accumulates the rows (tree sums), writes 29
+// partials, meets the others at one grid barrier, then reduces all blocks'
+// partials in the same fixed order and one warp solves the 6x6 system, so
+// every block holds the same new pose without a second barrier. Partials
+// alternate between two buffers: a block can only overwrite buffer i%2 after
+// the barrier of iteration i+1, which every block reaches only after reading it.
 __global__ void __launch_bounds__(kFusedThreads, 1)
     k_icp_fused(IcpPlan plan, double *pose, IcpWorkspace *ws, of_icp_stats_t *stats) {
   extern __shared__ float4 s_pts[];  // 2 per cached model point
-  __shared__ FusedState S;
-  unsigned barriers = 0;
-  fused_start(ws, S);
-  fused_finish(plan, pose, ws, stats, S, s_pts, &barriers, false);
-}
-
-// The tracker step's raycast (of frame k - 1, at `pose`) and ICP (of frame
-// k) in one cooperative launch; see the section comment.
-template <int STORAGE>
-__global__ void __launch_bounds__(kFusedThreads, 1)
-    k_track_step(IcpPlan plan, RayQueue rays, double *pose, IcpWorkspace *ws,
-                 of_icp_stats_t *stats) {
-  extern __shared__ float4 s_pts[];
-  __shared__ FusedState S;
-  __shared__ RaySetup setup;
-  unsigned barriers = 0;
-  if (threadIdx.x == 0) ray_setup(pose, rays.desc, &setup);
-  fused_start(ws, S);  // (its block barriers publish the setup)
-  // a plain frame's coarse levels run on the group as soon as the coarse
-  // rays are written, beside the other blocks' rays
-  const bool group = plan.group > 0 && S.warm == 0 && plan.levels > 1;
-  const bool member = group && (int)blockIdx.x < plan.group;
-  ray_chunks<STORAGE>(rays, setup, ws, member);
-  if (member) {
-    __syncthreads();
+  __shared__ double s_pose[16];
+  __shared__ Rigid s_c2w, s_w2c;
+  __shared__ float s_red[kFusedThreads / 32][32];
+  __shared__ float s_tot[32];
+  __shared__ int s_warp_n[kFusedThreads / 32];
+  __shared__ int s_stop, s_inl, s_its, s_err, s_npts, s_conv, s_warm, s_examined;
+  __shared__ double s_res, s_piv;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kWarps = kFusedThreads / 32;
+  // pass 0 starts from the warm start when this frame has one, else from the
+  // frame's starting pose (ws->pose_init: the begin step's, with any prior
+  // applied); pass 1, from the starting pose, runs only when the judge
+  // replaces the warm-started result
+  const bool warm = ws->has_warm != 0;
+  const unsigned epoch = ws->epoch;
+  if (threadIdx.x < 16)
+    s_pose[threadIdx.x] = warm ? ws->warm_pose[threadIdx.x] : ws->pose_init[threadIdx.x];
+  if (threadIdx.x == 0) {
+    s_stop = 0; s_err = 0; s_its = 0; s_inl = 0; s_res = 0.0; s_piv = 0.0; s_examined = 0;
+    s_warm = warm ? 1 : 0;
+  }
+  __syncthreads();  // every thread reads the flags and the pose below
+  if (threadIdx.x == 0) pose_to_rigid(s_pose, &s_c2w, &s_w2c);
+  // the fault-injection hook holds every exchange for an arrival that never
+  // comes
+  const bool hold = ws->hold_barrier > 0;
+  const float dist2 = plan.dist_thresh * plan.dist_thresh, nthr = plan.normal_thresh;
+  int iter_global = 0;
+  for (int pass = 0; pass < 2; ++pass) {
+    const int top = (pass == 0 && warm) ? plan.warm_levels - 1 : plan.levels - 1;
+    for (int l = top; l >= 0 && !s_stop && !s_err; --l) {
+      const IcpLevel L = plan.lv[l];
+      const int npx = L.mw * L.mh;
+      // model pixels are dealt to blocks in chunks of 32 (one warp), round
+      // robin, so every block gets an even, spatially spread share: chunk
+      // c_k = block + k * grid, k = 0 .. my_chunks - 1; the first kc chunks
+      // are kept in shared memory, the rest is read at every iteration
+      const int G = (int)gridDim.x;
+      const int nchunks = (npx + 31) >> 5;
+      const int my_chunks = nchunks > (int)blockIdx.x ? (nchunks - 1 - (int)blockIdx.x) / G + 1 : 0;
+      const int kc = min(my_chunks, plan.cache_pts >> 5);
+      // ---- cache this block's valid model points of the level, in chunk order
+      if (threadIdx.x == 0) { s_npts = 0; s_conv = 0; }
+      __syncthreads();
+      for (int k0 = 0; k0 < kc; k0 += kWarps) {
+        const int k = k0 + warp;
+        const int p = ((int)blockIdx.x + k * G) * 32 + lane;
+        float4 s = make_float4(0.f, 0.f, 0.f, 0.f), ns = s;
+        bool valid = false;
+        if (k < kc && p < npx) {
+          s = __ldg(L.model + 2 * p);
+          ns = __ldg(L.model + 2 * p + 1);
+          valid = s.w != 0.f && ns.w != 0.f;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, valid);
+        if (lane == 0) s_warp_n[warp] = __popc(m);
+        __syncthreads();
+        int off = s_npts;
+        for (int w = 0; w < warp; ++w) off += s_warp_n[w];
+        if (valid) {
+          const int slot = off + __popc(m & ((1u << lane) - 1u));
+          s_pts[2 * slot] = s;
+          s_pts[2 * slot + 1] = ns;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          int tot = 0;
+          for (int w = 0; w < kWarps; ++w) tot += s_warp_n[w];
+          s_npts += tot;
+        }
+        __syncthreads();
+      }
+      const int n = s_npts;
+      for (int it = 0; it < L.iters; ++it) {
+        float acc[kVals];
+        float examined = 0.f;  // model points that project into the frame
+#pragma unroll
+        for (int v = 0; v < kVals; ++v) acc[v] = 0.f;
+        // cached points, two per step
+        for (int i = threadIdx.x; i < n; i += 2 * kFusedThreads) {
+          const int j = i + kFusedThreads;
+          const int qA = associate(s_w2c, L.cam, s_pts[2 * i]);
+          const int qB = j < n ? associate(s_w2c, L.cam, s_pts[2 * j]) : -1;
+          float4 dA = make_float4(0.f, 0.f, 0.f, 0.f), cA = dA, dB = dA, cB = dA;
+          if (qA >= 0) { dA = __ldg(L.frame + 2 * qA); cA = __ldg(L.frame + 2 * qA + 1); }
+          if (qB >= 0) { dB = __ldg(L.frame + 2 * qB); cB = __ldg(L.frame + 2 * qB + 1); }
+          // the model points are read again from shared memory rather than
+          // held in registers across the gathers
+          asm volatile("" ::: "memory");
+          if (qA >= 0) {
+            examined += 1.f;
+            try_row(acc, s_c2w, s_pts[2 * i], s_pts[2 * i + 1], dA, cA, dist2, nthr);
+          }
+          if (qB >= 0) {
+            examined += 1.f;
+            try_row(acc, s_c2w, s_pts[2 * j], s_pts[2 * j + 1], dB, cB, dist2, nthr);
+          }
+        }
+        // the rest of the block's chunks, from global memory
+        for (int k = kc + warp; k < my_chunks; k += kWarps) {
+          const int p = ((int)blockIdx.x + k * G) * 32 + lane;
+          if (p >= npx) continue;
+          const float4 s = __ldg(L.model + 2 * p);
+          const float4 ns = __ldg(L.model + 2 * p + 1);
+          if (s.w == 0.f || ns.w == 0.f) continue;
+          const int q = associate(s_w2c, L.cam, s);
+          if (q < 0) continue;
+          examined += 1.f;
+          try_row(acc, s_c2w, s, ns, __ldg(L.frame + 2 * q), __ldg(L.frame + 2 * q + 1), dist2,
+                  nthr);
+        }
+        // pairwise sums: a recursive-halving exchange across the warp (lanes
+        // trade half of their remaining values each step, 31 shuffles for 32
+        // values) leaves lane v with the warp's sum of value v; then a tree
+        // over the block's warps. Value kVals is the examined-point count. A
+        // warp that examined no point (the coarse levels leave most warps
+        // idle) holds only +0 and writes its zeros directly.
+        if (!__any_sync(0xffffffffu, examined > 0.f)) {
+          s_red[warp][lane] = 0.f;
+        } else {
+          float r[32];
+#pragma unroll
+          for (int v = 0; v < 32; ++v) r[v] = v < kVals ? acc[v] : (v == kVals ? examined : 0.f);
+#pragma unroll
+          for (int sft = 16; sft >= 1; sft >>= 1) {
+            const bool upper = (lane & sft) != 0;
+#pragma unroll
+            for (int i = 0; i < sft; ++i) {
+              float send = upper ? r[i] : r[i + sft];
+              float keep = upper ? r[i + sft] : r[i];
+              r[i] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
+            }
+          }
+          s_red[warp][lane] = r[0];
+        }
+        __syncthreads();
+        const int buf = iter_global & 1;
+        const unsigned seq = (epoch << kIterBits) | (unsigned)(iter_global + 1);
+        if (warp == 0) {
+          float y[kWarps];
+#pragma unroll
+          for (int w = 0; w < kWarps; ++w) y[w] = s_red[w][lane];
+#pragma unroll
+          for (int span = 1; span < kWarps; span *= 2)
+#pragma unroll
+            for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
+          // publish: each value with this iteration's sequence number in one
+          // 64-bit store (no fence: a slot validates itself)
+          if (lane <= kVals)
+            st_relaxed_gpu(&ws->fused_rows[buf][blockIdx.x][lane],
+                           (unsigned long long)__float_as_uint(y[0]) |
+                               ((unsigned long long)seq << 32));
+          // the fault-injection hook: an arrival that never comes
+          if (hold && lane == 0 && !wait_seq(ws, &ws->bar_gen, 0xffffffffu)) {
+            atomicExch(&ws->error, 1);
+            s_err = 1;
+          }
+        }
+        // every block: wait for each block's row of this iteration, then
+        // Kahan over its strided share of the rows and a tree over the
+        // groups, in a fixed order. Seeing every slot of this iteration is
+        // this iteration's grid barrier. Lane v of warp g reads value v of
+        // rows g, g + 32, ...; a round re-reads only the slots not yet seen.
+        {
+          constexpr int kPer = (kFusedMaxBlocks + kWarps - 1) / kWarps;
+          const int v = lane, grp = warp;
+          float vals[kPer];
+          unsigned pending = 0;
+#pragma unroll
+          for (int q = 0; q < kPer; ++q) {
+            vals[q] = 0.f;
+            if (v <= kVals && grp + q * kWarps < (int)gridDim.x) pending |= 1u << q;
+          }
+          unsigned spins = 0;
+          for (;;) {
+#pragma unroll
+            for (int q = 0; q < kPer; ++q) {
+              if (!((pending >> q) & 1u)) continue;
+              const unsigned long long w =
+                  ld_relaxed_gpu(&ws->fused_rows[buf][grp + q * kWarps][v]);
+              if ((unsigned)(w >> 32) == seq) {
+                vals[q] = __uint_as_float((unsigned)w);
+                pending &= ~(1u << q);
+              }
+            }
+            if (__all_sync(0xffffffffu, pending == 0u)) break;
+            if (++spins > kSpinLimit ||
+                ((spins & 255u) == 0u && ld_acquire_gpu(reinterpret_cast<unsigned *>(&ws->error)))) {
+              if (lane == 0) {
+                atomicExch(&ws->error, 1);
+                s_err = 1;
+              }
+              break;
+            }
+            __nanosleep(32);
+          }
+          float sum = 0.f, c = 0.f;
+#pragma unroll
+          for (int q = 0; q < kPer; ++q) {
+            float y = vals[q] - c;
+            float t = sum + y;
+            c = (t - sum) - y;
+            sum = t;
+          }
+          s_red[grp][v] = sum - c;
+        }
+        // a wait that gave up (here or, later, in every other block) ends this
+        // frame's tracking; the final status reads the workspace's flag
+        __syncthreads();
+        if (s_err) break;
+        if (threadIdx.x < 32) {
+          float y[kWarps];
+#pragma unroll
+          for (int w = 0; w < kWarps; ++w) y[w] = s_red[w][threadIdx.x];
+#pragma unroll
+          for (int span = 1; span < kWarps; span *= 2)
+#pragma unroll
+            for (int w = 0; w + span < kWarps; w += 2 * span) y[w] += y[w + span];
+          s_tot[threadIdx.x] = y[0];
+          __syncwarp();
+          double minpiv = 0.0;
+          float inc_rot = 0.f, inc_trans = 0.f;
+          // (on success the warp also writes the new pose's rigid transforms)
+          const bool ok =
+              warp_solve_update(s_tot, s_pose, &minpiv, &inc_rot, &inc_trans, &s_c2w, &s_w2c);
+          if (threadIdx.x == 0) {
+            s_its += 1;
+            s_inl = (int)s_tot[28];
+            s_examined = (int)s_tot[kVals];
+            s_res = (double)s_tot[27];
+            s_piv = minpiv;
+            if (!ok) {
+              for (int i = 0; i < 16; ++i) s_pose[i] = ws->pose_init[i];
+              s_stop = 1;
+              pose_to_rigid(s_pose, &s_c2w, &s_w2c);
+            } else if (plan.stop_rot > 0.f && inc_rot < plan.stop_rot &&
+                       inc_trans < plan.stop_trans) {
+              s_conv = 1;  // converged at this level
+            }
+          }
+        }
+        __syncthreads();
+        ++iter_global;
+        if (s_stop || s_conv) break;
+      }
+    }
+    // ---- judge a warm-started result; replace it by plain ICP if it fails
+    if (pass == 1 || !warm || s_err) break;
     if (threadIdx.x == 0) {
-      const unsigned ncc = (unsigned)((rays.w1 * rays.h1 + 31) / 32);
-      if (!wait_count(ws, &ws->coarse_done, ncc)) S.err = 1;
+      const bool keep = !s_stop && judge_keep(plan, ws->warm_pose, s_pose, s_res, s_inl, s_examined);
+      s_warm = keep ? 1 : 2;
+      if (!keep) {
+        s_stop = 0;
+        for (int i = 0; i < 16; ++i) s_pose[i] = ws->pose_init[i];
+        pose_to_rigid(s_pose, &s_c2w, &s_w2c);
+      }
     }
     __syncthreads();
-    const unsigned epoch = ws->epoch;
-    const bool hold = ws->hold_barrier > 0;
-    for (int l = plan.levels - 1; l >= 1 && !S.stop && !S.err; --l)
-      icp_level(plan, l, plan.group, ws, S, s_pts, hold, epoch);
-    put_group_state(ws, S);
-    ray_chunks<STORAGE>(rays, setup, ws, false);
+    if (s_warm == 1) break;
   }
-  // every ray written before any block caches a level's model points (a
-  // grouped pass has its own barrier, which also hands over the group state)
-  if (!group) grid_barrier(ws, ++barriers, S);
-  fused_finish(plan, pose, ws, stats, S, s_pts, &barriers, group);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    int err = *((volatile int *)&ws->error);
+    for (int i = 0; i < 16; ++i) pose[i] = err ? ws->pose_init[i] : s_pose[i];
+    if (plan.hist) {
+      const unsigned long long c = *plan.hist_count;
+      double *dst = plan.hist + (size_t)(c % (unsigned long long)plan.hist_cap) * 16;
+      for (int i = 0; i < 16; ++i) dst[i] = err ? ws->pose_init[i] : s_pose[i];
+      *plan.hist_count = c + 1;
+    }
+    ws->iterations = s_its;
+    if (stats) {
+      stats->status = err ? 2 : (s_stop ? 1 : 0);
+      stats->inliers = s_inl;
+      stats->iterations = s_its;
+      stats->warm = warm ? s_warm : 0;
+      stats->residual_sq = s_res;
+      stats->min_pivot = s_piv;
+    }
+  }
 }
 
 // Start of a frame's tracking: the starting pose (with the optional prior
 // increment applied; the caller's pose buffer is left as it is until the
 // result is written), the optional warm start (`warm`, a device FP64 pose),
-// cleared flags and counters.
+// cleared flags. It reads only the pose of the previous frame, so a tracker
+// step runs it on a graph branch beside the fusion.
 __global__ void k_icp_begin(double *pose, IcpWorkspace *ws, of_icp_stats_t *stats,
                             const double *warm) {
   // a new epoch: no slot carries this frame's sequence numbers yet. Slots are
@@ -1116,8 +898,6 @@ __global__ void k_icp_begin(double *pose, IcpWorkspace *ws, of_icp_stats_t *stat
   ws->iterations = 0;
   ws->error = 0;
   ws->bar_count = 0;
-  ws->ray_next = 0;
-  ws->coarse_done = 0;
   if (stats) {
     stats->status = 0;
     stats->inliers = 0;
@@ -1175,19 +955,16 @@ static bool icp_params_ok(const of_icp_params_t *p) {
   return p->dist_thresh_mm > 0.f;
 }
 
-// Launch shape of the fused kernels on the current device: every block
-// co-resident (cooperative launch), the coarse levels on a group of
-// kGroupBlocks blocks, and room in shared memory for a block's slice of any
-// level's model points (up to kMaxCachePts). k_icp_fused and k_track_step
-// get the same shape, so their sums run in the same order.
+// Launch shape of the fused kernel on the current device: every block
+// co-resident (cooperative launch), with room in shared memory for the
+// block's slice of the finest level's model points (up to kMaxCachePts).
 constexpr int kMaxCachePts = 6144;  // 192 KiB of points per block
 struct FusedShape {
   int grid;       // co-resident blocks (may exceed kFusedMaxBlocks: then refused)
-  int group;      // blocks of the coarse levels (0: all)
   int cache_pts;
   size_t smem;
 };
-static of_status_t fused_shape(const of_camera_t *cam, int levels, FusedShape *fs) {
+static of_status_t fused_shape(const of_camera_t *cam, FusedShape *fs) {
   constexpr int kMaxDevices = 64;
   static int grid_of[kMaxDevices] = {};
   static std::mutex mu;
@@ -1198,77 +975,23 @@ static of_status_t fused_shape(const of_camera_t *cam, int levels, FusedShape *f
   // The shared-memory opt-in belongs to the function in the current context:
   // it is set on every call (a host-side call), so that a context created
   // after cudaDeviceReset gets it too. The grid depends only on the device.
-  const void *fns[] = {(const void *)k_icp_fused, (const void *)k_track_step<OF_TSDF_I16>,
-                       (const void *)k_track_step<OF_TSDF_F16>};
-  for (const void *f : fns)
-    OF_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  OF_CUDA_TRY(cudaFuncSetAttribute((const void *)k_icp_fused,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
   {
     std::lock_guard<std::mutex> lock(mu);
     if (grid_of[dev] == 0) {
-      int sms = 0, per_sm = 1 << 30;
+      int sms = 0, per_sm = 0;
       OF_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-      for (const void *f : fns) {
-        int n = 0;
-        OF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, kFusedThreads, max_smem));
-        per_sm = n < per_sm ? n : per_sm;
-      }
+      OF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_icp_fused,
+                                                                kFusedThreads, max_smem));
       grid_of[dev] = sms * (per_sm < 1 ? 1 : per_sm);
     }
     fs->grid = grid_of[dev];
   }
-  fs->group = (levels > 1 && fs->grid >= 2 * kGroupBlocks) ? kGroupBlocks : 0;
-  long cache = 32;
-  for (int l = 0; l < levels; ++l) {
-    const of_camera_t cl = camera_level(*cam, l);
-    const long npx = (long)cl.width * cl.height;
-    const long G = (l >= 1 && fs->group) ? fs->group : fs->grid;
-    const long per_block = ((npx + 31) / 32 + G - 1) / G * 32;
-    cache = per_block > cache ? per_block : cache;
-  }
-  fs->cache_pts = (int)(cache < kMaxCachePts ? cache : kMaxCachePts);
+  const long npx = (long)cam->width * cam->height;
+  const long per_block = ((npx + 31) / 32 + fs->grid - 1) / fs->grid * 32;
+  fs->cache_pts = (int)(per_block < kMaxCachePts ? per_block : kMaxCachePts);
   fs->smem = (size_t)fs->cache_pts * 2 * sizeof(float4);
-  return OF_OK;
-}
-
-// The plan and launch shape of a frame's fused launch.
-static of_status_t make_plan(const of_camera_t *cam, const of_icp_params_t *ip, const void *d_frame,
-                             const void *d_model, double *d_hist,
-                             unsigned long long *d_hist_count, int hist_cap, IcpPlan *plan,
-                             FusedShape *fs) {
-  of_pyramid_layout_t lay;
-  of_status_t st = of_pyramid_layout(cam, ip->levels, &lay);
-  if (st != OF_OK) return st;
-  st = fused_shape(cam, ip->levels, fs);
-  if (st != OF_OK) return st;
-  if (fs->grid > kFusedMaxBlocks) return OF_ERR_TOO_LARGE;
-  memset(plan, 0, sizeof(*plan));
-  plan->levels = ip->levels;
-  plan->group = fs->group;
-  plan->cache_pts = fs->cache_pts;
-  plan->dist_thresh = ip->dist_thresh_mm;
-  plan->normal_thresh = ip->normal_thresh;
-  plan->stop_rot = ip->stop_rot_rad;
-  plan->stop_trans = ip->stop_trans_mm;
-  plan->judge_rms = ip->judge_max_rms_mm;
-  plan->judge_frac = ip->judge_min_inlier_frac;
-  plan->judge_rot = ip->judge_max_rot_rad;
-  plan->judge_trans = ip->judge_max_trans_mm;
-  plan->warm_levels = (ip->warm_levels > 0 && ip->warm_levels < ip->levels) ? ip->warm_levels
-                                                                           : ip->levels;
-  if (d_hist && d_hist_count && hist_cap > 0) {
-    plan->hist = d_hist;
-    plan->hist_count = d_hist_count;
-    plan->hist_cap = hist_cap;
-  }
-  for (int l = 0; l < ip->levels; ++l) {
-    of_camera_t cl = camera_level(*cam, l);
-    plan->lv[l].cam = make_cam(cl);
-    plan->lv[l].frame = (const float4 *)((const char *)d_frame + lay.points_offset[l]);
-    plan->lv[l].model = (const float4 *)((const char *)d_model + lay.points_offset[l]);
-    plan->lv[l].mw = cl.width;
-    plan->lv[l].mh = cl.height;
-    plan->lv[l].iters = ip->iters[l];
-  }
   return OF_OK;
 }
 
@@ -1280,80 +1003,78 @@ of_status_t of_icp_begin_launch(double *pose, void *d_ws, of_icp_stats_t *stats,
   return of_launch_status();
 }
 
+// The fused launch of one frame (`begin`: preceded by the begin kernel on
+// the same stream; else a begin launch made elsewhere, e.g. on a tracker
+// step's graph branch, must precede it).
+static of_status_t icp_fused_launch(const of_camera_t *cam, const of_icp_params_t *ip,
+                                    const void *d_frame, const void *d_model, double *pose,
+                                    void *d_ws, of_icp_stats_t *stats, cudaStream_t s,
+                                    const double *d_warm, double *d_hist,
+                                    unsigned long long *d_hist_count, int hist_cap, bool begin) {
+  of_pyramid_layout_t lay;
+  of_status_t st = of_pyramid_layout(cam, ip->levels, &lay);
+  if (st != OF_OK) return st;
+  IcpWorkspace *ws = (IcpWorkspace *)d_ws;
+  FusedShape fs;
+  st = fused_shape(cam, &fs);
+  if (st != OF_OK) return st;
+  if (fs.grid > kFusedMaxBlocks) return OF_ERR_TOO_LARGE;
+  IcpPlan plan;
+  memset(&plan, 0, sizeof(plan));
+  plan.levels = ip->levels;
+  plan.cache_pts = fs.cache_pts;
+  plan.dist_thresh = ip->dist_thresh_mm;
+  plan.normal_thresh = ip->normal_thresh;
+  plan.stop_rot = ip->stop_rot_rad;
+  plan.stop_trans = ip->stop_trans_mm;
+  plan.judge_rms = ip->judge_max_rms_mm;
+  plan.judge_frac = ip->judge_min_inlier_frac;
+  plan.judge_rot = ip->judge_max_rot_rad;
+  plan.judge_trans = ip->judge_max_trans_mm;
+  plan.warm_levels = (ip->warm_levels > 0 && ip->warm_levels < ip->levels) ? ip->warm_levels
+                                                                          : ip->levels;
+  if (d_hist && d_hist_count && hist_cap > 0) {
+    plan.hist = d_hist;
+    plan.hist_count = d_hist_count;
+    plan.hist_cap = hist_cap;
+  }
+  for (int l = 0; l < ip->levels; ++l) {
+    of_camera_t cl = camera_level(*cam, l);
+    plan.lv[l].cam = make_cam(cl);
+    plan.lv[l].frame = (const float4 *)((const char *)d_frame + lay.points_offset[l]);
+    plan.lv[l].model = (const float4 *)((const char *)d_model + lay.points_offset[l]);
+    plan.lv[l].mw = cl.width;
+    plan.lv[l].mh = cl.height;
+    plan.lv[l].iters = ip->iters[l];
+  }
+  if (begin) {
+    st = of_icp_begin_launch(pose, ws, stats, d_warm, s);
+    if (st != OF_OK) return st;
+  }
+  void *args[] = {&plan, &pose, &ws, &stats};
+  OF_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)k_icp_fused, dim3(fs.grid),
+                                          dim3(kFusedThreads), args, fs.smem, s));
+  return OF_OK;
+}
+
 // Launches the whole coarse-to-fine ICP of one frame: a begin kernel and one
 // cooperative launch of the fused kernel.
 of_status_t of_icp_launch(const of_camera_t *cam, const of_icp_params_t *ip, const void *d_frame,
                           const void *d_model, double *pose, void *d_ws, of_icp_stats_t *stats,
                           cudaStream_t s, const double *d_warm, double *d_hist,
                           unsigned long long *d_hist_count, int hist_cap) {
-  IcpPlan plan;
-  FusedShape fs;
-  of_status_t st = make_plan(cam, ip, d_frame, d_model, d_hist, d_hist_count, hist_cap, &plan, &fs);
-  if (st != OF_OK) return st;
-  st = of_icp_begin_launch(pose, d_ws, stats, d_warm, s);
-  if (st != OF_OK) return st;
-  IcpWorkspace *ws = (IcpWorkspace *)d_ws;
-  void *args[] = {&plan, &pose, &ws, &stats};
-  OF_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)k_icp_fused, dim3(fs.grid),
-                                          dim3(kFusedThreads), args, fs.smem, s));
-  return OF_OK;
+  return icp_fused_launch(cam, ip, d_frame, d_model, pose, d_ws, stats, s, d_warm, d_hist,
+                          d_hist_count, hist_cap, true);
 }
 
-// The fused launch alone, after a begin launch made elsewhere (the tracker's
-// branches).
+// The fused launch alone, after the frame's begin launch (made on a tracker
+// step's graph branch).
 of_status_t of_icp_fused_launch(const of_camera_t *cam, const of_icp_params_t *ip,
                                 const void *d_frame, const void *d_model, double *pose, void *d_ws,
                                 of_icp_stats_t *stats, cudaStream_t s, double *d_hist,
                                 unsigned long long *d_hist_count, int hist_cap) {
-  IcpPlan plan;
-  FusedShape fs;
-  of_status_t st = make_plan(cam, ip, d_frame, d_model, d_hist, d_hist_count, hist_cap, &plan, &fs);
-  if (st != OF_OK) return st;
-  IcpWorkspace *ws = (IcpWorkspace *)d_ws;
-  void *args[] = {&plan, &pose, &ws, &stats};
-  OF_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)k_icp_fused, dim3(fs.grid),
-                                          dim3(kFusedThreads), args, fs.smem, s));
-  return OF_OK;
-}
-
-// A tracker step's raycast of the model at `pose` (into `d_model`, every
-// level) and the frame's ICP in one cooperative launch (k_track_step). The
-// frame's begin launch (of_icp_begin_launch) must precede it.
-of_status_t of_track_step_launch(const of_volume_desc_t *vd, const void *vol,
-                                 const of_camera_t *cam, const of_raycast_params_t *rp,
-                                 const of_icp_params_t *ip, const void *d_frame, void *d_model,
-                                 double *pose, void *d_ws, of_icp_stats_t *stats, cudaStream_t s,
-                                 double *d_hist, unsigned long long *d_hist_count, int hist_cap) {
-  if (!rp || rp->min_step_vox <= 0.f || rp->far_step_frac < 0.f || rp->refine_iters < 0 ||
-      rp->refine_iters > 16)
-    return OF_ERR_INVALID_ARGUMENT;
-  IcpPlan plan;
-  FusedShape fs;
-  of_status_t st = make_plan(cam, ip, d_frame, d_model, d_hist, d_hist_count, hist_cap, &plan, &fs);
-  if (st != OF_OK) return st;
-  of_pyramid_layout_t lay;
-  st = of_pyramid_layout(cam, ip->levels, &lay);
-  if (st != OF_OK) return st;
-  RayQueue rq;
-  memset(&rq, 0, sizeof(rq));
-  rq.vol = (const uint32_t *)vol;
-  rq.desc = *vd;
-  rq.cam = make_cam(*cam);
-  rq.rp = *rp;
-  rq.pts = (float4 *)((char *)d_model + lay.points_offset[0]);
-  rq.coarse.levels = ip->levels;
-  for (int l = 0; l < ip->levels; ++l) {
-    rq.coarse.pts[l] = (float4 *)((char *)d_model + lay.points_offset[l]);
-    rq.coarse.w[l] = lay.width[l];
-  }
-  rq.w1 = (cam->width + 1) / 2;
-  rq.h1 = (cam->height + 1) / 2;
-  IcpWorkspace *ws = (IcpWorkspace *)d_ws;
-  void *args[] = {&plan, &rq, &pose, &ws, &stats};
-  const void *fn = vd->storage == OF_TSDF_I16 ? (const void *)k_track_step<OF_TSDF_I16>
-                                              : (const void *)k_track_step<OF_TSDF_F16>;
-  OF_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(fs.grid), dim3(kFusedThreads), args, fs.smem, s));
-  return OF_OK;
+  return icp_fused_launch(cam, ip, d_frame, d_model, pose, d_ws, stats, s, nullptr, d_hist,
+                          d_hist_count, hist_cap, false);
 }
 
 extern "C" of_status_t of_icp_track(const of_camera_t *cam, const of_icp_params_t *ip,
@@ -1473,7 +1194,7 @@ extern "C" of_status_t of_icp_track_static(const of_camera_t *cam, const of_icp_
   // the array holds partials for kFusedMaxBlocks blocks: a device whose
   // co-resident grid would need more is refused
   FusedShape fs;
-  of_status_t sh = fused_shape(cam, ip->levels, &fs);
+  of_status_t sh = fused_shape(cam, &fs);
   if (sh != OF_OK) return sh;
   if (fs.grid > kFusedMaxBlocks) return OF_ERR_TOO_LARGE;
   void *ws = nullptr;

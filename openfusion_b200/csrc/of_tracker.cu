@@ -35,11 +35,7 @@ of_status_t of_icp_fused_launch(const of_camera_t *cam, const of_icp_params_t *i
                                 const void *d_frame, const void *d_model, double *pose, void *d_ws,
                                 of_icp_stats_t *stats, cudaStream_t s, double *d_hist,
                                 unsigned long long *d_hist_count, int hist_cap);
-of_status_t of_track_step_launch(const of_volume_desc_t *vd, const void *vol,
-                                 const of_camera_t *cam, const of_raycast_params_t *rp,
-                                 const of_icp_params_t *ip, const void *d_frame, void *d_model,
-                                 double *pose, void *d_ws, of_icp_stats_t *stats, cudaStream_t s,
-                                 double *d_hist, unsigned long long *d_hist_count, int hist_cap);
+
 
 struct of_tracker {
   of_tracker_desc_t desc;
@@ -73,8 +69,7 @@ struct of_tracker {
   bool last_fused = false;  // of_tracker_flush fused the last frame already
   int kernels_first = 0;
   int kernels_track = 0;
-  bool tuned = false;    // desc.tune: the online tuning has run
-  bool combined = true;  // raycast and ICP of a step in one launch (else desc.raycast.tile)
+  bool tuned = false;  // desc.tune: the online tuning has run
   cudaGraphExec_t g_first = nullptr;
   cudaGraphExec_t g_track[2] = {nullptr, nullptr};
 };
@@ -115,13 +110,12 @@ of_status_t enqueue_fuse(of_tracker *t, const uint16_t *depth, cudaStream_t s) {
                     nullptr, s);
 }
 
-// The step of frame k >= 1 (depth[cur]): integrate(k-1) on `s`, beside
-// pre-process(k) and the CNN(k-1, k) on their branches, each branch closed by
-// the frame's ICP start (the begin kernel: after the CNN when it predicts the
-// warm start, else after pre-processing); after the join one launch raycasts
-// the model of frame k-1 and tracks frame k (of_track_step_launch). `fuse` =
-// false when of_tracker_flush fused and raycast frame k-1 already: then the
-// join is followed by the ICP launch alone.
+// The step of frame k >= 1 (depth[cur]): integrate(k-1) -> raycast(k-1) on
+// `s`, beside pre-process(k) and the CNN(k-1, k) on their branches, each
+// branch closed by the frame's ICP start (the begin kernel, which reads only
+// the previous pose: after the CNN when it predicts the warm start, else
+// after pre-processing); ICP(k) after the join. `fuse` = false when
+// of_tracker_flush fused frame k-1.
 of_status_t enqueue_track(of_tracker *t, int cur, bool fuse, cudaStream_t s) {
   const of_tracker_desc_t &d = t->desc;
   const uint16_t *now = t->depth[cur], *before = t->depth[cur ^ 1];
@@ -152,12 +146,7 @@ of_status_t enqueue_track(of_tracker *t, int cur, bool fuse, cudaStream_t s) {
       sb = of_icp_begin_launch(t->pose, t->icp_ws, t->stats, nullptr, t->pre);
     pre_recorded = ok(cudaEventRecord(t->ev_pre, t->pre));
   }
-  of_status_t sf = OF_OK;
-  if (fuse && t->combined)
-    sf = of_integrate_tiled(&d.volume, t->volume, &d.camera, before, d.camera.width, t->pose,
-                            t->lambda, t->scratch, s);
-  else if (fuse)
-    sf = enqueue_fuse(t, before, s);
+  of_status_t sf = fuse ? enqueue_fuse(t, before, s) : OF_OK;
   if (pre_recorded) ok(cudaStreamWaitEvent(s, t->ev_pre, 0));
   if (cnn_recorded) ok(cudaStreamWaitEvent(s, t->ev_cnn, 0));
   if (first != cudaSuccess) return of_set_cuda_error(first);
@@ -166,12 +155,8 @@ of_status_t enqueue_track(of_tracker *t, int cur, bool fuse, cudaStream_t s) {
   if (sb != OF_OK) return sb;
   if (sf != OF_OK) return sf;
   // the ICP kernel appends the frame's pose to the history itself
-  if (!fuse || !t->combined)
-    return of_icp_fused_launch(&d.camera, &d.icp, t->frame, t->model, t->pose, t->icp_ws, t->stats,
-                               s, t->hist, t->hist_count, t->hist_cap);
-  return of_track_step_launch(&d.volume, t->volume, &d.camera, &d.raycast, &d.icp, t->frame,
-                              t->model, t->pose, t->icp_ws, t->stats, s, t->hist, t->hist_count,
-                              t->hist_cap);
+  return of_icp_fused_launch(&d.camera, &d.icp, t->frame, t->model, t->pose, t->icp_ws, t->stats,
+                             s, t->hist, t->hist_count, t->hist_cap);
 }
 
 int count_kernel_nodes(cudaGraph_t g) {
@@ -206,52 +191,33 @@ of_status_t capture(of_tracker *t, int cur, cudaGraphExec_t *out) {
   return OF_OK;
 }
 
-// The online tuning (desc.tune) of the step shape, which changes no result:
-// the raycast of the volume as this step left it as its own launch with each
-// of the four block shapes followed by the ICP launch, or both in one launch
-// (of_track_step_launch). Each candidate runs twice, at the tracked pose,
-// into scratch buffers (model, pose, ICP workspace; the tracker's state is
-// left alone), timed with CUDA events on `s`; the fastest run wins. Then the
-// step graphs are captured with the winner.
-constexpr int kTuneCands = 5;  // tiles 0..3 with separate launches, then the combined launch
+// The online tuning (desc.tune): every raycast block shape, twice each, on
+// the volume as this step left it, at the tracked pose, into a scratch
+// pyramid (the tracker's model is left alone); CUDA events on `s`, the
+// fastest run wins. Then the step graphs are captured with the winner.
+constexpr int kTuneTiles = 4;
 constexpr int kTuneReps = 2;
 of_status_t tune_shapes(of_tracker *t, cudaStream_t s) {
-  const of_tracker_desc_t &d = t->desc;
-  void *model = nullptr, *ws = nullptr;
-  double *pose = nullptr;
-  of_icp_stats_t *stats = nullptr;
-  cudaEvent_t ev[2 * kTuneCands * kTuneReps] = {};
+  void *tmp = nullptr;
+  cudaEvent_t ev[2 * kTuneTiles * kTuneReps] = {};
   of_status_t st = OF_OK;
-  cudaError_t e = cudaMalloc(&model, t->lay.total_bytes);
-  if (e == cudaSuccess) e = cudaMalloc(&ws, of_icp_workspace_size());
-  if (e == cudaSuccess) e = cudaMalloc((void **)&pose, 16 * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc((void **)&stats, sizeof(of_icp_stats_t));
-  if (e == cudaSuccess) e = cudaMemsetAsync(ws, 0, of_icp_workspace_size(), s);
-  for (int i = 0; e == cudaSuccess && i < 2 * kTuneCands * kTuneReps; ++i) e = cudaEventCreate(&ev[i]);
-  for (int c = 0; c < kTuneCands && e == cudaSuccess && st == OF_OK; ++c)
+  cudaError_t e = cudaMalloc(&tmp, t->lay.total_bytes);
+  for (int i = 0; e == cudaSuccess && i < 2 * kTuneTiles * kTuneReps; ++i) e = cudaEventCreate(&ev[i]);
+  for (int c = 0; c < kTuneTiles && e == cudaSuccess && st == OF_OK; ++c)
     for (int r = 0; r < kTuneReps && e == cudaSuccess && st == OF_OK; ++r) {
       const int i = 2 * (c * kTuneReps + r);
-      e = cudaMemcpyAsync(pose, t->pose, 16 * sizeof(double), cudaMemcpyDeviceToDevice, s);
-      if (e == cudaSuccess) e = cudaEventRecord(ev[i], s);
-      if (e != cudaSuccess) break;
-      st = of_icp_begin_launch(pose, ws, stats, nullptr, s);
-      if (st == OF_OK && c < 4) {
-        of_raycast_params_t rp = d.raycast;
-        rp.tile = c;
-        st = of_raycast(&d.volume, t->volume, &d.camera, &rp, d.icp.levels, pose, model, nullptr, s);
-        if (st == OF_OK)
-          st = of_icp_fused_launch(&d.camera, &d.icp, t->frame, model, pose, ws, stats, s, nullptr,
-                                   nullptr, 0);
-      } else if (st == OF_OK) {
-        st = of_track_step_launch(&d.volume, t->volume, &d.camera, &d.raycast, &d.icp, t->frame,
-                                  model, pose, ws, stats, s, nullptr, nullptr, 0);
-      }
-      if (st == OF_OK) e = cudaEventRecord(ev[i + 1], s);
+      of_raycast_params_t rp = t->desc.raycast;
+      rp.tile = c;
+      e = cudaEventRecord(ev[i], s);
+      if (e == cudaSuccess)
+        st = of_raycast(&t->desc.volume, t->volume, &t->desc.camera, &rp, t->desc.icp.levels,
+                        t->pose, tmp, nullptr, s);
+      if (e == cudaSuccess && st == OF_OK) e = cudaEventRecord(ev[i + 1], s);
     }
   if (e == cudaSuccess && st == OF_OK) e = cudaStreamSynchronize(s);
-  int best = -1;
+  int best = t->desc.raycast.tile;
   float best_ms = 1e30f;
-  for (int c = 0; c < kTuneCands && e == cudaSuccess && st == OF_OK; ++c)
+  for (int c = 0; c < kTuneTiles && e == cudaSuccess && st == OF_OK; ++c)
     for (int r = 0; r < kTuneReps && e == cudaSuccess; ++r) {
       float ms = 0.f;
       const int i = 2 * (c * kTuneReps + r);
@@ -260,12 +226,10 @@ of_status_t tune_shapes(of_tracker *t, cudaStream_t s) {
     }
   for (cudaEvent_t x : ev)
     if (x) cudaEventDestroy(x);
-  for (void *b : {model, ws, (void *)pose, (void *)stats})
-    if (b) cudaFree(b);
+  if (tmp) cudaFree(tmp);
   if (st != OF_OK) return st;
   if (e != cudaSuccess) return of_set_cuda_error(e);
-  t->combined = best == 4;
-  if (best >= 0 && best < 4) t->desc.raycast.tile = best;
+  t->desc.raycast.tile = best;
   t->tuned = true;
   if (t->desc.use_graph) {
     st = capture(t, 0, &t->g_track[0]);
@@ -463,10 +427,8 @@ extern "C" of_status_t of_tracker_pose_history(of_tracker_t t, double *poses, in
   return OF_OK;
 }
 
-extern "C" of_status_t of_tracker_tuning(of_tracker_t t, int32_t *combined, int32_t *ray_tile,
-                                         int32_t *tuned) {
-  if (!t || !combined || !ray_tile || !tuned) return OF_ERR_INVALID_ARGUMENT;
-  *combined = t->combined ? 1 : 0;
+extern "C" of_status_t of_tracker_tuning(of_tracker_t t, int32_t *ray_tile, int32_t *tuned) {
+  if (!t || !ray_tile || !tuned) return OF_ERR_INVALID_ARGUMENT;
   *ray_tile = t->desc.raycast.tile;
   *tuned = t->tuned ? 1 : 0;
   return OF_OK;
