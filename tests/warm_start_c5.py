@@ -3,7 +3,7 @@ oracle (large-motion workload: 640x480, 512^3 over 3 m, inter-frame motion
 U[0, 10] cm / U[0, 5] deg).
 
     python tests/warm_start_c5.py [--seeds 910000 910001 910002] [--frames 121]
-                                  [--out results.json]
+                                  [--out results.json] [--weights file.npy]
 
 Both arms run through the tracker (one CUDA graph per frame) with the same
 early exit. After every frame the tracker's own ICP inputs are read back --
@@ -135,13 +135,13 @@ def summarise(recs):
     return out
 
 
-def run(seeds, frames, dev, timed=True, log=None):
+def run(seeds, frames, dev, timed=True, log=None, weights_path=None):
     import openfusion_b200 as of
     from openfusion_b200 import learned
     from openfusion_b200.train_warm_start import eval_config
     from oracle import Oracle
     ora = Oracle("f64")
-    weights = learned.load_weights()
+    weights = learned.load_weights(weights_path)
     res = {"workload": "c5: 640x480, 512^3 over 3 m, motion U[0,10] cm / U[0,5] deg per frame",
            "seeds": list(seeds), "frames_per_seed": frames - 1}
     cfg0 = eval_config(of)
@@ -189,10 +189,13 @@ def main():
     ap.add_argument("--seeds", type=int, nargs="+", default=[910000, 910001, 910002])
     ap.add_argument("--frames", type=int, default=121)
     ap.add_argument("--out", type=Path, default=None)
+    ap.add_argument("--weights", type=Path, default=None,
+                    help="warm-start CNN weights (default: the committed ones)")
     a = ap.parse_args()
     import torch
     dev = torch.device("cuda:0")
-    res = run(a.seeds, a.frames, dev, log=lambda m: print(m, file=sys.stderr, flush=True))
+    res = run(a.seeds, a.frames, dev, log=lambda m: print(m, file=sys.stderr, flush=True),
+              weights_path=a.weights)
     line = json.dumps(res)
     if a.out:
         a.out.parent.mkdir(parents=True, exist_ok=True)
