@@ -567,6 +567,21 @@ def warm_start_comparison(of, args, dev, world, rank):
         if arm == "warm":
             out[arm]["warm_start_kept_frac"] = float(np.mean(kept == 1))
     out["warm_over_plain_frames_per_s"] = out["warm"]["frames_per_s"] / out["plain"]["frames_per_s"]
+    # the per-frame FP64 oracle comparison of both arms is a test run
+    # (tests/warm_start_c5.py); its recorded summary is carried here, labelled
+    rec = ROOT / "profiles" / "warm_start_c5_oracle_study.json"
+    if rec.exists():
+        st = json.loads(rec.read_text())
+        out["oracle_study_recorded"] = {
+            "source": str(rec.relative_to(ROOT)), "command": st["command"],
+            "seeds": st["seeds"], "frames_per_seed": st["frames_per_seed"],
+            "bar": st["equal_error"]["bar"],
+            "plain_within": st["equal_error"]["plain_within"],
+            "warm_within": st["equal_error"]["warm_within"],
+            **{f"{arm}_max_{k}_vs_fp64_oracle": st[arm][f"max_{k}_vs_full_oracle"]
+               for arm in ("plain", "warm") for k in ("rot_rad", "trans_mm")},
+            "warm_over_plain_frames_per_s": st["warm_over_plain_frames_per_s"],
+            "note": "recorded by the oracle study, not re-measured by this run"}
     return out
 
 

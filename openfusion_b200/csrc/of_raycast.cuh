@@ -1,6 +1,5 @@
 // of_raycast.cuh -- the per-ray device code of the raycast, shared by the
-// raycast launches (of_raycast.cu) and the combined raycast + ICP launch of a
-// tracker step (of_icp.cu).
+// single-stream and the batched raycast launches (of_raycast.cu).
 //
 // Follows d_raycast (Source/src/Raycaster.cu:97-230): one ray per pixel from
 // the camera position through the pixel's point at z = -1 in camera space

@@ -407,6 +407,55 @@ static R trilinear(const vol_view *V, R px, R py, R pz) {
   return c0 + f[0] * (c1 - c0);
 }
 
+/* The surface of a + -> - bracket [t, tn] (f(t) = fp > 0 >= f(tn) = fn) along
+ * o + t dir: the bracket is narrowed to one min_step by stepping from its
+ * positive end, then `iters` Illinois regula-falsi steps (Dowell & Jarratt
+ * 1971) refine it; returns the final secant point. */
+static R refine_root(const vol_view *V, const R *o, const R *dir, R t, R fp, R tn, R fn,
+                     R min_step, int iters) {
+  R ta = t, fa = fp, tb = tn, fb = fn;
+  while (tb - ta > min_step * (R)1.0001) {
+    R tm = ta + min_step;
+    R fm = trilinear(V, o[0] + tm * dir[0], o[1] + tm * dir[1], o[2] + tm * dir[2]);
+    if (fm > 0) { ta = tm; fa = fm; } else { tb = tm; fb = fm; break; }
+  }
+  int side = 0;
+  for (int r = 0; r < iters; ++r) {
+    R tm = ta + (tb - ta) * (fa / (fa - fb));
+    R fm = trilinear(V, o[0] + tm * dir[0], o[1] + tm * dir[1], o[2] + tm * dir[2]);
+    if (fm > 0) {
+      ta = tm; fa = fm;
+      if (side == 1) fb *= (R)0.5;
+      side = 1;
+    } else {
+      tb = tm; fb = fm;
+      if (side == -1) fa *= (R)0.5;
+      side = -1;
+    }
+  }
+  return ta + (tb - ta) * (fa / (fa - fb));
+}
+
+/* Whether a refined surface depends on where rounding puts the march: the
+ * bracket moved by +-shift (FP32 rounding of a metre-long march reaches a
+ * few micrometres and the tsdf-scaled steps can carry it on) must keep its
+ * sign change and give a surface within `tol` of `ts`. A bracket that holds a
+ * non-monotonic stretch of the field (a ray clipping a thin negative dip, with
+ * its negative end near the dip's far zero crossing) leaves the few Illinois
+ * steps far from converged, and their result then moves with the bracket. */
+static int refine_is_sensitive(const vol_view *V, const R *o, const R *dir, R t, R tn, R ts,
+                               R min_step, int iters, R shift, R tol) {
+  for (int k = -1; k <= 1; k += 2) {
+    const R a = t + (R)k * shift, b = tn + (R)k * shift;
+    const R fa = trilinear(V, o[0] + a * dir[0], o[1] + a * dir[1], o[2] + a * dir[2]);
+    const R fb = trilinear(V, o[0] + b * dir[0], o[1] + b * dir[1], o[2] + b * dir[2]);
+    if (!(fa > 0) || !(fb <= 0)) return 1;
+    const R tp = refine_root(V, o, dir, a, fa, b, fb, min_step, iters);
+    if (fabs((double)(tp - ts)) > (double)tol) return 1;
+  }
+  return 0;
+}
+
 /* Raycast: d_raycast (Source/src/Raycaster.cu:97-230) -- ray from the camera
  * position through the pixel's point at z = -1 (:117-125), slab clip
  * (:35-55) to the box of voxel centres, march to the first surface. The
@@ -420,8 +469,13 @@ static R trilinear(const vol_view *V, R px, R py, R pz) {
  * voxel apart; the march is limited to [dmin, dmax] depth. With `flags` (one
  * byte per 8^3 brick, clear = the brick and its 26 neighbours hold only +1
  * voxels) the march jumps over clear bricks: empty-space skipping, as the
- * CUDA kernel does; it cannot change which crossing is found, only where the
- * samples before it fall. */
+ * CUDA kernel does. Every skipped sample would have read +1, but the samples
+ * after a jump fall elsewhere than a plain march's, so a negative stretch
+ * thinner than one step can be found by one march and stepped over by the
+ * other. `ambig` flags a ray whose skip landing or step ends
+ * within 0.05 mm of the range end, whose march sample lies within 2e-4 of
+ * zero, whose normal's samples touch the box within 0.05 mm, or whose refined
+ * surface is sensitive to rounding (refine_is_sensitive). */
 void ora_raycast(const ora_vol *v, const uint32_t *words, const uint8_t *flags, const ora_cam *c,
                  const ora_params *p, const double *P, R *pts, uint8_t *ambig) {
   const int n = v->n;
@@ -517,29 +571,10 @@ void ora_raycast(const ora_vol *v, const uint32_t *words, const uint8_t *flags, 
           R fn = trilinear(&V, o[0] + tn * dir[0], o[1] + tn * dir[1], o[2] + tn * dir[2]);
           if (ambig && fabs((double)fn) < 2e-4) amb = 1;
           if (fp > 0 && fn <= 0) {
-            R ta = t, fa = fp, tb = tn, fb = fn;
-            /* narrow a long bracket with minimum steps from its positive end */
-            while (tb - ta > min_step * (R)1.0001) {
-              R tm = ta + min_step;
-              R fm = trilinear(&V, o[0] + tm * dir[0], o[1] + tm * dir[1], o[2] + tm * dir[2]);
-              if (fm > 0) { ta = tm; fa = fm; } else { tb = tm; fb = fm; break; }
-            }
-            /* Illinois regula falsi (Dowell & Jarratt 1971) */
-            int side = 0;
-            for (int r = 0; r < p->refine_iters; ++r) {
-              R tm = ta + (tb - ta) * (fa / (fa - fb));
-              R fm = trilinear(&V, o[0] + tm * dir[0], o[1] + tm * dir[1], o[2] + tm * dir[2]);
-              if (fm > 0) {
-                ta = tm; fa = fm;
-                if (side == 1) fb *= (R)0.5;
-                side = 1;
-              } else {
-                tb = tm; fb = fm;
-                if (side == -1) fa *= (R)0.5;
-                side = -1;
-              }
-            }
-            ts = ta + (tb - ta) * (fa / (fa - fb));
+            ts = refine_root(&V, o, dir, t, fp, tn, fn, min_step, p->refine_iters);
+            if (ambig && refine_is_sensitive(&V, o, dir, t, tn, ts, min_step, p->refine_iters,
+                                             (R)0.01, (R)0.02))
+              amb = 1;
             hit = 1;
             break;
           }

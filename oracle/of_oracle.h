@@ -78,7 +78,9 @@ int64_t ora_integrate(const ora_vol *v, uint32_t *words, const ora_cam *c, const
 
 /* raycast; pts is [h*w][8] world vertex/normal; flags (may be NULL): one
  * byte per brick for empty-space skipping; ambig (may be NULL) flags pixels
- * whose sign or range decisions are within rounding of a boundary. */
+ * whose sign or range decisions are within rounding of a boundary, and hits
+ * whose refined surface moves by more than 0.02 mm when the bracket moves by
+ * 0.01 mm (unconverged refinement: the result depends on FP rounding). */
 void ora_raycast(const ora_vol *v, const uint32_t *words, const uint8_t *flags, const ora_cam *c,
                  const ora_params *p, const double *pose, ora_real *pts, uint8_t *ambig);
 /* model level l+1 from level l by subsampling (2x, 2y) */

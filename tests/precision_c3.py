@@ -80,6 +80,8 @@ def check_raycast(cfg, ora, words, flags, pose, gv, gn) -> dict:
     nb = both & (gn[..., 3] > 0) & (opts[..., 7] > 0)
     nerr = np.linalg.norm(gn[..., :3][nb] - opts[..., 4:7][nb], axis=-1)
     return {"hit_frac": float(hit_o.mean()), "hit_mismatch_frac": float((hit_g != hit_o)[ok].mean()),
+            "flagged_frac": float((~ok).mean()),
+            "vertex_err_mm_max": float(verr.max()),
             "vertex_err_mm_q999": float(np.quantile(verr, 0.999)),
             "vertex_err_mm_median": float(np.median(verr)),
             "normal_err_median": float(np.median(nerr))}
@@ -165,6 +167,7 @@ def run_study(frames: int, checkpoints: list[int], log=print) -> dict:
     out["summary"] = {
         "max_tsdf_err_fp16_ulp": max(c["integrate"]["max_tsdf_err_fp16_ulp"] for c in cps),
         "weights_equal": all(c["integrate"]["weights_equal"] for c in cps),
+        "max_vertex_err_mm": max(c["raycast"]["vertex_err_mm_max"] for c in cps),
         "max_vertex_err_mm_q999": max(c["raycast"]["vertex_err_mm_q999"] for c in cps),
         "max_pose_err_rad": max(c["icp"]["rot_err_rad"] for c in cps),
         "max_pose_err_mm": max(c["icp"]["trans_err_mm"] for c in cps),

@@ -7,7 +7,7 @@ boundary (pixel rounding at .5, a depth at the range limit, an SDF at -trunc,
 a tsdf sample at 0) are flagged by the oracle and excluded; their number is
 bounded. Tolerances (from the path's precision targets):
   TSDF      within 1 int16 quantisation step (trunc / 32767)
-  vertices  within 1e-4 m = 0.1 mm
+  vertices  within 1e-4 m = 0.1 mm (every ray the oracle does not flag)
   pose      within 1e-5 rad and 1e-5 m = 0.01 mm
 """
 import numpy as np
@@ -232,9 +232,10 @@ def test_ragged_frame_sizes(of, ora, cuda, size):
     hit_g, hit_o = gv[..., 3] > 0, opts[..., 3] > 0
     assert hit_o.mean() > 0.3, "the scene should be mostly visible"
     assert (hit_g != hit_o)[ok].mean() < 1e-3
+    assert (~ok).mean() < 1e-2
     both = hit_g & hit_o & ok
     verr = np.linalg.norm(gv[..., :3][both] - opts[..., :3][both], axis=-1)
-    assert np.quantile(verr, 0.999) < 0.1, f"vertex err q99.9 {np.quantile(verr, 0.999)} mm"
+    assert verr.max() < 0.1, f"vertex err max {verr.max()} mm"
     for l in range(1, cfg.levels):
         vl, nl = (t.cpu().numpy() for t in of.unpack_points(cfg, model, l))
         s = 1 << l
@@ -295,20 +296,27 @@ def test_raycast_matches_oracle(of, ora, cuda, name, res):
     pad[:nb, :nb, :nb] = flags.reshape(nb, nb, nb)
     assert np.array_equal(sflags != 0, pad.reshape(ns, 4, ns, 4, ns, 4).max(axis=(1, 3, 5)) != 0)
     opts, amb = ora.raycast(cfg, words, pose, ambig=True, flags=flags)
-    # the skip is exact: the oracle without it finds the same surface
+    # Empty-space skipping only moves where the samples after a jump fall:
+    # the oracle without it finds the same surface on all but the rays whose
+    # negative stretch is thinner than one step (found by one march, stepped
+    # over by the other).
     plain, _ = ora.raycast(cfg, words, pose)
     hp = (plain[..., 3] > 0) & (opts[..., 3] > 0)
     assert ((plain[..., 3] > 0) != (opts[..., 3] > 0)).mean() < 5e-3
     dp = np.linalg.norm(plain[..., :3][hp] - opts[..., :3][hp], axis=-1)
     assert np.quantile(dp, 0.99) < 0.1
+    # The GPU against the oracle with the same skipping: every ray that the
+    # oracle does not flag (a decision within rounding of a boundary, or a
+    # refined surface that moves with the bracket) within 0.1 mm.
     gv, gn = (t.cpu().numpy().astype(np.float64) for t in of.unpack_points(cfg, model, 0))
     ok = amb == 0
     hit_g, hit_o = gv[..., 3] > 0, opts[..., 3] > 0
     assert hit_o.mean() > 0.5, "scene should be mostly visible"
+    assert (~ok).mean() < 1e-2
     assert (hit_g != hit_o)[ok].mean() < 1e-3
     both = hit_g & hit_o & ok
     verr = np.linalg.norm(gv[..., :3][both] - opts[..., :3][both], axis=-1)
-    assert np.quantile(verr, 0.999) < 0.1, f"vertex err q99.9 {np.quantile(verr, 0.999)} mm"
+    assert verr.max() < 0.1, f"vertex err max {verr.max()} mm"
     assert np.median(verr) < 0.01
     nb = both & (gn[..., 3] > 0) & (opts[..., 7] > 0)
     nerr = np.linalg.norm(gn[..., :3][nb] - opts[..., 4:7][nb], axis=-1)
