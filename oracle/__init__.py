@@ -88,6 +88,8 @@ class Oracle:
         L.ora_integrate.argtypes = [C.POINTER(Vol), P, C.POINTER(Cam), P, P, P]
         L.ora_integrate.restype = C.c_int64
         L.ora_raycast.argtypes = [C.POINTER(Vol), P, P, C.POINTER(Cam), C.POINTER(Params), P, P, P]
+        L.ora_raycast_pixels.argtypes = [C.POINTER(Vol), P, P, C.POINTER(Cam), C.POINTER(Params), P,
+                                         C.c_int32, P, C.c_int32, P, P]
         L.ora_model_down.argtypes = [P, C.c_int32, P, C.c_int32, C.c_int32]
         L.ora_icp_system.argtypes = [C.POINTER(Cam), P, C.c_int32, C.c_int32, P, P, C.c_double,
                                      C.c_double, P, P]
@@ -224,6 +226,24 @@ class Oracle:
                              C.byref(self.params(cfg)), P_.ctypes.data, pts.ctypes.data,
                              None if am is None else am.ctypes.data)
         return pts, am
+
+    def raycast_pixels(self, cfg, words: np.ndarray, pose: np.ndarray, flags, pixels,
+                       perts) -> np.ndarray:
+        """The march of the given (x, y) pixels with every position update
+        moved by each perturbation (mm); returns [len(pixels), len(perts), 4]
+        vertex + hit flag."""
+        P_ = np.ascontiguousarray(pose, np.float64)
+        xy = np.ascontiguousarray(np.asarray(pixels, np.int32).reshape(-1, 2))
+        pe = np.ascontiguousarray(perts, np.float64)
+        out = np.zeros((len(xy), len(pe), 4), self.real)
+        fl = None if flags is None else np.ascontiguousarray(flags, np.uint8)
+        if len(xy):
+            self.lib.ora_raycast_pixels(C.byref(self.vol(cfg)), words.ctypes.data,
+                                        None if fl is None else fl.ctypes.data,
+                                        C.byref(self.cam(cfg)), C.byref(self.params(cfg)),
+                                        P_.ctypes.data, len(xy), xy.ctypes.data, len(pe),
+                                        pe.ctypes.data, out.ctypes.data)
+        return out
 
     @staticmethod
     def shade_rgba(cfg, pose: np.ndarray, normals: np.ndarray) -> np.ndarray:

@@ -456,6 +456,90 @@ static int refine_is_sensitive(const vol_view *V, const R *o, const R *dir, R t,
   return 0;
 }
 
+/* What a ray's march needs besides the ray. */
+typedef struct {
+  const vol_view *V;
+  const uint8_t *flags, *sflags;  /* brick / super-brick flags (NULL: no skipping) */
+  int n, nbk, ns;
+  double vs;
+  R min_step, far_k;
+  int refine_iters;
+} march_ctx;
+
+/* The march of one ray over [t0, t1] (see ora_raycast); returns whether it
+ * hit, with the refined surface in *ts. `pert` is added to every position
+ * update (each step's end and each skip's landing): 0 for the method itself,
+ * a small shift to test whether the result depends on rounding. With `amb`,
+ * decisions within rounding of a boundary set *amb. */
+static int march_ray(const march_ctx *M, const R *o, const R *dir, R t0, R t1, R pert, R *ts,
+                     int *amb) {
+  const vol_view *V = M->V;
+  const int n = M->n, nbk = M->nbk, ns = M->ns;
+  const double vs = M->vs;
+  const R min_step = M->min_step, far_k = M->far_k;
+  if (!(t0 < t1)) return 0;
+  R t = t0;
+  R fp = 1;
+  int sampled = 0;
+  for (int it = 0; it < (1 << 16); ++it) {
+    R px = o[0] + t * dir[0], py = o[1] + t * dir[1], pz = o[2] + t * dir[2];
+    if (M->flags) {
+      /* empty-space skip: a brick whose flag is clear holds, with its 26
+       * neighbours, only +1 voxels; every sample whose cell base is in it
+       * reads +1, so the march jumps past its region (past the region of the
+       * whole super-brick when its flag is clear) */
+      int bi[3];
+      R pp[3] = {px, py, pz};
+      for (int a = 0; a < 3; ++a) {
+        int q = (int)floor(((double)pp[a] - V->org) * V->inv_vs - 0.5);
+        if (q < 0) q = 0;
+        if (q > n - 2) q = n - 2;
+        bi[a] = q >> 3;
+      }
+      const int super_clear = !M->sflags[((size_t)(bi[0] / 4) * ns + bi[1] / 4) * ns + bi[2] / 4];
+      if (super_clear || !M->flags[((size_t)bi[0] * nbk + bi[1]) * nbk + bi[2]]) {
+        const int span = super_clear ? 32 : 8;
+        R te = (R)1e30;
+        for (int a = 0; a < 3; ++a) {
+          if (fabs((double)dir[a]) <= 1e-12) continue;
+          const int ci = super_clear ? bi[a] / 4 : bi[a];
+          double edge = dir[a] > 0 ? V->org + vs * ((double)span * (ci + 1) + 0.5)
+                                   : V->org + vs * ((double)span * ci + 0.5);
+          R ta = (R)((edge - (double)o[a]) / (double)dir[a]);
+          if (ta < te) te = ta;
+        }
+        t = (te > t ? te : t) + (R)(0.01 * vs) + pert;
+        fp = 1;
+        sampled = 1;
+        if (amb && fabs((double)(t - t1)) < 0.05) *amb = 1;
+        if (t > t1) return 0;
+        continue;
+      }
+    }
+    if (!sampled) {
+      fp = trilinear(V, px, py, pz);
+      sampled = 1;
+    }
+    R step = fp > 0 ? (far_k * fp > min_step ? far_k * fp : min_step) : min_step;
+    R tn = t + step + pert;
+    if (amb && fabs((double)(tn - t1)) < 0.05) *amb = 1;
+    if (tn > t1) return 0;
+    R fn = trilinear(V, o[0] + tn * dir[0], o[1] + tn * dir[1], o[2] + tn * dir[2]);
+    if (amb && fabs((double)fn) < 2e-4) *amb = 1;
+    if (fp > 0 && fn <= 0) {
+      *ts = refine_root(V, o, dir, t, fp, tn, fn, min_step, M->refine_iters);
+      if (amb && refine_is_sensitive(V, o, dir, t, tn, *ts, min_step, M->refine_iters, (R)0.01,
+                                     (R)0.02))
+        *amb = 1;
+      return 1;
+    }
+    if (fp < 0 && fn > 0) return 0;
+    t = tn;
+    fp = fn;
+  }
+  return 0;
+}
+
 /* Raycast: d_raycast (Source/src/Raycaster.cu:97-230) -- ray from the camera
  * position through the pixel's point at z = -1 (:117-125), slab clip
  * (:35-55) to the box of voxel centres, march to the first surface. The
@@ -474,8 +558,12 @@ static int refine_is_sensitive(const vol_view *V, const R *o, const R *dir, R t,
  * thinner than one step can be found by one march and stepped over by the
  * other. `ambig` flags a ray whose skip landing or step ends
  * within 0.05 mm of the range end, whose march sample lies within 2e-4 of
- * zero, whose normal's samples touch the box within 0.05 mm, or whose refined
- * surface is sensitive to rounding (refine_is_sensitive). */
+ * zero, whose normal's samples touch the box within 0.05 mm, whose refined
+ * surface is sensitive to rounding (refine_is_sensitive), or whose march finds
+ * another hit or miss, or a surface more than 0.05 mm away, when every
+ * position update moves by +-2e-3 mm: where the field is steep (noise),
+ * tsdf-scaled steps amplify position differences, and a negative stretch
+ * thinner than a step is caught by one march and stepped over by another. */
 void ora_raycast(const ora_vol *v, const uint32_t *words, const uint8_t *flags, const ora_cam *c,
                  const ora_params *p, const double *P, R *pts, uint8_t *ambig) {
   const int n = v->n;
@@ -496,6 +584,7 @@ void ora_raycast(const ora_vol *v, const uint32_t *words, const uint8_t *flags, 
         for (int k = 0; k < nbk; ++k)
           if (flags[((size_t)i * nbk + j) * nbk + k]) sflags[((size_t)(i / 4) * ns + j / 4) * ns + k / 4] = 1;
   }
+  const march_ctx M = {&V, flags, sflags, n, nbk, ns, vs, min_step, far_k, p->refine_iters};
 #pragma omp parallel for schedule(dynamic, 4)
   for (int y = 0; y < c->h; ++y) {
     for (int x = 0; x < c->w; ++x) {
@@ -519,68 +608,17 @@ void ora_raycast(const ora_vol *v, const uint32_t *words, const uint8_t *flags, 
       }
       R t0 = tnear > (R)c->dmin * lam ? tnear : (R)c->dmin * lam;
       R t1 = tfar < (R)c->dmax * lam ? tfar : (R)c->dmax * lam;
-      int hit = 0;
       R ts = 0;
-      if (t0 < t1) {
-        R t = t0;
-        R fp = 1;
-        int sampled = 0;
-        for (int it = 0; it < (1 << 16); ++it) {
-          R px = o[0] + t * dir[0], py = o[1] + t * dir[1], pz = o[2] + t * dir[2];
-          if (flags) {
-            /* empty-space skip: a brick whose flag is clear holds, with its
-             * 26 neighbours, only +1 voxels; every sample whose cell base is
-             * in it reads +1, so the march jumps past its region (past the
-             * region of the whole super-brick when its flag is clear) */
-            int bi[3];
-            R pp[3] = {px, py, pz};
-            for (int a = 0; a < 3; ++a) {
-              int q = (int)floor(((double)pp[a] - V.org) * V.inv_vs - 0.5);
-              if (q < 0) q = 0;
-              if (q > n - 2) q = n - 2;
-              bi[a] = q >> 3;
-            }
-            const int super_clear = !sflags[((size_t)(bi[0] / 4) * ns + bi[1] / 4) * ns + bi[2] / 4];
-            if (super_clear || !flags[((size_t)bi[0] * nbk + bi[1]) * nbk + bi[2]]) {
-              const int span = super_clear ? 32 : 8;
-              R te = (R)1e30;
-              for (int a = 0; a < 3; ++a) {
-                if (fabs((double)dir[a]) <= 1e-12) continue;
-                const int ci = super_clear ? bi[a] / 4 : bi[a];
-                double edge = dir[a] > 0 ? V.org + vs * ((double)span * (ci + 1) + 0.5)
-                                         : V.org + vs * ((double)span * ci + 0.5);
-                R ta = (R)((edge - (double)o[a]) / (double)dir[a]);
-                if (ta < te) te = ta;
-              }
-              t = (te > t ? te : t) + (R)(0.01 * vs);
-              fp = 1;
-              sampled = 1;
-              if (ambig && fabs((double)(t - t1)) < 0.05) amb = 1;
-              if (t > t1) break;
-              continue;
-            }
-          }
-          if (!sampled) {
-            fp = trilinear(&V, px, py, pz);
-            sampled = 1;
-          }
-          R step = fp > 0 ? (far_k * fp > min_step ? far_k * fp : min_step) : min_step;
-          R tn = t + step;
-          if (ambig && fabs((double)(tn - t1)) < 0.05) amb = 1;
-          if (tn > t1) break;
-          R fn = trilinear(&V, o[0] + tn * dir[0], o[1] + tn * dir[1], o[2] + tn * dir[2]);
-          if (ambig && fabs((double)fn) < 2e-4) amb = 1;
-          if (fp > 0 && fn <= 0) {
-            ts = refine_root(&V, o, dir, t, fp, tn, fn, min_step, p->refine_iters);
-            if (ambig && refine_is_sensitive(&V, o, dir, t, tn, ts, min_step, p->refine_iters,
-                                             (R)0.01, (R)0.02))
-              amb = 1;
-            hit = 1;
-            break;
-          }
-          if (fp < 0 && fn > 0) break;
-          t = tn;
-          fp = fn;
+      const int hit = march_ray(&M, o, dir, t0, t1, 0, &ts, ambig ? &amb : NULL);
+      if (ambig && !amb && t0 < t1) {
+        /* the found surface must not depend on where rounding puts the
+         * march: every position update moved by +-2e-3 mm (FP32 rounding
+         * of one update of a metre-long march is ~1e-4 mm) must find the
+         * same hit or miss, and a surface within 0.05 mm */
+        for (int k = -1; k <= 1 && !amb; k += 2) {
+          R tp = 0;
+          const int hp = march_ray(&M, o, dir, t0, t1, (R)(2e-3 * k), &tp, NULL);
+          if (hp != hit || (hit && fabs((double)(tp - ts)) > 0.05)) amb = 1;
         }
       }
       R *out = pts + 8 * pix;
@@ -606,6 +644,61 @@ void ora_raycast(const ora_vol *v, const uint32_t *words, const uint8_t *flags, 
       }
       if (ambig) ambig[pix] = (uint8_t)amb;
     }
+  }
+  free(sflags);
+}
+
+/* The march of chosen pixels with every position update moved by each of
+ * `npert` perturbations (mm): out[(i * npert + k) * 4] = hit vertex (x, y, z,
+ * 1) or zeros, for pixel (xy[2 i], xy[2 i + 1]). Explains a disagreement with
+ * another arithmetic: the surface a march finds when its positions move by a
+ * bounded amount. */
+void ora_raycast_pixels(const ora_vol *v, const uint32_t *words, const uint8_t *flags,
+                        const ora_cam *c, const ora_params *p, const double *P, int32_t npix,
+                        const int32_t *xy, int32_t npert, const double *perts, R *out) {
+  const int n = v->n;
+  const double vs = v->size / n;
+  vol_view V = {words, n, v->storage, -0.5 * v->size, 1.0 / vs};
+  const R lo = (R)(-0.5 * v->size + 0.5 * vs + 1e-3), hi = (R)(0.5 * v->size - 0.5 * vs - 1e-3);
+  const R o[3] = {(R)P[3], (R)P[7], (R)P[11]};
+  const int nbk = n / 8, ns = (nbk + 3) / 4;
+  uint8_t *sflags = NULL;
+  if (flags) {
+    sflags = (uint8_t *)calloc((size_t)ns * ns * ns, 1);
+    for (int i = 0; i < nbk; ++i)
+      for (int j = 0; j < nbk; ++j)
+        for (int k = 0; k < nbk; ++k)
+          if (flags[((size_t)i * nbk + j) * nbk + k]) sflags[((size_t)(i / 4) * ns + j / 4) * ns + k / 4] = 1;
+  }
+  const march_ctx M = {&V, flags, sflags, n, nbk, ns, vs, (R)(p->min_step_vox * vs),
+                       (R)(p->far_step_frac * v->trunc), p->refine_iters};
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int i = 0; i < npix * npert; ++i) {
+    const int q = i / npert, k = i % npert;
+    const int x = xy[2 * q], y = xy[2 * q + 1];
+    R dc[3] = {(R)(-((double)x - c->cx) / c->fx), (R)(-((double)y - c->cy) / c->fy), -1};
+    R lam = (R)sqrt((double)(dc[0] * dc[0] + dc[1] * dc[1] + 1));
+    R dir[3];
+    for (int a = 0; a < 3; ++a)
+      dir[a] = ((R)P[4 * a] * dc[0] + (R)P[4 * a + 1] * dc[1] + (R)P[4 * a + 2] * dc[2]) / lam;
+    R tnear = (R)-1e30, tfar = (R)1e30;
+    for (int a = 0; a < 3; ++a) {
+      if (fabs((double)dir[a]) < 1e-12) {
+        if (o[a] < lo || o[a] > hi) { tnear = (R)1e30; tfar = (R)-1e30; }
+      } else {
+        R t0 = (lo - o[a]) / dir[a], t1 = (hi - o[a]) / dir[a];
+        R mn = t0 < t1 ? t0 : t1, mx = t0 < t1 ? t1 : t0;
+        if (mn > tnear) tnear = mn;
+        if (mx < tfar) tfar = mx;
+      }
+    }
+    R t0 = tnear > (R)c->dmin * lam ? tnear : (R)c->dmin * lam;
+    R t1 = tfar < (R)c->dmax * lam ? tfar : (R)c->dmax * lam;
+    R ts = 0;
+    const int hit = march_ray(&M, o, dir, t0, t1, (R)perts[k], &ts, NULL);
+    R *dst = out + 4 * (size_t)i;
+    for (int a = 0; a < 3; ++a) dst[a] = hit ? o[a] + ts * dir[a] : 0;
+    dst[3] = hit ? 1 : 0;
   }
   free(sflags);
 }

@@ -78,11 +78,18 @@ int64_t ora_integrate(const ora_vol *v, uint32_t *words, const ora_cam *c, const
 
 /* raycast; pts is [h*w][8] world vertex/normal; flags (may be NULL): one
  * byte per brick for empty-space skipping; ambig (may be NULL) flags pixels
- * whose sign or range decisions are within rounding of a boundary, and hits
+ * whose sign or range decisions are within rounding of a boundary, hits
  * whose refined surface moves by more than 0.02 mm when the bracket moves by
- * 0.01 mm (unconverged refinement: the result depends on FP rounding). */
+ * 0.01 mm (unconverged refinement), and rays whose hit or surface changes when
+ * every march position moves by 2e-3 mm (the result depends on FP rounding). */
 void ora_raycast(const ora_vol *v, const uint32_t *words, const uint8_t *flags, const ora_cam *c,
                  const ora_params *p, const double *pose, ora_real *pts, uint8_t *ambig);
+/* the march of chosen pixels (xy[2 i], xy[2 i + 1]) under each position
+ * perturbation perts[k] (mm per update): out[(i npert + k) 4] = vertex, 1 or
+ * zeros on a miss */
+void ora_raycast_pixels(const ora_vol *v, const uint32_t *words, const uint8_t *flags,
+                        const ora_cam *c, const ora_params *p, const double *pose, int32_t npix,
+                        const int32_t *xy, int32_t npert, const double *perts, ora_real *out);
 /* model level l+1 from level l by subsampling (2x, 2y) */
 void ora_model_down(const ora_real *src, int32_t sw, ora_real *dst, int32_t dw, int32_t dh);
 

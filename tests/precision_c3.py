@@ -72,18 +72,21 @@ def check_integrate(cfg, ora, before: np.ndarray, after: np.ndarray, depth, pose
 
 
 def check_raycast(cfg, ora, words, flags, pose, gv, gn) -> dict:
+    import raycast_check
     opts, amb = ora.raycast(cfg, words, pose, ambig=True, flags=flags)
     ok = amb == 0
     hit_g, hit_o = gv[..., 3] > 0, opts[..., 3] > 0
     both = hit_g & hit_o & ok
-    verr = np.linalg.norm(gv[..., :3][both] - opts[..., :3][both], axis=-1)
+    r = raycast_check.compare(ora, cfg, words, flags, pose, gv, opts, amb)
     nb = both & (gn[..., 3] > 0) & (opts[..., 7] > 0)
     nerr = np.linalg.norm(gn[..., :3][nb] - opts[..., 4:7][nb], axis=-1)
     return {"hit_frac": float(hit_o.mean()), "hit_mismatch_frac": float((hit_g != hit_o)[ok].mean()),
             "flagged_frac": float((~ok).mean()),
-            "vertex_err_mm_max": float(verr.max()),
-            "vertex_err_mm_q999": float(np.quantile(verr, 0.999)),
-            "vertex_err_mm_median": float(np.median(verr)),
+            "vertex_err_mm_max": r["max_err_mm"],
+            "vertex_err_mm_q999": r["q999_err_mm"],
+            "vertex_err_mm_median": r["median_err_mm"],
+            "rounding_sensitive_rays": r["rounding_sensitive"],
+            "unexplained_rays": r["unexplained"],
             "normal_err_median": float(np.median(nerr))}
 
 
@@ -168,6 +171,8 @@ def run_study(frames: int, checkpoints: list[int], log=print) -> dict:
         "max_tsdf_err_fp16_ulp": max(c["integrate"]["max_tsdf_err_fp16_ulp"] for c in cps),
         "weights_equal": all(c["integrate"]["weights_equal"] for c in cps),
         "max_vertex_err_mm": max(c["raycast"]["vertex_err_mm_max"] for c in cps),
+        "max_rounding_sensitive_rays": max(c["raycast"]["rounding_sensitive_rays"] for c in cps),
+        "unexplained_rays": sum(len(c["raycast"]["unexplained_rays"]) for c in cps),
         "max_vertex_err_mm_q999": max(c["raycast"]["vertex_err_mm_q999"] for c in cps),
         "max_pose_err_rad": max(c["icp"]["rot_err_rad"] for c in cps),
         "max_pose_err_mm": max(c["icp"]["trans_err_mm"] for c in cps),

@@ -7,7 +7,9 @@ boundary (pixel rounding at .5, a depth at the range limit, an SDF at -trunc,
 a tsdf sample at 0) are flagged by the oracle and excluded; their number is
 bounded. Tolerances (from the path's precision targets):
   TSDF      within 1 int16 quantisation step (trunc / 32767)
-  vertices  within 1e-4 m = 0.1 mm (every ray the oracle does not flag)
+  vertices  within 1e-4 m = 0.1 mm (every ray the oracle does not flag; a
+            ray whose march is chaotic must be reproduced by the oracle's
+            march under a bounded position perturbation)
   pose      within 1e-5 rad and 1e-5 m = 0.01 mm
 """
 import numpy as np
@@ -39,6 +41,20 @@ def build_state(of, cfg, frames, device):
         of.integrate(cfg, vol, d, dev_pose(seq.poses[k], device), lam)
     torch.cuda.synchronize()
     return seq, vol, lam
+
+
+def check_rays(ora, cfg, words, flags, pose, gv, opts, amb, flagged_max=1e-2):
+    """Every ray the oracle does not flag: hit and miss as the oracle, vertex
+    within 0.1 mm, or, for a ray whose march is chaotic, the GPU's result
+    reproduced by the oracle's march under a position perturbation of at most
+    0.05 mm per update (tests/raycast_check.py); such rays are few."""
+    import raycast_check
+    r = raycast_check.compare(ora, cfg, words, flags, pose, gv, opts, amb)
+    assert r["flagged"] <= flagged_max * r["rays"], r
+    assert not r["unexplained"], r
+    assert r["rounding_sensitive"] <= max(3, 1e-4 * r["rays"]), r
+    assert r["max_err_mm"] < 0.1 and r["median_err_mm"] < 0.01, r
+    return r
 
 
 def gpu_pyramid_to_oracle(of, ora, cfg, pyr, with_depth=True):
@@ -228,14 +244,8 @@ def test_ragged_frame_sizes(of, ora, cuda, size):
     opts, amb = ora.raycast(cfg, words, pose, ambig=True, flags=flags)
     v0, n0 = (t.cpu().numpy() for t in of.unpack_points(cfg, model, 0))
     gv = v0.astype(np.float64)
-    ok = amb == 0
-    hit_g, hit_o = gv[..., 3] > 0, opts[..., 3] > 0
-    assert hit_o.mean() > 0.3, "the scene should be mostly visible"
-    assert (hit_g != hit_o)[ok].mean() < 1e-3
-    assert (~ok).mean() < 1e-2
-    both = hit_g & hit_o & ok
-    verr = np.linalg.norm(gv[..., :3][both] - opts[..., :3][both], axis=-1)
-    assert verr.max() < 0.1, f"vertex err max {verr.max()} mm"
+    assert (opts[..., 3] > 0).mean() > 0.3, "the scene should be mostly visible"
+    check_rays(ora, cfg, words, flags, pose, gv, opts, amb)
     for l in range(1, cfg.levels):
         vl, nl = (t.cpu().numpy() for t in of.unpack_points(cfg, model, l))
         s = 1 << l
@@ -305,19 +315,13 @@ def test_raycast_matches_oracle(of, ora, cuda, name, res):
     assert ((plain[..., 3] > 0) != (opts[..., 3] > 0)).mean() < 5e-3
     dp = np.linalg.norm(plain[..., :3][hp] - opts[..., :3][hp], axis=-1)
     assert np.quantile(dp, 0.99) < 0.1
-    # The GPU against the oracle with the same skipping: every ray that the
-    # oracle does not flag (a decision within rounding of a boundary, or a
-    # refined surface that moves with the bracket) within 0.1 mm.
+    # The GPU against the oracle with the same skipping, ray by ray.
     gv, gn = (t.cpu().numpy().astype(np.float64) for t in of.unpack_points(cfg, model, 0))
     ok = amb == 0
     hit_g, hit_o = gv[..., 3] > 0, opts[..., 3] > 0
     assert hit_o.mean() > 0.5, "scene should be mostly visible"
-    assert (~ok).mean() < 1e-2
-    assert (hit_g != hit_o)[ok].mean() < 1e-3
+    check_rays(ora, cfg, words, flags, pose, gv, opts, amb)
     both = hit_g & hit_o & ok
-    verr = np.linalg.norm(gv[..., :3][both] - opts[..., :3][both], axis=-1)
-    assert verr.max() < 0.1, f"vertex err max {verr.max()} mm"
-    assert np.median(verr) < 0.01
     nb = both & (gn[..., 3] > 0) & (opts[..., 7] > 0)
     nerr = np.linalg.norm(gn[..., :3][nb] - opts[..., 4:7][nb], axis=-1)
     assert np.median(nerr) < 1e-3
