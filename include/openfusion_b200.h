@@ -372,8 +372,12 @@ of_status_t of_tracker_destroy(of_tracker_t tracker);
  * branches); then this frame is tracked against that model. Frame 0 only
  * sets the pose (its initial pose). The pose is this frame's when the call's
  * work completes; the volume and model hold the frames before it until the
- * next call or of_tracker_flush. `depth_is_host` != 0: `depth` is host memory
- * (pinned for an asynchronous copy) and is copied on `stream`. */
+ * next call or of_tracker_flush. `depth_is_host` != 0: `depth` is host memory,
+ * copied on `stream`; with graphs, a pinned buffer (cudaMallocHost /
+ * cudaHostRegister) is copied by the step itself at the head of the
+ * pre-processing branch, beside the fusion of the previous frame, and any
+ * other host buffer before the step. The buffer must stay unchanged until the
+ * call's work completes. */
 of_status_t of_tracker_process(of_tracker_t tracker, const uint16_t *depth, int32_t depth_is_host,
                                of_stream_t stream);
 /* Fuses the last processed frame at its pose and raycasts the model there

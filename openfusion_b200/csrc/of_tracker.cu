@@ -45,7 +45,7 @@ struct of_tracker {
   // greatest stream priority (its cluster of whole SMs is placed before other
   // blocks fill them; kept in the graphs by cudaGraphInstantiateFlagUseNodePriority)
   cudaStream_t pre = nullptr, side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_pre = nullptr, ev_cnn = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_pre = nullptr, ev_cnn = nullptr, ev_up = nullptr;
   void *volume = nullptr;
   void *frame = nullptr;
   void *model = nullptr;
@@ -72,6 +72,14 @@ struct of_tracker {
   bool tuned = false;  // desc.tune: the online tuning has run
   cudaGraphExec_t g_first = nullptr;
   cudaGraphExec_t g_track[2] = {nullptr, nullptr};
+  // The step graphs upload a host frame themselves, at the head of the
+  // pre-processing branch (beside the fusion of the previous frame): a memcpy
+  // node captured from `stage` and pointed at the caller's pinned buffer at
+  // every launch, or disabled when the frame is already on the device. The
+  // graphs they were instantiated from stay alive for those node handles.
+  cudaGraph_t g_track_src[2] = {nullptr, nullptr};
+  cudaGraphNode_t up_node[2] = {nullptr, nullptr};
+  uint16_t *stage = nullptr;  // pinned placeholder source of the captured upload
 };
 
 namespace {
@@ -116,11 +124,13 @@ of_status_t enqueue_fuse(of_tracker *t, const uint16_t *depth, cudaStream_t s) {
 // the previous pose: after the CNN when it predicts the warm start, else
 // after pre-processing); ICP(k) after the join. `fuse` = false when
 // of_tracker_flush fused frame k-1.
-of_status_t enqueue_track(of_tracker *t, int cur, bool fuse, cudaStream_t s) {
+// `upload` (may be null): a pinned host frame that the pre-processing branch
+// copies into depth[cur] before anything reads it (the camera-side filters
+// follow on that branch, and the CNN branch waits for both).
+of_status_t enqueue_track(of_tracker *t, int cur, bool fuse, cudaStream_t s,
+                          const uint16_t *upload = nullptr) {
   const of_tracker_desc_t &d = t->desc;
   const uint16_t *now = t->depth[cur], *before = t->depth[cur ^ 1];
-  of_status_t sflt = enqueue_filters(t, cur, s);
-  if (sflt != OF_OK) return sflt;
   OF_CUDA_TRY(cudaEventRecord(t->ev_fork, s));  // nothing has forked before this
   // From the fork on, a failed call is remembered rather than returned at
   // once, so that every branch that forked also joins `s` before the error is
@@ -131,8 +141,16 @@ of_status_t enqueue_track(of_tracker *t, int cur, bool fuse, cudaStream_t s) {
     return e == cudaSuccess;
   };
   const bool pre_forked = ok(cudaStreamWaitEvent(t->pre, t->ev_fork, 0));
-  const bool side_forked = t->warm && ok(cudaStreamWaitEvent(t->side, t->ev_fork, 0));
-  of_status_t st = OF_OK, sp = OF_OK, sb = OF_OK;
+  of_status_t st = OF_OK, sp = OF_OK, sb = OF_OK, sflt = OF_OK;
+  bool up_recorded = false;
+  if (pre_forked) {
+    const size_t bytes = (size_t)d.camera.width * d.camera.height * sizeof(uint16_t);
+    if (upload)
+      ok(cudaMemcpyAsync(t->depth[cur], upload, bytes, cudaMemcpyHostToDevice, t->pre));
+    sflt = enqueue_filters(t, cur, t->pre);
+    up_recorded = t->warm && ok(cudaEventRecord(t->ev_up, t->pre));
+  }
+  const bool side_forked = up_recorded && ok(cudaStreamWaitEvent(t->side, t->ev_up, 0));
   bool cnn_recorded = false, pre_recorded = false;
   if (side_forked) {
     st = of_cnn_predict(t->cnn_params, t->cnn_master, before, now, d.camera.width,
@@ -141,7 +159,7 @@ of_status_t enqueue_track(of_tracker *t, int cur, bool fuse, cudaStream_t s) {
     cnn_recorded = ok(cudaEventRecord(t->ev_cnn, t->side));
   }
   if (pre_forked) {
-    sp = of_preprocess(&d.camera, &d.filter, now, d.camera.width, t->frame, t->pre);
+    if (sflt == OF_OK) sp = of_preprocess(&d.camera, &d.filter, now, d.camera.width, t->frame, t->pre);
     if (sp == OF_OK && !t->warm)
       sb = of_icp_begin_launch(t->pose, t->icp_ws, t->stats, nullptr, t->pre);
     pre_recorded = ok(cudaEventRecord(t->ev_pre, t->pre));
@@ -150,6 +168,7 @@ of_status_t enqueue_track(of_tracker *t, int cur, bool fuse, cudaStream_t s) {
   if (pre_recorded) ok(cudaStreamWaitEvent(s, t->ev_pre, 0));
   if (cnn_recorded) ok(cudaStreamWaitEvent(s, t->ev_cnn, 0));
   if (first != cudaSuccess) return of_set_cuda_error(first);
+  if (sflt != OF_OK) return sflt;
   if (st != OF_OK) return st;
   if (sp != OF_OK) return sp;
   if (sb != OF_OK) return sb;
@@ -173,11 +192,32 @@ int count_kernel_nodes(cudaGraph_t g) {
   return k;
 }
 
-// graph of frame 0 (cur < 0) or of a tracking step with depth[cur]
+// the graph's memcpy node whose source is `src` (the captured upload)
+cudaGraphNode_t find_upload(cudaGraph_t g, const void *src) {
+  size_t n = 0;
+  if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return nullptr;
+  cudaGraphNode_t *nodes = new cudaGraphNode_t[n];
+  cudaGraphNode_t found = nullptr;
+  if (cudaGraphGetNodes(g, nodes, &n) == cudaSuccess)
+    for (size_t i = 0; i < n && !found; ++i) {
+      cudaGraphNodeType ty;
+      cudaMemcpy3DParms p = {};
+      if (cudaGraphNodeGetType(nodes[i], &ty) == cudaSuccess && ty == cudaGraphNodeTypeMemcpy &&
+          cudaGraphMemcpyNodeGetParams(nodes[i], &p) == cudaSuccess && p.srcPtr.ptr == src)
+        found = nodes[i];
+    }
+  delete[] nodes;
+  return found;
+}
+
+// graph of frame 0 (cur < 0) or of a tracking step with depth[cur]; a step
+// graph keeps its source graph and its upload node (of_tracker_process points
+// the node at each host frame)
 of_status_t capture(of_tracker *t, int cur, cudaGraphExec_t *out) {
   cudaGraph_t g = nullptr;
   OF_CUDA_TRY(cudaStreamBeginCapture(t->cap, cudaStreamCaptureModeThreadLocal));
-  of_status_t st = cur < 0 ? enqueue_first(t, t->cap) : enqueue_track(t, cur, true, t->cap);
+  of_status_t st =
+      cur < 0 ? enqueue_first(t, t->cap) : enqueue_track(t, cur, true, t->cap, t->stage);
   cudaError_t e = cudaStreamEndCapture(t->cap, &g);
   if (st != OF_OK) {
     if (g) cudaGraphDestroy(g);
@@ -185,10 +225,17 @@ of_status_t capture(of_tracker *t, int cur, cudaGraphExec_t *out) {
   }
   if (e != cudaSuccess) return of_set_cuda_error(e);
   (cur >= 0 ? t->kernels_track : t->kernels_first) = count_kernel_nodes(g);
+  if (*out) cudaGraphExecDestroy(*out);
+  *out = nullptr;
   e = cudaGraphInstantiateWithFlags(out, g, cudaGraphInstantiateFlagUseNodePriority);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess) return of_set_cuda_error(e);
-  return OF_OK;
+  if (e != cudaSuccess || cur < 0) {
+    cudaGraphDestroy(g);
+    return e != cudaSuccess ? of_set_cuda_error(e) : OF_OK;
+  }
+  if (t->g_track_src[cur]) cudaGraphDestroy(t->g_track_src[cur]);
+  t->g_track_src[cur] = g;
+  t->up_node[cur] = find_upload(g, t->stage);
+  return t->up_node[cur] ? OF_OK : OF_ERR_CUDA;
 }
 
 // The online tuning (desc.tune): every raycast block shape, twice each, on
@@ -242,6 +289,9 @@ void release(of_tracker *t) {
   if (t->g_first) cudaGraphExecDestroy(t->g_first);
   for (cudaGraphExec_t g : t->g_track)
     if (g) cudaGraphExecDestroy(g);
+  for (cudaGraph_t g : t->g_track_src)
+    if (g) cudaGraphDestroy(g);
+  if (t->stage) cudaFreeHost(t->stage);
   void *bufs[] = {t->volume, t->frame, t->model, t->icp_ws, t->pose, t->hist, t->hist_count,
                   t->depth[0], t->depth[1], t->filter_scratch, t->lambda, t->scratch, t->stats, t->cnn_master,
                   t->cnn_params, t->cnn_out, t->warm_pose};
@@ -249,7 +299,7 @@ void release(of_tracker *t) {
     if (b) cudaFree(b);
   for (cudaStream_t q : {t->cap, t->pre, t->side})
     if (q) cudaStreamDestroy(q);
-  for (cudaEvent_t ev : {t->ev_fork, t->ev_pre, t->ev_cnn})
+  for (cudaEvent_t ev : {t->ev_fork, t->ev_pre, t->ev_cnn, t->ev_up})
     if (ev) cudaEventDestroy(ev);
   delete t;
 }
@@ -278,7 +328,11 @@ extern "C" of_status_t of_tracker_create(const of_tracker_desc_t *desc, of_track
     e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
     if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&t->side, cudaStreamNonBlocking, greatest);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_cnn, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->ev_up, cudaEventDisableTiming);
   }
+  if (e == cudaSuccess && desc->use_graph)
+    e = cudaMallocHost((void **)&t->stage, (size_t)desc->camera.width * desc->camera.height *
+                                               sizeof(uint16_t));
   if (e != cudaSuccess) { release(t); return of_set_cuda_error(e); }
   size_t vol_bytes = 0, lam_bytes = 0, scratch_bytes = 0;
   of_volume_bytes(&desc->volume, &vol_bytes);
@@ -361,13 +415,29 @@ extern "C" of_status_t of_tracker_process(of_tracker_t t, const uint16_t *depth,
   cudaStream_t s = (cudaStream_t)stream;
   const int cur = (int)(t->frames & 1);
   size_t bytes = (size_t)t->desc.camera.width * t->desc.camera.height * sizeof(uint16_t);
-  if (on_host) {
-    OF_CUDA_TRY(cudaMemcpyAsync(t->depth[cur], depth, bytes, cudaMemcpyHostToDevice, s));
-  } else if (depth != t->depth[cur]) {
-    OF_CUDA_TRY(cudaMemcpyAsync(t->depth[cur], depth, bytes, cudaMemcpyDeviceToDevice, s));
-  }
   const bool track = t->frames > 0;
   const bool graphs = t->desc.use_graph && (t->desc.tune == 0 || t->tuned);
+  // A step graph uploads a pinned host frame itself, beside the fusion of the
+  // previous frame; any other frame is copied before the step, as the eager
+  // path does.
+  bool in_graph = false;
+  if (graphs && track && !t->last_fused && t->up_node[cur]) {
+    cudaPointerAttributes a;
+    if (on_host && cudaPointerGetAttributes(&a, depth) == cudaSuccess &&
+        a.type == cudaMemoryTypeHost)
+      in_graph = cudaGraphExecMemcpyNodeSetParams1D(t->g_track[cur], t->up_node[cur],
+                                                    t->depth[cur], depth, bytes,
+                                                    cudaMemcpyHostToDevice) == cudaSuccess;
+    cudaGetLastError();  // a refused update falls back to the copy below
+    OF_CUDA_TRY(cudaGraphNodeSetEnabled(t->g_track[cur], t->up_node[cur], in_graph ? 1 : 0));
+  }
+  if (!in_graph) {
+    if (on_host) {
+      OF_CUDA_TRY(cudaMemcpyAsync(t->depth[cur], depth, bytes, cudaMemcpyHostToDevice, s));
+    } else if (depth != t->depth[cur]) {
+      OF_CUDA_TRY(cudaMemcpyAsync(t->depth[cur], depth, bytes, cudaMemcpyDeviceToDevice, s));
+    }
+  }
   if (t->desc.use_graph && !track) {
     OF_CUDA_TRY(cudaGraphLaunch(t->g_first, s));
   } else if (graphs && !t->last_fused) {

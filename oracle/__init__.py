@@ -88,6 +88,7 @@ class Oracle:
         L.ora_integrate.argtypes = [C.POINTER(Vol), P, C.POINTER(Cam), P, P, P]
         L.ora_integrate.restype = C.c_int64
         L.ora_raycast.argtypes = [C.POINTER(Vol), P, P, C.POINTER(Cam), C.POINTER(Params), P, P, P]
+        L.ora_tsdf_at.argtypes = [C.POINTER(Vol), P, C.c_int64, P, P]
         L.ora_raycast_pixels.argtypes = [C.POINTER(Vol), P, P, C.POINTER(Cam), C.POINTER(Params), P,
                                          C.c_int32, P, C.c_int32, P, P]
         L.ora_model_down.argtypes = [P, C.c_int32, P, C.c_int32, C.c_int32]
@@ -244,6 +245,15 @@ class Oracle:
                                         P_.ctypes.data, len(xy), xy.ctypes.data, len(pe),
                                         pe.ctypes.data, out.ctypes.data)
         return out
+
+    def tsdf_at(self, cfg, words: np.ndarray, xyz: np.ndarray) -> np.ndarray:
+        """The trilinear tsdf / trunc at world points [..., 3] (mm)."""
+        pts = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3))
+        out = np.zeros(len(pts), self.real)
+        if len(pts):
+            self.lib.ora_tsdf_at(C.byref(self.vol(cfg)), words.ctypes.data, len(pts),
+                                 pts.ctypes.data, out.ctypes.data)
+        return out.reshape(np.asarray(xyz).shape[:-1])
 
     @staticmethod
     def shade_rgba(cfg, pose: np.ndarray, normals: np.ndarray) -> np.ndarray:

@@ -703,6 +703,18 @@ void ora_raycast_pixels(const ora_vol *v, const uint32_t *words, const uint8_t *
   free(sflags);
 }
 
+/* The trilinear tsdf (tsdf / trunc) at world points xyz[3 i .. 3 i + 2]: the
+ * field the raycast marches (cell corners clamped as in `trilinear`). */
+void ora_tsdf_at(const ora_vol *v, const uint32_t *words, int64_t npts, const double *xyz,
+                 R *out) {
+  const int n = v->n;
+  const double vs = v->size / n;
+  vol_view V = {words, n, v->storage, -0.5 * v->size, 1.0 / vs};
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < npts; ++i)
+    out[i] = trilinear(&V, (R)xyz[3 * i], (R)xyz[3 * i + 1], (R)xyz[3 * i + 2]);
+}
+
 void ora_model_down(const R *src, int32_t sw, R *dst, int32_t dw, int32_t dh) {
   for (int y = 0; y < dh; ++y)
     for (int x = 0; x < dw; ++x)

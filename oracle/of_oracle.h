@@ -90,6 +90,9 @@ void ora_raycast(const ora_vol *v, const uint32_t *words, const uint8_t *flags, 
 void ora_raycast_pixels(const ora_vol *v, const uint32_t *words, const uint8_t *flags,
                         const ora_cam *c, const ora_params *p, const double *pose, int32_t npix,
                         const int32_t *xy, int32_t npert, const double *perts, ora_real *out);
+/* the trilinear tsdf / trunc at world points xyz[3 i .. 3 i + 2] */
+void ora_tsdf_at(const ora_vol *v, const uint32_t *words, int64_t npts, const double *xyz,
+                 ora_real *out);
 /* model level l+1 from level l by subsampling (2x, 2y) */
 void ora_model_down(const ora_real *src, int32_t sw, ora_real *dst, int32_t dw, int32_t dh);
 

@@ -609,3 +609,32 @@ def test_tracker_survives_corrupt_frames(of, cuda):
     tr.close()
     assert np.array_equal(hist[4], hist[3])  # singular: the pose stays
     assert np.all(np.isfinite(hist))
+
+
+@pytest.mark.parametrize("warm", [False, True])
+def test_tracker_uploads_pinned_frames_inside_the_step(of, cuda, warm):
+    """A pinned host frame is copied by the step graph itself, at the head of
+    the pre-processing branch (beside the fusion of the previous frame, with
+    the camera-side filters after it and the CNN branch waiting for both):
+    the poses equal, bit for bit, those of the same tracker fed device frames
+    and fed pageable host frames (copied before the step)."""
+    import torch
+    from openfusion_b200 import learned
+    cfg = small(of, "c1")
+    n = 7
+    seq = of.make_sequence(cfg, frames=n)
+    frames = [torch.from_numpy(seq.depth[k].astype(np.int16)) for k in range(n)]
+    pinned = [f.pin_memory() for f in frames]
+    device = [f.to(cuda) for f in frames]
+    w = learned.load_weights() if warm else None
+    p = of.depth_filter_params(["median5", "average"])
+    hist = []
+    for src in (device, pinned, frames):
+        tr = of.Tracker(cfg, seq.poses[0], warm_start_weights=w, depth_filter=p)
+        for f in src:
+            tr.process(f)
+        torch.cuda.synchronize()
+        hist.append(tr.pose_history(n))
+        tr.close()
+    assert np.array_equal(hist[0], hist[1])
+    assert np.array_equal(hist[0], hist[2])
