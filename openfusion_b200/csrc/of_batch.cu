@@ -138,7 +138,7 @@ of_status_t capture(of_batch *b, int cur, cudaGraphExec_t *out) {
   }
   if (e != cudaSuccess) return of_set_cuda_error(e);
   b->kernels_step = count_kernels(g);
-  e = cudaGraphInstantiate(out, g, 0);
+  e = cudaGraphInstantiateWithFlags(out, g, cudaGraphInstantiateFlagUseNodePriority);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return of_set_cuda_error(e);
   return OF_OK;
@@ -210,8 +210,13 @@ extern "C" of_status_t of_batch_create(const of_batch_desc_t *desc, of_batch_t *
   b->desc = *desc;
   b->streams.assign(desc->streams, desc->streams + n);
   b->desc.streams = b->streams.data();
-  cudaError_t e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
+  // the critical path above the pre-processing branch (as in a tracker step;
+  // the graphs keep the priorities as node priorities)
+  int least = 0, greatest = 0;
+  cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  if (e == cudaSuccess)
+    e = cudaStreamCreateWithPriority(&b->cap, cudaStreamNonBlocking, (least + greatest) / 2);
+  if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&b->side, cudaStreamNonBlocking, least);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_pre, cudaEventDisableTiming);
   for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaEventCreate(&b->ev_t[i]);
