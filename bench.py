@@ -511,7 +511,7 @@ def run_ours(args, cfg, world, rank, local):
         "e2e": {"value": e2e_fps, "unit": "frames/s",
                 "h2d_bytes_per_step": cfg.width * cfg.height * 2, "d2h_bytes_per_step": 128},
         "gpu_launches": kernels,
-        "tuning": {"raycast_block": ["16x16", "32x8", "8x32", "32x4"][ray_tile],
+        "tuning": {"raycast_block": ["16x16", "32x8", "8x32", "32x4", "16x8", "8x16", "8x8"][ray_tile],
                    "tuned_online": tuned, "at_warmup_step": tune},
         "clocks": sampler.summary(),
     }

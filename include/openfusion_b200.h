@@ -89,7 +89,8 @@ typedef struct of_raycast_params {
   float far_step_frac;   /* step as a fraction of tsdf*trunc when far from the surface (0.8) */
   int32_t refine_iters;  /* regula-falsi refinements of the zero crossing (3) */
   int32_t tile;          /* pixel block of one CTA (no result depends on it):
-                            0 = 16x16, 1 = 32x8, 2 = 8x32, 3 = 32x4 */
+                            0 = 16x16, 1 = 32x8, 2 = 8x32, 3 = 32x4, 4 = 16x8,
+                            5 = 8x16, 6 = 8x8 */
 } of_raycast_params_t;
 
 /* ICP (replaces ICP_ITERATIONS, DISTANCE_THRESHOLD, NORMAL_THRESHOLD,
@@ -496,7 +497,8 @@ typedef struct of_batch_stream {
 
 /* Tuning knobs of the batched stages; none changes a result. */
 typedef struct of_batch_tuning {
-  int32_t ray_tile;      /* raycast block: 0 = 16x16, 1 = 32x8, 2 = 8x32, 3 = 32x4 */
+  int32_t ray_tile;      /* raycast block (of_raycast_params_t.tile): 0 = 16x16, 1 = 32x8,
+                            2 = 8x32, 3 = 32x4, 4 = 16x8, 5 = 8x16, 6 = 8x8 */
   int32_t list_div;      /* integration blocks per stream = bricks / {16,32,64,128,256}[list_div] */
   int32_t icp_clusters;  /* resident 8-CTA clusters of the batched ICP (0 = as many as fit) */
   int32_t tuned;         /* (of_batch_tuning) 1 = chosen by measurement */

@@ -53,7 +53,8 @@ class Config:
     min_step_vox: float = 0.75
     far_step_frac: float = 0.8
     refine_iters: int = 3
-    ray_tile: int = 0               # raycast block shape (0 16x16, 1 32x8, 2 8x32, 3 32x4)
+    ray_tile: int = 0               # raycast block shape (0 16x16, 1 32x8, 2 8x32, 3 32x4,
+                                    # 4 16x8, 5 8x16, 6 8x8)
     scene_kind: int = 1
     motion: int = 0
     noise: float = 1.0

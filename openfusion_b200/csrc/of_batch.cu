@@ -300,7 +300,7 @@ extern "C" of_status_t of_batch_create(const of_batch_desc_t *desc, of_batch_t *
   b->knobs.icp_clusters = desc->tuning.icp_clusters;
   if (desc->tune) {
     b->plan.push_back({&b->knobs.list_div, {0, 1, 2, 3, 4}, 0});
-    b->plan.push_back({&b->knobs.ray_tile, {0, 1, 2, 3}, 1});
+    b->plan.push_back({&b->knobs.ray_tile, {0, 1, 2, 3, 4, 5, 6}, 1});
     std::vector<int> cl;
     for (int c : {maxc / 4, maxc / 2, maxc})
       if (c >= 1 && (cl.empty() || cl.back() != c)) cl.push_back(c);

@@ -37,7 +37,8 @@ struct BatchParams {
 // Tuning knobs of the batched stages. None changes a result: they choose tile
 // shapes and block counts only.
 struct BatchKnobs {
-  int ray_tile;        // raycast block shape: 0 = 16x16, 1 = 32x8, 2 = 8x32, 3 = 32x4
+  int ray_tile;        // raycast block shape: 0 = 16x16, 1 = 32x8, 2 = 8x32, 3 = 32x4,
+                       // 4 = 16x8, 5 = 8x16, 6 = 8x8
   int list_div;        // integrate: blocks per stream = ceil(bricks / list_div), capped
   int icp_clusters;    // batched ICP: resident clusters of the persistent grid
 };

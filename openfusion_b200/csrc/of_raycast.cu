@@ -50,9 +50,9 @@ struct DownJob {
 };
 
 // block shapes of the raycast (a tuning knob; every ray is the same)
-constexpr int kRayTiles = 4;
-constexpr int kRayTileX[kRayTiles] = {16, 32, 8, 32};
-constexpr int kRayTileY[kRayTiles] = {16, 8, 32, 4};
+constexpr int kRayTiles = 7;
+constexpr int kRayTileX[kRayTiles] = {16, 32, 8, 32, 16, 8, 8};
+constexpr int kRayTileY[kRayTiles] = {16, 8, 32, 4, 8, 16, 8};
 
 template <int STORAGE>
 __global__ void __launch_bounds__(256) k_raycast_batch(const RayJob *__restrict__ jobs,

@@ -243,7 +243,7 @@ of_status_t capture(of_tracker *t, int cur, cudaGraphExec_t *out) {
 // the volume as this step left it, at the tracked pose, into a scratch
 // pyramid (the tracker's model is left alone); CUDA events on `s`, the
 // fastest run wins. Then the step graphs are captured with the winner.
-constexpr int kTuneTiles = 4;
+constexpr int kTuneTiles = 7;  // every shape of of_raycast_params_t.tile
 constexpr int kTuneReps = 2;
 of_status_t tune_shapes(of_tracker *t, cudaStream_t s) {
   void *tmp = nullptr;

@@ -80,7 +80,7 @@ def main(frames: int):
     dd = torch.from_numpy(np.stack(depth).astype(np.int16)).to(dev)
 
     def run(cfg):
-        tr = of.Tracker(cfg, poses[0])
+        tr = of.Tracker(cfg, poses[0], tune=2)  # raycast block shape tuned at frame 2
         tr.process(dd[0])
         for k in range(1, 1 + warm):
             tr.process(dd[k])
@@ -136,7 +136,7 @@ def main(frames: int):
         return out
 
     ours_ms, hist = run(base)
-    exit_ms, hist_exit = run(dataclasses.replace(base, stop_rot_rad=2e-5, stop_trans_mm=0.02))
+    exit_ms, hist_exit = run(dataclasses.replace(base, stop_rot_rad=5e-6, stop_trans_mm=0.005))
     stage_us = stages(base)
     print(json.dumps({
         "workload": "640x480, 512^3 over 1024 mm (reference constants), %d frames" % frames,
@@ -150,7 +150,7 @@ def main(frames: int):
         "this_repo_convergence_exit": {"ms_per_frame": exit_ms, "frames_per_s": 1e3 / exit_ms,
                                        "max_pose_err_deg_mm": err(hist_exit),
                                        "icp": "3 levels, at most 10/5/4, a level ends when an "
-                                              "increment is below 2e-5 rad and 0.02 mm"},
+                                              "increment is below 5e-6 rad and 0.005 mm"},
         "speedup_convergence_exit": ref_ms / exit_ms,
         "stages_us": stage_us}))
 

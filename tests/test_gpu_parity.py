@@ -449,13 +449,13 @@ def test_tracker_online_tuning_changes_no_result(of, cuda, name):
         runs.append((tr.pose_history(6), tr.tuning()))
         tr.close()
     assert runs[0][1] == (0, False)
-    assert runs[1][1][1] and 0 <= runs[1][1][0] < 4, runs[1][1]
+    assert runs[1][1][1] and 0 <= runs[1][1][0] < 7, runs[1][1]
     assert np.array_equal(runs[0][0], runs[1][0])
     vol, lam = of.new_volume(cfg, cuda), of.lambda_table(cfg, cuda)
     for k in range(3):
         of.integrate(cfg, vol, depth[k], dev_pose(seq.poses[k], cuda), lam)
     models = [of.raycast(dataclasses.replace(cfg, ray_tile=t), vol, dev_pose(seq.poses[2], cuda))
-              for t in range(4)]
+              for t in range(7)]
     torch.cuda.synchronize()
     for m in models[1:]:
         assert torch.equal(m, models[0])
