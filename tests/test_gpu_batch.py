@@ -125,7 +125,7 @@ def test_tuned_and_graph_batches_equal_the_eager_one(of, cuda):
     """Online tuning (every knob's candidates timed on the first steps) and
     graph replay change no result: poses and a volume equal bit for bit."""
     cfgs = mixed_configs(of)[:4]
-    n = 30  # > the tuning steps (5 + 4 + up to 3 candidates, twice each)
+    n = 40  # > the tuning steps (7 + 5 + up to 3 candidates, twice each)
     seqs, depth = sequences(of, cfgs, n, cuda)
     runs = []
     for graph, tune in ((False, False), (True, True), (True, False)):
