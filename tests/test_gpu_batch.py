@@ -140,7 +140,7 @@ def test_tuned_and_graph_batches_equal_the_eager_one(of, cuda):
         runs.append((np.array(hist), t, w, (tun.ray_tile, tun.list_div, tun.icp_clusters, tun.tuned)))
         batch.close()
     assert runs[1][3][3] == 1, runs[1][3]
-    assert 0 <= runs[1][3][0] < 4 and 0 <= runs[1][3][1] < 5 and runs[1][3][2] >= 1
+    assert 0 <= runs[1][3][0] < 7 and 0 <= runs[1][3][1] < 5 and runs[1][3][2] >= 1
     for r in runs[1:]:
         assert np.array_equal(r[0], runs[0][0])
         assert np.array_equal(r[1], runs[0][1]) and np.array_equal(r[2], runs[0][2])
