@@ -38,6 +38,8 @@ constexpr float kEps = 1e-6f;  // _EPSILON_ (Constants.h:14)
 
 constexpr int kFusedThreads = 1024;
 constexpr int kFusedMaxBlocks = 2 * kSmCount;
+// model points a block of the fused kernel keeps in shared memory (192 KiB)
+constexpr int kMaxCachePts = 6144;
 // A partial-sum row slot of the fused kernel is one 64-bit word: the value's
 // bits, and above them the slot's sequence number (the frame's epoch << 13 |
 // the iteration + 1), so a reader that sees the number sees the value with it.
@@ -580,7 +582,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   __shared__ Rigid s_c2w, s_w2c;
   __shared__ float s_red[kFusedThreads / 32][32];
   __shared__ float s_tot[32];
-  __shared__ int s_warp_n[kFusedThreads / 32];
+  __shared__ int s_chunk_off[kMaxCachePts / 32];  // per cached chunk: its valid points, then their offset
   __shared__ int s_stop, s_inl, s_its, s_err, s_npts, s_conv, s_warm, s_examined;
   __shared__ double s_res, s_piv;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -617,37 +619,63 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       const int nchunks = (npx + 31) >> 5;
       const int my_chunks = nchunks > (int)blockIdx.x ? (nchunks - 1 - (int)blockIdx.x) / G + 1 : 0;
       const int kc = min(my_chunks, plan.cache_pts >> 5);
-      // ---- cache this block's valid model points of the level, in chunk order
-      if (threadIdx.x == 0) { s_npts = 0; s_conv = 0; }
+      // ---- cache this block's valid model points of the level, in chunk
+      // order: warp w counts the valid points of chunks w, w + 32, ...; one
+      // warp scans the counts into offsets; every warp stores its chunks'
+      // points there (reloaded, now from L1). Three block barriers per level.
+      for (int k = warp; k < kc; k += kWarps) {
+        const int p = ((int)blockIdx.x + k * G) * 32 + lane;
+        bool valid = false;
+        if (p < npx) valid = __ldg(&L.model[2 * p].w) != 0.f && __ldg(&L.model[2 * p + 1].w) != 0.f;
+        const unsigned m = __ballot_sync(0xffffffffu, valid);
+        if (lane == 0) s_chunk_off[k] = __popc(m);
+      }
       __syncthreads();
-      for (int k0 = 0; k0 < kc; k0 += kWarps) {
-        const int k = k0 + warp;
+      // every thread has read the previous level's exit flag by now
+      if (threadIdx.x == 0) s_conv = 0;
+      if (warp == 0) {
+        constexpr int kPer = (kMaxCachePts / 32 + 31) / 32;
+        int c[kPer];
+        int tot = 0;
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) {
+          const int k = lane * kPer + i;
+          c[i] = k < kc ? s_chunk_off[k] : 0;
+          tot += c[i];
+        }
+        int inc = tot;  // inclusive scan over the lanes
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, inc, o);
+          if (lane >= o) inc += y;
+        }
+        int run = inc - tot;
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) {
+          const int k = lane * kPer + i;
+          if (k < kc) s_chunk_off[k] = run;
+          run += c[i];
+        }
+        if (lane == 31) s_npts = inc;
+      }
+      __syncthreads();
+      for (int k = warp; k < kc; k += kWarps) {
         const int p = ((int)blockIdx.x + k * G) * 32 + lane;
         float4 s = make_float4(0.f, 0.f, 0.f, 0.f), ns = s;
         bool valid = false;
-        if (k < kc && p < npx) {
+        if (p < npx) {
           s = __ldg(L.model + 2 * p);
           ns = __ldg(L.model + 2 * p + 1);
           valid = s.w != 0.f && ns.w != 0.f;
         }
         const unsigned m = __ballot_sync(0xffffffffu, valid);
-        if (lane == 0) s_warp_n[warp] = __popc(m);
-        __syncthreads();
-        int off = s_npts;
-        for (int w = 0; w < warp; ++w) off += s_warp_n[w];
         if (valid) {
-          const int slot = off + __popc(m & ((1u << lane) - 1u));
+          const int slot = s_chunk_off[k] + __popc(m & ((1u << lane) - 1u));
           s_pts[2 * slot] = s;
           s_pts[2 * slot + 1] = ns;
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-          int tot = 0;
-          for (int w = 0; w < kWarps; ++w) tot += s_warp_n[w];
-          s_npts += tot;
-        }
-        __syncthreads();
       }
+      __syncthreads();
       const int n = s_npts;
       for (int it = 0; it < L.iters; ++it) {
         float acc[kVals];
@@ -824,6 +852,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     }
     // ---- judge a warm-started result; replace it by plain ICP if it fails
     if (pass == 1 || !warm || s_err) break;
+    __syncthreads();  // every thread has left the level loop (it reads s_stop)
     if (threadIdx.x == 0) {
       const bool keep = !s_stop && judge_keep(plan, ws->warm_pose, s_pose, s_res, s_inl, s_examined);
       s_warm = keep ? 1 : 2;
@@ -958,7 +987,6 @@ static bool icp_params_ok(const of_icp_params_t *p) {
 // Launch shape of the fused kernel on the current device: every block
 // co-resident (cooperative launch), with room in shared memory for the
 // block's slice of the finest level's model points (up to kMaxCachePts).
-constexpr int kMaxCachePts = 6144;  // 192 KiB of points per block
 struct FusedShape {
   int grid;       // co-resident blocks (may exceed kFusedMaxBlocks: then refused)
   int cache_pts;
@@ -1276,6 +1304,7 @@ __global__ void __cluster_dims__(kBatchCtas, 1, 1) __launch_bounds__(kBatchThrea
     for (int l = J.levels - 1; l >= 0 && !s_stop; --l) {
       const IcpLevel L = J.lv[l];
       const int npx = L.mw * L.mh;
+      __syncthreads();  // every thread has read the previous level's exit flag
       if (threadIdx.x == 0) s_conv = 0;
       __syncthreads();
       for (int it = 0; it < L.iters; ++it) {

@@ -255,7 +255,9 @@ __device__ __forceinline__ void raycast_pixel(const uint32_t *__restrict__ vol,
       }
       have_cell = false;
       const int bi = cell.x >> 3, bj = cell.y >> 3, bk = cell.z >> 3;
-      const int si = bi / kSuper, sj = bj / kSuper, sk = bk / kSuper;
+      // (cell indices are clamped to >= 0: unsigned division is a shift)
+      const int si = (int)((unsigned)bi / kSuper), sj = (int)((unsigned)bj / kSuper),
+                sk = (int)((unsigned)bk / kSuper);
       const int sidx = (si * ns + sj) * ns + sk;
       if (sidx != cur_s) {
         cur_s = sidx;
