@@ -538,35 +538,61 @@ def run_ours(args, cfg, world, rank, local):
 
 def warm_start_comparison(of, args, dev, world, rank):
     """The learned warm start against plain ICP on the large-motion workload
-    (640x480, 512^3 over 3 m, inter-frame motion up to 10 cm / 5 deg, held-out
-    seed): both trackers with the same early exit over the same rendered
-    frames, device-timed (CUDA events, max over ranks), with ICP iterations
-    and per-frame pose error against the ground truth."""
+    (640x480, 512^3 over 3 m, inter-frame motion up to 10 cm / 5 deg): three
+    held-out seeds (910000 + 3 rank + i), both trackers with the same early
+    exit over the same rendered frames. Per seed, one synchronous pass per arm
+    gives ICP iterations and pose error against the ground truth, then three
+    rounds of device-timed passes (CUDA events, max over ranks) alternate the
+    arms; a seed's frames/s are the median of its rounds."""
     import dataclasses
     from openfusion_b200 import learned
     from openfusion_b200.train_warm_start import eval_config, pose_errors, run_tracker
-    cfg = dataclasses.replace(eval_config(of), seed=910000 + rank)
-    scene = of.make_scene(cfg.scene_kind, cfg.seed, cfg.size_mm)
-    poses = of.make_trajectory(cfg.motion, cfg.seed + 1, cfg.size_mm, args.warm_frames)
-    depth = learned.render_device(cfg, scene, poses, device=dev)
-    out = {"workload": "c5: 640x480, 512^3 over 3 m, motion U[0,10] cm / U[0,5] deg per frame; "
-                       f"early exit {cfg.stop_rot_rad:g} rad / {cfg.stop_trans_mm:g} mm in both "
-                       "arms; warm pass on the finest level",
-           "frames": args.warm_frames - 1, "data": "synthetic (held-out seed, device renderer)"}
+    cfg0 = eval_config(of)
     weights = learned.load_weights()
-    for arm, w in (("plain", None), ("warm", weights)):
-        hist, its, kept, _ = run_tracker(of, cfg, depth, poses, w, timed=False)
-        barrier(world)
-        _, _, _, ms = run_tracker(of, cfg, depth, poses, w, timed=True)
-        ms = max_over_ranks(ms, world)
-        r, t = pose_errors(hist[1:], poses[1:])
-        out[arm] = {"frames_per_s": world * 1e3 / ms, "ms_per_frame": ms,
-                    "mean_icp_iterations": float(np.mean(its)),
-                    "max_rot_err_deg": float(np.max(r)), "mean_rot_err_deg": float(np.mean(r)),
-                    "max_trans_err_mm": float(np.max(t)), "mean_trans_err_mm": float(np.mean(t))}
+    seeds = [910000 + 3 * rank + i for i in range(3)]
+    out = {"workload": "c5: 640x480, 512^3 over 3 m, motion U[0,10] cm / U[0,5] deg per frame; "
+                       f"early exit {cfg0.stop_rot_rad:g} rad / {cfg0.stop_trans_mm:g} mm in both "
+                       "arms; warm pass on the finest level",
+           "seeds": seeds, "frames_per_seed": args.warm_frames - 1,
+           "data": "synthetic (held-out seeds, device renderer)",
+           "how": "per seed: median of 3 alternating device-timed passes per arm"}
+    arms = {"plain": None, "warm": weights}
+    acc = {arm: {"ms": [], "its": [], "rot": [], "trans": [], "kept": []} for arm in arms}
+    ratios = []
+    for seed in seeds:
+        cfg = dataclasses.replace(cfg0, seed=seed)
+        scene = of.make_scene(cfg.scene_kind, cfg.seed, cfg.size_mm)
+        poses = of.make_trajectory(cfg.motion, cfg.seed + 1, cfg.size_mm, args.warm_frames)
+        depth = learned.render_device(cfg, scene, poses, device=dev)
+        for arm, w in arms.items():
+            hist, its, kept, _ = run_tracker(of, cfg, depth, poses, w, timed=False)
+            r, t = pose_errors(hist[1:], poses[1:])
+            acc[arm]["its"] += list(its)
+            acc[arm]["rot"] += list(r)
+            acc[arm]["trans"] += list(t)
+            if arm == "warm":
+                acc[arm]["kept"] += list(kept == 1)
+        per = {arm: [] for arm in arms}
+        for _ in range(3):
+            for arm, w in arms.items():
+                barrier(world)
+                _, _, _, ms = run_tracker(of, cfg, depth, poses, w, timed=True)
+                per[arm].append(max_over_ranks(ms, world))
+        for arm in arms:
+            acc[arm]["ms"].append(float(np.median(per[arm])))
+        ratios.append(acc["plain"]["ms"][-1] / acc["warm"]["ms"][-1])
+    for arm in arms:
+        a = acc[arm]
+        out[arm] = {"frames_per_s": world * 1e3 / float(np.mean(a["ms"])),
+                    "frames_per_s_per_seed": [world * 1e3 / m for m in a["ms"]],
+                    "ms_per_frame": float(np.mean(a["ms"])),
+                    "mean_icp_iterations": float(np.mean(a["its"])),
+                    "max_rot_err_deg": float(np.max(a["rot"])), "mean_rot_err_deg": float(np.mean(a["rot"])),
+                    "max_trans_err_mm": float(np.max(a["trans"])), "mean_trans_err_mm": float(np.mean(a["trans"]))}
         if arm == "warm":
-            out[arm]["warm_start_kept_frac"] = float(np.mean(kept == 1))
-    out["warm_over_plain_frames_per_s"] = out["warm"]["frames_per_s"] / out["plain"]["frames_per_s"]
+            out[arm]["warm_start_kept_frac"] = float(np.mean(a["kept"]))
+    out["warm_over_plain_frames_per_s_per_seed"] = ratios
+    out["warm_over_plain_frames_per_s"] = float(np.mean(ratios))
     # the per-frame FP64 oracle comparison of both arms is a test run
     # (tests/warm_start_c5.py); its recorded summary is carried here, labelled
     rec = ROOT / "profiles" / "warm_start_c5_oracle_study.json"
