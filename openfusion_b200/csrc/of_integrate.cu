@@ -248,13 +248,24 @@ __device__ int classify_brick(const IntegrateSetup &S, const Cam &cam, const flo
   if ((tx1 - tx0 + 1) * (ty1 - ty0 + 1) > kMaxTiles) return kModeFull;
   float lmin = 3.4e38f, lmax = 0.f;
   bool dense = true;
-  for (int ty = ty0; ty <= ty1; ++ty)
-    for (int tx = tx0; tx <= tx1; ++tx) {
-      const float2 tb = __ldg(tiles + ty * tiles_x + tx);
-      lmin = fminf(lmin, tb.x);
-      lmax = fmaxf(lmax, fabsf(tb.y));
-      dense &= !signbit(tb.y);
+  // eight tiles of a row per step, their loads issued together (a near
+  // brick's footprint covers up to kMaxTiles tiles, mostly not yet in L1);
+  // the padding (3.4e38, +0) changes none of the three bounds
+  for (int ty = ty0; ty <= ty1; ++ty) {
+    const float2 *row = tiles + ty * tiles_x;
+    for (int tx = tx0; tx <= tx1; tx += 8) {
+      float2 tb[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        tb[k] = tx + k <= tx1 ? __ldg(row + tx + k) : make_float2(3.4e38f, 0.f);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        lmin = fminf(lmin, tb[k].x);
+        lmax = fmaxf(lmax, fabsf(tb[k].y));
+        dense &= !signbit(tb[k].y);
+      }
     }
+  }
   const float farb = fmaf(lmax, 1.f + 1e-5f, T + 0.05f) * (1.f + 2e-5f) + 0.02f;
   if (rlo > farb) return -1;
   const bool inside = pu0 >= 2 && pu1 <= cam.w - 3 && pv0 >= 2 && pv1 <= cam.h - 3 &&
