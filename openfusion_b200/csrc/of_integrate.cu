@@ -142,6 +142,8 @@ __device__ __forceinline__ void depth_tiles_block(const Cam &cam, const uint16_t
                                                   int bx) {
   const int tile = bx * 8 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
+  // step 2 may be launched now (it waits for this grid before reading)
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   if (bx == 0 && threadIdx.x == 0) {
     // for the next two steps: an empty work list, the frame's setup
     list_count[0] = 0;
@@ -607,6 +609,11 @@ __device__ __forceinline__ void classify_block(const of_volume_desc_t &desc, con
                                                unsigned int *__restrict__ list_count,
                                                const FrameSetup *__restrict__ setup, int bx) {
   __shared__ FrameSetup F;
+  // a programmatic launch (of_integrate_tiled outside graph capture) starts
+  // before step 1 has finished: allow step 3's launch, then wait for step 1
+  // (both are no-ops for a plain launch)
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   load_setup(setup, &F);
   const IntegrateSetup &S = F.S;
   const Plane *planes = F.planes;
@@ -690,6 +697,7 @@ __device__ __forceinline__ void integrate_list_block(uint32_t *__restrict__ vol,
   static_assert(kChunkBricks % 2 == 0, "two bricks per step of the 8 warps");
   __shared__ FrameSetup F;
   __shared__ unsigned s_chunk[2];
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // step 2's list (programmatic launch)
   load_setup(setup, &F);
   const IntegrateSetup &S = F.S;
   const unsigned n = *reinterpret_cast<volatile unsigned *>(list_count);
@@ -784,6 +792,27 @@ of_status_t launch_integrate(const of_volume_desc_t *d, void *vol, const of_came
   return of_launch_status();
 }
 
+// Launch of step 2 or 3 of of_integrate_tiled. Outside stream capture the
+// kernel is launched programmatically: its blocks may start while the
+// previous step's last blocks run and wait (griddepcontrol.wait) for that
+// grid's results, which hides the launch gap between the steps. A captured
+// step graph launches its nodes back to back already.
+template <typename... P, typename... A>
+void launch_step(void (*k)(P...), unsigned grid, cudaStream_t s, A... args) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(s, &cs);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(256);
+  cfg.stream = s;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr.val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = cs == cudaStreamCaptureStatusNone ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 of_status_t launch_integrate_tiled(const of_volume_desc_t *d, void *vol, const of_camera_t *cam,
                                    const uint16_t *depth, int pitch, const double *pose,
                                    const float *lam, void *scratch, cudaStream_t s) {
@@ -799,17 +828,20 @@ of_status_t launch_integrate_tiled(const of_volume_desc_t *d, void *vol, const o
                                               nt, list_count, pose, *d, setup);
   const size_t nb = (size_t)(d->resolution / 8);
   const unsigned nbr = (unsigned)(nb * nb * nb);
-  k_classify_bricks<<<(nbr + 255) / 256, 256, 0, s>>>(
-      *d, c, pose, tiles, tx, saturated_flags(vol, d->resolution), list, list_count, setup);
+  launch_step(k_classify_bricks, (nbr + 255) / 256, s, *d, c, (const double *)pose,
+              (const float2 *)tiles, tx, (const uint8_t *)saturated_flags(vol, d->resolution), list,
+              list_count, (const FrameSetup *)setup);
   const unsigned blocks = persistent_blocks(d);
+  const uint16_t *dp = depth;
+  const float2 *lp = (const float2 *)lam, *mp = lmap;
+  const uint4 *li = list;
+  const FrameSetup *su = setup;
   if (d->storage == OF_TSDF_I16)
-    k_integrate_list<OF_TSDF_I16><<<blocks, 256, 0, s>>>((uint32_t *)vol, *d, c, depth, pitch, pose,
-                                                         (const float2 *)lam, lmap, list,
-                                                         list_count, setup);
+    launch_step(k_integrate_list<OF_TSDF_I16>, blocks, s, (uint32_t *)vol, *d, c, dp, pitch, pose,
+                lp, mp, li, list_count, su);
   else
-    k_integrate_list<OF_TSDF_F16><<<blocks, 256, 0, s>>>((uint32_t *)vol, *d, c, depth, pitch, pose,
-                                                         (const float2 *)lam, lmap, list,
-                                                         list_count, setup);
+    launch_step(k_integrate_list<OF_TSDF_F16>, blocks, s, (uint32_t *)vol, *d, c, dp, pitch, pose,
+                lp, mp, li, list_count, su);
   return of_launch_status();
 }
 
