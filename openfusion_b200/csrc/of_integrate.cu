@@ -504,14 +504,24 @@ __device__ __forceinline__ void integrate_brick(
         }
       }
       // a warp that wrote a non-saturated voxel flags the brick and its 26
-      // neighbours, and their super-bricks (idempotent byte stores, lanes 0..26)
-      if (!CENSUS && __any_sync(0xffffffffu, near) && lane < 27) {
-        int ox = lane / 9 - 1, oy = (lane / 3) % 3 - 1, oz = lane % 3 - 1;
-        int qx = bx + ox, qy = by + oy, qz = bz + oz;
-        if ((unsigned)qx < (unsigned)nb && (unsigned)qy < (unsigned)nb && (unsigned)qz < (unsigned)nb) {
-          flags[(qx * nb + qy) * nb + qz] = 1;
-          const int ns = super_count(desc.resolution);
-          super_flags(vol, desc.resolution)[((qx / kSuper) * ns + qy / kSuper) * ns + qz / kSuper] = 1;
+      // neighbours, and their super-bricks (lanes 0..26), unless an earlier
+      // write did: bit 1 of the brick's own flag byte records that (flags are
+      // cleared only by a reset). Byte ORs into the flag words, so that the
+      // bytes come out the same in any order of the warps.
+      if (!CENSUS && __any_sync(0xffffffffu, near)) {
+        const bool done = (*reinterpret_cast<volatile uint8_t *>(flags + b) & 2u) != 0u;
+        if (!__shfl_sync(0xffffffffu, done, 0) && lane < 27) {
+          int ox = lane / 9 - 1, oy = (lane / 3) % 3 - 1, oz = lane % 3 - 1;
+          int qx = bx + ox, qy = by + oy, qz = bz + oz;
+          if ((unsigned)qx < (unsigned)nb && (unsigned)qy < (unsigned)nb && (unsigned)qz < (unsigned)nb) {
+            const unsigned q = (unsigned)((qx * nb + qy) * nb + qz);
+            const unsigned v = lane == 13 ? 3u : 1u;  // lane 13: the brick itself
+            atomicOr(reinterpret_cast<unsigned *>(flags) + (q >> 2), v << (8 * (q & 3u)));
+            const int ns = super_count(desc.resolution);
+            const unsigned s = (unsigned)(((qx / kSuper) * ns + qy / kSuper) * ns + qz / kSuper);
+            atomicOr(reinterpret_cast<unsigned *>(super_flags(vol, desc.resolution)) + (s >> 2),
+                     1u << (8 * (s & 3u)));
+          }
         }
       }
 }
