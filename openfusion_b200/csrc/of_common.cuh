@@ -146,11 +146,16 @@ __device__ __forceinline__ float2 df_add(float2 a, float2 b) {
   float lo = __fadd_rn(s.y, __fadd_rn(a.y, b.y));
   return two_sum(s.x, lo);
 }
-// sqrt of a float pair, one Newton correction.
+// sqrt of a float pair (a.x >= 0): r = a.x * rsqrt(a.x), within a few ulp,
+// then one Newton correction (a - r^2) / (2 r) from the residual, which the
+// fma forms exactly; the pair (r, correction) is within ~(ulp of r)^2 / r of
+// the root, some 1e-10 of the value.
 __device__ __forceinline__ float2 df_sqrt(float2 a) {
-  float r = __fsqrt_rn(a.x);
-  float e = __fadd_rn(__fmaf_rn(-r, r, a.x), a.y);
-  return make_float2(r, __fdiv_rn(e, 2.0f * r));
+  const float y = rsqrtf(a.x);
+  const bool pos = a.x > 0.f;
+  const float r = pos ? a.x * y : 0.f;
+  const float e = __fadd_rn(__fmaf_rn(-r, r, a.x), a.y);
+  return make_float2(r, pos ? e * (0.5f * y) : 0.f);
 }
 
 // ------------------------------------------------------------------ voxels --
