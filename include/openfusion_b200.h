@@ -359,8 +359,9 @@ typedef struct of_tracker_desc {
   /* Online tuning of the launch shapes that change no result (no reference
    * counterpart). 0: raycast.tile is used as given. k >= 1: step k times
    * every raycast block shape (of_raycast_params_t.tile) on the volume it has
-   * just fused, at its tracked pose, into a scratch model, keeps the fastest
-   * (of_tracker_tuning), and only then captures the step graphs; the steps
+   * just fused, at its tracked pose, into a scratch model (five launches each,
+   * interleaved), keeps the one with the least median time (of_tracker_tuning),
+   * and only then captures the step graphs; the steps
    * before it run without graphs and step k synchronises its stream. */
   int32_t tune;
 } of_tracker_desc_t;

@@ -14,6 +14,7 @@
 // depth-buffer parity) and replayed.
 #include "of_common.cuh"
 
+#include <algorithm>
 #include <new>
 #include <stdio.h>
 #include <string.h>
@@ -239,20 +240,23 @@ of_status_t capture(of_tracker *t, int cur, cudaGraphExec_t *out) {
   return t->up_node[cur] ? OF_OK : OF_ERR_CUDA;
 }
 
-// The online tuning (desc.tune): every raycast block shape, twice each, on
-// the volume as this step left it, at the tracked pose, into a scratch
-// pyramid (the tracker's model is left alone); CUDA events on `s`, the
-// fastest run wins. Then the step graphs are captured with the winner.
+// The online tuning (desc.tune): every raycast block shape kTuneReps times,
+// the shapes interleaved (round r times every shape once), on the volume as
+// this step left it, at the tracked pose, into a scratch pyramid (the
+// tracker's model is left alone); CUDA events on `s`. The shape with the
+// least median time wins (the shapes' times lie within a few percent of each
+// other, so one run each picks by noise). Then the step graphs are captured
+// with the winner.
 constexpr int kTuneTiles = 7;  // every shape of of_raycast_params_t.tile
-constexpr int kTuneReps = 2;
+constexpr int kTuneReps = 5;
 of_status_t tune_shapes(of_tracker *t, cudaStream_t s) {
   void *tmp = nullptr;
   cudaEvent_t ev[2 * kTuneTiles * kTuneReps] = {};
   of_status_t st = OF_OK;
   cudaError_t e = cudaMalloc(&tmp, t->lay.total_bytes);
   for (int i = 0; e == cudaSuccess && i < 2 * kTuneTiles * kTuneReps; ++i) e = cudaEventCreate(&ev[i]);
-  for (int c = 0; c < kTuneTiles && e == cudaSuccess && st == OF_OK; ++c)
-    for (int r = 0; r < kTuneReps && e == cudaSuccess && st == OF_OK; ++r) {
+  for (int r = 0; r < kTuneReps && e == cudaSuccess && st == OF_OK; ++r)
+    for (int c = 0; c < kTuneTiles && e == cudaSuccess && st == OF_OK; ++c) {
       const int i = 2 * (c * kTuneReps + r);
       of_raycast_params_t rp = t->desc.raycast;
       rp.tile = c;
@@ -265,13 +269,17 @@ of_status_t tune_shapes(of_tracker *t, cudaStream_t s) {
   if (e == cudaSuccess && st == OF_OK) e = cudaStreamSynchronize(s);
   int best = t->desc.raycast.tile;
   float best_ms = 1e30f;
-  for (int c = 0; c < kTuneTiles && e == cudaSuccess && st == OF_OK; ++c)
+  for (int c = 0; c < kTuneTiles && e == cudaSuccess && st == OF_OK; ++c) {
+    float ms[kTuneReps];
     for (int r = 0; r < kTuneReps && e == cudaSuccess; ++r) {
-      float ms = 0.f;
       const int i = 2 * (c * kTuneReps + r);
-      e = cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
-      if (e == cudaSuccess && ms < best_ms) { best_ms = ms; best = c; }
+      e = cudaEventElapsedTime(&ms[r], ev[i], ev[i + 1]);
     }
+    if (e != cudaSuccess) break;
+    std::sort(ms, ms + kTuneReps);
+    const float med = ms[kTuneReps / 2];
+    if (med < best_ms) { best_ms = med; best = c; }
+  }
   for (cudaEvent_t x : ev)
     if (x) cudaEventDestroy(x);
   if (tmp) cudaFree(tmp);
