@@ -808,9 +808,10 @@ of_status_t launch_integrate(const of_volume_desc_t *d, void *vol, const of_came
 // grid's results, which hides the launch gap between the steps. A captured
 // step graph launches its nodes back to back already.
 template <typename... P, typename... A>
-void launch_step(void (*k)(P...), unsigned grid, cudaStream_t s, A... args) {
+cudaError_t launch_step(void (*k)(P...), unsigned grid, cudaStream_t s, A... args) {
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-  cudaStreamIsCapturing(s, &cs);
+  // (a stream whose status cannot be read gets a plain launch)
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusActive;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(256);
@@ -820,7 +821,7 @@ void launch_step(void (*k)(P...), unsigned grid, cudaStream_t s, A... args) {
   attr.val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = &attr;
   cfg.numAttrs = cs == cudaStreamCaptureStatusNone ? 1 : 0;
-  cudaLaunchKernelEx(&cfg, k, args...);
+  return cudaLaunchKernelEx(&cfg, k, args...);
 }
 
 of_status_t launch_integrate_tiled(const of_volume_desc_t *d, void *vol, const of_camera_t *cam,
@@ -838,20 +839,23 @@ of_status_t launch_integrate_tiled(const of_volume_desc_t *d, void *vol, const o
                                               nt, list_count, pose, *d, setup);
   const size_t nb = (size_t)(d->resolution / 8);
   const unsigned nbr = (unsigned)(nb * nb * nb);
-  launch_step(k_classify_bricks, (nbr + 255) / 256, s, *d, c, (const double *)pose,
-              (const float2 *)tiles, tx, (const uint8_t *)saturated_flags(vol, d->resolution), list,
-              list_count, (const FrameSetup *)setup);
+  cudaError_t e = launch_step(k_classify_bricks, (nbr + 255) / 256, s, *d, c, (const double *)pose,
+                              (const float2 *)tiles, tx,
+                              (const uint8_t *)saturated_flags(vol, d->resolution), list,
+                              list_count, (const FrameSetup *)setup);
+  if (e != cudaSuccess) return of_set_cuda_error(e);
   const unsigned blocks = persistent_blocks(d);
   const uint16_t *dp = depth;
   const float2 *lp = (const float2 *)lam, *mp = lmap;
   const uint4 *li = list;
   const FrameSetup *su = setup;
   if (d->storage == OF_TSDF_I16)
-    launch_step(k_integrate_list<OF_TSDF_I16>, blocks, s, (uint32_t *)vol, *d, c, dp, pitch, pose,
-                lp, mp, li, list_count, su);
+    e = launch_step(k_integrate_list<OF_TSDF_I16>, blocks, s, (uint32_t *)vol, *d, c, dp, pitch,
+                    pose, lp, mp, li, list_count, su);
   else
-    launch_step(k_integrate_list<OF_TSDF_F16>, blocks, s, (uint32_t *)vol, *d, c, dp, pitch, pose,
-                lp, mp, li, list_count, su);
+    e = launch_step(k_integrate_list<OF_TSDF_F16>, blocks, s, (uint32_t *)vol, *d, c, dp, pitch,
+                    pose, lp, mp, li, list_count, su);
+  if (e != cudaSuccess) return of_set_cuda_error(e);
   return of_launch_status();
 }
 
