@@ -382,7 +382,7 @@ def run_ours(args, cfg, world, rank, local):
 
     # the tracker tunes its raycast block shape online at a warm-up step,
     # before its step graphs are captured (never inside the timed region)
-    tune = min(10, args.warmup) if args.warmup >= 1 else 0
+    tune = args.warmup if args.warmup >= 1 else 0
     # ---- device-resident loop: value
     tr = of.Tracker(cfg, seq.poses[0], use_graph=True, pose_history=total, tune=tune)
     tr.process(depth_dev[order[0]])
