@@ -32,12 +32,15 @@ struct RaySetup {
 // Stored tsdf of a voxel word, in storage units: q for int16 (q / 32767 is
 // the normalised tsdf), the value itself for fp16. An unobserved voxel
 // (weight 0) holds the +1 pattern (the reset and import write it), so no
-// weight test is needed. int16 without I2F: with u = q + 32768 (offset
-// binary, the low half XOR 0x8000), 1.5 * 2^23 + u is exact in FP32.
+// weight test is needed. int16 by an integer-to-float conversion (exact):
+// the raycast's integer/logic pipe is its busiest (57 % at C2) and the
+// conversion pipe its idlest (12 %), so the conversion beats the
+// mask-and-add form that runs one logic operation per corner (raycast
+// stage 115.1 -> 111.8 us, the same bits).
 template <int STORAGE>
 __device__ __forceinline__ float ray_value(uint32_t w) {
   if (STORAGE == OF_TSDF_I16)
-    return __int_as_float((w & 0xffffu) ^ 0x4B408000u) - 12615680.0f;  // 1.5 * 2^23 + 2^15
+    return __int2float_rn((int)(short)(w & 0xffffu));
   else
     return __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
 }
