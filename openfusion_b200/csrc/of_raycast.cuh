@@ -49,6 +49,12 @@ constexpr float ray_scale() {
   return STORAGE == OF_TSDF_I16 ? 1.0f / kQ : 1.0f;
 }
 
+// floor(g) clamped to [0, n-2]: the unsigned conversion saturates negative
+// values (and NaN) to 0 itself, which leaves one integer min.
+__device__ __forceinline__ int cell_index(float g, int n) {
+  return (int)min(__float2uint_rd(g), (unsigned)(n - 2));
+}
+
 // Trilinear tsdf at a world position. Corner (i0, j0, k0) is clamped to
 // [0, n-2]; the seven other corners are the base address plus an axis step
 // that crosses into the next brick when the local coordinate is 7. Volume
@@ -60,9 +66,7 @@ __device__ __forceinline__ float trilinear(const uint32_t *__restrict__ vol, int
   float gx = fmaf(px - org, inv_vs, -0.5f);
   float gy = fmaf(py - org, inv_vs, -0.5f);
   float gz = fmaf(pz - org, inv_vs, -0.5f);
-  int ix = min(max(__float2int_rd(gx), 0), n - 2);
-  int iy = min(max(__float2int_rd(gy), 0), n - 2);
-  int iz = min(max(__float2int_rd(gz), 0), n - 2);
+  int ix = cell_index(gx, n), iy = cell_index(gy, n), iz = cell_index(gz, n);
   float fx = gx - (float)ix, fy = gy - (float)iy, fz = gz - (float)iz;
   if (cell) *cell = make_int3(ix, iy, iz);
   unsigned base = ((((unsigned)(ix >> 3) * nb + (unsigned)(iy >> 3)) * nb + (unsigned)(iz >> 3)) << 9) |
@@ -252,9 +256,9 @@ __device__ __forceinline__ void raycast_pixel(const uint32_t *__restrict__ vol,
     for (int it = 0; it < (1 << 16); ++it) {
       if (!have_cell) {
         const float px = fmaf(t, dir.x, ox), py = fmaf(t, dir.y, oy), pz = fmaf(t, dir.z, oz);
-        cell.x = min(max(__float2int_rd(fmaf(px - org, inv_vs, -0.5f)), 0), n - 2);
-        cell.y = min(max(__float2int_rd(fmaf(py - org, inv_vs, -0.5f)), 0), n - 2);
-        cell.z = min(max(__float2int_rd(fmaf(pz - org, inv_vs, -0.5f)), 0), n - 2);
+        cell.x = cell_index(fmaf(px - org, inv_vs, -0.5f), n);
+        cell.y = cell_index(fmaf(py - org, inv_vs, -0.5f), n);
+        cell.z = cell_index(fmaf(pz - org, inv_vs, -0.5f), n);
       }
       have_cell = false;
       const int bi = cell.x >> 3, bj = cell.y >> 3, bk = cell.z >> 3;
