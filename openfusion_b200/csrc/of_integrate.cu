@@ -326,13 +326,15 @@ __device__ __forceinline__ float3 brick_base(const IntegrateSetup &S, int bx, in
 // with tsdf' = +1 when its pixel holds a valid depth (always, when dense),
 // with no ray length or distance evaluated; kModeInside drops the per-voxel
 // frustum checks.
-template <int STORAGE, int CENSUS, bool EARLY_LOAD = false, bool LMAP = false>
+template <int STORAGE, int CENSUS, bool EARLY_LOAD = false, bool LMAP = false, int MODE = -1>
 __device__ __forceinline__ void integrate_brick(
     uint32_t *__restrict__ vol, uint8_t *__restrict__ flags, const of_volume_desc_t &desc,
     const Cam &cam, const uint16_t *__restrict__ depth, int pitch,
     const float2 *__restrict__ lam, const IntegrateSetup &S, const VoxelConsts &K, int t,
-    int lane, int b, int bx, int by, int bz, int mode, float3 base, unsigned &my_count,
+    int lane, int b, int bx, int by, int bz, int mode_arg, float3 base, unsigned &my_count,
     int sat_old = -1, const float2 *__restrict__ lmap = nullptr) {
+  // the brick's mode, a constant when the caller instantiates one per mode
+  const int mode = MODE >= 0 ? MODE : mode_arg;
   const float T = K.T, inv_T = K.inv_T, dspan = K.dspan, cxh = K.cxh, cyh = K.cyh;
   const float dlo = K.dlo, dhi = K.dhi;
   const unsigned uspan = K.uspan, vspan = K.vspan;
@@ -732,10 +734,22 @@ __device__ __forceinline__ void integrate_list_block(uint32_t *__restrict__ vol,
       const int bz = (int)((en.x >> 16) & 0xffu), mode = (int)((en.x >> 24) & 3u);
       const int sat_old = (int)((en.x >> 26) & 0xfu);
       const int b = (bx * nb + by) * nb + bz;
-      integrate_brick<STORAGE, 0, true, true>(
-          vol, flags, desc, cam, depth, pitch, lam, S, K, t, lane, b, bx, by, bz, mode,
-          make_float3(__uint_as_float(en.y), __uint_as_float(en.z), __uint_as_float(en.w)),
-          my_count, sat_old, lmap);
+      const float3 base =
+          make_float3(__uint_as_float(en.y), __uint_as_float(en.z), __uint_as_float(en.w));
+      // (the mode is the same for the whole warp: one instantiation each for
+      // the two per-voxel modes, whose tests it fixes)
+      if (mode == kModeInside)
+        integrate_brick<STORAGE, 0, true, true, kModeInside>(vol, flags, desc, cam, depth, pitch,
+                                                              lam, S, K, t, lane, b, bx, by, bz,
+                                                              mode, base, my_count, sat_old, lmap);
+      else if (mode == kModeFull)
+        integrate_brick<STORAGE, 0, true, true, kModeFull>(vol, flags, desc, cam, depth, pitch,
+                                                            lam, S, K, t, lane, b, bx, by, bz,
+                                                            mode, base, my_count, sat_old, lmap);
+      else
+        integrate_brick<STORAGE, 0, true, true>(vol, flags, desc, cam, depth, pitch, lam, S, K, t,
+                                                lane, b, bx, by, bz, mode, base, my_count,
+                                                sat_old, lmap);
     }
     if (threadIdx.x == 0) s_chunk[buf] = nxt;
     __syncthreads();
