@@ -82,7 +82,7 @@ __device__ __forceinline__ float ex2_approx(float x) {
 // difference overflows to +inf and their weight 2^-inf is exactly 0, so no
 // per-tap select is needed. One ex2 per tap.
 // (tile (bx, by) of the image; the kernels below pass their block index)
-template <int R>
+template <int R, bool UNROLL_ROWS>
 __device__ __forceinline__ void bilateral_tile(const uint16_t *__restrict__ depth, int pitch,
                                                int w, int h, float dmin, float dmax, float ks,
                                                float kr, float *__restrict__ out, int bx, int by) {
@@ -111,8 +111,9 @@ __device__ __forceinline__ void bilateral_tile(const uint16_t *__restrict__ dept
   if (c > 0.f) {
     const float nkr = -kr;
     float sw = 0.f, sd = 0.f;
-#pragma unroll
-    for (int dy = -R; dy <= R; ++dy) {
+    // single-stream filter: rows not unrolled (32 registers a thread, see
+    // filter_footprint); the batched one unrolls them (the same sums)
+    auto row = [&](int dy) {
       const float ry = -(float)(dy * dy) * ks;
 #pragma unroll
       for (int dx = -R; dx <= R; ++dx) {
@@ -123,6 +124,13 @@ __device__ __forceinline__ void bilateral_tile(const uint16_t *__restrict__ dept
         sw += wt;
         sd = fmaf(wt, q, sd);
       }
+    };
+    if (UNROLL_ROWS) {
+#pragma unroll
+      for (int dy = -R; dy <= R; ++dy) row(dy);
+    } else {
+#pragma unroll 1
+      for (int dy = -R; dy <= R; ++dy) row(dy);
     }
     result = sd / sw;
   }
@@ -133,7 +141,7 @@ template <int R>
 __global__ void __launch_bounds__(256) k_bilateral_r(const uint16_t *__restrict__ depth, int pitch,
                                                      int w, int h, float dmin, float dmax,
                                                      float ks, float kr, float *__restrict__ out) {
-  bilateral_tile<R>(depth, pitch, w, h, dmin, dmax, ks, kr, out, blockIdx.x, blockIdx.y);
+  bilateral_tile<R, false>(depth, pitch, w, h, dmin, dmax, ks, kr, out, blockIdx.x, blockIdx.y);
 }
 
 // No filter: the raw depth as float, invalid -> 0 (the reference converts the
@@ -255,9 +263,41 @@ __global__ void __launch_bounds__(256) k_bilateral_batch(const FilterJob *__rest
   const int j = batch_job(first, n, blockIdx.x);
   const FilterJob &J = jobs[j];
   const int b = blockIdx.x - __ldg(first + j);
-  bilateral_tile<R>(J.depth[parity], J.pitch, J.w, J.h, J.dmin, J.dmax, ks, kr, J.out, b % J.gx,
+  bilateral_tile<R, true>(J.depth[parity], J.pitch, J.w, J.h, J.dmin, J.dmax, ks, kr, J.out, b % J.gx,
                     b / J.gx);
 }
+// The single-stream filter runs on the step graph's pre-processing branch, at
+// the lower stream priority, beside the integration and the raycast. A block of it that
+// sits on an SM holds registers and threads that their blocks then wait for,
+// so the filter keeps a small footprint: 32 registers a thread and at most
+// kFilterBlocksPerSm blocks per SM, set by a reservation of dynamic shared
+// memory that the kernel leaves unused. Measured at C2 (300 frames, alternating
+// runs on one B200): fully unrolled rows (128 registers, two blocks filling
+// the register file) 2956 / 2903-2916 frames/s (value / e2e); 32 registers
+// and two blocks per SM 3008 / 2941-2946; three per SM 2964-2967; one per SM
+// gained `value` but lost `e2e` (the branch then took 108 us); 32 registers
+// with no cap (eight per SM) lost 3 %. The filtered depth is the same bits.
+// (The batched filter keeps the unrolled rows and no cap: capped the same way
+// it lost 5 % of the 64-stream batch's frames/s.)
+constexpr int kFilterBlocksPerSm = 2;
+template <typename Kernel>
+cudaError_t filter_footprint(Kernel *k, size_t *dyn) {
+  int dev = 0, smem_sm = 0, reserved = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+  cudaFuncAttributes fa = {};
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, (const void *)k);
+  if (e != cudaSuccess) return e;
+  long d = (long)smem_sm / kFilterBlocksPerSm - (long)fa.sharedSizeBytes - reserved;
+  if (d < 0) d = 0;
+  *dyn = (size_t)d;
+  // (set on every call: the attribute belongs to the current context)
+  return cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d);
+}
+
 __global__ void k_depth_raw_batch(const FilterJob *__restrict__ jobs, const int *__restrict__ first,
                                   int n, int parity) {
   const int j = batch_job(first, n, blockIdx.x);
@@ -401,7 +441,11 @@ of_status_t preprocess_batch_launch(const PreprocessBatch *b, int parity, cudaSt
     k_depth_raw_batch<<<b->filter_blocks, dim3(32, 8), 0, s>>>(b->filter, b->filter_first, b->n,
                                                                parity);
   } else {
-#define OF_BILATERAL_BATCH(RR)                                                                 case RR:                                                                                       k_bilateral_batch<RR><<<b->filter_blocks, kTileX * kTileY, 0, s>>>(                              b->filter, b->filter_first, b->n, parity, b->ks, b->kr);                                 break;
+#define OF_BILATERAL_BATCH(RR)                                                          \
+  case RR:                                                                              \
+    k_bilateral_batch<RR><<<b->filter_blocks, kTileX * kTileY, 0, s>>>(                 \
+        b->filter, b->filter_first, b->n, parity, b->ks, b->kr);                        \
+    break;
     switch (b->radius) {
       OF_BILATERAL_BATCH(3)
       OF_BILATERAL_BATCH(4)
@@ -456,11 +500,14 @@ extern "C" of_status_t of_preprocess(const of_camera_t *cam, const of_filter_par
     float *o = (float *)(base + lay.depth_offset[0]);
     const int W = cam->width, H = cam->height;
     const float dmn = cam->min_depth_mm, dmx = cam->max_depth_mm;
-#define OF_BILATERAL_CASE(RR)                                                              \
-  case RR:                                                                                 \
-    k_bilateral_r<RR><<<grid, kTileX * kTileY, 0, s>>>(d_depth, pitch, W, H, dmn, dmx, ks, \
-                                                        kr, o);                           \
-    break;
+#define OF_BILATERAL_CASE(RR)                                                           \
+  case RR: {                                                                            \
+    size_t dyn_ = 0;                                                                    \
+    const cudaError_t fe_ = filter_footprint(k_bilateral_r<RR>, &dyn_);                 \
+    if (fe_ != cudaSuccess) return of_set_cuda_error(fe_);                              \
+    k_bilateral_r<RR><<<grid, kTileX * kTileY, dyn_, s>>>(d_depth, pitch, W, H, dmn, dmx, \
+                                                           ks, kr, o);                  \
+  } break;
     switch (R) {
       OF_BILATERAL_CASE(3)
       OF_BILATERAL_CASE(4)
