@@ -36,6 +36,7 @@ FP32 OpenMP build of the oracle restatement) on the host cores.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import subprocess
@@ -370,7 +371,6 @@ def run_ours(args, cfg, world, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     if rank:
-        import dataclasses
         cfg = dataclasses.replace(cfg, seed=cfg.seed + 7919 * rank)
     seq = of.make_sequence(cfg, frames=args.frames)
     n_seq = len(seq.depth)
@@ -380,8 +380,8 @@ def run_ours(args, cfg, world, rank, local):
     depth_host = torch.from_numpy(seq.depth.astype(np.int16)).pin_memory()
     stream = torch.cuda.current_stream(dev)
 
-    # the tracker tunes its raycast block shape online at a warm-up step,
-    # before its step graphs are captured (never inside the timed region)
+    # the tracker tunes its raycast block shape online at the last warm-up
+    # step, before its step graphs are captured (never inside the timed region)
     tune = args.warmup if args.warmup >= 1 else 0
     # ---- device-resident loop: value
     tr = of.Tracker(cfg, seq.poses[0], use_graph=True, pose_history=total, tune=tune)
@@ -446,7 +446,6 @@ def run_ours(args, cfg, world, rank, local):
 
     # ---- per-stage kernel times (stage-wise launches with CUDA events), with
     # the raycast block shape the tracker chose
-    import dataclasses
     stages = stage_times(of, dataclasses.replace(cfg, ray_tile=ray_tile), seq, depth_dev, order,
                          args, dev)
 
@@ -544,7 +543,6 @@ def warm_start_comparison(of, args, dev, world, rank):
     gives ICP iterations and pose error against the ground truth, then three
     rounds of device-timed passes (CUDA events, max over ranks) alternate the
     arms; a seed's frames/s are the median of its rounds."""
-    import dataclasses
     from openfusion_b200 import learned
     from openfusion_b200.train_warm_start import eval_config, pose_errors, run_tracker
     cfg0 = eval_config(of)
