@@ -155,7 +155,7 @@ def main(argv=None):
         def rms(a):
             return float(np.sqrt(np.mean(np.sum(a ** 2, axis=1))))
         weights = net.weights()
-        out = a.out or (root / "gpurun_out" / "warm_start_c5.npy")
+        out = a.out or Path("warm_start_c5.npy")  # (the working directory by default)
         out.parent.mkdir(parents=True, exist_ok=True)
         np.save(out, weights)
         info = {"pairs": int(x.shape[0]), "sequences": seqs, "data_s": t1 - t0,
